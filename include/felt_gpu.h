@@ -1,0 +1,160 @@
+/* felt_gpu.h - C ABI of the B200 (sm_100a) sparse-field level-set engine.
+ *
+ * This is the thin boundary under the C++ facade felt_b200/include/felt_gpu/surface.hpp, which
+ * mirrors the Felt reference API (Felt::Surface<D,L>, Felt::Polys<S>). Every entry point below
+ * replaces one reference member function; the reference file:line is given beside each one
+ * (paths relative to the feltech/Felt source tree). No C++ or torch types cross this boundary:
+ * plain pointers, sizes and int status codes (0 = OK, negative = error; fg_last_error() gives
+ * the message of the calling thread's last failure). No exceptions cross it.
+ *
+ * Device memory is owned by the handles; host buffers passed in are owned by the caller.
+ * Calls on one handle are issued to that handle's CUDA stream; query calls synchronise it.
+ * One host thread per handle at a time.
+ *
+ * Naming: "layer index" is the reference's TupleIdx layer_idx = layer_id + L, in [0, 2L].
+ * Partition indices are row-major (last axis fastest) over the children grid, as in the
+ * reference (include/Felt/Impl/Util.hpp:23-40); leaf indices are row-major within a partition.
+ */
+#ifndef FELT_GPU_H
+#define FELT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+enum {
+	FG_OK = 0,
+	FG_ERR_ARG = -1,        /* invalid argument or handle                                   */
+	FG_ERR_CUDA = -2,       /* CUDA runtime failure (no device, launch failure, ...)        */
+	FG_ERR_NOMEM = -3,      /* device or host allocation failed                             */
+	FG_ERR_POOL = -4,       /* brick pool exhausted (raise fg_config.brick_capacity)        */
+	FG_ERR_NONFINITE = -10, /* a layer id was taken of NaN/inf (reference: iround throws)   */
+	FG_ERR_OUTSIDE = -11,   /* a band node would be tracked outside the grid                */
+	FG_ERR_INACTIVE = -12,  /* write to an inactive partition (reference: undefined)        */
+	FG_ERR_CAPACITY = -13,  /* an output buffer or geometry arena is too small              */
+	FG_ERR_TIMEOUT = -14,   /* a bounded device wait gave up                                 */
+	FG_ERR_STATE = -15      /* call out of sequence (e.g. update_end without update_start)  */
+};
+
+/* ---- builtin speed functors ----
+ * delta(pos) = [a * curv(pos)] + [n * h(pos, seed)] + [c], each bracket present when its flag
+ * is set, summed left to right in FP32. curv is the reference's difference-of-normals mean
+ * curvature (include/Felt/Impl/Mixin/NumericMixin.hpp:72-156); h is a fixed 32-bit integer hash
+ * of (pos, seed) mapped exactly to [-1, 1). */
+enum { FG_SPEED_CONST = 1, FG_SPEED_CURV = 2, FG_SPEED_NOISE = 4 };
+typedef struct fg_speed {
+	int kind;      /* OR of FG_SPEED_* */
+	float c;       /* constant term */
+	float a;       /* curvature coefficient */
+	float n;       /* noise coefficient */
+	uint32_t seed; /* noise seed */
+} fg_speed;
+
+typedef struct fg_config {
+	size_t brick_capacity; /* bricks (partitions) the device pool can hold; 0 = automatic   */
+	size_t vertex_capacity;/* polygonisation arena, vertices; 0 = automatic                 */
+	int use_graph;         /* capture the global update step as a CUDA graph when nonzero   */
+	int reserved[7];
+} fg_config;
+
+typedef struct fg_surface fg_surface;
+typedef struct fg_polys fg_polys;
+typedef struct fg_batch fg_batch;
+
+const char* fg_last_error(void);
+
+/* Surface(size, size_partition) (include/Felt/Surface.hpp:163-173). dims in {2,3},
+ * layers (L) in {1,2,3,4}; size and part hold `dims` ints. cfg may be NULL. */
+int fg_surface_create(int dims, int layers, const int* size, const int* part,
+                      const fg_config* cfg, fg_surface** out);
+int fg_surface_destroy(fg_surface* s);
+
+/* seed(pos) (include/Felt/Surface.hpp:207-241). */
+int fg_seed(fg_surface* s, const int* pos);
+
+/* update(fn) with a builtin speed functor (include/Felt/Surface.hpp:254-296). */
+int fg_update_builtin(fg_surface* s, const fg_speed* speed);
+
+/* update(fn) with a caller-supplied device functor: the facade's templated delta kernel,
+ * compiled in the caller's nvcc translation unit, runs between these two calls.
+ * fg_update_begin_global performs update_start() and the delta track_children step
+ * (include/Felt/Surface.hpp:257-263) and returns the device view the kernel needs;
+ * fg_update_finish_global runs update_end_global() (include/Felt/Surface.hpp:739-762). */
+typedef struct fg_device_view fg_device_view; /* defined in felt_gpu/device.cuh */
+int fg_update_begin_global(fg_surface* s, const fg_device_view** view, void** stream);
+int fg_update_finish_global(fg_surface* s);
+
+/* update(lo, hi, fn) bounded update with a builtin speed (include/Felt/Surface.hpp:310-386). */
+int fg_update_bounded(fg_surface* s, const int* lo, const int* hi, const fg_speed* speed);
+
+/* update_start() (include/Felt/Surface.hpp:393-399), delta(pos, val) (441-459) and
+ * update_end() (404-430): the local update. fg_delta_n applies n deltas in order. */
+int fg_update_start(fg_surface* s);
+int fg_delta(fg_surface* s, const int* pos, float val);
+int fg_delta_n(fg_surface* s, const int* pos, const float* val, size_t n);
+int fg_update_end(fg_surface* s);
+
+/* isogrid().snapshot() (include/Felt/Impl/Mixin/PartitionedMixin.hpp:642-660): dense grid,
+ * row-major over the whole isogrid. dst holds n >= prod(size) floats, on the host or, when
+ * dst_is_device, in device memory of the surface's GPU. */
+int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device);
+
+/* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */
+int fg_get(fg_surface* s, const int* pos, float* out);
+
+/* Geometry of the children (partition) grid: count, size and offset of the children grid. */
+int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);
+
+/* isogrid().children().get(p).lookup().list(layer_idx) (LookupMixin.hpp:261-275): the ordered
+ * leaf list of one partition. Writes min(n, cap) entries, returns the full count in *n. */
+int fg_layer_list(fg_surface* s, size_t part, int layer_idx, uint32_t* out, size_t cap,
+                  size_t* n);
+
+/* isogrid().children().lookup().list(layer_idx) (PartitionedMixin.hpp:104-115): ordered list
+ * of partitions tracked in a layer. */
+int fg_partition_list(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+
+/* delta(layer_idx) (include/Felt/Surface.hpp:637-640) and status_change(layer_idx) (648-651):
+ * partitions touched by the last update. */
+int fg_delta_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+int fg_status_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+
+/* children().get(p).is_active() and background() (GridMixin.hpp:56-69). */
+int fg_partition_state(fg_surface* s, size_t part, int* active, float* background);
+
+/* stats() (include/Felt/Surface.hpp:623-629). */
+int fg_stats(fg_surface* s, size_t* active_isogrid_partitions, size_t* active_delta_partitions);
+
+/* Narrow-band node count at the start of the last update: sum over the 2L+1 layers. */
+int fg_band_size(fg_surface* s, size_t* n);
+
+/* Canonical state encoding used by parity tests (uint32 words):
+ *   D, L, P (partition count);
+ *   per partition: active, background (float bits), then per layer: n, n leaf indices;
+ *   per layer: isogrid partition list (n, entries);
+ *   per layer: delta partition list; per layer: status-change partition list.
+ * Writes min(total, cap) words and the full word count in *n. */
+int fg_dump(fg_surface* s, uint32_t* out, size_t cap, size_t* n);
+
+/* ---- Polys<Surface> (include/Felt/Polys.hpp) ---- */
+int fg_polys_create(fg_surface* s, fg_polys** out);   /* Polys.hpp:58-84   */
+int fg_polys_destroy(fg_polys* p);
+int fg_polys_notify(fg_polys* p);                       /* Polys.hpp:92-133  */
+int fg_polys_march(fg_polys* p);                        /* Polys.hpp:138-165 */
+int fg_polys_invalidate(fg_polys* p);                   /* Polys.hpp:171-191 */
+int fg_polys_changes(fg_polys* p, uint32_t* out, size_t cap, size_t* n); /* Polys.hpp:198-201 */
+/* children().get(part).{vtxs(),spxs(),is_active()} (Poly.hpp:155-186). vtx receives per vertex
+ * D position floats then, in 3D, D normal floats; spx receives D uint32 indices per simplex. */
+int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_cap, uint32_t* spx,
+                       size_t spx_cap, size_t* nv, size_t* ns, int* active);
+/* Totals over all partitions. */
+int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,443 @@
+// C ABI over the CPU oracle (felt_oracle.hpp), mirroring include/felt_gpu.h with an `fo_`
+// prefix so that tests can drive the oracle and the device engine through identical call
+// sequences and compare their dumps. TEST INFRASTRUCTURE ONLY.
+#include "felt_oracle.hpp"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+
+namespace {
+
+thread_local std::string g_err;
+
+struct SurfBase {
+	int dims = 0, layers = 0;
+	virtual ~SurfBase() = default;
+	virtual void seed(const int* p) = 0;
+	virtual void update(const fo::Speed& s) = 0;
+	virtual void update_bounded(const int* lo, const int* hi, const fo::Speed& s) = 0;
+	virtual void update_start() = 0;
+	virtual void delta(const int* p, float v) = 0;
+	virtual void update_end() = 0;
+	virtual void snapshot(float* dst, size_t n) = 0;
+	virtual float get(const int* p) = 0;
+	virtual size_t nparts() = 0;
+	virtual void partitions(int* csize, int* coff) = 0;
+	virtual const std::vector<size_t>* leaf_list(size_t part, int l) = 0;
+	virtual const std::vector<size_t>* plist(int which, int l) = 0;
+	virtual void pstate(size_t part, int* active, float* bg) = 0;
+	virtual void stats(size_t* a, size_t* b) = 0;
+	virtual size_t band_size() = 0;
+	virtual void curv(const int* p, float* out) = 0;
+};
+
+struct PolysBase {
+	virtual ~PolysBase() = default;
+	virtual void notify() = 0;
+	virtual void march() = 0;
+	virtual void invalidate() = 0;
+	virtual void march_partition(size_t pc) = 0;
+	virtual const std::vector<size_t>& changes() = 0;
+	virtual void part(size_t pc, float* vtx, size_t vcap, uint32_t* spx, size_t scap, size_t* nv,
+	                  size_t* ns, int* active) = 0;
+	virtual void totals(size_t* nv, size_t* ns) = 0;
+};
+
+template <int D, int L>
+struct Surf : SurfBase {
+	fo::Surface<D, L, float> s;
+	static fo::Vi<D> v(const int* p)
+	{
+		fo::Vi<D> r;
+		for (int a = 0; a < D; a++) r[a] = p[a];
+		return r;
+	}
+	Surf(const int* size, const int* part) : s(v(size), v(part))
+	{
+		this->dims = D;
+		this->layers = L;
+	}
+	void seed(const int* p) override { s.seed(v(p)); }
+	void update(const fo::Speed& sp) override { s.update(sp); }
+	void update_bounded(const int* lo, const int* hi, const fo::Speed& sp) override
+	{
+		s.update_bounded(v(lo), v(hi), sp);
+	}
+	void update_start() override { s.update_start(); }
+	void delta(const int* p, float val) override { s.delta(v(p), val); }
+	void update_end() override { s.update_end(); }
+	void snapshot(float* dst, size_t n) override
+	{
+		// PartitionedMixin.hpp:642-660: row-major over the grid, each node via get().
+		fo::Vi<D> size = s.iso.size, off = s.iso.off;
+		size_t tot = 1;
+		for (int a = 0; a < D; a++) tot *= size_t(size[a]);
+		if (n < tot) throw fo::Error(-13, "snapshot buffer too small");
+		for (size_t i = 0; i < tot; i++) dst[i] = s.iso.get(fo::pos_of<D>(i, size, off));
+	}
+	float get(const int* p) override { return s.iso.get(v(p)); }
+	size_t nparts() override { return s.iso.nchildren(); }
+	void partitions(int* csize, int* coff) override
+	{
+		for (int a = 0; a < D; a++) {
+			csize[a] = s.iso.ccount[a];
+			coff[a] = s.iso.coff[a];
+		}
+	}
+	const std::vector<size_t>* leaf_list(size_t part, int l) override
+	{
+		return &s.iso.ch[part].lists[l];
+	}
+	const std::vector<size_t>* plist(int which, int l) override
+	{
+		switch (which) {
+		case 0: return &s.iso.clists[l];
+		case 1: return &s.delta_.clists[l];
+		case 2: return &s.status.clists[l];
+		case 3: return &s.aff.clists[l];
+		default: return nullptr;
+		}
+	}
+	void pstate(size_t part, int* active, float* bg) override
+	{
+		*active = s.iso.active(part) ? 1 : 0;
+		*bg = s.iso.ch[part].bg;
+	}
+	void stats(size_t* a, size_t* b) override
+	{
+		*a = s.num_active(s.iso);
+		*b = s.num_active(s.delta_);
+	}
+	size_t band_size() override
+	{
+		size_t n = 0;
+		for (int l = 0; l < 2 * L + 1; l++)
+			for (size_t pc : s.iso.clists[l]) n += s.iso.ch[pc].lists[l].size();
+		return n;
+	}
+	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
+};
+
+template <int D, int L>
+struct PolysImpl : PolysBase {
+	fo::Polys<D, L> p;
+	explicit PolysImpl(const fo::Surface<D, L, float>& s) : p(s) {}
+	void notify() override { p.notify(); }
+	void march() override { p.march(); }
+	void invalidate() override { p.invalidate(); }
+	void march_partition(size_t pc) override { p.march_partition(pc); }
+	const std::vector<size_t>& changes() override { return p.changes(); }
+	void part(size_t pc, float* vtx, size_t vcap, uint32_t* spx, size_t scap, size_t* nv,
+	          size_t* ns, int* active) override
+	{
+		const auto& c = p.ch[pc];
+		*nv = c.vtxs.size();
+		*ns = c.spxs.size();
+		*active = c.active() ? 1 : 0;
+		const size_t per = (D == 3) ? 2 * D : D;
+		for (size_t i = 0; i < c.vtxs.size() && (i + 1) * per <= vcap; i++) {
+			for (int a = 0; a < D; a++) vtx[i * per + a] = c.vtxs[i].pos[a];
+			if (D == 3)
+				for (int a = 0; a < D; a++) vtx[i * per + D + a] = c.vtxs[i].norm[a];
+		}
+		for (size_t i = 0; i < c.spxs.size() && (i + 1) * D <= scap; i++)
+			for (int a = 0; a < D; a++) spx[i * D + a] = c.spxs[i][a];
+	}
+	void totals(size_t* nv, size_t* ns) override
+	{
+		*nv = 0;
+		*ns = 0;
+		for (const auto& c : p.ch) {
+			*nv += c.vtxs.size();
+			*ns += c.spxs.size();
+		}
+	}
+};
+
+struct PolysHandle {
+	std::unique_ptr<PolysBase> impl;
+};
+
+template <class F>
+int guard(F&& f)
+{
+	try {
+		f();
+		return 0;
+	} catch (const fo::Error& e) {
+		g_err = e.what();
+		return e.code;
+	} catch (const std::exception& e) {
+		g_err = e.what();
+		return -1;
+	}
+}
+
+SurfBase* make(int D, int L, const int* size, const int* part)
+{
+#define FO_CASE(d, l) \
+	if (D == d && L == l) return new Surf<d, l>(size, part);
+	FO_CASE(2, 1) FO_CASE(2, 2) FO_CASE(2, 3) FO_CASE(2, 4)
+	FO_CASE(3, 1) FO_CASE(3, 2) FO_CASE(3, 3) FO_CASE(3, 4)
+#undef FO_CASE
+	return nullptr;
+}
+
+PolysBase* make_polys(SurfBase* s)
+{
+#define FO_CASE(d, l) \
+	if (s->dims == d && s->layers == l) return new PolysImpl<d, l>(static_cast<Surf<d, l>*>(s)->s);
+	FO_CASE(2, 1) FO_CASE(2, 2) FO_CASE(2, 3) FO_CASE(2, 4)
+	FO_CASE(3, 1) FO_CASE(3, 2) FO_CASE(3, 3) FO_CASE(3, 4)
+#undef FO_CASE
+	return nullptr;
+}
+
+fo::Speed to_speed(const int kind, const float c, const float a, const float n, uint32_t seed)
+{
+	return fo::Speed{kind, c, a, n, seed};
+}
+
+void put_list(const std::vector<size_t>& l, uint32_t* out, size_t cap, size_t* n)
+{
+	*n = l.size();
+	for (size_t i = 0; i < l.size() && i < cap; i++) out[i] = uint32_t(l[i]);
+}
+
+}  // namespace
+
+extern "C" {
+
+struct fo_speed {
+	int kind;
+	float c, a, n;
+	uint32_t seed;
+};
+
+const char* fo_last_error(void) { return g_err.c_str(); }
+
+int fo_surface_create(int dims, int layers, const int* size, const int* part, void** out)
+{
+	return guard([&] {
+		SurfBase* s = make(dims, layers, size, part);
+		if (!s) throw fo::Error(-1, "unsupported dims/layers");
+		*out = s;
+	});
+}
+int fo_surface_destroy(void* s)
+{
+	delete static_cast<SurfBase*>(s);
+	return 0;
+}
+int fo_seed(void* s, const int* pos)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->seed(pos); });
+}
+int fo_update_builtin(void* s, const fo_speed* sp)
+{
+	return guard([&] {
+		static_cast<SurfBase*>(s)->update(to_speed(sp->kind, sp->c, sp->a, sp->n, sp->seed));
+	});
+}
+int fo_update_bounded(void* s, const int* lo, const int* hi, const fo_speed* sp)
+{
+	return guard([&] {
+		static_cast<SurfBase*>(s)->update_bounded(lo, hi,
+		                                         to_speed(sp->kind, sp->c, sp->a, sp->n, sp->seed));
+	});
+}
+int fo_update_start(void* s)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->update_start(); });
+}
+int fo_delta(void* s, const int* pos, float v)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->delta(pos, v); });
+}
+int fo_delta_n(void* s, const int* pos, const float* v, size_t n)
+{
+	return guard([&] {
+		SurfBase* b = static_cast<SurfBase*>(s);
+		for (size_t i = 0; i < n; i++) b->delta(pos + i * size_t(b->dims), v[i]);
+	});
+}
+int fo_update_end(void* s)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->update_end(); });
+}
+int fo_snapshot(void* s, float* dst, size_t n)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->snapshot(dst, n); });
+}
+int fo_get(void* s, const int* pos, float* out)
+{
+	return guard([&] { *out = static_cast<SurfBase*>(s)->get(pos); });
+}
+int fo_curv(void* s, const int* pos, float* out)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->curv(pos, out); });
+}
+/* curv over a dense grid (values row-major, `bg` outside), for the stencil golden tests. */
+int fo_curv_dense(int dims, const float* vals, const int* size, const int* off, float bg,
+                  const int* pos, float* out)
+{
+	return guard([&] {
+		auto run = [&](auto dtag) {
+			constexpr int D = decltype(dtag)::value;
+			fo::Vi<D> sz, of, hi, p;
+			for (int a = 0; a < D; a++) {
+				sz[a] = size[a];
+				of[a] = off[a];
+				hi[a] = off[a] + size[a];
+				p[a] = pos[a];
+			}
+			auto get = [&](const fo::Vi<D>& q) {
+				if (!fo::inside<D>(q, of, hi)) return bg;
+				return vals[fo::index_of<D>(q, sz, of)];
+			};
+			*out = fo::curv_at<D, float>(get, p);
+		};
+		if (dims == 2)
+			run(std::integral_constant<int, 2>{});
+		else if (dims == 3)
+			run(std::integral_constant<int, 3>{});
+		else
+			throw fo::Error(-1, "dims");
+	});
+}
+int fo_partitions(void* s, size_t* count, int* csize, int* coff)
+{
+	return guard([&] {
+		*count = static_cast<SurfBase*>(s)->nparts();
+		static_cast<SurfBase*>(s)->partitions(csize, coff);
+	});
+}
+int fo_layer_list(void* s, size_t part, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(*static_cast<SurfBase*>(s)->leaf_list(part, l), out, cap, n); });
+}
+int fo_partition_list(void* s, int which, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(*static_cast<SurfBase*>(s)->plist(which, l), out, cap, n); });
+}
+int fo_partition_state(void* s, size_t part, int* active, float* bg)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->pstate(part, active, bg); });
+}
+int fo_stats(void* s, size_t* a, size_t* b)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->stats(a, b); });
+}
+int fo_band_size(void* s, size_t* n)
+{
+	return guard([&] { *n = static_cast<SurfBase*>(s)->band_size(); });
+}
+
+/* Canonical dump; same encoding as fg_dump in include/felt_gpu.h. */
+int fo_dump(void* sv, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		SurfBase* s = static_cast<SurfBase*>(sv);
+		const int NL = 2 * s->layers + 1;
+		size_t w = 0;
+		auto put = [&](uint32_t x) {
+			if (w < cap) out[w] = x;
+			w++;
+		};
+		const size_t P = s->nparts();
+		put(uint32_t(s->dims));
+		put(uint32_t(s->layers));
+		put(uint32_t(P));
+		for (size_t pc = 0; pc < P; pc++) {
+			int act;
+			float bg;
+			s->pstate(pc, &act, &bg);
+			uint32_t bits;
+			std::memcpy(&bits, &bg, 4);
+			put(uint32_t(act));
+			put(bits);
+			for (int l = 0; l < NL; l++) {
+				const auto& lst = *s->leaf_list(pc, l);
+				put(uint32_t(lst.size()));
+				for (size_t x : lst) put(uint32_t(x));
+			}
+		}
+		for (int which = 0; which < 3; which++)
+			for (int l = 0; l < NL; l++) {
+				const auto& lst = *s->plist(which, l);
+				put(uint32_t(lst.size()));
+				for (size_t x : lst) put(uint32_t(x));
+			}
+		*n = w;
+	});
+}
+
+int fo_polys_create(void* s, void** out)
+{
+	return guard([&] {
+		PolysBase* p = make_polys(static_cast<SurfBase*>(s));
+		if (!p) throw fo::Error(-1, "unsupported dims/layers");
+		*out = p;
+	});
+}
+int fo_polys_destroy(void* p)
+{
+	delete static_cast<PolysBase*>(p);
+	return 0;
+}
+int fo_polys_notify(void* p)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->notify(); });
+}
+int fo_polys_march(void* p)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->march(); });
+}
+int fo_polys_invalidate(void* p)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->invalidate(); });
+}
+int fo_polys_march_partition(void* p, size_t part)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->march_partition(part); });
+}
+int fo_polys_changes(void* p, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(static_cast<PolysBase*>(p)->changes(), out, cap, n); });
+}
+int fo_polys_partition(void* p, size_t part, float* vtx, size_t vcap, uint32_t* spx, size_t scap,
+                       size_t* nv, size_t* ns, int* active)
+{
+	return guard(
+	    [&] { static_cast<PolysBase*>(p)->part(part, vtx, vcap, spx, scap, nv, ns, active); });
+}
+int fo_polys_totals(void* p, size_t* nv, size_t* ns)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->totals(nv, ns); });
+}
+
+/* Timing helper for the CPU baseline: run `steps` global updates with a builtin speed and
+ * return the node-updates processed (sum of band sizes at the start of each step) and the
+ * wall seconds spent inside the updates. */
+int fo_run_steps(void* sv, const fo_speed* sp, int steps, double* node_updates, double* seconds)
+{
+	return guard([&] {
+		SurfBase* s = static_cast<SurfBase*>(sv);
+		const fo::Speed speed = to_speed(sp->kind, sp->c, sp->a, sp->n, sp->seed);
+		double nu = 0, secs = 0;
+		for (int i = 0; i < steps; i++) {
+			nu += double(s->band_size());
+			const auto t0 = std::chrono::steady_clock::now();
+			s->update(speed);
+			const auto t1 = std::chrono::steady_clock::now();
+			secs += std::chrono::duration<double>(t1 - t0).count();
+		}
+		*node_updates = nu;
+		*seconds = secs;
+	});
+}
+
+}  // extern "C"

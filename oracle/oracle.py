@@ -1,0 +1,244 @@
+"""ctypes wrapper over the CPU oracle library (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, as the checker. The product (felt_b200/) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"oracle error {code}: {msg}")
+        self.code = code
+
+
+class Speed(C.Structure):
+    _fields_ = [("kind", C.c_int), ("c", C.c_float), ("a", C.c_float), ("n", C.c_float),
+                ("seed", C.c_uint32)]
+
+
+CONST, CURV, NOISE = 1, 2, 4
+
+
+def build():
+    """Compile liboracle.so from its sources (make in oracle/)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        _lib = C.CDLL(_LIB)
+        _lib.fo_last_error.restype = C.c_char_p
+    return _lib
+
+
+def _chk(rc):
+    if rc != 0:
+        raise OracleError(rc, lib().fo_last_error().decode())
+
+
+def _ivec(v):
+    return (C.c_int * len(v))(*[int(x) for x in v])
+
+
+def _fetch_list(fn, *args):
+    n = C.c_size_t(0)
+    cap = 256
+    while True:
+        buf = (C.c_uint32 * cap)()
+        _chk(fn(*args, buf, C.c_size_t(cap), C.byref(n)))
+        if n.value <= cap:
+            return list(buf[: n.value])
+        cap = n.value
+
+
+class Surface:
+    """Oracle Surface<D,L>(size, part) with the same call surface as felt_b200.Surface."""
+
+    def __init__(self, size, part, layers):
+        self.D = len(size)
+        self.L = layers
+        self.size = tuple(int(s) for s in size)
+        self.part = tuple(int(p) for p in part)
+        h = C.c_void_p()
+        _chk(lib().fo_surface_create(self.D, self.L, _ivec(size), _ivec(part), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fo_surface_destroy(h)
+            self._h = None
+
+    @staticmethod
+    def layer_idx(layer_id, L):
+        return layer_id + L
+
+    def seed(self, pos):
+        _chk(lib().fo_seed(self._h, _ivec(pos)))
+
+    def update(self, c=None, a=None, n=None, seed=0):
+        kind = 0
+        if a is not None:
+            kind |= CURV
+        if n is not None:
+            kind |= NOISE
+        if c is not None:
+            kind |= CONST
+        sp = Speed(kind, float(c or 0.0), float(a or 0.0), float(n or 0.0), int(seed))
+        _chk(lib().fo_update_builtin(self._h, C.byref(sp)))
+
+    def update_bounded(self, lo, hi, c=None, a=None, n=None, seed=0):
+        kind = (CURV if a is not None else 0) | (NOISE if n is not None else 0) | (
+            CONST if c is not None else 0)
+        sp = Speed(kind, float(c or 0.0), float(a or 0.0), float(n or 0.0), int(seed))
+        _chk(lib().fo_update_bounded(self._h, _ivec(lo), _ivec(hi), C.byref(sp)))
+
+    def update_start(self):
+        _chk(lib().fo_update_start(self._h))
+
+    def delta(self, pos, val):
+        _chk(lib().fo_delta(self._h, _ivec(pos), C.c_float(val)))
+
+    def update_end(self):
+        _chk(lib().fo_update_end(self._h))
+
+    def snapshot(self):
+        n = int(np.prod(self.size))
+        out = np.zeros(n, dtype=np.float32)
+        _chk(lib().fo_snapshot(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(n)))
+        return out.reshape(self.size)
+
+    def get(self, pos):
+        v = C.c_float()
+        _chk(lib().fo_get(self._h, _ivec(pos), C.byref(v)))
+        return v.value
+
+    def curv(self, pos):
+        v = C.c_float()
+        _chk(lib().fo_curv(self._h, _ivec(pos), C.byref(v)))
+        return v.value
+
+    def partitions(self):
+        cnt = C.c_size_t()
+        cs = (C.c_int * self.D)()
+        co = (C.c_int * self.D)()
+        _chk(lib().fo_partitions(self._h, C.byref(cnt), cs, co))
+        return cnt.value, tuple(cs), tuple(co)
+
+    def layer_list(self, part, layer_idx):
+        return _fetch_list(lib().fo_layer_list, self._h, C.c_size_t(part), C.c_int(layer_idx))
+
+    def partition_list(self, layer_idx, which=0):
+        return _fetch_list(lib().fo_partition_list, self._h, C.c_int(which), C.c_int(layer_idx))
+
+    def delta_partitions(self, layer_idx):
+        return self.partition_list(layer_idx, which=1)
+
+    def status_partitions(self, layer_idx):
+        return self.partition_list(layer_idx, which=2)
+
+    def affected_partitions(self, layer_idx):
+        return self.partition_list(layer_idx, which=3)
+
+    def partition_state(self, part):
+        a = C.c_int()
+        bg = C.c_float()
+        _chk(lib().fo_partition_state(self._h, C.c_size_t(part), C.byref(a), C.byref(bg)))
+        return bool(a.value), bg.value
+
+    def stats(self):
+        a = C.c_size_t()
+        b = C.c_size_t()
+        _chk(lib().fo_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def band_size(self):
+        n = C.c_size_t()
+        _chk(lib().fo_band_size(self._h, C.byref(n)))
+        return n.value
+
+    def layer_size(self, layer_id):
+        """Total nodes in a layer over all partitions (test_Surface.cpp:1711-1727)."""
+        li = layer_id + self.L
+        return sum(len(self.layer_list(p, li)) for p in self.partition_list(li))
+
+    def dump(self):
+        return np.array(_fetch_list(lib().fo_dump, self._h), dtype=np.uint32)
+
+    def run_steps(self, steps, c=None, a=None, n=None, seed=0):
+        kind = (CURV if a is not None else 0) | (NOISE if n is not None else 0) | (
+            CONST if c is not None else 0)
+        sp = Speed(kind, float(c or 0.0), float(a or 0.0), float(n or 0.0), int(seed))
+        nu = C.c_double()
+        secs = C.c_double()
+        _chk(lib().fo_run_steps(self._h, C.byref(sp), C.c_int(steps), C.byref(nu),
+                                C.byref(secs)))
+        return nu.value, secs.value
+
+
+class Polys:
+    def __init__(self, surface: Surface):
+        self.surface = surface
+        h = C.c_void_p()
+        _chk(lib().fo_polys_create(surface._h, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fo_polys_destroy(h)
+            self._h = None
+
+    def notify(self):
+        _chk(lib().fo_polys_notify(self._h))
+
+    def march(self):
+        _chk(lib().fo_polys_march(self._h))
+
+    def invalidate(self):
+        _chk(lib().fo_polys_invalidate(self._h))
+
+    def march_partition(self, part):
+        _chk(lib().fo_polys_march_partition(self._h, C.c_size_t(part)))
+
+    def changes(self):
+        return _fetch_list(lib().fo_polys_changes, self._h)
+
+    def partition(self, part):
+        D = self.surface.D
+        per = 2 * D if D == 3 else D
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        act = C.c_int()
+        _chk(lib().fo_polys_partition(self._h, C.c_size_t(part), None, C.c_size_t(0), None,
+                                      C.c_size_t(0), C.byref(nv), C.byref(ns), C.byref(act)))
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
+        spx = np.zeros(max(1, ns.value * D), dtype=np.uint32)
+        _chk(lib().fo_polys_partition(self._h, C.c_size_t(part),
+                                      vtx.ctypes.data_as(C.POINTER(C.c_float)),
+                                      C.c_size_t(vtx.size),
+                                      spx.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                      C.c_size_t(spx.size), C.byref(nv), C.byref(ns),
+                                      C.byref(act)))
+        return (vtx[: nv.value * per].reshape(nv.value, per), spx[: ns.value * D].reshape(
+            ns.value, D), bool(act.value))
+
+    def totals(self):
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        _chk(lib().fo_polys_totals(self._h, C.byref(nv), C.byref(ns)))
+        return nv.value, ns.value

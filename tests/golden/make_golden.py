@@ -1,0 +1,240 @@
+"""Extract golden vectors from the Felt reference's own Catch tests into JSON fixtures.
+
+The reference test sources are read as text; each case names the scenario it comes from
+(file:line), restates the scenario's actions as a list of steps, and takes the expected values
+(dense isogrid literals, layer sizes, vertices, simplices, curvatures) from the lines cited.
+Run in an environment where the reference source tree is available:
+
+    python tests/golden/make_golden.py /path/to/felt-reference
+
+and commit the resulting tests/golden/reference_golden.json. The tests never read the reference
+tree themselves.
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+NUM = r"-?\d+(?:\.\d+)?"
+
+
+def lines_of(root, rel):
+    with open(os.path.join(root, rel)) as f:
+        return f.read().split("\n")
+
+
+def data_block(lines, start):
+    """Numbers of the `... = { ... };` literal whose opening line is `start` (1-based)."""
+    i = start - 1
+    while not re.search(r"(data\(\)|grid) = \{", lines[i]):
+        i += 1
+    text = ""
+    depth = 0
+    first = i
+    while True:
+        ln = re.sub(r"//.*", "", lines[i])
+        for ch in ln:
+            if ch == "{":
+                depth += 1
+            elif ch == "}":
+                depth -= 1
+        text += ln + "\n"
+        if depth == 0 and i > first or (depth == 0 and "}" in ln):
+            break
+        i += 1
+    body = text[text.index("{") + 1: text.rindex("}")]
+    return [float(x) for x in re.findall(NUM, body)], i + 1
+
+
+def layer_checks(lines, start, end):
+    """CHECK(layer_size(surface, id) == n) lines within [start, end] -> {id: n}."""
+    out = {}
+    for ln in lines[start - 1: end]:
+        m = re.search(r"layer_size\((?:surface|surface_loaded), (-?\d+)\) == (\d+)", ln)
+        if m:
+            out[int(m.group(1))] = int(m.group(2))
+    return out
+
+
+def part_layer_checks(lines, start, end):
+    out = []
+    for ln in lines[start - 1: end]:
+        m = re.search(r"layer_size<\d,\d>\(surface, Vec\di\(([-\d, ]+)\), (-?\d+)\)\)\s*==\s*(\d+)",
+                      ln)
+        if m:
+            out.append([[int(x) for x in m.group(1).split(",")], int(m.group(2)),
+                        int(m.group(3))])
+    return out
+
+
+def surface_cases(root):
+    f = "src/tests/test_Surface.cpp"
+    L = lines_of(root, f)
+    cases = []
+
+    def grid_case(name, at, size, part, layers, steps, grid_line, checks_to, extra=None):
+        vals, end = data_block(L, grid_line)
+        case = dict(name=name, ref=f"{f}:{at}", size=size, part=part, layers=layers,
+                    steps=steps, grid=vals, grid_ref=f"{f}:{grid_line}-{end}",
+                    layer_sizes=layer_checks(L, grid_line, checks_to))
+        if extra:
+            case.update(extra)
+        cases.append(case)
+
+    seed = ["seed", [0, 0]]
+    upd = lambda c: ["update", c]
+    grid_case("seed_9x9", "58-103", [9, 9], [3, 3], 2, [seed], 79, 102)
+    grid_case("radius1_9x9", "104-158", [9, 9], [3, 3], 2, [seed, upd(-1.0)], 108, 131)
+    grid_case("radius2_9x9", "180-210", [9, 9], [3, 3], 2, [seed, upd(-1.0), upd(-1.0)], 192,
+              209)
+    grid_case("consumed_9x9", "212-251", [9, 9], [3, 3], 2, [seed] + [upd(-1.0)] * 11, 226, 249)
+    grid_case("collapse_to_seed_9x9", "254-293", [9, 9], [3, 3], 2,
+              [seed, upd(-1.0), upd(1.0)], 267, 294)
+    grid_case("collapse_to_nothing_9x9", "295-346", [9, 9], [3, 3], 2,
+              [seed, upd(-1.0), upd(1.0), upd(1.0)], 324, 346)
+    grid_case("expand_0.6_9x9", "353-389", [9, 9], [3, 3], 2, [seed, upd(-0.6)], 364, 389)
+    grid_case("contract_0.6_9x9", "391-424", [9, 9], [3, 3], 2, [seed, upd(-0.6), upd(0.6)], 402,
+              424)
+    grid_case("contract_0.6_again_9x9", "426-459", [9, 9], [3, 3], 2,
+              [seed, upd(-0.6), upd(0.6), upd(0.6)], 437, 459)
+    grid_case("central_partition_deactivated_21x21", "519-580", [21, 21], [2, 2], 2,
+              [seed] + [upd(-1.0)] * 5, 540, 566,
+              dict(partition_active={"0,1": True, "0,-1": True, "1,0": True, "-1,0": True,
+                                     "0,0": False},
+                   partition_active_ref=f"{f}:569-578"))
+    # Local updates (update_start / delta / update_end).
+    lseed = [seed]
+    grid_case("local_contract_9x9", "598-633", [9, 9], [2, 2], 2,
+              lseed + [["update_start"], ["delta", [0, 0], 1.0], ["update_end"]], 608, 632)
+    grid_case("local_expand_9x9", "635-666", [9, 9], [2, 2], 2,
+              lseed + [["update_start"], ["delta", [0, 0], -1.0], ["update_end"]], 643, 665)
+    grid_case("bounded_update_9x9", "811-880", [9, 9], [2, 2], 2,
+              lseed + [["update_bounded", [-1, -1], [1, 1], -0.6]], 816, 839)
+    # Layer interactions.
+    two = [["seed", [-4, 0]], ["seed", [4, 0]], upd(-1.0)]
+    grid_case("two_seeds_16x9", "888-932", [16, 9], [3, 3], 2, two, 911, 931,
+              dict(partition_layer_sizes=part_layer_checks(L, 903, 907)))
+    towards = [["update_start"], ["delta", [-3, 0], -1.0], ["delta", [3, 0], -1.0],
+               ["update_end"]]
+    grid_case("two_seeds_towards_16x9", "934-973", [16, 9], [3, 3], 2, two + towards, 951, 972,
+              dict(partition_layer_sizes=part_layer_checks(L, 943, 947)))
+    back = [["update_start"], ["delta", [-3, 1], 1.0], ["delta", [-2, 0], 1.0],
+            ["delta", [-3, -1], 1.0], ["delta", [3, 1], 1.0], ["delta", [2, 0], 1.0],
+            ["delta", [3, -1], 1.0], ["update_end"]]
+    grid_case("two_seeds_cycle_16x9", "975-1027", [16, 9], [3, 3], 2, two + (towards + back) * 10,
+              1005, 1026, dict(partition_layer_sizes=part_layer_checks(L, 997, 1001)))
+    # Surface<2,3>: two diagonal seeds, local updates (test_Surface.cpp:1083-1216).
+    diag = [["seed", [-2, -2]], ["seed", [2, 2]]]
+    for p in ([-2, -2], [-1, -2], [0, -2]):
+        diag += [["update_start"], ["delta", p, -1.0], ["update_end"]]
+    diag += [["update_start"], ["delta", [1, -2], -1.0], ["delta", [2, 2], 1.0], ["update_end"],
+             ["update_start"], ["delta", [1, -1], -1.0], ["update_end"]]
+    grid_case("diagonal_seeds_local_12x12_L3", "1083-1216", [12, 12], [2, 2], 3, diag, 1188,
+              1216)
+    # 3D layer sizes.
+    s3 = [["seed", [0, 0, 0]], upd(-1.0)]
+    cases.append(dict(name="radius1_11cubed_L3", ref=f"{f}:1031-1052", size=[11, 11, 11],
+                      part=[3, 3, 3], layers=3, steps=s3, grid=None,
+                      layer_sizes=layer_checks(L, 1043, 1052)))
+    local3 = [["update_start"], ["delta", [0, 1, 0], -1.0], ["update_end"], ["update_start"],
+              ["delta", [0, 2, 0], 1.0], ["delta", [1, 1, 0], 1.0], ["delta", [-1, 1, 0], 1.0],
+              ["delta", [0, 1, 1], 1.0], ["delta", [0, 1, -1], 1.0], ["update_end"]]
+    cases.append(dict(name="local_3d_11cubed_L3", ref=f"{f}:1054-1080", size=[11, 11, 11],
+                      part=[3, 3, 3], layers=3, steps=s3 + local3, grid=None,
+                      layer_sizes=layer_checks(L, 1070, 1079)))
+    return cases
+
+
+def poly_cases(root):
+    f = "src/tests/test_Poly.cpp"
+    L = lines_of(root, f)
+    out = []
+
+    def vec_checks(start, end, field):
+        res = []
+        for ln in L[start - 1: end]:
+            m = re.search(r"vtxs\(\)\[(\d+)\]\.%s == ApproxVec\(Vec\df\{([^}]*)\}\)" % field, ln)
+            if m:
+                res.append([int(m.group(1))] + [float(x.replace("f", "")) for x in
+                                                 m.group(2).split(",")])
+        return res
+
+    def spx_checks(start, end):
+        res = []
+        for ln in L[start - 1: end]:
+            m = re.search(r"spxs\(\)\[(\d+)\]\.idxs == \(Vec\du\{([^}]*)\}\)", ln)
+            if m:
+                res.append([int(m.group(1))] + [int(x) for x in m.group(2).split(",")])
+        return res
+
+    def count(start, end, what):
+        """First nonzero `poly.<what>().size() == n` check within [start, end]."""
+        for ln in L[start - 1: end]:
+            m = re.search(r"poly\.%s\(\)\.size\(\) == (\d+)" % what, ln)
+            if m and int(m.group(1)) > 0:
+                return int(m.group(1))
+        return None
+
+    out.append(dict(name="poly_single_3d", ref=f"{f}:14-104", size=[9, 9, 9], part=[3, 3, 3],
+                    layers=3, steps=[["seed", [0, 0, 0]], ["update", -0.4]], partition=[0, 0, 0],
+                    nvtx=count(62, 76, "vtxs"), nspx=count(62, 76, "spxs"),
+                    pos=vec_checks(75, 84, "pos"), norm=vec_checks(85, 92, "norm"),
+                    spx=spx_checks(94, 104)))
+    # 2D single poly.
+    two = dict(name="poly_single_2d", ref=f"{f}:134-211", size=[9, 9], part=[3, 3], layers=3,
+               partition=[0, 0])
+    # steps and counts parsed from the 2D scenario text
+    text = "\n".join(L[133:241])
+    m = re.search(r"return (-?[\d.]+)f;", text)
+    two["steps"] = [["seed", [0, 0]], ["update", float(m.group(1))]]
+    two["nvtx"] = count(134, 241, "vtxs")
+    two["nspx"] = count(134, 241, "spxs")
+    two["pos"] = vec_checks(134, 241, "pos")
+    two["spx"] = spx_checks(134, 241)
+    out.append(two)
+    # Polys: central partition of a 15^3 / 5^3 surface.
+    m1 = re.search(r"get\(Vec3i\(0,0,0\)\)\.vtxs\(\)\.size\(\) == (\d+)", L[341])
+    m2 = re.search(r"get\(Vec3i\(0,0,0\)\)\.spxs\(\)\.size\(\) == (\d+)", L[342])
+    out.append(dict(name="polys_central_15cubed", ref=f"{f}:326-344", size=[15, 15, 15],
+                    part=[5, 5, 5], layers=3, steps=[["seed", [0, 0, 0]], ["update", -1.0]],
+                    partition=[0, 0, 0], nvtx=int(m1.group(1)), nspx=int(m2.group(1))))
+    return out
+
+
+def curvature_cases(root):
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+    out = []
+    for start, dims, want_line in [(2198, 2, 2206), (2212, 2, 2222), (2319, 3, 2350),
+                                   (2356, 3, 2372), (2378, 3, 2396)]:
+        vals, end = data_block(L, start)
+        m = re.search(r"curv\(Vec\di\([^)]*\)\) == (" + NUM + ")", "\n".join(L[end - 1:want_line]))
+        out.append(dict(ref=f"{f}:{start}-{want_line}", dims=dims, size=[3] * dims,
+                        offset=[-1] * dims, background=0.0, values=vals, pos=[0] * dims,
+                        curv=float(m.group(1))))
+    return out
+
+
+def neighs_case(root):
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+    text = "\n".join(L[2398:2416])
+    vs = re.findall(r"Vec3i\((-?\d+), (-?\d+), (-?\d+)\)", text)
+    pts = [[int(a), int(b), int(c)] for a, b, c in vs]
+    return dict(ref=f"{f}:2398-2416", centre=pts[0], order=pts[1:])
+
+
+def main():
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    out = dict(surface=surface_cases(root), poly=poly_cases(root),
+               curvature=curvature_cases(root), neighs=neighs_case(root))
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", dst, {k: (len(v) if isinstance(v, list) else 1) for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()
