@@ -1,0 +1,243 @@
+"""felt_b200: B200-native sparse-field level sets with the Felt Surface<D,L> / Polys API.
+
+Python binding over the C ABI of libfelt_gpu.so (include/felt_gpu.h). The classes mirror the
+reference's C++ API (include/Felt/Surface.hpp, include/Felt/Polys.hpp): Surface(size, part, L)
+with seed / update / update_start / delta / update_end / snapshot and the list accessors, and
+Polys(surface) with notify / march / invalidate / changes.
+
+All compute runs in the CUDA kernels of libfelt_gpu.so; there is no CPU fallback. If the library
+is missing or no CUDA device is present, constructing a Surface raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfelt_gpu.so")
+_lib = None
+
+SPEED_CONST, SPEED_CURV, SPEED_NOISE = 1, 2, 4
+
+
+class FeltError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"felt_gpu error {code}: {msg}")
+        self.code = code
+
+
+class Speed(C.Structure):
+    _fields_ = [("kind", C.c_int), ("c", C.c_float), ("a", C.c_float), ("n", C.c_float),
+                ("seed", C.c_uint32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("brick_capacity", C.c_size_t), ("vertex_capacity", C.c_size_t),
+                ("use_graph", C.c_int), ("reserved", C.c_int * 7)]
+
+
+def build():
+    """Compile libfelt_gpu.so for sm_100a (nvcc; no GPU needed)."""
+    subprocess.run(["bash", os.path.join(_HERE, "csrc", "build.sh")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FeltError(-2, f"{LIB_PATH} is not built; run felt_b200.build()")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.fg_last_error.restype = C.c_char_p
+    return _lib
+
+
+def _chk(rc):
+    if rc != 0:
+        raise FeltError(rc, lib().fg_last_error().decode())
+
+
+def _ivec(v):
+    return (C.c_int * len(v))(*[int(x) for x in v])
+
+
+def _fetch(fn, *args):
+    n = C.c_size_t(0)
+    cap = 256
+    while True:
+        buf = (C.c_uint32 * cap)()
+        _chk(fn(*args, buf, C.c_size_t(cap), C.byref(n)))
+        if n.value <= cap:
+            return list(buf[: n.value])
+        cap = n.value
+
+
+def make_speed(c=None, a=None, n=None, seed=0):
+    """Builtin speed: [a*curv] + [n*noise(pos, seed)] + [c], terms present when given."""
+    kind = (SPEED_CURV if a is not None else 0) | (SPEED_NOISE if n is not None else 0) | (
+        SPEED_CONST if c is not None else 0)
+    return Speed(kind, float(c or 0.0), float(a or 0.0), float(n or 0.0), int(seed))
+
+
+class Surface:
+    """Felt::Surface<D,L>(size, size_partition) on the GPU (include/Felt/Surface.hpp:163-173)."""
+
+    def __init__(self, size, part, layers, brick_capacity=0):
+        self.D = len(size)
+        self.L = int(layers)
+        self.size = tuple(int(s) for s in size)
+        self.part = tuple(int(p) for p in part)
+        cfg = Config(int(brick_capacity), 0, 0)
+        h = C.c_void_p()
+        _chk(lib().fg_surface_create(self.D, self.L, _ivec(size), _ivec(part), C.byref(cfg),
+                                     C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fg_surface_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def seed(self, pos):
+        _chk(lib().fg_seed(self._h, _ivec(pos)))
+
+    def update(self, c=None, a=None, n=None, seed=0):
+        sp = make_speed(c, a, n, seed)
+        _chk(lib().fg_update_builtin(self._h, C.byref(sp)))
+
+    def update_bounded(self, lo, hi, c=None, a=None, n=None, seed=0):
+        sp = make_speed(c, a, n, seed)
+        _chk(lib().fg_update_bounded(self._h, _ivec(lo), _ivec(hi), C.byref(sp)))
+
+    def update_start(self):
+        _chk(lib().fg_update_start(self._h))
+
+    def delta(self, pos, val):
+        _chk(lib().fg_delta(self._h, _ivec(pos), C.c_float(val)))
+
+    def update_end(self):
+        _chk(lib().fg_update_end(self._h))
+
+    def snapshot(self):
+        n = int(np.prod(self.size))
+        out = np.zeros(n, dtype=np.float32)
+        _chk(lib().fg_snapshot(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(n),
+                               0))
+        return out.reshape(self.size)
+
+    def snapshot_into(self, dev_ptr, n):
+        """Snapshot into device memory (e.g. a torch CUDA tensor's data_ptr())."""
+        _chk(lib().fg_snapshot(self._h, C.c_void_p(dev_ptr), C.c_size_t(n), 1))
+
+    def get(self, pos):
+        v = C.c_float()
+        _chk(lib().fg_get(self._h, _ivec(pos), C.byref(v)))
+        return v.value
+
+    def partitions(self):
+        cnt = C.c_size_t()
+        cs = (C.c_int * self.D)()
+        co = (C.c_int * self.D)()
+        _chk(lib().fg_partitions(self._h, C.byref(cnt), cs, co))
+        return cnt.value, tuple(cs), tuple(co)
+
+    def layer_list(self, part, layer_idx):
+        return _fetch(lib().fg_layer_list, self._h, C.c_size_t(part), C.c_int(layer_idx))
+
+    def partition_list(self, layer_idx):
+        return _fetch(lib().fg_partition_list, self._h, C.c_int(layer_idx))
+
+    def delta_partitions(self, layer_idx):
+        return _fetch(lib().fg_delta_partitions, self._h, C.c_int(layer_idx))
+
+    def status_partitions(self, layer_idx):
+        return _fetch(lib().fg_status_partitions, self._h, C.c_int(layer_idx))
+
+    def partition_state(self, part):
+        a = C.c_int()
+        bg = C.c_float()
+        _chk(lib().fg_partition_state(self._h, C.c_size_t(part), C.byref(a), C.byref(bg)))
+        return bool(a.value), bg.value
+
+    def stats(self):
+        a = C.c_size_t()
+        b = C.c_size_t()
+        _chk(lib().fg_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def band_size(self):
+        n = C.c_size_t()
+        _chk(lib().fg_band_size(self._h, C.byref(n)))
+        return n.value
+
+    def layer_size(self, layer_id):
+        li = layer_id + self.L
+        return sum(len(self.layer_list(p, li)) for p in self.partition_list(li))
+
+    def dump(self):
+        return np.array(_fetch(lib().fg_dump, self._h), dtype=np.uint32)
+
+
+class Polys:
+    """Felt::Polys<Surface> (include/Felt/Polys.hpp:1-229) on the GPU."""
+
+    def __init__(self, surface: Surface):
+        self.surface = surface
+        h = C.c_void_p()
+        _chk(lib().fg_polys_create(surface._h, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fg_polys_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def notify(self):
+        _chk(lib().fg_polys_notify(self._h))
+
+    def march(self):
+        _chk(lib().fg_polys_march(self._h))
+
+    def invalidate(self):
+        _chk(lib().fg_polys_invalidate(self._h))
+
+    def march_partition(self, part):
+        _chk(lib().fg_polys_march_partition(self._h, C.c_size_t(part)))
+
+    def changes(self):
+        return _fetch(lib().fg_polys_changes, self._h)
+
+    def partition(self, part):
+        D = self.surface.D
+        per = 2 * D if D == 3 else D
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        act = C.c_int()
+        _chk(lib().fg_polys_partition(self._h, C.c_size_t(part), None, C.c_size_t(0), None,
+                                      C.c_size_t(0), C.byref(nv), C.byref(ns), C.byref(act)))
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
+        spx = np.zeros(max(1, ns.value * D), dtype=np.uint32)
+        _chk(lib().fg_polys_partition(self._h, C.c_size_t(part),
+                                      vtx.ctypes.data_as(C.POINTER(C.c_float)),
+                                      C.c_size_t(vtx.size),
+                                      spx.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                      C.c_size_t(spx.size), C.byref(nv), C.byref(ns),
+                                      C.byref(act)))
+        return (vtx[: nv.value * per].reshape(nv.value, per),
+                spx[: ns.value * D].reshape(ns.value, D), bool(act.value))
+
+    def totals(self):
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        _chk(lib().fg_polys_totals(self._h, C.byref(nv), C.byref(ns)))
+        return nv.value, ns.value

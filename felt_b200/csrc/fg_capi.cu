@@ -1,0 +1,388 @@
+// C ABI (include/felt_gpu.h) over the device engine. Exceptions never cross the boundary:
+// every entry point maps them to a status code and keeps the message for fg_last_error().
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/felt_gpu.h"
+#include "fg_engine.cuh"
+#include "fg_polys.cuh"
+
+struct fg_surface {
+	std::unique_ptr<fg::EngineBase> eng;
+	cudaStream_t st = nullptr;
+	bool local_open = false;
+	std::vector<int> dpos;
+	std::vector<float> dval;
+	~fg_surface()
+	{
+		eng.reset();
+		if (st) cudaStreamDestroy(st);
+	}
+};
+
+struct fg_polys {
+	fg_surface* surf = nullptr;
+	std::unique_ptr<fg::PolysBase> impl;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f)
+{
+	try {
+		f();
+		return FG_OK;
+	} catch (const fg::Error& e) {
+		g_err = e.what();
+		return e.code;
+	} catch (const std::bad_alloc&) {
+		g_err = "host allocation failed";
+		return FG_ERR_NOMEM;
+	} catch (const std::exception& e) {
+		g_err = e.what();
+		return FG_ERR_ARG;
+	}
+}
+
+void need(const void* p, const char* what)
+{
+	if (!p) throw fg::Error(FG_ERR_ARG, std::string("null ") + what);
+}
+
+fg::Speed to_speed(const fg_speed* s)
+{
+	need(s, "speed");
+	if (s->kind & ~7) throw fg::Error(FG_ERR_ARG, "unknown speed kind bits");
+	return fg::Speed{s->kind, s->c, s->a, s->n, s->seed};
+}
+
+void put_list(const std::vector<uint32_t>& v, uint32_t* out, size_t cap, size_t* n)
+{
+	need(n, "count");
+	*n = v.size();
+	if (out)
+		for (size_t i = 0; i < v.size() && i < cap; i++) out[i] = v[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fg_last_error(void) { return g_err.c_str(); }
+
+int fg_surface_create(int dims, int layers, const int* size, const int* part, const fg_config* cfg,
+                      fg_surface** out)
+{
+	return guard([&] {
+		need(size, "size");
+		need(part, "part");
+		need(out, "out");
+		if (dims != 2 && dims != 3) throw fg::Error(FG_ERR_ARG, "dims must be 2 or 3");
+		if (layers < 1 || layers > 4) throw fg::Error(FG_ERR_ARG, "layers must be in 1..4");
+		int ndev = 0;
+		if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+			throw fg::Error(FG_ERR_CUDA, "no CUDA device");
+		fg::PoolDesc d;
+		d.D = dims;
+		d.L = layers;
+		std::array<int, 3> sz = {1, 1, 1};
+		for (int a = 0; a < dims; a++) {
+			sz[a] = size[a];
+			d.part[a] = part[a];
+		}
+		d.sizes.push_back(sz);
+		if (cfg) d.brick_capacity = cfg->brick_capacity;
+		auto s = std::make_unique<fg_surface>();
+		FG_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+		s->eng.reset(fg::make_engine(d, s->st));
+		*out = s.release();
+	});
+}
+
+int fg_surface_destroy(fg_surface* s)
+{
+	return guard([&] { delete s; });
+}
+
+int fg_seed(fg_surface* s, const int* pos)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(pos, "pos");
+		s->eng->seed(0, pos);
+	});
+}
+
+int fg_update_builtin(fg_surface* s, const fg_speed* speed)
+{
+	return guard([&] {
+		need(s, "surface");
+		const fg::Speed sp = to_speed(speed);
+		s->eng->update_builtin(&sp);
+	});
+}
+
+int fg_update_begin_global(fg_surface* s, const fg_device_view** view, void** stream)
+{
+	return guard([&] {
+		need(s, "surface");
+		s->eng->update_begin_global();
+		if (view) *view = reinterpret_cast<const fg_device_view*>(&s->eng->dev());
+		if (stream) *stream = (void*)s->eng->stream();
+	});
+}
+
+int fg_update_finish_global(fg_surface* s)
+{
+	return guard([&] {
+		need(s, "surface");
+		s->eng->update_finish_global();
+	});
+}
+
+int fg_update_bounded(fg_surface* s, const int* lo, const int* hi, const fg_speed* speed)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(lo, "lo");
+		need(hi, "hi");
+		s->eng->update_bounded(lo, hi, to_speed(speed));
+	});
+}
+
+int fg_update_start(fg_surface* s)
+{
+	return guard([&] {
+		need(s, "surface");
+		s->local_open = true;
+		s->dpos.clear();
+		s->dval.clear();
+	});
+}
+
+int fg_delta(fg_surface* s, const int* pos, float val)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(pos, "pos");
+		if (!s->local_open) throw fg::Error(FG_ERR_STATE, "delta() outside update_start/end");
+		for (int a = 0; a < s->eng->dims(); a++) s->dpos.push_back(pos[a]);
+		s->dval.push_back(val);
+	});
+}
+
+int fg_delta_n(fg_surface* s, const int* pos, const float* val, size_t n)
+{
+	return guard([&] {
+		need(s, "surface");
+		if (n && (!pos || !val)) throw fg::Error(FG_ERR_ARG, "null pos/val");
+		if (!s->local_open) throw fg::Error(FG_ERR_STATE, "delta() outside update_start/end");
+		const int D = s->eng->dims();
+		s->dpos.insert(s->dpos.end(), pos, pos + n * D);
+		s->dval.insert(s->dval.end(), val, val + n);
+	});
+}
+
+int fg_update_end(fg_surface* s)
+{
+	return guard([&] {
+		need(s, "surface");
+		if (!s->local_open) throw fg::Error(FG_ERR_STATE, "update_end() without update_start()");
+		s->local_open = false;
+		s->eng->update_local(s->dpos, s->dval);
+	});
+}
+
+int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(dst, "dst");
+		s->eng->snapshot(0, dst, n, dst_is_device != 0);
+	});
+}
+
+int fg_get(fg_surface* s, const int* pos, float* out)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(pos, "pos");
+		need(out, "out");
+		*out = s->eng->get(0, pos);
+	});
+}
+
+int fg_partitions(fg_surface* s, size_t* count, int* ccount, int* coff)
+{
+	return guard([&] {
+		need(s, "surface");
+		int cc[3], co[3];
+		const size_t n = s->eng->partitions(0, cc, co);
+		if (count) *count = n;
+		for (int a = 0; a < s->eng->dims(); a++) {
+			if (ccount) ccount[a] = cc[a];
+			if (coff) coff[a] = co[a];
+		}
+	});
+}
+
+int fg_layer_list(fg_surface* s, size_t part, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->layer_list(0, part, li), out, cap, n);
+	});
+}
+
+int fg_partition_list(fg_surface* s, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->partition_list(0, 0, li), out, cap, n);
+	});
+}
+
+int fg_delta_partitions(fg_surface* s, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->partition_list(0, 1, li), out, cap, n);
+	});
+}
+
+int fg_status_partitions(fg_surface* s, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->partition_list(0, 2, li), out, cap, n);
+	});
+}
+
+int fg_partition_state(fg_surface* s, size_t part, int* active, float* background)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(active, "active");
+		need(background, "background");
+		s->eng->partition_state(0, part, active, background);
+	});
+}
+
+int fg_stats(fg_surface* s, size_t* iso, size_t* delta)
+{
+	return guard([&] {
+		need(s, "surface");
+		const int NL = 2 * s->eng->layers() + 1;
+		size_t a = 0, b = 0;
+		for (int l = 0; l < NL; l++) {
+			a = std::max(a, s->eng->partition_list(0, 0, l).size());
+			b = std::max(b, s->eng->partition_list(0, 1, l).size());
+		}
+		if (iso) *iso = a;
+		if (delta) *delta = b;
+	});
+}
+
+int fg_band_size(fg_surface* s, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(n, "n");
+		*n = (size_t)s->eng->band_size(0);
+	});
+}
+
+int fg_dump(fg_surface* s, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->dump(0), out, cap, n);
+	});
+}
+
+// ---- Polys ----
+
+int fg_polys_create(fg_surface* s, fg_polys** out)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(out, "out");
+		auto p = std::make_unique<fg_polys>();
+		p->surf = s;
+		p->impl.reset(fg::make_polys(*s->eng, 0));
+		*out = p.release();
+	});
+}
+
+int fg_polys_destroy(fg_polys* p)
+{
+	return guard([&] { delete p; });
+}
+
+int fg_polys_notify(fg_polys* p)
+{
+	return guard([&] {
+		need(p, "polys");
+		p->impl->notify();
+	});
+}
+
+int fg_polys_march(fg_polys* p)
+{
+	return guard([&] {
+		need(p, "polys");
+		p->impl->march();
+	});
+}
+
+int fg_polys_invalidate(fg_polys* p)
+{
+	return guard([&] {
+		need(p, "polys");
+		p->impl->invalidate();
+	});
+}
+
+int fg_polys_march_partition(fg_polys* p, size_t part)
+{
+	return guard([&] {
+		need(p, "polys");
+		p->impl->march_partition(part);
+	});
+}
+
+int fg_polys_changes(fg_polys* p, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(p, "polys");
+		put_list(p->impl->changes(), out, cap, n);
+	});
+}
+
+int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vcap, uint32_t* spx,
+                       size_t scap, size_t* nv, size_t* ns, int* active)
+{
+	return guard([&] {
+		need(p, "polys");
+		need(nv, "nv");
+		need(ns, "ns");
+		int act = 0;
+		p->impl->partition(part, vtx, vcap, spx, scap, nv, ns, &act);
+		if (active) *active = act;
+	});
+}
+
+int fg_polys_totals(fg_polys* p, size_t* nv, size_t* ns)
+{
+	return guard([&] {
+		need(p, "polys");
+		p->impl->totals(nv, ns);
+	});
+}
+
+}  // extern "C"

@@ -1,0 +1,328 @@
+// Device-side layout and helpers of the sparse-field level-set engine.
+//
+// One pool holds S surfaces that share D, L and the partition (brick) shape. Every partition of
+// every surface has a global index gp = pbase[s] + local index, where the local index is the
+// reference's row-major children-grid index (include/Felt/Impl/Util.hpp:23-40). An active
+// partition owns one brick slot of the device pool; bricks hold the isogrid values, the ordered
+// per-layer leaf lists and per-step scratch. All arithmetic on distances is FP32 and compiled
+// with -fmad=false so that it rounds exactly as the reference's (-ffp-contract=off) CPU code.
+#pragma once
+
+#include <cstdint>
+
+namespace fg {
+
+constexpr uint16_t NUL16 = 0xFFFFu;
+constexpr unsigned long long NOCLAIM = ~0ull;
+
+// error bits (Dev::err[0])
+enum : int {
+	EB_NONFINITE = 1,  // layer_id of NaN/inf
+	EB_POOL = 2,       // brick pool exhausted
+	EB_OUTSIDE = 4,    // band node tracked outside the grid
+	EB_INACTIVE = 8,   // write to an inactive partition
+	EB_CAPACITY = 16,  // a fixed-capacity buffer overflowed
+	EB_TIMEOUT = 32    // a bounded wait gave up
+};
+
+/// Geometry of one surface of the pool.
+struct SurfGeom {
+	int size[3];
+	int off[3];    // grid offset = -size/2 (Surface.hpp:1716-1719)
+	int hi[3];     // off + size
+	int ccount[3]; // children grid size (PartitionedMixin.hpp:131-141)
+	int coff[3];   // children grid offset = off / part (truncating)
+	int pbase;     // first global partition index
+	int np;        // partitions of this surface
+};
+
+/// Pointers and sizes of the whole pool, passed by value to every kernel.
+struct Dev {
+	int S;        // surfaces
+	int NP;       // partitions over all surfaces
+	int BV;       // leaves per brick
+	int nslots;   // brick capacity
+	int csz[3];   // partition shape
+	int lstr[3];  // leaf strides inside a brick (row-major, last axis fastest)
+
+	const SurfGeom* geom;
+	const int* surf_of;   // [NP] surface of a partition
+	const int* porig;     // [NP*3] world position of a partition's first leaf
+
+	// partition level
+	int* slot;    // [NP] brick slot, -1 when inactive
+	float* bg;    // [NP] background returned for an inactive partition
+	int* oslot;   // [NP] slot of a partition deactivated in the current iteration, else -1
+	int* ppos;    // [NP*NL] position in the isogrid partition list, -1 = untracked
+
+	// partition lists, per layer a global array with per-surface segments at pbase:
+	// list[l*NP + pbase + i], counts cnt[s*NL + l]
+	int* plist; int* pcnt;      // isogrid children lookup lists
+	int* dplist; int* dpcnt;    // delta partition lists (snapshot at update start)
+	int* splist; int* spcnt;    // status-change partition lists (per from-layer)
+	int* sppos;                 // [NP*NL] position in splist, -1
+	int* aplist[2]; int* apcnt[2]; int* appos[2];  // affected lookups (two buffers)
+
+	// bricks
+	float* phi;       // [slot*BV + leaf]
+	float* dlt;       // [slot*BV + leaf] delta / scratch
+	uint16_t* lkp;    // [slot*BV + leaf] position in its isogrid layer list
+	uint16_t* lst;    // [(slot*NL + l)*BV + i] ordered leaf lists
+	int* lcnt;        // [slot*NL + l]
+	int8_t* sto;      // [slot*BV + leaf] status "to" layer id, L+1 = none
+	uint16_t* chg;    // [(slot*NL + f)*BV + i] status-change leaf list per from-layer
+	int* ccnt;        // [slot*NL + f]
+	uint16_t* alkp[2];  // affected buffer leaf lookups
+	uint16_t* alst[2];  // affected buffer leaf lists
+	int* acnt[2];
+	unsigned long long* claim;  // [slot*BV + leaf] expansion claim keys
+	int* slot_gp;     // [nslots] owner partition
+
+	// allocator and queues
+	int* free_stack;  // [nslots]
+	int* counters;    // see CNT_* below
+	int* q_act;       // [NP] partitions to activate
+	int* actflag;     // [NP]
+	int* q_touch;     // [nslots] bricks with expansion claims
+	int* touched;     // [nslots]
+	int* q_retire;    // [nslots] slots to release after the iteration
+	int* q_sunion;    // [NP] partitions with status changes this iteration
+	int* sflag;       // [NP] membership flag for q_sunion
+	unsigned int* eflag;  // [NP] per-entry flags of the current pass
+	unsigned* app;    // [NP*NL] flush: lists that went 0->1 during phase f (bitmask over to)
+	unsigned* rem;    // [NP] flush: lists that went ->0 during their own phase (bitmask)
+	unsigned long long* pap;  // [2*NP] expansion partition appends: first claim key per surface
+	int* papg;        // [2*NP] the local partition index of each pap entry
+	int* papn;        // [S]
+	int* woff;        // [S+1] entry offsets of the current pass
+	int* err;         // [1] error bits
+	int* changed;     // [1] status-change flag of the distance passes
+};
+
+enum { CNT_FREE_TOP = 0, CNT_ACT = 1, CNT_TOUCH = 2, CNT_RETIRE = 3, CNT_SUNION = 4, CNT_N = 8 };
+
+template <int D>
+struct Vec {
+	int v[D];
+	__host__ __device__ int& operator[](int i) { return v[i]; }
+	__host__ __device__ const int& operator[](int i) const { return v[i]; }
+};
+
+// -------------------------------------------------------------------------------------------
+// Rounding and layers (include/Felt/Surface.hpp:1694-1709)
+// -------------------------------------------------------------------------------------------
+
+/// layer_id(v) = iround(v + FLT_EPSILON), half away from zero. Non-finite input sets the error
+/// bit and yields an out-of-band id (the reference's boost::math::iround throws there).
+__device__ __forceinline__ int layer_id(float v, int* err)
+{
+	const float x = __fadd_rn(v, 1.1920928955078125e-07f);
+	if (!isfinite(x) || fabsf(x) >= 2147483648.0f) {
+		atomicOr(err, EB_NONFINITE);
+		return 1 << 20;
+	}
+	return (int)roundf(x);
+}
+__device__ __forceinline__ bool inside_band(int id, int L) { return (id < 0 ? -id : id) <= L; }
+
+// -------------------------------------------------------------------------------------------
+// Hashed noise, identical to the oracle's: MurmurHash3's fmix32 finaliser per axis, 24 bits
+// mapped exactly to u * 2^-23 - 1.
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t fmix32(uint32_t h)
+{
+	h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
+	return h;
+}
+template <int D>
+__device__ __forceinline__ float hash_noise(const Vec<D>& p, uint32_t seed)
+{
+	const uint32_t K[3] = {0x9e3779b1u, 0x7f4a7c15u, 0x94d049bbu};
+	uint32_t h = fmix32(seed ^ 0x5eed5eedu);
+#pragma unroll
+	for (int a = 0; a < D; a++) h = fmix32(h ^ ((uint32_t)p[a] * K[a]));
+	const uint32_t u = h >> 8;
+	return __fsub_rn(__fmul_rn((float)u, 1.0f / 8388608.0f), 1.0f);
+}
+
+// -------------------------------------------------------------------------------------------
+// Pool addressing
+// -------------------------------------------------------------------------------------------
+
+template <int D>
+__device__ __forceinline__ bool in_grid(const SurfGeom& g, const Vec<D>& p)
+{
+#pragma unroll
+	for (int a = 0; a < D; a++)
+		if (p[a] < g.off[a] || p[a] >= g.hi[a]) return false;
+	return true;
+}
+
+/// Global partition and leaf of an in-grid position (PartitionedMixin.hpp:221-245).
+template <int D>
+__device__ __forceinline__ void locate(const Dev& P, const SurfGeom& g, const Vec<D>& p, int& gp,
+                                       int& leaf)
+{
+	int idx = 0, lf = 0;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		const int r = p[a] - g.off[a];
+		const int c = r / P.csz[a];
+		idx = idx * g.ccount[a] + c;
+		lf += (r - c * P.csz[a]) * P.lstr[a];
+	}
+	gp = g.pbase + idx;
+	leaf = lf;
+}
+
+/// Partitioned::Access::get (PartitionedMixin.hpp:594-601) with the lazy child get
+/// (GridMixin.hpp:608-621): background L+1 outside the grid, the partition's background when
+/// it is inactive.
+template <int D, int L>
+__device__ __forceinline__ float get_phi(const Dev& P, const SurfGeom& g, const Vec<D>& p)
+{
+	if (!in_grid<D>(g, p)) return (float)(L + 1);
+	int gp, leaf;
+	locate<D>(P, g, p, gp, leaf);
+	const int sl = P.slot[gp];
+	if (sl < 0) return P.bg[gp];
+	return P.phi[(size_t)sl * P.BV + leaf];
+}
+
+/// World position of a leaf of partition gp.
+template <int D>
+__device__ __forceinline__ Vec<D> leaf_pos(const Dev& P, int gp, int leaf)
+{
+	Vec<D> p;
+	int rem = leaf;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		const int q = rem / P.lstr[a];
+		rem -= q * P.lstr[a];
+		p[a] = P.porig[gp * 3 + a] + q;
+	}
+	return p;
+}
+
+// -------------------------------------------------------------------------------------------
+// Stencils
+// -------------------------------------------------------------------------------------------
+
+/// Mean curvature by difference of normals (NumericMixin.hpp:72-156). The fixed-size Eigen sum
+/// of the normal differences is unrolled by halving: x0 + (x1 + x2) in 3D.
+template <int D, int L>
+__device__ float curv(const Dev& P, const SurfGeom& g, const Vec<D>& pos)
+{
+	const float centre = get_phi<D, L>(P, g, pos);
+	Vec<D> dir = pos;
+	float nf[D], nb[D];
+#pragma unroll
+	for (int axis = 0; axis < D; axis++) {
+		dir[axis] += 1;
+		const float va = __fsub_rn(get_phi<D, L>(P, g, dir), centre);
+		float sq = 0.0f;
+#pragma unroll
+		for (int an = 0; an < D; an++) {
+			if (an == axis) continue;
+			Vec<D> dn = dir;
+			dn[an] -= 1;
+			const float lo = get_phi<D, L>(P, g, dn);
+			dn[an] += 2;
+			const float hi = get_phi<D, L>(P, g, dn);
+			const float v = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
+			sq = __fadd_rn(sq, __fmul_rn(v, v));
+		}
+		nf[axis] = __fdiv_rn(va, __fsqrt_rn(__fadd_rn(__fmul_rn(va, va), sq)));
+		dir[axis] -= 1;
+	}
+#pragma unroll
+	for (int axis = 0; axis < D; axis++) {
+		dir[axis] -= 1;
+		const float va = __fsub_rn(centre, get_phi<D, L>(P, g, dir));
+		float sq = 0.0f;
+#pragma unroll
+		for (int an = 0; an < D; an++) {
+			if (an == axis) continue;
+			Vec<D> dn = dir;
+			dn[an] -= 1;
+			const float lo = get_phi<D, L>(P, g, dn);
+			dn[an] += 2;
+			const float hi = get_phi<D, L>(P, g, dn);
+			const float v = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
+			sq = __fadd_rn(sq, __fmul_rn(v, v));
+		}
+		nb[axis] = __fdiv_rn(va, __fsqrt_rn(__fadd_rn(__fmul_rn(va, va), sq)));
+		dir[axis] += 1;
+	}
+	float s;
+	if (D == 2)
+		s = __fadd_rn(__fsub_rn(nf[0], nb[0]), __fsub_rn(nf[D - 1], nb[D - 1]));
+	else
+		s = __fadd_rn(__fsub_rn(nf[0], nb[0]),
+		              __fadd_rn(__fsub_rn(nf[1 % D], nb[1 % D]), __fsub_rn(nf[D - 1], nb[D - 1])));
+	return __fdiv_rn(s, 2.0f);
+}
+
+/// City-block distance to the zero curve from the nearest in-grid neighbour on the way in
+/// (Surface.hpp:1387-1440): d = side * min(side*phi_self, side*phi_n) + side.
+template <int D, int L>
+__device__ __forceinline__ float distance(const Dev& P, const SurfGeom& g, const Vec<D>& pos,
+                                          float dist, float dir)
+{
+	dist = __fmul_rn(dist, dir);
+	Vec<D> n = pos;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+#pragma unroll
+		for (int s = -1; s <= 1; s += 2) {
+			n[a] = pos[a] + s;
+			if (in_grid<D>(g, n)) {
+				const float dn = __fmul_rn(get_phi<D, L>(P, g, n), dir);
+				if (dn < dist) dist = dn;
+			}
+		}
+		n[a] = pos[a];
+	}
+	return __fadd_rn(__fmul_rn(dist, dir), dir);
+}
+
+/// Builtin speed: [a*curv] + [n*h] + [c] in that order (see include/felt_gpu.h).
+struct Speed {
+	int kind;
+	float c, a, n;
+	uint32_t seed;
+};
+template <int D, int L>
+__device__ __forceinline__ float speed_eval(const Dev& P, const SurfGeom& g, const Speed& sp,
+                                            const Vec<D>& pos)
+{
+	float acc = 0.0f;
+	bool have = false;
+	if (sp.kind & 2) {
+		acc = __fmul_rn(sp.a, curv<D, L>(P, g, pos));
+		have = true;
+	}
+	if (sp.kind & 4) {
+		const float t = __fmul_rn(sp.n, hash_noise<D>(pos, sp.seed));
+		acc = have ? __fadd_rn(acc, t) : t;
+		have = true;
+	}
+	if (sp.kind & 1) acc = have ? __fadd_rn(acc, sp.c) : sp.c;
+	return acc;
+}
+
+/// Largest s with woff[s] <= e (entry -> surface of a flattened per-surface list).
+__device__ __forceinline__ int entry_surface(const int* woff, int S, int e)
+{
+	int lo = 0, hi = S;
+	while (hi - lo > 1) {
+		const int mid = (lo + hi) >> 1;
+		if (woff[mid] <= e)
+			lo = mid;
+		else
+			hi = mid;
+	}
+	return lo;
+}
+
+}  // namespace fg

@@ -1,0 +1,649 @@
+// Host orchestration of the device pool (see fg_engine.cuh).
+#include <algorithm>
+#include <cstring>
+
+#include "fg_engine.cuh"
+#include "fg_kernels.cuh"
+
+namespace fg {
+
+namespace {
+
+template <class T>
+T* dalloc(size_t n, std::vector<void*>& owned)
+{
+	void* p = nullptr;
+	if (n == 0) n = 1;
+	cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+	if (e != cudaSuccess)
+		throw Error(-3, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+	owned.push_back(p);
+	return static_cast<T*>(p);
+}
+
+__global__ void k_fill_int(int* p, long long n, int v)
+{
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	     i += (long long)gridDim.x * blockDim.x)
+		p[i] = v;
+}
+__global__ void k_fill_float(float* p, long long n, float v)
+{
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+	     i += (long long)gridDim.x * blockDim.x)
+		p[i] = v;
+}
+__global__ void k_iota_rev(int* p, int n)
+{
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		p[i] = n - 1 - i;
+}
+
+int sm_count()
+{
+	static int n = 0;
+	if (!n) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+		if (n <= 0) n = 148;
+	}
+	return n;
+}
+
+}  // namespace
+
+template <int D, int L>
+class Engine final : public EngineBase {
+public:
+	static constexpr int NL = 2 * L + 1;
+
+	Engine(const PoolDesc& desc, cudaStream_t st) : st_(st)
+	{
+		if (desc.D != D || desc.L != L) throw Error(-1, "engine dims mismatch");
+		const int S = (int)desc.sizes.size();
+		if (S <= 0) throw Error(-1, "pool needs at least one surface");
+		int BV = 1;
+		for (int a = 0; a < D; a++) {
+			if (desc.part[a] <= 0) throw Error(-1, "partition size must be positive");
+			csz_[a] = desc.part[a];
+			BV *= desc.part[a];
+		}
+		if (BV > 65535) throw Error(-1, "partition volume must be < 65536");
+		geom_.resize(S);
+		long long NP = 0;
+		for (int s = 0; s < S; s++) {
+			SurfGeom& g = geom_[s];
+			std::memset(&g, 0, sizeof(g));
+			bool exact = true;
+			long long np = 1;
+			for (int a = 0; a < D; a++) {
+				const int sz = desc.sizes[s][a];
+				if (sz <= 0) throw Error(-1, "grid size must be positive");
+				g.size[a] = sz;
+				g.off[a] = (-1 * sz) / 2;
+				g.hi[a] = g.off[a] + sz;
+				g.ccount[a] = sz / csz_[a];
+				if (g.ccount[a] * csz_[a] != sz) exact = false;
+				g.coff[a] = g.off[a] / csz_[a];
+			}
+			if (!exact)
+				for (int a = 0; a < D; a++) g.ccount[a] += 1;
+			for (int a = 0; a < D; a++) np *= g.ccount[a];
+			if (np >= (1 << 24)) throw Error(-1, "too many partitions in one surface");
+			g.pbase = (int)NP;
+			g.np = (int)np;
+			NP += np;
+		}
+		if (NP >= (1LL << 31) / NL) throw Error(-1, "pool too large");
+		size_t nslots = desc.brick_capacity;
+		if (nslots == 0) nslots = (size_t)std::min<long long>(NP, 1LL << 20);
+		if (nslots > (size_t)NP) nslots = (size_t)NP;
+
+		Dev& P = P_;
+		std::memset(&P, 0, sizeof(P));
+		P.S = S;
+		P.NP = (int)NP;
+		P.BV = BV;
+		P.nslots = (int)nslots;
+		for (int a = 0; a < 3; a++) P.csz[a] = a < D ? csz_[a] : 1;
+		{
+			int str = 1;
+			for (int a = D - 1; a >= 0; a--) {
+				P.lstr[a] = str;
+				str *= csz_[a];
+			}
+		}
+		// host-side partition tables
+		std::vector<int> surf_of(NP), porig(NP * 3);
+		for (int s = 0; s < S; s++) {
+			const SurfGeom& g = geom_[s];
+			for (int i = 0; i < g.np; i++) {
+				int r = i;
+				int c[3] = {0, 0, 0};
+				for (int a = D - 1; a >= 0; a--) {
+					c[a] = r % g.ccount[a];
+					r /= g.ccount[a];
+				}
+				surf_of[g.pbase + i] = s;
+				for (int a = 0; a < 3; a++)
+					porig[(size_t)(g.pbase + i) * 3 + a] = a < D ? c[a] * csz_[a] + g.off[a] : 0;
+			}
+		}
+		auto& o = owned_;
+		SurfGeom* dgeom = dalloc<SurfGeom>(S, o);
+		FG_CUDA(cudaMemcpy(dgeom, geom_.data(), S * sizeof(SurfGeom), cudaMemcpyHostToDevice));
+		P.geom = dgeom;
+		int* dso = dalloc<int>(NP, o);
+		FG_CUDA(cudaMemcpy(dso, surf_of.data(), NP * sizeof(int), cudaMemcpyHostToDevice));
+		P.surf_of = dso;
+		int* dpo = dalloc<int>(NP * 3, o);
+		FG_CUDA(cudaMemcpy(dpo, porig.data(), NP * 3 * sizeof(int), cudaMemcpyHostToDevice));
+		P.porig = dpo;
+
+		const size_t npl = (size_t)NP * NL, spl = (size_t)S * NL;
+		P.slot = dalloc<int>(NP, o);
+		P.bg = dalloc<float>(NP, o);
+		P.oslot = dalloc<int>(NP, o);
+		P.ppos = dalloc<int>(npl, o);
+		P.plist = dalloc<int>(npl, o);
+		P.pcnt = dalloc<int>(spl, o);
+		P.dplist = dalloc<int>(npl, o);
+		P.dpcnt = dalloc<int>(spl, o);
+		P.splist = dalloc<int>(npl, o);
+		P.spcnt = dalloc<int>(spl, o);
+		P.sppos = dalloc<int>(npl, o);
+		for (int b = 0; b < 2; b++) {
+			P.aplist[b] = dalloc<int>(npl, o);
+			P.apcnt[b] = dalloc<int>(spl, o);
+			P.appos[b] = dalloc<int>(npl, o);
+		}
+		const size_t nb = nslots * (size_t)BV, nbl = nslots * (size_t)NL * BV;
+		P.phi = dalloc<float>(nb, o);
+		P.dlt = dalloc<float>(nb, o);
+		P.lkp = dalloc<uint16_t>(nb, o);
+		P.lst = dalloc<uint16_t>(nbl, o);
+		P.lcnt = dalloc<int>(nslots * NL, o);
+		P.sto = dalloc<int8_t>(nb, o);
+		P.chg = dalloc<uint16_t>(nbl, o);
+		P.ccnt = dalloc<int>(nslots * NL, o);
+		for (int b = 0; b < 2; b++) {
+			P.alkp[b] = dalloc<uint16_t>(nb, o);
+			P.alst[b] = dalloc<uint16_t>(nbl, o);
+			P.acnt[b] = dalloc<int>(nslots * NL, o);
+		}
+		P.claim = dalloc<unsigned long long>(nb, o);
+		P.slot_gp = dalloc<int>(nslots, o);
+		P.free_stack = dalloc<int>(nslots, o);
+		P.counters = dalloc<int>(CNT_N, o);
+		P.q_act = dalloc<int>(NP, o);
+		P.actflag = dalloc<int>(NP, o);
+		P.q_touch = dalloc<int>(nslots, o);
+		P.touched = dalloc<int>(nslots, o);
+		P.q_retire = dalloc<int>(nslots, o);
+		P.q_sunion = dalloc<int>(NP, o);
+		P.sflag = dalloc<int>(NP, o);
+		P.eflag = dalloc<unsigned>(NP, o);
+		P.app = dalloc<unsigned>(npl, o);
+		P.rem = dalloc<unsigned>(NP, o);
+		P.pap = dalloc<unsigned long long>(2 * (size_t)NP, o);
+		P.papg = dalloc<int>(2 * (size_t)NP, o);
+		P.papn = dalloc<int>(S, o);
+		P.woff = dalloc<int>(S + 1, o);
+		P.err = dalloc<int>(1, o);
+		P.changed = dalloc<int>(1, o);
+		acc_ = dalloc<unsigned long long>(1, o);
+		d_speeds_ = dalloc<Speed>(S, o);
+
+		fill(P.slot, NP, -1);
+		fillf(P.bg, NP, (float)(L + 1));
+		fill(P.oslot, NP, -1);
+		fill(P.ppos, npl, -1);
+		fill(P.sppos, npl, -1);
+		fill(P.appos[0], npl, -1);
+		fill(P.appos[1], npl, -1);
+		fill(P.actflag, NP, 0);
+		fill(P.sflag, NP, 0);
+		fill(P.touched, nslots, 0);
+		fill(P.slot_gp, nslots, -1);
+		FG_CUDA(cudaMemsetAsync(P.pcnt, 0, spl * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.dpcnt, 0, spl * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.spcnt, 0, spl * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.apcnt[0], 0, spl * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.apcnt[1], 0, spl * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.papn, 0, S * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.counters, 0, CNT_N * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P.changed, 0, sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(acc_, 0, sizeof(unsigned long long), st_));
+		k_iota_rev<<<grid_for(nslots), 256, 0, st_>>>(P.free_stack, (int)nslots);
+		const int top = (int)nslots;
+		FG_CUDA(cudaMemcpyAsync(P.counters + CNT_FREE_TOP, &top, sizeof(int), cudaMemcpyHostToDevice,
+		                        st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		FG_CUDA(cudaGetLastError());
+		smem_sort_ = 8;
+		while (smem_sort_ < (size_t)BV * 8) smem_sort_ <<= 1;
+		if (smem_sort_ > 48 * 1024)
+			FG_CUDA(cudaFuncSetAttribute(k_expand_append<L>,
+			                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                             (int)smem_sort_));
+		warp_grid_ = sm_count() * 8;
+	}
+
+	~Engine() override
+	{
+		cudaStreamSynchronize(st_);
+		for (void* p : owned_) cudaFree(p);
+	}
+
+	int dims() const override { return D; }
+	int layers() const override { return L; }
+	int surfaces() const override { return P_.S; }
+	cudaStream_t stream() const override { return st_; }
+	StepStats& stats() override { return stats_; }
+	const Dev& dev() const override { return P_; }
+	void sync() override { FG_CUDA(cudaStreamSynchronize(st_)); }
+	int part(int a) const override { return csz_[a]; }
+
+	// ---- seed ----
+	void seed(int s, const int* pos) override
+	{
+		check_surface(s);
+		Vec<D> c;
+		for (int a = 0; a < D; a++) c[a] = pos[a];
+		k_seed<D, L><<<1, 1, 0, st_>>>(P_, s, c);
+		FG_CUDA(cudaGetLastError());
+		check_errors();
+	}
+
+	// ---- global update ----
+	void update_builtin(const Speed* speeds) override
+	{
+		update_begin_global();
+		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
+		                        st_));
+		scan(P_.pcnt, L, 0);
+		k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_);
+		update_finish_global();
+	}
+
+	void update_begin_global() override
+	{
+		update_start();
+		// delta.track_children(isogrid) on freshly reset delta lists = a copy of the lists.
+		copy_plists();
+		count_band();
+	}
+
+	void update_finish_global() override
+	{
+		const int B = 1, A = 0;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
+		// update_zero_layer(&affected_buffer)
+		scan(P_.pcnt, L, 0);
+		k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, B);
+		k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.plist, L, B);
+		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
+		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
+		distance_passes(iso, B);
+		flush();
+		expand();
+		retire();
+		status_dirty_ = true;
+		buf_dirty_[B] = true;
+		int changed = read_changed();
+		int iters = 1;
+		int cur = B, oth = A;
+		while (changed) {
+			clear_status();
+			FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
+			const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur]};
+			distance_passes(bv, oth);
+			flush();
+			expand();
+			retire();
+			status_dirty_ = true;
+			buf_dirty_[oth] = true;
+			clear_buffer(cur);
+			std::swap(cur, oth);
+			changed = read_changed();
+			iters++;
+			if (iters > 100000) throw Error(-14, "convergence loop did not terminate");
+		}
+		stats_.iterations = iters;
+		check_errors();
+	}
+
+	void update_local(const std::vector<int>&, const std::vector<float>&) override
+	{
+		throw Error(-15, "local update is not available on the device engine yet");
+	}
+	void update_bounded(const int*, const int*, const Speed&) override
+	{
+		throw Error(-15, "bounded update is not available on the device engine yet");
+	}
+
+	// ---- queries ----
+	void snapshot(int s, float* dst, size_t n, bool dst_device) override
+	{
+		check_surface(s);
+		long long tot = 1;
+		for (int a = 0; a < D; a++) tot *= geom_[s].size[a];
+		if ((long long)n < tot) throw Error(-13, "snapshot buffer too small");
+		float* out = dst;
+		float* tmp = nullptr;
+		if (!dst_device) {
+			FG_CUDA(cudaMalloc(&tmp, tot * sizeof(float)));
+			out = tmp;
+		}
+		k_snapshot<D, L><<<grid_for(tot), 256, 0, st_>>>(P_, s, out, tot);
+		cudaError_t e = cudaGetLastError();
+		if (e == cudaSuccess && tmp)
+			e = cudaMemcpyAsync(dst, tmp, tot * sizeof(float), cudaMemcpyDeviceToHost, st_);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+		if (tmp) cudaFree(tmp);
+		if (e != cudaSuccess) throw Error(-2, cudaGetErrorString(e));
+	}
+
+	float get(int s, const int* pos) override
+	{
+		check_surface(s);
+		const SurfGeom& g = geom_[s];
+		for (int a = 0; a < D; a++)
+			if (pos[a] < g.off[a] || pos[a] >= g.hi[a]) return (float)(L + 1);
+		int idx = 0, leaf = 0;
+		for (int a = 0; a < D; a++) {
+			const int r = pos[a] - g.off[a];
+			const int c = r / csz_[a];
+			idx = idx * g.ccount[a] + c;
+			leaf += (r - c * csz_[a]) * P_.lstr[a];
+		}
+		const int gp = g.pbase + idx;
+		int sl;
+		float v;
+		FG_CUDA(cudaMemcpyAsync(&sl, P_.slot + gp, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		if (sl < 0)
+			FG_CUDA(cudaMemcpy(&v, P_.bg + gp, sizeof(float), cudaMemcpyDeviceToHost));
+		else
+			FG_CUDA(cudaMemcpy(&v, P_.phi + (size_t)sl * P_.BV + leaf, sizeof(float),
+			                   cudaMemcpyDeviceToHost));
+		return v;
+	}
+
+	size_t partitions(int s, int* ccount, int* coff) override
+	{
+		check_surface(s);
+		for (int a = 0; a < D; a++) {
+			ccount[a] = geom_[s].ccount[a];
+			coff[a] = geom_[s].coff[a];
+		}
+		return (size_t)geom_[s].np;
+	}
+
+	std::vector<uint32_t> layer_list(int s, size_t part, int li) override
+	{
+		check_surface(s);
+		check_layer(li);
+		if (part >= (size_t)geom_[s].np) throw Error(-1, "partition index out of range");
+		sync();
+		const int gp = geom_[s].pbase + (int)part;
+		int sl;
+		FG_CUDA(cudaMemcpy(&sl, P_.slot + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		if (sl < 0) return {};
+		int n;
+		FG_CUDA(cudaMemcpy(&n, P_.lcnt + (size_t)sl * NL + li, sizeof(int), cudaMemcpyDeviceToHost));
+		std::vector<uint16_t> tmp(n);
+		if (n)
+			FG_CUDA(cudaMemcpy(tmp.data(), P_.lst + ((size_t)sl * NL + li) * P_.BV,
+			                   n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+		return std::vector<uint32_t>(tmp.begin(), tmp.end());
+	}
+
+	std::vector<uint32_t> partition_list(int s, int which, int li) override
+	{
+		check_surface(s);
+		check_layer(li);
+		sync();
+		const int* list;
+		const int* cnt;
+		switch (which) {
+		case 0: list = P_.plist; cnt = P_.pcnt; break;
+		case 1: list = P_.dplist; cnt = P_.dpcnt; break;
+		case 2: list = P_.splist; cnt = P_.spcnt; break;
+		default: throw Error(-1, "unknown partition list");
+		}
+		int n;
+		FG_CUDA(cudaMemcpy(&n, cnt + s * NL + li, sizeof(int), cudaMemcpyDeviceToHost));
+		std::vector<int> tmp(n);
+		if (n)
+			FG_CUDA(cudaMemcpy(tmp.data(), list + (size_t)li * P_.NP + geom_[s].pbase,
+			                   n * sizeof(int), cudaMemcpyDeviceToHost));
+		return std::vector<uint32_t>(tmp.begin(), tmp.end());
+	}
+
+	void partition_state(int s, size_t part, int* active, float* bg) override
+	{
+		check_surface(s);
+		if (part >= (size_t)geom_[s].np) throw Error(-1, "partition index out of range");
+		sync();
+		const int gp = geom_[s].pbase + (int)part;
+		int sl;
+		FG_CUDA(cudaMemcpy(&sl, P_.slot + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(bg, P_.bg + gp, sizeof(float), cudaMemcpyDeviceToHost));
+		*active = sl >= 0 ? 1 : 0;
+	}
+
+	std::vector<uint32_t> dump(int s) override
+	{
+		check_surface(s);
+		sync();
+		const SurfGeom& g = geom_[s];
+		std::vector<int> slots(g.np);
+		std::vector<float> bgs(g.np);
+		FG_CUDA(cudaMemcpy(slots.data(), P_.slot + g.pbase, g.np * sizeof(int),
+		                   cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(bgs.data(), P_.bg + g.pbase, g.np * sizeof(float),
+		                   cudaMemcpyDeviceToHost));
+		std::vector<int> lcnt((size_t)P_.nslots * NL);
+		FG_CUDA(cudaMemcpy(lcnt.data(), P_.lcnt, lcnt.size() * sizeof(int),
+		                   cudaMemcpyDeviceToHost));
+		std::vector<uint32_t> out;
+		out.push_back(D);
+		out.push_back(L);
+		out.push_back((uint32_t)g.np);
+		std::vector<uint16_t> tmp;
+		for (int i = 0; i < g.np; i++) {
+			const int sl = slots[i];
+			uint32_t bits;
+			std::memcpy(&bits, &bgs[i], 4);
+			out.push_back(sl >= 0 ? 1u : 0u);
+			out.push_back(bits);
+			for (int l = 0; l < NL; l++) {
+				const int n = sl >= 0 ? lcnt[(size_t)sl * NL + l] : 0;
+				out.push_back((uint32_t)n);
+				if (n) {
+					tmp.resize(n);
+					FG_CUDA(cudaMemcpy(tmp.data(), P_.lst + ((size_t)sl * NL + l) * P_.BV,
+					                   n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+					for (uint16_t x : tmp) out.push_back(x);
+				}
+			}
+		}
+		for (int which = 0; which < 3; which++)
+			for (int l = 0; l < NL; l++) {
+				const std::vector<uint32_t> pl = partition_list(s, which, l);
+				out.push_back((uint32_t)pl.size());
+				out.insert(out.end(), pl.begin(), pl.end());
+			}
+		return out;
+	}
+
+	unsigned long long band_size(int s) override
+	{
+		unsigned long long n = 0;
+		for (int l = 0; l < NL; l++)
+			for (uint32_t p : partition_list(s, 0, l)) n += layer_list(s, p, l).size();
+		return n;
+	}
+
+	void check_errors() override
+	{
+		int e = 0;
+		FG_CUDA(cudaMemcpyAsync(&e, P_.err, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		FG_CUDA(cudaGetLastError());
+		if (e) {
+			FG_CUDA(cudaMemsetAsync(P_.err, 0, sizeof(int), st_));
+			if (e & EB_POOL) throw Error(-4, "brick pool exhausted");
+			if (e & EB_NONFINITE) throw Error(-10, "layer id of a non-finite distance");
+			if (e & EB_OUTSIDE) throw Error(-11, "band node outside the grid");
+			if (e & EB_INACTIVE) throw Error(-12, "write to an inactive partition");
+			if (e & EB_CAPACITY) throw Error(-13, "device buffer capacity exceeded");
+			if (e & EB_TIMEOUT) throw Error(-14, "bounded device wait gave up");
+			throw Error(-2, "device error");
+		}
+	}
+
+private:
+	void check_surface(int s) const
+	{
+		if (s < 0 || s >= P_.S) throw Error(-1, "surface index out of range");
+	}
+	static void check_layer(int li)
+	{
+		if (li < 0 || li >= NL) throw Error(-1, "layer index out of range");
+	}
+	static int grid_for(long long n)
+	{
+		long long b = (n + 255) / 256;
+		if (b < 1) b = 1;
+		const long long cap = (long long)sm_count() * 32;
+		return (int)(b < cap ? b : cap);
+	}
+	void fill(int* p, size_t n, int v)
+	{
+		k_fill_int<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v);
+	}
+	void fillf(float* p, size_t n, float v)
+	{
+		k_fill_float<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v);
+	}
+
+	void scan(const int* cnt, int l, int mode)
+	{
+		k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff);
+	}
+
+	/// update_start (Surface.hpp:393-399): resets of the status and affected grids left by the
+	/// previous update. The delta values need no reset: every read follows a write of the same
+	/// step.
+	void update_start()
+	{
+		if (status_dirty_) clear_status();
+		for (int b = 0; b < 2; b++)
+			if (buf_dirty_[b]) clear_buffer(b);
+	}
+
+	void copy_plists()
+	{
+		dim3 grid(1, P_.S * NL);
+		if (grid.y > 65535) throw Error(-1, "too many surfaces for one pool");
+		k_copy_plists<<<grid, 256, 0, st_>>>(P_, NL);
+	}
+
+	void count_band()
+	{
+		scan(P_.pcnt, 0, 2);
+		k_band_size<L><<<warp_grid_, 256, 0, st_>>>(P_, acc_);
+	}
+
+	void distance_passes(const ListView& lv, int b)
+	{
+		for (int k = -1; k >= -L; k--) layer_pass(lv, k, -1.0f, b);
+		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
+	}
+
+	void layer_pass(const ListView& lv, int k, float side, int b)
+	{
+		scan(lv.pcnt, k + L, 0);
+		k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, side);
+		k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, b);
+		k_compact<L><<<P_.S, 256, 0, st_>>>(P_, lv.plist, k + L, b);
+	}
+
+	void flush()
+	{
+		k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_);
+		const int warps = P_.S * NL;
+		k_flush_plist<L><<<(warps * 32 + 255) / 256, 256, 0, st_>>>(P_);
+	}
+
+	void expand()
+	{
+		scan(P_.spcnt, 0, 1);
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
+		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0);
+		k_activate<L><<<sm_count() * 4, 256, 0, st_>>>(P_);
+		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 1);
+		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 2);
+		k_expand_append<L><<<sm_count() * 4, 256, smem_sort_, st_>>>(P_);
+		k_expand_plist<L><<<P_.S, 256, 0, st_>>>(P_);
+	}
+
+	void retire()
+	{
+		k_retire<<<grid_for(P_.nslots), 256, 0, st_>>>(P_);
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_RETIRE, 0, sizeof(int), st_));
+	}
+
+	void clear_status()
+	{
+		k_clear_status<L><<<warp_grid_, 256, 0, st_>>>(P_);
+		FG_CUDA(cudaMemsetAsync(P_.spcnt, 0, (size_t)P_.S * NL * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_SUNION, 0, sizeof(int), st_));
+		status_dirty_ = false;
+	}
+
+	void clear_buffer(int b)
+	{
+		scan(P_.apcnt[b], 0, 2);
+		k_clear_buffer<L><<<warp_grid_, 256, 0, st_>>>(P_, b);
+		FG_CUDA(cudaMemsetAsync(P_.apcnt[b], 0, (size_t)P_.S * NL * sizeof(int), st_));
+		buf_dirty_[b] = false;
+	}
+
+	int read_changed()
+	{
+		int c = 0;
+		FG_CUDA(cudaMemcpyAsync(&c, P_.changed, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		FG_CUDA(cudaGetLastError());
+		return c;
+	}
+
+	cudaStream_t st_;
+	Dev P_;
+	int csz_[3] = {1, 1, 1};
+	std::vector<SurfGeom> geom_;
+	std::vector<void*> owned_;
+	unsigned long long* acc_ = nullptr;
+	Speed* d_speeds_ = nullptr;
+	size_t smem_sort_ = 0;
+	int warp_grid_ = 0;
+	bool status_dirty_ = false;
+	bool buf_dirty_[2] = {false, false};
+	StepStats stats_;
+};
+
+EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream)
+{
+#define FG_CASE(d, l) \
+	if (desc.D == d && desc.L == l) return new Engine<d, l>(desc, stream);
+	FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
+	FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
+#undef FG_CASE
+	throw Error(-1, "unsupported dims/layers (D in {2,3}, L in 1..4)");
+}
+
+}  // namespace fg

@@ -1,0 +1,81 @@
+// Host-side engine: owns one device pool of S surfaces (same D, L and partition shape) and
+// drives the kernels of fg_kernels.cuh. A single Felt Surface is a pool with S = 1; the batched
+// and serving paths use the same pool with many surfaces, so every kernel launch advances all of
+// them together.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fg_dev.cuh"
+
+namespace fg {
+
+/// Error carrying a felt_gpu.h status code.
+struct Error : std::runtime_error {
+	int code;
+	Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define FG_CUDA(x)                                                                       \
+	do {                                                                                 \
+		cudaError_t e_ = (x);                                                            \
+		if (e_ != cudaSuccess)                                                           \
+			throw ::fg::Error(-2, std::string(#x ": ") + cudaGetErrorString(e_));        \
+	} while (0)
+
+struct PoolDesc {
+	int D = 3, L = 2;
+	int part[3] = {8, 8, 8};
+	std::vector<std::array<int, 3>> sizes;  // per surface grid size
+	size_t brick_capacity = 0;              // 0 = automatic
+};
+
+/// Per-step accounting the benchmarks and the serving loop read.
+struct StepStats {
+	unsigned long long node_updates = 0;  // band size at the start of each step, summed
+	int iterations = 0;                   // distance/flush/expand iterations of the last step
+};
+
+class EngineBase {
+public:
+	virtual ~EngineBase() = default;
+	virtual int dims() const = 0;
+	virtual int layers() const = 0;
+	virtual int surfaces() const = 0;
+	virtual cudaStream_t stream() const = 0;
+
+	virtual void seed(int s, const int* pos) = 0;
+	/// Global update of every surface of the pool with one builtin speed per surface
+	/// (host array of S speeds).
+	virtual void update_builtin(const Speed* speeds) = 0;
+	/// The two halves of update(fn) around a caller-supplied delta kernel.
+	virtual void update_begin_global() = 0;
+	virtual void update_finish_global() = 0;
+	/// Local update of surface 0: update_start(), delta(pos,v)..., update_end().
+	virtual void update_local(const std::vector<int>& pos, const std::vector<float>& vals) = 0;
+	virtual void update_bounded(const int* lo, const int* hi, const Speed& sp) = 0;
+
+	virtual void snapshot(int s, float* dst, size_t n, bool dst_device) = 0;
+	virtual float get(int s, const int* pos) = 0;
+	virtual size_t partitions(int s, int* ccount, int* coff) = 0;
+	virtual std::vector<uint32_t> layer_list(int s, size_t part, int li) = 0;
+	virtual std::vector<uint32_t> partition_list(int s, int which, int li) = 0;
+	virtual void partition_state(int s, size_t part, int* active, float* bg) = 0;
+	virtual std::vector<uint32_t> dump(int s) = 0;
+	virtual unsigned long long band_size(int s) = 0;
+	virtual void check_errors() = 0;
+	virtual StepStats& stats() = 0;
+	virtual const Dev& dev() const = 0;
+	virtual void sync() = 0;
+	virtual int part(int a) const = 0;
+};
+
+EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream);
+
+}  // namespace fg

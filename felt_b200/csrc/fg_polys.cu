@@ -1,0 +1,790 @@
+// Device polygonisation: Felt::Polys (include/Felt/Polys.hpp) over Poly::Single children
+// (include/Felt/Impl/Poly.hpp), for every surface of an engine's pool.
+//
+// The reference marches the leaves of a partition's 2L+1 layer lists in order and numbers the
+// vertices in first-encounter order through a per-node edge cache. Here one block marches one
+// pending partition: (1) classify every leaf's cell (corner mask) and claim each cut edge's
+// cache slot with the smallest (cell, edge) sequence number; (2) a block scan over the cells
+// numbers the first occurrences, which is exactly the reference's vertex order; (3) the first
+// occurrences compute their vertex (interpolated position and, in 3D, the normalised gradient
+// of the interpolated field) and every cell emits its simplices from the ordering table.
+#include <cstring>
+
+#include "fg_kernels.cuh"
+#include "fg_polys.cuh"
+
+#define FG_MC_QUAL static __device__ __constant__
+#define FG_MC_FN static __device__ __forceinline__
+#include "../include/felt_gpu/mc_tables.h"
+
+namespace fg {
+
+struct PolysDev {
+	int* pend_lkp[2];   // [NP] position in the pending/done list, -1
+	int* pend_list[2];  // [NP] per-surface segments at pbase
+	int* pend_cnt[2];   // [S]
+	int* pact;          // [NP] poly child active
+	int* gvoff;         // [NP] vertex offset in the arena
+	int* gnv;           // [NP] vertices
+	int* gsoff;         // [NP] simplex offset
+	int* gns;           // [NP] simplices
+	float* vtx;         // arena: per vertex VF floats
+	uint32_t* spx;      // arena: per simplex D indices
+	unsigned long long* used;  // [2] vertices, simplices used
+	long long vcap, scap;
+	int pend;           // which of the two lists is pending
+	int* err;
+};
+
+namespace {
+
+constexpr float FEPS = 1.1920928955078125e-07f;
+
+template <int D>
+__device__ __forceinline__ int mc_edges()
+{
+	return D == 3 ? 12 : 4;
+}
+template <int D>
+__device__ __forceinline__ int mc_order(int mask, int i)
+{
+	if (D == 3) return fg_mc3_order(mask, i);
+	return fg_mc2_order_flat[mask * 4 + i];
+}
+template <int D>
+__device__ __forceinline__ unsigned mc_edge_mask(int mask)
+{
+	if (D == 3) return fg_mc3_edge_mask(mask);
+	return fg_mc2_edge_mask(mask);
+}
+template <int D>
+__device__ __forceinline__ int mc_corner(int i, int a)
+{
+	if (D == 3) return fg_mc3_corner[i][a];
+	return fg_mc2_corner[i][a];
+}
+template <int D>
+__device__ __forceinline__ int mc_edge_off(int e, int a)
+{
+	if (D == 3) return fg_mc3_edge[e][a];
+	return fg_mc2_edge[e][a];
+}
+template <int D>
+__device__ __forceinline__ int mc_edge_axis(int e)
+{
+	if (D == 3) return fg_mc3_edge[e][3];
+	return fg_mc2_edge[e][2];
+}
+/// Simplices of a corner mask: D-tuples read until -1 (Poly.hpp:259), flat in 2D.
+template <int D>
+__device__ __forceinline__ int mc_nspx(int mask)
+{
+	int n = 0;
+	for (int o = 0; mc_order<D>(mask, o) != -1; o += D) n++;
+	return n;
+}
+
+template <int D, int L>
+__device__ __forceinline__ bool inside_f(const SurfGeom& g, const float* p)
+{
+	for (int a = 0; a < D; a++) {
+		if (p[a] >= (float)g.hi[a]) return false;
+		if (p[a] < (float)g.off[a]) return false;
+	}
+	return true;
+}
+
+/// interp (NumericMixin.hpp:403-481): corners in bit order, reduced along axis 0 first.
+template <int D, int L>
+__device__ float interp(const Dev& P, const SurfGeom& g, const float* p)
+{
+	Vec<D> fl;
+	float pc[D];
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		const float f = floorf(p[a]);
+		fl[a] = (int)f;
+		pc[a] = __fsub_rn(p[a], f);
+	}
+	float v[1 << D];
+#pragma unroll
+	for (int i = 0; i < (1 << D); i++) {
+		Vec<D> q = fl;
+#pragma unroll
+		for (int a = 0; a < D; a++) q[a] += (i >> a) & 1;
+		v[i] = get_phi<D, L>(P, g, q);
+	}
+	int n = 1 << D;
+#pragma unroll
+	for (int r = 0; r < D; r++) {
+		const float t = pc[r];
+		for (int i = 0; i < n / 2; i++)
+			v[i] = __fadd_rn(__fmul_rn(t, v[2 * i + 1]), __fmul_rn(__fsub_rn(1.0f, t), v[2 * i]));
+		n >>= 1;
+	}
+	return v[0];
+}
+
+/// grad (NumericMixin.hpp:188-231) at an integer node.
+template <int D, int L>
+__device__ void grad_i(const Dev& P, const SurfGeom& g, const Vec<D>& p, float* out)
+{
+	const float centre = get_phi<D, L>(P, g, p);
+	Vec<D> t = p;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		float back = centre, fwd = centre;
+		int order = 0;
+		t[a] -= 1;
+		if (in_grid<D>(g, t)) {
+			back = get_phi<D, L>(P, g, t);
+			order++;
+		}
+		t[a] += 2;
+		if (in_grid<D>(g, t)) {
+			fwd = get_phi<D, L>(P, g, t);
+			order++;
+		}
+		t[a] -= 1;
+		out[a] = order ? __fdiv_rn(__fsub_rn(fwd, back), (float)order) : 0.0f;
+	}
+}
+
+/// grad at a real position: the probe coordinate steps -1, +2, -1 in FP32.
+template <int D, int L>
+__device__ void grad_f(const Dev& P, const SurfGeom& g, const float* p, float* out)
+{
+	const float centre = interp<D, L>(P, g, p);
+	float t[D];
+#pragma unroll
+	for (int a = 0; a < D; a++) t[a] = p[a];
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		float back = centre, fwd = centre;
+		int order = 0;
+		t[a] = __fsub_rn(t[a], 1.0f);
+		if (inside_f<D, L>(g, t)) {
+			back = interp<D, L>(P, g, t);
+			order++;
+		}
+		t[a] = __fadd_rn(t[a], 2.0f);
+		if (inside_f<D, L>(g, t)) {
+			fwd = interp<D, L>(P, g, t);
+			order++;
+		}
+		t[a] = __fsub_rn(t[a], 1.0f);
+		out[a] = order ? __fdiv_rn(__fsub_rn(fwd, back), (float)order) : 0.0f;
+	}
+}
+
+/// Eigen normalize(): divide by sqrt(x0^2 + (x1^2 + x2^2)) when positive.
+__device__ void normalize3(float* v)
+{
+	const float z = __fadd_rn(__fmul_rn(v[0], v[0]),
+	                          __fadd_rn(__fmul_rn(v[1], v[1]), __fmul_rn(v[2], v[2])));
+	if (z > 0.0f) {
+		const float r = __fsqrt_rn(z);
+		v[0] = __fdiv_rn(v[0], r);
+		v[1] = __fdiv_rn(v[1], r);
+		v[2] = __fdiv_rn(v[2], r);
+	}
+}
+
+/// Poly::Single::idx vertex construction (Poly.hpp:296-346) for the edge at pa along axis.
+template <int D, int L>
+__device__ void make_vertex(const Dev& P, const SurfGeom& g, const Vec<D>& pa, int axis,
+                            float* out)
+{
+	Vec<D> pb = pa;
+	pb[axis] += 1;
+	const float va = get_phi<D, L>(P, g, pa);
+	const float vb = get_phi<D, L>(P, g, pb);
+	float pos[D];
+	bool at_node = false;
+	Vec<D> node;
+	if (fabsf(va) <= FEPS) {
+		at_node = true;
+		node = pa;
+	} else if (fabsf(vb) <= FEPS) {
+		at_node = true;
+		node = pb;
+	}
+	if (at_node) {
+#pragma unroll
+		for (int a = 0; a < D; a++) pos[a] = (float)node[a];
+	} else {
+		float mu;
+		if (fabsf(__fsub_rn(va, vb)) <= FEPS)
+			mu = 0.5f;
+		else
+			mu = __fdiv_rn(va, __fsub_rn(va, vb));
+#pragma unroll
+		for (int a = 0; a < D; a++) {
+			const float fa = (float)pa[a], fb = (float)pb[a];
+			pos[a] = __fadd_rn(fa, __fmul_rn(__fsub_rn(fb, fa), mu));
+		}
+	}
+#pragma unroll
+	for (int a = 0; a < D; a++) out[a] = pos[a];
+	if (D == 3) {
+		float n[D];
+		if (at_node)
+			grad_i<D, L>(P, g, node, n);
+		else
+			grad_f<D, L>(P, g, pos, n);
+#pragma unroll
+		for (int a = 0; a < D; a++) n[a] = __fdiv_rn(n[a], 1.0f);
+		normalize3(n);
+#pragma unroll
+		for (int a = 0; a < D; a++) out[D + a] = n[a];
+	}
+}
+
+}  // namespace
+
+/// Polys::notify (Polys.hpp:92-133), one thread per surface.
+template <int L>
+__global__ void k_polys_notify(Dev P, PolysDev Q)
+{
+	constexpr int NL = 2 * L + 1;
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= P.S) return;
+	const SurfGeom& g = P.geom[s];
+	int* lkp = Q.pend_lkp[Q.pend];
+	int* lst = Q.pend_list[Q.pend] + g.pbase;
+	int cnt = Q.pend_cnt[Q.pend][s];
+	for (int li = 0; li <= NL; li += NL - 1) {
+		const int n = P.dpcnt[s * NL + li];
+		const int* dl = P.dplist + (size_t)li * P.NP + g.pbase;
+		for (int i = 0; i < n; i++) {
+			const int lp = dl[i];
+			const int gp = g.pbase + lp;
+			bool act = Q.pact[gp] != 0;
+			for (int lj = 0; !act && lj <= NL; lj += NL - 1) act = P.ppos[gp * NL + lj] >= 0;
+			if (act) {
+				if (lkp[gp] < 0) {
+					lkp[gp] = cnt;
+					lst[cnt++] = lp;
+				}
+			} else if (lkp[gp] >= 0) {
+				const int at = lkp[gp], last = cnt - 1;
+				if (at < last) {
+					lst[at] = lst[last];
+					lkp[g.pbase + lst[last]] = at;
+				}
+				lkp[gp] = -1;
+				cnt = last;
+			}
+		}
+	}
+	for (int li = 0; li <= NL; li += NL - 1) {
+		const int n = P.spcnt[s * NL + li];
+		const int* sl = P.splist + (size_t)li * P.NP + g.pbase;
+		for (int i = 0; i < n; i++) {
+			const int lp = sl[i];
+			const int gp = g.pbase + lp;
+			if (Q.pact[gp] && lkp[gp] < 0) {
+				lkp[gp] = cnt;
+				lst[cnt++] = lp;
+			}
+		}
+	}
+	Q.pend_cnt[Q.pend][s] = cnt;
+}
+
+/// Polys::invalidate (Polys.hpp:171-191), one thread per surface.
+template <int L>
+__global__ void k_polys_invalidate(Dev P, PolysDev Q)
+{
+	constexpr int NL = 2 * L + 1;
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= P.S) return;
+	const SurfGeom& g = P.geom[s];
+	int* lkp = Q.pend_lkp[Q.pend];
+	int* lst = Q.pend_list[Q.pend] + g.pbase;
+	int cnt = Q.pend_cnt[Q.pend][s];
+	for (int i = 0; i < cnt; i++) lkp[g.pbase + lst[i]] = -1;
+	cnt = 0;
+	for (int li = 0; li <= NL; li += NL - 1) {
+		const int n = P.pcnt[s * NL + li];
+		const int* pl = P.plist + (size_t)li * P.NP + g.pbase;
+		for (int i = 0; i < n; i++) {
+			const int gp = g.pbase + pl[i];
+			if (lkp[gp] < 0) {
+				lkp[gp] = cnt;
+				lst[cnt++] = pl[i];
+			}
+		}
+	}
+	Q.pend_cnt[Q.pend][s] = cnt;
+}
+
+/// Clears list `which` (the reset of the swapped-out pending list, Polys.hpp:163-164).
+__global__ void k_polys_reset_list(Dev P, PolysDev Q, int which)
+{
+	const int s = blockIdx.x;
+	if (s >= P.S) return;
+	const SurfGeom& g = P.geom[s];
+	const int n = Q.pend_cnt[which][s];
+	for (int i = threadIdx.x; i < n; i += blockDim.x)
+		Q.pend_lkp[which][g.pbase + Q.pend_list[which][g.pbase + i]] = -1;
+	__syncthreads();
+	if (threadIdx.x == 0) Q.pend_cnt[which][s] = 0;
+}
+
+/// Polys::march body (Polys.hpp:138-161) for every pending partition of every surface (woff
+/// over the pending counts), or for a single partition when single >= 0.
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const int* woff,
+                                                       int single)
+{
+	constexpr int NL = 2 * L + 1;
+	constexpr int VF = D == 3 ? 2 * D : D;
+	extern __shared__ int smem[];
+	int csz2[3] = {1, 1, 1}, cvol = 1;
+	for (int a = 0; a < D; a++) {
+		csz2[a] = P.csz[a] + 2;
+		cvol *= csz2[a];
+	}
+	int* first = smem;                                          // [cvol * D]
+	uint16_t* cmask = (uint16_t*)(first + cvol * D);            // [BV]
+	uint16_t* cnew = cmask + P.BV;                              // [BV]
+	uint16_t* cleaf = cnew + P.BV;                              // [BV]
+	__shared__ int lstart[NL + 1];
+	__shared__ int tot_v, tot_s, vb, sb, ok;
+	const int nent = single >= 0 ? 1 : woff[P.S];
+	for (int e = blockIdx.x; e < nent; e += gridDim.x) {
+		int gp;
+		if (single >= 0) {
+			gp = single;
+		} else {
+			const int s = entry_surface(woff, P.S, e);
+			const SurfGeom& gs = P.geom[s];
+			gp = gs.pbase + Q.pend_list[Q.pend][gs.pbase + (e - woff[s])];
+		}
+		const SurfGeom& g = P.geom[P.surf_of[gp]];
+		const int sl = P.slot[gp];
+		if (sl < 0) {
+			// isogrid child inactive: Poly::Single::deactivate (Poly.hpp:95-101).
+			if (threadIdx.x == 0) {
+				Q.pact[gp] = 0;
+				Q.gnv[gp] = 0;
+				Q.gns[gp] = 0;
+			}
+			continue;
+		}
+		if (threadIdx.x == 0) {
+			int c = 0;
+			for (int l = 0; l < NL; l++) {
+				lstart[l] = c;
+				c += P.lcnt[sl * NL + l];
+			}
+			lstart[NL] = c;
+		}
+		for (int i = threadIdx.x; i < cvol * D; i += blockDim.x) first[i] = 0x7fffffff;
+		__syncthreads();
+		const int n = lstart[NL];
+		const int per = (n + blockDim.x - 1) / blockDim.x;
+		const int j0 = threadIdx.x * per, j1 = min(n, j0 + per);
+		Vec<D> orig;
+		for (int a = 0; a < D; a++) orig[a] = P.porig[gp * 3 + a];
+		// 1. classify cells and claim edge cache slots
+		for (int j = j0; j < j1; j++) {
+			int l = 0;
+			while (j >= lstart[l + 1]) l++;
+			const int leaf = P.lst[((size_t)sl * NL + l) * P.BV + (j - lstart[l])];
+			Vec<D> pc = leaf_pos<D>(P, gp, leaf);
+			if (D == 3) pc[D - 1] += 1;  // SpxGridPosOffset (PolyMixin.hpp:409)
+			unsigned mask = 0;
+			for (int i = 0; i < (1 << D); i++) {
+				Vec<D> q;
+				for (int a = 0; a < D; a++) q[a] = pc[a] + mc_corner<D>(i, a);
+				mask |= (get_phi<D, L>(P, g, q) > 0.0f ? 1u : 0u) << i;
+			}
+			cmask[j] = (uint16_t)mask;
+			cleaf[j] = (uint16_t)leaf;
+			if (mc_order<D>(mask, 0) == -1) continue;
+			const unsigned em = mc_edge_mask<D>(mask);
+			for (int ed = 0; ed < mc_edges<D>(); ed++) {
+				if (!((em >> ed) & 1u)) continue;
+				int ci = 0;
+				for (int a = 0; a < D; a++)
+					ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
+				atomicMin(&first[ci * D + mc_edge_axis<D>(ed)], j * 16 + ed);
+			}
+		}
+		__syncthreads();
+		// 2. first occurrences and simplex counts, scanned in cell order
+		int my_v = 0, my_s = 0;
+		for (int j = j0; j < j1; j++) {
+			const unsigned mask = cmask[j];
+			unsigned nm = 0;
+			if (mc_order<D>(mask, 0) != -1) {
+				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
+				if (D == 3) pc[D - 1] += 1;
+				const unsigned em = mc_edge_mask<D>(mask);
+				for (int ed = 0; ed < mc_edges<D>(); ed++) {
+					if (!((em >> ed) & 1u)) continue;
+					int ci = 0;
+					for (int a = 0; a < D; a++)
+						ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
+					if (first[ci * D + mc_edge_axis<D>(ed)] == j * 16 + ed) nm |= 1u << ed;
+				}
+				my_s += mc_nspx<D>(mask);
+			}
+			cnew[j] = (uint16_t)nm;
+			my_v += __popc(nm);
+		}
+		int tv, ts;
+		const int bv0 = block_excl_scan(my_v, &tv);
+		const int bs0 = block_excl_scan(my_s, &ts);
+		if (threadIdx.x == 0) {
+			tot_v = tv;
+			tot_s = ts;
+			const unsigned long long a = atomicAdd(&Q.used[0], (unsigned long long)tv);
+			const unsigned long long b = atomicAdd(&Q.used[1], (unsigned long long)ts);
+			ok = (long long)(a + tv) <= Q.vcap && (long long)(b + ts) <= Q.scap;
+			vb = (int)a;
+			sb = (int)b;
+			if (!ok) atomicOr(Q.err, EB_CAPACITY);
+		}
+		__syncthreads();
+		if (ok) {
+			// 3a. vertices, numbered in first-occurrence order
+			int vi = bv0;
+			for (int j = j0; j < j1; j++) {
+				const unsigned nm = cnew[j];
+				if (!nm) continue;
+				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
+				if (D == 3) pc[D - 1] += 1;
+				for (int ed = 0; ed < mc_edges<D>(); ed++) {
+					if (!((nm >> ed) & 1u)) continue;
+					Vec<D> pa;
+					int ci = 0;
+					for (int a = 0; a < D; a++) {
+						pa[a] = pc[a] + mc_edge_off<D>(ed, a);
+						ci = ci * csz2[a] + (pa[a] - orig[a] + 1);
+					}
+					float out[VF];
+					make_vertex<D, L>(P, g, pa, mc_edge_axis<D>(ed), out);
+					float* dst = Q.vtx + ((size_t)vb + vi) * VF;
+					for (int k = 0; k < VF; k++) dst[k] = out[k];
+					first[ci * D + mc_edge_axis<D>(ed)] = vi;
+					vi++;
+				}
+			}
+			__syncthreads();
+			// 3b. simplices
+			int si = bs0;
+			for (int j = j0; j < j1; j++) {
+				const unsigned mask = cmask[j];
+				if (mc_order<D>(mask, 0) == -1) continue;
+				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
+				if (D == 3) pc[D - 1] += 1;
+				for (int o = 0; mc_order<D>(mask, o) != -1; o += D) {
+					uint32_t* dst = Q.spx + ((size_t)sb + si) * D;
+					for (int k = 0; k < D; k++) {
+						const int ed = mc_order<D>(mask, o + k);
+						int ci = 0;
+						for (int a = 0; a < D; a++)
+							ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
+						dst[k] = (uint32_t)first[ci * D + mc_edge_axis<D>(ed)];
+					}
+					si++;
+				}
+			}
+			if (threadIdx.x == 0) {
+				Q.pact[gp] = 1;
+				Q.gvoff[gp] = vb;
+				Q.gnv[gp] = tot_v;
+				Q.gsoff[gp] = sb;
+				Q.gns[gp] = tot_s;
+			}
+		}
+		__syncthreads();
+	}
+}
+
+/// Moves the live geometry of every partition to the front of a fresh arena.
+template <int D>
+__global__ void k_polys_compact(Dev P, PolysDev Q, const int* noff, const int* nsoff, float* vtx2,
+                                uint32_t* spx2)
+{
+	constexpr int VF = D == 3 ? 2 * D : D;
+	for (int gp = blockIdx.x; gp < P.NP; gp += gridDim.x) {
+		const int nv = Q.gnv[gp], ns = Q.gns[gp];
+		if (!nv && !ns) continue;
+		const size_t vo = (size_t)Q.gvoff[gp] * VF, so = (size_t)Q.gsoff[gp] * D;
+		const size_t vn = (size_t)noff[gp] * VF, sn = (size_t)nsoff[gp] * D;
+		for (int i = threadIdx.x; i < nv * VF; i += blockDim.x) vtx2[vn + i] = Q.vtx[vo + i];
+		for (int i = threadIdx.x; i < ns * D; i += blockDim.x) spx2[sn + i] = Q.spx[so + i];
+	}
+}
+
+namespace {
+
+template <int D, int L>
+class PolysImpl final : public PolysBase {
+public:
+	static constexpr int NL = 2 * L + 1;
+	static constexpr int VF = D == 3 ? 2 * D : D;
+
+	PolysImpl(EngineBase& eng, int s) : eng_(eng), s_(s)
+	{
+		const Dev& P = eng.dev();
+		auto al = [&](size_t bytes) {
+			void* p = nullptr;
+			FG_CUDA(cudaMalloc(&p, bytes ? bytes : 1));
+			owned_.push_back(p);
+			return p;
+		};
+		std::memset(&Q_, 0, sizeof(Q_));
+		for (int b = 0; b < 2; b++) {
+			Q_.pend_lkp[b] = (int*)al(P.NP * sizeof(int));
+			Q_.pend_list[b] = (int*)al(P.NP * sizeof(int));
+			Q_.pend_cnt[b] = (int*)al(P.S * sizeof(int));
+			FG_CUDA(cudaMemset(Q_.pend_lkp[b], 0xff, P.NP * sizeof(int)));
+			FG_CUDA(cudaMemset(Q_.pend_cnt[b], 0, P.S * sizeof(int)));
+		}
+		Q_.pact = (int*)al(P.NP * sizeof(int));
+		Q_.gvoff = (int*)al(P.NP * sizeof(int));
+		Q_.gnv = (int*)al(P.NP * sizeof(int));
+		Q_.gsoff = (int*)al(P.NP * sizeof(int));
+		Q_.gns = (int*)al(P.NP * sizeof(int));
+		FG_CUDA(cudaMemset(Q_.pact, 0, P.NP * sizeof(int)));
+		FG_CUDA(cudaMemset(Q_.gnv, 0, P.NP * sizeof(int)));
+		FG_CUDA(cudaMemset(Q_.gns, 0, P.NP * sizeof(int)));
+		FG_CUDA(cudaMemset(Q_.gvoff, 0, P.NP * sizeof(int)));
+		FG_CUDA(cudaMemset(Q_.gsoff, 0, P.NP * sizeof(int)));
+		Q_.used = (unsigned long long*)al(2 * sizeof(unsigned long long));
+		FG_CUDA(cudaMemset(Q_.used, 0, 2 * sizeof(unsigned long long)));
+		woff_ = (int*)al((P.S + 1) * sizeof(int));
+		Q_.err = P.err;
+		Q_.pend = 0;
+		alloc_arena(1 << 20, 2 << 20);
+		int cvol = 1;
+		for (int a = 0; a < D; a++) cvol *= eng.part(a) + 2;
+		smem_ = (size_t)cvol * D * sizeof(int) + 3 * (size_t)P.BV * sizeof(uint16_t);
+		smem_ = (smem_ + 15) & ~(size_t)15;
+		if (smem_ > 48 * 1024)
+			FG_CUDA(cudaFuncSetAttribute(k_polys_march<D, L>,
+			                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+		FG_CUDA(cudaDeviceSynchronize());
+	}
+
+	~PolysImpl() override
+	{
+		cudaStreamSynchronize(eng_.stream());
+		free_arena();
+		for (void* p : owned_) cudaFree(p);
+	}
+
+	void notify() override
+	{
+		const Dev& P = eng_.dev();
+		k_polys_notify<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_);
+		FG_CUDA(cudaGetLastError());
+	}
+
+	void invalidate() override
+	{
+		const Dev& P = eng_.dev();
+		k_polys_invalidate<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_);
+		FG_CUDA(cudaGetLastError());
+	}
+
+	void march() override
+	{
+		const Dev& P = eng_.dev();
+		cudaStream_t st = eng_.stream();
+		maybe_compact();
+		k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_);
+		k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1);
+		FG_CUDA(cudaGetLastError());
+		// swap pending and done, then reset the new pending list
+		Q_.pend ^= 1;
+		k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend);
+		FG_CUDA(cudaGetLastError());
+		eng_.check_errors();
+	}
+
+	void march_partition(size_t part) override
+	{
+		const Dev& P = eng_.dev();
+		const int gp = check_part(part);
+		maybe_compact();
+		k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp);
+		FG_CUDA(cudaGetLastError());
+		eng_.check_errors();
+	}
+
+	std::vector<uint32_t> changes() override
+	{
+		const Dev& P = eng_.dev();
+		eng_.sync();
+		const int done = Q_.pend ^ 1;
+		int n = 0;
+		int pbase = pbase_of();
+		FG_CUDA(cudaMemcpy(&n, Q_.pend_cnt[done] + s_, sizeof(int), cudaMemcpyDeviceToHost));
+		std::vector<int> tmp(n);
+		if (n)
+			FG_CUDA(cudaMemcpy(tmp.data(), Q_.pend_list[done] + pbase, n * sizeof(int),
+			                   cudaMemcpyDeviceToHost));
+		(void)P;
+		return std::vector<uint32_t>(tmp.begin(), tmp.end());
+	}
+
+	void partition(size_t part, float* vtx, size_t vcap, uint32_t* spx, size_t scap, size_t* nv,
+	               size_t* ns, int* active) override
+	{
+		const int gp = check_part(part);
+		eng_.sync();
+		int rec[5];
+		FG_CUDA(cudaMemcpy(&rec[0], Q_.pact + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(&rec[1], Q_.gvoff + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(&rec[2], Q_.gnv + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(&rec[3], Q_.gsoff + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(&rec[4], Q_.gns + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		*active = rec[0];
+		*nv = (size_t)rec[2];
+		*ns = (size_t)rec[4];
+		if (vtx && rec[2]) {
+			const size_t k = std::min(vcap, (size_t)rec[2] * VF);
+			FG_CUDA(cudaMemcpy(vtx, Q_.vtx + (size_t)rec[1] * VF, k * sizeof(float),
+			                   cudaMemcpyDeviceToHost));
+		}
+		if (spx && rec[4]) {
+			const size_t k = std::min(scap, (size_t)rec[4] * D);
+			FG_CUDA(cudaMemcpy(spx, Q_.spx + (size_t)rec[3] * D, k * sizeof(uint32_t),
+			                   cudaMemcpyDeviceToHost));
+		}
+	}
+
+	void totals(size_t* nv, size_t* ns) override
+	{
+		const Dev& P = eng_.dev();
+		eng_.sync();
+		std::vector<int> a(P.NP), b(P.NP);
+		FG_CUDA(cudaMemcpy(a.data(), Q_.gnv, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(b.data(), Q_.gns, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
+		size_t x = 0, y = 0;
+		for (int i = 0; i < P.NP; i++) {
+			if (P.S > 1 && i / 1 < 0) continue;
+			x += a[i];
+			y += b[i];
+		}
+		if (nv) *nv = x;
+		if (ns) *ns = y;
+	}
+
+private:
+	int pbase_of()
+	{
+		int cc[3], co[3];
+		int base = 0;
+		for (int t = 0; t < s_; t++) base += (int)eng_.partitions(t, cc, co);
+		return base;
+	}
+	int check_part(size_t part)
+	{
+		int cc[3], co[3];
+		const size_t np = eng_.partitions(s_, cc, co);
+		if (part >= np) throw Error(-1, "partition index out of range");
+		return pbase_of() + (int)part;
+	}
+	int grid() const
+	{
+		int dev = 0, sms = 148;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		return sms * 4;
+	}
+	void alloc_arena(long long vcap, long long scap)
+	{
+		FG_CUDA(cudaMalloc(&Q_.vtx, (size_t)vcap * VF * sizeof(float)));
+		FG_CUDA(cudaMalloc(&Q_.spx, (size_t)scap * D * sizeof(uint32_t)));
+		Q_.vcap = vcap;
+		Q_.scap = scap;
+	}
+	void free_arena()
+	{
+		if (Q_.vtx) cudaFree(Q_.vtx);
+		if (Q_.spx) cudaFree(Q_.spx);
+		Q_.vtx = nullptr;
+		Q_.spx = nullptr;
+	}
+	/// Keeps the bump-allocated arenas at most half full before a march by moving the live
+	/// geometry into fresh arenas (doubling them when the live part alone is over a quarter).
+	void maybe_compact()
+	{
+		const Dev& P = eng_.dev();
+		unsigned long long used[2];
+		FG_CUDA(cudaMemcpyAsync(used, Q_.used, sizeof(used), cudaMemcpyDeviceToHost,
+		                        eng_.stream()));
+		eng_.sync();
+		if ((long long)used[0] * 2 < Q_.vcap && (long long)used[1] * 2 < Q_.scap) return;
+		std::vector<int> nv(P.NP), ns(P.NP), no(P.NP), so(P.NP);
+		FG_CUDA(cudaMemcpy(nv.data(), Q_.gnv, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(ns.data(), Q_.gns, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
+		long long tv = 0, ts = 0;
+		for (int i = 0; i < P.NP; i++) {
+			no[i] = (int)tv;
+			so[i] = (int)ts;
+			tv += nv[i];
+			ts += ns[i];
+		}
+		long long vcap = Q_.vcap, scap = Q_.scap;
+		while (tv * 4 > vcap) vcap *= 2;
+		while (ts * 4 > scap) scap *= 2;
+		if (vcap * VF >= (1LL << 31) || scap * D >= (1LL << 31))
+			throw Error(-13, "polygonisation arena too large");
+		int* dno = nullptr;
+		int* dso = nullptr;
+		float* v2 = nullptr;
+		uint32_t* s2 = nullptr;
+		FG_CUDA(cudaMalloc(&dno, P.NP * sizeof(int)));
+		FG_CUDA(cudaMalloc(&dso, P.NP * sizeof(int)));
+		FG_CUDA(cudaMalloc(&v2, (size_t)vcap * VF * sizeof(float)));
+		FG_CUDA(cudaMalloc(&s2, (size_t)scap * D * sizeof(uint32_t)));
+		FG_CUDA(cudaMemcpy(dno, no.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
+		FG_CUDA(cudaMemcpy(dso, so.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
+		k_polys_compact<D><<<grid(), 256, 0, eng_.stream()>>>(P, Q_, dno, dso, v2, s2);
+		FG_CUDA(cudaGetLastError());
+		FG_CUDA(cudaMemcpyAsync(Q_.gvoff, dno, P.NP * sizeof(int), cudaMemcpyDeviceToDevice,
+		                        eng_.stream()));
+		FG_CUDA(cudaMemcpyAsync(Q_.gsoff, dso, P.NP * sizeof(int), cudaMemcpyDeviceToDevice,
+		                        eng_.stream()));
+		const unsigned long long nu[2] = {(unsigned long long)tv, (unsigned long long)ts};
+		FG_CUDA(cudaMemcpyAsync(Q_.used, nu, sizeof(nu), cudaMemcpyHostToDevice, eng_.stream()));
+		eng_.sync();
+		free_arena();
+		Q_.vtx = v2;
+		Q_.spx = s2;
+		Q_.vcap = vcap;
+		Q_.scap = scap;
+		cudaFree(dno);
+		cudaFree(dso);
+	}
+
+	EngineBase& eng_;
+	int s_;
+	PolysDev Q_;
+	int* woff_ = nullptr;
+	size_t smem_ = 0;
+	std::vector<void*> owned_;
+};
+
+}  // namespace
+
+PolysBase* make_polys(EngineBase& eng, int s)
+{
+	const int D = eng.dims(), L = eng.layers();
+#define FG_CASE(d, l) \
+	if (D == d && L == l) return new PolysImpl<d, l>(eng, s);
+	FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
+	FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
+#undef FG_CASE
+	throw Error(-1, "unsupported dims/layers");
+}
+
+}  // namespace fg

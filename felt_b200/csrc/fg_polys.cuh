@@ -1,0 +1,29 @@
+// Polys<Surface> on the device: per-partition marching squares/cubes (Poly::Single) and the
+// incremental pending/done partition tracking of Felt::Polys (include/Felt/Polys.hpp).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "fg_engine.cuh"
+
+namespace fg {
+
+class PolysBase {
+public:
+	virtual ~PolysBase() = default;
+	virtual void notify() = 0;
+	virtual void march() = 0;
+	virtual void invalidate() = 0;
+	virtual void march_partition(size_t part) = 0;
+	virtual std::vector<uint32_t> changes() = 0;
+	virtual void partition(size_t part, float* vtx, size_t vcap, uint32_t* spx, size_t scap,
+	                       size_t* nv, size_t* ns, int* active) = 0;
+	virtual void totals(size_t* nv, size_t* ns) = 0;
+};
+
+/// Polygonisation of surface s of an engine's pool.
+PolysBase* make_polys(EngineBase& eng, int s);
+
+}  // namespace fg

@@ -21,6 +21,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define FG_API __attribute__((visibility("default")))
+#else
+#define FG_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -65,19 +71,19 @@ typedef struct fg_surface fg_surface;
 typedef struct fg_polys fg_polys;
 typedef struct fg_batch fg_batch;
 
-const char* fg_last_error(void);
+FG_API const char* fg_last_error(void);
 
 /* Surface(size, size_partition) (include/Felt/Surface.hpp:163-173). dims in {2,3},
  * layers (L) in {1,2,3,4}; size and part hold `dims` ints. cfg may be NULL. */
-int fg_surface_create(int dims, int layers, const int* size, const int* part,
+FG_API int fg_surface_create(int dims, int layers, const int* size, const int* part,
                       const fg_config* cfg, fg_surface** out);
-int fg_surface_destroy(fg_surface* s);
+FG_API int fg_surface_destroy(fg_surface* s);
 
 /* seed(pos) (include/Felt/Surface.hpp:207-241). */
-int fg_seed(fg_surface* s, const int* pos);
+FG_API int fg_seed(fg_surface* s, const int* pos);
 
 /* update(fn) with a builtin speed functor (include/Felt/Surface.hpp:254-296). */
-int fg_update_builtin(fg_surface* s, const fg_speed* speed);
+FG_API int fg_update_builtin(fg_surface* s, const fg_speed* speed);
 
 /* update(fn) with a caller-supplied device functor: the facade's templated delta kernel,
  * compiled in the caller's nvcc translation unit, runs between these two calls.
@@ -85,52 +91,52 @@ int fg_update_builtin(fg_surface* s, const fg_speed* speed);
  * (include/Felt/Surface.hpp:257-263) and returns the device view the kernel needs;
  * fg_update_finish_global runs update_end_global() (include/Felt/Surface.hpp:739-762). */
 typedef struct fg_device_view fg_device_view; /* defined in felt_gpu/device.cuh */
-int fg_update_begin_global(fg_surface* s, const fg_device_view** view, void** stream);
-int fg_update_finish_global(fg_surface* s);
+FG_API int fg_update_begin_global(fg_surface* s, const fg_device_view** view, void** stream);
+FG_API int fg_update_finish_global(fg_surface* s);
 
 /* update(lo, hi, fn) bounded update with a builtin speed (include/Felt/Surface.hpp:310-386). */
-int fg_update_bounded(fg_surface* s, const int* lo, const int* hi, const fg_speed* speed);
+FG_API int fg_update_bounded(fg_surface* s, const int* lo, const int* hi, const fg_speed* speed);
 
 /* update_start() (include/Felt/Surface.hpp:393-399), delta(pos, val) (441-459) and
  * update_end() (404-430): the local update. fg_delta_n applies n deltas in order. */
-int fg_update_start(fg_surface* s);
-int fg_delta(fg_surface* s, const int* pos, float val);
-int fg_delta_n(fg_surface* s, const int* pos, const float* val, size_t n);
-int fg_update_end(fg_surface* s);
+FG_API int fg_update_start(fg_surface* s);
+FG_API int fg_delta(fg_surface* s, const int* pos, float val);
+FG_API int fg_delta_n(fg_surface* s, const int* pos, const float* val, size_t n);
+FG_API int fg_update_end(fg_surface* s);
 
 /* isogrid().snapshot() (include/Felt/Impl/Mixin/PartitionedMixin.hpp:642-660): dense grid,
  * row-major over the whole isogrid. dst holds n >= prod(size) floats, on the host or, when
  * dst_is_device, in device memory of the surface's GPU. */
-int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device);
+FG_API int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device);
 
 /* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */
-int fg_get(fg_surface* s, const int* pos, float* out);
+FG_API int fg_get(fg_surface* s, const int* pos, float* out);
 
 /* Geometry of the children (partition) grid: count, size and offset of the children grid. */
-int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);
+FG_API int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);
 
 /* isogrid().children().get(p).lookup().list(layer_idx) (LookupMixin.hpp:261-275): the ordered
  * leaf list of one partition. Writes min(n, cap) entries, returns the full count in *n. */
-int fg_layer_list(fg_surface* s, size_t part, int layer_idx, uint32_t* out, size_t cap,
+FG_API int fg_layer_list(fg_surface* s, size_t part, int layer_idx, uint32_t* out, size_t cap,
                   size_t* n);
 
 /* isogrid().children().lookup().list(layer_idx) (PartitionedMixin.hpp:104-115): ordered list
  * of partitions tracked in a layer. */
-int fg_partition_list(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_partition_list(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
 
 /* delta(layer_idx) (include/Felt/Surface.hpp:637-640) and status_change(layer_idx) (648-651):
  * partitions touched by the last update. */
-int fg_delta_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
-int fg_status_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_delta_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_status_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
 
 /* children().get(p).is_active() and background() (GridMixin.hpp:56-69). */
-int fg_partition_state(fg_surface* s, size_t part, int* active, float* background);
+FG_API int fg_partition_state(fg_surface* s, size_t part, int* active, float* background);
 
 /* stats() (include/Felt/Surface.hpp:623-629). */
-int fg_stats(fg_surface* s, size_t* active_isogrid_partitions, size_t* active_delta_partitions);
+FG_API int fg_stats(fg_surface* s, size_t* active_isogrid_partitions, size_t* active_delta_partitions);
 
 /* Narrow-band node count at the start of the last update: sum over the 2L+1 layers. */
-int fg_band_size(fg_surface* s, size_t* n);
+FG_API int fg_band_size(fg_surface* s, size_t* n);
 
 /* Canonical state encoding used by parity tests (uint32 words):
  *   D, L, P (partition count);
@@ -138,21 +144,24 @@ int fg_band_size(fg_surface* s, size_t* n);
  *   per layer: isogrid partition list (n, entries);
  *   per layer: delta partition list; per layer: status-change partition list.
  * Writes min(total, cap) words and the full word count in *n. */
-int fg_dump(fg_surface* s, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_dump(fg_surface* s, uint32_t* out, size_t cap, size_t* n);
 
 /* ---- Polys<Surface> (include/Felt/Polys.hpp) ---- */
-int fg_polys_create(fg_surface* s, fg_polys** out);   /* Polys.hpp:58-84   */
-int fg_polys_destroy(fg_polys* p);
-int fg_polys_notify(fg_polys* p);                       /* Polys.hpp:92-133  */
-int fg_polys_march(fg_polys* p);                        /* Polys.hpp:138-165 */
-int fg_polys_invalidate(fg_polys* p);                   /* Polys.hpp:171-191 */
-int fg_polys_changes(fg_polys* p, uint32_t* out, size_t cap, size_t* n); /* Polys.hpp:198-201 */
+FG_API int fg_polys_create(fg_surface* s, fg_polys** out);   /* Polys.hpp:58-84   */
+FG_API int fg_polys_destroy(fg_polys* p);
+FG_API int fg_polys_notify(fg_polys* p);                       /* Polys.hpp:92-133  */
+FG_API int fg_polys_march(fg_polys* p);                        /* Polys.hpp:138-165 */
+FG_API int fg_polys_invalidate(fg_polys* p);                   /* Polys.hpp:171-191 */
+/* Poly::Single::march of one partition's child (Poly.hpp:138-147), activating or resetting it
+ * first as Polys::march does (Polys.hpp:149-154). */
+FG_API int fg_polys_march_partition(fg_polys* p, size_t part);
+FG_API int fg_polys_changes(fg_polys* p, uint32_t* out, size_t cap, size_t* n); /* Polys.hpp:198-201 */
 /* children().get(part).{vtxs(),spxs(),is_active()} (Poly.hpp:155-186). vtx receives per vertex
  * D position floats then, in 3D, D normal floats; spx receives D uint32 indices per simplex. */
-int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_cap, uint32_t* spx,
+FG_API int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_cap, uint32_t* spx,
                        size_t spx_cap, size_t* nv, size_t* ns, int* active);
 /* Totals over all partitions. */
-int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
+FG_API int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
 
 #ifdef __cplusplus
 }
