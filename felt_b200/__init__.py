@@ -74,6 +74,37 @@ def _fetch(fn, *args):
         cap = n.value
 
 
+def launch_count():
+    """Kernels launched by libfelt_gpu.so in this process."""
+    n = C.c_longlong()
+    _chk(lib().fg_launch_count(C.byref(n)))
+    return n.value
+
+
+def profile_enable(on=True):
+    """Bracket every library kernel launch with CUDA events (per-kernel device time)."""
+    _chk(lib().fg_profile_enable(1 if on else 0))
+
+
+def profile_reset():
+    _chk(lib().fg_profile_reset())
+
+
+def profile_read():
+    """{kernel name: (total ms, launches)} accumulated while profiling was enabled."""
+    n = C.c_size_t()
+    _chk(lib().fg_profile_count(C.byref(n)))
+    out = {}
+    name = C.create_string_buffer(128)
+    for i in range(n.value):
+        ms = C.c_double()
+        k = C.c_longlong()
+        _chk(lib().fg_profile_entry(C.c_size_t(i), name, C.c_size_t(128), C.byref(ms),
+                                    C.byref(k)))
+        out[name.value.decode()] = (ms.value, k.value)
+    return out
+
+
 def make_speed(c=None, a=None, n=None, seed=0):
     """Builtin speed: [a*curv] + [n*noise(pos, seed)] + [c], terms present when given."""
     kind = (SPEED_CURV if a is not None else 0) | (SPEED_NOISE if n is not None else 0) | (
@@ -174,6 +205,12 @@ class Surface:
     def band_size(self):
         n = C.c_size_t()
         _chk(lib().fg_band_size(self._h, C.byref(n)))
+        return n.value
+
+    def node_updates(self):
+        """Band nodes processed by all global updates so far (band size at each start)."""
+        n = C.c_ulonglong()
+        _chk(lib().fg_node_updates(self._h, C.byref(n)))
         return n.value
 
     def layer_size(self, layer_id):

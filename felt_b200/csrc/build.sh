@@ -7,14 +7,14 @@ NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 FLAGS=(-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 -fmad=false
        -Xcompiler -fPIC -Xcompiler -fvisibility=hidden --expt-relaxed-constexpr
        -I"$HERE/../include")
-SRCS=(fg_engine.cu fg_polys.cu fg_capi.cu)
+SRCS=(fg_engine.cu fg_polys.cu fg_capi.cu fg_prof.cu)
 OBJS=()
 PIDS=()
 mkdir -p "$OUT/_build"
 for s in "${SRCS[@]}"; do
   o="$OUT/_build/${s%.cu}.o"
   if [[ ! -f "$o" || "$HERE/$s" -nt "$o" || -n "$(find "$HERE" -name '*.cuh' -newer "$o" -print -quit)" || -n "$(find "$HERE/../include" "$HERE/../../include" -newer "$o" -print -quit)" ]]; then
-    "$NVCC" "${FLAGS[@]}" -dc "$HERE/$s" -o "$o" &
+    "$NVCC" "${FLAGS[@]}" -c "$HERE/$s" -o "$o" &
     PIDS+=($!)
   fi
   OBJS+=("$o")

@@ -377,6 +377,58 @@ int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vcap, uint32
 	});
 }
 
+int fg_node_updates(fg_surface* s, unsigned long long* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(n, "n");
+		*n = s->eng->node_updates();
+	});
+}
+
+int fg_launch_count(long long* n)
+{
+	return guard([&] {
+		need(n, "n");
+		*n = fg::launch_count();
+	});
+}
+
+int fg_profile_enable(int on)
+{
+	return guard([&] { fg::prof_enable(on != 0); });
+}
+
+int fg_profile_reset(void)
+{
+	return guard([&] { fg::prof_reset(); });
+}
+
+static std::vector<fg::ProfEntry> g_prof_snapshot;
+
+int fg_profile_count(size_t* n)
+{
+	return guard([&] {
+		need(n, "n");
+		g_prof_snapshot = fg::prof_read();
+		*n = g_prof_snapshot.size();
+	});
+}
+
+int fg_profile_entry(size_t i, char* name, size_t name_cap, double* ms, long long* launches)
+{
+	return guard([&] {
+		if (i >= g_prof_snapshot.size()) throw fg::Error(FG_ERR_ARG, "profile entry out of range");
+		const fg::ProfEntry& e = g_prof_snapshot[i];
+		if (name && name_cap) {
+			std::strncpy(name, e.name.c_str(), name_cap - 1);
+			name[name_cap - 1] = 0;
+		}
+		if (ms) *ms = e.ms;
+		if (launches) *launches = e.launches;
+	});
+}
+
 int fg_polys_totals(fg_polys* p, size_t* nv, size_t* ns)
 {
 	return guard([&] {

@@ -216,7 +216,7 @@ public:
 		FG_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st_));
 		FG_CUDA(cudaMemsetAsync(P.changed, 0, sizeof(int), st_));
 		FG_CUDA(cudaMemsetAsync(acc_, 0, sizeof(unsigned long long), st_));
-		k_iota_rev<<<grid_for(nslots), 256, 0, st_>>>(P.free_stack, (int)nslots);
+		FG_RUN("k_iota_rev", st_, k_iota_rev<<<grid_for(nslots), 256, 0, st_>>>(P.free_stack, (int)nslots););
 		const int top = (int)nslots;
 		FG_CUDA(cudaMemcpyAsync(P.counters + CNT_FREE_TOP, &top, sizeof(int), cudaMemcpyHostToDevice,
 		                        st_));
@@ -242,6 +242,13 @@ public:
 	int surfaces() const override { return P_.S; }
 	cudaStream_t stream() const override { return st_; }
 	StepStats& stats() override { return stats_; }
+	unsigned long long node_updates() override
+	{
+		unsigned long long n = 0;
+		FG_CUDA(cudaMemcpyAsync(&n, acc_, sizeof(n), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		return n;
+	}
 	const Dev& dev() const override { return P_; }
 	void sync() override { FG_CUDA(cudaStreamSynchronize(st_)); }
 	int part(int a) const override { return csz_[a]; }
@@ -252,7 +259,7 @@ public:
 		check_surface(s);
 		Vec<D> c;
 		for (int a = 0; a < D; a++) c[a] = pos[a];
-		k_seed<D, L><<<1, 1, 0, st_>>>(P_, s, c);
+		FG_RUN("k_seed", st_, k_seed<D, L><<<1, 1, 0, st_>>>(P_, s, c););
 		FG_CUDA(cudaGetLastError());
 		check_errors();
 	}
@@ -264,7 +271,7 @@ public:
 		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
 		scan(P_.pcnt, L, 0);
-		k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_);
+		FG_RUN("k_delta_builtin", st_, k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_););
 		update_finish_global();
 	}
 
@@ -281,8 +288,8 @@ public:
 		const int B = 1, A = 0;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
 		// update_zero_layer(&affected_buffer)
 		scan(P_.pcnt, L, 0);
-		k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, B);
-		k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.plist, L, B);
+		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, B););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.plist, L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		distance_passes(iso, B);
@@ -336,7 +343,7 @@ public:
 			FG_CUDA(cudaMalloc(&tmp, tot * sizeof(float)));
 			out = tmp;
 		}
-		k_snapshot<D, L><<<grid_for(tot), 256, 0, st_>>>(P_, s, out, tot);
+		FG_RUN("k_snapshot", st_, k_snapshot<D, L><<<grid_for(tot), 256, 0, st_>>>(P_, s, out, tot););
 		cudaError_t e = cudaGetLastError();
 		if (e == cudaSuccess && tmp)
 			e = cudaMemcpyAsync(dst, tmp, tot * sizeof(float), cudaMemcpyDeviceToHost, st_);
@@ -523,16 +530,16 @@ private:
 	}
 	void fill(int* p, size_t n, int v)
 	{
-		k_fill_int<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v);
+		FG_RUN("k_fill_int", st_, k_fill_int<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v););
 	}
 	void fillf(float* p, size_t n, float v)
 	{
-		k_fill_float<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v);
+		FG_RUN("k_fill_float", st_, k_fill_float<<<grid_for(n), 256, 0, st_>>>(p, (long long)n, v););
 	}
 
 	void scan(const int* cnt, int l, int mode)
 	{
-		k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff);
+		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff););
 	}
 
 	/// update_start (Surface.hpp:393-399): resets of the status and affected grids left by the
@@ -549,13 +556,13 @@ private:
 	{
 		dim3 grid(1, P_.S * NL);
 		if (grid.y > 65535) throw Error(-1, "too many surfaces for one pool");
-		k_copy_plists<<<grid, 256, 0, st_>>>(P_, NL);
+		FG_RUN("k_copy_plists", st_, k_copy_plists<<<grid, 256, 0, st_>>>(P_, NL););
 	}
 
 	void count_band()
 	{
 		scan(P_.pcnt, 0, 2);
-		k_band_size<L><<<warp_grid_, 256, 0, st_>>>(P_, acc_);
+		FG_RUN("k_band_size", st_, k_band_size<L><<<warp_grid_, 256, 0, st_>>>(P_, acc_););
 	}
 
 	void distance_passes(const ListView& lv, int b)
@@ -567,39 +574,39 @@ private:
 	void layer_pass(const ListView& lv, int k, float side, int b)
 	{
 		scan(lv.pcnt, k + L, 0);
-		k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, side);
-		k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, b);
-		k_compact<L><<<P_.S, 256, 0, st_>>>(P_, lv.plist, k + L, b);
+		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, side););
+		FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, b););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, lv.plist, k + L, b););
 	}
 
 	void flush()
 	{
-		k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_);
+		FG_RUN("k_flush_leaf", st_, k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_););
 		const int warps = P_.S * NL;
-		k_flush_plist<L><<<(warps * 32 + 255) / 256, 256, 0, st_>>>(P_);
+		FG_RUN("k_flush_plist", st_, k_flush_plist<L><<<(warps * 32 + 255) / 256, 256, 0, st_>>>(P_););
 	}
 
 	void expand()
 	{
 		scan(P_.spcnt, 0, 1);
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
-		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0);
-		k_activate<L><<<sm_count() * 4, 256, 0, st_>>>(P_);
-		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 1);
-		k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 2);
-		k_expand_append<L><<<sm_count() * 4, 256, smem_sort_, st_>>>(P_);
-		k_expand_plist<L><<<P_.S, 256, 0, st_>>>(P_);
+		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0););
+		FG_RUN("k_activate", st_, k_activate<L><<<sm_count() * 4, 256, 0, st_>>>(P_););
+		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 1););
+		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 2););
+		FG_RUN("k_expand_append", st_, k_expand_append<L><<<sm_count() * 4, 256, smem_sort_, st_>>>(P_););
+		FG_RUN("k_expand_plist", st_, k_expand_plist<L><<<P_.S, 256, 0, st_>>>(P_););
 	}
 
 	void retire()
 	{
-		k_retire<<<grid_for(P_.nslots), 256, 0, st_>>>(P_);
+		FG_RUN("k_retire", st_, k_retire<<<grid_for(P_.nslots), 256, 0, st_>>>(P_););
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_RETIRE, 0, sizeof(int), st_));
 	}
 
 	void clear_status()
 	{
-		k_clear_status<L><<<warp_grid_, 256, 0, st_>>>(P_);
+		FG_RUN("k_clear_status", st_, k_clear_status<L><<<warp_grid_, 256, 0, st_>>>(P_););
 		FG_CUDA(cudaMemsetAsync(P_.spcnt, 0, (size_t)P_.S * NL * sizeof(int), st_));
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_SUNION, 0, sizeof(int), st_));
 		status_dirty_ = false;
@@ -608,7 +615,7 @@ private:
 	void clear_buffer(int b)
 	{
 		scan(P_.apcnt[b], 0, 2);
-		k_clear_buffer<L><<<warp_grid_, 256, 0, st_>>>(P_, b);
+		FG_RUN("k_clear_buffer", st_, k_clear_buffer<L><<<warp_grid_, 256, 0, st_>>>(P_, b););
 		FG_CUDA(cudaMemsetAsync(P_.apcnt[b], 0, (size_t)P_.S * NL * sizeof(int), st_));
 		buf_dirty_[b] = false;
 	}

@@ -71,11 +71,36 @@ public:
 	virtual unsigned long long band_size(int s) = 0;
 	virtual void check_errors() = 0;
 	virtual StepStats& stats() = 0;
+	/// Sum over all global updates so far of the band size at each update's start.
+	virtual unsigned long long node_updates() = 0;
 	virtual const Dev& dev() const = 0;
 	virtual void sync() = 0;
 	virtual int part(int a) const = 0;
 };
 
 EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream);
+
+// ---- launch accounting and per-kernel timing ----
+/// Called around every kernel launch of the library: counts launches and, when profiling is
+/// enabled, brackets the launch with CUDA events on its stream.
+void prof_begin(const char* name, cudaStream_t st);
+void prof_end(cudaStream_t st);
+long long launch_count();
+void prof_enable(bool on);
+/// Synchronises pending events and returns (name, total ms, launches) per kernel name.
+struct ProfEntry {
+	std::string name;
+	double ms;
+	long long launches;
+};
+std::vector<ProfEntry> prof_read();
+void prof_reset();
+
+#define FG_RUN(name, st, ...)            \
+	do {                                 \
+		::fg::prof_begin(name, st);      \
+		__VA_ARGS__;                     \
+		::fg::prof_end(st);              \
+	} while (0)
 
 }  // namespace fg

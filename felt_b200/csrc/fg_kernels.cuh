@@ -56,7 +56,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 // Entry offsets: woff[s] = sum of per-surface counts before s.
 // mode 0: cnt[s*NL + l]; mode 1: cnt[s*NL] + cnt[s*NL + NL-1]; mode 2: sum over layers.
 // ---------------------------------------------------------------------------------------------
-__global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff)
+static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff)
 {
 	__shared__ int carry;
 	if (threadIdx.x == 0) {
@@ -778,7 +778,7 @@ __global__ void k_clear_buffer(Dev P, int b)
 }
 
 /// Returns the bricks of partitions deactivated in this iteration to the free pool.
-__global__ void k_retire(Dev P)
+static __global__ void k_retire(Dev P)
 {
 	const int n = P.counters[CNT_RETIRE];
 	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -793,7 +793,7 @@ __global__ void k_retire(Dev P)
 /// Copies the isogrid partition lists to the delta partition lists (track_children of the
 /// delta grid at update start, Surface.hpp:261 / PartitionedMixin.hpp:319-334, which mirrors
 /// the isogrid lists into the freshly reset delta lists). Grid y = s*NL + l.
-__global__ void k_copy_plists(Dev P, int NL)
+static __global__ void k_copy_plists(Dev P, int NL)
 {
 	const int s = blockIdx.y / NL, l = blockIdx.y % NL;
 	const SurfGeom& g = P.geom[s];

@@ -526,7 +526,6 @@ namespace {
 template <int D, int L>
 class PolysImpl final : public PolysBase {
 public:
-	static constexpr int NL = 2 * L + 1;
 	static constexpr int VF = D == 3 ? 2 * D : D;
 
 	PolysImpl(EngineBase& eng, int s) : eng_(eng), s_(s)
@@ -582,14 +581,14 @@ public:
 	void notify() override
 	{
 		const Dev& P = eng_.dev();
-		k_polys_notify<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_);
+		FG_RUN("k_polys_notify", eng_.stream(), k_polys_notify<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_););
 		FG_CUDA(cudaGetLastError());
 	}
 
 	void invalidate() override
 	{
 		const Dev& P = eng_.dev();
-		k_polys_invalidate<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_);
+		FG_RUN("k_polys_invalidate", eng_.stream(), k_polys_invalidate<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_););
 		FG_CUDA(cudaGetLastError());
 	}
 
@@ -598,12 +597,12 @@ public:
 		const Dev& P = eng_.dev();
 		cudaStream_t st = eng_.stream();
 		maybe_compact();
-		k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_);
-		k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1);
+		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_););
+		FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1););
 		FG_CUDA(cudaGetLastError());
 		// swap pending and done, then reset the new pending list
 		Q_.pend ^= 1;
-		k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend);
+		FG_RUN("k_polys_reset_list", st, k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend););
 		FG_CUDA(cudaGetLastError());
 		eng_.check_errors();
 	}
@@ -613,7 +612,7 @@ public:
 		const Dev& P = eng_.dev();
 		const int gp = check_part(part);
 		maybe_compact();
-		k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp);
+		FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
 		FG_CUDA(cudaGetLastError());
 		eng_.check_errors();
 	}
@@ -748,7 +747,7 @@ private:
 		FG_CUDA(cudaMalloc(&s2, (size_t)scap * D * sizeof(uint32_t)));
 		FG_CUDA(cudaMemcpy(dno, no.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
 		FG_CUDA(cudaMemcpy(dso, so.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
-		k_polys_compact<D><<<grid(), 256, 0, eng_.stream()>>>(P, Q_, dno, dso, v2, s2);
+		FG_RUN("k_polys_compact", eng_.stream(), k_polys_compact<D><<<grid(), 256, 0, eng_.stream()>>>(P, Q_, dno, dso, v2, s2););
 		FG_CUDA(cudaGetLastError());
 		FG_CUDA(cudaMemcpyAsync(Q_.gvoff, dno, P.NP * sizeof(int), cudaMemcpyDeviceToDevice,
 		                        eng_.stream()));

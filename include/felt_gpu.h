@@ -163,6 +163,18 @@ FG_API int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_c
 /* Totals over all partitions. */
 FG_API int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
 
+/* ---- instrumentation (no counterpart in the reference; Surface.hpp has no timers) ----
+ * fg_node_updates: narrow-band node-updates processed by all global updates of a surface so
+ * far (band size at the start of each update, summed). fg_launch_count: kernels this library
+ * has launched in the process. fg_profile_*: per-kernel device time from CUDA events recorded
+ * around every launch while profiling is enabled. */
+FG_API int fg_node_updates(fg_surface* s, unsigned long long* n);
+FG_API int fg_launch_count(long long* n);
+FG_API int fg_profile_enable(int on);
+FG_API int fg_profile_reset(void);
+FG_API int fg_profile_count(size_t* n);
+FG_API int fg_profile_entry(size_t i, char* name, size_t name_cap, double* ms, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif
