@@ -207,6 +207,18 @@ class Surface:
         _chk(lib().fg_band_size(self._h, C.byref(n)))
         return n.value
 
+    def work_units(self):
+        """(distance-pass nodes, zero-layer nodes, flush edits, marched cells) so far."""
+        out = (C.c_ulonglong * 8)()
+        _chk(lib().fg_work_units(self._h, out, C.c_size_t(8)))
+        return tuple(out[:4])
+
+    def stream(self):
+        """cudaStream_t (as int) that all work of this surface runs on."""
+        p = C.c_void_p()
+        _chk(lib().fg_surface_stream(self._h, C.byref(p)))
+        return p.value or 0
+
     def node_updates(self):
         """Band nodes processed by all global updates so far (band size at each start)."""
         n = C.c_ulonglong()

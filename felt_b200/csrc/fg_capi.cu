@@ -386,6 +386,27 @@ int fg_node_updates(fg_surface* s, unsigned long long* n)
 	});
 }
 
+int fg_work_units(fg_surface* s, unsigned long long* out, size_t n)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(out, "out");
+		unsigned long long tmp[fg::KS_N];
+		s->eng->sync();
+		FG_CUDA(cudaMemcpy(tmp, s->eng->dev().kstat, sizeof(tmp), cudaMemcpyDeviceToHost));
+		for (size_t i = 0; i < n && i < (size_t)fg::KS_N; i++) out[i] = tmp[i];
+	});
+}
+
+int fg_surface_stream(fg_surface* s, void** stream)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(stream, "stream");
+		*stream = (void*)s->eng->stream();
+	});
+}
+
 int fg_launch_count(long long* n)
 {
 	return guard([&] {

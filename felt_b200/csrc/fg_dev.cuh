@@ -97,9 +97,14 @@ struct Dev {
 	int* woff;        // [S+1] entry offsets of the current pass
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes
+	unsigned long long* kstat;  // [8] work units processed, see KS_* below
 };
 
 enum { CNT_FREE_TOP = 0, CNT_ACT = 1, CNT_TOUCH = 2, CNT_RETIRE = 3, CNT_SUNION = 4, CNT_N = 8 };
+
+/// Work-unit counters (Dev::kstat): band nodes through the distance passes, zero-layer nodes
+/// through the speed functor, leaf edits replayed by the flush, cells marched by Polys.
+enum { KS_DIST = 0, KS_ZERO = 1, KS_FLUSH = 2, KS_MARCH = 3, KS_N = 8 };
 
 template <int D>
 struct Vec {

@@ -192,6 +192,8 @@ public:
 		P.woff = dalloc<int>(S + 1, o);
 		P.err = dalloc<int>(1, o);
 		P.changed = dalloc<int>(1, o);
+		P.kstat = dalloc<unsigned long long>(KS_N, o);
+		FG_CUDA(cudaMemsetAsync(P.kstat, 0, KS_N * sizeof(unsigned long long), st_));
 		acc_ = dalloc<unsigned long long>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
 

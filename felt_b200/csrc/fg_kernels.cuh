@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 			const int leaf = lst[j];
 			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval<D, L>(P, g, sp, leaf_pos<D>(P, gp, leaf));
 		}
+		if (lane == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
 	}
 }
 
@@ -232,6 +233,7 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, ListView lv, int k, float 
 			const size_t kk = (size_t)sl * P.BV + leaf;
 			P.dlt[kk] = distance<D, L>(P, g, leaf_pos<D>(P, gp, leaf), P.phi[kk], side);
 		}
+		if (lane == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
 	}
 }
 
@@ -392,6 +394,11 @@ __global__ void k_flush_leaf(Dev P)
 		}
 		for (int l = 0; l < NL; l++) P.lcnt[sl * NL + l] = cnt[l];
 		P.rem[gp] = remb;
+		{
+			int edits = 0;
+			for (int fi = 0; fi < NL; fi++) edits += P.ccnt[sl * NL + fi];
+			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)edits);
+		}
 		if (dead) {
 			P.oslot[gp] = sl;
 			P.slot[gp] = -1;

@@ -34,6 +34,7 @@ struct PolysDev {
 	long long vcap, scap;
 	int pend;           // which of the two lists is pending
 	int* err;
+	int* ovf;           // set when a march ran out of arena space
 };
 
 namespace {
@@ -384,6 +385,7 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 		for (int i = threadIdx.x; i < cvol * D; i += blockDim.x) first[i] = 0x7fffffff;
 		__syncthreads();
 		const int n = lstart[NL];
+		if (threadIdx.x == 0) atomicAdd(&P.kstat[KS_MARCH], (unsigned long long)n);
 		const int per = (n + blockDim.x - 1) / blockDim.x;
 		const int j0 = threadIdx.x * per, j1 = min(n, j0 + per);
 		Vec<D> orig;
@@ -446,7 +448,7 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			ok = (long long)(a + tv) <= Q.vcap && (long long)(b + ts) <= Q.scap;
 			vb = (int)a;
 			sb = (int)b;
-			if (!ok) atomicOr(Q.err, EB_CAPACITY);
+			if (!ok) atomicExch(Q.ovf, 1);
 		}
 		__syncthreads();
 		if (ok) {
@@ -559,6 +561,7 @@ public:
 		FG_CUDA(cudaMemset(Q_.used, 0, 2 * sizeof(unsigned long long)));
 		woff_ = (int*)al((P.S + 1) * sizeof(int));
 		Q_.err = P.err;
+		Q_.ovf = (int*)al(sizeof(int));
 		Q_.pend = 0;
 		alloc_arena(1 << 20, 2 << 20);
 		int cvol = 1;
@@ -596,10 +599,17 @@ public:
 	{
 		const Dev& P = eng_.dev();
 		cudaStream_t st = eng_.stream();
-		maybe_compact();
 		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_););
-		FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1););
-		FG_CUDA(cudaGetLastError());
+		// Re-marching a partition recomputes it from the isogrid, so a march that ran out of
+		// arena space is simply repeated after the arena has grown.
+		for (int attempt = 0;; attempt++) {
+			maybe_compact(attempt > 0);
+			FG_CUDA(cudaMemsetAsync(Q_.ovf, 0, sizeof(int), st));
+			FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1););
+			FG_CUDA(cudaGetLastError());
+			if (!overflowed()) break;
+			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
+		}
 		// swap pending and done, then reset the new pending list
 		Q_.pend ^= 1;
 		FG_RUN("k_polys_reset_list", st, k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend););
@@ -611,10 +621,23 @@ public:
 	{
 		const Dev& P = eng_.dev();
 		const int gp = check_part(part);
-		maybe_compact();
-		FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
-		FG_CUDA(cudaGetLastError());
+		for (int attempt = 0;; attempt++) {
+			maybe_compact(attempt > 0);
+			FG_CUDA(cudaMemsetAsync(Q_.ovf, 0, sizeof(int), eng_.stream()));
+			FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
+			FG_CUDA(cudaGetLastError());
+			if (!overflowed()) break;
+			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
+		}
 		eng_.check_errors();
+	}
+
+	bool overflowed()
+	{
+		int o = 0;
+		FG_CUDA(cudaMemcpyAsync(&o, Q_.ovf, sizeof(int), cudaMemcpyDeviceToHost, eng_.stream()));
+		eng_.sync();
+		return o != 0;
 	}
 
 	std::vector<uint32_t> changes() override
@@ -714,14 +737,14 @@ private:
 	}
 	/// Keeps the bump-allocated arenas at most half full before a march by moving the live
 	/// geometry into fresh arenas (doubling them when the live part alone is over a quarter).
-	void maybe_compact()
+	void maybe_compact(bool grow)
 	{
 		const Dev& P = eng_.dev();
 		unsigned long long used[2];
 		FG_CUDA(cudaMemcpyAsync(used, Q_.used, sizeof(used), cudaMemcpyDeviceToHost,
 		                        eng_.stream()));
 		eng_.sync();
-		if ((long long)used[0] * 2 < Q_.vcap && (long long)used[1] * 2 < Q_.scap) return;
+		if (!grow && (long long)used[0] * 2 < Q_.vcap && (long long)used[1] * 2 < Q_.scap) return;
 		std::vector<int> nv(P.NP), ns(P.NP), no(P.NP), so(P.NP);
 		FG_CUDA(cudaMemcpy(nv.data(), Q_.gnv, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
 		FG_CUDA(cudaMemcpy(ns.data(), Q_.gns, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
@@ -732,10 +755,10 @@ private:
 			tv += nv[i];
 			ts += ns[i];
 		}
-		long long vcap = Q_.vcap, scap = Q_.scap;
+		long long vcap = grow ? 2 * Q_.vcap : Q_.vcap, scap = grow ? 2 * Q_.scap : Q_.scap;
 		while (tv * 4 > vcap) vcap *= 2;
 		while (ts * 4 > scap) scap *= 2;
-		if (vcap * VF >= (1LL << 31) || scap * D >= (1LL << 31))
+		if (vcap >= (1LL << 31) || scap >= (1LL << 31))
 			throw Error(-13, "polygonisation arena too large");
 		int* dno = nullptr;
 		int* dso = nullptr;

@@ -169,6 +169,12 @@ FG_API int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
  * has launched in the process. fg_profile_*: per-kernel device time from CUDA events recorded
  * around every launch while profiling is enabled. */
 FG_API int fg_node_updates(fg_surface* s, unsigned long long* n);
+/* Work units processed so far on the surface's pool: [0] band nodes through the distance
+ * passes, [1] zero-layer nodes through the speed functor, [2] leaf edits of the status-change
+ * flush, [3] cells marched by Polys. Writes min(n, 8) counters. */
+FG_API int fg_work_units(fg_surface* s, unsigned long long* out, size_t n);
+/* The CUDA stream (cudaStream_t) every call on this surface is issued to. */
+FG_API int fg_surface_stream(fg_surface* s, void** stream);
 FG_API int fg_launch_count(long long* n);
 FG_API int fg_profile_enable(int on);
 FG_API int fg_profile_reset(void);
