@@ -9,23 +9,7 @@
 #include "fg_engine.cuh"
 #include "fg_polys.cuh"
 
-struct fg_surface {
-	std::unique_ptr<fg::EngineBase> eng;
-	cudaStream_t st = nullptr;
-	bool local_open = false;
-	std::vector<int> dpos;
-	std::vector<float> dval;
-	~fg_surface()
-	{
-		eng.reset();
-		if (st) cudaStreamDestroy(st);
-	}
-};
-
-struct fg_polys {
-	fg_surface* surf = nullptr;
-	std::unique_ptr<fg::PolysBase> impl;
-};
+#include "fg_handles.cuh"
 
 namespace {
 
@@ -70,6 +54,8 @@ void put_list(const std::vector<uint32_t>& v, uint32_t* out, size_t cap, size_t*
 }
 
 }  // namespace
+
+void fg::set_last_error(const std::string& msg) { g_err = msg; }
 
 extern "C" {
 

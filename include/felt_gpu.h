@@ -109,6 +109,17 @@ FG_API int fg_update_end(fg_surface* s);
  * dst_is_device, in device memory of the surface's GPU. */
 FG_API int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device);
 
+/* Dense snapshot into a host buffer that allocates no memory. No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory while they run (code inside a CUDA
+ * stream capture, processes whose device memory is budgeted by another allocator, real-time
+ * loops that must not enter the driver's allocator). It stages through a fixed device array of
+ * 2^21 floats (8 MiB) that every GPU loading this library holds until exit; grids with more
+ * nodes are rejected with FG_ERR_CAPACITY. Calls share that array (each call writes all it
+ * reads), are serialised by a process-wide lock and wait for their copy; calls that overlapped
+ * on the GPU would race. The first call on a device looks up the array's address on that device
+ * and should come before any stream capture. dst holds n >= prod(size) floats. */
+FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n);
+
 /* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */
 FG_API int fg_get(fg_surface* s, const int* pos, float* out);
 
