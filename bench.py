@@ -48,6 +48,7 @@ CONFIGS = {
 #                write + 2 B lookup write + 4 B swap-in (moved entry and its lookup).
 #  k_polys_march: per cell: 2 B leaf index + 4 B phi (corners are neighbours' phi).
 UNIT_BYTES = {"k_dist1": (0, 10), "k_dist2": (0, 10), "k_delta_builtin": (1, 10),
+              "k_delta_smem": (1, 10), "k_flush_smem": (2, 13),
               "k_flush_leaf": (2, 13), "k_polys_march": (3, 6)}
 
 

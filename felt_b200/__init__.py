@@ -190,6 +190,12 @@ class Surface:
     def status_partitions(self, layer_idx):
         return _fetch(lib().fg_status_partitions, self._h, C.c_int(layer_idx))
 
+    def affected_partitions(self, layer_idx):
+        return _fetch(lib().fg_affected_partitions, self._h, C.c_int(layer_idx))
+
+    def affected_list(self, part, layer_idx):
+        return _fetch(lib().fg_affected_list, self._h, C.c_size_t(part), C.c_int(layer_idx))
+
     def partition_state(self, part):
         a = C.c_int()
         bg = C.c_float()

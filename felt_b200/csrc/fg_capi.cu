@@ -249,6 +249,22 @@ int fg_status_partitions(fg_surface* s, int li, uint32_t* out, size_t cap, size_
 	});
 }
 
+int fg_affected_partitions(fg_surface* s, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->partition_list(0, 3, li), out, cap, n);
+	});
+}
+
+int fg_affected_list(fg_surface* s, size_t part, int li, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		put_list(s->eng->affected_list(0, part, li), out, cap, n);
+	});
+}
+
 int fg_partition_state(fg_surface* s, size_t part, int* active, float* background)
 {
 	return guard([&] {

@@ -98,6 +98,12 @@ struct Dev {
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes
 	unsigned long long* kstat;  // [8] work units processed, see KS_* below
+
+	// local update (update_start / delta / update_end)
+	int* dlcnt;       // [nslots] delta leaves of a partition: a prefix of its affected list L
+	int* ndp;         // [S] delta partitions: a prefix of the affected partition list L
+	int* ring_first;  // [NL*NP] calc_affected ring bounds per (layer, partition entry)
+	int* ring_last;   // [NL*NP]
 };
 
 enum { CNT_FREE_TOP = 0, CNT_ACT = 1, CNT_TOUCH = 2, CNT_RETIRE = 3, CNT_SUNION = 4, CNT_N = 8 };
@@ -215,25 +221,25 @@ __device__ __forceinline__ Vec<D> leaf_pos(const Dev& P, int gp, int leaf)
 
 /// Mean curvature by difference of normals (NumericMixin.hpp:72-156). The fixed-size Eigen sum
 /// of the normal differences is unrolled by halving: x0 + (x1 + x2) in 3D.
-template <int D, int L>
-__device__ float curv(const Dev& P, const SurfGeom& g, const Vec<D>& pos)
+template <int D, class Get>
+__device__ float curv_g(const Get& get, const Vec<D>& pos)
 {
-	const float centre = get_phi<D, L>(P, g, pos);
+	const float centre = get(pos);
 	Vec<D> dir = pos;
 	float nf[D], nb[D];
 #pragma unroll
 	for (int axis = 0; axis < D; axis++) {
 		dir[axis] += 1;
-		const float va = __fsub_rn(get_phi<D, L>(P, g, dir), centre);
+		const float va = __fsub_rn(get(dir), centre);
 		float sq = 0.0f;
 #pragma unroll
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
 			Vec<D> dn = dir;
 			dn[an] -= 1;
-			const float lo = get_phi<D, L>(P, g, dn);
+			const float lo = get(dn);
 			dn[an] += 2;
-			const float hi = get_phi<D, L>(P, g, dn);
+			const float hi = get(dn);
 			const float v = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
 			sq = __fadd_rn(sq, __fmul_rn(v, v));
 		}
@@ -243,16 +249,16 @@ __device__ float curv(const Dev& P, const SurfGeom& g, const Vec<D>& pos)
 #pragma unroll
 	for (int axis = 0; axis < D; axis++) {
 		dir[axis] -= 1;
-		const float va = __fsub_rn(centre, get_phi<D, L>(P, g, dir));
+		const float va = __fsub_rn(centre, get(dir));
 		float sq = 0.0f;
 #pragma unroll
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
 			Vec<D> dn = dir;
 			dn[an] -= 1;
-			const float lo = get_phi<D, L>(P, g, dn);
+			const float lo = get(dn);
 			dn[an] += 2;
-			const float hi = get_phi<D, L>(P, g, dn);
+			const float hi = get(dn);
 			const float v = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
 			sq = __fadd_rn(sq, __fmul_rn(v, v));
 		}
@@ -266,6 +272,20 @@ __device__ float curv(const Dev& P, const SurfGeom& g, const Vec<D>& pos)
 		s = __fadd_rn(__fsub_rn(nf[0], nb[0]),
 		              __fadd_rn(__fsub_rn(nf[1 % D], nb[1 % D]), __fsub_rn(nf[D - 1], nb[D - 1])));
 	return __fdiv_rn(s, 2.0f);
+}
+
+/// Reads the isogrid through the pool (global memory).
+template <int D, int L>
+struct PoolGet {
+	const Dev& P;
+	const SurfGeom& g;
+	__device__ float operator()(const Vec<D>& p) const { return get_phi<D, L>(P, g, p); }
+};
+
+template <int D, int L>
+__device__ float curv(const Dev& P, const SurfGeom& g, const Vec<D>& pos)
+{
+	return curv_g<D>(PoolGet<D, L>{P, g}, pos);
 }
 
 /// City-block distance to the zero curve from the nearest in-grid neighbour on the way in
@@ -297,6 +317,24 @@ struct Speed {
 	float c, a, n;
 	uint32_t seed;
 };
+template <int D, class Get>
+__device__ __forceinline__ float speed_eval_g(const Get& get, const Speed& sp, const Vec<D>& pos)
+{
+	float acc = 0.0f;
+	bool have = false;
+	if (sp.kind & 2) {
+		acc = __fmul_rn(sp.a, curv_g<D>(get, pos));
+		have = true;
+	}
+	if (sp.kind & 4) {
+		const float t = __fmul_rn(sp.n, hash_noise<D>(pos, sp.seed));
+		acc = have ? __fadd_rn(acc, t) : t;
+		have = true;
+	}
+	if (sp.kind & 1) acc = have ? __fadd_rn(acc, sp.c) : sp.c;
+	return acc;
+}
+
 template <int D, int L>
 __device__ __forceinline__ float speed_eval(const Dev& P, const SurfGeom& g, const Speed& sp,
                                             const Vec<D>& pos)

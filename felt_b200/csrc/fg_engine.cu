@@ -193,6 +193,10 @@ public:
 		P.err = dalloc<int>(1, o);
 		P.changed = dalloc<int>(1, o);
 		P.kstat = dalloc<unsigned long long>(KS_N, o);
+		P.dlcnt = dalloc<int>(nslots, o);
+		P.ndp = dalloc<int>(S, o);
+		P.ring_first = dalloc<int>(npl, o);
+		P.ring_last = dalloc<int>(npl, o);
 		FG_CUDA(cudaMemsetAsync(P.kstat, 0, KS_N * sizeof(unsigned long long), st_));
 		acc_ = dalloc<unsigned long long>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
@@ -231,12 +235,32 @@ public:
 			                             cudaFuncAttributeMaxDynamicSharedMemorySize,
 			                             (int)smem_sort_));
 		warp_grid_ = sm_count() * 8;
+		smem_halo_ = halo_smem_bytes(D, csz_);
+		if (smem_halo_ > 200 * 1024) {
+			smem_halo_ = 0;  // partition too large to stage with its halo
+		} else if (smem_halo_ > 48 * 1024) {
+			FG_CUDA(cudaFuncSetAttribute(k_delta_smem<D, L>,
+			                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                             (int)smem_halo_));
+		}
+		smem_flush_ = flush_smem_bytes(BV, NL);
+		if (smem_flush_ <= 200 * 1024) {
+			if (smem_flush_ > 48 * 1024)
+				FG_CUDA(cudaFuncSetAttribute(k_flush_smem<D, L>,
+				                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+				                             (int)smem_flush_));
+		} else {
+			smem_flush_ = 0;  // brick too large to stage: replay in global memory
+		}
 	}
 
 	~Engine() override
 	{
 		cudaStreamSynchronize(st_);
 		for (void* p : owned_) cudaFree(p);
+		if (d_lpos_) cudaFree(d_lpos_);
+		if (d_lval_) cudaFree(d_lval_);
+		if (d_lcount_) cudaFree(d_lcount_);
 	}
 
 	int dims() const override { return D; }
@@ -273,7 +297,12 @@ public:
 		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
 		scan(P_.pcnt, L, 0);
-		FG_RUN("k_delta_builtin", st_, k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_););
+		bool any_curv = false;
+		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
+		if (any_curv && smem_halo_)
+			FG_RUN("k_delta_smem", st_, k_delta_smem<D, L><<<sm_count() * 8, 128, smem_halo_, st_>>>(P_, d_speeds_););
+		else
+			FG_RUN("k_delta_builtin", st_, k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_););
 		update_finish_global();
 	}
 
@@ -287,14 +316,26 @@ public:
 
 	void update_finish_global() override
 	{
-		const int B = 1, A = 0;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
+		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
 		// update_zero_layer(&affected_buffer)
 		scan(P_.pcnt, L, 0);
-		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, B););
+		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
+		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, iso, nullptr, B););
 		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.plist, L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
-		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		distance_passes(iso, B);
+		converge();
+	}
+
+	/// The rest of update_end_global / update_end after the first distance passes, which
+	/// recorded their changes in buffer B: flush and expand, then repeat the distance passes on
+	/// the changed nodes until no layer changes (Surface.hpp:744-761, 417-428).
+	/// The global update resets the consumed buffer at the end of each iteration, the local one
+	/// at the start of the next (Surface.hpp:752-760 vs 420-428); the difference shows in the
+	/// affected() lookup a local update leaves behind.
+	void converge(bool local = false)
+	{
+		const int B = 1, A = 0;
 		flush();
 		expand();
 		retire();
@@ -304,6 +345,7 @@ public:
 		int iters = 1;
 		int cur = B, oth = A;
 		while (changed) {
+			if (local && buf_dirty_[oth]) clear_buffer(oth);
 			clear_status();
 			FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 			const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur]};
@@ -313,7 +355,7 @@ public:
 			retire();
 			status_dirty_ = true;
 			buf_dirty_[oth] = true;
-			clear_buffer(cur);
+			if (!local) clear_buffer(cur);
 			std::swap(cur, oth);
 			changed = read_changed();
 			iters++;
@@ -323,13 +365,79 @@ public:
 		check_errors();
 	}
 
-	void update_local(const std::vector<int>&, const std::vector<float>&) override
+	/// update_start(); delta(pos, v)...; update_end() on surface 0 (Surface.hpp:393-459,
+	/// 404-430).
+	void update_local(const std::vector<int>& pos, const std::vector<float>& vals) override
 	{
-		throw Error(-15, "local update is not available on the device engine yet");
+		const int n = (int)vals.size();
+		if (pos.size() != vals.size() * D) throw Error(-1, "delta positions/values mismatch");
+		update_start();
+		ensure_local_staging(n);
+		if (n) {
+			FG_CUDA(cudaMemcpyAsync(d_lpos_, pos.data(), pos.size() * sizeof(int),
+			                        cudaMemcpyHostToDevice, st_));
+			FG_CUDA(cudaMemcpyAsync(d_lval_, vals.data(), n * sizeof(float),
+			                        cudaMemcpyHostToDevice, st_));
+		}
+		FG_RUN("k_local_seed", st_, k_local_seed<D, L><<<1, 1, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n););
+		local_end();
 	}
-	void update_bounded(const int*, const int*, const Speed&) override
+
+	/// update(lo, hi, fn) with a builtin speed on surface 0 (Surface.hpp:310-386): the speed at
+	/// the zero-layer leaves inside the box becomes the deltas of a local update.
+	void update_bounded(const int* lo, const int* hi, const Speed& sp) override
 	{
-		throw Error(-15, "bounded update is not available on the device engine yet");
+		Vec<D> vlo, vhi;
+		for (int a = 0; a < D; a++) {
+			vlo[a] = lo[a];
+			vhi[a] = hi[a];
+		}
+		// capacity: every zero-layer leaf of the surface
+		unsigned long long nz = 0;
+		for (uint32_t p : partition_list(0, 0, L)) nz += layer_list(0, p, L).size();
+		ensure_local_staging((int)nz + 1);
+		update_start();
+		FG_RUN("k_bounded_collect", st_, k_bounded_collect<D, L><<<1, 1, 0, st_>>>(P_, 0, vlo, vhi, d_lpos_, lcap_, d_lcount_););
+		FG_RUN("k_bounded_speed", st_, k_bounded_speed<D, L><<<grid_for(nz + 1), 256, 0, st_>>>(P_, 0, sp, d_lpos_, d_lcount_, d_lval_););
+		int n = 0;
+		FG_CUDA(cudaMemcpyAsync(&n, d_lcount_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		FG_RUN("k_local_seed", st_, k_local_seed<D, L><<<1, 1, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n););
+		local_end();
+	}
+
+	/// update_end after the deltas are tracked (Surface.hpp:404-430).
+	void local_end()
+	{
+		const int A = 0, B = 1;
+		buf_dirty_[A] = true;
+		FG_RUN("k_calc_affected", st_, k_calc_affected<D, L><<<1, 1, 0, st_>>>(P_, 0););
+		FG_RUN("k_local_children", st_, k_local_children<L><<<1, 1, 0, st_>>>(P_, 0););
+		count_band();
+		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
+		// over the affected lists (update_distance(plookup = affected, buffer))
+		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff););
+		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
+		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, aff, P_.dlcnt, B););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.aplist[A], L, B););
+		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
+		distance_passes(aff, B);
+		converge(true);
+	}
+
+	void ensure_local_staging(int n)
+	{
+		if (n <= lcap_ && d_lpos_) return;
+		int cap = std::max(n, 1024);
+		cudaStreamSynchronize(st_);
+		if (d_lpos_) cudaFree(d_lpos_);
+		if (d_lval_) cudaFree(d_lval_);
+		d_lpos_ = nullptr;
+		d_lval_ = nullptr;
+		FG_CUDA(cudaMalloc(&d_lpos_, (size_t)cap * D * sizeof(int)));
+		FG_CUDA(cudaMalloc(&d_lval_, (size_t)cap * sizeof(float)));
+		if (!d_lcount_) FG_CUDA(cudaMalloc(&d_lcount_, sizeof(int)));
+		lcap_ = cap;
 	}
 
 	// ---- queries ----
@@ -420,6 +528,7 @@ public:
 		case 0: list = P_.plist; cnt = P_.pcnt; break;
 		case 1: list = P_.dplist; cnt = P_.dpcnt; break;
 		case 2: list = P_.splist; cnt = P_.spcnt; break;
+		case 3: list = P_.aplist[0]; cnt = P_.apcnt[0]; break;
 		default: throw Error(-1, "unknown partition list");
 		}
 		int n;
@@ -428,6 +537,28 @@ public:
 		if (n)
 			FG_CUDA(cudaMemcpy(tmp.data(), list + (size_t)li * P_.NP + geom_[s].pbase,
 			                   n * sizeof(int), cudaMemcpyDeviceToHost));
+		return std::vector<uint32_t>(tmp.begin(), tmp.end());
+	}
+
+	std::vector<uint32_t> affected_list(int s, size_t part, int li) override
+	{
+		check_surface(s);
+		check_layer(li);
+		if (part >= (size_t)geom_[s].np) throw Error(-1, "partition index out of range");
+		sync();
+		const int gp = geom_[s].pbase + (int)part;
+		int sl, ap;
+		FG_CUDA(cudaMemcpy(&ap, P_.appos[0] + (size_t)gp * NL + li, sizeof(int),
+		                   cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(&sl, P_.slot + gp, sizeof(int), cudaMemcpyDeviceToHost));
+		if (ap < 0 || sl < 0) return {};
+		int n;
+		FG_CUDA(cudaMemcpy(&n, P_.acnt[0] + (size_t)sl * NL + li, sizeof(int),
+		                   cudaMemcpyDeviceToHost));
+		std::vector<uint16_t> tmp(n);
+		if (n)
+			FG_CUDA(cudaMemcpy(tmp.data(), P_.alst[0] + ((size_t)sl * NL + li) * P_.BV,
+			                   n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
 		return std::vector<uint32_t>(tmp.begin(), tmp.end());
 	}
 
@@ -583,7 +714,10 @@ private:
 
 	void flush()
 	{
-		FG_RUN("k_flush_leaf", st_, k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_););
+		if (smem_flush_)
+			FG_RUN("k_flush_smem", st_, k_flush_smem<D, L><<<sm_count() * 8, 128, smem_flush_, st_>>>(P_););
+		else
+			FG_RUN("k_flush_leaf", st_, k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_););
 		const int warps = P_.S * NL;
 		FG_RUN("k_flush_plist", st_, k_flush_plist<L><<<(warps * 32 + 255) / 256, 256, 0, st_>>>(P_););
 	}
@@ -639,6 +773,12 @@ private:
 	unsigned long long* acc_ = nullptr;
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
+	size_t smem_flush_ = 0;
+	size_t smem_halo_ = 0;
+	int* d_lpos_ = nullptr;    // local-update staging: delta positions
+	float* d_lval_ = nullptr;  // delta values
+	int* d_lcount_ = nullptr;
+	int lcap_ = 0;
 	int warp_grid_ = 0;
 	bool status_dirty_ = false;
 	bool buf_dirty_[2] = {false, false};

@@ -66,6 +66,8 @@ public:
 	virtual size_t partitions(int s, int* ccount, int* coff) = 0;
 	virtual std::vector<uint32_t> layer_list(int s, size_t part, int li) = 0;
 	virtual std::vector<uint32_t> partition_list(int s, int which, int li) = 0;
+	/// Leaf list of the affected lookup (Surface::affected(), Surface.hpp:693-696).
+	virtual std::vector<uint32_t> affected_list(int s, size_t part, int li) = 0;
 	virtual void partition_state(int s, size_t part, int* active, float* bg) = 0;
 	virtual std::vector<uint32_t> dump(int s) = 0;
 	virtual unsigned long long band_size(int s) = 0;

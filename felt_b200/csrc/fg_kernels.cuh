@@ -179,20 +179,115 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 	}
 }
 
+/// Fills box with the isogrid over a partition and a one-node halo ((part+2)^D values, row-major,
+/// last axis fastest): interior nodes straight from the brick, halo nodes through the pool
+/// (neighbour bricks, inactive-partition backgrounds, the grid background outside the grid).
+template <int D, int L>
+__device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, float* box)
+{
+	int ext[D], vol = 1;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		ext[a] = P.csz[a] + 2;
+		vol *= ext[a];
+	}
+	const float* brick = P.phi + (size_t)sl * P.BV;
+	for (int i = threadIdx.x; i < vol; i += blockDim.x) {
+		int r = i, leaf = 0;
+		bool interior = true;
+		Vec<D> c;
+#pragma unroll
+		for (int a = D - 1; a >= 0; a--) {
+			c[a] = r % ext[a] - 1;
+			r /= ext[a];
+			if (c[a] < 0 || c[a] >= P.csz[a]) interior = false;
+			leaf += c[a] * P.lstr[a];
+		}
+		if (interior) {
+			box[i] = brick[leaf];
+		} else {
+			Vec<D> p;
+#pragma unroll
+			for (int a = 0; a < D; a++) p[a] = P.porig[gp * 3 + a] + c[a];
+			box[i] = get_phi<D, L>(P, g, p);
+		}
+	}
+}
+
+/// Reads a staged box (stage_halo) by world position.
+template <int D>
+struct BoxGet {
+	const float* box;
+	int org[D];  // world position of box index 0
+	int ext[D];
+	__device__ float operator()(const Vec<D>& p) const
+	{
+		int i = 0;
+#pragma unroll
+		for (int a = 0; a < D; a++) i = i * ext[a] + (p[a] - org[a]);
+		return box[i];
+	}
+};
+
+/// Shared-memory bytes of a staged partition with a one-node halo.
+__host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
+{
+	size_t v = 1;
+	for (int a = 0; a < D; a++) v *= (size_t)(csz[a] + 2);
+	return v * sizeof(float);
+}
+
+/// k_delta_builtin with the partition and its halo staged in shared memory, for speeds with a
+/// curvature term: every stencil read of the zero-layer nodes hits shared memory. One block per
+/// zero-layer partition.
+template <int D, int L>
+__global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
+{
+	constexpr int NL = 2 * L + 1;
+	extern __shared__ float hbox[];
+	const int total = P.woff[P.S];
+	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+		const int s = entry_surface(P.woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const Speed sp = speeds[s];
+		const int gp = g.pbase + P.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
+		const int sl = P.slot[gp];
+		stage_halo<D, L>(P, g, gp, sl, hbox);
+		__syncthreads();
+		BoxGet<D> get;
+		get.box = hbox;
+#pragma unroll
+		for (int a = 0; a < D; a++) {
+			get.org[a] = P.porig[gp * 3 + a] - 1;
+			get.ext[a] = P.csz[a] + 2;
+		}
+		const int n = P.lcnt[sl * NL + L];
+		const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
+		for (int j = threadIdx.x; j < n; j += blockDim.x) {
+			const int leaf = lst[j];
+			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval_g<D>(get, sp, leaf_pos<D>(P, gp, leaf));
+		}
+		if (threadIdx.x == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
+		__syncthreads();
+	}
+}
+
 /// update_zero_layer (Surface.hpp:920-979) over the isogrid's zero-layer lists, which the delta
 /// grid mirrors in the global update.
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_zero_apply(Dev P, int b)
+__global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const int* ncount, int b)
 {
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
 		const int s = entry_surface(P.woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + P.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
+		const int gp = g.pbase + lv.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
 		const int sl = P.slot[gp];
-		const int n = P.lcnt[sl * NL + L];
-		const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
+		// the delta grid's zero-layer leaves: the isogrid list in the global update, a prefix of
+		// the affected list (the delta() calls' leaves) in the local update
+		const int n = ncount ? ncount[sl] : lv.lcnt[sl * NL + L];
+		const uint16_t* lst = lv.lst + ((size_t)sl * NL + L) * P.BV;
 		unsigned flags = 0;
 		bool any = false;
 		for (int base = 0; base < n; base += 32) {
@@ -404,6 +499,120 @@ __global__ void k_flush_leaf(Dev P)
 			P.slot[gp] = -1;
 			P.q_retire[atomicAdd(&P.counters[CNT_RETIRE], 1)] = sl;
 		}
+	}
+}
+
+/// Shared-memory bytes k_flush_smem needs for a brick of BV leaves and NL lists.
+__host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
+{
+	return (size_t)(NL + 2) * BV * sizeof(uint16_t) + (size_t)BV + 16;
+}
+
+/// k_flush_leaf with the partition staged in shared memory: one block per partition loads its
+/// leaf lists, leaf lookups and status entries, one thread replays the ordered edits on them
+/// (the replay is inherently sequential: each swap-with-last removal depends on the previous
+/// one), and the block writes the lists back. Same results as k_flush_leaf.
+template <int D, int L>
+__global__ void __launch_bounds__(128) k_flush_smem(Dev P)
+{
+	constexpr int NL = 2 * L + 1;
+	extern __shared__ __align__(16) unsigned char fsm[];
+	const int BV = P.BV;
+	uint16_t* slst = (uint16_t*)fsm;                 // [NL * BV]
+	uint16_t* slkp = slst + (size_t)NL * BV;         // [BV]
+	uint16_t* schg = slkp + BV;                      // [BV] status entries, phase-major
+	int8_t* ssto = (int8_t*)(schg + BV);             // [BV]
+	__shared__ int cnt[NL], coff[NL + 1], live0;
+	const int n = P.counters[CNT_SUNION];
+	const size_t bv = (size_t)BV;
+	for (int e = blockIdx.x; e < n; e += gridDim.x) {
+		const int gp = P.q_sunion[e];
+		const int sl = P.slot[gp];
+		if (threadIdx.x == 0) {
+			int c = 0, lv = 0;
+			for (int l = 0; l < NL; l++) {
+				cnt[l] = P.lcnt[sl * NL + l];
+				lv += cnt[l];
+				coff[l] = c;
+				c += P.ccnt[sl * NL + l];
+			}
+			coff[NL] = c;
+			live0 = lv;
+		}
+		__syncthreads();
+		for (int l = 0; l < NL; l++) {
+			const uint16_t* src = P.lst + ((size_t)sl * NL + l) * bv;
+			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x) slst[l * bv + i] = src[i];
+		}
+		for (int i = threadIdx.x; i < BV; i += blockDim.x) slkp[i] = P.lkp[sl * bv + i];
+		for (int fi = 0; fi < NL; fi++) {
+			const uint16_t* src = P.chg + ((size_t)sl * NL + fi) * bv;
+			const int nc = coff[fi + 1] - coff[fi];
+			for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+				const int leaf = src[c];
+				schg[coff[fi] + c] = (uint16_t)leaf;
+				ssto[coff[fi] + c] = P.sto[sl * bv + leaf];
+			}
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			int live = live0;
+			unsigned remb = 0;
+			bool dead = false;
+			int deadto = 0;
+			for (int fi = 0; fi < NL; fi++) {
+				unsigned appf = 0;
+				uint16_t* lf = slst + fi * bv;
+				for (int c = coff[fi]; c < coff[fi + 1]; c++) {
+					const int leaf = schg[c];
+					const int to = ssto[c];
+					const int pos = slkp[leaf];
+					const int last = cnt[fi] - 1;
+					if (pos < last) {
+						const int moved = lf[last];
+						lf[pos] = (uint16_t)moved;
+						slkp[moved] = (uint16_t)pos;
+					}
+					slkp[leaf] = NUL16;
+					cnt[fi] = last;
+					if (inside_band(to, L)) {
+						const int ti = to + L;
+						slst[ti * bv + cnt[ti]] = (uint16_t)leaf;
+						slkp[leaf] = (uint16_t)cnt[ti];
+						if (cnt[ti] == 0) appf |= 1u << ti;
+						cnt[ti]++;
+						if (last == 0) remb |= 1u << fi;
+					} else {
+						P.phi[sl * bv + leaf] = (float)to;
+						live--;
+						if (last == 0) {
+							remb |= 1u << fi;
+							if (live == 0) {
+								dead = true;
+								deadto = to;
+							}
+						}
+					}
+				}
+				P.app[gp * NL + fi] = appf;
+			}
+			P.rem[gp] = remb;
+			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)coff[NL]);
+			if (dead) {
+				P.bg[gp] = (float)deadto;
+				P.oslot[gp] = sl;
+				P.slot[gp] = -1;
+				P.q_retire[atomicAdd(&P.counters[CNT_RETIRE], 1)] = sl;
+			}
+		}
+		__syncthreads();
+		for (int l = 0; l < NL; l++) {
+			uint16_t* dst = P.lst + ((size_t)sl * NL + l) * bv;
+			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x) dst[i] = slst[l * bv + i];
+			if (threadIdx.x == 0) P.lcnt[sl * NL + l] = cnt[l];
+		}
+		for (int i = threadIdx.x; i < BV; i += blockDim.x) P.lkp[sl * bv + i] = slkp[i];
+		__syncthreads();
 	}
 }
 
@@ -911,6 +1120,215 @@ __global__ void k_seed(Dev P, int s, Vec<D> centre)
 			P.lkp[(size_t)sl * P.BV + leaf] = (uint16_t)c;
 			P.lcnt[sl * NL + li] = c + 1;
 		}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// Local update: update_start / delta / update_end (Surface.hpp:393-459, 404-430, 780-913).
+// The delta() calls and calc_affected's ring growth are sequential in the reference and define
+// list orders, so they run on one thread; everything after reuses the parallel passes.
+// ---------------------------------------------------------------------------------------------
+
+/// Partitioned::Lookup::track (PartitionedMixin.hpp:388-413) into affected buffer b: the
+/// partition joins list t on first use, the leaf joins it unless already in a list.
+template <int L>
+__device__ void a_track(const Dev& P, int b, const SurfGeom& g, int s, int gp, int sl, int leaf,
+                        int t)
+{
+	constexpr int NL = 2 * L + 1;
+	if (P.appos[b][gp * NL + t] < 0) {
+		const int c = P.apcnt[b][s * NL + t];
+		P.aplist[b][(size_t)t * P.NP + g.pbase + c] = gp - g.pbase;
+		P.appos[b][gp * NL + t] = c;
+		P.apcnt[b][s * NL + t] = c + 1;
+	}
+	const size_t k = (size_t)sl * P.BV + leaf;
+	if (P.alkp[b][k] == NUL16) {
+		const int c = P.acnt[b][sl * NL + t];
+		P.alst[b][((size_t)sl * NL + t) * P.BV + c] = (uint16_t)leaf;
+		P.alkp[b][k] = (uint16_t)c;
+		P.acnt[b][sl * NL + t] = c + 1;
+	}
+}
+
+/// The delta(pos, val) calls (Surface.hpp:441-459), in call order, followed by the first step of
+/// calc_affected (Surface.hpp:788-799), which tracks exactly those leaves, in the same order,
+/// into affected buffer 0. The delta grid's zero-layer lists are therefore the prefixes of the
+/// affected zero-layer lists recorded in dlcnt / ndp. Later values at a leaf overwrite earlier
+/// ones, as the delta grid's track does.
+template <int D, int L>
+__global__ void k_local_seed(Dev P, int s, const int* pos, const float* val, int n)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	for (int i = 0; i < n; i++) {
+		Vec<D> p;
+		for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+		if (!in_grid<D>(g, p)) {
+			atomicOr(P.err, EB_OUTSIDE);
+			continue;
+		}
+		int gp, leaf;
+		locate<D>(P, g, p, gp, leaf);
+		const int sl = P.slot[gp];
+		if (sl < 0) {
+			atomicOr(P.err, EB_INACTIVE);
+			continue;
+		}
+		P.dlt[(size_t)sl * P.BV + leaf] = val[i];
+		a_track<L>(P, 0, g, s, gp, sl, leaf, L);
+	}
+	const int np = P.apcnt[0][s * NL + L];
+	for (int i = 0; i < np; i++) {
+		const int gp = g.pbase + P.aplist[0][(size_t)L * P.NP + g.pbase + i];
+		const int sl = P.slot[gp];
+		P.dlcnt[sl] = P.acnt[0][sl * NL + L];
+	}
+	P.ndp[s] = np;
+}
+
+/// calc_affected rings (Surface.hpp:801-912): L times, the in-band neighbours of the leaves
+/// added by the previous ring join affected buffer 0 under their current layer.
+template <int D, int L>
+__global__ void k_calc_affected(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	int* first = P.ring_first;
+	int* last = P.ring_last;
+	int nsnap[NL], prev[NL];
+	for (int l = 0; l < NL; l++) prev[l] = 0;
+	for (int ud = 1; ud <= L; ud++) {
+		for (int l = 0; l < NL; l++) {
+			const int nc = P.apcnt[0][s * NL + l];
+			for (int i = 0; i < nc; i++) {
+				const size_t o = (size_t)l * P.NP + g.pbase + i;
+				if (i >= prev[l]) first[o] = 0;
+				const int gp = g.pbase + P.aplist[0][o];
+				last[o] = P.acnt[0][P.slot[gp] * NL + l];
+			}
+			nsnap[l] = nc;
+			prev[l] = nc;
+		}
+		for (int l = 0; l < NL; l++) {
+			for (int ic = 0; ic < nsnap[l]; ic++) {
+				const size_t o = (size_t)l * P.NP + g.pbase + ic;
+				const int gp = g.pbase + P.aplist[0][o];
+				const int sl = P.slot[gp];
+				for (int in = first[o]; in < last[o]; in++) {
+					const int leaf = P.alst[0][((size_t)sl * NL + l) * P.BV + in];
+					const Vec<D> c = leaf_pos<D>(P, gp, leaf);
+					for (int nb = 0; nb < 2 * D; nb++) {
+						Vec<D> q = c;
+						q[nb >> 1] += (nb & 1) ? 1 : -1;
+						const int lid = layer_id(get_phi<D, L>(P, g, q), P.err);
+						if (!inside_band(lid, L)) continue;
+						int gpn, leafn;
+						locate<D>(P, g, q, gpn, leafn);
+						const int sln = P.slot[gpn];
+						if (sln < 0) {
+							atomicOr(P.err, EB_INACTIVE);
+							continue;
+						}
+						a_track<L>(P, 0, g, s, gpn, sln, leafn, lid + L);
+					}
+				}
+			}
+		}
+		for (int l = 0; l < NL; l++)
+			for (int ic = 0; ic < nsnap[l]; ic++) {
+				const size_t o = (size_t)l * P.NP + g.pbase + ic;
+				first[o] = last[o];
+			}
+	}
+}
+
+/// isogrid.track_children(affected) and delta.track_children(affected) of update_end
+/// (Surface.hpp:409-410; PartitionedMixin.hpp:319-334). The delta partition lists, reset at
+/// update_start and holding the delta() partitions first, end up equal to the affected lists.
+template <int L>
+__global__ void k_local_children(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	for (int l = 0; l < NL; l++) {
+		const int na = P.apcnt[0][s * NL + l];
+		for (int i = 0; i < na; i++) {
+			const size_t o = (size_t)l * P.NP + g.pbase + i;
+			const int lp = P.aplist[0][o];
+			const int gp = g.pbase + lp;
+			if (P.ppos[gp * NL + l] < 0) {
+				const int c = P.pcnt[s * NL + l];
+				P.plist[(size_t)l * P.NP + g.pbase + c] = lp;
+				P.ppos[gp * NL + l] = c;
+				P.pcnt[s * NL + l] = c + 1;
+			}
+			P.dplist[o] = lp;
+		}
+		P.dpcnt[s * NL + l] = na;
+	}
+}
+
+/// update(lo, hi, fn) (Surface.hpp:310-386): the zero-layer leaves of the partitions covering
+/// the box, in the reference's order (box partitions row-major, leaf list order), that lie in
+/// [lo, hi]. Writes their positions; *n receives the count (up to cap).
+template <int D, int L>
+__global__ void k_bounded_collect(Dev P, int s, Vec<D> lo, Vec<D> hi, int* pos, int cap, int* n)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	Vec<D> cl, cu, box, lub;
+	long long nb = 1;
+	for (int a = 0; a < D; a++) {
+		// pos_child (truncating division, PartitionedMixin.hpp:233-245) of the grid's corners
+		// and of the box corners, in zero-based children coordinates (Surface.hpp:313-330)
+		const int grid_lo = 0;
+		const int grid_hi = (g.hi[a] - 1 - g.off[a]) / P.csz[a];
+		cl[a] = max(grid_lo, (lo[a] - g.off[a]) / P.csz[a]);
+		cu[a] = min(grid_hi, (hi[a] - g.off[a]) / P.csz[a]);
+		box[a] = cu[a] - cl[a] + 1;
+		lub[a] = min(g.hi[a], hi[a] + 1);
+		nb *= box[a] > 0 ? box[a] : 0;
+	}
+	int c = 0;
+	for (long long ci = 0; ci < nb; ci++) {
+		Vec<D> pc;
+		long long r = ci;
+		for (int a = D - 1; a >= 0; a--) {
+			pc[a] = (int)(r % box[a]) + cl[a];
+			r /= box[a];
+		}
+		int idx = 0;
+		for (int a = 0; a < D; a++) idx = idx * g.ccount[a] + pc[a];
+		const int gp = g.pbase + idx;
+		const int sl = P.slot[gp];
+		if (sl < 0) continue;
+		const int nl = P.lcnt[sl * NL + L];
+		for (int j = 0; j < nl; j++) {
+			const int leaf = P.lst[((size_t)sl * NL + L) * P.BV + j];
+			const Vec<D> p = leaf_pos<D>(P, gp, leaf);
+			bool in = true;
+			for (int a = 0; a < D; a++)
+				if (p[a] < lo[a] || p[a] >= lub[a]) in = false;
+			if (!in) continue;
+			if (c < cap)
+				for (int a = 0; a < D; a++) pos[c * D + a] = p[a];
+			c++;
+		}
+	}
+	*n = c;
+}
+
+/// The speed functor at each collected position, before any value changes.
+template <int D, int L>
+__global__ void k_bounded_speed(Dev P, int s, Speed sp, const int* pos, const int* n, float* val)
+{
+	const SurfGeom& g = P.geom[s];
+	const int m = *n;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+		Vec<D> p;
+		for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+		val[i] = speed_eval<D, L>(P, g, sp, p);
 	}
 }
 

@@ -140,6 +140,13 @@ FG_API int fg_partition_list(fg_surface* s, int layer_idx, uint32_t* out, size_t
 FG_API int fg_delta_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
 FG_API int fg_status_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
 
+/* affected() (include/Felt/Surface.hpp:693-696): the affected lookup's partition list for a
+ * layer and one partition's ordered leaf list, as left by the last update (calc_affected's
+ * rings after a local update). */
+FG_API int fg_affected_partitions(fg_surface* s, int layer_idx, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_affected_list(fg_surface* s, size_t part, int layer_idx, uint32_t* out, size_t cap,
+                            size_t* n);
+
 /* children().get(p).is_active() and background() (GridMixin.hpp:56-69). */
 FG_API int fg_partition_state(fg_surface* s, size_t part, int* active, float* background);
 

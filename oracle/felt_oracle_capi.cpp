@@ -28,6 +28,7 @@ struct SurfBase {
 	virtual void partitions(int* csize, int* coff) = 0;
 	virtual const std::vector<size_t>* leaf_list(size_t part, int l) = 0;
 	virtual const std::vector<size_t>* plist(int which, int l) = 0;
+	virtual const std::vector<size_t>* affected_list(size_t part, int l) = 0;
 	virtual void pstate(size_t part, int* active, float* bg) = 0;
 	virtual void stats(size_t* a, size_t* b) = 0;
 	virtual size_t band_size() = 0;
@@ -100,6 +101,10 @@ struct Surf : SurfBase {
 		case 3: return &s.aff.clists[l];
 		default: return nullptr;
 		}
+	}
+	const std::vector<size_t>* affected_list(size_t part, int l) override
+	{
+		return &s.aff.ch[part].lists[l];
 	}
 	void pstate(size_t part, int* active, float* bg) override
 	{
@@ -322,6 +327,10 @@ int fo_layer_list(void* s, size_t part, int l, uint32_t* out, size_t cap, size_t
 int fo_partition_list(void* s, int which, int l, uint32_t* out, size_t cap, size_t* n)
 {
 	return guard([&] { put_list(*static_cast<SurfBase*>(s)->plist(which, l), out, cap, n); });
+}
+int fo_affected_list(void* s, size_t part, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(*static_cast<SurfBase*>(s)->affected_list(part, l), out, cap, n); });
 }
 int fo_partition_state(void* s, size_t part, int* active, float* bg)
 {

@@ -154,6 +154,9 @@ class Surface:
     def affected_partitions(self, layer_idx):
         return self.partition_list(layer_idx, which=3)
 
+    def affected_list(self, part, layer_idx):
+        return _fetch_list(lib().fo_affected_list, self._h, C.c_size_t(part), C.c_int(layer_idx))
+
     def partition_state(self, part):
         a = C.c_int()
         bg = C.c_float()

@@ -112,6 +112,24 @@ def surface_cases(root):
               lseed + [["update_start"], ["delta", [0, 0], -1.0], ["update_end"]], 643, 665)
     grid_case("bounded_update_9x9", "811-880", [9, 9], [2, 2], 2,
               lseed + [["update_bounded", [-1, -1], [1, 1], -0.6]], 816, 839)
+    # affected() after a local update of two zero-layer points (test_Surface.cpp:668-759):
+    # per layer the set of affected leaf positions (layer 0 not checked by the reference).
+    aff = {}
+    for ln in L[679:704]:
+        m = re.search(r"check_layers_pos\[2 \+ (-?\d+)\]", ln)
+        if m:
+            cur = int(m.group(1))
+            aff[cur] = []
+        if "//" in ln.split("Vec2i")[0] if "Vec2i" in ln else False:
+            continue
+        for a, b in re.findall(r"Vec2i\((-?\d+), (-?\d+)\)", re.sub(r"//.*", "", ln)):
+            aff[cur].append([int(a), int(b)])
+    cases.append(dict(name="affected_after_local_update_9x9", ref=f"{f}:668-759", size=[9, 9],
+                      part=[2, 2], layers=2, grid=None, layer_sizes={},
+                      steps=lseed + [["update_start"], ["delta", [0, 0], -1.0], ["update_end"],
+                                     ["update_start"], ["delta", [0, 1], 0.3],
+                                     ["delta", [1, 0], 0.3], ["update_end"]],
+                      affected={k: v for k, v in aff.items() if k != 0}))
     # Layer interactions.
     two = [["seed", [-4, 0]], ["seed", [4, 0]], upd(-1.0)]
     grid_case("two_seeds_16x9", "888-932", [16, 9], [3, 3], 2, two, 911, 931,

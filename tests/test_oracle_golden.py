@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.scenario import child_index, run_steps
+from tests.scenario import affected_positions, child_index, run_steps
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -41,6 +41,9 @@ def test_surface_golden(case):
         pos_child = [int(x) for x in key.split(",")]
         active, _ = s.partition_state(child_index(pos_child, ccount, coff))
         assert active == want_active, key
+    for lid, want in (case.get("affected") or {}).items():
+        got = affected_positions(s, int(lid) + case["layers"])
+        assert sorted(got) == sorted(want), f"affected layer {lid}"
 
 
 @pytest.mark.parametrize("case", _cases("poly"), ids=lambda c: c["name"])
