@@ -239,6 +239,102 @@ class Surface:
         return np.array(_fetch(lib().fg_dump, self._h), dtype=np.uint32)
 
 
+class Batch:
+    """Many independent Surface<D,L> (same D, L, partition shape; any grid sizes) advanced by the
+    same kernel launches. Per surface the results equal a separate Surface's."""
+
+    def __init__(self, sizes, part, layers, brick_capacity=0):
+        self.n = len(sizes)
+        self.D = len(part)
+        self.L = int(layers)
+        self.part = tuple(int(p) for p in part)
+        self.sizes = [tuple(int(x) for x in s) for s in sizes]
+        flat = [x for s in self.sizes for x in s]
+        cfg = Config(int(brick_capacity), 0, 0)
+        h = C.c_void_p()
+        _chk(lib().fg_batch_create(self.D, self.L, _ivec(part), C.c_size_t(self.n), _ivec(flat),
+                                   C.byref(cfg), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fg_batch_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def seed(self, centres):
+        flat = [int(x) for c in centres for x in c]
+        _chk(lib().fg_batch_seed(self._h, _ivec(flat)))
+
+    def update(self, speeds):
+        """speeds: one dict(c=, a=, n=, seed=) per surface (or one dict for all)."""
+        if isinstance(speeds, dict):
+            speeds = [speeds] * self.n
+        arr = (Speed * self.n)(*[make_speed(**s) for s in speeds])
+        _chk(lib().fg_batch_update(self._h, arr))
+
+    def polys_notify(self):
+        _chk(lib().fg_batch_polys_notify(self._h))
+
+    def polys_march(self):
+        _chk(lib().fg_batch_polys_march(self._h))
+
+    def polys_invalidate(self):
+        _chk(lib().fg_batch_polys_invalidate(self._h))
+
+    def snapshot(self, i):
+        n = int(np.prod(self.sizes[i]))
+        out = np.zeros(n, dtype=np.float32)
+        _chk(lib().fg_batch_snapshot(self._h, C.c_size_t(i),
+                                     out.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(n)))
+        return out.reshape(self.sizes[i])
+
+    def dump(self, i):
+        return np.array(_fetch(lib().fg_batch_dump, self._h, C.c_size_t(i)), dtype=np.uint32)
+
+    def polys_changes(self, i):
+        return _fetch(lib().fg_batch_polys_changes, self._h, C.c_size_t(i))
+
+    def polys_partition(self, i, part):
+        D = self.D
+        per = 2 * D if D == 3 else D
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        act = C.c_int()
+        _chk(lib().fg_batch_polys_partition(self._h, C.c_size_t(i), C.c_size_t(part), None,
+                                            C.c_size_t(0), None, C.c_size_t(0), C.byref(nv),
+                                            C.byref(ns), C.byref(act)))
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
+        spx = np.zeros(max(1, ns.value * D), dtype=np.uint32)
+        _chk(lib().fg_batch_polys_partition(self._h, C.c_size_t(i), C.c_size_t(part),
+                                            vtx.ctypes.data_as(C.POINTER(C.c_float)),
+                                            C.c_size_t(vtx.size),
+                                            spx.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                            C.c_size_t(spx.size), C.byref(nv), C.byref(ns),
+                                            C.byref(act)))
+        return (vtx[: nv.value * per].reshape(nv.value, per),
+                spx[: ns.value * D].reshape(ns.value, D), bool(act.value))
+
+    def polys_totals(self):
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        _chk(lib().fg_batch_polys_totals(self._h, C.byref(nv), C.byref(ns)))
+        return nv.value, ns.value
+
+    def node_updates(self):
+        n = C.c_ulonglong()
+        _chk(lib().fg_batch_node_updates(self._h, C.byref(n)))
+        return n.value
+
+    def stream(self):
+        p = C.c_void_p()
+        _chk(lib().fg_batch_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+
 class Polys:
     """Felt::Polys<Surface> (include/Felt/Polys.hpp:1-229) on the GPU."""
 

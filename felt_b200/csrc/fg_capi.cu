@@ -388,6 +388,162 @@ int fg_node_updates(fg_surface* s, unsigned long long* n)
 	});
 }
 
+// ---- batches ----
+
+int fg_batch_create(int dims, int layers, const int* part, size_t n, const int* sizes,
+                    const fg_config* cfg, fg_batch** out)
+{
+	return guard([&] {
+		need(part, "part");
+		need(sizes, "sizes");
+		need(out, "out");
+		if (dims != 2 && dims != 3) throw fg::Error(FG_ERR_ARG, "dims must be 2 or 3");
+		if (layers < 1 || layers > 4) throw fg::Error(FG_ERR_ARG, "layers must be in 1..4");
+		if (n == 0) throw fg::Error(FG_ERR_ARG, "a batch needs at least one surface");
+		int ndev = 0;
+		if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+			throw fg::Error(FG_ERR_CUDA, "no CUDA device");
+		fg::PoolDesc d;
+		d.D = dims;
+		d.L = layers;
+		for (int a = 0; a < dims; a++) d.part[a] = part[a];
+		for (size_t i = 0; i < n; i++) {
+			std::array<int, 3> sz = {1, 1, 1};
+			for (int a = 0; a < dims; a++) sz[a] = sizes[i * dims + a];
+			d.sizes.push_back(sz);
+		}
+		if (cfg) d.brick_capacity = cfg->brick_capacity;
+		auto b = std::make_unique<fg_batch>();
+		FG_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+		b->eng.reset(fg::make_engine(d, b->st));
+		*out = b.release();
+	});
+}
+
+int fg_batch_destroy(fg_batch* b)
+{
+	return guard([&] { delete b; });
+}
+
+int fg_batch_seed(fg_batch* b, const int* centres)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(centres, "centres");
+		b->eng->seed_all(centres);
+	});
+}
+
+int fg_batch_update(fg_batch* b, const fg_speed* speeds)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(speeds, "speeds");
+		const int S = b->eng->surfaces();
+		std::vector<fg::Speed> sp(S);
+		for (int i = 0; i < S; i++) sp[i] = to_speed(&speeds[i]);
+		b->eng->update_builtin(sp.data());
+	});
+}
+
+static fg::PolysBase& batch_polys(fg_batch* b)
+{
+	if (!b->polys) b->polys.reset(fg::make_polys(*b->eng, 0));
+	return *b->polys;
+}
+
+int fg_batch_polys_notify(fg_batch* b)
+{
+	return guard([&] {
+		need(b, "batch");
+		batch_polys(b).notify();
+	});
+}
+
+int fg_batch_polys_march(fg_batch* b)
+{
+	return guard([&] {
+		need(b, "batch");
+		batch_polys(b).march();
+	});
+}
+
+int fg_batch_polys_invalidate(fg_batch* b)
+{
+	return guard([&] {
+		need(b, "batch");
+		batch_polys(b).invalidate();
+	});
+}
+
+int fg_batch_snapshot(fg_batch* b, size_t surface, float* dst, size_t n)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(dst, "dst");
+		b->eng->snapshot((int)surface, dst, n, false);
+	});
+}
+
+int fg_batch_dump(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(b, "batch");
+		put_list(b->eng->dump((int)surface), out, cap, n);
+	});
+}
+
+int fg_batch_polys_partition(fg_batch* b, size_t surface, size_t part, float* vtx, size_t vcap,
+                             uint32_t* spx, size_t scap, size_t* nv, size_t* ns, int* active)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(nv, "nv");
+		need(ns, "ns");
+		fg::PolysBase& p = batch_polys(b);
+		p.select((int)surface);
+		int act = 0;
+		p.partition(part, vtx, vcap, spx, scap, nv, ns, &act);
+		if (active) *active = act;
+	});
+}
+
+int fg_batch_polys_changes(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(b, "batch");
+		fg::PolysBase& p = batch_polys(b);
+		p.select((int)surface);
+		put_list(p.changes(), out, cap, n);
+	});
+}
+
+int fg_batch_polys_totals(fg_batch* b, size_t* nv, size_t* ns)
+{
+	return guard([&] {
+		need(b, "batch");
+		batch_polys(b).totals(nv, ns);
+	});
+}
+
+int fg_batch_node_updates(fg_batch* b, unsigned long long* n)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(n, "n");
+		*n = b->eng->node_updates();
+	});
+}
+
+int fg_batch_stream(fg_batch* b, void** stream)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(stream, "stream");
+		*stream = (void*)b->eng->stream();
+	});
+}
+
 int fg_work_units(fg_surface* s, unsigned long long* out, size_t n)
 {
 	return guard([&] {

@@ -290,6 +290,21 @@ public:
 		check_errors();
 	}
 
+	void seed_all(const int* centres) override
+	{
+		int* d = nullptr;
+		FG_CUDA(cudaMalloc(&d, (size_t)P_.S * D * sizeof(int)));
+		cudaError_t e = cudaMemcpyAsync(d, centres, (size_t)P_.S * D * sizeof(int),
+		                                cudaMemcpyHostToDevice, st_);
+		if (e == cudaSuccess) {
+			FG_RUN("k_seed_all", st_, k_seed_all<D, L><<<(P_.S + 63) / 64, 64, 0, st_>>>(P_, d););
+			e = cudaStreamSynchronize(st_);
+		}
+		cudaFree(d);
+		if (e != cudaSuccess) throw Error(-2, cudaGetErrorString(e));
+		check_errors();
+	}
+
 	// ---- global update ----
 	void update_builtin(const Speed* speeds) override
 	{

@@ -51,6 +51,8 @@ public:
 	virtual cudaStream_t stream() const = 0;
 
 	virtual void seed(int s, const int* pos) = 0;
+	/// One seed per surface, centres holding S*D ints.
+	virtual void seed_all(const int* centres) = 0;
 	/// Global update of every surface of the pool with one builtin speed per surface
 	/// (host array of S speeds).
 	virtual void update_builtin(const Speed* speeds) = 0;

@@ -27,6 +27,18 @@ struct fg_polys {
 	std::unique_ptr<fg::PolysBase> impl;
 };
 
+struct fg_batch {
+	std::unique_ptr<fg::PolysBase> polys;  // destroyed before the engine it refers to
+	std::unique_ptr<fg::EngineBase> eng;
+	cudaStream_t st = nullptr;
+	~fg_batch()
+	{
+		polys.reset();
+		eng.reset();
+		if (st) cudaStreamDestroy(st);
+	}
+};
+
 namespace fg {
 /// Records the message fg_last_error() returns on the calling thread.
 void set_last_error(const std::string& msg);

@@ -1059,10 +1059,31 @@ __global__ void k_snapshot(Dev P, int s, float* out, long long total)
 	}
 }
 
+template <int D, int L>
+__device__ void seed_one(const Dev& P, int s, Vec<D> centre);
+
 /// seed (Surface.hpp:207-241) executed by one thread: the window walk and its track calls are
 /// sequential in the reference and set the initial list orders.
 template <int D, int L>
 __global__ void k_seed(Dev P, int s, Vec<D> centre)
+{
+	seed_one<D, L>(P, s, centre);
+}
+
+/// One seed per surface of the pool (centres[s*D..]), one thread per surface: surfaces share
+/// no list state, only the brick allocator, which is atomic.
+template <int D, int L>
+__global__ void k_seed_all(Dev P, const int* centres)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= P.S) return;
+	Vec<D> c;
+	for (int a = 0; a < D; a++) c[a] = centres[s * D + a];
+	seed_one<D, L>(P, s, c);
+}
+
+template <int D, int L>
+__device__ void seed_one(const Dev& P, int s, Vec<D> centre)
 {
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];

@@ -788,6 +788,14 @@ private:
 		cudaFree(dso);
 	}
 
+public:
+	void select(int s) override
+	{
+		if (s < 0 || s >= eng_.surfaces()) throw Error(-1, "surface index out of range");
+		s_ = s;
+	}
+
+private:
 	EngineBase& eng_;
 	int s_;
 	PolysDev Q_;

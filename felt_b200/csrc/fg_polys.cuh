@@ -21,6 +21,8 @@ public:
 	virtual void partition(size_t part, float* vtx, size_t vcap, uint32_t* spx, size_t scap,
 	                       size_t* nv, size_t* ns, int* active) = 0;
 	virtual void totals(size_t* nv, size_t* ns) = 0;
+	/// Surface of the pool that changes(), partition() and march_partition() refer to.
+	virtual void select(int s) = 0;
 };
 
 /// Polygonisation of surface s of an engine's pool.

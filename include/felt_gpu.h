@@ -181,6 +181,34 @@ FG_API int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_c
 /* Totals over all partitions. */
 FG_API int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
 
+/* ---- batches: many independent surfaces advanced by the same kernel launches ----
+ * The reference runs one Surface at a time; a batch holds n surfaces that share D, L and the
+ * partition shape but may differ in grid size, and every update / polygonisation call advances
+ * all of them in the same launches. Per surface the results are exactly those of a separate
+ * fg_surface (same lists, orders and values). sizes holds n*dims ints. */
+FG_API int fg_batch_create(int dims, int layers, const int* part, size_t n, const int* sizes,
+                           const fg_config* cfg, fg_batch** out);
+FG_API int fg_batch_destroy(fg_batch* b);
+/* seed(pos) of every surface (centres: n*dims ints), one seed per surface. */
+FG_API int fg_batch_seed(fg_batch* b, const int* centres);
+/* update(fn) of every surface with its own builtin speed (speeds: n entries). */
+FG_API int fg_batch_update(fg_batch* b, const fg_speed* speeds);
+/* Polys over the batch: notify / march / invalidate for all surfaces at once. */
+FG_API int fg_batch_polys_notify(fg_batch* b);
+FG_API int fg_batch_polys_march(fg_batch* b);
+FG_API int fg_batch_polys_invalidate(fg_batch* b);
+/* Per-surface queries, as the fg_surface ones. */
+FG_API int fg_batch_snapshot(fg_batch* b, size_t surface, float* dst, size_t n);
+FG_API int fg_batch_dump(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_batch_polys_partition(fg_batch* b, size_t surface, size_t part, float* vtx,
+                                    size_t vtx_cap, uint32_t* spx, size_t spx_cap, size_t* nv,
+                                    size_t* ns, int* active);
+FG_API int fg_batch_polys_changes(fg_batch* b, size_t surface, uint32_t* out, size_t cap,
+                                  size_t* n);
+FG_API int fg_batch_polys_totals(fg_batch* b, size_t* vertices, size_t* simplices);
+FG_API int fg_batch_node_updates(fg_batch* b, unsigned long long* n);
+FG_API int fg_batch_stream(fg_batch* b, void** stream);
+
 /* ---- instrumentation (no counterpart in the reference; Surface.hpp has no timers) ----
  * fg_node_updates: narrow-band node-updates processed by all global updates of a surface so
  * far (band size at the start of each update, summed). fg_launch_count: kernels this library
