@@ -1,24 +1,31 @@
 """Benchmark of the sparse-field level-set hot path (Surface<D,L>::update + Polys) on B200.
 
-Workload (default, --config c2): Surface<3,3> float32, 512^3 isogrid with 16^3 partitions,
+Default workload (--config c2): Surface<3,3> float32, 512^3 isogrid with 16^3 partitions,
 seeded at the origin and expanded to radius ~100 with 100 untimed steps of speed -1, then timed
 steps of delta = -0.2*curv(pos) + 0.1*h(pos, 1234) (h = hashed uniform [-1,1) noise), with
 Polys::notify every step and Polys::march every 10th step. A "step" is one Surface::update plus
 that repolygonisation. Metric: narrow-band node-updates/s (band size at each step's start).
 
+Other configs: c1 (Surface<3,2> 64^3, 8^3 partitions, speed -0.5), c3 (4096 Surface<2,2>, grid
+edges log-uniform 128..1024, 16^2 partitions, constant speeds U[-0.8,-0.2], marching squares
+each step) and c4 (256 Surface<3,2>, edges from {32,48,64,96,128}, 8^3 partitions, speed
+-0.3*curv + U[-0.6,0.3], marching cubes at the end), both run as one batch (all surfaces in the
+same launches) and also, on a subset, one surface per launch sequence (the plain path).
+
 Arms:
-  default           the device engine (libfelt_gpu.so) driven through its C ABI.
+  default           the device engine (libfelt_gpu.so) through its C ABI.
   --impl reference  the reference algorithm's CPU implementation (the oracle port, compiled
                     from oracle/), on the same workload and metric, bounded sample.
 
 Prints ONE JSON line on rank 0. Multi-GPU (torchrun): every rank advances its own independent
-surface (replicas; a single surface does not shard), value = all ranks' node-updates / the
-slowest rank's time.
+replica of the workload (a single surface does not shard), value = all ranks' node-updates /
+the slowest rank's time.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -30,34 +37,63 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    # name: (D, L, size, part, expansion steps, timed speed, march every)
-    "c2": dict(D=3, L=3, size=(512, 512, 512), part=(16, 16, 16), expand=100,
-               speed=dict(a=-0.2, n=0.1, seed=1234), march_every=10,
-               workload="Surface<3,3> 512^3 / 16^3 partitions, r~100, "
-                        "speed -0.2*curv + 0.1*hash_noise, repolygonise every 10 steps"),
-    "c1": dict(D=3, L=2, size=(64, 64, 64), part=(8, 8, 8), expand=0,
-               speed=dict(c=-0.5), march_every=0,
-               workload="Surface<3,2> 64^3 / 8^3 partitions, speed -0.5"),
+    "c1": dict(kind="single", D=3, L=2, size=(64, 64, 64), part=(8, 8, 8), expand=0,
+               speed=dict(c=-0.5), march_every=0, march_end=True, steps=50,
+               workload="Surface<3,2> 64^3 / 8^3 partitions, seed at origin, speed -0.5, "
+                        "marching cubes at the end"),
+    "c2": dict(kind="single", D=3, L=3, size=(512, 512, 512), part=(16, 16, 16), expand=100,
+               speed=dict(a=-0.2, n=0.1, seed=1234), march_every=10, march_end=False,
+               steps=40,
+               workload="Surface<3,3> 512^3 / 16^3 partitions, r~100, speed -0.2*curv + "
+                        "0.1*hash_noise, repolygonise every 10 steps"),
+    "c3": dict(kind="batch", D=2, L=2, n=4096, part=(16, 16), march_every=1, march_end=False,
+               steps=100, plain_subset=16, cpu_subset=16, cpu_steps=100,
+               workload="4096 x Surface<2,2>, edges log-uniform 128..1024, 16^2 partitions, "
+                        "constant speed U[-0.8,-0.2] per surface, marching squares every step"),
+    "c4": dict(kind="batch", D=3, L=2, n=256, part=(8, 8, 8), march_every=0, march_end=True,
+               steps=100, plain_subset=16, cpu_subset=4, cpu_steps=50,
+               workload="256 x Surface<3,2>, edges from {32,48,64,96,128}, 8^3 partitions, "
+                        "speed -0.3*curv + U[-0.6,0.3], marching cubes at the end"),
 }
 
-# Algorithmic bytes per work unit of the kernels whose roofline is reported (see DESIGN.md):
+# Algorithmic bytes per work unit of the kernels whose roofline is reported:
 #  k_dist1: per band node of the layer: 2 B list index + 4 B phi read + 4 B delta write.
 #  k_dist2: per band node: 2 B list index + 4 B delta read + 4 B phi write.
-#  k_delta_builtin: per zero-layer node: 2 B index + 4 B phi + 4 B delta write.
-#  k_flush_leaf: per leaf edit: 2 B status entry + 1 B to-layer + 2 B lookup read + 2 B list
-#                write + 2 B lookup write + 4 B swap-in (moved entry and its lookup).
+#  k_delta_*: per zero-layer node: 2 B index + 4 B phi + 4 B delta write.
+#  k_flush_*: per leaf edit: 2 B status entry + 1 B to-layer + 2 B lookup read + 2 B list
+#             write + 2 B lookup write + 4 B swap-in (moved entry and its lookup).
 #  k_polys_march: per cell: 2 B leaf index + 4 B phi (corners are neighbours' phi).
 UNIT_BYTES = {"k_dist1": (0, 10), "k_dist2": (0, 10), "k_delta_builtin": (1, 10),
-              "k_delta_smem": (1, 10), "k_flush_smem": (2, 13),
-              "k_flush_leaf": (2, 13), "k_polys_march": (3, 6)}
+              "k_delta_smem": (1, 10), "k_flush_smem": (2, 13), "k_flush_leaf": (2, 13),
+              "k_polys_march": (3, 6)}
+
+
+def batch_surfaces(name, cfg):
+    """Seeded synthetic surfaces of a batched config: sizes, seed centres, speeds."""
+    import numpy as np
+    rng = np.random.default_rng(0x5EED0000 + int(name[1:]))
+    L, D = cfg["L"], cfg["D"]
+    sizes, centres, speeds = [], [], []
+    for _ in range(cfg["n"]):
+        if name == "c3":
+            e = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
+            speed = dict(c=float(rng.uniform(-0.8, -0.2)))
+        else:
+            e = int(rng.choice([32, 48, 64, 96, 128]))
+            speed = dict(a=-0.3, c=float(rng.uniform(-0.6, 0.3)))
+        size = (e,) * D
+        lo, hi = -e // 2 + L + 1, e // 2 - L - 2
+        c = tuple(int(rng.integers(lo, hi + 1)) for _ in range(D))
+        sizes.append(size)
+        centres.append(c)
+        speeds.append(speed)
+    return sizes, centres, speeds
 
 
 def load_peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
 
@@ -70,10 +106,7 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
-        self.thread = None
+        self.gpu, self.proc, self.lines, self.thread = gpu_index, None, [], None
 
     def start(self):
         try:
@@ -120,16 +153,154 @@ class ClockSampler:
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def cpu_baseline(cfg, steps, warm=3):
-    """The oracle port on a bounded sample of the same workload: the same setup (seed and
-    expansion), then `steps` timed steps of the same speed with the same repolygonisation.
-    Returns (node-updates/s, sample description)."""
+# ---------------------------------------------------------------------------------------------
+# Device workloads
+# ---------------------------------------------------------------------------------------------
+
+class SingleWork:
+    """One Surface (+ Polys) through the C ABI."""
+
+    def __init__(self, fb, cfg):
+        self.fb, self.cfg = fb, cfg
+        self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"])
+        self.p = fb.Polys(self.s)
+        self.s.seed((0,) * cfg["D"])
+        for _ in range(cfg["expand"]):
+            self.s.update(c=-1.0)
+
+    def step(self, i, last=False):
+        c = self.cfg
+        self.s.update(**c["speed"])
+        self.p.notify()
+        if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+            self.p.march()
+            return True
+        return False
+
+    def node_updates(self):
+        return self.s.node_updates()
+
+    def stream(self):
+        return self.s.stream()
+
+    def work_units(self):
+        return self.s.work_units()
+
+    def fetch_geometry(self):
+        """D2H of the polygons of the partitions re-marched last (what a viewer would read),
+        in one gather call."""
+        vtx, spx, _ = self.p.gather(self.p.changes())
+        return vtx.nbytes + spx.nbytes
+
+
+class BatchWork:
+    """All surfaces of a batched config in one batch."""
+
+    def __init__(self, fb, cfg, name):
+        self.fb, self.cfg = fb, cfg
+        sizes, centres, self.speeds = batch_surfaces(name, cfg)
+        self.b = fb.Batch(sizes, cfg["part"], cfg["L"])
+        self.b.seed(centres)
+        self.surface0 = None
+
+    def step(self, i, last=False):
+        c = self.cfg
+        self.b.update(self.speeds)
+        self.b.polys_notify()
+        if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+            self.b.polys_march()
+            return True
+        return False
+
+    def node_updates(self):
+        return self.b.node_updates()
+
+    def stream(self):
+        return self.b.stream()
+
+    def work_units(self):
+        return self.b.work_units()
+
+    def fetch_geometry(self):
+        """Polygon counts of the batch (a viewer of many small surfaces reads totals)."""
+        self.b.polys_totals()
+        return 16
+
+
+class PlainSubset:
+    """The plain path on the first k surfaces of a batched config: one Surface each, advanced
+    one surface at a time (every update its own launch sequence)."""
+
+    def __init__(self, fb, cfg, name, k):
+        sizes, centres, speeds = batch_surfaces(name, cfg)
+        self.cfg = cfg
+        self.items = []
+        for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
+            s = fb.Surface(sz, cfg["part"], cfg["L"])
+            s.seed(c)
+            self.items.append((s, fb.Polys(s), sp))
+
+    def step(self, i, last=False):
+        c = self.cfg
+        keep = []
+        for s, p, sp in self.items:
+            try:
+                s.update(**sp)
+            except Exception:  # stopped: its convergence loop did not terminate
+                self.done += s.node_updates()
+                continue
+            p.notify()
+            if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+                p.march()
+            keep.append((s, p, sp))
+        self.items = keep
+
+    done = 0
+
+    def node_updates(self):
+        return self.done + sum(s.node_updates() for s, _, _ in self.items)
+
+
+def time_steps(torch, work, stream, steps, warm, flush, start=0):
+    """Times `steps` steps two ways over the same work: device time (CUDA events on the work's
+    stream around the update/polygonisation launches) and end-to-end wall time through the C
+    ABI (the host-side speed structs going in, the step's result coming out: the node-update
+    counter every step and, after a march, the re-marched polygons). L2 is flushed (256 MB
+    write, > 126 MB L2) before each step, outside both timed intervals."""
+    for i in range(warm):
+        work.step(start + i)
+    torch.cuda.synchronize()
+    nu0 = work.node_updates()
+    total, wall, d2h = 0.0, 0.0, 0
+    for i in range(steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        marched = work.step(start + warm + i, last=(i == steps - 1))
+        b.record(stream)
+        if marched:
+            d2h += work.fetch_geometry()
+        work.node_updates()
+        d2h += 8
+        wall += time.perf_counter() - t0
+        b.synchronize()
+        total += a.elapsed_time(b)
+    torch.cuda.synchronize()
+    return total, wall, work.node_updates() - nu0, d2h
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU (oracle port)
+# ---------------------------------------------------------------------------------------------
+
+def cpu_single(cfg, steps, warm=3):
     from oracle import oracle as O
     s = O.Surface(cfg["size"], cfg["part"], cfg["L"])
     p = O.Polys(s)
@@ -139,44 +310,127 @@ def cpu_baseline(cfg, steps, warm=3):
     for _ in range(warm):
         s.update(**cfg["speed"])
         p.notify()
-    nu = 0.0
-    secs = 0.0
+    nu, secs = 0.0, 0.0
     for i in range(steps):
         nu += s.band_size()
         t0 = time.perf_counter()
         s.update(**cfg["speed"])
         p.notify()
-        if cfg["march_every"] and (i + 1) % cfg["march_every"] == 0:
+        if (cfg["march_every"] and (i + 1) % cfg["march_every"] == 0) or (
+                i == steps - 1 and cfg["march_end"]):
             p.march()
         secs += time.perf_counter() - t0
     return nu / secs, nu, secs
 
 
-def run_reference(args, cfg):
+def cpu_batch(name, cfg, steps, k):
+    from oracle import oracle as O
+    sizes, centres, speeds = batch_surfaces(name, cfg)
+    items = []
+    for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
+        s = O.Surface(sz, cfg["part"], cfg["L"])
+        s.seed(c)
+        items.append((s, O.Polys(s), sp))
+    nu, secs = 0.0, 0.0
+    for i in range(steps):
+        keep = []
+        for s, p, sp in items:
+            band = s.band_size()
+            t0 = time.perf_counter()
+            try:
+                s.update(**sp)
+            except O.OracleError:  # the reference's loop would not terminate: drop it
+                secs += time.perf_counter() - t0
+                continue
+            p.notify()
+            if (cfg["march_every"] and (i + 1) % cfg["march_every"] == 0) or (
+                    i == steps - 1 and cfg["march_end"]):
+                p.march()
+            secs += time.perf_counter() - t0
+            nu += band
+            keep.append((s, p, sp))
+        items = keep
+    return nu / secs, nu, secs
+
+
+def cpu_baseline(name, cfg, steps):
+    if cfg["kind"] == "single":
+        rate, nu, secs = cpu_single(cfg, steps)
+        sample = f"{steps} timed steps after the same setup"
+    else:
+        k = cfg["cpu_subset"]
+        rate, nu, secs = cpu_batch(name, cfg, steps, k)
+        sample = f"first {k} surfaces of the workload, {steps} steps each, one after another"
+    return {"value": rate, "unit": "node-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{sample} ({nu:.3g} node-updates in {secs:.2f} s, single thread)"}
+
+
+def run_reference(args, name, cfg):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    from oracle import oracle as O  # noqa: F401  (builds liboracle.so if missing)
-    steps = args.steps
-    for _ in range(args.warmup):
-        pass
-    rate, nu, secs = cpu_baseline(cfg, steps)
+    steps = args.steps or cfg["steps"]
+    if cfg["kind"] == "single":
+        steps = min(steps, 20)
+    else:
+        steps = min(steps, 10)
+    base = cpu_baseline(name, cfg, steps)
     line = {
-        "impl": "reference",
-        "metric": "narrow-band node-updates/s", "value": rate, "unit": "node-updates/s",
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * secs / max(steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "steps_timed": steps},
-        "cpu_baseline": {"value": rate, "unit": "node-updates/s", "cores": 1, "kind": "port",
-                         "sample": f"{steps} steps of the timed speed after the same setup"},
-        "e2e": {"value": rate, "unit": "node-updates/s", "h2d_bytes_per_step": 0,
+        "impl": "reference", "metric": "narrow-band node-updates/s", "value": base["value"],
+        "unit": "node-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "name": name},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "node-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_felt(args, cfg):
+# ---------------------------------------------------------------------------------------------
+# Device arm
+# ---------------------------------------------------------------------------------------------
+
+def roofline(fb, work, cfg, stream_steps):
+    units0 = work.work_units()
+    fb.profile_reset()
+    fb.profile_enable(True)
+    for i in range(stream_steps):
+        work.step(10_000 + i, last=(i == stream_steps - 1))
+    import torch
+    torch.cuda.synchronize()
+    fb.profile_enable(False)
+    prof = fb.profile_read()
+    units1 = work.work_units()
+    tot = sum(v[0] for v in prof.values())
+    ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
+    hbm, peak_kind = load_peaks()
+    out = {"bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_kind": peak_kind,
+           "kernel_ms_per_step": tot / stream_steps,
+           "top_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:10]]}
+    dom = next((k for k, _ in ranked if k in UNIT_BYTES), None)
+    if dom and any(units1[i] - units0[i] for i in range(4)):
+        ms, nl = prof[dom]
+        ui, per = UNIT_BYTES[dom]
+        units = units1[ui] - units0[ui]
+        bpl = per * units / nl
+        achieved = bpl / (ms / nl * 1e-3) / 1e9
+        out.update({"kernel": dom, "achieved": achieved, "frac": achieved / hbm,
+                    "traffic": None, "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
+                    "share_of_step_kernel_time": ms / tot})
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            try:
+                t = json.load(open(tf)).get(dom)
+                if t:
+                    out["traffic"] = t["bytes_per_unit"] * units / nl
+            except Exception:
+                pass
+    return out
+
+
+def run_felt(args, name, cfg):
     import torch
     import felt_b200 as fb
 
@@ -184,144 +438,71 @@ def run_felt(args, cfg):
     torch.cuda.set_device(local)
     pg = None
     if ws > 1:
+        import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    D = cfg["D"]
-    s = fb.Surface(cfg["size"], cfg["part"], cfg["L"])
-    p = fb.Polys(s)
-    s.seed((0,) * D)
-    for _ in range(cfg["expand"]):
-        s.update(c=-1.0)
-    stream = torch.cuda.ExternalStream(s.stream())
+    steps = args.steps or cfg["steps"]
+    work = SingleWork(fb, cfg) if cfg["kind"] == "single" else BatchWork(fb, cfg, name)
+    stream = torch.cuda.ExternalStream(work.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def step(i):
-        s.update(**cfg["speed"])
-        p.notify()
-        if cfg["march_every"] and (i + 1) % cfg["march_every"] == 0:
-            p.march()
-
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize()
     if pg:
         pg.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    nu0 = s.node_updates()
     l0 = fb.launch_count()
-    total_ms = 0.0
-    for i in range(args.steps):
-        flush.fill_(float(i))  # L2 flush (256 MB > 126 MB L2) between timed steps, untimed
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        step(i)
-        b.record(stream)
-        b.synchronize()
-        total_ms += a.elapsed_time(b)
-    torch.cuda.synchronize()
+    t_ms, wall_s, nu, d2h = time_steps(torch, work, stream, steps, args.warmup, flush)
     launches = fb.launch_count() - l0
-    nu = s.node_updates() - nu0
     clk = clocks.stop()
-    t_ms = total_ms
     if pg:
-        tt = torch.tensor([t_ms, float(nu)], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([t_ms, wall_s, float(nu)], dtype=torch.float64, device="cuda")
         mx = tt.clone()
-        pg.all_reduce(mx[:1], op=pg.ReduceOp.MAX)
-        pg.all_reduce(tt[1:], op=pg.ReduceOp.SUM)
-        t_ms = float(mx[0])
-        nu = float(tt[1])
+        pg.all_reduce(mx[:2], op=pg.ReduceOp.MAX)
+        pg.all_reduce(tt[2:], op=pg.ReduceOp.SUM)
+        t_ms, wall_s, nu = float(mx[0]), float(mx[1]), float(tt[2])
     value = nu / (t_ms / 1e3)
-
-    # ---- end to end through the C ABI with host buffers ----
     import ctypes as C
-    lib = fb.lib()
-    e2e_steps = max(3, min(args.steps, 20))
-    h2d = C.sizeof(fb.Speed)
-    d2h = 0
-    e2e_s = 0.0
-    e2e_nu = 0
-    for i in range(e2e_steps):
-        flush.fill_(float(i))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        n0 = s.node_updates()
-        sp = fb.make_speed(**cfg["speed"])
-        fb._chk(lib.fg_update_builtin(s._h, C.byref(sp)))
-        p.notify()
-        if cfg["march_every"] and (i + 1) % cfg["march_every"] == 0:
-            p.march()
-            for part in p.changes():
-                vtx, spx, _ = p.partition(part)
-                d2h += vtx.nbytes + spx.nbytes
-        n1 = s.node_updates()
-        d2h += 16
-        e2e_s += time.perf_counter() - t0
-        e2e_nu += n1 - n0
-    e2e = {"value": e2e_nu / e2e_s, "unit": "node-updates/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // e2e_steps}
+    e2e = {"value": nu / wall_s, "unit": "node-updates/s",
+           "h2d_bytes_per_step": C.sizeof(fb.Speed) * (cfg.get("n") or 1),
+           "d2h_bytes_per_step": d2h // steps}
 
-    # ---- per-kernel device times for the roofline (separate pass, profiling on) ----
+    extra = {}
     roof = None
     if rank == 0:
-        units0 = s.work_units()
-        fb.profile_reset()
-        fb.profile_enable(True)
-        nprof = max(cfg["march_every"] or 5, 10)
-        for i in range(nprof):
-            step(i)
-        torch.cuda.synchronize()
-        fb.profile_enable(False)
-        prof = fb.profile_read()
-        units1 = s.work_units()
-        tot = sum(v[0] for v in prof.values())
-        ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
-        hbm, peak_kind = load_peaks()
-        dom = next((k for k, _ in ranked if k in UNIT_BYTES), None)
-        if dom:
-            ms, nl = prof[dom]
-            ui, per = UNIT_BYTES[dom]
-            units = units1[ui] - units0[ui]
-            bytes_per_launch = per * units / nl
-            achieved = bytes_per_launch / (ms / nl * 1e-3) / 1e9
-            roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
-                    "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                    "traffic": None, "bytes_per_launch": bytes_per_launch,
-                    "avg_launch_us": 1e3 * ms / nl,
-                    "share_of_step_kernel_time": prof[dom][0] / tot if tot else None,
-                    "top_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:8]]}
-            tf = os.path.join(ROOT, "profiles", "traffic.json")
-            if os.path.exists(tf):
-                try:
-                    t = json.load(open(tf)).get(dom)
-                    if t:
-                        roof["traffic"] = t["bytes_per_unit"] * units / nl
-                except Exception:
-                    pass
-
+        roof = roofline(fb, work, cfg, max(cfg["march_every"] or 5, 5))
+        if cfg["kind"] == "batch" and not args.no_plain:
+            plain = PlainSubset(fb, cfg, name, cfg["plain_subset"])
+            ps = torch.cuda.ExternalStream(0)
+            p_steps = min(steps, 10)
+            t0 = time.perf_counter()
+            nu0 = plain.node_updates()
+            for i in range(p_steps):
+                plain.step(i, last=(i == p_steps - 1))
+            torch.cuda.synchronize()
+            p_rate = (plain.node_updates() - nu0) / (time.perf_counter() - t0)
+            del ps
+            extra["plain"] = {"value": p_rate, "unit": "node-updates/s",
+                              "surfaces": cfg["plain_subset"], "steps": p_steps,
+                              "how": "one Surface per launch sequence, surfaces one after "
+                                     "another, wall clock"}
+            extra["batched_over_plain"] = value / p_rate
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        rate, cnu, csecs = cpu_baseline(cfg, args.cpu_steps)
-        cpu = {"value": rate, "unit": "node-updates/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_steps} timed steps after the same seed+expansion setup "
-                         f"({cnu:.3g} node-updates in {csecs:.2f} s, single thread)"}
+        cpu = cpu_baseline(name, cfg, args.cpu_steps if cfg["kind"] == "single"
+                           else cfg["cpu_steps"])
 
     if rank == 0:
+        config = {"workload": cfg["workload"], "name": name, "parallelism": f"replicas{ws}",
+                  "l2": "flushed between timed steps (256 MB write)", "node_updates": nu}
+        config.update(extra)
         line = {
             "metric": "narrow-band node-updates/s", "value": value, "unit": "node-updates/s",
-            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "parallelism": f"replicas{ws}",
-                       "l2": "flushed between timed steps (256 MB write)",
-                       "node_updates": nu},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": launches,
+            "n_gpus": ws, "steps": steps, "warmup": args.warmup, "ms_per_step": t_ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config, "roofline": roof, "cpu_baseline": cpu,
+            "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -332,18 +513,19 @@ def run_felt(args, cfg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=0, help="timed steps (default per config)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="felt", choices=["felt", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
-        run_reference(args, cfg)
+        run_reference(args, args.config, cfg)
     else:
-        run_felt(args, cfg)
+        run_felt(args, args.config, cfg)
 
 
 if __name__ == "__main__":

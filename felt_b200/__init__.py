@@ -329,6 +329,18 @@ class Batch:
         _chk(lib().fg_batch_node_updates(self._h, C.byref(n)))
         return n.value
 
+    def work_units(self):
+        out = (C.c_ulonglong * 8)()
+        _chk(lib().fg_batch_work_units(self._h, out, C.c_size_t(8)))
+        return tuple(out[:4])
+
+    def stopped(self, i):
+        """True once surface i was stopped after an update whose convergence loop did not
+        terminate (the reference would loop forever there)."""
+        v = C.c_int()
+        _chk(lib().fg_batch_surface_stopped(self._h, C.c_size_t(i), C.byref(v)))
+        return bool(v.value)
+
     def stream(self):
         p = C.c_void_p()
         _chk(lib().fg_batch_stream(self._h, C.byref(p)))
@@ -392,3 +404,26 @@ class Polys:
         ns = C.c_size_t()
         _chk(lib().fg_polys_totals(self._h, C.byref(nv), C.byref(ns)))
         return nv.value, ns.value
+
+    def gather(self, parts):
+        """Vertices and simplices of several partitions in one call: (vtx, spx, counts)."""
+        D = self.surface.D
+        per = 2 * D if D == 3 else D
+        parts = list(parts)
+        arr = (C.c_uint32 * max(1, len(parts)))(*parts)
+        counts = np.zeros(2 * max(1, len(parts)), dtype=np.uint32)
+        nv = C.c_size_t()
+        ns = C.c_size_t()
+        _chk(lib().fg_polys_gather(self._h, arr, C.c_size_t(len(parts)), None, C.c_size_t(0),
+                                   None, C.c_size_t(0),
+                                   counts.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(nv),
+                                   C.byref(ns)))
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
+        spx = np.zeros(max(1, ns.value * D), dtype=np.uint32)
+        _chk(lib().fg_polys_gather(self._h, arr, C.c_size_t(len(parts)),
+                                   vtx.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(vtx.size),
+                                   spx.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_size_t(spx.size),
+                                   counts.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(nv),
+                                   C.byref(ns)))
+        return (vtx[: nv.value * per].reshape(nv.value, per),
+                spx[: ns.value * D].reshape(ns.value, D), counts[: 2 * len(parts)].reshape(-1, 2))

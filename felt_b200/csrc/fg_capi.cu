@@ -416,7 +416,18 @@ int fg_batch_create(int dims, int layers, const int* part, size_t n, const int* 
 		auto b = std::make_unique<fg_batch>();
 		FG_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
 		b->eng.reset(fg::make_engine(d, b->st));
+		b->eng->set_throw_on_freeze(false);
 		*out = b.release();
+	});
+}
+
+int fg_batch_surface_stopped(fg_batch* b, size_t surface, int* stopped)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(stopped, "stopped");
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index");
+		*stopped = b->eng->frozen((int)surface) ? 1 : 0;
 	});
 }
 
@@ -535,6 +546,18 @@ int fg_batch_node_updates(fg_batch* b, unsigned long long* n)
 	});
 }
 
+int fg_batch_work_units(fg_batch* b, unsigned long long* out, size_t n)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(out, "out");
+		unsigned long long tmp[fg::KS_N];
+		b->eng->sync();
+		FG_CUDA(cudaMemcpy(tmp, b->eng->dev().kstat, sizeof(tmp), cudaMemcpyDeviceToHost));
+		for (size_t i = 0; i < n && i < (size_t)fg::KS_N; i++) out[i] = tmp[i];
+	});
+}
+
 int fg_batch_stream(fg_batch* b, void** stream)
 {
 	return guard([&] {
@@ -605,6 +628,18 @@ int fg_profile_entry(size_t i, char* name, size_t name_cap, double* ms, long lon
 		}
 		if (ms) *ms = e.ms;
 		if (launches) *launches = e.launches;
+	});
+}
+
+int fg_polys_gather(fg_polys* p, const uint32_t* parts, size_t n, float* vtx, size_t vcap,
+                    uint32_t* spx, size_t scap, uint32_t* counts, size_t* nv, size_t* ns)
+{
+	return guard([&] {
+		need(p, "polys");
+		need(nv, "nv");
+		need(ns, "ns");
+		if (n && !parts) throw fg::Error(FG_ERR_ARG, "null parts");
+		p->impl->gather(parts, n, vtx, vcap, spx, scap, counts, nv, ns);
 	});
 }
 

@@ -190,6 +190,9 @@ public:
 		P.papg = dalloc<int>(2 * (size_t)NP, o);
 		P.papn = dalloc<int>(S, o);
 		P.woff = dalloc<int>(S + 1, o);
+		P.sfrozen = dalloc<int>(S, o);
+		FG_CUDA(cudaMemsetAsync(P.sfrozen, 0, S * sizeof(int), st_));
+		frozen_.assign(S, 0);
 		P.err = dalloc<int>(1, o);
 		P.changed = dalloc<int>(1, o);
 		P.kstat = dalloc<unsigned long long>(KS_N, o);
@@ -323,6 +326,7 @@ public:
 
 	void update_begin_global() override
 	{
+		check_not_frozen();
 		update_start();
 		// delta.track_children(isogrid) on freshly reset delta lists = a copy of the lists.
 		copy_plists();
@@ -374,11 +378,55 @@ public:
 			std::swap(cur, oth);
 			changed = read_changed();
 			iters++;
-			if (iters > 100000) throw Error(-14, "convergence loop did not terminate");
+			if (changed && iters % kMaxIterations == 0) freeze_oscillating(cur);
 		}
 		stats_.iterations = iters;
 		check_errors();
+		if (!newly_frozen_.empty() && throw_on_freeze_) {
+			newly_frozen_.clear();
+			throw Error(-14, "the convergence loop of the update did not terminate (layer "
+			                 "changes keep oscillating, typically where the band meets the grid "
+			                 "edge); the surface is stopped");
+		}
+		newly_frozen_.clear();
 	}
+
+	/// The reference loops `while (is_status_changed)` with no bound (Surface.hpp:752-760,
+	/// 420-428); where the band reaches the grid edge its layer changes can oscillate forever.
+	/// After kMaxIterations iterations the surfaces still changing are frozen: no kernel works
+	/// on them again, so the loop ends for the rest of the pool.
+	void freeze_oscillating(int cur)
+	{
+		std::vector<int> cnt((size_t)P_.S * NL);
+		FG_CUDA(cudaMemcpyAsync(cnt.data(), P_.apcnt[cur], cnt.size() * sizeof(int),
+		                        cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		for (int s = 0; s < P_.S; s++) {
+			int tot = 0;
+			for (int l = 0; l < NL; l++) tot += cnt[(size_t)s * NL + l];
+			if (tot && !frozen_[s]) {
+				frozen_[s] = 1;
+				newly_frozen_.push_back(s);
+			}
+		}
+		FG_CUDA(cudaMemcpyAsync(P_.sfrozen, frozen_.data(), frozen_.size() * sizeof(int),
+		                        cudaMemcpyHostToDevice, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+	}
+
+public:
+	bool frozen(int s) const override { return frozen_[s] != 0; }
+	void set_throw_on_freeze(bool on) override { throw_on_freeze_ = on; }
+
+private:
+	void check_not_frozen()
+	{
+		for (int s = 0; s < P_.S; s++)
+			if (!frozen_[s]) return;
+		throw Error(-15, "every surface of the pool is stopped after a non-terminating update");
+	}
+
+public:
 
 	/// update_start(); delta(pos, v)...; update_end() on surface 0 (Surface.hpp:393-459,
 	/// 404-430).
@@ -386,6 +434,7 @@ public:
 	{
 		const int n = (int)vals.size();
 		if (pos.size() != vals.size() * D) throw Error(-1, "delta positions/values mismatch");
+		check_not_frozen();
 		update_start();
 		ensure_local_staging(n);
 		if (n) {
@@ -407,6 +456,7 @@ public:
 			vlo[a] = lo[a];
 			vhi[a] = hi[a];
 		}
+		check_not_frozen();
 		// capacity: every zero-layer leaf of the surface
 		unsigned long long nz = 0;
 		for (uint32_t p : partition_list(0, 0, L)) nz += layer_list(0, p, L).size();
@@ -431,7 +481,7 @@ public:
 		count_band();
 		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
 		// over the affected lists (update_distance(plookup = affected, buffer))
-		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff););
+		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
 		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
 		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, aff, P_.dlcnt, B););
 		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.aplist[A], L, B););
@@ -687,7 +737,7 @@ private:
 
 	void scan(const int* cnt, int l, int mode)
 	{
-		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff););
+		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff, P_.sfrozen););
 	}
 
 	/// update_start (Surface.hpp:393-399): resets of the status and affected grids left by the
@@ -797,6 +847,10 @@ private:
 	int warp_grid_ = 0;
 	bool status_dirty_ = false;
 	bool buf_dirty_[2] = {false, false};
+	static constexpr int kMaxIterations = 64;
+	std::vector<int> frozen_;
+	std::vector<int> newly_frozen_;
+	bool throw_on_freeze_ = true;
 	StepStats stats_;
 };
 

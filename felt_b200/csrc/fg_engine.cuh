@@ -77,6 +77,12 @@ public:
 	virtual StepStats& stats() = 0;
 	/// Sum over all global updates so far of the band size at each update's start.
 	virtual unsigned long long node_updates() = 0;
+	/// True once surface s has been stopped after an update whose convergence loop did not
+	/// terminate; no kernel works on it afterwards.
+	virtual bool frozen(int s) const = 0;
+	/// Whether an update that stops a surface raises (single surfaces) or only records it
+	/// (batches, serving).
+	virtual void set_throw_on_freeze(bool on) = 0;
 	virtual const Dev& dev() const = 0;
 	virtual void sync() = 0;
 	virtual int part(int a) const = 0;

@@ -55,8 +55,10 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 // ---------------------------------------------------------------------------------------------
 // Entry offsets: woff[s] = sum of per-surface counts before s.
 // mode 0: cnt[s*NL + l]; mode 1: cnt[s*NL] + cnt[s*NL + NL-1]; mode 2: sum over layers.
+// Frozen surfaces (frozen[s] != 0) contribute no entries, so no kernel works on them.
 // ---------------------------------------------------------------------------------------------
-static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff)
+static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff,
+                                     const int* frozen)
 {
 	__shared__ int carry;
 	if (threadIdx.x == 0) {
@@ -67,7 +69,7 @@ static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, in
 	for (int base = 0; base < S; base += blockDim.x) {
 		const int s = base + threadIdx.x;
 		int v = 0;
-		if (s < S) {
+		if (s < S && !(frozen && frozen[s])) {
 			if (mode == 0)
 				v = cnt[s * NL + l];
 			else if (mode == 1)

@@ -249,7 +249,7 @@ __global__ void k_polys_notify(Dev P, PolysDev Q)
 {
 	constexpr int NL = 2 * L + 1;
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if (s >= P.S) return;
+	if (s >= P.S || P.sfrozen[s]) return;
 	const SurfGeom& g = P.geom[s];
 	int* lkp = Q.pend_lkp[Q.pend];
 	int* lst = Q.pend_list[Q.pend] + g.pbase;
@@ -507,6 +507,22 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 	}
 }
 
+/// Copies the geometry of the requested partitions (job: src vertex offset, vertex count, src
+/// simplex offset, simplex count, index) to consecutive destination ranges. Block per job.
+template <int D>
+__global__ void k_polys_gather(PolysDev Q, const int* job, const long long* dst, int n, float* sv,
+                               uint32_t* ss)
+{
+	constexpr int VF = D == 3 ? 2 * D : D;
+	for (int i = blockIdx.x; i < n; i += gridDim.x) {
+		const size_t vo = (size_t)job[5 * i] * VF, so = (size_t)job[5 * i + 2] * D;
+		const int nv = job[5 * i + 1] * VF, ns = job[5 * i + 3] * D;
+		const size_t vd = (size_t)dst[2 * i] * VF, sd = (size_t)dst[2 * i + 1] * D;
+		for (int k = threadIdx.x; k < nv; k += blockDim.x) sv[vd + k] = Q.vtx[vo + k];
+		for (int k = threadIdx.x; k < ns; k += blockDim.x) ss[sd + k] = Q.spx[so + k];
+	}
+}
+
 /// Moves the live geometry of every partition to the front of a fresh arena.
 template <int D>
 __global__ void k_polys_compact(Dev P, PolysDev Q, const int* noff, const int* nsoff, float* vtx2,
@@ -579,6 +595,7 @@ public:
 		cudaStreamSynchronize(eng_.stream());
 		free_arena();
 		for (void* p : owned_) cudaFree(p);
+		if (stage_) cudaFree(stage_);
 	}
 
 	void notify() override
@@ -599,7 +616,7 @@ public:
 	{
 		const Dev& P = eng_.dev();
 		cudaStream_t st = eng_.stream();
-		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_););
+		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_, P.sfrozen););
 		// Re-marching a partition recomputes it from the isogrid, so a march that ran out of
 		// arena space is simply repeated after the arena has grown.
 		for (int attempt = 0;; attempt++) {
@@ -795,11 +812,83 @@ public:
 		s_ = s;
 	}
 
+	void gather(const uint32_t* parts, size_t n, float* vtx, size_t vcap, uint32_t* spx,
+	            size_t scap, uint32_t* counts, size_t* nv, size_t* ns) override
+	{
+		int cc[3], co[3];
+		const int np = (int)eng_.partitions(s_, cc, co);
+		const int pb = pbase_of();
+		eng_.sync();
+		std::vector<int> gnv(np), gns(np), gvo(np), gso(np);
+		FG_CUDA(cudaMemcpy(gnv.data(), Q_.gnv + pb, np * sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(gns.data(), Q_.gns + pb, np * sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(gvo.data(), Q_.gvoff + pb, np * sizeof(int), cudaMemcpyDeviceToHost));
+		FG_CUDA(cudaMemcpy(gso.data(), Q_.gsoff + pb, np * sizeof(int), cudaMemcpyDeviceToHost));
+		// per requested partition: source offsets, counts and destination offsets
+		std::vector<int> job(5 * n);
+		long long tv = 0, ts = 0;
+		for (size_t i = 0; i < n; i++) {
+			if (parts[i] >= (uint32_t)np) throw Error(-1, "partition index out of range");
+			const int p = (int)parts[i];
+			job[5 * i + 0] = gvo[p];
+			job[5 * i + 1] = gnv[p];
+			job[5 * i + 2] = gso[p];
+			job[5 * i + 3] = gns[p];
+			job[5 * i + 4] = (int)i;
+			if (counts) {
+				counts[2 * i] = (uint32_t)gnv[p];
+				counts[2 * i + 1] = (uint32_t)gns[p];
+			}
+			tv += gnv[p];
+			ts += gns[p];
+		}
+		*nv = (size_t)tv;
+		*ns = (size_t)ts;
+		if (!n || (!vtx && !spx)) return;
+		if ((size_t)tv * VF > vcap || (size_t)ts * D > scap)
+			throw Error(-13, "gather buffers too small");
+		std::vector<long long> dst(2 * n);
+		long long av = 0, as = 0;
+		for (size_t i = 0; i < n; i++) {
+			dst[2 * i] = av;
+			dst[2 * i + 1] = as;
+			av += job[5 * i + 1];
+			as += job[5 * i + 3];
+		}
+		const size_t need = (size_t)tv * VF * sizeof(float) + (size_t)ts * D * sizeof(uint32_t) +
+		                    job.size() * sizeof(int) + dst.size() * sizeof(long long) + 64;
+		if (need > stage_cap_) {
+			if (stage_) cudaFree(stage_);
+			stage_ = nullptr;
+			stage_cap_ = std::max(need, (size_t)1 << 20);
+			FG_CUDA(cudaMalloc(&stage_, stage_cap_));
+		}
+		char* base = static_cast<char*>(stage_);
+		float* sv = reinterpret_cast<float*>(base);
+		uint32_t* ss = reinterpret_cast<uint32_t*>(base + (size_t)tv * VF * sizeof(float));
+		int* dj = reinterpret_cast<int*>(ss + (size_t)ts * D);
+		long long* dd = reinterpret_cast<long long*>(
+		    (reinterpret_cast<uintptr_t>(dj + job.size()) + 15) & ~(uintptr_t)15);
+		cudaStream_t st = eng_.stream();
+		FG_CUDA(cudaMemcpyAsync(dj, job.data(), job.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dd, dst.data(), dst.size() * sizeof(long long),
+		                        cudaMemcpyHostToDevice, st));
+		FG_RUN("k_polys_gather", st, k_polys_gather<D><<<grid(), 256, 0, st>>>(Q_, dj, dd, (int)n, sv, ss););
+		FG_CUDA(cudaGetLastError());
+		if (vtx && tv)
+			FG_CUDA(cudaMemcpyAsync(vtx, sv, (size_t)tv * VF * sizeof(float), cudaMemcpyDeviceToHost, st));
+		if (spx && ts)
+			FG_CUDA(cudaMemcpyAsync(spx, ss, (size_t)ts * D * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+		FG_CUDA(cudaStreamSynchronize(st));
+	}
+
 private:
 	EngineBase& eng_;
 	int s_;
 	PolysDev Q_;
 	int* woff_ = nullptr;
+	void* stage_ = nullptr;  // gather staging buffer
+	size_t stage_cap_ = 0;
 	size_t smem_ = 0;
 	std::vector<void*> owned_;
 };

@@ -23,6 +23,10 @@ public:
 	virtual void totals(size_t* nv, size_t* ns) = 0;
 	/// Surface of the pool that changes(), partition() and march_partition() refer to.
 	virtual void select(int s) = 0;
+	/// Geometry of several partitions of the selected surface, concatenated in the given order
+	/// (one gather kernel, two copies); counts receives (vertices, simplices) per partition.
+	virtual void gather(const uint32_t* parts, size_t n, float* vtx, size_t vcap, uint32_t* spx,
+	                    size_t scap, uint32_t* counts, size_t* nv, size_t* ns) = 0;
 };
 
 /// Polygonisation of surface s of an engine's pool.

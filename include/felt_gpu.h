@@ -178,6 +178,15 @@ FG_API int fg_polys_changes(fg_polys* p, uint32_t* out, size_t cap, size_t* n); 
  * D position floats then, in 3D, D normal floats; spx receives D uint32 indices per simplex. */
 FG_API int fg_polys_partition(fg_polys* p, size_t part, float* vtx, size_t vtx_cap, uint32_t* spx,
                        size_t spx_cap, size_t* nv, size_t* ns, int* active);
+/* The geometry of several partitions in one call (what a viewer reads after a march, e.g. the
+ * partitions of fg_polys_changes): vertices and simplices of parts[0..n) concatenated in that
+ * order, counts[2*i] / counts[2*i+1] the vertex / simplex count of parts[i]. Simplex indices
+ * stay local to their partition, as in children().get(p).spxs(). With vtx and spx NULL only the
+ * counts and totals are returned. */
+FG_API int fg_polys_gather(fg_polys* p, const uint32_t* parts, size_t n, float* vtx,
+                           size_t vtx_cap, uint32_t* spx, size_t spx_cap, uint32_t* counts,
+                           size_t* nv, size_t* ns);
+
 /* Totals over all partitions. */
 FG_API int fg_polys_totals(fg_polys* p, size_t* vertices, size_t* simplices);
 
@@ -207,6 +216,13 @@ FG_API int fg_batch_polys_changes(fg_batch* b, size_t surface, uint32_t* out, si
                                   size_t* n);
 FG_API int fg_batch_polys_totals(fg_batch* b, size_t* vertices, size_t* simplices);
 FG_API int fg_batch_node_updates(fg_batch* b, unsigned long long* n);
+/* Whether a surface has been stopped. The reference's convergence loop (Surface.hpp:752-760)
+ * has no bound and, where the band meets the grid edge, its layer changes can oscillate
+ * forever; after 64 iterations the surfaces still changing are stopped (left as they are, never
+ * worked on again) so the rest of the batch completes. A single fg_surface reports the same
+ * event as FG_ERR_TIMEOUT from the update, and FG_ERR_STATE from later updates. */
+FG_API int fg_batch_surface_stopped(fg_batch* b, size_t surface, int* stopped);
+FG_API int fg_batch_work_units(fg_batch* b, unsigned long long* out, size_t n);
 FG_API int fg_batch_stream(fg_batch* b, void** stream);
 
 /* ---- instrumentation (no counterpart in the reference; Surface.hpp has no timers) ----

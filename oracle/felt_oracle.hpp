@@ -665,6 +665,7 @@ public:
 		bool changed = update_distance(*pl, *pb);
 		flush_status_change();
 		expand_narrow_band();
+		int iters = 1;
 		while (changed) {
 			pl->reset(iso, false);
 			std::swap(pl, pb);
@@ -672,7 +673,17 @@ public:
 			changed = update_distance(*pl, *pb);
 			flush_status_change();
 			expand_narrow_band();
+			if (changed && ++iters % kMaxIterations == 0) throw_oscillation();
 		}
+	}
+
+	/// The reference's convergence loops (Surface.hpp:420-428, 752-760) are unbounded; where
+	/// the band meets the grid edge layer changes can oscillate forever. Both this oracle and
+	/// the device engine stop after kMaxIterations iterations (this one by raising).
+	static constexpr int kMaxIterations = 64;
+	[[noreturn]] static void throw_oscillation()
+	{
+		throw Error(-14, "convergence loop did not terminate (oscillating layer changes)");
 	}
 
 	/// update_end_global (Surface.hpp:739-762).
@@ -685,6 +696,7 @@ public:
 		if (changed) {
 			Affected* pl = &affb;
 			Affected* pb = &aff;
+			int iters = 1;
 			while (changed) {
 				status.reset(iso, true);
 				changed = update_distance(*pl, *pb);
@@ -692,6 +704,7 @@ public:
 				expand_narrow_band();
 				pl->reset(iso, false);
 				std::swap(pl, pb);
+				if (changed && ++iters % kMaxIterations == 0) throw_oscillation();
 			}
 		}
 	}

@@ -56,6 +56,47 @@ def test_batch_2d_uneven_sizes_and_speeds():
     _run_batch(2, 2, (16, 16), sizes, centres, steps, march_every=1)
 
 
+def test_oscillating_surface_stops_at_the_same_step():
+    """Anti-diffusive curvature speed drives this surface into the grid edge, where the
+    reference's unbounded convergence loop would cycle forever; the device engine and the
+    oracle both stop it after the same number of iterations in the same update, and in a
+    batch only that surface stops."""
+    import felt_b200 as fb
+    size, centre, c = (48, 48, 48), (-19, 3, 18), -0.5259483650318802
+    g = fb.Surface(size, (8, 8, 8), 2)
+    o = O.Surface(size, (8, 8, 8), 2)
+    g.seed(centre)
+    o.seed(centre)
+    failed_at = None
+    for step in range(70):
+        try:
+            o.update(a=-0.3, c=c)
+        except O.OracleError as e:
+            assert e.code == -14
+            failed_at = step
+            with pytest.raises(fb.FeltError) as ei:
+                g.update(a=-0.3, c=c)
+            assert ei.value.code == -14
+            break
+        g.update(a=-0.3, c=c)
+        assert first_difference(g.dump(), o.dump()) is None, f"step {step}"
+    assert failed_at is not None
+    with pytest.raises(fb.FeltError) as ei:
+        g.update(a=-0.3, c=c)
+    assert ei.value.code == -15
+    # in a batch the other surface carries on, identical to its own oracle run
+    b = fb.Batch([size, (32, 32, 32)], (8, 8, 8), 2)
+    b.seed([centre, (0, 0, 0)])
+    o2 = O.Surface((32, 32, 32), (8, 8, 8), 2)
+    o2.seed((0, 0, 0))
+    for step in range(failed_at + 3):
+        b.update([dict(a=-0.3, c=c), dict(a=-0.3, c=-0.2)])
+        o2.update(a=-0.3, c=-0.2)
+        assert b.stopped(0) == (step >= failed_at)
+        assert not b.stopped(1)
+        assert first_difference(b.dump(1), o2.dump()) is None, f"batch step {step}"
+
+
 def test_batch_3d_curvature_mixed_contraction():
     rng = random.Random(11)
     sizes = [(32, 32, 32), (48, 48, 48), (24, 32, 40), (32, 32, 32)]
