@@ -17,9 +17,10 @@ Arms:
   --impl reference  the reference algorithm's CPU implementation (the oracle port, compiled
                     from oracle/), on the same workload and metric, bounded sample.
 
-Prints ONE JSON line on rank 0. Multi-GPU (torchrun): every rank advances its own independent
-replica of the workload (a single surface does not shard), value = all ranks' node-updates /
-the slowest rank's time.
+Prints ONE JSON line on rank 0. Multi-GPU (torchrun): a single surface does not shard, so for
+c1/c2 every rank advances its own replica; for the batched configs every rank advances its own
+shard of independent surfaces (same distribution, rank-seeded). No collective touches the data
+path; value = all ranks' node-updates / the slowest rank's device time.
 """
 from __future__ import annotations
 
@@ -68,10 +69,12 @@ UNIT_BYTES = {"k_dist1": (0, 10), "k_dist2": (0, 10), "k_delta_builtin": (1, 10)
               "k_polys_march": (3, 6)}
 
 
-def batch_surfaces(name, cfg):
-    """Seeded synthetic surfaces of a batched config: sizes, seed centres, speeds."""
+def batch_surfaces(name, cfg, shard=0):
+    """Seeded synthetic surfaces of a batched config: sizes, seed centres, speeds. Under torchrun
+    each rank advances its own shard of independent surfaces (shard = rank; shard 0 is the
+    single-GPU workload)."""
     import numpy as np
-    rng = np.random.default_rng(0x5EED0000 + int(name[1:]))
+    rng = np.random.default_rng(0x5EED0000 + int(name[1:]) + (shard << 16))
     L, D = cfg["L"], cfg["D"]
     sizes, centres, speeds = [], [], []
     for _ in range(cfg["n"]):
@@ -157,6 +160,16 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def combine_ranks(dist, t_ms, wall_s, node_updates, device):
+    """Job totals over ranks: the slowest rank's device and wall time, all ranks' node updates."""
+    import torch
+    mx = torch.tensor([t_ms, wall_s], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(node_updates)], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(mx[1]), float(sm[0])
+
+
 # ---------------------------------------------------------------------------------------------
 # Device workloads
 # ---------------------------------------------------------------------------------------------
@@ -164,9 +177,9 @@ def dist_env():
 class SingleWork:
     """One Surface (+ Polys) through the C ABI."""
 
-    def __init__(self, fb, cfg):
+    def __init__(self, fb, cfg, brick_capacity=0):
         self.fb, self.cfg = fb, cfg
-        self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"])
+        self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=brick_capacity)
         self.p = fb.Polys(self.s)
         self.s.seed((0,) * cfg["D"])
         for _ in range(cfg["expand"]):
@@ -200,9 +213,9 @@ class SingleWork:
 class BatchWork:
     """All surfaces of a batched config in one batch."""
 
-    def __init__(self, fb, cfg, name):
+    def __init__(self, fb, cfg, name, shard=0):
         self.fb, self.cfg = fb, cfg
-        sizes, centres, self.speeds = batch_surfaces(name, cfg)
+        sizes, centres, self.speeds = batch_surfaces(name, cfg, shard)
         self.b = fb.Batch(sizes, cfg["part"], cfg["L"])
         self.b.seed(centres)
         self.surface0 = None
@@ -444,7 +457,8 @@ def run_felt(args, name, cfg):
         pg = dist
 
     steps = args.steps or cfg["steps"]
-    work = SingleWork(fb, cfg) if cfg["kind"] == "single" else BatchWork(fb, cfg, name)
+    work = (SingleWork(fb, cfg, args.brick_capacity) if cfg["kind"] == "single"
+            else BatchWork(fb, cfg, name, shard=rank))
     stream = torch.cuda.ExternalStream(work.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     if pg:
@@ -453,15 +467,12 @@ def run_felt(args, name, cfg):
     clocks.start()
     time.sleep(0.3)
     l0 = fb.launch_count()
+    print(f"launches before the timed region: {l0}", file=sys.stderr, flush=True)
     t_ms, wall_s, nu, d2h = time_steps(torch, work, stream, steps, args.warmup, flush)
     launches = fb.launch_count() - l0
     clk = clocks.stop()
     if pg:
-        tt = torch.tensor([t_ms, wall_s, float(nu)], dtype=torch.float64, device="cuda")
-        mx = tt.clone()
-        pg.all_reduce(mx[:2], op=pg.ReduceOp.MAX)
-        pg.all_reduce(tt[2:], op=pg.ReduceOp.SUM)
-        t_ms, wall_s, nu = float(mx[0]), float(mx[1]), float(tt[2])
+        t_ms, wall_s, nu = combine_ranks(pg, t_ms, wall_s, nu, "cuda")
     value = nu / (t_ms / 1e3)
     import ctypes as C
     e2e = {"value": nu / wall_s, "unit": "node-updates/s",
@@ -494,7 +505,9 @@ def run_felt(args, name, cfg):
                            else cfg["cpu_steps"])
 
     if rank == 0:
-        config = {"workload": cfg["workload"], "name": name, "parallelism": f"replicas{ws}",
+        par = (f"replicas{ws}" if cfg["kind"] == "single"
+               else f"surface shards x{ws} (independent surfaces per rank)")
+        config = {"workload": cfg["workload"], "name": name, "parallelism": par,
                   "l2": "flushed between timed steps (256 MB write)", "node_updates": nu}
         config.update(extra)
         line = {
@@ -520,6 +533,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--brick-capacity", type=int, default=0,
+                    help="brick pool capacity of single-surface configs (0 = automatic)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":

@@ -314,7 +314,6 @@ public:
 		update_begin_global();
 		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
-		scan(P_.pcnt, L, 0);
 		bool any_curv = false;
 		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
 		if (any_curv && smem_halo_)
@@ -331,6 +330,8 @@ public:
 		// delta.track_children(isogrid) on freshly reset delta lists = a copy of the lists.
 		copy_plists();
 		count_band();
+		// entry offsets over the zero-layer partitions, for the delta kernel that follows
+		scan(P_.pcnt, L, 0);
 	}
 
 	void update_finish_global() override

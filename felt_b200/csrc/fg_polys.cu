@@ -5,9 +5,11 @@
 // vertices in first-encounter order through a per-node edge cache. Here one block marches one
 // pending partition: (1) classify every leaf's cell (corner mask) and claim each cut edge's
 // cache slot with the smallest (cell, edge) sequence number; (2) a block scan over the cells
-// numbers the first occurrences, which is exactly the reference's vertex order; (3) the first
-// occurrences compute their vertex (interpolated position and, in 3D, the normalised gradient
-// of the interpolated field) and every cell emits its simplices from the ordering table.
+// numbers the first occurrences, which is exactly the reference's vertex order; (3) every cell
+// emits its simplices from the ordering table, and every first occurrence leaves a descriptor in
+// its vertex slot. A second, flat kernel then computes all vertices of the march (interpolated
+// position and, in 3D, the normalised gradient of the interpolated field), one thread each, so
+// the long gradient stencils do not hold a partition's block at its barriers.
 #include <cstring>
 
 #include "fg_kernels.cuh"
@@ -35,6 +37,7 @@ struct PolysDev {
 	int pend;           // which of the two lists is pending
 	int* err;
 	int* ovf;           // set when a march ran out of arena space
+	unsigned long long* vstart;  // [1] vertex arena position when the current march began
 };
 
 namespace {
@@ -96,8 +99,8 @@ __device__ __forceinline__ bool inside_f(const SurfGeom& g, const float* p)
 }
 
 /// interp (NumericMixin.hpp:403-481): corners in bit order, reduced along axis 0 first.
-template <int D, int L>
-__device__ float interp(const Dev& P, const SurfGeom& g, const float* p)
+template <int D, class Get>
+__device__ float interp(const Get& get, const float* p)
 {
 	Vec<D> fl;
 	float pc[D];
@@ -113,7 +116,7 @@ __device__ float interp(const Dev& P, const SurfGeom& g, const float* p)
 		Vec<D> q = fl;
 #pragma unroll
 		for (int a = 0; a < D; a++) q[a] += (i >> a) & 1;
-		v[i] = get_phi<D, L>(P, g, q);
+		v[i] = get(q);
 	}
 	int n = 1 << D;
 #pragma unroll
@@ -127,10 +130,10 @@ __device__ float interp(const Dev& P, const SurfGeom& g, const float* p)
 }
 
 /// grad (NumericMixin.hpp:188-231) at an integer node.
-template <int D, int L>
-__device__ void grad_i(const Dev& P, const SurfGeom& g, const Vec<D>& p, float* out)
+template <int D, class Get>
+__device__ void grad_i(const Get& get, const SurfGeom& g, const Vec<D>& p, float* out)
 {
-	const float centre = get_phi<D, L>(P, g, p);
+	const float centre = get(p);
 	Vec<D> t = p;
 #pragma unroll
 	for (int a = 0; a < D; a++) {
@@ -138,12 +141,12 @@ __device__ void grad_i(const Dev& P, const SurfGeom& g, const Vec<D>& p, float* 
 		int order = 0;
 		t[a] -= 1;
 		if (in_grid<D>(g, t)) {
-			back = get_phi<D, L>(P, g, t);
+			back = get(t);
 			order++;
 		}
 		t[a] += 2;
 		if (in_grid<D>(g, t)) {
-			fwd = get_phi<D, L>(P, g, t);
+			fwd = get(t);
 			order++;
 		}
 		t[a] -= 1;
@@ -152,10 +155,10 @@ __device__ void grad_i(const Dev& P, const SurfGeom& g, const Vec<D>& p, float* 
 }
 
 /// grad at a real position: the probe coordinate steps -1, +2, -1 in FP32.
-template <int D, int L>
-__device__ void grad_f(const Dev& P, const SurfGeom& g, const float* p, float* out)
+template <int D, int L, class Get>
+__device__ void grad_f(const Get& get, const SurfGeom& g, const float* p, float* out)
 {
-	const float centre = interp<D, L>(P, g, p);
+	const float centre = interp<D>(get, p);
 	float t[D];
 #pragma unroll
 	for (int a = 0; a < D; a++) t[a] = p[a];
@@ -165,12 +168,12 @@ __device__ void grad_f(const Dev& P, const SurfGeom& g, const float* p, float* o
 		int order = 0;
 		t[a] = __fsub_rn(t[a], 1.0f);
 		if (inside_f<D, L>(g, t)) {
-			back = interp<D, L>(P, g, t);
+			back = interp<D>(get, t);
 			order++;
 		}
 		t[a] = __fadd_rn(t[a], 2.0f);
 		if (inside_f<D, L>(g, t)) {
-			fwd = interp<D, L>(P, g, t);
+			fwd = interp<D>(get, t);
 			order++;
 		}
 		t[a] = __fsub_rn(t[a], 1.0f);
@@ -192,14 +195,14 @@ __device__ void normalize3(float* v)
 }
 
 /// Poly::Single::idx vertex construction (Poly.hpp:296-346) for the edge at pa along axis.
-template <int D, int L>
-__device__ void make_vertex(const Dev& P, const SurfGeom& g, const Vec<D>& pa, int axis,
+template <int D, int L, class Get>
+__device__ void make_vertex(const Get& get, const SurfGeom& g, const Vec<D>& pa, int axis,
                             float* out)
 {
 	Vec<D> pb = pa;
 	pb[axis] += 1;
-	const float va = get_phi<D, L>(P, g, pa);
-	const float vb = get_phi<D, L>(P, g, pb);
+	const float va = get(pa);
+	const float vb = get(pb);
 	float pos[D];
 	bool at_node = false;
 	Vec<D> node;
@@ -230,9 +233,9 @@ __device__ void make_vertex(const Dev& P, const SurfGeom& g, const Vec<D>& pa, i
 	if (D == 3) {
 		float n[D];
 		if (at_node)
-			grad_i<D, L>(P, g, node, n);
+			grad_i<D>(get, g, node, n);
 		else
-			grad_f<D, L>(P, g, pos, n);
+			grad_f<D, L>(get, g, pos, n);
 #pragma unroll
 		for (int a = 0; a < D; a++) n[a] = __fdiv_rn(n[a], 1.0f);
 		normalize3(n);
@@ -241,56 +244,98 @@ __device__ void make_vertex(const Dev& P, const SurfGeom& g, const Vec<D>& pa, i
 	}
 }
 
+/// Index, in a marched partition's staged box (origin = partition origin, extent bext,
+/// row-major), of a leaf's cell origin: the leaf's node, moved one node along the last axis in
+/// 3D (SpxGridPosOffset, PolyMixin.hpp:409), since the 3D cube's corners and edges step -z
+/// from it (PolyMixin.hpp:377-406). The last axis has stride 1 in the box.
+template <int D>
+__device__ __forceinline__ int box_index(const Dev& P, const int* bext, int leaf)
+{
+	int bi = 0;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		const int q = leaf / P.lstr[a];
+		leaf -= q * P.lstr[a];
+		bi = bi * bext[a] + q;
+	}
+	return D == 3 ? bi + 1 : bi;
+}
+
 }  // namespace
 
-/// Polys::notify (Polys.hpp:92-133), one thread per surface.
+/// Polys::notify (Polys.hpp:92-133), one warp per surface. The reference walks the delta lists
+/// of layers 0 and 2L tracking (appending) or untracking (swap-with-last removing) each
+/// partition in the pending list, then tracks the poly-active partitions of the outermost
+/// status lists. Whether each entry is a real append or removal depends only on the state
+/// before its chunk (a partition appears once per list), so each 32-entry chunk appends its
+/// runs in parallel by ballot and replays the (rare) removals one at a time in list order.
 template <int L>
 __global__ void k_polys_notify(Dev P, PolysDev Q)
 {
 	constexpr int NL = 2 * L + 1;
-	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	const int lane = lane_id();
+	const unsigned lt = (1u << lane) - 1u;
+	const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (s >= P.S || P.sfrozen[s]) return;
 	const SurfGeom& g = P.geom[s];
 	int* lkp = Q.pend_lkp[Q.pend];
 	int* lst = Q.pend_list[Q.pend] + g.pbase;
 	int cnt = Q.pend_cnt[Q.pend][s];
-	for (int li = 0; li <= NL; li += NL - 1) {
-		const int n = P.dpcnt[s * NL + li];
-		const int* dl = P.dplist + (size_t)li * P.NP + g.pbase;
-		for (int i = 0; i < n; i++) {
-			const int lp = dl[i];
-			const int gp = g.pbase + lp;
-			bool act = Q.pact[gp] != 0;
-			for (int lj = 0; !act && lj <= NL; lj += NL - 1) act = P.ppos[gp * NL + lj] >= 0;
-			if (act) {
-				if (lkp[gp] < 0) {
-					lkp[gp] = cnt;
-					lst[cnt++] = lp;
+	for (int pass = 0; pass < 4; pass++) {
+		const bool status = pass >= 2;
+		const int li = (pass & 1) ? NL - 1 : 0;
+		const int n = status ? P.spcnt[s * NL + li] : P.dpcnt[s * NL + li];
+		const int* src = (status ? P.splist : P.dplist) + (size_t)li * P.NP + g.pbase;
+		for (int base = 0; base < n; base += 32) {
+			const int i = base + lane;
+			int lp = 0, gp = 0;
+			bool app = false, rem = false;
+			if (i < n) {
+				lp = src[i];
+				gp = g.pbase + lp;
+				const bool in = lkp[gp] >= 0;
+				if (status) {
+					app = Q.pact[gp] && !in;
+				} else {
+					bool act = Q.pact[gp] != 0;
+					for (int lj = 0; !act && lj <= NL; lj += NL - 1)
+						act = P.ppos[gp * NL + lj] >= 0;
+					app = act && !in;
+					rem = !act && in;
 				}
-			} else if (lkp[gp] >= 0) {
-				const int at = lkp[gp], last = cnt - 1;
-				if (at < last) {
-					lst[at] = lst[last];
-					lkp[g.pbase + lst[last]] = at;
+			}
+			unsigned ma = __ballot_sync(FULL, app), mr = __ballot_sync(FULL, rem);
+			while (ma | mr) {
+				const int r = mr ? __ffs(mr) - 1 : 32;
+				const unsigned seg = ma & (r == 32 ? FULL : ((1u << r) - 1u));
+				if (seg) {
+					if ((seg >> lane) & 1u) {
+						const int pos = cnt + __popc(seg & lt);
+						lst[pos] = lp;
+						lkp[gp] = pos;
+					}
+					cnt += __popc(seg);
+					ma &= ~seg;
+					__syncwarp();
 				}
-				lkp[gp] = -1;
-				cnt = last;
+				if (r < 32) {
+					if (lane == r) {
+						const int at = lkp[gp], last = cnt - 1;
+						if (at < last) {
+							const int mv = lst[last];
+							lst[at] = mv;
+							lkp[g.pbase + mv] = at;
+						}
+						lkp[gp] = -1;
+					}
+					cnt -= 1;
+					mr &= ~(1u << r);
+					__syncwarp();
+				}
 			}
 		}
 	}
-	for (int li = 0; li <= NL; li += NL - 1) {
-		const int n = P.spcnt[s * NL + li];
-		const int* sl = P.splist + (size_t)li * P.NP + g.pbase;
-		for (int i = 0; i < n; i++) {
-			const int lp = sl[i];
-			const int gp = g.pbase + lp;
-			if (Q.pact[gp] && lkp[gp] < 0) {
-				lkp[gp] = cnt;
-				lst[cnt++] = lp;
-			}
-		}
-	}
-	Q.pend_cnt[Q.pend][s] = cnt;
+	if (lane == 0) Q.pend_cnt[Q.pend][s] = cnt;
 }
 
 /// Polys::invalidate (Polys.hpp:171-191), one thread per surface.
@@ -334,7 +379,14 @@ __global__ void k_polys_reset_list(Dev P, PolysDev Q, int which)
 }
 
 /// Polys::march body (Polys.hpp:138-161) for every pending partition of every surface (woff
-/// over the pending counts), or for a single partition when single >= 0.
+/// over the pending counts), or for a single partition when single >= 0: classification of the
+/// partition's cells, the first-occurrence vertex numbering of Poly::Single::idx and the simplex
+/// index triplets. Vertex positions and normals are left to k_polys_vertices: each new vertex's
+/// arena slot receives an 8-byte descriptor (partition, cell leaf, edge) instead.
+///
+/// The partition's values plus the one-node halo its cell corners reach (above the partition on
+/// every axis; in 3D the cells' -z corners stay inside) are staged in shared memory, so
+/// classification reads no global memory per corner.
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const int* woff,
                                                        int single)
@@ -342,13 +394,14 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 	constexpr int NL = 2 * L + 1;
 	constexpr int VF = D == 3 ? 2 * D : D;
 	extern __shared__ int smem[];
-	int csz2[3] = {1, 1, 1}, cvol = 1;
+	int bext[3] = {1, 1, 1}, bvol = 1;
 	for (int a = 0; a < D; a++) {
-		csz2[a] = P.csz[a] + 2;
-		cvol *= csz2[a];
+		bext[a] = P.csz[a] + 1;
+		bvol *= bext[a];
 	}
-	int* first = smem;                                          // [cvol * D]
-	uint16_t* cmask = (uint16_t*)(first + cvol * D);            // [BV]
+	int* first = smem;                                          // [bvol * D] edge slots
+	float* box = (float*)(first + bvol * D);                    // [bvol] staged phi
+	uint16_t* cmask = (uint16_t*)(box + bvol);                  // [BV]
 	uint16_t* cnew = cmask + P.BV;                              // [BV]
 	uint16_t* cleaf = cnew + P.BV;                              // [BV]
 	__shared__ int lstart[NL + 1];
@@ -382,26 +435,41 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			}
 			lstart[NL] = c;
 		}
-		for (int i = threadIdx.x; i < cvol * D; i += blockDim.x) first[i] = 0x7fffffff;
+		Vec<D> bo;  // world position of box index 0
+		for (int a = 0; a < D; a++) bo[a] = P.porig[gp * 3 + a];
+		const float* brick = P.phi + (size_t)sl * P.BV;
+		for (int i = threadIdx.x; i < bvol; i += blockDim.x) {
+			first[i * D] = 0x7fffffff;
+			for (int a = 1; a < D; a++) first[i * D + a] = 0x7fffffff;
+			int r = i, leaf = 0;
+			bool own = true;
+			Vec<D> p;
+			for (int a = D - 1; a >= 0; a--) {
+				const int c = r % bext[a];
+				r /= bext[a];
+				p[a] = bo[a] + c;
+				const int lc = p[a] - P.porig[gp * 3 + a];
+				own = own && lc < P.csz[a] && p[a] < g.hi[a];
+				leaf += lc * P.lstr[a];
+			}
+			box[i] = own ? brick[leaf] : get_phi<D, L>(P, g, p);
+		}
 		__syncthreads();
 		const int n = lstart[NL];
 		if (threadIdx.x == 0) atomicAdd(&P.kstat[KS_MARCH], (unsigned long long)n);
 		const int per = (n + blockDim.x - 1) / blockDim.x;
 		const int j0 = threadIdx.x * per, j1 = min(n, j0 + per);
-		Vec<D> orig;
-		for (int a = 0; a < D; a++) orig[a] = P.porig[gp * 3 + a];
-		// 1. classify cells and claim edge cache slots
+		// 1. classify cells and claim edge slots: the lowest (cell, edge) claims a slot
 		for (int j = j0; j < j1; j++) {
 			int l = 0;
 			while (j >= lstart[l + 1]) l++;
 			const int leaf = P.lst[((size_t)sl * NL + l) * P.BV + (j - lstart[l])];
-			Vec<D> pc = leaf_pos<D>(P, gp, leaf);
-			if (D == 3) pc[D - 1] += 1;  // SpxGridPosOffset (PolyMixin.hpp:409)
+			const int bi = box_index<D>(P, bext, leaf);  // the cell's lowest corner
 			unsigned mask = 0;
 			for (int i = 0; i < (1 << D); i++) {
-				Vec<D> q;
-				for (int a = 0; a < D; a++) q[a] = pc[a] + mc_corner<D>(i, a);
-				mask |= (get_phi<D, L>(P, g, q) > 0.0f ? 1u : 0u) << i;
+				int o = 0;
+				for (int a = 0; a < D; a++) o = o * bext[a] + mc_corner<D>(i, a);
+				mask |= (box[bi + o] > 0.0f ? 1u : 0u) << i;
 			}
 			cmask[j] = (uint16_t)mask;
 			cleaf[j] = (uint16_t)leaf;
@@ -409,10 +477,9 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			const unsigned em = mc_edge_mask<D>(mask);
 			for (int ed = 0; ed < mc_edges<D>(); ed++) {
 				if (!((em >> ed) & 1u)) continue;
-				int ci = 0;
-				for (int a = 0; a < D; a++)
-					ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
-				atomicMin(&first[ci * D + mc_edge_axis<D>(ed)], j * 16 + ed);
+				int o = 0;
+				for (int a = 0; a < D; a++) o = o * bext[a] + mc_edge_off<D>(ed, a);
+				atomicMin(&first[(bi + o) * D + mc_edge_axis<D>(ed)], j * 16 + ed);
 			}
 		}
 		__syncthreads();
@@ -422,15 +489,13 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			const unsigned mask = cmask[j];
 			unsigned nm = 0;
 			if (mc_order<D>(mask, 0) != -1) {
-				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
-				if (D == 3) pc[D - 1] += 1;
+				const int bi = box_index<D>(P, bext, cleaf[j]);
 				const unsigned em = mc_edge_mask<D>(mask);
 				for (int ed = 0; ed < mc_edges<D>(); ed++) {
 					if (!((em >> ed) & 1u)) continue;
-					int ci = 0;
-					for (int a = 0; a < D; a++)
-						ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
-					if (first[ci * D + mc_edge_axis<D>(ed)] == j * 16 + ed) nm |= 1u << ed;
+					int o = 0;
+					for (int a = 0; a < D; a++) o = o * bext[a] + mc_edge_off<D>(ed, a);
+					if (first[(bi + o) * D + mc_edge_axis<D>(ed)] == j * 16 + ed) nm |= 1u << ed;
 				}
 				my_s += mc_nspx<D>(mask);
 			}
@@ -452,26 +517,20 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 		}
 		__syncthreads();
 		if (ok) {
-			// 3a. vertices, numbered in first-occurrence order
+			// 3a. vertex descriptors, numbered in first-occurrence order
 			int vi = bv0;
 			for (int j = j0; j < j1; j++) {
 				const unsigned nm = cnew[j];
 				if (!nm) continue;
-				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
-				if (D == 3) pc[D - 1] += 1;
+				const int bi = box_index<D>(P, bext, cleaf[j]);
 				for (int ed = 0; ed < mc_edges<D>(); ed++) {
 					if (!((nm >> ed) & 1u)) continue;
-					Vec<D> pa;
-					int ci = 0;
-					for (int a = 0; a < D; a++) {
-						pa[a] = pc[a] + mc_edge_off<D>(ed, a);
-						ci = ci * csz2[a] + (pa[a] - orig[a] + 1);
-					}
-					float out[VF];
-					make_vertex<D, L>(P, g, pa, mc_edge_axis<D>(ed), out);
-					float* dst = Q.vtx + ((size_t)vb + vi) * VF;
-					for (int k = 0; k < VF; k++) dst[k] = out[k];
-					first[ci * D + mc_edge_axis<D>(ed)] = vi;
+					int o = 0;
+					for (int a = 0; a < D; a++) o = o * bext[a] + mc_edge_off<D>(ed, a);
+					*(unsigned long long*)(Q.vtx + ((size_t)vb + vi) * VF) =
+					    ((unsigned long long)gp << 21) | ((unsigned long long)cleaf[j] << 4) |
+					    (unsigned long long)ed;
+					first[(bi + o) * D + mc_edge_axis<D>(ed)] = vi;
 					vi++;
 				}
 			}
@@ -481,16 +540,14 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			for (int j = j0; j < j1; j++) {
 				const unsigned mask = cmask[j];
 				if (mc_order<D>(mask, 0) == -1) continue;
-				Vec<D> pc = leaf_pos<D>(P, gp, cleaf[j]);
-				if (D == 3) pc[D - 1] += 1;
+				const int bi = box_index<D>(P, bext, cleaf[j]);
 				for (int o = 0; mc_order<D>(mask, o) != -1; o += D) {
 					uint32_t* dst = Q.spx + ((size_t)sb + si) * D;
 					for (int k = 0; k < D; k++) {
 						const int ed = mc_order<D>(mask, o + k);
-						int ci = 0;
-						for (int a = 0; a < D; a++)
-							ci = ci * csz2[a] + (pc[a] + mc_edge_off<D>(ed, a) - orig[a] + 1);
-						dst[k] = (uint32_t)first[ci * D + mc_edge_axis<D>(ed)];
+						int eo = 0;
+						for (int a = 0; a < D; a++) eo = eo * bext[a] + mc_edge_off<D>(ed, a);
+						dst[k] = (uint32_t)first[(bi + eo) * D + mc_edge_axis<D>(ed)];
 					}
 					si++;
 				}
@@ -504,6 +561,31 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 			}
 		}
 		__syncthreads();
+	}
+}
+
+/// Poly::Single::idx vertex construction (Poly.hpp:296-346) for every vertex that the last
+/// k_polys_march placed in the arena range [vstart, used): decodes the descriptor in the slot
+/// and overwrites it with the position (and, in 3D, the normal). One thread per vertex.
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_polys_vertices(Dev P, PolysDev Q)
+{
+	constexpr int VF = D == 3 ? 2 * D : D;
+	const long long v0 = (long long)Q.vstart[0], v1 = (long long)Q.used[0];
+	for (long long i = v0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < v1;
+	     i += (long long)gridDim.x * blockDim.x) {
+		float* slot = Q.vtx + (size_t)i * VF;
+		const unsigned long long d = *(const unsigned long long*)slot;
+		const int gp = (int)(d >> 21), leaf = (int)((d >> 4) & 0x1ffff), ed = (int)(d & 15);
+		const SurfGeom& g = P.geom[P.surf_of[gp]];
+		Vec<D> pa = leaf_pos<D>(P, gp, leaf);
+		if (D == 3) pa[D - 1] += 1;  // SpxGridPosOffset (PolyMixin.hpp:409)
+#pragma unroll
+		for (int a = 0; a < D; a++) pa[a] += mc_edge_off<D>(ed, a);
+		float out[VF];
+		make_vertex<D, L>(PoolGet<D, L>{P, g}, g, pa, mc_edge_axis<D>(ed), out);
+#pragma unroll
+		for (int k = 0; k < VF; k++) slot[k] = out[k];
 	}
 }
 
@@ -578,11 +660,13 @@ public:
 		woff_ = (int*)al((P.S + 1) * sizeof(int));
 		Q_.err = P.err;
 		Q_.ovf = (int*)al(sizeof(int));
+		Q_.vstart = (unsigned long long*)al(sizeof(unsigned long long));
 		Q_.pend = 0;
 		alloc_arena(1 << 20, 2 << 20);
-		int cvol = 1;
-		for (int a = 0; a < D; a++) cvol *= eng.part(a) + 2;
-		smem_ = (size_t)cvol * D * sizeof(int) + 3 * (size_t)P.BV * sizeof(uint16_t);
+		int bvol = 1;
+		for (int a = 0; a < D; a++) bvol *= eng.part(a) + 1;
+		smem_ = (size_t)bvol * (D * sizeof(int) + sizeof(float)) +
+		        3 * (size_t)P.BV * sizeof(uint16_t);
 		smem_ = (smem_ + 15) & ~(size_t)15;
 		if (smem_ > 48 * 1024)
 			FG_CUDA(cudaFuncSetAttribute(k_polys_march<D, L>,
@@ -601,7 +685,7 @@ public:
 	void notify() override
 	{
 		const Dev& P = eng_.dev();
-		FG_RUN("k_polys_notify", eng_.stream(), k_polys_notify<L><<<(P.S + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_););
+		FG_RUN("k_polys_notify", eng_.stream(), k_polys_notify<L><<<(P.S * 32 + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_););
 		FG_CUDA(cudaGetLastError());
 	}
 
@@ -620,13 +704,13 @@ public:
 		// Re-marching a partition recomputes it from the isogrid, so a march that ran out of
 		// arena space is simply repeated after the arena has grown.
 		for (int attempt = 0;; attempt++) {
-			maybe_compact(attempt > 0);
-			FG_CUDA(cudaMemsetAsync(Q_.ovf, 0, sizeof(int), st));
+			begin_attempt(attempt);
 			FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1););
 			FG_CUDA(cudaGetLastError());
 			if (!overflowed()) break;
 			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
 		}
+		vertices();
 		// swap pending and done, then reset the new pending list
 		Q_.pend ^= 1;
 		FG_RUN("k_polys_reset_list", st, k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend););
@@ -639,14 +723,32 @@ public:
 		const Dev& P = eng_.dev();
 		const int gp = check_part(part);
 		for (int attempt = 0;; attempt++) {
-			maybe_compact(attempt > 0);
-			FG_CUDA(cudaMemsetAsync(Q_.ovf, 0, sizeof(int), eng_.stream()));
+			begin_attempt(attempt);
 			FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
 			FG_CUDA(cudaGetLastError());
 			if (!overflowed()) break;
 			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
 		}
+		vertices();
 		eng_.check_errors();
+	}
+
+	/// Resets the overflow flag and records where this attempt's vertices begin in the arena.
+	void begin_attempt(int attempt)
+	{
+		cudaStream_t st = eng_.stream();
+		maybe_compact(attempt > 0);
+		FG_CUDA(cudaMemsetAsync(Q_.ovf, 0, sizeof(int), st));
+		FG_CUDA(cudaMemcpyAsync(Q_.vstart, Q_.used, sizeof(unsigned long long),
+		                        cudaMemcpyDeviceToDevice, st));
+	}
+
+	/// Positions (and normals) of the vertices the last successful march attempt described.
+	void vertices()
+	{
+		cudaStream_t st = eng_.stream();
+		FG_RUN("k_polys_vertices", st, k_polys_vertices<D, L><<<grid() * 2, 256, 0, st>>>(eng_.dev(), Q_););
+		FG_CUDA(cudaGetLastError());
 	}
 
 	bool overflowed()

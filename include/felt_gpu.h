@@ -42,8 +42,10 @@ enum {
 	FG_ERR_OUTSIDE = -11,   /* a band node would be tracked outside the grid                */
 	FG_ERR_INACTIVE = -12,  /* write to an inactive partition (reference: undefined)        */
 	FG_ERR_CAPACITY = -13,  /* an output buffer or geometry arena is too small              */
-	FG_ERR_TIMEOUT = -14,   /* a bounded device wait gave up                                 */
-	FG_ERR_STATE = -15      /* call out of sequence (e.g. update_end without update_start)  */
+	FG_ERR_TIMEOUT = -14,   /* an update's convergence loop did not settle in 64 iterations,
+	                           or a bounded device wait gave up                              */
+	FG_ERR_STATE = -15      /* call out of sequence (e.g. update_end without update_start),
+	                           or an update of a surface stopped by FG_ERR_TIMEOUT          */
 };
 
 /* ---- builtin speed functors ----
