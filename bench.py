@@ -55,6 +55,13 @@ CONFIGS = {
                steps=100, plain_subset=16, cpu_subset=4, cpu_steps=50,
                workload="256 x Surface<3,2>, edges from {32,48,64,96,128}, 8^3 partitions, "
                         "speed -0.3*curv + U[-0.6,0.3], marching cubes at the end"),
+    "c5": dict(kind="serve", D=3, L=2, part=(8, 8, 8), lambdas=(100, 300, 1000, 3000, 10000),
+               max_requests=3000, max_seconds=2.0, budget=150e9, workers=4, plain_subset=24,
+               cpu_subset=200,
+               workload="served requests, Poisson arrivals at 100..10k/s: Surface<3,2>, edge "
+                        "log-uniform 32..256, 8^3 partitions, speed constant U[-0.6,-0.1] | "
+                        "-0.3*curv-0.2 | 0.2*hash_noise-0.2, 1..64 steps, polygonise p=0.5, "
+                        "admission by a 150 GB brick-pool budget"),
 }
 
 # Algorithmic bytes per work unit of the kernels whose roofline is reported:
@@ -278,15 +285,20 @@ class PlainSubset:
         return self.done + sum(s.node_updates() for s, _, _ in self.items)
 
 
-def time_steps(torch, work, stream, steps, warm, flush, start=0):
+def time_steps(torch, work, stream, steps, warm, flush, start=0, profile=False):
     """Times `steps` steps two ways over the same work: device time (CUDA events on the work's
     stream around the update/polygonisation launches) and end-to-end wall time through the C
     ABI (the host-side speed structs going in, the step's result coming out: the node-update
     counter every step and, after a march, the re-marched polygons). L2 is flushed (256 MB
-    write, > 126 MB L2) before each step, outside both timed intervals."""
+    write, > 126 MB L2) before each step, outside both timed intervals. With profile, the timed
+    steps run between cudaProfilerStart and cudaProfilerStop (for ncu --profile-from-start off).
+    """
     for i in range(warm):
         work.step(start + i)
     torch.cuda.synchronize()
+    if profile:
+        u0 = work.work_units()
+        torch.cuda.profiler.start()
     nu0 = work.node_updates()
     total, wall, d2h = 0.0, 0.0, 0
     for i in range(steps):
@@ -306,6 +318,11 @@ def time_steps(torch, work, stream, steps, warm, flush, start=0):
         b.synchronize()
         total += a.elapsed_time(b)
     torch.cuda.synchronize()
+    if profile:
+        torch.cuda.profiler.stop()
+        u1 = work.work_units()
+        print("profiled region work units (dist, zero, flush, march): "
+              + json.dumps([b - a for a, b in zip(u0, u1)]), file=sys.stderr, flush=True)
     return total, wall, work.node_updates() - nu0, d2h
 
 
@@ -382,12 +399,13 @@ def run_reference(args, name, cfg):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    steps = args.steps or cfg["steps"]
-    if cfg["kind"] == "single":
-        steps = min(steps, 20)
+    if cfg["kind"] == "serve":
+        steps = None
+        base = serve_cpu(cfg, cfg["cpu_subset"])
     else:
-        steps = min(steps, 10)
-    base = cpu_baseline(name, cfg, steps)
+        steps = args.steps or cfg["steps"]
+        steps = min(steps, 20 if cfg["kind"] == "single" else 10)
+        base = cpu_baseline(name, cfg, steps)
     line = {
         "impl": "reference", "metric": "narrow-band node-updates/s", "value": base["value"],
         "unit": "node-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
@@ -443,6 +461,168 @@ def roofline(fb, work, cfg, stream_steps):
     return out
 
 
+def serve_requests(cfg, lam, shard=0):
+    """Seeded Poisson request stream at rate lam: (arrival offset s, Request) pairs."""
+    import numpy as np
+    from felt_b200.serving import Request
+    rng = np.random.default_rng(0x5EED0005 + int(lam) + (shard << 20))
+    L = cfg["L"]
+    n = int(min(cfg["max_requests"], lam * cfg["max_seconds"]))
+    t, out = 0.0, []
+    for k in range(n):
+        t += float(rng.exponential(1.0 / lam))
+        e = int(round(math.exp(rng.uniform(math.log(32), math.log(256)))))
+        kind = ("constant", "curvature", "noise")[int(rng.integers(0, 3))]
+        if kind == "constant":
+            sp = dict(c=float(rng.uniform(-0.6, -0.1)))
+        elif kind == "curvature":
+            sp = dict(a=-0.3, c=-0.2)
+        else:
+            sp = dict(n=0.2, seed=int(rng.integers(0, 2**31)), c=-0.2)
+        lo, hi = -e // 2 + L + 1, e // 2 - L - 2
+        c = tuple(int(rng.integers(lo, hi + 1)) for _ in range(3))
+        steps = int(rng.integers(1, 65))
+        polys = bool(rng.random() < 0.5)
+        out.append((t, Request((e, e, e), c, sp, steps, polys, kind, rid=k)))
+    return out
+
+
+def serve_one_rate(fb, cfg, lam, shard=0):
+    """Feeds one rate's stream into a Server in real time; latency and throughput figures."""
+    from felt_b200.serving import Server
+    stream = serve_requests(cfg, lam, shard)
+    srv = Server(layers=cfg["L"], part=cfg["part"], budget_bytes=cfg["budget"],
+                 workers=cfg["workers"])
+    try:
+        t_first = srv.now()
+        for off, req in stream:
+            due = t_first + off
+            while srv.now() < due:
+                time.sleep(min(0.0005, max(0.0, due - srv.now())))
+            req.arrival = due
+            srv.submit(req)
+        if not srv.drain(timeout=900):
+            raise RuntimeError("serving did not drain")
+        res = srv.results()
+        t_end = max((r.done for r in res), default=t_first)
+        lat = sorted(r.latency for r in res)
+        pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] * 1e3) if lat else (lambda q: None)
+        return {"lambda_per_s": lam, "requests": len(stream), "admitted": srv.admitted,
+                "rejected": srv.rejected, "stopped": sum(r.stopped for r in res),
+                "p50_ms": pct(0.50), "p99_ms": pct(0.99),
+                "node_updates_per_s": srv.node_updates / max(t_end - t_first, 1e-9),
+                "node_updates": srv.node_updates, "seconds": t_end - t_first}
+    finally:
+        srv.close()
+
+
+def serve_plain(fb, cfg, k):
+    """The plain path on the first k requests of the 1k/s stream: one Surface (+ Polys) per
+    request, one request after another, wall clock."""
+    reqs = [r for _, r in serve_requests(cfg, 1000)[:k]]
+    nu, secs = 0, 0.0
+    for r in reqs:
+        t0 = time.perf_counter()
+        s = fb.Surface(r.size, cfg["part"], cfg["L"])
+        p = fb.Polys(s)
+        s.seed(r.centre)
+        for _ in range(r.steps):
+            s.update(**r.speed)
+            p.notify()
+        if r.polys:
+            p.march()
+        n = s.node_updates()
+        secs += time.perf_counter() - t0
+        nu += n
+        del p, s
+    return nu / secs, nu, secs
+
+
+def serve_cpu(cfg, k):
+    """The oracle on the first k requests of the 1k/s stream, one after another."""
+    from oracle import oracle as O
+    reqs = [r for _, r in serve_requests(cfg, 1000)[:k]]
+    nu, secs = 0.0, 0.0
+    for r in reqs:
+        s = O.Surface(r.size, cfg["part"], cfg["L"])
+        p = O.Polys(s)
+        s.seed(r.centre)
+        for _ in range(r.steps):
+            band = s.band_size()
+            t0 = time.perf_counter()
+            try:
+                s.update(**r.speed)
+            except O.OracleError:
+                secs += time.perf_counter() - t0
+                break
+            p.notify()
+            secs += time.perf_counter() - t0
+            nu += band
+        if r.polys:
+            t0 = time.perf_counter()
+            p.march()
+            secs += time.perf_counter() - t0
+    return {"value": nu / secs, "unit": "node-updates/s", "cores": 1, "kind": "port",
+            "sample": f"first {k} requests of the 1k/s stream, one after another "
+                      f"({nu:.3g} node-updates in {secs:.2f} s, single thread)"}
+
+
+def run_serve(args, name, cfg):
+    import torch
+    import felt_b200 as fb
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    # warm-up: one small wave through every code path
+    serve_one_rate(fb, dict(cfg, max_requests=8), 1000, shard=rank)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = fb.launch_count()
+    sweep = [serve_one_rate(fb, cfg, lam, shard=rank) for lam in cfg["lambdas"]]
+    launches = fb.launch_count() - l0
+    clk = clocks.stop()
+    best = max(sweep, key=lambda r: r["node_updates_per_s"])
+    value = best["node_updates_per_s"]
+    if pg:
+        secs, _, nu = combine_ranks(pg, best["seconds"], 0.0, best["node_updates"], "cuda")
+        value = nu / secs
+    extra = {}
+    cpu = None
+    if rank == 0:
+        p_rate, _, _ = serve_plain(fb, cfg, cfg["plain_subset"])
+        extra["plain"] = {"value": p_rate, "unit": "node-updates/s",
+                          "requests": cfg["plain_subset"],
+                          "how": "one Surface per request, requests one after another, wall clock"}
+        extra["served_over_plain"] = value / p_rate
+        if ws == 1 and not args.no_cpu:
+            cpu = serve_cpu(cfg, cfg["cpu_subset"])
+    if rank == 0:
+        config = {"workload": cfg["workload"], "name": name,
+                  "parallelism": f"surface shards x{ws} (independent request streams per rank)",
+                  "sweep": sweep, "value_at_lambda": best["lambda_per_s"]}
+        config.update(extra)
+        line = {
+            "metric": "narrow-band node-updates/s", "value": value, "unit": "node-updates/s",
+            "n_gpus": ws, "steps": None, "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config, "roofline": None, "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None,
+                    "how": "wall clock from each request's arrival to its result, through the "
+                           "public API"},
+            "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 def run_felt(args, name, cfg):
     import torch
     import felt_b200 as fb
@@ -468,7 +648,8 @@ def run_felt(args, name, cfg):
     time.sleep(0.3)
     l0 = fb.launch_count()
     print(f"launches before the timed region: {l0}", file=sys.stderr, flush=True)
-    t_ms, wall_s, nu, d2h = time_steps(torch, work, stream, steps, args.warmup, flush)
+    t_ms, wall_s, nu, d2h = time_steps(torch, work, stream, steps, args.warmup, flush,
+                                       profile=args.profile_region)
     launches = fb.launch_count() - l0
     clk = clocks.stop()
     if pg:
@@ -535,10 +716,14 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--brick-capacity", type=int, default=0,
                     help="brick pool capacity of single-surface configs (0 = automatic)")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, args.config, cfg)
+    elif cfg["kind"] == "serve":
+        run_serve(args, args.config, cfg)
     else:
         run_felt(args, args.config, cfg)
 

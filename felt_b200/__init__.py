@@ -341,6 +341,11 @@ class Batch:
         _chk(lib().fg_batch_surface_stopped(self._h, C.c_size_t(i), C.byref(v)))
         return bool(v.value)
 
+    def pause(self, i, paused=True):
+        """Pause (or resume) surface i: later batch calls skip it, leaving it exactly as after
+        its own last update."""
+        _chk(lib().fg_batch_pause(self._h, C.c_size_t(i), C.c_int(1 if paused else 0)))
+
     def stream(self):
         p = C.c_void_p()
         _chk(lib().fg_batch_stream(self._h, C.byref(p)))

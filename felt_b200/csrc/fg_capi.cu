@@ -431,6 +431,15 @@ int fg_batch_surface_stopped(fg_batch* b, size_t surface, int* stopped)
 	});
 }
 
+int fg_batch_pause(fg_batch* b, size_t surface, int paused)
+{
+	return guard([&] {
+		need(b, "batch");
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index");
+		b->eng->set_paused((int)surface, paused != 0);
+	});
+}
+
 int fg_batch_destroy(fg_batch* b)
 {
 	return guard([&] { delete b; });

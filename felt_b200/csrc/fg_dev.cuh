@@ -312,6 +312,43 @@ __device__ __forceinline__ float distance(const Dev& P, const SurfGeom& g, const
 	return __fadd_rn(__fmul_rn(dist, dir), dir);
 }
 
+/// distance() for leaf `leaf` of partition gp (brick slot sl): neighbours inside the same
+/// partition are read straight from the brick (no partition lookup); the others through
+/// get_phi. Same result as distance() at the leaf's position.
+template <int D, int L>
+__device__ __forceinline__ float distance_leaf(const Dev& P, const SurfGeom& g, int gp, int sl,
+                                               int leaf, float dist, float dir)
+{
+	dist = __fmul_rn(dist, dir);
+	const float* brick = P.phi + (size_t)sl * P.BV;
+	int q[D];
+	Vec<D> pos;
+	int rem = leaf;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		q[a] = rem / P.lstr[a];
+		rem -= q[a] * P.lstr[a];
+		pos[a] = P.porig[gp * 3 + a] + q[a];
+	}
+	Vec<D> n = pos;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+#pragma unroll
+		for (int s = -1; s <= 1; s += 2) {
+			n[a] = pos[a] + s;
+			if (in_grid<D>(g, n)) {
+				const int qa = q[a] + s;
+				const float v = (qa >= 0 && qa < P.csz[a]) ? brick[leaf + s * P.lstr[a]]
+				                                           : get_phi<D, L>(P, g, n);
+				const float dn = __fmul_rn(v, dir);
+				if (dn < dist) dist = dn;
+			}
+		}
+		n[a] = pos[a];
+	}
+	return __fadd_rn(__fmul_rn(dist, dir), dir);
+}
+
 /// Builtin speed: [a*curv] + [n*h] + [c] in that order (see include/felt_gpu.h).
 struct Speed {
 	int kind;

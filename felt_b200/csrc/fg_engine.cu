@@ -193,6 +193,7 @@ public:
 		P.sfrozen = dalloc<int>(S, o);
 		FG_CUDA(cudaMemsetAsync(P.sfrozen, 0, S * sizeof(int), st_));
 		frozen_.assign(S, 0);
+		paused_.assign(S, 0);
 		P.err = dalloc<int>(1, o);
 		P.changed = dalloc<int>(1, o);
 		P.kstat = dalloc<unsigned long long>(KS_N, o);
@@ -410,7 +411,15 @@ public:
 				newly_frozen_.push_back(s);
 			}
 		}
-		FG_CUDA(cudaMemcpyAsync(P_.sfrozen, frozen_.data(), frozen_.size() * sizeof(int),
+		push_stopped();
+	}
+
+	/// Device copy of the per-surface skip flags: stopped (frozen) or paused.
+	void push_stopped()
+	{
+		stopped_.resize(frozen_.size());
+		for (size_t s = 0; s < frozen_.size(); s++) stopped_[s] = frozen_[s] | paused_[s];
+		FG_CUDA(cudaMemcpyAsync(P_.sfrozen, stopped_.data(), stopped_.size() * sizeof(int),
 		                        cudaMemcpyHostToDevice, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
 	}
@@ -418,6 +427,14 @@ public:
 public:
 	bool frozen(int s) const override { return frozen_[s] != 0; }
 	void set_throw_on_freeze(bool on) override { throw_on_freeze_ = on; }
+	void set_paused(int s, bool on) override
+	{
+		check_surface(s);
+		if ((paused_[s] != 0) == on) return;
+		paused_[s] = on ? 1 : 0;
+		push_stopped();
+	}
+	bool paused(int s) const override { return paused_[s] != 0; }
 
 private:
 	void check_not_frozen()
@@ -850,6 +867,8 @@ private:
 	bool buf_dirty_[2] = {false, false};
 	static constexpr int kMaxIterations = 64;
 	std::vector<int> frozen_;
+	std::vector<int> paused_;
+	std::vector<int> stopped_;  // host staging of frozen_ | paused_
 	std::vector<int> newly_frozen_;
 	bool throw_on_freeze_ = true;
 	StepStats stats_;

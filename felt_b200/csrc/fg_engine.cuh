@@ -83,6 +83,10 @@ public:
 	/// Whether an update that stops a surface raises (single surfaces) or only records it
 	/// (batches, serving).
 	virtual void set_throw_on_freeze(bool on) = 0;
+	/// Pauses (or resumes) surface s: while paused no kernel works on it, so its state stays
+	/// exactly as after its last update. Used to retire finished requests of a served batch.
+	virtual void set_paused(int s, bool on) = 0;
+	virtual bool paused(int s) const = 0;
 	virtual const Dev& dev() const = 0;
 	virtual void sync() = 0;
 	virtual int part(int a) const = 0;

@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 }
 
 /// update_distance first pass (Surface.hpp:1028-1073): distance of every leaf of layer k to
-/// the zero curve, into the delta array.
+/// the zero curve, into the delta array. Each lane takes two leaves per round so that their
+/// neighbour reads are in flight together (the pass is bound by load latency).
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist1(Dev P, ListView lv, int k, float side)
 {
@@ -325,10 +326,16 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, ListView lv, int k, float 
 		const int sl = P.slot[gp];
 		const int n = lv.lcnt[sl * NL + li];
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
-		for (int j = lane; j < n; j += 32) {
-			const int leaf = lst[j];
-			const size_t kk = (size_t)sl * P.BV + leaf;
-			P.dlt[kk] = distance<D, L>(P, g, leaf_pos<D>(P, gp, leaf), P.phi[kk], side);
+		const size_t b0 = (size_t)sl * P.BV;
+		for (int j = lane; j < n; j += 64) {
+			const bool two = j + 32 < n;
+			const int l1 = lst[j];
+			const int l2 = two ? lst[j + 32] : l1;
+			const float p1 = P.phi[b0 + l1], p2 = P.phi[b0 + l2];
+			const float d1 = distance_leaf<D, L>(P, g, gp, sl, l1, p1, side);
+			const float d2 = distance_leaf<D, L>(P, g, gp, sl, l2, p2, side);
+			P.dlt[b0 + l1] = d1;
+			if (two) P.dlt[b0 + l2] = d2;
 		}
 		if (lane == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
 	}
@@ -507,26 +514,40 @@ __global__ void k_flush_leaf(Dev P)
 /// Shared-memory bytes k_flush_smem needs for a brick of BV leaves and NL lists.
 __host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
 {
-	return (size_t)(NL + 2) * BV * sizeof(uint16_t) + (size_t)BV + 16;
+	return (size_t)(NL + 3) * BV * sizeof(uint16_t) + (size_t)BV + 16;
 }
 
 /// k_flush_leaf with the partition staged in shared memory: one block per partition loads its
-/// leaf lists, leaf lookups and status entries, one thread replays the ordered edits on them
-/// (the replay is inherently sequential: each swap-with-last removal depends on the previous
-/// one), and the block writes the lists back. Same results as k_flush_leaf.
+/// leaf lists, leaf lookups and status entries, replays the edits on them and writes the lists
+/// back. Same results as k_flush_leaf.
+///
+/// The reference replays the edits one by one: from-layer phases in ascending order, each
+/// removing its leaves from list `from` (swap-with-last) and appending the in-band ones to list
+/// `to`. A leaf has one status entry, so list t only receives appends in the phases before and
+/// after its own removal phase, and those appends land at positions that follow from counts.
+/// So every list replays on its own warp: appends of earlier phases (ballot-ordered), its own
+/// removal chain (one lane; a swap-with-last removal depends on the previous one), appends of
+/// later phases. Leaves appended before the removals are tagged (bit 15) while in the list so
+/// that their positions go to a separate lookup (another list's warp may still read their old
+/// one). A leaf whose status ends where it started (to == from, a leaf that changed twice in
+/// one iteration) is removed and re-appended within its own phase; the removal lane handles it.
 template <int D, int L>
 __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 {
 	constexpr int NL = 2 * L + 1;
+	constexpr uint16_t TAG = 0x8000u;
 	extern __shared__ __align__(16) unsigned char fsm[];
 	const int BV = P.BV;
 	uint16_t* slst = (uint16_t*)fsm;                 // [NL * BV]
 	uint16_t* slkp = slst + (size_t)NL * BV;         // [BV]
 	uint16_t* schg = slkp + BV;                      // [BV] status entries, phase-major
-	int8_t* ssto = (int8_t*)(schg + BV);             // [BV]
-	__shared__ int cnt[NL], coff[NL + 1], live0;
+	uint16_t* snew = schg + BV;                      // [BV] positions of leaves appended to a list
+	int8_t* ssto = (int8_t*)(snew + BV);             // [BV]
+	__shared__ int cnt[NL], coff[NL + 1], live0, nout, lastout;
+	__shared__ unsigned appb[NL], remb;
 	const int n = P.counters[CNT_SUNION];
 	const size_t bv = (size_t)BV;
+	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	for (int e = blockIdx.x; e < n; e += gridDim.x) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
@@ -540,7 +561,11 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 			}
 			coff[NL] = c;
 			live0 = lv;
+			nout = 0;
+			lastout = -1;
+			remb = 0;
 		}
+		if (threadIdx.x < NL) appb[threadIdx.x] = 0;
 		__syncthreads();
 		for (int l = 0; l < NL; l++) {
 			const uint16_t* src = P.lst + ((size_t)sl * NL + l) * bv;
@@ -552,56 +577,105 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 			const int nc = coff[fi + 1] - coff[fi];
 			for (int c = threadIdx.x; c < nc; c += blockDim.x) {
 				const int leaf = src[c];
+				const int to = P.sto[sl * bv + leaf];
 				schg[coff[fi] + c] = (uint16_t)leaf;
-				ssto[coff[fi] + c] = P.sto[sl * bv + leaf];
+				ssto[coff[fi] + c] = (int8_t)to;
+				if (!inside_band(to, L)) {
+					// Untrack (PartitionedMixin.hpp:530-558): the node leaves the band
+					P.phi[sl * bv + leaf] = (float)to;
+					atomicAdd(&nout, 1);
+					atomicMax(&lastout, coff[fi] + c);
+				}
 			}
 		}
 		__syncthreads();
-		if (threadIdx.x == 0) {
-			int live = live0;
-			unsigned remb = 0;
-			bool dead = false;
-			int deadto = 0;
-			for (int fi = 0; fi < NL; fi++) {
-				unsigned appf = 0;
-				uint16_t* lf = slst + fi * bv;
-				for (int c = coff[fi]; c < coff[fi + 1]; c++) {
+		const int total = coff[NL];
+		for (int t = warp; t < NL; t += nwarps) {
+			uint16_t* lf = slst + t * bv;
+			int len = cnt[t];
+			// appends to list t from the phases before t
+			for (int base = 0; base < coff[t]; base += 32) {
+				const int c = base + lane;
+				const bool hit = c < coff[t] && ssto[c] + L == t;
+				const unsigned m = __ballot_sync(FULL, hit);
+				if (hit) {
+					const int pos = len + __popc(m & ((1u << lane) - 1u));
 					const int leaf = schg[c];
-					const int to = ssto[c];
+					lf[pos] = (uint16_t)(leaf | TAG);
+					snew[leaf] = (uint16_t)pos;
+					if (pos == 0) {
+						int f = 0;
+						while (c >= coff[f + 1]) f++;
+						atomicOr(&appb[f], 1u << t);
+					}
+				}
+				len += __popc(m);
+			}
+			__syncwarp();
+			// phase t: swap-with-last removals (LookupMixin.hpp:339-371), in order
+			if (lane == 0) {
+				for (int c = coff[t]; c < coff[t + 1]; c++) {
+					const int leaf = schg[c];
 					const int pos = slkp[leaf];
-					const int last = cnt[fi] - 1;
+					const int last = len - 1;
 					if (pos < last) {
 						const int moved = lf[last];
 						lf[pos] = (uint16_t)moved;
-						slkp[moved] = (uint16_t)pos;
+						if (moved & TAG)
+							snew[moved & ~TAG] = (uint16_t)pos;
+						else
+							slkp[moved] = (uint16_t)pos;
 					}
 					slkp[leaf] = NUL16;
-					cnt[fi] = last;
-					if (inside_band(to, L)) {
-						const int ti = to + L;
-						slst[ti * bv + cnt[ti]] = (uint16_t)leaf;
-						slkp[leaf] = (uint16_t)cnt[ti];
-						if (cnt[ti] == 0) appf |= 1u << ti;
-						cnt[ti]++;
-						if (last == 0) remb |= 1u << fi;
-					} else {
-						P.phi[sl * bv + leaf] = (float)to;
-						live--;
-						if (last == 0) {
-							remb |= 1u << fi;
-							if (live == 0) {
-								dead = true;
-								deadto = to;
-							}
-						}
+					len = last;
+					if (last == 0) atomicOr(&remb, 1u << t);
+					if (ssto[c] + L == t) {  // back to its own list: re-appended at the end
+						lf[len] = (uint16_t)leaf;
+						slkp[leaf] = (uint16_t)len;
+						if (len == 0) atomicOr(&appb[t], 1u << t);
+						len++;
 					}
 				}
-				P.app[gp * NL + fi] = appf;
 			}
+			len = __shfl_sync(FULL, len, 0);
+			__syncwarp();
+			// appends to list t from the phases after t
+			for (int base = coff[t + 1]; base < total; base += 32) {
+				const int c = base + lane;
+				const bool hit = c < total && ssto[c] + L == t;
+				const unsigned m = __ballot_sync(FULL, hit);
+				if (hit) {
+					const int pos = len + __popc(m & ((1u << lane) - 1u));
+					const int leaf = schg[c];
+					lf[pos] = (uint16_t)leaf;
+					snew[leaf] = (uint16_t)pos;
+					if (pos == 0) {
+						int f = 0;
+						while (c >= coff[f + 1]) f++;
+						atomicOr(&appb[f], 1u << t);
+					}
+				}
+				len += __popc(m);
+			}
+			if (lane == 0) cnt[t] = len;
+		}
+		__syncthreads();
+		// leaves that moved to another list take their position there
+		for (int c = threadIdx.x; c < total; c += blockDim.x) {
+			const int to = ssto[c];
+			if (!inside_band(to, L)) continue;
+			int f = 0;
+			while (c >= coff[f + 1]) f++;
+			if (to + L != f) slkp[schg[c]] = snew[schg[c]];
+		}
+		if (threadIdx.x < NL) P.app[gp * NL + threadIdx.x] = appb[threadIdx.x];
+		if (threadIdx.x == 0) {
 			P.rem[gp] = remb;
-			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)coff[NL]);
-			if (dead) {
-				P.bg[gp] = (float)deadto;
+			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)total);
+			if (nout > 0 && nout == live0) {
+				// the last leaf left the band: the partition deactivates with the background
+				// of that leaf's side (PartitionedMixin.hpp:530-558)
+				P.bg[gp] = (float)ssto[lastout];
 				P.oslot[gp] = sl;
 				P.slot[gp] = -1;
 				P.q_retire[atomicAdd(&P.counters[CNT_RETIRE], 1)] = sl;
@@ -610,7 +684,8 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 		__syncthreads();
 		for (int l = 0; l < NL; l++) {
 			uint16_t* dst = P.lst + ((size_t)sl * NL + l) * bv;
-			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x) dst[i] = slst[l * bv + i];
+			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x)
+				dst[i] = (uint16_t)(slst[l * bv + i] & ~TAG);
 			if (threadIdx.x == 0) P.lcnt[sl * NL + l] = cnt[l];
 		}
 		for (int i = threadIdx.x; i < BV; i += blockDim.x) P.lkp[sl * bv + i] = slkp[i];

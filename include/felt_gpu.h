@@ -224,6 +224,11 @@ FG_API int fg_batch_node_updates(fg_batch* b, unsigned long long* n);
  * worked on again) so the rest of the batch completes. A single fg_surface reports the same
  * event as FG_ERR_TIMEOUT from the update, and FG_ERR_STATE from later updates. */
 FG_API int fg_batch_surface_stopped(fg_batch* b, size_t surface, int* stopped);
+/* Pauses (paused != 0) or resumes one surface of a batch. No counterpart in the reference: a
+ * server retires a finished request this way, so later batch updates, notifies and marches skip
+ * it and its state stays exactly as after its own last update (equal to a separate fg_surface
+ * advanced by the same updates). */
+FG_API int fg_batch_pause(fg_batch* b, size_t surface, int paused);
 FG_API int fg_batch_work_units(fg_batch* b, unsigned long long* out, size_t n);
 FG_API int fg_batch_stream(fg_batch* b, void** stream);
 
