@@ -95,6 +95,7 @@ struct Dev {
 	int* papg;        // [2*NP] the local partition index of each pap entry
 	int* papn;        // [S]
 	int* woff;        // [S+1] entry offsets of the current pass
+	int* woffl;       // [NL*(S+1)] entry offsets of every layer's list, for the distance passes
 	int* sfrozen;     // [S] surfaces stopped after a non-terminating update (no further work)
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes

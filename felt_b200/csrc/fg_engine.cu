@@ -190,6 +190,7 @@ public:
 		P.papg = dalloc<int>(2 * (size_t)NP, o);
 		P.papn = dalloc<int>(S, o);
 		P.woff = dalloc<int>(S + 1, o);
+		P.woffl = dalloc<int>((size_t)NL * (S + 1), o);
 		P.sfrozen = dalloc<int>(S, o);
 		FG_CUDA(cudaMemsetAsync(P.sfrozen, 0, S * sizeof(int), st_));
 		frozen_.assign(S, 0);
@@ -247,6 +248,7 @@ public:
 			                             cudaFuncAttributeMaxDynamicSharedMemorySize,
 			                             (int)smem_halo_));
 		}
+		dist_split_ = BV >= 4096 ? 4 : BV >= 1024 ? 2 : 1;
 		smem_flush_ = flush_smem_bytes(BV, NL);
 		if (smem_flush_ <= 200 * 1024) {
 			if (smem_flush_ > 48 * 1024)
@@ -342,7 +344,7 @@ public:
 		scan(P_.pcnt, L, 0);
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, iso, nullptr, B););
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.plist, L, B););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.plist, L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(iso, B);
 		converge();
@@ -502,7 +504,7 @@ public:
 		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
 		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
 		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, aff, P_.dlcnt, B););
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.aplist[A], L, B););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.aplist[A], L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(aff, B);
 		converge(true);
@@ -781,18 +783,22 @@ private:
 		FG_RUN("k_band_size", st_, k_band_size<L><<<warp_grid_, 256, 0, st_>>>(P_, acc_););
 	}
 
+	/// The 2L layer passes of update_distance (Surface.hpp:989-1125). The pass lists do not
+	/// change while the passes run (they append to the other buffer), so one launch scans the
+	/// entry offsets of every layer up front.
 	void distance_passes(const ListView& lv, int b)
 	{
+		FG_RUN("k_scan_layers", st_, k_scan_layers<<<1, 1024, 0, st_>>>(lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
 		for (int k = -1; k >= -L; k--) layer_pass(lv, k, -1.0f, b);
 		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
 	}
 
 	void layer_pass(const ListView& lv, int k, float side, int b)
 	{
-		scan(lv.pcnt, k + L, 0);
-		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, side););
-		FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, k, b););
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, lv.plist, k + L, b););
+		const int* woff = P_.woffl + (size_t)(k + L) * (P_.S + 1);
+		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, side, dist_split_););
+		FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
+		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, woff, lv.plist, k + L, b););
 	}
 
 	void flush()
@@ -863,6 +869,7 @@ private:
 	int* d_lcount_ = nullptr;
 	int lcap_ = 0;
 	int warp_grid_ = 0;
+	int dist_split_ = 1;  // warps per partition entry in the first distance pass
 	bool status_dirty_ = false;
 	bool buf_dirty_[2] = {false, false};
 	static constexpr int kMaxIterations = 64;

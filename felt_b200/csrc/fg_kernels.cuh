@@ -86,6 +86,30 @@ static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, in
 	}
 }
 
+/// k_scan_counts mode 0 for every layer index at once: woffl[l*(S+1) + s].
+static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, const int* frozen)
+{
+	__shared__ int carry;
+	for (int l = 0; l < NL; l++) {
+		int* woff = woffl + (size_t)l * (S + 1);
+		if (threadIdx.x == 0) {
+			carry = 0;
+			woff[0] = 0;
+		}
+		__syncthreads();
+		for (int base = 0; base < S; base += blockDim.x) {
+			const int s = base + threadIdx.x;
+			const int v = (s < S && !(frozen && frozen[s])) ? cnt[s * NL + l] : 0;
+			int tot;
+			const int ex = block_excl_scan(v, &tot);
+			if (s < S) woff[s + 1] = carry + ex + v;
+			__syncthreads();
+			if (threadIdx.x == 0) carry += tot;
+			__syncthreads();
+		}
+	}
+}
+
 #define FG_WARP_LOOP(woff_)                                                         \
 	const int lane = lane_id();                                                     \
 	const int nwarps = (gridDim.x * blockDim.x) >> 5;                              \
@@ -311,62 +335,80 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 }
 
 /// update_distance first pass (Surface.hpp:1028-1073): distance of every leaf of layer k to
-/// the zero curve, into the delta array. Each lane takes two leaves per round so that their
-/// neighbour reads are in flight together (the pass is bound by load latency).
+/// the zero curve, into the delta array. The pass is bound by load latency, so each partition
+/// entry gets `split` warps that take interleaved 32-leaf chunks (large bricks: the fullest
+/// partitions no longer set the pass's length alone), and each lane takes two leaves per round
+/// so that their neighbour reads are in flight together. The order of the writes does not
+/// matter (Jacobi).
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_dist1(Dev P, ListView lv, int k, float side)
+__global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
+                                               float side, int split)
 {
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
-	FG_WARP_LOOP(P.woff)
-	{
-		const int s = entry_surface(P.woff, P.S, e);
+	const int lane = lane_id();
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	const int total = woff[P.S] * split;
+	for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
+		const int e = v / split, part = v - e * split;
+		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - P.woff[s])];
+		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
 		const int sl = P.slot[gp];
 		const int n = lv.lcnt[sl * NL + li];
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
-		for (int j = lane; j < n; j += 64) {
-			const bool two = j + 32 < n;
+		const int STRIDE = 32 * split;
+		for (int j = part * 32 + lane; j < n; j += 2 * STRIDE) {
+			const bool two = j + STRIDE < n;
 			const int l1 = lst[j];
-			const int l2 = two ? lst[j + 32] : l1;
+			const int l2 = two ? lst[j + STRIDE] : l1;
 			const float p1 = P.phi[b0 + l1], p2 = P.phi[b0 + l2];
 			const float d1 = distance_leaf<D, L>(P, g, gp, sl, l1, p1, side);
 			const float d2 = distance_leaf<D, L>(P, g, gp, sl, l2, p2, side);
 			P.dlt[b0 + l1] = d1;
 			if (two) P.dlt[b0 + l2] = d2;
 		}
-		if (lane == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
+		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
 	}
 }
 
 /// update_distance second pass (Surface.hpp:1075-1121): apply and record status changes.
+/// The next chunk's list entry and delta are loaded before the current chunk's status records
+/// (which must stay in list order), so the two load latencies overlap the record work.
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_dist2(Dev P, ListView lv, int k, int b)
+__global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
 {
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
-	FG_WARP_LOOP(P.woff)
+	FG_WARP_LOOP(woff)
 	{
-		const int s = entry_surface(P.woff, P.S, e);
+		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - P.woff[s])];
+		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
 		const int sl = P.slot[gp];
 		const int n = lv.lcnt[sl * NL + li];
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
+		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
 		bool any = false;
+		bool vnext = lane < n;
+		int lnext = vnext ? lst[lane] : 0;
+		float dnext = vnext ? P.dlt[b0 + lnext] : 0.0f;
 		for (int base = 0; base < n; base += 32) {
-			const int j = base + lane;
-			const bool valid = j < n;
-			int leaf = 0, to = 0;
+			const bool valid = vnext;
+			const int leaf = lnext;
+			const float d = dnext;
+			const int jn = base + 32 + lane;
+			vnext = jn < n;
+			if (vnext) {
+				lnext = lst[jn];
+				dnext = P.dlt[b0 + lnext];
+			}
+			int to = 0;
 			if (valid) {
-				leaf = lst[j];
-				const size_t kk = (size_t)sl * P.BV + leaf;
-				const float d = P.dlt[kk];
 				to = layer_id(d, P.err);
-				P.phi[kk] = d;
+				P.phi[b0 + leaf] = d;
 			}
 			status_chunk<L>(P, gp, sl, k, valid, leaf, to, b, flags, any);
 		}
@@ -381,56 +423,51 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, ListView lv, int k, int b)
 /// Appends, in the pass's partition order, the partitions that gained status changes to the
 /// status partition list of layer index `li`, and those newly tracked in buffer b's partition
 /// lists (the children-level track_child calls of status_change, PartitionedMixin.hpp:201-213).
-/// One block per surface.
+/// One block per surface; each of its warps owns whole lists (list t < NL: buffer list t,
+/// list NL: the status list) and ranks the entries that join it with ballots, so no block-wide
+/// barrier sits in the walk.
 template <int L>
-__global__ void k_compact(Dev P, const int* plist, int li, int b)
+__global__ void __launch_bounds__(256) k_compact(Dev P, const int* woff, const int* plist, int li,
+                                                 int b)
 {
 	constexpr int NL = 2 * L + 1;
 	const int s = blockIdx.x;
 	const SurfGeom& g = P.geom[s];
-	const int e0 = P.woff[s], e1 = P.woff[s + 1];
-	__shared__ int cnt_s, cnt_a[NL];
-	if (threadIdx.x == 0) cnt_s = P.spcnt[s * NL + li];
-	if (threadIdx.x < NL) cnt_a[threadIdx.x] = P.apcnt[b][s * NL + threadIdx.x];
-	__syncthreads();
-	for (int base = e0; base < e1; base += blockDim.x) {
-		const int e = base + threadIdx.x;
-		unsigned f = 0;
-		int lp = 0;
-		if (e < e1) {
-			f = P.eflag[e];
-			lp = plist[(size_t)li * P.NP + g.pbase + (e - e0)];
-		}
-		const int gp = g.pbase + lp;
-		int tot;
-		const bool fs = (f & 0x80000000u) != 0;
-		const int ps = block_excl_scan(fs ? 1 : 0, &tot);
-		if (fs) {
-			const int pos = cnt_s + ps;
-			P.splist[(size_t)li * P.NP + g.pbase + pos] = lp;
-			P.sppos[gp * NL + li] = pos;
-			if (atomicExch(&P.sflag[gp], 1) == 0)
-				P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
-		}
-		__syncthreads();
-		if (threadIdx.x == 0) cnt_s += tot;
-		for (int t = 0; t < NL; t++) {
-			const bool ft = (f >> t) & 1u;
-			int tt;
-			const int pt = block_excl_scan(ft ? 1 : 0, &tt);
-			if (ft) {
-				const int pos = cnt_a[t] + pt;
-				P.aplist[b][(size_t)t * P.NP + g.pbase + pos] = lp;
-				P.appos[b][gp * NL + t] = pos;
+	const int e0 = woff[s], e1 = woff[s + 1];
+	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const unsigned lt = (1u << lane) - 1u;
+	for (int t = warp; t <= NL; t += nwarps) {
+		const bool status = t == NL;
+		const unsigned bit = status ? 0x80000000u : (1u << t);
+		int cnt = status ? P.spcnt[s * NL + li] : P.apcnt[b][s * NL + t];
+		int* list = status ? P.splist + (size_t)li * P.NP + g.pbase
+		                   : P.aplist[b] + (size_t)t * P.NP + g.pbase;
+		for (int base = e0; base < e1; base += 32) {
+			const int e = base + lane;
+			const bool hit = e < e1 && (P.eflag[e] & bit);
+			const unsigned m = __ballot_sync(FULL, hit);
+			if (hit) {
+				const int lp = plist[(size_t)li * P.NP + g.pbase + (e - e0)];
+				const int gp = g.pbase + lp;
+				const int pos = cnt + __popc(m & lt);
+				list[pos] = lp;
+				if (status) {
+					P.sppos[gp * NL + li] = pos;
+					if (atomicExch(&P.sflag[gp], 1) == 0)
+						P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
+				} else {
+					P.appos[b][gp * NL + t] = pos;
+				}
 			}
-			__syncthreads();
-			if (threadIdx.x == 0) cnt_a[t] += tt;
+			cnt += __popc(m);
 		}
-		__syncthreads();
+		if (lane == 0) {
+			if (status)
+				P.spcnt[s * NL + li] = cnt;
+			else
+				P.apcnt[b][s * NL + t] = cnt;
+		}
 	}
-	__syncthreads();
-	if (threadIdx.x == 0) P.spcnt[s * NL + li] = cnt_s;
-	if (threadIdx.x < NL) P.apcnt[b][s * NL + threadIdx.x] = cnt_a[threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -511,26 +548,28 @@ __global__ void k_flush_leaf(Dev P)
 	}
 }
 
-/// Shared-memory bytes k_flush_smem needs for a brick of BV leaves and NL lists.
+/// Shared-memory bytes k_flush_smem needs for a brick of BV leaves.
 __host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
 {
-	return (size_t)(NL + 3) * BV * sizeof(uint16_t) + (size_t)BV + 16;
+	(void)NL;
+	return (size_t)4 * BV * sizeof(uint16_t) + (size_t)BV + 16;
 }
 
-/// k_flush_leaf with the partition staged in shared memory: one block per partition loads its
-/// leaf lists, leaf lookups and status entries, replays the edits on them and writes the lists
-/// back. Same results as k_flush_leaf.
+/// k_flush_leaf for one block per partition, touching only what the edits touch. Same results.
 ///
 /// The reference replays the edits one by one: from-layer phases in ascending order, each
 /// removing its leaves from list `from` (swap-with-last) and appending the in-band ones to list
 /// `to`. A leaf has one status entry, so list t only receives appends in the phases before and
 /// after its own removal phase, and those appends land at positions that follow from counts.
 /// So every list replays on its own warp: appends of earlier phases (ballot-ordered), its own
-/// removal chain (one lane; a swap-with-last removal depends on the previous one), appends of
-/// later phases. Leaves appended before the removals are tagged (bit 15) while in the list so
-/// that their positions go to a separate lookup (another list's warp may still read their old
-/// one). A leaf whose status ends where it started (to == from, a leaf that changed twice in
-/// one iteration) is removed and re-appended within its own phase; the removal lane handles it.
+/// removal chain (one lane; each swap-with-last removal depends on the previous one), appends of
+/// later phases. A list of length n losing m leaves only ever takes its moved entries from its
+/// last m slots (the removal window), so only that window is staged in shared memory; every
+/// other write goes straight to the brick's list. Leaves appended before the removals are tagged
+/// (bit 15) while in the window so that their positions go to a separate lookup (the warp of
+/// their old list may still read the old one). A leaf whose status ends where it started
+/// (to == from: it changed twice in one iteration) is removed and re-appended within its own
+/// phase by the removal lane.
 template <int D, int L>
 __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 {
@@ -538,19 +577,21 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 	constexpr uint16_t TAG = 0x8000u;
 	extern __shared__ __align__(16) unsigned char fsm[];
 	const int BV = P.BV;
-	uint16_t* slst = (uint16_t*)fsm;                 // [NL * BV]
-	uint16_t* slkp = slst + (size_t)NL * BV;         // [BV]
-	uint16_t* schg = slkp + BV;                      // [BV] status entries, phase-major
-	uint16_t* snew = schg + BV;                      // [BV] positions of leaves appended to a list
-	int8_t* ssto = (int8_t*)(snew + BV);             // [BV]
-	__shared__ int cnt[NL], coff[NL + 1], live0, nout, lastout;
+	uint16_t* slkp = (uint16_t*)fsm;       // [BV] positions of the leaves the removals touch
+	uint16_t* schg = slkp + BV;            // [BV] status entries, phase-major
+	uint16_t* snew = schg + BV;            // [BV] positions of leaves appended to another list
+	uint16_t* swin = snew + BV;            // [BV] removal window of list t at coff[t]
+	int8_t* ssto = (int8_t*)(swin + BV);   // [BV] status "to" of each entry
+	__shared__ int cnt[NL], coff[NL + 1], nbef[NL], live0, nout, lastout;
 	__shared__ unsigned appb[NL], remb;
 	const int n = P.counters[CNT_SUNION];
 	const size_t bv = (size_t)BV;
 	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const unsigned lt = (1u << lane) - 1u;
 	for (int e = blockIdx.x; e < n; e += gridDim.x) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
+		uint16_t* lkp = P.lkp + sl * bv;
 		if (threadIdx.x == 0) {
 			int c = 0, lv = 0;
 			for (int l = 0; l < NL; l++) {
@@ -565,13 +606,13 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 			lastout = -1;
 			remb = 0;
 		}
-		if (threadIdx.x < NL) appb[threadIdx.x] = 0;
-		__syncthreads();
-		for (int l = 0; l < NL; l++) {
-			const uint16_t* src = P.lst + ((size_t)sl * NL + l) * bv;
-			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x) slst[l * bv + i] = src[i];
+		if (threadIdx.x < NL) {
+			appb[threadIdx.x] = 0;
+			nbef[threadIdx.x] = 0;
 		}
-		for (int i = threadIdx.x; i < BV; i += blockDim.x) slkp[i] = P.lkp[sl * bv + i];
+		__syncthreads();
+		// status entries, the removed leaves' positions, and how many leaves each list receives
+		// from earlier phases
 		for (int fi = 0; fi < NL; fi++) {
 			const uint16_t* src = P.chg + ((size_t)sl * NL + fi) * bv;
 			const int nc = coff[fi + 1] - coff[fi];
@@ -580,28 +621,49 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 				const int to = P.sto[sl * bv + leaf];
 				schg[coff[fi] + c] = (uint16_t)leaf;
 				ssto[coff[fi] + c] = (int8_t)to;
+				slkp[leaf] = lkp[leaf];
 				if (!inside_band(to, L)) {
 					// Untrack (PartitionedMixin.hpp:530-558): the node leaves the band
 					P.phi[sl * bv + leaf] = (float)to;
 					atomicAdd(&nout, 1);
 					atomicMax(&lastout, coff[fi] + c);
+				} else if (to + L > fi) {
+					atomicAdd(&nbef[to + L], 1);
 				}
+			}
+		}
+		__syncthreads();
+		// each list's removal window: its original entries there
+		for (int t = warp; t < NL; t += nwarps) {
+			const int m = coff[t + 1] - coff[t];
+			const int w0 = cnt[t] + nbef[t] - m;
+			const uint16_t* src = P.lst + ((size_t)sl * NL + t) * bv;
+			for (int pos = w0 + lane; pos < cnt[t]; pos += 32) {
+				const int x = src[pos];
+				swin[coff[t] + pos - w0] = (uint16_t)x;
+				slkp[x] = (uint16_t)pos;
 			}
 		}
 		__syncthreads();
 		const int total = coff[NL];
 		for (int t = warp; t < NL; t += nwarps) {
-			uint16_t* lf = slst + t * bv;
+			uint16_t* lf = P.lst + ((size_t)sl * NL + t) * bv;
+			uint16_t* win = swin + coff[t];
+			const int m = coff[t + 1] - coff[t];
 			int len = cnt[t];
+			const int w0 = len + nbef[t] - m;
 			// appends to list t from the phases before t
 			for (int base = 0; base < coff[t]; base += 32) {
 				const int c = base + lane;
 				const bool hit = c < coff[t] && ssto[c] + L == t;
-				const unsigned m = __ballot_sync(FULL, hit);
+				const unsigned msk = __ballot_sync(FULL, hit);
 				if (hit) {
-					const int pos = len + __popc(m & ((1u << lane) - 1u));
+					const int pos = len + __popc(msk & lt);
 					const int leaf = schg[c];
-					lf[pos] = (uint16_t)(leaf | TAG);
+					if (pos >= w0)
+						win[pos - w0] = (uint16_t)(leaf | TAG);
+					else
+						lf[pos] = (uint16_t)leaf;
 					snew[leaf] = (uint16_t)pos;
 					if (pos == 0) {
 						int f = 0;
@@ -609,7 +671,7 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 						atomicOr(&appb[f], 1u << t);
 					}
 				}
-				len += __popc(m);
+				len += __popc(msk);
 			}
 			__syncwarp();
 			// phase t: swap-with-last removals (LookupMixin.hpp:339-371), in order
@@ -619,18 +681,23 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 					const int pos = slkp[leaf];
 					const int last = len - 1;
 					if (pos < last) {
-						const int moved = lf[last];
-						lf[pos] = (uint16_t)moved;
-						if (moved & TAG)
-							snew[moved & ~TAG] = (uint16_t)pos;
+						const int moved = win[last - w0];
+						if (pos >= w0)
+							win[pos - w0] = (uint16_t)moved;
 						else
+							lf[pos] = (uint16_t)(moved & ~TAG);
+						if (moved & TAG) {
+							snew[moved & ~TAG] = (uint16_t)pos;
+						} else {
 							slkp[moved] = (uint16_t)pos;
+							lkp[moved] = (uint16_t)pos;
+						}
 					}
 					slkp[leaf] = NUL16;
 					len = last;
 					if (last == 0) atomicOr(&remb, 1u << t);
 					if (ssto[c] + L == t) {  // back to its own list: re-appended at the end
-						lf[len] = (uint16_t)leaf;
+						win[len - w0] = (uint16_t)leaf;
 						slkp[leaf] = (uint16_t)len;
 						if (len == 0) atomicOr(&appb[t], 1u << t);
 						len++;
@@ -639,13 +706,15 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 			}
 			len = __shfl_sync(FULL, len, 0);
 			__syncwarp();
+			// what is left of the window (re-appended leaves) joins the list
+			for (int pos = w0 + lane; pos < len; pos += 32) lf[pos] = (uint16_t)(win[pos - w0] & ~TAG);
 			// appends to list t from the phases after t
 			for (int base = coff[t + 1]; base < total; base += 32) {
 				const int c = base + lane;
 				const bool hit = c < total && ssto[c] + L == t;
-				const unsigned m = __ballot_sync(FULL, hit);
+				const unsigned msk = __ballot_sync(FULL, hit);
 				if (hit) {
-					const int pos = len + __popc(m & ((1u << lane) - 1u));
+					const int pos = len + __popc(msk & lt);
 					const int leaf = schg[c];
 					lf[pos] = (uint16_t)leaf;
 					snew[leaf] = (uint16_t)pos;
@@ -655,20 +724,23 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 						atomicOr(&appb[f], 1u << t);
 					}
 				}
-				len += __popc(m);
+				len += __popc(msk);
 			}
 			if (lane == 0) cnt[t] = len;
 		}
 		__syncthreads();
-		// leaves that moved to another list take their position there
+		// the final position of every leaf with a status entry
 		for (int c = threadIdx.x; c < total; c += blockDim.x) {
+			const int leaf = schg[c];
 			const int to = ssto[c];
-			if (!inside_band(to, L)) continue;
 			int f = 0;
 			while (c >= coff[f + 1]) f++;
-			if (to + L != f) slkp[schg[c]] = snew[schg[c]];
+			lkp[leaf] = !inside_band(to, L) ? NUL16 : (to + L != f ? snew[leaf] : slkp[leaf]);
 		}
-		if (threadIdx.x < NL) P.app[gp * NL + threadIdx.x] = appb[threadIdx.x];
+		if (threadIdx.x < NL) {
+			P.app[gp * NL + threadIdx.x] = appb[threadIdx.x];
+			P.lcnt[sl * NL + threadIdx.x] = cnt[threadIdx.x];
+		}
 		if (threadIdx.x == 0) {
 			P.rem[gp] = remb;
 			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)total);
@@ -682,24 +754,19 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 			}
 		}
 		__syncthreads();
-		for (int l = 0; l < NL; l++) {
-			uint16_t* dst = P.lst + ((size_t)sl * NL + l) * bv;
-			for (int i = threadIdx.x; i < cnt[l]; i += blockDim.x)
-				dst[i] = (uint16_t)(slst[l * bv + i] & ~TAG);
-			if (threadIdx.x == 0) P.lcnt[sl * NL + l] = cnt[l];
-		}
-		for (int i = threadIdx.x; i < BV; i += blockDim.x) P.lkp[sl * bv + i] = slkp[i];
-		__syncthreads();
 	}
 }
 
 /// Children-level half of the flush: one warp per (surface, list k) replays, in the reference's
 /// order (from-layer ascending, then status partition list order), the appends to list k and
-/// the swap-with-last removals from it (LookupMixin.hpp:483-556).
+/// the swap-with-last removals from it (LookupMixin.hpp:483-556). The events only read the leaf
+/// flush's records (app, rem), which this kernel does not change, so AHEAD chunks of them are
+/// loaded together before their (rare) events are replayed in order.
 template <int L>
 __global__ void k_flush_plist(Dev P)
 {
 	constexpr int NL = 2 * L + 1;
+	constexpr int AHEAD = 4;
 	const int lane = lane_id();
 	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (w >= P.S * NL) return;
@@ -710,44 +777,56 @@ __global__ void k_flush_plist(Dev P)
 	for (int fi = 0; fi < NL; fi++) {
 		const int ns = P.spcnt[s * NL + fi];
 		const int* sp = P.splist + (size_t)fi * P.NP + g.pbase;
-		for (int base = 0; base < ns; base += 32) {
-			const int i = base + lane;
-			int lp = 0, ev = 0;
-			if (i < ns) {
-				lp = sp[i];
-				const int gp = g.pbase + lp;
-				if (fi == k)
-					ev = ((P.rem[gp] >> k) & 1u) ? 2 : 0;
-				else
-					ev = ((P.app[gp * NL + fi] >> k) & 1u) ? 1 : 0;
+		for (int base = 0; base < ns; base += 32 * AHEAD) {
+			int lpa[AHEAD], eva[AHEAD];
+#pragma unroll
+			for (int u = 0; u < AHEAD; u++) {
+				const int i = base + 32 * u + lane;
+				lpa[u] = i < ns ? sp[i] : 0;
 			}
-			unsigned m = __ballot_sync(FULL, ev != 0);
-			while (m) {
-				const int src = __ffs(m) - 1;
-				m &= m - 1;
-				const int lps = __shfl_sync(FULL, lp, src);
-				const int evs = __shfl_sync(FULL, ev, src);
-				if (lane == 0) {
-					const int gp = g.pbase + lps;
-					int* at = &P.ppos[gp * NL + k];
-					if (evs == 1) {
-						if (*at < 0) {
-							pl[cnt] = lps;
-							*at = cnt;
-							cnt++;
-						}
-					} else if (*at >= 0) {
-						const int last = cnt - 1;
-						if (*at < last) {
-							const int mv = pl[last];
-							pl[*at] = mv;
-							P.ppos[(g.pbase + mv) * NL + k] = *at;
-						}
-						*at = -1;
-						cnt = last;
-					}
+#pragma unroll
+			for (int u = 0; u < AHEAD; u++) {
+				const int i = base + 32 * u + lane;
+				int ev = 0;
+				if (i < ns) {
+					const int gp = g.pbase + lpa[u];
+					if (fi == k)
+						ev = ((P.rem[gp] >> k) & 1u) ? 2 : 0;
+					else
+						ev = ((P.app[gp * NL + fi] >> k) & 1u) ? 1 : 0;
 				}
-				__syncwarp();
+				eva[u] = ev;
+			}
+#pragma unroll
+			for (int u = 0; u < AHEAD; u++) {
+				unsigned m = __ballot_sync(FULL, eva[u] != 0);
+				while (m) {
+					const int src = __ffs(m) - 1;
+					m &= m - 1;
+					const int lp = __shfl_sync(FULL, lpa[u], src);
+					const int ev = __shfl_sync(FULL, eva[u], src);
+					if (lane == 0) {
+						const int gp = g.pbase + lp;
+						int* at = &P.ppos[gp * NL + k];
+						if (ev == 1) {
+							if (*at < 0) {
+								pl[cnt] = lp;
+								*at = cnt;
+								cnt++;
+							}
+						} else if (*at >= 0) {
+							const int last = cnt - 1;
+							if (*at < last) {
+								const int mv = pl[last];
+								pl[*at] = mv;
+								P.ppos[(g.pbase + mv) * NL + k] = *at;
+							}
+							*at = -1;
+							cnt = last;
+						}
+					}
+					__syncwarp();
+				}
 			}
 		}
 	}

@@ -286,24 +286,33 @@ __global__ void k_polys_notify(Dev P, PolysDev Q)
 		const int li = (pass & 1) ? NL - 1 : 0;
 		const int n = status ? P.spcnt[s * NL + li] : P.dpcnt[s * NL + li];
 		const int* src = (status ? P.splist : P.dplist) + (size_t)li * P.NP + g.pbase;
-		for (int base = 0; base < n; base += 32) {
-			const int i = base + lane;
-			int lp = 0, gp = 0;
-			bool app = false, rem = false;
-			if (i < n) {
-				lp = src[i];
-				gp = g.pbase + lp;
-				const bool in = lkp[gp] >= 0;
-				if (status) {
-					app = Q.pact[gp] && !in;
-				} else {
-					bool act = Q.pact[gp] != 0;
-					for (int lj = 0; !act && lj <= NL; lj += NL - 1)
-						act = P.ppos[gp * NL + lj] >= 0;
-					app = act && !in;
-					rem = !act && in;
-				}
+		// decisions of entry i; a list holds a partition once, so the pending-list membership
+		// read for the next chunk stays valid while this chunk's edits are applied
+		auto decide = [&](int i, int& lp, int& gp, bool& app, bool& rem) {
+			lp = 0;
+			gp = 0;
+			app = rem = false;
+			if (i >= n) return;
+			lp = src[i];
+			gp = g.pbase + lp;
+			const bool in = lkp[gp] >= 0;
+			if (status) {
+				app = Q.pact[gp] && !in;
+			} else {
+				bool act = Q.pact[gp] != 0;
+				for (int lj = 0; !act && lj <= NL; lj += NL - 1)
+					act = P.ppos[gp * NL + lj] >= 0;
+				app = act && !in;
+				rem = !act && in;
 			}
+		};
+		int lpn, gpn;
+		bool apn, rmn;
+		decide(lane, lpn, gpn, apn, rmn);
+		for (int base = 0; base < n; base += 32) {
+			const int lp = lpn, gp = gpn;
+			const bool app = apn, rem = rmn;
+			decide(base + 32 + lane, lpn, gpn, apn, rmn);
 			unsigned ma = __ballot_sync(FULL, app), mr = __ballot_sync(FULL, rem);
 			while (ma | mr) {
 				const int r = mr ? __ffs(mr) - 1 : 32;
