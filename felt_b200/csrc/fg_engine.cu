@@ -249,6 +249,7 @@ public:
 			                             (int)smem_halo_));
 		}
 		dist_split_ = BV >= 4096 ? 4 : BV >= 1024 ? 2 : 1;
+		block_passes_ = BV >= 2048;
 		smem_flush_ = flush_smem_bytes(BV, NL);
 		if (smem_flush_ <= 200 * 1024) {
 			if (smem_flush_ > 48 * 1024)
@@ -343,7 +344,7 @@ public:
 		// update_zero_layer(&affected_buffer)
 		scan(P_.pcnt, L, 0);
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
-		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, iso, nullptr, B););
+		zero_apply(iso, nullptr, B);
 		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.plist, L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(iso, B);
@@ -503,7 +504,7 @@ public:
 		// over the affected lists (update_distance(plookup = affected, buffer))
 		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
 		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
-		FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, aff, P_.dlcnt, B););
+		zero_apply(aff, P_.dlcnt, B);
 		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.aplist[A], L, B););
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(aff, B);
@@ -797,8 +798,20 @@ private:
 	{
 		const int* woff = P_.woffl + (size_t)(k + L) * (P_.S + 1);
 		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, side, dist_split_););
-		FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
+		if (block_passes_)
+			FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
+		else
+			FG_RUN("k_dist2", st_, k_dist2_warp<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
 		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, woff, lv.plist, k + L, b););
+	}
+
+	/// update_zero_layer: block-per-partition for large bricks, warp-per-partition for small ones.
+	void zero_apply(const ListView& lv, const int* ncount, int b)
+	{
+		if (block_passes_)
+			FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, ncount, b););
+		else
+			FG_RUN("k_zero_apply", st_, k_zero_apply_warp<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, ncount, b););
 	}
 
 	void flush()
@@ -870,6 +883,9 @@ private:
 	int lcap_ = 0;
 	int warp_grid_ = 0;
 	int dist_split_ = 1;  // warps per partition entry in the first distance pass
+	// whole blocks (not warps) per partition entry in the record-keeping passes: pays off when
+	// a brick holds thousands of leaves, costs idle threads when it holds a few hundred
+	bool block_passes_ = false;
 	bool status_dirty_ = false;
 	bool buf_dirty_[2] = {false, false};
 	static constexpr int kMaxIterations = 64;

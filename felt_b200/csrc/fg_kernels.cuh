@@ -180,6 +180,34 @@ __device__ __forceinline__ unsigned warp_or(unsigned v)
 	return v;
 }
 
+/// The status records of one block-wide round over a partition's list: the block's changed
+/// leaves (ch: to != from) are compacted in list order into shared memory, and warp 0 records
+/// them 32 at a time with status_chunk, which keeps the reference's order. Every thread of the
+/// block calls it; flags and any_change accumulate in warp 0.
+template <int L>
+__device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int from, bool ch,
+                                             int leaf, int to, int b, unsigned& flags,
+                                             bool& any_change, uint16_t* cl, int* ct)
+{
+	if (!__syncthreads_or(ch)) return;
+	int tot;
+	const int pos = block_excl_scan(ch ? 1 : 0, &tot);
+	if (ch) {
+		cl[pos] = (uint16_t)leaf;
+		ct[pos] = to;
+	}
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		for (int c0 = 0; c0 < tot; c0 += 32) {
+			const int c = c0 + (int)threadIdx.x;
+			const bool v = c < tot;
+			status_chunk<L>(P, gp, sl, from, v, v ? cl[c] : 0, v ? ct[c] : from, b, flags,
+			                any_change);
+		}
+	}
+	__syncthreads();
+}
+
 // ---------------------------------------------------------------------------------------------
 // update(fn) functor loop (Surface.hpp:263-294) with a builtin speed: delta of every zero-layer
 // leaf, written to the brick's delta array.
@@ -299,9 +327,50 @@ __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
 }
 
 /// update_zero_layer (Surface.hpp:920-979) over the isogrid's zero-layer lists, which the delta
-/// grid mirrors in the global update.
+/// grid mirrors in the global update. One block per partition entry (bricks of thousands of
+/// leaves): every thread applies one leaf, and the rare layer changes are recorded in list order
+/// (status_round).
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const int* ncount, int b)
+{
+	constexpr int NL = 2 * L + 1;
+	__shared__ uint16_t cl[256];
+	__shared__ int ct[256];
+	const int total = P.woff[P.S];
+	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+		const int s = entry_surface(P.woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const int gp = g.pbase + lv.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
+		const int sl = P.slot[gp];
+		// the delta grid's zero-layer leaves: the isogrid list in the global update, a prefix of
+		// the affected list (the delta() calls' leaves) in the local update
+		const int n = ncount ? ncount[sl] : lv.lcnt[sl * NL + L];
+		const uint16_t* lst = lv.lst + ((size_t)sl * NL + L) * P.BV;
+		const size_t b0 = (size_t)sl * P.BV;
+		unsigned flags = 0;
+		bool any = false;
+		for (int base = 0; base < n; base += blockDim.x) {
+			const int j = base + threadIdx.x;
+			int leaf = 0, to = 0;
+			if (j < n) {
+				leaf = lst[j];
+				const float nw = __fadd_rn(P.phi[b0 + leaf], P.dlt[b0 + leaf]);
+				to = layer_id(nw, P.err);
+				P.phi[b0 + leaf] = nw;
+			}
+			status_round<L>(P, gp, sl, 0, j < n && to != 0, leaf, to, b, flags, any, cl, ct);
+		}
+		if (threadIdx.x < 32) {
+			flags = warp_or(flags);
+			if (threadIdx.x == 0) P.eflag[e] = flags;
+		}
+	}
+}
+
+/// update_zero_layer (Surface.hpp:920-979) over the isogrid's zero-layer lists, which the delta
+/// grid mirrors in the global update. One warp per partition entry (bricks of few leaves).
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, const int* ncount, int b)
 {
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
@@ -373,11 +442,53 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView 
 	}
 }
 
-/// update_distance second pass (Surface.hpp:1075-1121): apply and record status changes.
-/// The next chunk's list entry and delta are loaded before the current chunk's status records
-/// (which must stay in list order), so the two load latencies overlap the record work.
+/// update_distance second pass (Surface.hpp:1075-1121): apply and record status changes. One
+/// block per partition entry (bricks of thousands of leaves): every thread commits one leaf,
+/// and the rare layer changes are recorded in list order (status_round).
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
+{
+	constexpr int NL = 2 * L + 1;
+	const int li = k + L;
+	__shared__ uint16_t cl[256];
+	__shared__ int ct[256];
+	const int total = woff[P.S];
+	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+		const int s = entry_surface(woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
+		const int sl = P.slot[gp];
+		const int n = lv.lcnt[sl * NL + li];
+		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
+		const size_t b0 = (size_t)sl * P.BV;
+		unsigned flags = 0;
+		bool any = false;
+		for (int base = 0; base < n; base += blockDim.x) {
+			const int j = base + threadIdx.x;
+			int leaf = 0, to = k;
+			if (j < n) {
+				leaf = lst[j];
+				const float d = P.dlt[b0 + leaf];
+				to = layer_id(d, P.err);
+				P.phi[b0 + leaf] = d;
+			}
+			status_round<L>(P, gp, sl, k, j < n && to != k, leaf, to, b, flags, any, cl, ct);
+		}
+		if (threadIdx.x < 32) {
+			flags = warp_or(flags);
+			if (threadIdx.x == 0) {
+				P.eflag[e] = flags;
+				if (any) atomicOr(P.changed, 1);
+			}
+		}
+	}
+}
+
+/// k_dist2 with one warp per partition entry (bricks of few leaves). The next chunk's list
+/// entry and delta are loaded before the current chunk's status records (which must stay in
+/// list order), so the two load latencies overlap the record work.
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, ListView lv, int k, int b)
 {
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
@@ -423,50 +534,64 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView 
 /// Appends, in the pass's partition order, the partitions that gained status changes to the
 /// status partition list of layer index `li`, and those newly tracked in buffer b's partition
 /// lists (the children-level track_child calls of status_change, PartitionedMixin.hpp:201-213).
-/// One block per surface; each of its warps owns whole lists (list t < NL: buffer list t,
-/// list NL: the status list) and ranks the entries that join it with ballots, so no block-wide
-/// barrier sits in the walk.
+/// One block per surface: the block stages a tile of the entries' flags in shared memory, then
+/// each warp owns whole lists (list t < NL: buffer list t, list NL: the status list) and ranks
+/// the entries that join it with ballots.
 template <int L>
 __global__ void __launch_bounds__(256) k_compact(Dev P, const int* woff, const int* plist, int li,
                                                  int b)
 {
 	constexpr int NL = 2 * L + 1;
+	constexpr int TILE = 2048;
+	__shared__ unsigned sf[TILE];
+	__shared__ int scnt[NL + 1];
 	const int s = blockIdx.x;
 	const SurfGeom& g = P.geom[s];
 	const int e0 = woff[s], e1 = woff[s + 1];
 	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const unsigned lt = (1u << lane) - 1u;
-	for (int t = warp; t <= NL; t += nwarps) {
-		const bool status = t == NL;
-		const unsigned bit = status ? 0x80000000u : (1u << t);
-		int cnt = status ? P.spcnt[s * NL + li] : P.apcnt[b][s * NL + t];
-		int* list = status ? P.splist + (size_t)li * P.NP + g.pbase
-		                   : P.aplist[b] + (size_t)t * P.NP + g.pbase;
-		for (int base = e0; base < e1; base += 32) {
-			const int e = base + lane;
-			const bool hit = e < e1 && (P.eflag[e] & bit);
-			const unsigned m = __ballot_sync(FULL, hit);
-			if (hit) {
-				const int lp = plist[(size_t)li * P.NP + g.pbase + (e - e0)];
-				const int gp = g.pbase + lp;
-				const int pos = cnt + __popc(m & lt);
-				list[pos] = lp;
-				if (status) {
-					P.sppos[gp * NL + li] = pos;
-					if (atomicExch(&P.sflag[gp], 1) == 0)
-						P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
-				} else {
-					P.appos[b][gp * NL + t] = pos;
+	if (threadIdx.x <= NL)
+		scnt[threadIdx.x] = threadIdx.x == NL ? P.spcnt[s * NL + li]
+		                                      : P.apcnt[b][s * NL + threadIdx.x];
+	for (int t0 = e0; t0 < e1; t0 += TILE) {
+		const int nt = min(TILE, e1 - t0);
+		__syncthreads();
+		for (int i = threadIdx.x; i < nt; i += blockDim.x) sf[i] = P.eflag[t0 + i];
+		__syncthreads();
+		for (int t = warp; t <= NL; t += nwarps) {
+			const bool status = t == NL;
+			const unsigned bit = status ? 0x80000000u : (1u << t);
+			int* list = status ? P.splist + (size_t)li * P.NP + g.pbase
+			                   : P.aplist[b] + (size_t)t * P.NP + g.pbase;
+			int cnt = scnt[t];
+			for (int base = 0; base < nt; base += 32) {
+				const int i = base + lane;
+				const bool hit = i < nt && (sf[i] & bit);
+				const unsigned m = __ballot_sync(FULL, hit);
+				if (hit) {
+					const int lp = plist[(size_t)li * P.NP + g.pbase + (t0 + i - e0)];
+					const int gp = g.pbase + lp;
+					const int pos = cnt + __popc(m & lt);
+					list[pos] = lp;
+					if (status) {
+						P.sppos[gp * NL + li] = pos;
+						if (atomicExch(&P.sflag[gp], 1) == 0)
+							P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
+					} else {
+						P.appos[b][gp * NL + t] = pos;
+					}
 				}
+				cnt += __popc(m);
 			}
-			cnt += __popc(m);
+			if (lane == 0) scnt[t] = cnt;
 		}
-		if (lane == 0) {
-			if (status)
-				P.spcnt[s * NL + li] = cnt;
-			else
-				P.apcnt[b][s * NL + t] = cnt;
-		}
+	}
+	__syncthreads();
+	if (threadIdx.x <= NL) {
+		if (threadIdx.x == NL)
+			P.spcnt[s * NL + li] = scnt[NL];
+		else
+			P.apcnt[b][s * NL + threadIdx.x] = scnt[threadIdx.x];
 	}
 }
 

@@ -883,9 +883,11 @@ private:
 			tv += nv[i];
 			ts += ns[i];
 		}
+		// 16x headroom over the live geometry: a march re-emits the geometry of the partitions
+		// it re-marches, so with less room a polygonisation every step compacts every step
 		long long vcap = grow ? 2 * Q_.vcap : Q_.vcap, scap = grow ? 2 * Q_.scap : Q_.scap;
-		while (tv * 4 > vcap) vcap *= 2;
-		while (ts * 4 > scap) scap *= 2;
+		while (tv * 16 > vcap) vcap *= 2;
+		while (ts * 16 > scap) scap *= 2;
 		if (vcap >= (1LL << 31) || scap >= (1LL << 31))
 			throw Error(-13, "polygonisation arena too large");
 		int* dno = nullptr;

@@ -23,8 +23,42 @@
 #include <limits>
 #include <stdexcept>
 #include <vector>
+#include <atomic>
+#include <exception>
+#include <thread>
 
 namespace fo {
+
+/// Threads of the loops the reference runs in parallel (set through fo_set_threads; 1 = the
+/// plain sequential order, which these loops do not depend on anyway).
+inline std::atomic<int> g_threads{1};
+
+/// fn(i) for i in [0, n): on g_threads threads taking indices in turn when the loop has enough
+/// items to pay for them, else inline. fn must only write state owned by item i.
+template <class Fn>
+void parallel_items(long n, Fn&& fn)
+{
+	const int nt = (int)std::min<long>(g_threads.load(), n / 8);
+	if (nt <= 1) {
+		for (long i = 0; i < n; i++) fn(i);
+		return;
+	}
+	std::atomic<long> next{0};
+	std::exception_ptr err;
+	std::atomic<bool> failed{false};
+	auto work = [&] {
+		try {
+			for (long i; (i = next.fetch_add(1)) < n && !failed.load();) fn(i);
+		} catch (...) {
+			if (!failed.exchange(true)) err = std::current_exception();
+		}
+	};
+	std::vector<std::thread> pool;
+	for (int t = 1; t < nt; t++) pool.emplace_back(work);
+	work();
+	for (auto& th : pool) th.join();
+	if (err) std::rethrow_exception(err);
+}
 
 using PosIdx = std::size_t;
 constexpr std::size_t NUL = std::numeric_limits<std::size_t>::max();
@@ -592,13 +626,17 @@ public:
 		update_start();
 		delta_.track_children(iso);
 		const std::vector<PosIdx>& parts = iso.clists[lidx(0)];
-		for (PosIdx pc : parts) {
+		// The reference runs this loop across OpenMP threads (Surface.hpp:284-292); each
+		// partition's leaves stay with one thread, so results and orders do not depend on the
+		// thread count.
+		parallel_items((long)parts.size(), [&](long i) {
+			const PosIdx pc = parts[(size_t)i];
 			for (PosIdx leaf : iso.ch[pc].lists[lidx(0)]) {
 				const Vi<D> pos = iso.pos_leaf(pc, leaf);
 				const Real d = fn(pos);
 				delta_.child_track(d, pc, leaf, lidx(0));
 			}
-		}
+		});
 		update_end_global();
 	}
 	void update(const Speed& s)
@@ -778,12 +816,15 @@ public:
 		bool changed = false;
 		const int li = lidx(id);
 		const std::vector<PosIdx> parts = g.clists[li];
-		for (PosIdx pc : parts) {
+		// first pass across threads, as the reference runs it (Surface.hpp:1028-1073):
+		// partition-local writes only, so the thread count changes nothing
+		parallel_items((long)parts.size(), [&](long i) {
+			const PosIdx pc = parts[(size_t)i];
 			for (PosIdx leaf : g.ch[pc].lists[li]) {
 				const Real d = distance(pc, leaf, side);
 				delta_.child_track(d, pc, leaf, li);
 			}
-		}
+		});
 		for (PosIdx pc : parts) {
 			const std::vector<PosIdx> leaves = g.ch[pc].lists[li];
 			for (PosIdx leaf : leaves) {

@@ -224,6 +224,14 @@ struct fo_speed {
 
 const char* fo_last_error(void) { return g_err.c_str(); }
 
+/// Threads of the parallel loops (the functor loop and the first distance pass); results do not
+/// depend on it. Returns the count in effect.
+int fo_set_threads(int n)
+{
+	if (n > 0) fo::g_threads.store(n);
+	return fo::g_threads.load();
+}
+
 int fo_surface_create(int dims, int layers, const int* size, const int* part, void** out)
 {
 	return guard([&] {

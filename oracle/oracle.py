@@ -42,7 +42,14 @@ def lib():
             build()
         _lib = C.CDLL(_LIB)
         _lib.fo_last_error.restype = C.c_char_p
+        _lib.fo_set_threads(1)  # results never depend on it; callers that time may raise it
     return _lib
+
+
+def set_threads(n):
+    """Threads of the oracle's parallel loops (the speed functor loop and the first distance
+    pass, which the reference runs with OpenMP). Returns the count in effect."""
+    return int(lib().fo_set_threads(int(n)))
 
 
 def _chk(rc):

@@ -123,3 +123,11 @@ def test_determinism_two_runs():
                         every=12)
     assert np.array_equal(g1.dump(), g2.dump())
     assert np.array_equal(g1.snapshot(), g2.snapshot())
+
+
+def test_c2_shaped_16cubed_bricks_L3():
+    """The headline workload's shape at a size the oracle finishes quickly: 16^3 partitions
+    (4096-leaf bricks: split first pass, block-per-partition record passes, windowed flush),
+    L=3, expansion then curvature + hashed noise."""
+    run_compare((96, 96, 96), (16, 16, 16), 3, [(0, 0, 0)],
+                [(20, dict(c=-1.0)), (16, dict(a=-0.2, n=0.1, seed=1234))], every=4)

@@ -78,6 +78,12 @@ def test_polys_2d_saddles_and_merge():
               [(12, dict(c=-0.55)), (8, dict(a=-0.4, c=0.15))], march_every=1)
 
 
+def test_polys_3d_16cubed_bricks_noise():
+    """16^3 bricks: the staged box of the march is 17^3 and most cells' corners lie inside it."""
+    run_polys((80, 80, 80), (16, 16, 16), 3, [(0, 0, 0)],
+              [(16, dict(c=-1.0)), (8, dict(a=-0.2, n=0.1, seed=99))], march_every=4)
+
+
 def test_polys_3d_uneven_partitions():
     run_polys((30, 18, 26), (16, 8, 16), 2, [(0, 0, 0)],
               [(7, dict(c=-0.8)), (4, dict(a=-0.3, c=-0.1))], march_every=1)
