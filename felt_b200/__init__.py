@@ -115,12 +115,12 @@ def make_speed(c=None, a=None, n=None, seed=0):
 class Surface:
     """Felt::Surface<D,L>(size, size_partition) on the GPU (include/Felt/Surface.hpp:163-173)."""
 
-    def __init__(self, size, part, layers, brick_capacity=0):
+    def __init__(self, size, part, layers, brick_capacity=0, vertex_capacity=0):
         self.D = len(size)
         self.L = int(layers)
         self.size = tuple(int(s) for s in size)
         self.part = tuple(int(p) for p in part)
-        cfg = Config(int(brick_capacity), 0, 0)
+        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
         h = C.c_void_p()
         _chk(lib().fg_surface_create(self.D, self.L, _ivec(size), _ivec(part), C.byref(cfg),
                                      C.byref(h)))
@@ -243,14 +243,14 @@ class Batch:
     """Many independent Surface<D,L> (same D, L, partition shape; any grid sizes) advanced by the
     same kernel launches. Per surface the results equal a separate Surface's."""
 
-    def __init__(self, sizes, part, layers, brick_capacity=0):
+    def __init__(self, sizes, part, layers, brick_capacity=0, vertex_capacity=0):
         self.n = len(sizes)
         self.D = len(part)
         self.L = int(layers)
         self.part = tuple(int(p) for p in part)
         self.sizes = [tuple(int(x) for x in s) for s in sizes]
         flat = [x for s in self.sizes for x in s]
-        cfg = Config(int(brick_capacity), 0, 0)
+        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
         h = C.c_void_p()
         _chk(lib().fg_batch_create(self.D, self.L, _ivec(part), C.c_size_t(self.n), _ivec(flat),
                                    C.byref(cfg), C.byref(h)))

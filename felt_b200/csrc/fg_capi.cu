@@ -84,6 +84,7 @@ int fg_surface_create(int dims, int layers, const int* size, const int* part, co
 		d.sizes.push_back(sz);
 		if (cfg) d.brick_capacity = cfg->brick_capacity;
 		auto s = std::make_unique<fg_surface>();
+		if (cfg) s->vertex_capacity = cfg->vertex_capacity;
 		FG_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
 		s->eng.reset(fg::make_engine(d, s->st));
 		*out = s.release();
@@ -316,7 +317,7 @@ int fg_polys_create(fg_surface* s, fg_polys** out)
 		need(out, "out");
 		auto p = std::make_unique<fg_polys>();
 		p->surf = s;
-		p->impl.reset(fg::make_polys(*s->eng, 0));
+		p->impl.reset(fg::make_polys(*s->eng, 0, s->vertex_capacity));
 		*out = p.release();
 	});
 }
@@ -414,6 +415,7 @@ int fg_batch_create(int dims, int layers, const int* part, size_t n, const int* 
 		}
 		if (cfg) d.brick_capacity = cfg->brick_capacity;
 		auto b = std::make_unique<fg_batch>();
+		if (cfg) b->vertex_capacity = cfg->vertex_capacity;
 		FG_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
 		b->eng.reset(fg::make_engine(d, b->st));
 		b->eng->set_throw_on_freeze(false);
@@ -468,7 +470,7 @@ int fg_batch_update(fg_batch* b, const fg_speed* speeds)
 
 static fg::PolysBase& batch_polys(fg_batch* b)
 {
-	if (!b->polys) b->polys.reset(fg::make_polys(*b->eng, 0));
+	if (!b->polys) b->polys.reset(fg::make_polys(*b->eng, 0, b->vertex_capacity));
 	return *b->polys;
 }
 

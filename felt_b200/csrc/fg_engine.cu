@@ -345,7 +345,7 @@ public:
 		scan(P_.pcnt, L, 0);
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		zero_apply(iso, nullptr, B);
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.plist, L, B););
+		defer_compact(P_.woff, P_.plist, L, B);
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(iso, B);
 		converge();
@@ -505,7 +505,7 @@ public:
 		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
 		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
 		zero_apply(aff, P_.dlcnt, B);
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, P_.woff, P_.aplist[A], L, B););
+		defer_compact(P_.woff, P_.aplist[A], L, B);
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(aff, B);
 		converge(true);
@@ -792,17 +792,36 @@ private:
 		FG_RUN("k_scan_layers", st_, k_scan_layers<<<1, 1024, 0, st_>>>(lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
 		for (int k = -1; k >= -L; k--) layer_pass(lv, k, -1.0f, b);
 		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
+		const CompactArgs ca = take_compact();
+		if (ca.nblocks)
+			FG_RUN("k_compact", st_, k_compact<L><<<ca.nblocks, 256, 0, st_>>>(P_, ca););
+	}
+
+	/// A pass's compaction waits to ride on the next first-pass launch (k_dist1).
+	void defer_compact(const int* woff, const int* plist, int li, int b)
+	{
+		const CompactArgs stale = take_compact();  // none is left behind on the normal path
+		if (stale.nblocks)
+			FG_RUN("k_compact", st_, k_compact<L><<<stale.nblocks, 256, 0, st_>>>(P_, stale););
+		pending_ = CompactArgs{P_.S, woff, plist, li, b};
+	}
+	CompactArgs take_compact()
+	{
+		const CompactArgs ca = pending_;
+		pending_ = CompactArgs{0, nullptr, nullptr, 0, 0};
+		return ca;
 	}
 
 	void layer_pass(const ListView& lv, int k, float side, int b)
 	{
 		const int* woff = P_.woffl + (size_t)(k + L) * (P_.S + 1);
-		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, side, dist_split_););
+		const CompactArgs ca = take_compact();
+		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_ + ca.nblocks, 256, 0, st_>>>(P_, woff, lv, k, side, dist_split_, ca););
 		if (block_passes_)
 			FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
 		else
 			FG_RUN("k_dist2", st_, k_dist2_warp<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
-		FG_RUN("k_compact", st_, k_compact<L><<<P_.S, 256, 0, st_>>>(P_, woff, lv.plist, k + L, b););
+		defer_compact(woff, lv.plist, k + L, b);
 	}
 
 	/// update_zero_layer: block-per-partition for large bricks, warp-per-partition for small ones.
@@ -883,6 +902,7 @@ private:
 	int lcap_ = 0;
 	int warp_grid_ = 0;
 	int dist_split_ = 1;  // warps per partition entry in the first distance pass
+	CompactArgs pending_{0, nullptr, nullptr, 0, 0};  // compaction riding on the next k_dist1
 	// whole blocks (not warps) per partition entry in the record-keeping passes: pays off when
 	// a brick holds thousands of leaves, costs idle threads when it holds a few hundred
 	bool block_passes_ = false;

@@ -11,6 +11,7 @@
 
 struct fg_surface {
 	std::unique_ptr<fg::EngineBase> eng;
+	size_t vertex_capacity = 0;  // initial polygonisation arena (fg_config)
 	cudaStream_t st = nullptr;
 	bool local_open = false;
 	std::vector<int> dpos;
@@ -29,6 +30,7 @@ struct fg_polys {
 
 struct fg_batch {
 	std::unique_ptr<fg::PolysBase> polys;  // destroyed before the engine it refers to
+	size_t vertex_capacity = 0;            // initial polygonisation arena (fg_config)
 	std::unique_ptr<fg::EngineBase> eng;
 	cudaStream_t st = nullptr;
 	~fg_batch()

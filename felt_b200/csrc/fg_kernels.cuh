@@ -403,22 +403,118 @@ __global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, con
 	}
 }
 
+/// Appends, in the pass's partition order, the partitions that gained status changes to the
+/// status partition list of layer index `li`, and those newly tracked in buffer b's partition
+/// lists (the children-level track_child calls of status_change, PartitionedMixin.hpp:201-213),
+/// for surface s, by one block. The block stages a tile of the entries' flags and partition
+/// indices in shared memory; each warp owns whole lists (list t < NL: buffer list t, list NL:
+/// the status list) and ranks the entries that join it with ballots (stores only, nothing
+/// waited on); then the whole block adds the tile's partitions with status changes to the
+/// flush's work queue (any order).
+struct CompactArgs {
+	int nblocks;        // blocks of the launch that compact (one per surface), 0 = none
+	const int* woff;    // entry offsets of the pass being compacted
+	const int* plist;   // its partition lists
+	int li;             // its layer index
+	int b;              // affected buffer its changes went to
+};
+
+template <int L>
+__device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	constexpr int TILE = 1024;
+	__shared__ unsigned sf[TILE];
+	__shared__ int slp[TILE];
+	__shared__ int scnt[NL + 1];
+	const int li = a.li, b = a.b;
+	const SurfGeom& g = P.geom[s];
+	const int e0 = a.woff[s], e1 = a.woff[s + 1];
+	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const unsigned lt = (1u << lane) - 1u;
+	if (threadIdx.x <= NL)
+		scnt[threadIdx.x] = threadIdx.x == NL ? P.spcnt[s * NL + li]
+		                                      : P.apcnt[b][s * NL + threadIdx.x];
+	for (int t0 = e0; t0 < e1; t0 += TILE) {
+		const int nt = min(TILE, e1 - t0);
+		__syncthreads();
+		for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+			const unsigned f = P.eflag[t0 + i];
+			sf[i] = f;
+			slp[i] = f ? a.plist[(size_t)li * P.NP + g.pbase + (t0 + i - e0)] : 0;
+		}
+		__syncthreads();
+		for (int t = warp; t <= NL; t += nwarps) {
+			const bool status = t == NL;
+			const unsigned bit = status ? 0x80000000u : (1u << t);
+			int* list = status ? P.splist + (size_t)li * P.NP + g.pbase
+			                   : P.aplist[b] + (size_t)t * P.NP + g.pbase;
+			int cnt = scnt[t];
+			for (int base = 0; base < nt; base += 32) {
+				const int i = base + lane;
+				const bool hit = i < nt && (sf[i] & bit);
+				const unsigned m = __ballot_sync(FULL, hit);
+				if (hit) {
+					const int lp = slp[i];
+					const int gp = g.pbase + lp;
+					const int pos = cnt + __popc(m & lt);
+					list[pos] = lp;
+					if (status)
+						P.sppos[gp * NL + li] = pos;
+					else
+						P.appos[b][gp * NL + t] = pos;
+				}
+				cnt += __popc(m);
+			}
+			if (lane == 0) scnt[t] = cnt;
+		}
+		for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+			if (!(sf[i] & 0x80000000u)) continue;
+			const int gp = g.pbase + slp[i];
+			if (atomicExch(&P.sflag[gp], 1) == 0)
+				P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x <= NL) {
+		if (threadIdx.x == NL)
+			P.spcnt[s * NL + li] = scnt[NL];
+		else
+			P.apcnt[b][s * NL + threadIdx.x] = scnt[threadIdx.x];
+	}
+}
+
+/// The compaction of one pass on its own launch, one block per surface.
+template <int L>
+__global__ void __launch_bounds__(256) k_compact(Dev P, CompactArgs a)
+{
+	compact_surface<L>(P, a, blockIdx.x);
+}
+
 /// update_distance first pass (Surface.hpp:1028-1073): distance of every leaf of layer k to
 /// the zero curve, into the delta array. The pass is bound by load latency, so each partition
 /// entry gets `split` warps that take interleaved 32-leaf chunks (large bricks: the fullest
 /// partitions no longer set the pass's length alone), and each lane takes two leaves per round
 /// so that their neighbour reads are in flight together. The order of the writes does not
-/// matter (Jacobi).
+/// matter (Jacobi). The launch's first ca.nblocks blocks compact the previous pass instead
+/// (compact_surface): that work only touches the previous pass's records and the status and
+/// buffer lists, none of which this pass reads, so it overlaps this pass instead of taking a
+/// launch of its own.
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
-                                               float side, int split)
+                                               float side, int split, CompactArgs ca)
 {
 	constexpr int NL = 2 * L + 1;
+	if ((int)blockIdx.x < ca.nblocks) {
+		compact_surface<L>(P, ca, blockIdx.x);
+		return;
+	}
 	const int li = k + L;
 	const int lane = lane_id();
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	const int nwarps = ((gridDim.x - ca.nblocks) * blockDim.x) >> 5;
 	const int total = woff[P.S] * split;
-	for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
+	for (int v = ((blockIdx.x - ca.nblocks) * blockDim.x + threadIdx.x) >> 5; v < total;
+	     v += nwarps) {
 		const int e = v / split, part = v - e * split;
 		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
@@ -528,70 +624,6 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 			P.eflag[e] = flags;
 			if (any) atomicOr(P.changed, 1);
 		}
-	}
-}
-
-/// Appends, in the pass's partition order, the partitions that gained status changes to the
-/// status partition list of layer index `li`, and those newly tracked in buffer b's partition
-/// lists (the children-level track_child calls of status_change, PartitionedMixin.hpp:201-213).
-/// One block per surface: the block stages a tile of the entries' flags in shared memory, then
-/// each warp owns whole lists (list t < NL: buffer list t, list NL: the status list) and ranks
-/// the entries that join it with ballots.
-template <int L>
-__global__ void __launch_bounds__(256) k_compact(Dev P, const int* woff, const int* plist, int li,
-                                                 int b)
-{
-	constexpr int NL = 2 * L + 1;
-	constexpr int TILE = 2048;
-	__shared__ unsigned sf[TILE];
-	__shared__ int scnt[NL + 1];
-	const int s = blockIdx.x;
-	const SurfGeom& g = P.geom[s];
-	const int e0 = woff[s], e1 = woff[s + 1];
-	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-	const unsigned lt = (1u << lane) - 1u;
-	if (threadIdx.x <= NL)
-		scnt[threadIdx.x] = threadIdx.x == NL ? P.spcnt[s * NL + li]
-		                                      : P.apcnt[b][s * NL + threadIdx.x];
-	for (int t0 = e0; t0 < e1; t0 += TILE) {
-		const int nt = min(TILE, e1 - t0);
-		__syncthreads();
-		for (int i = threadIdx.x; i < nt; i += blockDim.x) sf[i] = P.eflag[t0 + i];
-		__syncthreads();
-		for (int t = warp; t <= NL; t += nwarps) {
-			const bool status = t == NL;
-			const unsigned bit = status ? 0x80000000u : (1u << t);
-			int* list = status ? P.splist + (size_t)li * P.NP + g.pbase
-			                   : P.aplist[b] + (size_t)t * P.NP + g.pbase;
-			int cnt = scnt[t];
-			for (int base = 0; base < nt; base += 32) {
-				const int i = base + lane;
-				const bool hit = i < nt && (sf[i] & bit);
-				const unsigned m = __ballot_sync(FULL, hit);
-				if (hit) {
-					const int lp = plist[(size_t)li * P.NP + g.pbase + (t0 + i - e0)];
-					const int gp = g.pbase + lp;
-					const int pos = cnt + __popc(m & lt);
-					list[pos] = lp;
-					if (status) {
-						P.sppos[gp * NL + li] = pos;
-						if (atomicExch(&P.sflag[gp], 1) == 0)
-							P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
-					} else {
-						P.appos[b][gp * NL + t] = pos;
-					}
-				}
-				cnt += __popc(m);
-			}
-			if (lane == 0) scnt[t] = cnt;
-		}
-	}
-	__syncthreads();
-	if (threadIdx.x <= NL) {
-		if (threadIdx.x == NL)
-			P.spcnt[s * NL + li] = scnt[NL];
-		else
-			P.apcnt[b][s * NL + threadIdx.x] = scnt[threadIdx.x];
 	}
 }
 

@@ -614,6 +614,83 @@ __global__ void k_polys_gather(PolysDev Q, const int* job, const long long* dst,
 	}
 }
 
+/// Arena compaction offsets, step 1: per chunk of ARENA_CHUNK partitions, the sums of their
+/// vertex and simplex counts.
+constexpr int ARENA_CHUNK = 4096;
+__global__ void __launch_bounds__(256) k_arena_chunk_sums(PolysDev Q, int NP,
+                                                          unsigned long long* csum)
+{
+	const int c0 = blockIdx.x * ARENA_CHUNK, c1 = min(NP, c0 + ARENA_CHUNK);
+	unsigned long long v = 0, s = 0;
+	for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+		v += (unsigned long long)Q.gnv[i];
+		s += (unsigned long long)Q.gns[i];
+	}
+	__shared__ unsigned long long rv[256], rs[256];
+	rv[threadIdx.x] = v;
+	rs[threadIdx.x] = s;
+	__syncthreads();
+	for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+		if ((int)threadIdx.x < o) {
+			rv[threadIdx.x] += rv[threadIdx.x + o];
+			rs[threadIdx.x] += rs[threadIdx.x + o];
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		csum[2 * blockIdx.x] = rv[0];
+		csum[2 * blockIdx.x + 1] = rs[0];
+	}
+}
+
+/// Step 2: exclusive scan of the chunk sums in place (one thread; there are NP / 4096 chunks)
+/// and the totals.
+__global__ void k_arena_chunk_scan(unsigned long long* csum, int nchunks, unsigned long long* tot)
+{
+	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	unsigned long long v = 0, s = 0;
+	for (int c = 0; c < nchunks; c++) {
+		const unsigned long long a = csum[2 * c], b = csum[2 * c + 1];
+		csum[2 * c] = v;
+		csum[2 * c + 1] = s;
+		v += a;
+		s += b;
+	}
+	tot[0] = v;
+	tot[1] = s;
+}
+
+/// Step 3: every partition's new vertex and simplex offsets (exclusive scan of the counts in
+/// partition order, the order the host-side compaction used).
+__global__ void __launch_bounds__(256) k_arena_offsets(PolysDev Q, int NP,
+                                                       const unsigned long long* csum,
+                                                       int* noff, int* nsoff)
+{
+	constexpr int PER = ARENA_CHUNK / 256;
+	const int c0 = blockIdx.x * ARENA_CHUNK;
+	const int i0 = c0 + threadIdx.x * PER;
+	int v = 0, s = 0;
+	for (int k = 0; k < PER; k++) {
+		const int i = i0 + k;
+		if (i < NP) {
+			v += Q.gnv[i];
+			s += Q.gns[i];
+		}
+	}
+	int tv, ts;
+	const int ev = block_excl_scan(v, &tv);
+	const int es = block_excl_scan(s, &ts);
+	long long ov = (long long)csum[2 * blockIdx.x] + ev, os = (long long)csum[2 * blockIdx.x + 1] + es;
+	for (int k = 0; k < PER; k++) {
+		const int i = i0 + k;
+		if (i >= NP) break;
+		noff[i] = (int)ov;
+		nsoff[i] = (int)os;
+		ov += Q.gnv[i];
+		os += Q.gns[i];
+	}
+}
+
 /// Moves the live geometry of every partition to the front of a fresh arena.
 template <int D>
 __global__ void k_polys_compact(Dev P, PolysDev Q, const int* noff, const int* nsoff, float* vtx2,
@@ -637,7 +714,7 @@ class PolysImpl final : public PolysBase {
 public:
 	static constexpr int VF = D == 3 ? 2 * D : D;
 
-	PolysImpl(EngineBase& eng, int s) : eng_(eng), s_(s)
+	PolysImpl(EngineBase& eng, int s, size_t vertex_capacity) : eng_(eng), s_(s)
 	{
 		const Dev& P = eng.dev();
 		auto al = [&](size_t bytes) {
@@ -670,13 +747,24 @@ public:
 		Q_.err = P.err;
 		Q_.ovf = (int*)al(sizeof(int));
 		Q_.vstart = (unsigned long long*)al(sizeof(unsigned long long));
+		nchunks_ = (P.NP + ARENA_CHUNK - 1) / ARENA_CHUNK;
+		noff_ = (int*)al(P.NP * sizeof(int));
+		nsoff_ = (int*)al(P.NP * sizeof(int));
+		csum_ = (unsigned long long*)al(2 * (size_t)nchunks_ * sizeof(unsigned long long));
+		ctot_ = (unsigned long long*)al(2 * sizeof(unsigned long long));
 		Q_.pend = 0;
-		alloc_arena(1 << 20, 2 << 20);
+		const long long vc = vertex_capacity ? std::max<long long>((long long)vertex_capacity, 64)
+		                                     : (1LL << 20);
+		if (vc >= (1LL << 30)) throw Error(-1, "vertex capacity too large");
+		alloc_arena(vc, 2 * vc);
 		int bvol = 1;
 		for (int a = 0; a < D; a++) bvol *= eng.part(a) + 1;
 		smem_ = (size_t)bvol * (D * sizeof(int) + sizeof(float)) +
 		        3 * (size_t)P.BV * sizeof(uint16_t);
 		smem_ = (smem_ + 15) & ~(size_t)15;
+		// threads per marched partition: a block per partition, sized to its cells (a 2D 16^2
+		// brick has a few dozen band cells, a 3D 16^3 brick thousands)
+		march_threads_ = P.BV >= 2048 ? 256 : P.BV >= 512 ? 128 : 64;
 		if (smem_ > 48 * 1024)
 			FG_CUDA(cudaFuncSetAttribute(k_polys_march<D, L>,
 			                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
@@ -687,6 +775,8 @@ public:
 	{
 		cudaStreamSynchronize(eng_.stream());
 		free_arena();
+		if (spare_v_) cudaFree(spare_v_);
+		if (spare_s_) cudaFree(spare_s_);
 		for (void* p : owned_) cudaFree(p);
 		if (stage_) cudaFree(stage_);
 	}
@@ -714,7 +804,7 @@ public:
 		// arena space is simply repeated after the arena has grown.
 		for (int attempt = 0;; attempt++) {
 			begin_attempt(attempt);
-			FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid(), 256, smem_, st>>>(P, Q_, woff_, -1););
+			FG_RUN("k_polys_march", st, k_polys_march<D, L><<<grid() * (256 / march_threads_), march_threads_, smem_, st>>>(P, Q_, woff_, -1););
 			FG_CUDA(cudaGetLastError());
 			if (!overflowed()) break;
 			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
@@ -733,7 +823,7 @@ public:
 		const int gp = check_part(part);
 		for (int attempt = 0;; attempt++) {
 			begin_attempt(attempt);
-			FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, 256, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
+			FG_RUN("k_polys_march", eng_.stream(), k_polys_march<D, L><<<1, march_threads_, smem_, eng_.stream()>>>(P, Q_, woff_, gp););
 			FG_CUDA(cudaGetLastError());
 			if (!overflowed()) break;
 			if (attempt > 8) throw Error(-13, "polygonisation arena cannot grow further");
@@ -864,25 +954,25 @@ private:
 		Q_.spx = nullptr;
 	}
 	/// Keeps the bump-allocated arenas at most half full before a march by moving the live
-	/// geometry into fresh arenas (doubling them when the live part alone is over a quarter).
+	/// geometry to the front of the other arena (kept between compactions, regrown when the
+	/// live part needs more than 1/16 of it). The new offsets are scanned on the device; the
+	/// host only reads the two totals.
 	void maybe_compact(bool grow)
 	{
 		const Dev& P = eng_.dev();
+		cudaStream_t st = eng_.stream();
 		unsigned long long used[2];
-		FG_CUDA(cudaMemcpyAsync(used, Q_.used, sizeof(used), cudaMemcpyDeviceToHost,
-		                        eng_.stream()));
+		FG_CUDA(cudaMemcpyAsync(used, Q_.used, sizeof(used), cudaMemcpyDeviceToHost, st));
 		eng_.sync();
 		if (!grow && (long long)used[0] * 2 < Q_.vcap && (long long)used[1] * 2 < Q_.scap) return;
-		std::vector<int> nv(P.NP), ns(P.NP), no(P.NP), so(P.NP);
-		FG_CUDA(cudaMemcpy(nv.data(), Q_.gnv, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
-		FG_CUDA(cudaMemcpy(ns.data(), Q_.gns, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
-		long long tv = 0, ts = 0;
-		for (int i = 0; i < P.NP; i++) {
-			no[i] = (int)tv;
-			so[i] = (int)ts;
-			tv += nv[i];
-			ts += ns[i];
-		}
+		FG_RUN("k_arena_chunk_sums", st, k_arena_chunk_sums<<<nchunks_, 256, 0, st>>>(Q_, P.NP, csum_););
+		FG_RUN("k_arena_chunk_scan", st, k_arena_chunk_scan<<<1, 32, 0, st>>>(csum_, nchunks_, ctot_););
+		FG_RUN("k_arena_offsets", st, k_arena_offsets<<<nchunks_, 256, 0, st>>>(Q_, P.NP, csum_, noff_, nsoff_););
+		FG_CUDA(cudaGetLastError());
+		unsigned long long tot[2];
+		FG_CUDA(cudaMemcpyAsync(tot, ctot_, sizeof(tot), cudaMemcpyDeviceToHost, st));
+		eng_.sync();
+		const long long tv = (long long)tot[0], ts = (long long)tot[1];
 		// 16x headroom over the live geometry: a march re-emits the geometry of the partitions
 		// it re-marches, so with less room a polygonisation every step compacts every step
 		long long vcap = grow ? 2 * Q_.vcap : Q_.vcap, scap = grow ? 2 * Q_.scap : Q_.scap;
@@ -890,33 +980,33 @@ private:
 		while (ts * 16 > scap) scap *= 2;
 		if (vcap >= (1LL << 31) || scap >= (1LL << 31))
 			throw Error(-13, "polygonisation arena too large");
-		int* dno = nullptr;
-		int* dso = nullptr;
-		float* v2 = nullptr;
-		uint32_t* s2 = nullptr;
-		FG_CUDA(cudaMalloc(&dno, P.NP * sizeof(int)));
-		FG_CUDA(cudaMalloc(&dso, P.NP * sizeof(int)));
-		FG_CUDA(cudaMalloc(&v2, (size_t)vcap * VF * sizeof(float)));
-		FG_CUDA(cudaMalloc(&s2, (size_t)scap * D * sizeof(uint32_t)));
-		FG_CUDA(cudaMemcpy(dno, no.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
-		FG_CUDA(cudaMemcpy(dso, so.data(), P.NP * sizeof(int), cudaMemcpyHostToDevice));
-		FG_RUN("k_polys_compact", eng_.stream(), k_polys_compact<D><<<grid(), 256, 0, eng_.stream()>>>(P, Q_, dno, dso, v2, s2););
+		if (spare_vcap_ < vcap) {
+			if (spare_v_) cudaFree(spare_v_);
+			spare_v_ = nullptr;
+			spare_vcap_ = 0;
+			FG_CUDA(cudaMalloc(&spare_v_, (size_t)vcap * VF * sizeof(float)));
+			spare_vcap_ = vcap;
+		}
+		if (spare_scap_ < scap) {
+			if (spare_s_) cudaFree(spare_s_);
+			spare_s_ = nullptr;
+			spare_scap_ = 0;
+			FG_CUDA(cudaMalloc(&spare_s_, (size_t)scap * D * sizeof(uint32_t)));
+			spare_scap_ = scap;
+		}
+		FG_RUN("k_polys_compact", st, k_polys_compact<D><<<grid(), 256, 0, st>>>(P, Q_, noff_, nsoff_, spare_v_, spare_s_););
 		FG_CUDA(cudaGetLastError());
-		FG_CUDA(cudaMemcpyAsync(Q_.gvoff, dno, P.NP * sizeof(int), cudaMemcpyDeviceToDevice,
-		                        eng_.stream()));
-		FG_CUDA(cudaMemcpyAsync(Q_.gsoff, dso, P.NP * sizeof(int), cudaMemcpyDeviceToDevice,
-		                        eng_.stream()));
-		const unsigned long long nu[2] = {(unsigned long long)tv, (unsigned long long)ts};
-		FG_CUDA(cudaMemcpyAsync(Q_.used, nu, sizeof(nu), cudaMemcpyHostToDevice, eng_.stream()));
-		eng_.sync();
-		free_arena();
-		Q_.vtx = v2;
-		Q_.spx = s2;
-		Q_.vcap = vcap;
-		Q_.scap = scap;
-		cudaFree(dno);
-		cudaFree(dso);
+		FG_CUDA(cudaMemcpyAsync(Q_.gvoff, noff_, P.NP * sizeof(int), cudaMemcpyDeviceToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(Q_.gsoff, nsoff_, P.NP * sizeof(int), cudaMemcpyDeviceToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(Q_.used, ctot_, 2 * sizeof(unsigned long long),
+		                        cudaMemcpyDeviceToDevice, st));
+		// the old arena becomes the spare
+		std::swap(Q_.vtx, spare_v_);
+		std::swap(Q_.spx, spare_s_);
+		std::swap(Q_.vcap, spare_vcap_);
+		std::swap(Q_.scap, spare_scap_);
 	}
+
 
 public:
 	void select(int s) override
@@ -1003,16 +1093,25 @@ private:
 	void* stage_ = nullptr;  // gather staging buffer
 	size_t stage_cap_ = 0;
 	size_t smem_ = 0;
+	int march_threads_ = 256;
+	int nchunks_ = 0;                        // arena compaction: chunks of partitions
+	int* noff_ = nullptr;                    // [NP] new vertex offsets
+	int* nsoff_ = nullptr;                   // [NP] new simplex offsets
+	unsigned long long* csum_ = nullptr;     // [2 * nchunks] chunk sums, then their scan
+	unsigned long long* ctot_ = nullptr;     // [2] live vertices, simplices
+	float* spare_v_ = nullptr;               // the other vertex arena
+	uint32_t* spare_s_ = nullptr;            // the other simplex arena
+	long long spare_vcap_ = 0, spare_scap_ = 0;
 	std::vector<void*> owned_;
 };
 
 }  // namespace
 
-PolysBase* make_polys(EngineBase& eng, int s)
+PolysBase* make_polys(EngineBase& eng, int s, size_t vertex_capacity)
 {
 	const int D = eng.dims(), L = eng.layers();
 #define FG_CASE(d, l) \
-	if (D == d && L == l) return new PolysImpl<d, l>(eng, s);
+	if (D == d && L == l) return new PolysImpl<d, l>(eng, s, vertex_capacity);
 	FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
 	FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
 #undef FG_CASE

@@ -29,7 +29,8 @@ public:
 	                    size_t scap, uint32_t* counts, size_t* nv, size_t* ns) = 0;
 };
 
-/// Polygonisation of surface s of an engine's pool.
-PolysBase* make_polys(EngineBase& eng, int s);
+/// Polygonisation of surface s of an engine's pool. vertex_capacity: initial vertex arena
+/// (simplex arena twice that), 0 = 2^20; the arenas grow on demand.
+PolysBase* make_polys(EngineBase& eng, int s, size_t vertex_capacity = 0);
 
 }  // namespace fg

@@ -64,8 +64,9 @@ typedef struct fg_speed {
 
 typedef struct fg_config {
 	size_t brick_capacity; /* bricks (partitions) the device pool can hold; 0 = automatic   */
-	size_t vertex_capacity;/* polygonisation arena, vertices; 0 = automatic                 */
-	int use_graph;         /* capture the global update step as a CUDA graph when nonzero   */
+	size_t vertex_capacity;/* initial polygonisation arena, vertices (simplices: twice that);
+	                          0 = 2^20; it grows on demand                                  */
+	int use_graph;         /* reserved, must be 0                                          */
 	int reserved[7];
 } fg_config;
 

@@ -34,9 +34,9 @@ def compare_polys(gp, op, nparts, where):
             assert err <= VTX_TOL, f"{where}: partition {p} vertex error {err}"
 
 
-def run_polys(size, part, L, seeds, schedule, march_every=1, invalidate_at=()):
+def run_polys(size, part, L, seeds, schedule, march_every=1, invalidate_at=(), vertex_capacity=0):
     fb = _fb()
-    g = fb.Surface(size, part, L)
+    g = fb.Surface(size, part, L, vertex_capacity=vertex_capacity)
     o = O.Surface(size, part, L)
     gp = fb.Polys(g)
     op = O.Polys(o)
@@ -82,6 +82,15 @@ def test_polys_3d_16cubed_bricks_noise():
     """16^3 bricks: the staged box of the march is 17^3 and most cells' corners lie inside it."""
     run_polys((80, 80, 80), (16, 16, 16), 3, [(0, 0, 0)],
               [(16, dict(c=-1.0)), (8, dict(a=-0.2, n=0.1, seed=99))], march_every=4)
+
+
+def test_polys_arena_growth_and_compaction():
+    """A 64-vertex initial arena: marches overflow and are retried after growth, and the arena
+    is compacted (device-side offsets, alternating arenas) many times; the geometry stays the
+    oracle's."""
+    run_polys((40, 40, 40), (8, 8, 8), 2, [(0, 0, 0)],
+              [(10, dict(c=-1.0)), (10, dict(a=-0.3, n=0.2, seed=5, c=-0.1))], march_every=1,
+              vertex_capacity=64)
 
 
 def test_polys_3d_uneven_partitions():
