@@ -191,6 +191,7 @@ class SingleWork:
         self.s.seed((0,) * cfg["D"])
         for _ in range(cfg["expand"]):
             self.s.update(c=-1.0)
+        self._pinned()
 
     def step(self, i, last=False):
         c = self.cfg
@@ -212,9 +213,18 @@ class SingleWork:
 
     def fetch_geometry(self):
         """D2H of the polygons of the partitions re-marched last (what a viewer would read),
-        in one gather call."""
-        vtx, spx, _ = self.p.gather(self.p.changes())
+        in one gather call, into pinned host buffers kept between steps."""
+        vtx, spx, _ = self.p.gather(self.p.changes(), *self._pinned())
         return vtx.nbytes + spx.nbytes
+
+    def _pinned(self, vfloats=16 << 20, sints=24 << 20):
+        """Pinned destination arrays (grown by the gather's own fallback if ever too small)."""
+        if getattr(self, "_pv", None) is None:
+            import torch
+            self._pv = torch.empty(vfloats, dtype=torch.float32, pin_memory=True).numpy()
+            self._ps = torch.empty(sints, dtype=torch.int32, pin_memory=True).numpy().view(
+                "uint32")
+        return self._pv, self._ps
 
 
 class BatchWork:

@@ -410,8 +410,10 @@ class Polys:
         _chk(lib().fg_polys_totals(self._h, C.byref(nv), C.byref(ns)))
         return nv.value, ns.value
 
-    def gather(self, parts):
-        """Vertices and simplices of several partitions in one call: (vtx, spx, counts)."""
+    def gather(self, parts, vtx_out=None, spx_out=None):
+        """Vertices and simplices of several partitions in one call: (vtx, spx, counts).
+        vtx_out / spx_out: optional flat float32 / uint32 arrays to copy into (e.g. views of
+        pinned host memory kept between calls); they are used when large enough."""
         D = self.surface.D
         per = 2 * D if D == 3 else D
         parts = list(parts)
@@ -423,8 +425,11 @@ class Polys:
                                    None, C.c_size_t(0),
                                    counts.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(nv),
                                    C.byref(ns)))
-        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
-        spx = np.zeros(max(1, ns.value * D), dtype=np.uint32)
+        need_v, need_s = max(1, nv.value * per), max(1, ns.value * D)
+        vtx = vtx_out if vtx_out is not None and vtx_out.size >= need_v else np.zeros(
+            need_v, dtype=np.float32)
+        spx = spx_out if spx_out is not None and spx_out.size >= need_s else np.zeros(
+            need_s, dtype=np.uint32)
         _chk(lib().fg_polys_gather(self._h, arr, C.c_size_t(len(parts)),
                                    vtx.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(vtx.size),
                                    spx.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_size_t(spx.size),

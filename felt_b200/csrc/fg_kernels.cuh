@@ -831,11 +831,17 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 				len += __popc(msk);
 			}
 			__syncwarp();
-			// phase t: swap-with-last removals (LookupMixin.hpp:339-371), in order
+			// phase t: swap-with-last removals (LookupMixin.hpp:339-371), in order. The next
+			// removal's leaf and position are read a step ahead (off the chain's critical path);
+			// the position is fixed up when this step moves that very leaf.
 			if (lane == 0) {
-				for (int c = coff[t]; c < coff[t + 1]; c++) {
-					const int leaf = schg[c];
-					const int pos = slkp[leaf];
+				const int c0 = coff[t], c1 = coff[t + 1];
+				int leaf = c0 < c1 ? schg[c0] : 0;
+				int pos = c0 < c1 ? slkp[leaf] : 0;
+				for (int c = c0; c < c1; c++) {
+					const bool more = c + 1 < c1;
+					const int nleaf = more ? schg[c + 1] : 0;
+					int npos = more ? slkp[nleaf] : 0;
 					const int last = len - 1;
 					if (pos < last) {
 						const int moved = win[last - w0];
@@ -848,6 +854,7 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 						} else {
 							slkp[moved] = (uint16_t)pos;
 							lkp[moved] = (uint16_t)pos;
+							if (more && moved == nleaf) npos = pos;
 						}
 					}
 					slkp[leaf] = NUL16;
@@ -859,6 +866,8 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 						if (len == 0) atomicOr(&appb[t], 1u << t);
 						len++;
 					}
+					leaf = nleaf;
+					pos = npos;
 				}
 			}
 			len = __shfl_sync(FULL, len, 0);
