@@ -232,9 +232,10 @@ class BatchWork:
 
     def __init__(self, fb, cfg, name, shard=0):
         self.fb, self.cfg = fb, cfg
-        sizes, centres, self.speeds = batch_surfaces(name, cfg, shard)
+        sizes, centres, speeds = batch_surfaces(name, cfg, shard)
         self.b = fb.Batch(sizes, cfg["part"], cfg["L"])
         self.b.seed(centres)
+        self.speeds = self.b.speed_array(speeds)  # converted once; the speeds are fixed
         self.surface0 = None
 
     def step(self, i, last=False):

@@ -269,11 +269,19 @@ class Batch:
         flat = [int(x) for c in centres for x in c]
         _chk(lib().fg_batch_seed(self._h, _ivec(flat)))
 
-    def update(self, speeds):
-        """speeds: one dict(c=, a=, n=, seed=) per surface (or one dict for all)."""
+    def speed_array(self, speeds):
+        """The per-surface speeds as the C array update() passes down (build it once when the
+        speeds do not change from step to step)."""
         if isinstance(speeds, dict):
             speeds = [speeds] * self.n
-        arr = (Speed * self.n)(*[make_speed(**s) for s in speeds])
+        if len(speeds) != self.n:
+            raise ValueError("one speed per surface")
+        return (Speed * self.n)(*[make_speed(**s) for s in speeds])
+
+    def update(self, speeds):
+        """speeds: one dict(c=, a=, n=, seed=) per surface, one dict for all, or an array from
+        speed_array()."""
+        arr = speeds if isinstance(speeds, C.Array) else self.speed_array(speeds)
         _chk(lib().fg_batch_update(self._h, arr))
 
     def polys_notify(self):

@@ -122,11 +122,49 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 // tracks the leaf into affected buffer b under its new layer. Per-entry flags: bit 31 = the
 // partition must join the status partition list of `from`; bit t = it must join the buffer's
 // partition list t.
+//
+// While a warp records one partition entry nothing else writes that partition's list counts,
+// so they stay in registers for the whole entry (StatusCache): every lane holds the status
+// list count of `from`; lane t < NL holds buffer list t's leaf count and whether the partition
+// is already in the buffer's partition list t (compaction, which changes that, runs after the
+// pass). They are loaded at the entry's first change (most chunks have none). A chunk with
+// changes then costs one round of loads (the leaves' status and buffer lookups).
 // ---------------------------------------------------------------------------------------------
+struct StatusCache {
+	int ccnt = 0;         // leaves in the status list of `from`
+	int acnt = 0;         // lane t < NL: leaves in buffer list t
+	bool tracked = true;  // lane t < NL: the partition is in the buffer's partition list t
+	bool loaded = false;
+};
+
+template <int L>
+__device__ __forceinline__ StatusCache status_load(const Dev& P, int gp, int sl, int from, int b)
+{
+	constexpr int NL = 2 * L + 1;
+	const int lane = lane_id();
+	StatusCache c;
+	c.ccnt = P.ccnt[sl * NL + from + L];
+	c.acnt = lane < NL ? P.acnt[b][sl * NL + lane] : 0;
+	c.tracked = lane < NL ? P.appos[b][gp * NL + lane] >= 0 : true;
+	c.loaded = true;
+	return c;
+}
+
+template <int L>
+__device__ __forceinline__ void status_store(const Dev& P, int sl, int from, int b,
+                                             const StatusCache& c)
+{
+	constexpr int NL = 2 * L + 1;
+	const int lane = lane_id();
+	if (!c.loaded) return;
+	if (lane == 0) P.ccnt[sl * NL + from + L] = c.ccnt;
+	if (lane < NL) P.acnt[b][sl * NL + lane] = c.acnt;
+}
+
 template <int L>
 __device__ __forceinline__ void status_chunk(const Dev& P, int gp, int sl, int from, bool valid,
                                              int leaf, int to, int b, unsigned& flags,
-                                             bool& any_change)
+                                             bool& any_change, StatusCache& sc)
 {
 	constexpr int NL = 2 * L + 1;
 	const int lane = lane_id();
@@ -134,42 +172,40 @@ __device__ __forceinline__ void status_chunk(const Dev& P, int gp, int sl, int f
 	const bool chgd = valid && to != from;
 	if (__ballot_sync(FULL, chgd) == 0) return;
 	any_change = true;
+	if (!sc.loaded) sc = status_load<L>(P, gp, sl, from, b);
 	const size_t bv = (size_t)P.BV;
-	bool app = false;
+	const bool inb = chgd && inside_band(to, L);
+	const int t = inb ? to + L : -1;
+	bool app = false, isnew = false;
 	if (chgd) {
 		const int cur = P.sto[sl * bv + leaf];
+		if (inb) isnew = P.alkp[b][sl * bv + leaf] == NUL16;
 		app = cur == L + 1;
 		P.sto[sl * bv + leaf] = (int8_t)to;
 	}
 	const unsigned ma = __ballot_sync(FULL, app);
 	if (ma) {
 		const int fi = from + L;
-		const int base = P.ccnt[sl * NL + fi];
-		if (app) P.chg[((size_t)sl * NL + fi) * bv + base + __popc(ma & lt)] = (uint16_t)leaf;
-		__syncwarp();
-		if (lane == 0) P.ccnt[sl * NL + fi] = base + __popc(ma);
+		if (app) P.chg[((size_t)sl * NL + fi) * bv + sc.ccnt + __popc(ma & lt)] = (uint16_t)leaf;
+		sc.ccnt += __popc(ma);
 		flags |= 0x80000000u;
 	}
-	const bool inb = chgd && inside_band(to, L);
 	if (__ballot_sync(FULL, inb)) {
-		const int t = inb ? to + L : -1;
 		const unsigned grp = __match_any_sync(FULL, t);
-		const bool isnew = inb && P.alkp[b][sl * bv + leaf] == NUL16;
 		const unsigned mn = __ballot_sync(FULL, isnew) & grp;
-		int base = 0;
-		if (inb) base = P.acnt[b][sl * NL + t];
-		__syncwarp();
+		const int base = __shfl_sync(FULL, sc.acnt, inb ? t : 0);
+		const bool trk = __shfl_sync(FULL, sc.tracked, inb ? t : 0);
 		if (isnew) {
 			const int pos = base + __popc(mn & lt);
 			P.alst[b][((size_t)sl * NL + t) * bv + pos] = (uint16_t)leaf;
 			P.alkp[b][sl * bv + leaf] = (uint16_t)pos;
 		}
-		const bool leader = inb && (__ffs(grp) - 1) == lane;
-		if (leader) {
-			P.acnt[b][sl * NL + t] = base + __popc(mn);
-			if (P.appos[b][gp * NL + t] < 0) flags |= 1u << t;
+		if (inb && !trk) flags |= 1u << t;
+#pragma unroll
+		for (int l = 0; l < NL; l++) {
+			const int add = __popc(__ballot_sync(FULL, isnew && t == l));
+			if (lane == l) sc.acnt += add;
 		}
-		__syncwarp();
 	}
 }
 
@@ -187,7 +223,8 @@ __device__ __forceinline__ unsigned warp_or(unsigned v)
 template <int L>
 __device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int from, bool ch,
                                              int leaf, int to, int b, unsigned& flags,
-                                             bool& any_change, uint16_t* cl, int* ct)
+                                             bool& any_change, uint16_t* cl, int* ct,
+                                             StatusCache& sc)
 {
 	if (!__syncthreads_or(ch)) return;
 	int tot;
@@ -202,7 +239,7 @@ __device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int f
 			const int c = c0 + (int)threadIdx.x;
 			const bool v = c < tot;
 			status_chunk<L>(P, gp, sl, from, v, v ? cl[c] : 0, v ? ct[c] : from, b, flags,
-			                any_change);
+			                any_change, sc);
 		}
 	}
 	__syncthreads();
@@ -349,6 +386,7 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
 		bool any = false;
+		StatusCache sc;
 		for (int base = 0; base < n; base += blockDim.x) {
 			const int j = base + threadIdx.x;
 			int leaf = 0, to = 0;
@@ -358,9 +396,10 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 				to = layer_id(nw, P.err);
 				P.phi[b0 + leaf] = nw;
 			}
-			status_round<L>(P, gp, sl, 0, j < n && to != 0, leaf, to, b, flags, any, cl, ct);
+			status_round<L>(P, gp, sl, 0, j < n && to != 0, leaf, to, b, flags, any, cl, ct, sc);
 		}
 		if (threadIdx.x < 32) {
+			status_store<L>(P, sl, 0, b, sc);
 			flags = warp_or(flags);
 			if (threadIdx.x == 0) P.eflag[e] = flags;
 		}
@@ -385,6 +424,7 @@ __global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, con
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + L) * P.BV;
 		unsigned flags = 0;
 		bool any = false;
+		StatusCache sc;
 		for (int base = 0; base < n; base += 32) {
 			const int j = base + lane;
 			const bool valid = j < n;
@@ -396,8 +436,9 @@ __global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, con
 				to = layer_id(nw, P.err);
 				P.phi[k] = nw;
 			}
-			status_chunk<L>(P, gp, sl, 0, valid, leaf, to, b, flags, any);
+			status_chunk<L>(P, gp, sl, 0, valid, leaf, to, b, flags, any, sc);
 		}
+		status_store<L>(P, sl, 0, b, sc);
 		flags = warp_or(flags);
 		if (lane == 0) P.eflag[e] = flags;
 	}
@@ -559,6 +600,7 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView 
 		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
 		bool any = false;
+		StatusCache sc;
 		for (int base = 0; base < n; base += blockDim.x) {
 			const int j = base + threadIdx.x;
 			int leaf = 0, to = k;
@@ -568,9 +610,10 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView 
 				to = layer_id(d, P.err);
 				P.phi[b0 + leaf] = d;
 			}
-			status_round<L>(P, gp, sl, k, j < n && to != k, leaf, to, b, flags, any, cl, ct);
+			status_round<L>(P, gp, sl, k, j < n && to != k, leaf, to, b, flags, any, cl, ct, sc);
 		}
 		if (threadIdx.x < 32) {
+			status_store<L>(P, sl, k, b, sc);
 			flags = warp_or(flags);
 			if (threadIdx.x == 0) {
 				P.eflag[e] = flags;
@@ -599,6 +642,7 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
 		bool any = false;
+		StatusCache sc;
 		bool vnext = lane < n;
 		int lnext = vnext ? lst[lane] : 0;
 		float dnext = vnext ? P.dlt[b0 + lnext] : 0.0f;
@@ -617,8 +661,9 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 				to = layer_id(d, P.err);
 				P.phi[b0 + leaf] = d;
 			}
-			status_chunk<L>(P, gp, sl, k, valid, leaf, to, b, flags, any);
+			status_chunk<L>(P, gp, sl, k, valid, leaf, to, b, flags, any, sc);
 		}
+		status_store<L>(P, sl, k, b, sc);
 		flags = warp_or(flags);
 		if (lane == 0) {
 			P.eflag[e] = flags;

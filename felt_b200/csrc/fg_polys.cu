@@ -900,21 +900,20 @@ public:
 		}
 	}
 
+	/// Vertex and simplex totals over every partition of the pool, summed on the device (the
+	/// compaction's chunk sums); 16 bytes come back.
 	void totals(size_t* nv, size_t* ns) override
 	{
 		const Dev& P = eng_.dev();
+		cudaStream_t st = eng_.stream();
+		FG_RUN("k_arena_chunk_sums", st, k_arena_chunk_sums<<<nchunks_, 256, 0, st>>>(Q_, P.NP, csum_););
+		FG_RUN("k_arena_chunk_scan", st, k_arena_chunk_scan<<<1, 32, 0, st>>>(csum_, nchunks_, ctot_););
+		FG_CUDA(cudaGetLastError());
+		unsigned long long tot[2];
+		FG_CUDA(cudaMemcpyAsync(tot, ctot_, sizeof(tot), cudaMemcpyDeviceToHost, st));
 		eng_.sync();
-		std::vector<int> a(P.NP), b(P.NP);
-		FG_CUDA(cudaMemcpy(a.data(), Q_.gnv, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
-		FG_CUDA(cudaMemcpy(b.data(), Q_.gns, P.NP * sizeof(int), cudaMemcpyDeviceToHost));
-		size_t x = 0, y = 0;
-		for (int i = 0; i < P.NP; i++) {
-			if (P.S > 1 && i / 1 < 0) continue;
-			x += a[i];
-			y += b[i];
-		}
-		if (nv) *nv = x;
-		if (ns) *ns = y;
+		if (nv) *nv = (size_t)tot[0];
+		if (ns) *ns = (size_t)tot[1];
 	}
 
 private:

@@ -167,7 +167,7 @@ class Server:
         b = Batch([r.size for r in reqs], self.part, self.L, brick_capacity=max(w.bricks, 1))
         try:
             b.seed([r.centre for r in reqs])
-            speeds = [r.speed for r in reqs]
+            speeds = b.speed_array([r.speed for r in reqs])
             nu = 0
             for step in range(1, max(r.steps for r in reqs) + 1):
                 b.update(speeds)

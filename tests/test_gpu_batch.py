@@ -44,6 +44,14 @@ def _run_batch(D, L, part, sizes, centres, speeds_per_step, march_every=1):
                     assert ga == oa and np.array_equal(gs, os2), f"surface {i} partition {p}"
                     if ov.size:
                         assert float(np.abs(gv - ov).max()) <= 1e-5
+        if march:
+            tv = ts = 0
+            for o, op in zip(os_, ops):
+                for p in range(o.partitions()[0]):
+                    ov, os2, _ = op.partition(p)
+                    tv += ov.shape[0]
+                    ts += os2.shape[0]
+            assert b.polys_totals() == (tv, ts), f"step {step} totals"
     return b
 
 

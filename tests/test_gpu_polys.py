@@ -22,6 +22,12 @@ def _fb():
 
 def compare_polys(gp, op, nparts, where):
     assert gp.changes() == op.changes(), f"{where}: changes differ"
+    tv = ts = 0
+    for p in range(nparts):
+        ov, os_, _ = op.partition(p)
+        tv += ov.shape[0]
+        ts += os_.shape[0]
+    assert gp.totals() == (tv, ts), f"{where}: totals {gp.totals()} vs {(tv, ts)}"
     for p in range(nparts):
         gv, gs, ga = gp.partition(p)
         ov, os_, oa = op.partition(p)
