@@ -76,6 +76,11 @@ struct Dev {
 	uint16_t* alst[2];  // affected buffer leaf lists
 	int* acnt[2];
 	unsigned long long* claim;  // [slot*BV + leaf] expansion claim keys
+	// expansion candidates of the current iteration (key, partition, leaf), cand_cap at most
+	unsigned long long* cand_key;
+	int* cand_gp;
+	int* cand_leaf;
+	int cand_cap;
 	int* slot_gp;     // [nslots] owner partition
 
 	// allocator and queues
@@ -108,7 +113,15 @@ struct Dev {
 	int* ring_last;   // [NL*NP]
 };
 
-enum { CNT_FREE_TOP = 0, CNT_ACT = 1, CNT_TOUCH = 2, CNT_RETIRE = 3, CNT_SUNION = 4, CNT_N = 8 };
+enum {
+	CNT_FREE_TOP = 0,
+	CNT_ACT = 1,
+	CNT_TOUCH = 2,
+	CNT_RETIRE = 3,
+	CNT_SUNION = 4,
+	CNT_CAND = 5,  // expansion candidates recorded this iteration
+	CNT_N = 8
+};
 
 /// Work-unit counters (Dev::kstat): band nodes through the distance passes, zero-layer nodes
 /// through the speed functor, leaf edits replayed by the flush, cells marched by Polys.

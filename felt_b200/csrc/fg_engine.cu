@@ -173,6 +173,12 @@ public:
 			P.acnt[b] = dalloc<int>(nslots * NL, o);
 		}
 		P.claim = dalloc<unsigned long long>(nb, o);
+		// expansion candidates: most iterations need a few thousand; past the cap the claim
+		// and compute phases walk the status lists again instead
+		P.cand_cap = (int)std::min<size_t>(nb / 4 + 1024, (size_t)1 << 22);
+		P.cand_key = dalloc<unsigned long long>((size_t)P.cand_cap, o);
+		P.cand_gp = dalloc<int>((size_t)P.cand_cap, o);
+		P.cand_leaf = dalloc<int>((size_t)P.cand_cap, o);
 		P.slot_gp = dalloc<int>(nslots, o);
 		P.free_stack = dalloc<int>(nslots, o);
 		P.counters = dalloc<int>(CNT_N, o);
@@ -847,6 +853,7 @@ private:
 	{
 		scan(P_.spcnt, 0, 1);
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_CAND, 0, sizeof(int), st_));
 		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0););
 		FG_RUN("k_activate", st_, k_activate<L><<<sm_count() * 4, 256, 0, st_>>>(P_););
 		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 1););

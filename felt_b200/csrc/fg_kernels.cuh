@@ -790,9 +790,27 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 	const size_t bv = (size_t)BV;
 	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const unsigned lt = (1u << lane) - 1u;
+	// The kernel lasts as long as its longest removal chain. Partitions with a long chain go in
+	// a first sweep, so that they all start at once; the rest follow.
+	constexpr int LONG_CHAIN = 64;
+	__shared__ int take;
+	for (int sweep = 0; sweep < 2; sweep++)
 	for (int e = blockIdx.x; e < n; e += gridDim.x) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
+		if (threadIdx.x == 0) {
+			// sweep 1 finds a partition of sweep 0 already done: skipped by its chain length,
+			// or, when it deactivated, by its slot (the status counts are not changed here)
+			int mx = 0;
+			if (sl >= 0)
+				for (int l = 0; l < NL; l++) mx = max(mx, P.ccnt[sl * NL + l]);
+			take = sl >= 0 && (mx >= LONG_CHAIN) == (sweep == 0);
+		}
+		__syncthreads();
+		if (!take) {
+			__syncthreads();
+			continue;
+		}
 		uint16_t* lkp = P.lkp + sl * bv;
 		if (threadIdx.x == 0) {
 			int c = 0, lv = 0;
@@ -1058,6 +1076,33 @@ template <int D, int L>
 __global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
 {
 	constexpr int NL = 2 * L + 1;
+	// Modes 1 and 2 take the candidates that mode 0 recorded, one thread each, unless there
+	// were more than the buffer holds: then they walk the status lists like mode 0.
+	const int ncand = P.counters[CNT_CAND];
+	if (mode > 0 && ncand <= P.cand_cap) {
+		for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
+			const unsigned long long key = P.cand_key[i];
+			const int gpn = P.cand_gp[i], leafn = P.cand_leaf[i];
+			const int sn = P.slot[gpn];
+			if (sn < 0) {
+				atomicOr(P.err, EB_POOL);
+				continue;
+			}
+			unsigned long long* cl = &P.claim[(size_t)sn * P.BV + leafn];
+			if (mode == 1) {
+				atomicMin(cl, key);
+				if (atomicExch(&P.touched[sn], 1) == 0)
+					P.q_touch[atomicAdd(&P.counters[CNT_TOUCH], 1)] = sn;
+			} else if (*cl == key) {
+				const SurfGeom& g = P.geom[P.surf_of[gpn]];
+				const float side = ((key >> 43) & 1ull) ? 1.0f : -1.0f;
+				const float v = P.phi[(size_t)sn * P.BV + leafn];
+				P.dlt[(size_t)sn * P.BV + leafn] =
+				    distance<D, L>(P, g, leaf_pos<D>(P, gpn, leafn), v, side);
+			}
+		}
+		return;
+	}
 	FG_WARP_LOOP(P.woff)
 	{
 		const int s = entry_surface(P.woff, P.S, e);
@@ -1093,6 +1138,12 @@ __global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
 				if (mode == 0) {
 					if (P.slot[gpn] < 0 && atomicExch(&P.actflag[gpn], 1) == 0)
 						P.q_act[atomicAdd(&P.counters[CNT_ACT], 1)] = gpn;
+					const int ci = atomicAdd(&P.counters[CNT_CAND], 1);
+					if (ci < P.cand_cap) {
+						P.cand_key[ci] = key;
+						P.cand_gp[ci] = gpn;
+						P.cand_leaf[ci] = leafn;
+					}
 				} else {
 					const int sn = P.slot[gpn];
 					if (sn < 0) {
