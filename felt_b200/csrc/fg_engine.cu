@@ -270,6 +270,8 @@ public:
 	~Engine() override
 	{
 		cudaStreamSynchronize(st_);
+		for (cudaGraphExec_t& ex : iter_exec_)
+			if (ex) cudaGraphExecDestroy(ex);
 		for (void* p : owned_) cudaFree(p);
 		if (d_lpos_) cudaFree(d_lpos_);
 		if (d_lval_) cudaFree(d_lval_);
@@ -376,16 +378,10 @@ public:
 		int cur = B, oth = A;
 		while (changed) {
 			if (local && buf_dirty_[oth]) clear_buffer(oth);
-			clear_status();
-			FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
-			const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur]};
-			distance_passes(bv, oth);
-			flush();
-			expand();
-			retire();
+			if (local || !replay_iteration(cur, oth)) iteration(local, cur, oth);
 			status_dirty_ = true;
 			buf_dirty_[oth] = true;
-			if (!local) clear_buffer(cur);
+			if (!local) buf_dirty_[cur] = false;
 			std::swap(cur, oth);
 			changed = read_changed();
 			iters++;
@@ -400,6 +396,63 @@ public:
 			                 "edge); the surface is stopped");
 		}
 		newly_frozen_.clear();
+	}
+
+	/// One iteration of the convergence loop after the first: the distance passes over the
+	/// nodes that changed in the previous one (buffer cur), recording into buffer oth, then
+	/// flush, expansion and, in the global update, the reset of buffer cur.
+	void iteration(bool local, int cur, int oth)
+	{
+		clear_status();
+		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
+		const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur]};
+		distance_passes(bv, oth);
+		flush();
+		expand();
+		retire();
+		if (!local) clear_buffer(cur);
+	}
+
+	/// The global update's iteration as a CUDA graph, captured on first use (one per buffer
+	/// parity) and replayed: one launch instead of ~30, all of whose launch parameters are
+	/// fixed. Returns false (and the caller launches the kernels one by one) while per-launch
+	/// profiling is on or if capture is not possible.
+	bool replay_iteration(int cur, int oth)
+	{
+		if (!graphs_ok_ || prof_on()) return false;
+		cudaGraphExec_t& ex = iter_exec_[cur];
+		if (!ex) {
+			cudaGraph_t gph = nullptr;
+			if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+				cudaGetLastError();
+				graphs_ok_ = false;
+				return false;
+			}
+			const long long l0 = launch_count();
+			bool threw = false;
+			try {
+				iteration(false, cur, oth);
+			} catch (...) {
+				threw = true;
+			}
+			const cudaError_t e = cudaStreamEndCapture(st_, &gph);
+			const long long captured = launch_count() - l0;
+			add_launches(-captured);  // counted when they run
+			if (threw || e != cudaSuccess || !gph ||
+			    cudaGraphInstantiate(&ex, gph, 0) != cudaSuccess) {
+				if (gph) cudaGraphDestroy(gph);
+				ex = nullptr;
+				cudaGetLastError();
+				graphs_ok_ = false;
+				if (threw) throw Error(-2, "capture of the update iteration failed");
+				return false;
+			}
+			cudaGraphDestroy(gph);
+			iter_launches_[cur] = captured;
+		}
+		FG_CUDA(cudaGraphLaunch(ex, st_));
+		add_launches(iter_launches_[cur]);
+		return true;
 	}
 
 	/// The reference loops `while (is_status_changed)` with no bound (Surface.hpp:752-760,
@@ -845,8 +898,7 @@ private:
 			FG_RUN("k_flush_smem", st_, k_flush_smem<D, L><<<sm_count() * 8, 128, smem_flush_, st_>>>(P_););
 		else
 			FG_RUN("k_flush_leaf", st_, k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_););
-		const int warps = P_.S * NL;
-		FG_RUN("k_flush_plist", st_, k_flush_plist<L><<<(warps * 32 + 255) / 256, 256, 0, st_>>>(P_););
+		FG_RUN("k_flush_plist", st_, k_flush_plist<L><<<P_.S * NL, 256, 0, st_>>>(P_););
 	}
 
 	void expand()
@@ -909,6 +961,9 @@ private:
 	int lcap_ = 0;
 	int warp_grid_ = 0;
 	int dist_split_ = 1;  // warps per partition entry in the first distance pass
+	cudaGraphExec_t iter_exec_[2] = {nullptr, nullptr};  // global iteration, by buffer parity
+	long long iter_launches_[2] = {0, 0};
+	bool graphs_ok_ = true;
 	CompactArgs pending_{0, nullptr, nullptr, 0, 0};  // compaction riding on the next k_dist1
 	// whole blocks (not warps) per partition entry in the record-keeping passes: pays off when
 	// a brick holds thousands of leaves, costs idle threads when it holds a few hundred

@@ -100,6 +100,10 @@ EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream);
 void prof_begin(const char* name, cudaStream_t st);
 void prof_end(cudaStream_t st);
 long long launch_count();
+/// Accounts for launches made by a graph replay (each captured launch counted once per replay).
+void add_launches(long long n);
+/// Whether per-launch profiling is on (launches then go one by one, not through graphs).
+bool prof_on();
 void prof_enable(bool on);
 /// Synchronises pending events and returns (name, total ms, launches) per kernel name.
 struct ProfEntry {

@@ -986,55 +986,54 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 	}
 }
 
-/// Children-level half of the flush: one warp per (surface, list k) replays, in the reference's
-/// order (from-layer ascending, then status partition list order), the appends to list k and
-/// the swap-with-last removals from it (LookupMixin.hpp:483-556). The events only read the leaf
-/// flush's records (app, rem), which this kernel does not change, so AHEAD chunks of them are
-/// loaded together before their (rare) events are replayed in order.
+/// Children-level half of the flush: one block per (surface, list k) replays, in the
+/// reference's order (from-layer ascending, then status partition list order), the appends to
+/// list k and the swap-with-last removals from it (LookupMixin.hpp:483-556). The events only
+/// read the leaf flush's records (app, rem), which this kernel does not change: the block loads
+/// a tile of them into shared memory at once, then one warp replays the (rare) events in order.
 template <int L>
-__global__ void k_flush_plist(Dev P)
+__global__ void __launch_bounds__(256) k_flush_plist(Dev P)
 {
 	constexpr int NL = 2 * L + 1;
-	constexpr int AHEAD = 4;
-	const int lane = lane_id();
-	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	constexpr int TILE = 2048;
+	__shared__ int slp[TILE];
+	__shared__ unsigned char sev[TILE];  // 1 append, 2 removal
+	const int w = blockIdx.x;
 	if (w >= P.S * NL) return;
+	const int lane = lane_id();
 	const int s = w / NL, k = w % NL;
 	const SurfGeom& g = P.geom[s];
 	int* pl = P.plist + (size_t)k * P.NP + g.pbase;
-	int cnt = P.pcnt[s * NL + k];
+	int cnt = P.pcnt[s * NL + k];  // kept by warp 0
 	for (int fi = 0; fi < NL; fi++) {
 		const int ns = P.spcnt[s * NL + fi];
 		const int* sp = P.splist + (size_t)fi * P.NP + g.pbase;
-		for (int base = 0; base < ns; base += 32 * AHEAD) {
-			int lpa[AHEAD], eva[AHEAD];
-#pragma unroll
-			for (int u = 0; u < AHEAD; u++) {
-				const int i = base + 32 * u + lane;
-				lpa[u] = i < ns ? sp[i] : 0;
+		for (int t0 = 0; t0 < ns; t0 += TILE) {
+			const int nt = min(TILE, ns - t0);
+			__syncthreads();
+			for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+				const int lp = sp[t0 + i];
+				const int gp = g.pbase + lp;
+				unsigned char ev;
+				if (fi == k)
+					ev = ((P.rem[gp] >> k) & 1u) ? 2 : 0;
+				else
+					ev = ((P.app[gp * NL + fi] >> k) & 1u) ? 1 : 0;
+				slp[i] = lp;
+				sev[i] = ev;
 			}
-#pragma unroll
-			for (int u = 0; u < AHEAD; u++) {
-				const int i = base + 32 * u + lane;
-				int ev = 0;
-				if (i < ns) {
-					const int gp = g.pbase + lpa[u];
-					if (fi == k)
-						ev = ((P.rem[gp] >> k) & 1u) ? 2 : 0;
-					else
-						ev = ((P.app[gp * NL + fi] >> k) & 1u) ? 1 : 0;
-				}
-				eva[u] = ev;
-			}
-#pragma unroll
-			for (int u = 0; u < AHEAD; u++) {
-				unsigned m = __ballot_sync(FULL, eva[u] != 0);
+			__syncthreads();
+			if (threadIdx.x >= 32) continue;
+			for (int base = 0; base < nt; base += 32) {
+				const int i = base + lane;
+				const int ev0 = i < nt ? sev[i] : 0;
+				unsigned m = __ballot_sync(FULL, ev0 != 0);
 				while (m) {
 					const int src = __ffs(m) - 1;
 					m &= m - 1;
-					const int lp = __shfl_sync(FULL, lpa[u], src);
-					const int ev = __shfl_sync(FULL, eva[u], src);
 					if (lane == 0) {
+						const int lp = slp[base + src];
+						const int ev = sev[base + src];
 						const int gp = g.pbase + lp;
 						int* at = &P.ppos[gp * NL + k];
 						if (ev == 1) {
@@ -1059,7 +1058,7 @@ __global__ void k_flush_plist(Dev P)
 			}
 		}
 	}
-	if (lane == 0) P.pcnt[s * NL + k] = cnt;
+	if (threadIdx.x == 0) P.pcnt[s * NL + k] = cnt;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -263,88 +263,97 @@ __device__ __forceinline__ int box_index(const Dev& P, const int* bext, int leaf
 
 }  // namespace
 
-/// Polys::notify (Polys.hpp:92-133), one warp per surface. The reference walks the delta lists
+/// Polys::notify (Polys.hpp:92-133), one block per surface. The reference walks the delta lists
 /// of layers 0 and 2L tracking (appending) or untracking (swap-with-last removing) each
 /// partition in the pending list, then tracks the poly-active partitions of the outermost
-/// status lists. Whether each entry is a real append or removal depends only on the state
-/// before its chunk (a partition appears once per list), so each 32-entry chunk appends its
-/// runs in parallel by ballot and replays the (rare) removals one at a time in list order.
+/// status lists. Within one list a partition appears once, so whether each entry is a real
+/// append or removal depends only on the state before the list: the whole block decides a tile
+/// of entries at once into shared memory, then one warp replays them in list order, appending
+/// runs by ballot and replaying the (rare) removals one at a time.
 template <int L>
-__global__ void k_polys_notify(Dev P, PolysDev Q)
+__global__ void __launch_bounds__(256) k_polys_notify(Dev P, PolysDev Q)
 {
 	constexpr int NL = 2 * L + 1;
+	constexpr int TILE = 1024;
+	__shared__ int slp[TILE];
+	__shared__ unsigned char sdec[TILE];  // bit 0 append, bit 1 remove
+	__shared__ int cnt_s;
+	const int s = blockIdx.x;
+	if (s >= P.S || P.sfrozen[s]) return;
 	const int lane = lane_id();
 	const unsigned lt = (1u << lane) - 1u;
-	const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	if (s >= P.S || P.sfrozen[s]) return;
 	const SurfGeom& g = P.geom[s];
 	int* lkp = Q.pend_lkp[Q.pend];
 	int* lst = Q.pend_list[Q.pend] + g.pbase;
-	int cnt = Q.pend_cnt[Q.pend][s];
+	if (threadIdx.x == 0) cnt_s = Q.pend_cnt[Q.pend][s];
 	for (int pass = 0; pass < 4; pass++) {
 		const bool status = pass >= 2;
 		const int li = (pass & 1) ? NL - 1 : 0;
 		const int n = status ? P.spcnt[s * NL + li] : P.dpcnt[s * NL + li];
 		const int* src = (status ? P.splist : P.dplist) + (size_t)li * P.NP + g.pbase;
-		// decisions of entry i; a list holds a partition once, so the pending-list membership
-		// read for the next chunk stays valid while this chunk's edits are applied
-		auto decide = [&](int i, int& lp, int& gp, bool& app, bool& rem) {
-			lp = 0;
-			gp = 0;
-			app = rem = false;
-			if (i >= n) return;
-			lp = src[i];
-			gp = g.pbase + lp;
-			const bool in = lkp[gp] >= 0;
-			if (status) {
-				app = Q.pact[gp] && !in;
-			} else {
-				bool act = Q.pact[gp] != 0;
-				for (int lj = 0; !act && lj <= NL; lj += NL - 1)
-					act = P.ppos[gp * NL + lj] >= 0;
-				app = act && !in;
-				rem = !act && in;
+		for (int t0 = 0; t0 < n; t0 += TILE) {
+			const int nt = min(TILE, n - t0);
+			__syncthreads();  // the previous tile's edits are visible
+			for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+				const int lp = src[t0 + i];
+				const int gp = g.pbase + lp;
+				const bool in = lkp[gp] >= 0;
+				unsigned char dec = 0;
+				if (status) {
+					dec = (Q.pact[gp] && !in) ? 1 : 0;
+				} else {
+					bool act = Q.pact[gp] != 0;
+					for (int lj = 0; !act && lj <= NL; lj += NL - 1)
+						act = P.ppos[gp * NL + lj] >= 0;
+					dec = (act && !in) ? 1 : (!act && in) ? 2 : 0;
+				}
+				slp[i] = lp;
+				sdec[i] = dec;
 			}
-		};
-		int lpn, gpn;
-		bool apn, rmn;
-		decide(lane, lpn, gpn, apn, rmn);
-		for (int base = 0; base < n; base += 32) {
-			const int lp = lpn, gp = gpn;
-			const bool app = apn, rem = rmn;
-			decide(base + 32 + lane, lpn, gpn, apn, rmn);
-			unsigned ma = __ballot_sync(FULL, app), mr = __ballot_sync(FULL, rem);
-			while (ma | mr) {
-				const int r = mr ? __ffs(mr) - 1 : 32;
-				const unsigned seg = ma & (r == 32 ? FULL : ((1u << r) - 1u));
-				if (seg) {
-					if ((seg >> lane) & 1u) {
-						const int pos = cnt + __popc(seg & lt);
-						lst[pos] = lp;
-						lkp[gp] = pos;
-					}
-					cnt += __popc(seg);
-					ma &= ~seg;
-					__syncwarp();
-				}
-				if (r < 32) {
-					if (lane == r) {
-						const int at = lkp[gp], last = cnt - 1;
-						if (at < last) {
-							const int mv = lst[last];
-							lst[at] = mv;
-							lkp[g.pbase + mv] = at;
+			__syncthreads();
+			if (threadIdx.x < 32) {
+				int cnt = cnt_s;
+				for (int base = 0; base < nt; base += 32) {
+					const int i = base + lane;
+					const unsigned char dec = i < nt ? sdec[i] : 0;
+					const int lp = i < nt ? slp[i] : 0;
+					const int gp = g.pbase + lp;
+					unsigned ma = __ballot_sync(FULL, dec & 1), mr = __ballot_sync(FULL, dec & 2);
+					while (ma | mr) {
+						const int r = mr ? __ffs(mr) - 1 : 32;
+						const unsigned seg = ma & (r == 32 ? FULL : ((1u << r) - 1u));
+						if (seg) {
+							if ((seg >> lane) & 1u) {
+								const int pos = cnt + __popc(seg & lt);
+								lst[pos] = lp;
+								lkp[gp] = pos;
+							}
+							cnt += __popc(seg);
+							ma &= ~seg;
+							__syncwarp();
 						}
-						lkp[gp] = -1;
+						if (r < 32) {
+							if (lane == r) {
+								const int at = lkp[gp], last = cnt - 1;
+								if (at < last) {
+									const int mv = lst[last];
+									lst[at] = mv;
+									lkp[g.pbase + mv] = at;
+								}
+								lkp[gp] = -1;
+							}
+							cnt -= 1;
+							mr &= ~(1u << r);
+							__syncwarp();
+						}
 					}
-					cnt -= 1;
-					mr &= ~(1u << r);
-					__syncwarp();
 				}
+				if (lane == 0) cnt_s = cnt;
 			}
 		}
 	}
-	if (lane == 0) Q.pend_cnt[Q.pend][s] = cnt;
+	__syncthreads();
+	if (threadIdx.x == 0) Q.pend_cnt[Q.pend][s] = cnt_s;
 }
 
 /// Polys::invalidate (Polys.hpp:171-191), one thread per surface.
@@ -784,7 +793,7 @@ public:
 	void notify() override
 	{
 		const Dev& P = eng_.dev();
-		FG_RUN("k_polys_notify", eng_.stream(), k_polys_notify<L><<<(P.S * 32 + 127) / 128, 128, 0, eng_.stream()>>>(P, Q_););
+		FG_RUN("k_polys_notify", eng_.stream(), k_polys_notify<L><<<P.S, 256, 0, eng_.stream()>>>(P, Q_););
 		FG_CUDA(cudaGetLastError());
 	}
 
@@ -973,8 +982,14 @@ private:
 		eng_.sync();
 		const long long tv = (long long)tot[0], ts = (long long)tot[1];
 		// 16x headroom over the live geometry: a march re-emits the geometry of the partitions
-		// it re-marches, so with less room a polygonisation every step compacts every step
+		// it re-marches, so with less room a polygonisation every step compacts every step.
+		// After an overflowed march, `used` holds everything that march asked for (every
+		// partition reserves its range, fitting or not): sized from it, the retry fits.
 		long long vcap = grow ? 2 * Q_.vcap : Q_.vcap, scap = grow ? 2 * Q_.scap : Q_.scap;
+		if (grow) {
+			while (vcap < 2 * (long long)used[0] + tv) vcap *= 2;
+			while (scap < 2 * (long long)used[1] + ts) scap *= 2;
+		}
 		while (tv * 16 > vcap) vcap *= 2;
 		while (ts * 16 > scap) scap *= 2;
 		if (vcap >= (1LL << 31) || scap >= (1LL << 31))

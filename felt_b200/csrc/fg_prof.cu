@@ -85,6 +85,15 @@ void prof_end(cudaStream_t st)
 
 long long launch_count() { return g_launches.load(); }
 
+void add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+bool prof_on()
+{
+	Prof& p = prof();
+	std::lock_guard<std::mutex> lk(p.mu);
+	return p.on;
+}
+
 void prof_enable(bool on)
 {
 	Prof& p = prof();
