@@ -192,7 +192,8 @@ class SingleWork:
         for _ in range(cfg["expand"]):
             self.s.update(c=-1.0)
         self._pinned()
-        # one polygonisation and readback at setup, so that their buffers exist before timing
+        # a full polygonisation and readback at setup, so that their buffers exist before timing
+        self.p.invalidate()
         self.p.march()
         self.fetch_geometry()
 
@@ -239,7 +240,8 @@ class BatchWork:
         self.b = fb.Batch(sizes, cfg["part"], cfg["L"])
         self.b.seed(centres)
         self.speeds = self.b.speed_array(speeds)  # converted once; the speeds are fixed
-        # one polygonisation at setup, so that its buffers exist before timing
+        # a full polygonisation at setup, so that its buffers exist before timing
+        self.b.polys_invalidate()
         self.b.polys_march()
         self.b.polys_totals()
         self.surface0 = None

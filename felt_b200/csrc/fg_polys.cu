@@ -765,6 +765,18 @@ public:
 		const long long vc = vertex_capacity ? std::max<long long>((long long)vertex_capacity, 64)
 		                                     : (1LL << 20);
 		if (vc >= (1LL << 30)) throw Error(-1, "vertex capacity too large");
+		// freed arena memory stays in this process's stream-ordered pool for the next regrowth
+		// instead of going back to the driver at every synchronisation
+		{
+			int dev = 0;
+			cudaMemPool_t pool;
+			cudaGetDevice(&dev);
+			if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+				uint64_t keep = UINT64_MAX;
+				cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+			}
+			cudaGetLastError();
+		}
 		alloc_arena(vc, 2 * vc);
 		int bvol = 1;
 		for (int a = 0; a < D; a++) bvol *= eng.part(a) + 1;
@@ -782,12 +794,14 @@ public:
 
 	~PolysImpl() override
 	{
-		cudaStreamSynchronize(eng_.stream());
+		cudaStream_t st = eng_.stream();
+		cudaStreamSynchronize(st);
 		free_arena();
-		if (spare_v_) cudaFree(spare_v_);
-		if (spare_s_) cudaFree(spare_s_);
+		if (spare_v_) cudaFreeAsync(spare_v_, st);
+		if (spare_s_) cudaFreeAsync(spare_s_, st);
+		if (stage_) cudaFreeAsync(stage_, st);
+		cudaStreamSynchronize(st);
 		for (void* p : owned_) cudaFree(p);
-		if (stage_) cudaFree(stage_);
 	}
 
 	void notify() override
@@ -947,17 +961,22 @@ private:
 		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 		return sms * 4;
 	}
+	// The arenas and the gather staging come from the stream-ordered allocator: they are
+	// regrown while marching (the geometry grows with the surfaces), and its pooled,
+	// stream-ordered frees do not stall the device the way cudaFree does.
 	void alloc_arena(long long vcap, long long scap)
 	{
-		FG_CUDA(cudaMalloc(&Q_.vtx, (size_t)vcap * VF * sizeof(float)));
-		FG_CUDA(cudaMalloc(&Q_.spx, (size_t)scap * D * sizeof(uint32_t)));
+		cudaStream_t st = eng_.stream();
+		FG_CUDA(cudaMallocAsync((void**)&Q_.vtx, (size_t)vcap * VF * sizeof(float), st));
+		FG_CUDA(cudaMallocAsync((void**)&Q_.spx, (size_t)scap * D * sizeof(uint32_t), st));
 		Q_.vcap = vcap;
 		Q_.scap = scap;
 	}
 	void free_arena()
 	{
-		if (Q_.vtx) cudaFree(Q_.vtx);
-		if (Q_.spx) cudaFree(Q_.spx);
+		cudaStream_t st = eng_.stream();
+		if (Q_.vtx) cudaFreeAsync(Q_.vtx, st);
+		if (Q_.spx) cudaFreeAsync(Q_.spx, st);
 		Q_.vtx = nullptr;
 		Q_.spx = nullptr;
 	}
@@ -995,17 +1014,17 @@ private:
 		if (vcap >= (1LL << 31) || scap >= (1LL << 31))
 			throw Error(-13, "polygonisation arena too large");
 		if (spare_vcap_ < vcap) {
-			if (spare_v_) cudaFree(spare_v_);
+			if (spare_v_) FG_CUDA(cudaFreeAsync(spare_v_, st));
 			spare_v_ = nullptr;
 			spare_vcap_ = 0;
-			FG_CUDA(cudaMalloc(&spare_v_, (size_t)vcap * VF * sizeof(float)));
+			FG_CUDA(cudaMallocAsync((void**)&spare_v_, (size_t)vcap * VF * sizeof(float), st));
 			spare_vcap_ = vcap;
 		}
 		if (spare_scap_ < scap) {
-			if (spare_s_) cudaFree(spare_s_);
+			if (spare_s_) FG_CUDA(cudaFreeAsync(spare_s_, st));
 			spare_s_ = nullptr;
 			spare_scap_ = 0;
-			FG_CUDA(cudaMalloc(&spare_s_, (size_t)scap * D * sizeof(uint32_t)));
+			FG_CUDA(cudaMallocAsync((void**)&spare_s_, (size_t)scap * D * sizeof(uint32_t), st));
 			spare_scap_ = scap;
 		}
 		FG_RUN("k_polys_compact", st, k_polys_compact<D><<<grid(), 256, 0, st>>>(P, Q_, noff_, nsoff_, spare_v_, spare_s_););
@@ -1075,10 +1094,10 @@ public:
 		const size_t need = (size_t)tv * VF * sizeof(float) + (size_t)ts * D * sizeof(uint32_t) +
 		                    job.size() * sizeof(int) + dst.size() * sizeof(long long) + 64;
 		if (need > stage_cap_) {
-			if (stage_) cudaFree(stage_);
+			if (stage_) FG_CUDA(cudaFreeAsync(stage_, eng_.stream()));
 			stage_ = nullptr;
 			stage_cap_ = std::max(need, (size_t)1 << 20);
-			FG_CUDA(cudaMalloc(&stage_, stage_cap_));
+			FG_CUDA(cudaMallocAsync(&stage_, stage_cap_, eng_.stream()));
 		}
 		char* base = static_cast<char*>(stage_);
 		float* sv = reinterpret_cast<float*>(base);
