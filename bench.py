@@ -6,6 +6,9 @@ steps of delta = -0.2*curv(pos) + 0.1*h(pos, 1234) (h = hashed uniform [-1,1) no
 Polys::notify every step and Polys::march every 10th step. A "step" is one Surface::update plus
 that repolygonisation. Metric: narrow-band node-updates/s (band size at each step's start).
 
+Config "ray" measures the raycasting row instead: Surface::ray, 2^20 rays per step at the c2
+surface (metric rays/s).
+
 Other configs: c1 (Surface<3,2> 64^3, 8^3 partitions, speed -0.5), c3 (4096 Surface<2,2>, grid
 edges log-uniform 128..1024, 16^2 partitions, constant speeds U[-0.8,-0.2], marching squares
 each step) and c4 (256 Surface<3,2>, edges from {32,48,64,96,128}, 8^3 partitions, speed
@@ -62,6 +65,12 @@ CONFIGS = {
                         "log-uniform 32..256, 8^3 partitions, speed constant U[-0.6,-0.1] | "
                         "-0.3*curv-0.2 | 0.2*hash_noise-0.2, 1..64 steps, polygonise p=0.5, "
                         "admission by a 150 GB brick-pool budget"),
+    "ray": dict(kind="ray", D=3, L=3, size=(512, 512, 512), part=(16, 16, 16), expand=100,
+                rays=1 << 20, steps=20, cpu_min_seconds=10.0,
+                workload="Surface::ray on Surface<3,3> 512^3 / 16^3 partitions, r~100 (100 "
+                         "steps of speed -1): 2^20 rays per step from uniform points on a "
+                         "radius-240 sphere, aimed at uniform points within radius 150 of the "
+                         "centre"),
 }
 
 # Algorithmic bytes per work unit of the kernels whose roofline is reported:
@@ -71,6 +80,8 @@ CONFIGS = {
 #  k_flush_*: per leaf edit: 2 B status entry + 1 B to-layer + 2 B lookup read + 2 B list
 #             write + 2 B lookup write + 4 B swap-in (moved entry and its lookup).
 #  k_polys_march: per cell: 2 B leaf index + 4 B phi (corners are neighbours' phi).
+#  k_ray: per ray: origin and direction in, hit out (3 x 12 B in 3D); the nodes it samples
+#         are reads of the resident isogrid and are not counted.
 UNIT_BYTES = {"k_dist1": (0, 10), "k_dist2": (0, 10), "k_delta_builtin": (1, 10),
               "k_delta_smem": (1, 10), "k_flush_smem": (2, 13), "k_flush_leaf": (2, 13),
               "k_polys_march": (3, 6)}
@@ -427,21 +438,26 @@ def run_reference(args, name, cfg):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
+    metric, unit = "narrow-band node-updates/s", "node-updates/s"
     if cfg["kind"] == "serve":
         steps = None
         base = serve_cpu(cfg, cfg["cpu_subset"])
+    elif cfg["kind"] == "ray":
+        steps = 1
+        base = cpu_rays(cfg)
+        metric, unit = "rays/s", "rays/s"
     else:
         steps = args.steps or cfg["steps"]
         steps = min(steps, 20 if cfg["kind"] == "single" else 10)
         base = cpu_baseline(name, cfg, steps)
     line = {
-        "impl": "reference", "metric": "narrow-band node-updates/s", "value": base["value"],
-        "unit": "node-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "impl": "reference", "metric": metric, "value": base["value"],
+        "unit": unit, "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": cfg["workload"], "name": name},
         "cpu_baseline": base,
-        "e2e": {"value": base["value"], "unit": "node-updates/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": base["value"], "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -487,6 +503,165 @@ def roofline(fb, work, cfg, stream_steps):
             except Exception:
                 pass
     return out
+
+
+def ray_inputs(cfg, n, seed):
+    """Seeded rays of the ray config: origins uniform on a radius-240 sphere, each aimed at a
+    point uniform in the radius-150 ball around the centre; float32, unit directions."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    D = cfg["D"]
+    u = rng.normal(size=(n, D))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    o = u * 240.0
+    v = rng.normal(size=(n, D))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    tgt = v * 150.0 * rng.random((n, 1)) ** (1.0 / D)
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return o.astype(np.float32), d.astype(np.float32)
+
+
+def cpu_rays(cfg, seed=0):
+    """The oracle's Surface::ray over the config's rays on every host core, passes over the
+    same 2^20 rays until cpu_min_seconds of casting have elapsed."""
+    import numpy as np
+    from oracle import oracle as O
+    threads = cpu_threads()
+    s = O.Surface(cfg["size"], cfg["part"], cfg["L"])
+    s.seed((0,) * cfg["D"])
+    s.run_steps(cfg["expand"], c=-1.0)
+    o, d = ray_inputs(cfg, cfg["rays"], seed)
+    n, secs, passes = 0, 0.0, 0
+    while secs < cfg["cpu_min_seconds"] and passes < 20:
+        t0 = time.perf_counter()
+        s.rays(o, d)
+        secs += time.perf_counter() - t0
+        n += o.shape[0]
+        passes += 1
+    return {"value": n / secs, "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"{passes} pass(es) over the {o.shape[0]} rays of the workload on the "
+                      f"same surface ({n} rays in {secs:.2f} s, rays spread over {threads} "
+                      f"threads)"}
+
+
+def run_ray(args, name, cfg):
+    """Surface::ray throughput: value = rays/s of the device kernel with rays resident in HBM;
+    e2e = rays/s through fg_ray with pinned host arrays (copies in, hits out)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    import felt_b200 as fb
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    steps = args.steps or cfg["steps"]
+    s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=args.brick_capacity)
+    s.seed((0,) * cfg["D"])
+    for _ in range(cfg["expand"]):
+        s.update(c=-1.0)
+    n = cfg["rays"]
+    o, d = ray_inputs(cfg, n, seed=rank)
+    to, td = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+    th = torch.empty_like(to)
+    ho = torch.from_numpy(o).pin_memory()
+    hd = torch.from_numpy(d).pin_memory()
+    hh = torch.empty_like(ho).pin_memory()
+    stream = torch.cuda.ExternalStream(s.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lib = fb.lib()
+
+    def cast_device():
+        s.rays_device(to.data_ptr(), td.data_ptr(), n, th.data_ptr())
+
+    def cast_host():
+        fb._chk(lib.fg_ray(s._h, C.c_void_p(ho.data_ptr()), C.c_void_p(hd.data_ptr()),
+                           C.c_size_t(n), C.c_void_p(hh.data_ptr())))
+
+    for _ in range(args.warmup):
+        cast_device()
+        cast_host()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = fb.launch_count()
+    total = 0.0
+    for i in range(steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cast_device()
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    wall = 0.0
+    for i in range(steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cast_host()
+        wall += time.perf_counter() - t0
+    launches = fb.launch_count() - l0
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    hits = float(np.mean(np.any(th.cpu().numpy() != np.float32(np.finfo(np.float32).max),
+                                axis=1)))
+    same = bool(torch.equal(th.cpu(), hh))
+    if pg:
+        t_ms, wall, _ = combine_ranks(pg, total, wall, 0.0, "cuda")
+        total = t_ms
+    value = ws * n * steps / (total / 1e3)
+    e2e = {"value": ws * n * steps / wall, "unit": "rays/s",
+           "h2d_bytes_per_step": 2 * o.nbytes, "d2h_bytes_per_step": o.nbytes,
+           "how": "fg_ray with pinned host arrays, wall clock, copies inside"}
+    roof = None
+    cpu = None
+    if rank == 0:
+        fb.profile_reset()
+        fb.profile_enable(True)
+        for _ in range(3):
+            cast_device()
+        torch.cuda.synchronize()
+        fb.profile_enable(False)
+        ms, nl = fb.profile_read()["k_ray"]
+        hbm, peak_kind = load_peaks()
+        per = 3 * 4 * cfg["D"]
+        achieved = per * n / (ms / nl * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_ray", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / hbm,
+                "traffic": None, "bytes_per_launch": per * n, "avg_launch_us": 1e3 * ms / nl}
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            t = json.load(open(tf)).get("k_ray")
+            if t:
+                roof["traffic"] = t["bytes_per_unit"] * n
+        if ws == 1 and not args.no_cpu:
+            cpu = cpu_rays(cfg)
+        config = {"workload": cfg["workload"], "name": name, "rays_per_step": n,
+                  "parallelism": f"replicas{ws}", "hit_fraction": hits,
+                  "device_and_host_paths_agree": same,
+                  "l2": "flushed between timed steps (256 MB write)"}
+        line = {
+            "metric": "rays/s", "value": value, "unit": "rays/s", "n_gpus": ws,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": total / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config, "roofline": roof, "cpu_baseline": cpu,
+            "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
 
 
 def serve_requests(cfg, lam, shard=0):
@@ -754,6 +929,8 @@ def main():
         run_reference(args, args.config, cfg)
     elif cfg["kind"] == "serve":
         run_serve(args, args.config, cfg)
+    elif cfg["kind"] == "ray":
+        run_ray(args, args.config, cfg)
     else:
         run_felt(args, args.config, cfg)
 

@@ -22,6 +22,9 @@ _lib = None
 
 SPEED_CONST, SPEED_CURV, SPEED_NOISE = 1, 2, 4
 
+# Surface::ray_miss (include/Felt/Surface.hpp:62-64): FLT_MAX in every component.
+RAY_MISS = float(np.finfo(np.float32).max)
+
 
 class FeltError(RuntimeError):
     def __init__(self, code, msg):
@@ -72,6 +75,14 @@ def _fetch(fn, *args):
         if n.value <= cap:
             return list(buf[: n.value])
         cap = n.value
+
+
+def _ray_arrays(origins, dirs, D):
+    o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, D)
+    d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, D)
+    if o.shape != d.shape:
+        raise ValueError(f"origins {o.shape} and dirs {d.shape} differ")
+    return o, d
 
 
 def launch_count():
@@ -170,6 +181,27 @@ class Surface:
         v = C.c_float()
         _chk(lib().fg_get(self._h, _ivec(pos), C.byref(v)))
         return v.value
+
+    def rays(self, origins, dirs):
+        """Surface::ray (include/Felt/Surface.hpp:468-616) for each (origin, direction) row: the
+        point where the ray meets the zero curve, or a row of RAY_MISS where it misses."""
+        o, d = _ray_arrays(origins, dirs, self.D)
+        out = np.empty_like(o)
+        _chk(lib().fg_ray(self._h, o.ctypes.data_as(C.POINTER(C.c_float)),
+                          d.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(o.shape[0]),
+                          out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def ray(self, origin, direction):
+        """Surface::ray(origin, dir) for one ray."""
+        return self.rays([origin], [direction])[0]
+
+    def rays_device(self, origins_ptr, dirs_ptr, n, hits_ptr, buffer=-1):
+        """rays() over device arrays of n*D floats (e.g. torch CUDA tensors' data_ptr()).
+        buffer: candidate partitions a ray sorts in place (0..64, -1 = 64); the hits do not
+        depend on it."""
+        _chk(lib().fg_ray_device(self._h, C.c_void_p(origins_ptr), C.c_void_p(dirs_ptr),
+                                 C.c_size_t(n), C.c_void_p(hits_ptr), C.c_int(buffer)))
 
     def partitions(self):
         cnt = C.c_size_t()
@@ -299,6 +331,15 @@ class Batch:
         _chk(lib().fg_batch_snapshot(self._h, C.c_size_t(i),
                                      out.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(n)))
         return out.reshape(self.sizes[i])
+
+    def rays(self, i, origins, dirs):
+        """Surface::ray of surface i for each (origin, direction) row (RAY_MISS rows on a miss)."""
+        o, d = _ray_arrays(origins, dirs, self.D)
+        out = np.empty_like(o)
+        _chk(lib().fg_batch_ray(self._h, C.c_size_t(i), o.ctypes.data_as(C.POINTER(C.c_float)),
+                                d.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(o.shape[0]),
+                                out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
 
     def dump(self, i):
         return np.array(_fetch(lib().fg_batch_dump, self._h, C.c_size_t(i)), dtype=np.uint32)

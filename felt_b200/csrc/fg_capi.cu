@@ -8,6 +8,7 @@
 #include "../../include/felt_gpu.h"
 #include "fg_engine.cuh"
 #include "fg_polys.cuh"
+#include "fg_ray.cuh"
 
 #include "fg_handles.cuh"
 
@@ -201,6 +202,35 @@ int fg_get(fg_surface* s, const int* pos, float* out)
 		need(pos, "pos");
 		need(out, "out");
 		*out = s->eng->get(0, pos);
+	});
+}
+
+int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits)
+{
+	return guard([&] {
+		need(s, "surface");
+		if (n) {
+			need(origins, "origins");
+			need(dirs, "dirs");
+			need(hits, "hits");
+		}
+		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, false);
+	});
+}
+
+int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits,
+                  int buffer)
+{
+	return guard([&] {
+		need(s, "surface");
+		if (n) {
+			need(origins, "origins");
+			need(dirs, "dirs");
+			need(hits, "hits");
+		}
+		if (buffer < -1 || buffer > fg::ray_buffer_max())
+			throw fg::Error(FG_ERR_ARG, "candidate buffer out of range");
+		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, true, buffer);
 	});
 }
 
@@ -504,6 +534,21 @@ int fg_batch_snapshot(fg_batch* b, size_t surface, float* dst, size_t n)
 		need(b, "batch");
 		need(dst, "dst");
 		b->eng->snapshot((int)surface, dst, n, false);
+	});
+}
+
+int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float* dirs, size_t n,
+                 float* hits)
+{
+	return guard([&] {
+		need(b, "batch");
+		if (n) {
+			need(origins, "origins");
+			need(dirs, "dirs");
+			need(hits, "hits");
+		}
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
+		fg::ray_batch(*b->eng, (int)surface, origins, dirs, n, hits, false);
 	});
 }
 

@@ -3,7 +3,8 @@
 // felt_gpu::Polys<D,L> for Felt::Polys<Surface> (include/Felt/Polys.hpp).
 //
 // Differences a caller of the reference meets:
-//  - Positions are std::array<int, D> (the reference uses Eigen VecDi); index order is the same.
+//  - Positions are std::array<int, D> and ray points std::array<float, D> (the reference uses
+//    Eigen VecDi / VecDf); index order is the same.
 //  - update() takes either a builtin speed (Speed: constant, curvature, hashed noise and their
 //    sum) or, in a translation unit compiled by nvcc that includes felt_gpu/device.cuh, any
 //    __device__ functor with one of the reference's three signatures.
@@ -15,6 +16,7 @@
 
 #include <array>
 #include <cstdint>
+#include <limits>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -43,6 +45,8 @@ inline void check(int rc)
 
 template <int D>
 using VecDi = std::array<int, D>;
+template <int D>
+using VecDf = std::array<float, D>;
 
 /// Builtin speed: delta = [a * curv] + [n * h(pos, seed)] + [c], FP32, left to right.
 struct Speed {
@@ -130,6 +134,29 @@ public:
 		float v = 0.0f;
 		check(fg_get(h_, pos.data(), &v));
 		return v;
+	}
+
+	/// ray(origin, dir) (Surface.hpp:468-616): the point where the ray meets the zero curve,
+	/// or ray_miss.
+	VecDf<D> ray(const VecDf<D>& origin, const VecDf<D>& dir) const
+	{
+		VecDf<D> hit{};
+		check(fg_ray(h_, origin.data(), dir.data(), 1, hit.data()));
+		return hit;
+	}
+
+	/// ray() for n rays in one launch: origins, dirs and hits hold n*D floats (host memory).
+	void rays(const float* origins, const float* dirs, size_t n, float* hits) const
+	{
+		check(fg_ray(h_, origins, dirs, n, hits));
+	}
+
+	/// Surface::ray_miss (Surface.hpp:62-64): FLT_MAX in every component.
+	static VecDf<D> ray_miss()
+	{
+		VecDf<D> m;
+		m.fill(std::numeric_limits<float>::max());
+		return m;
 	}
 
 	/// isogrid().snapshot()->data(): dense, row-major, last axis fastest.

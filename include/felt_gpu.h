@@ -126,6 +126,19 @@ FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n);
 /* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */
 FG_API int fg_get(fg_surface* s, const int* pos, float* out);
 
+/* ray(origin, dir) (include/Felt/Surface.hpp:468-616, 1450-1598) for n rays at once: the
+ * point where each ray first meets the zero curve, or FLT_MAX in every component (the
+ * reference's ray_miss) when it misses. origins, dirs and hits hold n*dims floats each, in host
+ * memory; every ray runs on its own GPU thread, in the reference's FP32 arithmetic. */
+FG_API int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits);
+
+/* fg_ray with origins, dirs and hits in device memory of the surface's GPU, and an explicit
+ * per-ray candidate buffer (0..64 partitions; -1 = 64). Rays with more candidate partitions than
+ * the buffer holds re-walk their partition planes for each next candidate; the hits do not
+ * depend on the buffer size. */
+FG_API int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n,
+                         float* hits, int buffer);
+
 /* Geometry of the children (partition) grid: count, size and offset of the children grid. */
 FG_API int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);
 
@@ -212,6 +225,8 @@ FG_API int fg_batch_polys_invalidate(fg_batch* b);
 /* Per-surface queries, as the fg_surface ones. */
 FG_API int fg_batch_snapshot(fg_batch* b, size_t surface, float* dst, size_t n);
 FG_API int fg_batch_dump(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float* dirs,
+                         size_t n, float* hits);
 FG_API int fg_batch_polys_partition(fg_batch* b, size_t surface, size_t part, float* vtx,
                                     size_t vtx_cap, uint32_t* spx, size_t spx_cap, size_t* nv,
                                     size_t* ns, int* active);

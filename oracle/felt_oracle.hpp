@@ -957,6 +957,78 @@ template <> struct Geom<3> {
 	static Vi<3> spx_offset() { return {0, 0, -1}; }
 };
 
+/// interp (NumericMixin.hpp:403-481) of a grid at a real position: corners gathered in bit
+/// order, reduced axis 0 first.
+template <int D, class Grid>
+float field_interp(const Grid& iso, const std::array<float, D>& p)
+{
+	Vi<D> fl;
+	std::array<float, D> pc;
+	for (int ax = 0; ax < D; ax++) {
+		const float f = std::floor(p[ax]);
+		fl[ax] = int(f);
+		pc[ax] = p[ax] - f;
+	}
+	float v[1 << D];
+	for (int i = 0; i < (1 << D); i++) {
+		Vi<D> q = fl;
+		for (int ax = 0; ax < D; ax++) q[ax] += (i >> ax) & 1;
+		v[i] = iso.get(q);
+	}
+	int n = 1 << D;
+	while (n > 1) {
+		const int axis = D - __builtin_ctz(unsigned(n));
+		const float t = pc[axis];
+		for (int i = 0; i < n / 2; i++) {
+			const float lo = v[2 * i], hi = v[2 * i + 1];
+			v[i] = t * hi + (1.0f - t) * lo;
+		}
+		n >>= 1;
+	}
+	return v[0];
+}
+
+/// grad (NumericMixin.hpp:188-231) at a real position: the probe coordinate is stepped -1, +2,
+/// -1 in float, so it can drift by rounding, exactly as in the reference.
+template <int D, class Grid>
+std::array<float, D> field_grad_f(const Grid& iso, const std::array<float, D>& p)
+{
+	std::array<float, D> g;
+	const float centre = field_interp<D>(iso, p);
+	std::array<float, D> t = p;
+	for (int ax = 0; ax < D; ax++) {
+		float back = centre, fwd = centre;
+		int order = 0;
+		t[ax] -= 1;
+		if (inside<D>(t, iso.off, iso.hi)) {
+			back = field_interp<D>(iso, t);
+			order++;
+		}
+		t[ax] += 2;
+		if (inside<D>(t, iso.off, iso.hi)) {
+			fwd = field_interp<D>(iso, t);
+			order++;
+		}
+		t[ax] -= 1;
+		g[ax] = order != 0 ? (fwd - back) / float(order) : 0.0f;
+	}
+	for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
+	return g;
+}
+
+/// Eigen normalize(): divide by sqrt(x0^2 + (x1^2 + x2^2)) when that is positive.
+template <int D>
+void eigen_normalize(std::array<float, D>& v)
+{
+	std::array<float, D> sq;
+	for (int ax = 0; ax < D; ax++) sq[ax] = v[ax] * v[ax];
+	const float z = eigen_sum<float, D>(sq);
+	if (z > 0) {
+		const float r = std::sqrt(z);
+		for (int ax = 0; ax < D; ax++) v[ax] = v[ax] / r;
+	}
+}
+
 template <int D>
 struct Vertex {
 	std::array<float, D> pos;
@@ -1211,34 +1283,7 @@ public:
 
 	// --- 3D vertex normals: Vertex ctor (PolyMixin.hpp:142-148) ---
 
-	/// interp (NumericMixin.hpp:403-481): corners gathered in bit order, reduced axis 0 first.
-	float interp(const std::array<float, D>& p) const
-	{
-		Vi<D> fl;
-		std::array<float, D> pc;
-		for (int ax = 0; ax < D; ax++) {
-			const float f = std::floor(p[ax]);
-			fl[ax] = int(f);
-			pc[ax] = p[ax] - f;
-		}
-		float v[1 << D];
-		for (int i = 0; i < (1 << D); i++) {
-			Vi<D> q = fl;
-			for (int ax = 0; ax < D; ax++) q[ax] += (i >> ax) & 1;
-			v[i] = s->iso.get(q);
-		}
-		int n = 1 << D;
-		while (n > 1) {
-			const int axis = D - __builtin_ctz(unsigned(n));
-			const float t = pc[axis];
-			for (int i = 0; i < n / 2; i++) {
-				const float lo = v[2 * i], hi = v[2 * i + 1];
-				v[i] = t * hi + (1.0f - t) * lo;
-			}
-			n >>= 1;
-		}
-		return v[0];
-	}
+	float interp(const std::array<float, D>& p) const { return field_interp<D>(s->iso, p); }
 
 	/// grad (NumericMixin.hpp:188-231) at an integer position.
 	std::array<float, D> grad_i(const Vi<D>& p) const
@@ -1265,43 +1310,11 @@ public:
 		for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
 		return g;
 	}
-	/// grad at a real position: the probe coordinate is stepped -1, +2, -1 in float, so it can
-	/// drift by rounding, exactly as in the reference.
 	std::array<float, D> grad_f(const std::array<float, D>& p) const
 	{
-		std::array<float, D> g;
-		const float centre = interp(p);
-		std::array<float, D> t = p;
-		for (int ax = 0; ax < D; ax++) {
-			float back = centre, fwd = centre;
-			int order = 0;
-			t[ax] -= 1;
-			if (inside<D>(t, s->iso.off, s->iso.hi)) {
-				back = interp(t);
-				order++;
-			}
-			t[ax] += 2;
-			if (inside<D>(t, s->iso.off, s->iso.hi)) {
-				fwd = interp(t);
-				order++;
-			}
-			t[ax] -= 1;
-			g[ax] = order != 0 ? (fwd - back) / float(order) : 0.0f;
-		}
-		for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
-		return g;
+		return field_grad_f<D>(s->iso, p);
 	}
-	/// Eigen normalize(): divide by sqrt(x0^2 + (x1^2 + x2^2)) when that is positive.
-	static void normalize(std::array<float, D>& v)
-	{
-		std::array<float, D> sq;
-		for (int ax = 0; ax < D; ax++) sq[ax] = v[ax] * v[ax];
-		const float z = eigen_sum<float, D>(sq);
-		if (z > 0) {
-			const float r = std::sqrt(z);
-			for (int ax = 0; ax < D; ax++) v[ax] = v[ax] / r;
-		}
-	}
+	static void normalize(std::array<float, D>& v) { eigen_normalize<D>(v); }
 	Vertex<D> make_vertex_i(const Vi<D>& p) const
 	{
 		Vertex<D> v;
@@ -1325,6 +1338,171 @@ public:
 			v.norm.fill(0.0f);
 		}
 		return v;
+	}
+};
+
+
+// ---------------------------------------------------------------------------------------------
+// Raycasting (Surface.hpp:468-616, 1450-1598)
+// ---------------------------------------------------------------------------------------------
+
+/// Surface::ray: the zero-curve point a ray hits, or ray_miss (FLT_MAX in every component).
+/// Eigen semantics restated in FP32: ParametrizedLine::intersectionPoint(Hyperplane(n, d)) =
+/// o + t*dir with t = -(d + n.o) / (n.dir); pointAt(t) = o + dir*t; dot products and squared
+/// norms sum as x0 + (x1 + x2). Candidate partitions are ordered by squared distance from the
+/// origin, ties in the order they were found (std::sort leaves that order unspecified).
+template <int D, int L>
+class Raycast {
+public:
+	using Surf = Surface<D, L, float>;
+	using Vf = std::array<float, D>;
+	static constexpr int NL = Surf::NL;
+	static constexpr float TINY = 0.00001f;  // Surface.hpp:67
+	static constexpr int MAX_CONVERGE_STEPS = 100;
+	// bounds on the reference's open loops (never reached with a unit-length direction)
+	static constexpr int MAX_MARCH = 1 << 16;
+
+	explicit Raycast(const Surf& s) : s(&s) {}
+
+	static Vf miss()
+	{
+		Vf m;
+		m.fill(std::numeric_limits<float>::max());
+		return m;
+	}
+
+	Vf ray(const Vf& o, const Vf& dir) const
+	{
+		const auto& iso = s->iso;
+		if (inside<D>(o, iso.off, iso.hi)) {
+			Vi<D> pc;
+			for (int a = 0; a < D; a++) pc[a] = int(o[a]);  // Eigen cast<int>: truncation
+			const Vf h = ray_child(o, dir, iso.pidx_child(pc));
+			if (h != miss()) return h;
+		}
+		std::vector<std::pair<Vf, PosIdx>> hits;
+		for (int dim = 0; dim < D; dim++) {
+			const float dd = float(sgn(dir[dim]));
+			if (dd == 0) continue;
+			float pp = round_to_next(dim, dd, o[dim]);
+			Vf plane{};
+			plane[dim] = pp;
+			if (!inside<D>(plane, iso.off, iso.hi)) {
+				float pg;
+				if (dd == -1) {
+					pg = float(iso.off[dim] + iso.size[dim]);
+					if (pp < pg) continue;
+				} else {
+					pg = float(iso.off[dim]);
+					if (pp > pg) continue;
+				}
+				plane[dim] = pg;
+			}
+			check_track(hits, o, dir, dim, dd, plane[dim]);
+			pp = round_to_next(dim, dd, plane[dim]);
+			if (pp != plane[dim]) {
+				plane[dim] = pp;
+				if (!check_track(hits, o, dir, dim, dd, plane[dim])) continue;
+			}
+			const float cs = float(iso.csize[dim]);
+			for (int it = 0; it < MAX_MARCH; it++) {
+				plane[dim] += dd * cs;
+				if (!check_track(hits, o, dir, dim, dd, plane[dim])) break;
+			}
+		}
+		std::stable_sort(hits.begin(), hits.end(), [&](const auto& a, const auto& b) {
+			return dist2(a.first, o) < dist2(b.first, o);
+		});
+		hits.erase(std::unique(hits.begin(), hits.end(),
+		                       [](const auto& a, const auto& b) { return a.second == b.second; }),
+		           hits.end());
+		for (const auto& h : hits) {
+			const Vf p = ray_child(h.first, dir, h.second);
+			if (p != miss()) return p;
+		}
+		return miss();
+	}
+
+private:
+	const Surf* s;
+
+	static float dot(const Vf& a, const Vf& b)
+	{
+		Vf m;
+		for (int i = 0; i < D; i++) m[i] = a[i] * b[i];
+		return eigen_sum<float, D>(m);
+	}
+	static float dist2(const Vf& p, const Vf& o)
+	{
+		Vf d;
+		for (int i = 0; i < D; i++) d[i] = p[i] - o[i];
+		return dot(d, d);
+	}
+	static int sgn(float v) { return (0.0f < v) - (v < 0.0f); }
+
+	/// round_to_next (Surface.hpp:1582-1599).
+	float round_to_next(int dim, float dd, float pos) const
+	{
+		const auto& iso = s->iso;
+		float p = (pos - float(iso.off[dim])) / float(iso.csize[dim]);
+		p = dd == -1.0f ? std::floor(p) : std::ceil(p);
+		p *= float(iso.csize[dim]);
+		p += float(iso.off[dim]);
+		return p;
+	}
+
+	/// ray_check_track_child (Surface.hpp:1539-1577) for the plane x[dim] = plane_pos.
+	bool check_track(std::vector<std::pair<Vf, PosIdx>>& hits, const Vf& o, const Vf& dir,
+	                 int dim, float dd, float plane_pos) const
+	{
+		const auto& iso = s->iso;
+		// Hyperplane(normal = -dd e_dim, offset = plane_pos * dd)
+		const float nd = -dd, off = plane_pos * dd;
+		const float t = -(off + nd * o[dim]) / (nd * dir[dim]);
+		Vf p;
+		for (int i = 0; i < D; i++) p[i] = o[i] + dir[i] * t;
+		for (int i = 0; i < D; i++) p[i] = p[i] + dir[i] * TINY;
+		for (int i = 0; i < D; i++)
+			if ((dir[i] > 0 && p[i] > float(iso.size[i])) || (dir[i] < 0 && p[i] < float(iso.off[i])))
+				return false;
+		if (!inside<D>(p, iso.off, iso.hi)) return true;
+		Vi<D> pf;
+		for (int i = 0; i < D; i++) pf[i] = int(std::floor(p[i]));
+		const PosIdx pc = iso.pidx_child(pf);
+		const auto& lists = iso.ch[pc].lists;
+		if (lists[Surf::lidx(0)].size() || lists[Surf::lidx(1)].size() || lists[Surf::lidx(-1)].size())
+			hits.emplace_back(p, pc);
+		return true;
+	}
+
+	/// ray within one partition (Surface.hpp:1450-1530).
+	Vf ray_child(Vf pos, const Vf& dir, PosIdx pc) const
+	{
+		const auto& iso = s->iso;
+		Vi<D> chi;
+		for (int a = 0; a < D; a++) chi[a] = iso.ch[pc].off[a] + iso.csize[a];
+		const Vf o = pos;
+		float t = 0;
+		for (int it = 0; it < MAX_MARCH && inside<D>(pos, iso.ch[pc].off, chi); it++) {
+			if (s->layer_of(field_interp<D>(iso, pos)) == 0) {
+				Vf n = field_grad_f<D>(iso, pos);
+				eigen_normalize<D>(n);
+				if (dot(n, dir) < 0) {
+					for (int k = 0; k < MAX_CONVERGE_STEPS; k++) {
+						const float dist = field_interp<D>(iso, pos);
+						for (int a = 0; a < D; a++) pos[a] = pos[a] - n[a] * dist;
+						if (!inside<D>(pos, iso.off, iso.hi)) return miss();
+						if (std::abs(dist) <= TINY || dot(n, dir) >= 0) break;
+						n = field_grad_f<D>(iso, pos);
+						eigen_normalize<D>(n);
+					}
+					return pos;
+				}
+			}
+			t += 0.5f;
+			for (int a = 0; a < D; a++) pos[a] = o[a] + dir[a] * t;
+		}
+		return miss();
 	}
 };
 

@@ -33,6 +33,7 @@ struct SurfBase {
 	virtual void stats(size_t* a, size_t* b) = 0;
 	virtual size_t band_size() = 0;
 	virtual void curv(const int* p, float* out) = 0;
+	virtual void ray(const float* o, const float* d, float* out) = 0;
 };
 
 struct PolysBase {
@@ -124,6 +125,16 @@ struct Surf : SurfBase {
 		return n;
 	}
 	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
+	void ray(const float* o, const float* d, float* out) override
+	{
+		std::array<float, D> oo, dd;
+		for (int a = 0; a < D; a++) {
+			oo[a] = o[a];
+			dd[a] = d[a];
+		}
+		const auto h = fo::Raycast<D, L>(s).ray(oo, dd);
+		for (int a = 0; a < D; a++) out[a] = h[a];
+	}
 };
 
 template <int D, int L>
@@ -289,6 +300,21 @@ int fo_get(void* s, const int* pos, float* out)
 {
 	return guard([&] { *out = static_cast<SurfBase*>(s)->get(pos); });
 }
+/* Surface::ray for n rays (origins, directions: n*D floats); hits n*D floats, FLT_MAX when
+ * missed. */
+int fo_ray(void* s, const float* origins, const float* dirs, size_t n, float* hits)
+{
+	return guard([&] {
+		SurfBase* b = static_cast<SurfBase*>(s);
+		const int D = b->dims;
+		// rays are independent reads of the surface (Surface::ray is const): spread over the
+		// configured threads, each writing only its own hit
+		fo::parallel_items((long)n, [&](long i) {
+			b->ray(origins + i * D, dirs + i * D, hits + i * D);
+		});
+	});
+}
+
 int fo_curv(void* s, const int* pos, float* out)
 {
 	return guard([&] { static_cast<SurfBase*>(s)->curv(pos, out); });

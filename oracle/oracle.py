@@ -139,6 +139,19 @@ class Surface:
         _chk(lib().fo_curv(self._h, _ivec(pos), C.byref(v)))
         return v.value
 
+    def rays(self, origins, dirs):
+        """Surface::ray for each (origin, direction) row; rows of FLT_MAX where missed."""
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, self.D)
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, self.D)
+        out = np.zeros_like(o)
+        _chk(lib().fo_ray(self._h, o.ctypes.data_as(C.POINTER(C.c_float)),
+                          d.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(o.shape[0]),
+                          out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def ray(self, origin, direction):
+        return self.rays([origin], [direction])[0]
+
     def partitions(self):
         cnt = C.c_size_t()
         cs = (C.c_int * self.D)()

@@ -244,10 +244,94 @@ def neighs_case(root):
     return dict(ref=f"{f}:2398-2416", centre=pts[0], order=pts[1:])
 
 
+VEC = r"Vec([23])[fi]\(([^()]*)\)"
+
+
+def vec_of(text):
+    """Numbers of the first VecNf/VecNi(...) literal in a line."""
+    m = re.search(VEC, text)
+    return [float(x.strip().rstrip("f")) for x in m.group(2).split(",")]
+
+
+def ray_cases(root):
+    """Raycasting (test_Surface.cpp, SCENARIO "Surface - raycasting"): per case the surface set
+    up by its GIVEN (size, partition, layers, seed, updates), the ray (origin, direction,
+    whether the test normalises it) and the expectation: a hit position with its Approx epsilon,
+    a miss, or any hit. Rotation sweeps record the axis; the rays follow from it."""
+    rel = "src/tests/test_Surface.cpp"
+    ln = lines_of(root, rel)
+    at = lambda i: ln[i - 1]
+
+    def setup(decl_line):
+        m = re.search(r"Surface<(\d), (\d)> surface\((Vec\di\([^)]*\)), (Vec\di\([^)]*\))\)",
+                      at(decl_line))
+        D, L = int(m.group(1)), int(m.group(2))
+        size = [int(x) for x in vec_of(m.group(3))]
+        part = [int(x) for x in vec_of(m.group(4))]
+        return D, L, size, part
+
+    def updates(first, last):
+        out = []
+        for i in range(first, last + 1):
+            m = re.search(r"return (-?\d+(?:\.\d+)?)f;", at(i))
+            if m:
+                out.append(["update", float(m.group(1))])
+        return out
+
+    cases = []
+    # GIVEN at 1284: seed at 1286, three updates 1287-1295
+    D, L, size, part = setup(1284)
+    base = [["seed", [int(x) for x in vec_of(at(1286))]]] + updates(1287, 1295)
+    for ray_ln, chk_ln, extra in [(1301, 1305, []), (1311, 1315, []), (1321, 1325, []),
+                                  (1331, 1335, []), (1347, 1351, updates(1341, 1343)),
+                                  (1358, 1362, []), (1368, 1372, [])]:
+        r = at(ray_ln)
+        vecs = re.findall(VEC, r)
+        origin = [float(x.strip().rstrip("f")) for x in vecs[0][1].split(",")]
+        direction = [float(x.strip().rstrip("f")) for x in vecs[1][1].split(",")]
+        c = at(chk_ln)
+        if "!= surface.ray_miss" in c:
+            expect, hit = "hit", None
+        elif "== surface.ray_miss" in c:
+            expect, hit = "miss", None
+        else:
+            expect, hit = "at", vec_of(c)
+        cases.append(dict(ref=f"{rel}:{ray_ln}-{chk_ln}", dims=D, layers=L, size=size, part=part,
+                          steps=base + extra, origin=origin, dir=direction,
+                          normalize="normalized()" in r, expect=expect, hit=hit,
+                          epsilon=float(re.search(r"epsilon\(([\d.]+)\)", c).group(1))
+                          if "epsilon(" in c else None))
+    # 2D GIVEN at 1420: seed 1423, updates 1424-1432, ray 1438, check 1442
+    D2, L2, size2, part2 = setup(1420)
+    steps2 = [["seed", [int(x) for x in vec_of(at(1423))]]] + updates(1424, 1432)
+    r, c = at(1438), at(1442)
+    vecs = re.findall(VEC, r)
+    cases.append(dict(ref=f"{rel}:1438-1442", dims=D2, layers=L2, size=size2, part=part2,
+                      steps=steps2,
+                      origin=[float(x.strip().rstrip("f")) for x in vecs[0][1].split(",")],
+                      dir=[float(x.strip().rstrip("f")) for x in vecs[1][1].split(",")],
+                      normalize=False, expect="at", hit=vec_of(c),
+                      epsilon=float(re.search(r"epsilon\(([\d.]+)\)", c).group(1))))
+    # rotation sweeps (1373-1413 on the GIVEN at 1284; 1495-1533 on the GIVEN at 1479): rays
+    # from R*(0, 0, -10) along R*(0, 0, 1), R = AngleAxis(k * 0.1 * pi, axis), k = 0..19
+    for given, lo, hi in [(1284, 1373, 1413), (1479, 1495, 1533)]:
+        Dg, Lg, sz, pt = setup(given)
+        st = [["seed", [0, 0, 0]]] + updates(given + 3, given + 11)
+        for i in range(lo, hi + 1):
+            t = at(i)
+            if "check(Vec3f" not in t:
+                continue
+            axis = [0.0, 1.0, 0.0] if "UnitY" in t else vec_of(t)
+            cases.append(dict(ref=f"{rel}:{i}", dims=Dg, layers=Lg, size=sz, part=pt, steps=st,
+                              sweep_axis=axis, normalize_axis="normalized()" in t,
+                              expect="hit"))
+    return cases
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
-               curvature=curvature_cases(root), neighs=neighs_case(root))
+               curvature=curvature_cases(root), neighs=neighs_case(root), ray=ray_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

@@ -135,3 +135,23 @@ def test_tables_match_reference_source():
             nib = (packed[m] >> (4 * k)) & 0xF
             row.append(-1 if nib == 0xF else nib)
         assert row == ref[m * 16:(m + 1) * 16], m
+
+
+@pytest.mark.parametrize("case", _cases("ray"), ids=lambda c: c["ref"].split(":")[-1])
+def test_ray_golden(case):
+    """Surface::ray of the oracle against the reference's raycasting assertions."""
+    from tests.raycases import case_rays, check_case
+    s = O.Surface(case["size"], case["part"], case["layers"])
+    run_steps(s, case["steps"])
+    o, d = case_rays(case)
+    check_case(case, s.rays(o, d))
+
+
+def test_ray_sweep_count():
+    """A rotation sweep casts 20 rays: rot_mult = 0, 0.1, ..., 1.9 accumulated in float32 (the
+    twentieth addition of 0.1f reaches 2.0000002, which ends the loop)."""
+    from tests.raycases import sweep_rays
+    o, d = sweep_rays([0, 1, 0], False)
+    assert len(o) == 20
+    np.testing.assert_allclose(o[0], [0, 0, -10])
+    np.testing.assert_allclose(d[5], [1, 0, 0], atol=1e-6)
