@@ -219,7 +219,7 @@ int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, flo
 }
 
 int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits,
-                  int buffer)
+                  int exact_order)
 {
 	return guard([&] {
 		need(s, "surface");
@@ -228,9 +228,8 @@ int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t
 			need(dirs, "dirs");
 			need(hits, "hits");
 		}
-		if (buffer < -1 || buffer > fg::ray_buffer_max())
-			throw fg::Error(FG_ERR_ARG, "candidate buffer out of range");
-		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, true, buffer);
+		if (exact_order != 0 && exact_order != 1) throw fg::Error(FG_ERR_ARG, "exact_order is 0 or 1");
+		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, true, exact_order == 1);
 	});
 }
 

@@ -291,6 +291,7 @@ public:
 		return n;
 	}
 	const Dev& dev() const override { return P_; }
+	const SurfGeom& geometry(int s) const override { return geom_[s]; }
 	void sync() override { FG_CUDA(cudaStreamSynchronize(st_)); }
 	int part(int a) const override { return csz_[a]; }
 
@@ -979,8 +980,20 @@ private:
 	StepStats stats_;
 };
 
+void keep_pool_memory()
+{
+	int dev = 0;
+	cudaMemPool_t pool;
+	if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+		uint64_t keep = UINT64_MAX;
+		cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+	}
+	cudaGetLastError();
+}
+
 EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream)
 {
+	keep_pool_memory();
 #define FG_CASE(d, l) \
 	if (desc.D == d && desc.L == l) return new Engine<d, l>(desc, stream);
 	FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)

@@ -88,11 +88,18 @@ public:
 	virtual void set_paused(int s, bool on) = 0;
 	virtual bool paused(int s) const = 0;
 	virtual const Dev& dev() const = 0;
+	/// Host copy of surface s's geometry (the same as dev().geom[s]).
+	virtual const SurfGeom& geometry(int s) const = 0;
 	virtual void sync() = 0;
 	virtual int part(int a) const = 0;
 };
 
 EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream);
+
+/// Makes memory freed by cudaFreeAsync stay in the current device's stream-ordered pool for
+/// the next cudaMallocAsync (polygon arenas, ray queues) instead of going back to the driver
+/// at every synchronisation.
+void keep_pool_memory();
 
 // ---- launch accounting and per-kernel timing ----
 /// Called around every kernel launch of the library: counts launches and, when profiling is

@@ -17,6 +17,21 @@ __device__ __forceinline__ bool inside_f(const SurfGeom& g, const float* p)
 	return true;
 }
 
+/// The reduction of interp (NumericMixin.hpp:403-481): corner values v in bit order (bit a set
+/// = +1 along axis a), reduced along axis 0 first with weights from the fractions pc.
+template <int D>
+__device__ __forceinline__ float interp_reduce(float* v, const float* pc)
+{
+#pragma unroll
+	for (int r = 0; r < D; r++) {
+		const float t = pc[r];
+#pragma unroll
+		for (int i = 0; i < (1 << (D - 1 - r)); i++)
+			v[i] = __fadd_rn(__fmul_rn(t, v[2 * i + 1]), __fmul_rn(__fsub_rn(1.0f, t), v[2 * i]));
+	}
+	return v[0];
+}
+
 /// interp (NumericMixin.hpp:403-481): corners in bit order, reduced along axis 0 first.
 template <int D, class Get>
 __device__ __forceinline__ float interp(const Get& get, const float* p)
@@ -37,15 +52,7 @@ __device__ __forceinline__ float interp(const Get& get, const float* p)
 		for (int a = 0; a < D; a++) q[a] += (i >> a) & 1;
 		v[i] = get(q);
 	}
-	int n = 1 << D;
-#pragma unroll
-	for (int r = 0; r < D; r++) {
-		const float t = pc[r];
-		for (int i = 0; i < n / 2; i++)
-			v[i] = __fadd_rn(__fmul_rn(t, v[2 * i + 1]), __fmul_rn(__fsub_rn(1.0f, t), v[2 * i]));
-		n >>= 1;
-	}
-	return v[0];
+	return interp_reduce<D>(v, pc);
 }
 
 /// grad (NumericMixin.hpp:188-231) at an integer node.
@@ -73,11 +80,12 @@ __device__ __forceinline__ void grad_i(const Get& get, const SurfGeom& g, const 
 	}
 }
 
-/// grad at a real position: the probe coordinate steps -1, +2, -1 in FP32.
-template <int D, int L, class Get>
-__device__ __forceinline__ void grad_f(const Get& get, const SurfGeom& g, const float* p, float* out)
+/// grad (NumericMixin.hpp:188-231) at a real position whose interpolated value `centre` is
+/// known, over any interpolation ip(position): the probe coordinate steps -1, +2, -1 in FP32.
+template <int D, int L, class Interp>
+__device__ __forceinline__ void grad_with(const Interp& ip, const SurfGeom& g, const float* p,
+                                          float centre, float* out)
 {
-	const float centre = interp<D>(get, p);
 	float t[D];
 #pragma unroll
 	for (int a = 0; a < D; a++) t[a] = p[a];
@@ -87,17 +95,32 @@ __device__ __forceinline__ void grad_f(const Get& get, const SurfGeom& g, const 
 		int order = 0;
 		t[a] = __fsub_rn(t[a], 1.0f);
 		if (inside_f<D, L>(g, t)) {
-			back = interp<D>(get, t);
+			back = ip(t);
 			order++;
 		}
 		t[a] = __fadd_rn(t[a], 2.0f);
 		if (inside_f<D, L>(g, t)) {
-			fwd = interp<D>(get, t);
+			fwd = ip(t);
 			order++;
 		}
 		t[a] = __fsub_rn(t[a], 1.0f);
 		out[a] = order ? __fdiv_rn(__fsub_rn(fwd, back), (float)order) : 0.0f;
 	}
+}
+
+/// grad at a real position whose interpolated value `centre` is known.
+template <int D, int L, class Get>
+__device__ __forceinline__ void grad_fc(const Get& get, const SurfGeom& g, const float* p,
+                                        float centre, float* out)
+{
+	grad_with<D, L>([&](const float* t) { return interp<D>(get, t); }, g, p, centre, out);
+}
+
+/// grad at a real position (NumericMixin.hpp:188-231 over interp).
+template <int D, int L, class Get>
+__device__ __forceinline__ void grad_f(const Get& get, const SurfGeom& g, const float* p, float* out)
+{
+	grad_fc<D, L>(get, g, p, interp<D>(get, p), out);
 }
 
 /// Eigen's fixed-size dot product: products summed x0 + x1 in 2D, x0 + (x1 + x2) in 3D.

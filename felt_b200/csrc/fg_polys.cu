@@ -660,18 +660,7 @@ public:
 		const long long vc = vertex_capacity ? std::max<long long>((long long)vertex_capacity, 64)
 		                                     : (1LL << 20);
 		if (vc >= (1LL << 30)) throw Error(-1, "vertex capacity too large");
-		// freed arena memory stays in this process's stream-ordered pool for the next regrowth
-		// instead of going back to the driver at every synchronisation
-		{
-			int dev = 0;
-			cudaMemPool_t pool;
-			cudaGetDevice(&dev);
-			if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-				uint64_t keep = UINT64_MAX;
-				cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-			}
-			cudaGetLastError();
-		}
+		keep_pool_memory();
 		alloc_arena(vc, 2 * vc);
 		int bvol = 1;
 		for (int a = 0; a < D; a++) bvol *= eng.part(a) + 1;

@@ -9,13 +9,10 @@ namespace fg {
 
 /// Casts n rays (origins and directions, n*D floats each) at surface s of the pool; hits
 /// receives n*D floats, FLT_MAX in every component for a ray that misses. With device_ptrs the
-/// three arrays are device memory of the pool's GPU, else host memory. buffer: candidate
-/// partitions a ray sorts in registers/local memory before it falls back to re-walking its
-/// planes (< 0 = the default, ray_buffer_max()); the result does not depend on it.
+/// three arrays are device memory of the pool's GPU, else host memory. exact_order: find each
+/// next candidate partition by a full walk of the planes instead of merging the per-axis walks
+/// (the same order; used to test the merge).
 void ray_batch(EngineBase& eng, int s, const float* origins, const float* dirs, size_t n,
-               float* hits, bool device_ptrs, int buffer = -1);
-
-/// Largest candidate buffer a ray keeps.
-int ray_buffer_max();
+               float* hits, bool device_ptrs, bool exact_order = false);
 
 }  // namespace fg

@@ -129,15 +129,15 @@ FG_API int fg_get(fg_surface* s, const int* pos, float* out);
 /* ray(origin, dir) (include/Felt/Surface.hpp:468-616, 1450-1598) for n rays at once: the
  * point where each ray first meets the zero curve, or FLT_MAX in every component (the
  * reference's ray_miss) when it misses. origins, dirs and hits hold n*dims floats each, in host
- * memory; every ray runs on its own GPU thread, in the reference's FP32 arithmetic. */
+ * memory; each ray runs on one GPU thread, in the reference's FP32 arithmetic. */
 FG_API int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits);
 
-/* fg_ray with origins, dirs and hits in device memory of the surface's GPU, and an explicit
- * per-ray candidate buffer (0..64 partitions; -1 = 64). Rays with more candidate partitions than
- * the buffer holds re-walk their partition planes for each next candidate; the hits do not
- * depend on the buffer size. */
+/* fg_ray with origins, dirs and hits in device memory of the surface's GPU. exact_order = 1
+ * finds each ray's next candidate partition by a full walk of its planes instead of merging the
+ * per-axis walks; the order, and so the hits, are the same (it exists to test that); 0 is the
+ * fast default. */
 FG_API int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n,
-                         float* hits, int buffer);
+                         float* hits, int exact_order);
 
 /* Geometry of the children (partition) grid: count, size and offset of the children grid. */
 FG_API int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);

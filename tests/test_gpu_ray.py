@@ -113,20 +113,23 @@ def test_ray_random_parity(si):
     assert 0.05 < hit_frac < 1.0, hit_frac  # both hits and misses are exercised
 
 
-def test_ray_candidate_buffer_does_not_change_hits():
-    """A ray with more candidate partitions than its buffer re-walks its planes per candidate;
-    the hits are the same for every buffer size, including none."""
+@pytest.mark.parametrize("si", range(len(SCENES)))
+def test_ray_merge_order_equals_exact_order(si):
+    """The kernel orders a ray's candidates by merging its per-axis plane walks; finding each
+    next candidate by a full walk (the reference's sort, restated) gives the same hits."""
     import torch
-    g, o = _scene(SCENES[3])
-    org, d = random_rays(2, SCENES[3][0], 900, seed=7)
+    g, o = _scene(SCENES[si])
+    D = len(SCENES[si][0])
+    org, d = random_rays(D, SCENES[si][0], 900, seed=7 + si)
     want = o.rays(org, d)
     to = torch.from_numpy(org).cuda()
     td = torch.from_numpy(d).cuda()
-    for buf in (-1, 0, 1, 3, 64):
+    for exact in (False, True):
         th = torch.empty_like(to)
-        g.rays_device(to.data_ptr(), td.data_ptr(), org.shape[0], th.data_ptr(), buffer=buf)
+        g.rays_device(to.data_ptr(), td.data_ptr(), org.shape[0], th.data_ptr(),
+                      exact_order=exact)
         torch.cuda.synchronize()
-        assert_rays_equal(th.cpu().numpy(), want, f"buffer {buf}")
+        assert_rays_equal(th.cpu().numpy(), want, f"exact_order={exact}")
 
 
 def test_ray_edge_cases():
@@ -136,7 +139,7 @@ def test_ray_edge_cases():
     with pytest.raises(ValueError):
         g.rays(np.zeros((2, 3)), np.zeros((3, 3)))
     with pytest.raises(fb.FeltError):
-        g.rays_device(0, 0, 4, 0, buffer=65)
+        g.rays_device(0, 0, 4, 0, exact_order=2)
     # a zero direction never leaves its partition and finds no crossing: a miss on both sides
     org = np.array([[-3.0, 0.5, 0.25], [100.0, 0, 0], [-20.0, -20.0, -20.0]], np.float32)
     d = np.array([[0, 0, 0], [-1, 0, 0], [0, 0, 1]], np.float32)
@@ -162,3 +165,19 @@ def test_batch_rays_match_single_surfaces():
     for i, (o, sz) in enumerate(zip(os_, sizes)):
         org, d = random_rays(3, sz, 600, seed=40 + i)
         assert_rays_equal(b.rays(i, org, d), o.rays(org, d), f"surface {i}")
+
+
+def test_ray_convergence_leaving_the_grid_resumes():
+    """Where the zero curve meets the grid's walls, some convergences step out of the grid:
+    that partition gives ray_miss and the ray goes on with its next candidate (Surface.hpp:
+    1491-1494 and 607-614). The device runs those rays in a second pass of its find/converge
+    kernels; their hits must still equal the oracle's."""
+    fb = _fb()
+    scene = ((20, 20, 20), (5, 5, 5), 3, [(0, 0, 0)], [(13, dict(c=-1.0))])
+    g, o = _scene(scene)
+    org, d = random_rays(3, scene[0], 3000, seed=5)
+    l0 = fb.launch_count()
+    hits = g.rays(org, d)
+    passes = (fb.launch_count() - l0) // 2
+    assert passes >= 2, "no convergence left the grid: the scene no longer tests the resume"
+    assert_rays_equal(hits, o.rays(org, d), "resumed rays")
