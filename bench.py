@@ -636,20 +636,21 @@ def run_ray(args, name, cfg):
         torch.cuda.synchronize()
         fb.profile_enable(False)
         prof = fb.profile_read()
-        # one cast = k_ray_find + k_ray_conv (plus a pass of each per resumed round, rare)
+        # one cast = k_ray_ranges, k_ray_walk, k_ray_march, k_ray_find, k_ray_conv (plus
+        # k_ray_find and k_ray_conv again per resumed round, rare); the roofline covers them all
         ms = sum(v[0] for k, v in prof.items() if k.startswith("k_ray"))
         calls = 3
         hbm, peak_kind = load_peaks()
         per = 3 * 4 * cfg["D"]
         achieved = per * n / (ms / calls * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "k_ray_find+k_ray_conv", "achieved": achieved,
+        roof = {"bound": "hbm", "kernel": "k_ray_walk+march+conv", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / hbm,
                 "traffic": None, "bytes_per_launch": per * n, "avg_launch_us": 1e3 * ms / calls,
                 "kernels": {k: {"ms_per_cast": v[0] / calls, "launches": v[1]}
                             for k, v in prof.items()}}
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
-            t = json.load(open(tf)).get("k_ray_find+k_ray_conv")
+            t = json.load(open(tf)).get("k_ray_walk+march+conv")
             if t:
                 roof["traffic"] = t["bytes_per_unit"] * n
         if ws == 1 and not args.no_cpu:

@@ -196,12 +196,12 @@ class Surface:
         """Surface::ray(origin, dir) for one ray."""
         return self.rays([origin], [direction])[0]
 
-    def rays_device(self, origins_ptr, dirs_ptr, n, hits_ptr, exact_order=False):
+    def rays_device(self, origins_ptr, dirs_ptr, n, hits_ptr, order_mode=0):
         """rays() over device arrays of n*D floats (e.g. torch CUDA tensors' data_ptr()).
-        exact_order: each next candidate partition by a full walk of the planes instead of the
-        merge of the per-axis walks (same order and hits; slower)."""
+        order_mode: 0 (default) merges per-axis candidate lists, 1 finds each next candidate by
+        a full walk, 2 merges per-axis cursors; same order and hits, 1 and 2 are slower."""
         _chk(lib().fg_ray_device(self._h, C.c_void_p(origins_ptr), C.c_void_p(dirs_ptr),
-                                 C.c_size_t(n), C.c_void_p(hits_ptr), C.c_int(int(exact_order))))
+                                 C.c_size_t(n), C.c_void_p(hits_ptr), C.c_int(int(order_mode))))
 
     def partitions(self):
         cnt = C.c_size_t()

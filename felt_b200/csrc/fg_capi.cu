@@ -219,7 +219,7 @@ int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, flo
 }
 
 int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits,
-                  int exact_order)
+                  int order_mode)
 {
 	return guard([&] {
 		need(s, "surface");
@@ -228,8 +228,8 @@ int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t
 			need(dirs, "dirs");
 			need(hits, "hits");
 		}
-		if (exact_order != 0 && exact_order != 1) throw fg::Error(FG_ERR_ARG, "exact_order is 0 or 1");
-		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, true, exact_order == 1);
+		if (order_mode < 0 || order_mode > 2) throw fg::Error(FG_ERR_ARG, "order_mode is 0, 1 or 2");
+		fg::ray_batch(*s->eng, 0, origins, dirs, n, hits, true, order_mode);
 	});
 }
 

@@ -33,7 +33,7 @@
 // than any later one. As a safety net the kernel also checks the keys it consumes; a decrease
 // would make the ray restart its candidates in exact order (each next candidate by a full walk
 // of the planes, the (distance, discovery index) after the previous one), the order
-// fg_ray_device's exact_order selects for every ray.
+// fg_ray_device's mode 1 selects for every ray.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -406,15 +406,35 @@ struct ConvItem {
 /// A ray to continue after a convergence that left the grid (Surface.hpp:1491-1494): the
 /// partition's ray_child returned ray_miss, so the next candidate follows.
 struct ResumeItem {
-	int ray, m, exact;
+	int ray;
+	int m;       // candidates consumed before (replayed without marching)
+	int exact;   // candidates in exact order
+	int origin;  // the origin's partition is still to march
 };
 
+/// Queues of one pass. counters: [0] next input of k_ray_find, [1] queued convergences,
+/// [2] rays resumed by k_ray_conv, [3] next convergence, [4] next ray of k_ray_march,
+/// [5] rays k_ray_march leaves to k_ray_find.
 struct RayQueues {
-	int* counters;  // [0] next input of the find pass, [1] convergences, [2] resumes
+	int* counters;
 	ConvItem* conv;
-	const ResumeItem* resume_in;  // input of a resumed pass (null: every ray, from the start)
-	ResumeItem* resume_out;
-	int n_in;
+	const ResumeItem* find_in;  // input of k_ray_find
+	const int* find_n_ptr;      // its length in device memory, or null: find_n
+	int find_n;
+	ResumeItem* resume_out;     // rays k_ray_conv sends back
+	ResumeItem* slow;           // rays k_ray_march leaves to k_ray_find
+};
+
+/// Candidate lists of k_ray_walk, structure of arrays over the rays of a pass: entry j of ray
+/// r at j * n + r (the runs of axes 0..D-1 one after another, each in its walk's order; a
+/// candidate is its partition and plane, its key is recomputed from them), run lengths at
+/// a * n + r; a first run length of -1 sends the ray to k_ray_find.
+constexpr int RAY_LIST = 24;
+struct RayLists {
+	float* plane;
+	int* gp;
+	int* cnt;
+	int n;
 };
 
 __device__ __forceinline__ int fetch_next(int* counter)
@@ -426,14 +446,16 @@ __device__ __forceinline__ int fetch_next(int* counter)
 }
 
 /// Surface::ray up to the sample where a convergence starts (Surface.hpp:468-616 with
-/// ray_child, 1450-1487). Persistent threads, one ray at a time per thread: the origin's
-/// partition, then candidates in order, marching each; a ray with a convergence to run is
-/// queued for k_ray_conv, a ray without candidates left gets ray_miss.
+/// ray_child, 1450-1487), for the rays k_ray_walk could not list and those resumed after a
+/// convergence left the grid. Persistent threads, one ray at a time per thread: the origin's
+/// partition, then candidates in order (merged from per-axis cursors, or in exact order),
+/// marching each; a ray with a convergence to run is queued for k_ray_conv, a ray without
+/// candidates left gets ray_miss.
 template <int D, int L>
 __global__ void __launch_bounds__(RAY_THREADS) k_ray_find(const __grid_constant__ Dev P,
                                                           const __grid_constant__ SurfGeom G,
                                                           const float* org, const float* dirs,
-                                                          int exact_all, RayQueues Q, float* hit)
+                                                          RayQueues Q, float* hit)
 {
 	__shared__ AxisWalk s_aw[RAY_THREADS][D];
 	__shared__ Cursor s_cur[RAY_THREADS][D];
@@ -452,22 +474,16 @@ __global__ void __launch_bounds__(RAY_THREADS) k_ray_find(const __grid_constant_
 	float last_key = -1.0f;
 	int last_disc = -1;
 
+	const int n_in = Q.find_n_ptr ? *Q.find_n_ptr : Q.find_n;
 	for (;;) {
 		if (phase == PH_FETCH) {
 			const int idx = fetch_next(Q.counters);
-			if (idx >= Q.n_in) break;
-			bool origin = true;
-			if (Q.resume_in) {
-				const ResumeItem r = Q.resume_in[idx];
-				ray = r.ray;
-				replay = r.m;
-				exact = r.exact != 0;
-				origin = false;
-			} else {
-				ray = idx;
-				replay = 0;
-				exact = exact_all != 0;
-			}
+			if (idx >= n_in) break;
+			const ResumeItem r = Q.find_in[idx];
+			ray = r.ray;
+			replay = r.m;
+			exact = r.exact != 0;
+			const bool origin = r.origin != 0;
 #pragma unroll
 			for (int a = 0; a < D; a++) {
 				o[a] = __ldg(org + (size_t)ray * D + a);
@@ -616,13 +632,331 @@ __global__ void __launch_bounds__(RAY_THREADS) k_ray_find(const __grid_constant_
 	}
 }
 
+/// The isogrid value at an integer position, read relative to home h as HomeInterp reads its
+/// corners (positions more than one partition away through the partition lookup).
+template <int D, int L>
+__device__ __forceinline__ float home_get(const Dev& P, const SurfGeom& g, const Home& h,
+                                          const Vec<D>& q)
+{
+	if (!in_grid<D>(g, q)) return (float)(L + 1);
+	int nb = h.gp, leaf = 0, stride = 1;
+#pragma unroll
+	for (int a = D - 1; a >= 0; a--) {
+		const int cs = P.csz[a];
+		const int r = q[a] - h.lo[a];
+		if (r < -cs || r >= 2 * cs) return get_phi<D, L>(P, g, q);
+		const int st = (r >= cs) - (r < 0);
+		nb += st * stride;
+		leaf += (r - st * cs) * P.lstr[a];
+		stride *= g.ccount[a];
+	}
+	const int sl = nb == h.gp ? h.sl : __ldg(P.slot + nb);
+	if (sl >= 0) return __ldg(P.phi + (size_t)sl * P.BV + leaf);
+	return nb == h.gp ? h.bg : __ldg(P.bg + nb);
+}
+
+/// Sub-blocks of RAY_SB^D nodes of an active brick, for the march: a sample whose floor lies in
+/// sub-block b has its 2^D corners among the sub-block's nodes and the next node along each
+/// axis. If all of those are >= 0.5001 (or all <= -0.5001), every interpolation there is too (a
+/// convex combination, rounded), so its layer is not 0 and the sample can be stepped over.
+constexpr int RAY_SB = 4;
+
+__device__ __forceinline__ int sub_count(int cs) { return (cs + RAY_SB - 1) / RAY_SB; }
+
+/// Flags of every sub-block of every active brick of surface s (1: all >= 0.5001, 2: all
+/// <= -0.5001, else 0), brick slot major. One thread per (slot, sub-block).
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_ray_ranges(const __grid_constant__ Dev P,
+                                                    const __grid_constant__ SurfGeom G, int s,
+                                                    uint8_t* flags, int nsub)
+{
+	const SurfGeom& g = G;
+	const size_t total = (size_t)P.nslots * nsub;
+	for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+	     t += (size_t)gridDim.x * blockDim.x) {
+		const int slot = (int)(t / nsub);
+		const int gp = __ldg(P.slot_gp + slot);
+		uint8_t f = 0;
+		if (gp >= 0 && __ldg(P.surf_of + gp) == s && __ldg(P.slot + gp) == slot) {
+			const Home h = home_of<D>(P, gp);
+			int b[D], rem = (int)(t % nsub);
+#pragma unroll
+			for (int a = D - 1; a >= 0; a--) {
+				const int nb = sub_count(P.csz[a]);
+				b[a] = rem % nb;
+				rem /= nb;
+			}
+			float mn = __int_as_float(0x7f800000), mx = -mn;
+			constexpr int E = RAY_SB + 1;
+			int cnt = 1;
+#pragma unroll
+			for (int a = 0; a < D; a++) cnt *= E;
+			for (int i = 0; i < cnt; i++) {
+				Vec<D> q;
+				int r = i;
+#pragma unroll
+				for (int a = D - 1; a >= 0; a--) {
+					q[a] = h.lo[a] + b[a] * RAY_SB + r % E;
+					r /= E;
+				}
+				const float v = home_get<D, L>(P, g, h, q);
+				mn = fminf(mn, v);
+				mx = fmaxf(mx, v);
+			}
+			f = mn >= 0.5001f ? 1 : (mx <= -0.5001f ? 2 : 0);
+		}
+		flags[t] = f;
+	}
+}
+
+/// grad at x (value c) around home h, normalised: out of line for the march, which needs it only
+/// at zero-layer samples.
+template <int D, int L>
+__device__ __noinline__ float3 march_grad(const Dev& P, const SurfGeom& g, Home h, float x0,
+                                          float x1, float x2, float c)
+{
+	const float x[3] = {x0, x1, x2};
+	float gr[3] = {0.0f, 0.0f, 0.0f};
+	grad_with<D, L>(HomeInterp<D, L>{P, g, h}, g, x, c, gr);
+	normalize_d<D>(gr);
+	return make_float3(gr[0], gr[1], gr[2]);
+}
+
+/// The key (squared distance from the origin) of entry j of a ray's list, an axis-`dim` crossing:
+/// the same arithmetic as when the walk found it.
+template <int D>
+__device__ __forceinline__ float list_key(const RayLists& R, int ray, int j, const float* o,
+                                          const float* dir, int dim)
+{
+	const float plane = R.plane[(size_t)j * R.n + ray];
+	const float vd = pick<D>(dir, dim);
+	float p[D];
+	crossing<D>(o, dir, pick<D>(o, dim), vd, sgnf(vd), plane, p);
+	return dist2<D>(p, o);
+}
+
+/// The candidate walk of Surface::ray (Surface.hpp:520-600), one ray per thread: every
+/// plane of every axis, the candidates of each axis stored in its walk's order. A ray with more
+/// than RAY_LIST candidates, or whose keys decrease along an axis, is marked for k_ray_find.
+template <int D, int L>
+__global__ void __launch_bounds__(RAY_THREADS) k_ray_walk(const __grid_constant__ Dev P,
+                                                          const __grid_constant__ SurfGeom G,
+                                                          const float* org, const float* dirs,
+                                                          RayLists R)
+{
+	const SurfGeom& g = G;
+	const int n = R.n;
+	for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+		float o[D], dir[D];
+#pragma unroll
+		for (int a = 0; a < D; a++) {
+			o[a] = __ldg(org + (size_t)r * D + a);
+			dir[a] = __ldg(dirs + (size_t)r * D + a);
+		}
+		int total = 0;
+		bool ok = true;
+#pragma unroll 1
+		for (int dim = 0; dim < D; dim++) {
+			const AxisWalk w = axis_walk<D, L>(P, g, o, dir, dim);
+			int cnt = 0;
+			float last = -1.0f;
+#pragma unroll 1
+			for (int k = 0; k < w.kend; k++) {
+				const float plane = plane_at(w, k);
+				int gp = -1;
+				float key = 0.0f;
+				const int st = check_track<D, L>(P, g, o, dir, w.od, w.vd, w.dd, plane, gp, key);
+				if (st == -1 && k >= 1) break;
+				if (st != 1) continue;
+				ok = ok && key >= last;
+				last = key;
+				if (total < RAY_LIST) {
+					const size_t j = (size_t)total * n + r;
+					R.plane[j] = plane;
+					R.gp[j] = gp;
+				}
+				total++;
+				cnt++;
+			}
+			R.cnt[(size_t)dim * n + r] = cnt;
+		}
+		if (!ok || total > RAY_LIST) R.cnt[r] = -1;
+	}
+}
+
+/// Surface::ray up to the sample where a convergence starts, over k_ray_walk's lists: the
+/// origin's partition, then the candidates in order (the merge of the per-axis runs, ties to
+/// the lower axis), consecutive repeats of a partition dropped, marching each. Persistent
+/// threads; a ray with a convergence to run is queued for k_ray_conv, a ray without candidates
+/// left gets ray_miss, an unlisted ray goes to k_ray_find.
+template <int D, int L>
+__global__ void __launch_bounds__(RAY_THREADS, 8) k_ray_march(const __grid_constant__ Dev P,
+                                                           const __grid_constant__ SurfGeom G,
+                                                           const float* org, const float* dirs,
+                                                           int mode, RayLists R,
+                                                           const uint8_t* ranges, int nsub,
+                                                           RayQueues Q, float* hit)
+{
+	__shared__ int s_head[D][RAY_THREADS], s_end[D][RAY_THREADS];
+	__shared__ float s_key[D][RAY_THREADS];  // key of each run's head
+	const int tid = threadIdx.x;
+	const SurfGeom& g = G;
+	const int n = R.n;
+	int ray = 0, phase = PH_FETCH;
+	float o[D], dir[D];
+	float pos[D];  // start of the partition's march
+	Home hm;
+	bool bskip = false;
+	int k = 0;
+	int stale = 0;  // runs whose head key is to be computed (bit per axis)
+	int prev = -1, consumed = 0;
+	for (;;) {
+		if (phase == PH_FETCH) {
+			ray = fetch_next(Q.counters + 4);
+			if (ray >= n) break;
+			if (mode != 0 || R.cnt[ray] < 0) {
+				const int si = atomicAdd(Q.counters + 5, 1);
+				Q.slow[si] = ResumeItem{ray, 0, mode == 1 ? 1 : 0, 1};
+				continue;
+			}
+#pragma unroll
+			for (int a = 0; a < D; a++) {
+				o[a] = __ldg(org + (size_t)ray * D + a);
+				dir[a] = __ldg(dirs + (size_t)ray * D + a);
+			}
+			int start = 0;
+#pragma unroll
+			for (int a = 0; a < D; a++) {
+				s_head[a][tid] = start;
+				start += R.cnt[(size_t)a * n + ray];
+				s_end[a][tid] = start;
+			}
+			stale = (1 << D) - 1;
+			prev = -1;
+			consumed = 0;
+			phase = PH_NEXT;
+			if (inside_f<D, L>(g, o)) {
+				// the origin's partition first; Eigen cast<int> truncates
+				Vec<D> pc;
+#pragma unroll
+				for (int a = 0; a < D; a++) pc[a] = (int)o[a];
+				hm = home_of<D>(P, part_of<D>(P, g, pc));
+				bskip = skippable(hm);
+#pragma unroll
+				for (int a = 0; a < D; a++) pos[a] = o[a];
+				k = 0;
+				phase = PH_MARCH;
+			}
+		}
+		while (phase == PH_NEXT) {
+			int axis = -1;
+			float bk = 0.0f;
+#pragma unroll 1
+			for (int a = 0; a < D; a++) {
+				const int h = s_head[a][tid];
+				if (h >= s_end[a][tid]) continue;
+				if ((stale >> a) & 1) s_key[a][tid] = list_key<D>(R, ray, h, o, dir, a);
+				const float ka = s_key[a][tid];
+				if (axis < 0 || ka < bk) {  // ties go to the lower axis
+					bk = ka;
+					axis = a;
+				}
+			}
+			stale = 0;
+			if (axis < 0) {  // no candidate left: ray_miss
+#pragma unroll
+				for (int a = 0; a < D; a++) hit[(size_t)ray * D + a] = FLT_MAX;
+				phase = PH_FETCH;
+				break;
+			}
+			const int j = s_head[axis][tid]++;
+			stale = 1 << axis;
+			consumed++;
+			const int gp = R.gp[(size_t)j * n + ray];
+			if (gp == prev) continue;  // std::unique on the partition
+			prev = gp;
+			const float plane = R.plane[(size_t)j * n + ray];
+			const float vd = pick<D>(dir, axis);
+			crossing<D>(o, dir, pick<D>(o, axis), vd, sgnf(vd), plane, pos);
+			hm = home_of<D>(P, gp);
+			bskip = skippable(hm);
+			k = 0;
+			phase = PH_MARCH;
+		}
+		if (phase == PH_FETCH) continue;
+
+		// one sample of the partition's march (ray_child, Surface.hpp:1463-1480)
+		int blo[D], bhi[D];
+#pragma unroll
+		for (int a = 0; a < D; a++) {
+			blo[a] = hm.lo[a];
+			bhi[a] = blo[a] + P.csz[a];
+		}
+		float x[D];
+		bool in;
+		const uint8_t* rng = hm.sl >= 0 ? ranges + (size_t)hm.sl * nsub : nullptr;
+		for (;;) {
+			const float t = __fmul_rn(0.5f, (float)k);  // the reference's t += 0.5, exact
+#pragma unroll
+			for (int a = 0; a < D; a++)
+				x[a] = k == 0 ? pos[a] : __fadd_rn(pos[a], __fmul_rn(dir[a], t));
+			in = k < RAY_MAX_MARCH && inside_box<D>(x, blo, bhi);
+			if (!in) break;
+			// Samples that cannot be layer 0 are stepped over without interpolating: in an
+			// inactive partition, those whose corners all lie in it (they interpolate its
+			// background); in an active one, those in a sub-block of one sign, >= 0.5001 in
+			// magnitude (k_ray_ranges).
+			bool skip;
+			if (rng) {
+				int idx = 0;
+#pragma unroll
+				for (int a = 0; a < D; a++) {
+					const int r = (int)floorf(x[a]) - blo[a];
+					idx = idx * sub_count(P.csz[a]) + r / RAY_SB;
+				}
+				skip = __ldg(rng + idx) != 0;
+			} else {
+				skip = bskip && corners_inside<D>(P, g, blo, x);
+			}
+			if (!skip) break;
+			k++;
+		}
+		if (!in) {
+			phase = PH_NEXT;  // left the partition: next candidate
+			continue;
+		}
+		const float c = HomeInterp<D, L>{P, g, hm}(x);
+		if (layer_id(c, P.err) == 0) {
+			const float3 g3 = march_grad<D, L>(P, g, hm, x[0], x[1], D > 2 ? x[D - 1] : 0.0f, c);
+			const float gr[3] = {g3.x, g3.y, g3.z};
+			if (dot_e<D>(gr, dir) < 0.0f) {
+				const int qi = atomicAdd(Q.counters + 1, 1);
+				ConvItem& it = Q.conv[qi];
+#pragma unroll
+				for (int a = 0; a < D; a++) {
+					it.pos[a] = x[a];
+					it.nrm[a] = gr[a];
+				}
+				it.v = c;
+				it.ray = ray;
+				it.gp = hm.gp;
+				it.m = consumed;
+				it.exact = 0;
+				phase = PH_FETCH;
+				continue;
+			}
+		}
+		k++;
+	}
+}
+
 /// The convergence of ray_child (Surface.hpp:1487-1510): step along the normal by the
 /// interpolated distance until it is within TINY or the normal turns away, at most 100 steps.
 /// A point that leaves the grid is ray_miss for that partition, and the ray is queued to
 /// continue with its next candidate. Persistent threads: each loop iteration is one step of
 /// the thread's current ray; a thread whose ray is done takes the next queued one.
 template <int D, int L>
-__global__ void __launch_bounds__(RAY_THREADS) k_ray_conv(const __grid_constant__ Dev P,
+__global__ void __launch_bounds__(RAY_THREADS, 8) k_ray_conv(const __grid_constant__ Dev P,
                                                           const __grid_constant__ SurfGeom G,
                                                           const float* dirs, RayQueues Q,
                                                           float* hit)
@@ -654,7 +988,7 @@ __global__ void __launch_bounds__(RAY_THREADS) k_ray_conv(const __grid_constant_
 		if (!inside_f<D, L>(g, pos)) {
 			const ConvItem& it = Q.conv[i];
 			const int ri = atomicAdd(Q.counters + 2, 1);
-			Q.resume_out[ri] = ResumeItem{ray, it.m, it.exact};
+			Q.resume_out[ri] = ResumeItem{ray, it.m, it.exact, 0};
 			i = -1;
 			continue;
 		}
@@ -674,97 +1008,155 @@ __global__ void __launch_bounds__(RAY_THREADS) k_ray_conv(const __grid_constant_
 	}
 }
 
-template <int D, int L>
-void launch_rays(EngineBase& eng, int s, const float* o, const float* d, size_t n, int exact,
-                 char* work, float* h)
+/// Bytes of work memory for a pass over n rays.
+size_t ray_work_bytes(size_t n, int D)
 {
-	static int find_per_sm = 0, conv_per_sm = 0, sms = 0;
-	if (find_per_sm == 0) {
+	const size_t b = 256 + n * sizeof(ConvItem) + 3 * n * sizeof(ResumeItem) +
+	                 n * RAY_LIST * (sizeof(float) + sizeof(int)) + (size_t)D * n * sizeof(int);
+	return (b + 255) & ~(size_t)255;
+}
+
+/// Sub-blocks per brick.
+int ray_nsub(const EngineBase& eng)
+{
+	int nsub = 1;
+	for (int a = 0; a < eng.dims(); a++) nsub *= (eng.part(a) + RAY_SB - 1) / RAY_SB;
+	return nsub;
+}
+
+template <int D, int L>
+void launch_rays(EngineBase& eng, int s, const float* o, const float* d, size_t n, int mode,
+                 char* work, const uint8_t* ranges, float* h)
+{
+	struct Occ {
+		int sms = 0, walk = 0, march = 0, find = 0, conv = 0;
+	};
+	static Occ occ;
+	if (occ.sms == 0) {
 		int dev = 0;
 		FG_CUDA(cudaGetDevice(&dev));
-		FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&find_per_sm, k_ray_find<D, L>, RAY_THREADS, 0));
-		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&conv_per_sm, k_ray_conv<D, L>, RAY_THREADS, 0));
-		find_per_sm = std::max(find_per_sm, 1);
-		conv_per_sm = std::max(conv_per_sm, 1);
+		FG_CUDA(cudaDeviceGetAttribute(&occ.sms, cudaDevAttrMultiProcessorCount, dev));
+		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ.walk, k_ray_walk<D, L>, RAY_THREADS, 0));
+		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ.march, k_ray_march<D, L>, RAY_THREADS, 0));
+		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ.find, k_ray_find<D, L>, RAY_THREADS, 0));
+		FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ.conv, k_ray_conv<D, L>, RAY_THREADS, 0));
+		occ.walk = std::max(occ.walk, 1);
+		occ.march = std::max(occ.march, 1);
+		occ.find = std::max(occ.find, 1);
+		occ.conv = std::max(occ.conv, 1);
 	}
+	auto grid = [&](int per_sm) {
+		return (unsigned)std::min<size_t>((n + RAY_THREADS - 1) / RAY_THREADS, (size_t)occ.sms * per_sm);
+	};
 	cudaStream_t st = eng.stream();
 	const Dev& P = eng.dev();
 	const SurfGeom G = eng.geometry(s);
 	int* counters = (int*)work;
 	ConvItem* conv = (ConvItem*)(work + 256);
-	ResumeItem* res[2] = {(ResumeItem*)(conv + n), (ResumeItem*)(conv + n) + n};
-	RayQueues Q{counters, conv, nullptr, res[0], (int)n};
-	const unsigned conv_blocks = (unsigned)std::min<size_t>((n + RAY_THREADS - 1) / RAY_THREADS,
-	                                                        (size_t)sms * conv_per_sm);
+	ResumeItem* res[3] = {(ResumeItem*)(conv + n), (ResumeItem*)(conv + n) + n,
+	                      (ResumeItem*)(conv + n) + 2 * n};
+	float* lk = (float*)(res[2] + n);
+	RayLists R{lk, (int*)(lk + n * RAY_LIST), (int*)(lk + 2 * n * RAY_LIST), (int)n};
+	RayQueues Q{counters, conv, res[2], counters + 5, 0, res[0], res[2]};
+	FG_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(int), st));
+	if (mode == 0) {
+		FG_RUN("k_ray_walk", st, k_ray_walk<D, L><<<grid(occ.walk), RAY_THREADS, 0, st>>>(P, G, o, d, R););
+		FG_CUDA(cudaGetLastError());
+	}
+	FG_RUN("k_ray_march", st, k_ray_march<D, L><<<grid(occ.march), RAY_THREADS, 0, st>>>(P, G, o, d, mode, R, ranges, ray_nsub(eng), Q, h););
+	FG_CUDA(cudaGetLastError());
 	for (int pass = 0;; pass++) {
 		if (pass > RAY_MAX_MARCH) throw Error(-13, "raycasting did not finish");
-		const unsigned blocks = (unsigned)std::min<size_t>(((size_t)Q.n_in + RAY_THREADS - 1) / RAY_THREADS,
-		                                                   (size_t)sms * find_per_sm);
-		FG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int), st));
-		FG_RUN("k_ray_find", st, k_ray_find<D, L><<<blocks, RAY_THREADS, 0, st>>>(P, G, o, d, exact, Q, h););
+		FG_RUN("k_ray_find", st, k_ray_find<D, L><<<grid(occ.find), RAY_THREADS, 0, st>>>(P, G, o, d, Q, h););
 		FG_CUDA(cudaGetLastError());
-		FG_RUN("k_ray_conv", st, k_ray_conv<D, L><<<conv_blocks, RAY_THREADS, 0, st>>>(P, G, d, Q, h););
+		FG_RUN("k_ray_conv", st, k_ray_conv<D, L><<<grid(occ.conv), RAY_THREADS, 0, st>>>(P, G, d, Q, h););
 		FG_CUDA(cudaGetLastError());
 		int resumed = 0;
 		FG_CUDA(cudaMemcpyAsync(&resumed, counters + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
 		FG_CUDA(cudaStreamSynchronize(st));
 		if (resumed == 0) break;
 		// the rays whose convergence left the grid continue with their next candidates
-		Q.resume_in = Q.resume_out;
+		Q.find_in = Q.resume_out;
+		Q.find_n_ptr = nullptr;
+		Q.find_n = resumed;
 		Q.resume_out = res[(pass + 1) & 1];
-		Q.n_in = resumed;
+		FG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int), st));
 	}
+}
+
+/// k_ray_ranges over the bricks of surface s.
+void ranges_launch(EngineBase& eng, int s, uint8_t* ranges, int nsub)
+{
+	const Dev& P = eng.dev();
+	const SurfGeom G = eng.geometry(s);
+	const size_t total = (size_t)P.nslots * nsub;
+	const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+	cudaStream_t st = eng.stream();
+	const int D = eng.dims(), L = eng.layers();
+#define FG_CASE(dd, ll) \
+	if (D == dd && L == ll) FG_RUN("k_ray_ranges", st, k_ray_ranges<dd, ll><<<blocks, 256, 0, st>>>(P, G, s, ranges, nsub););
+	FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
+	FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
+#undef FG_CASE
+	FG_CUDA(cudaGetLastError());
 }
 
 }  // namespace
 
 void ray_batch(EngineBase& eng, int s, const float* origins, const float* dirs, size_t n,
-               float* hits, bool device_ptrs, bool exact_order)
+               float* hits, bool device_ptrs, int mode)
 {
 	if (s < 0 || s >= eng.surfaces()) throw Error(-1, "surface index out of range");
+	if (mode < 0 || mode > 2) throw Error(-1, "candidate order mode is 0, 1 or 2");
 	if (n == 0) return;
-	if (n >= (size_t)1 << 30) throw Error(-1, "too many rays in one call (at most 2^30 - 1)");
 	const int D = eng.dims(), L = eng.layers();
-	const size_t bytes = n * D * sizeof(float);
+	// passes of at most 2^21 rays bound the work memory (about 600 MB)
+	const size_t chunk = std::min<size_t>(n, (size_t)1 << 21);
+	const size_t cbytes = chunk * D * sizeof(float);
+	const size_t work = ray_work_bytes(chunk, D);
 	cudaStream_t st = eng.stream();
-	// one stream-ordered allocation: counters, the convergence queue, two resume queues, then
-	// (host arrays) origins, dirs and hits
-	const size_t work = 256 + n * sizeof(ConvItem) + 2 * n * sizeof(ResumeItem);
-	const size_t work_al = (work + 255) & ~(size_t)255;
+	// one stream-ordered allocation: the pass's work memory, then (host arrays) staging for
+	// origins, dirs and hits
+	const int nsub = ray_nsub(eng);
+	const size_t rbytes = ((size_t)eng.dev().nslots * nsub + 255) & ~(size_t)255;
 	char* dev = nullptr;
-	FG_CUDA(cudaMallocAsync((void**)&dev, work_al + (device_ptrs ? 0 : 3 * bytes), st));
-	const float* dorg = origins;
-	const float* ddir = dirs;
-	float* dhit = hits;
-	if (!device_ptrs) {
-		float* f = (float*)(dev + work_al);
-		FG_CUDA(cudaMemcpyAsync(f, origins, bytes, cudaMemcpyHostToDevice, st));
-		FG_CUDA(cudaMemcpyAsync(f + n * D, dirs, bytes, cudaMemcpyHostToDevice, st));
-		dorg = f;
-		ddir = f + n * D;
-		dhit = f + 2 * n * D;
-	}
-	bool launched = false;
+	FG_CUDA(cudaMallocAsync((void**)&dev, rbytes + work + (device_ptrs ? 0 : 3 * cbytes), st));
+	uint8_t* ranges = (uint8_t*)dev;
+	dev += rbytes;
 	try {
-#define FG_CASE(dd, ll)                                                               \
-	if (D == dd && L == ll) {                                                         \
-		launch_rays<dd, ll>(eng, s, dorg, ddir, n, exact_order ? 1 : 0, dev, dhit); \
-		launched = true;                                                              \
+		ranges_launch(eng, s, ranges, nsub);
+		for (size_t b = 0; b < n; b += chunk) {
+			const size_t m = std::min(chunk, n - b);
+			const size_t bytes = m * D * sizeof(float);
+			const float* dorg = origins + b * D;
+			const float* ddir = dirs + b * D;
+			float* dhit = hits + b * D;
+			if (!device_ptrs) {
+				float* f = (float*)(dev + work);
+				FG_CUDA(cudaMemcpyAsync(f, origins + b * D, bytes, cudaMemcpyHostToDevice, st));
+				FG_CUDA(cudaMemcpyAsync(f + chunk * D, dirs + b * D, bytes, cudaMemcpyHostToDevice, st));
+				dorg = f;
+				ddir = f + chunk * D;
+				dhit = f + 2 * chunk * D;
+			}
+			bool launched = false;
+#define FG_CASE(dd, ll)                                                              \
+	if (D == dd && L == ll) {                                                        \
+		launch_rays<dd, ll>(eng, s, dorg, ddir, m, mode, dev, ranges, dhit);         \
+		launched = true;                                                             \
 	}
-		FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
-		FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
+			FG_CASE(2, 1) FG_CASE(2, 2) FG_CASE(2, 3) FG_CASE(2, 4)
+			FG_CASE(3, 1) FG_CASE(3, 2) FG_CASE(3, 3) FG_CASE(3, 4)
 #undef FG_CASE
+			if (!launched) throw Error(-1, "unsupported dimension or layer count");
+			if (!device_ptrs)
+				FG_CUDA(cudaMemcpyAsync(hits + b * D, dhit, bytes, cudaMemcpyDeviceToHost, st));
+		}
 	} catch (...) {
-		cudaFreeAsync(dev, st);
+		cudaFreeAsync(dev - rbytes, st);
 		throw;
 	}
-	if (!launched) {
-		cudaFreeAsync(dev, st);
-		throw Error(-1, "unsupported dimension or layer count");
-	}
-	if (!device_ptrs) FG_CUDA(cudaMemcpyAsync(hits, dhit, bytes, cudaMemcpyDeviceToHost, st));
-	FG_CUDA(cudaFreeAsync(dev, st));
+	FG_CUDA(cudaFreeAsync(dev - rbytes, st));
 	eng.sync();
 	eng.check_errors();
 }

@@ -132,12 +132,13 @@ FG_API int fg_get(fg_surface* s, const int* pos, float* out);
  * memory; each ray runs on one GPU thread, in the reference's FP32 arithmetic. */
 FG_API int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t n, float* hits);
 
-/* fg_ray with origins, dirs and hits in device memory of the surface's GPU. exact_order = 1
- * finds each ray's next candidate partition by a full walk of its planes instead of merging the
- * per-axis walks; the order, and so the hits, are the same (it exists to test that); 0 is the
- * fast default. */
+/* fg_ray with origins, dirs and hits in device memory of the surface's GPU. order_mode chooses
+ * how each ray's candidate partitions are put in the reference's order: 0 (the fast default)
+ * merges per-axis lists made by a walk kernel, 1 finds each next candidate by a full walk of
+ * the planes, 2 merges per-axis cursors. The hits are the same for all three; 1 and 2 exist to
+ * test 0. */
 FG_API int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n,
-                         float* hits, int exact_order);
+                         float* hits, int order_mode);
 
 /* Geometry of the children (partition) grid: count, size and offset of the children grid. */
 FG_API int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);

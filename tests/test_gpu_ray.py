@@ -115,8 +115,9 @@ def test_ray_random_parity(si):
 
 @pytest.mark.parametrize("si", range(len(SCENES)))
 def test_ray_merge_order_equals_exact_order(si):
-    """The kernel orders a ray's candidates by merging its per-axis plane walks; finding each
-    next candidate by a full walk (the reference's sort, restated) gives the same hits."""
+    """The kernels order a ray's candidates by merging its per-axis plane walks, from stored
+    lists (mode 0) or from cursors (mode 2, the path of rays with long lists); finding each next
+    candidate by a full walk (mode 1, the reference's sort restated) gives the same hits."""
     import torch
     g, o = _scene(SCENES[si])
     D = len(SCENES[si][0])
@@ -124,12 +125,12 @@ def test_ray_merge_order_equals_exact_order(si):
     want = o.rays(org, d)
     to = torch.from_numpy(org).cuda()
     td = torch.from_numpy(d).cuda()
-    for exact in (False, True):
+    for mode in (0, 1, 2):
         th = torch.empty_like(to)
         g.rays_device(to.data_ptr(), td.data_ptr(), org.shape[0], th.data_ptr(),
-                      exact_order=exact)
+                      order_mode=mode)
         torch.cuda.synchronize()
-        assert_rays_equal(th.cpu().numpy(), want, f"exact_order={exact}")
+        assert_rays_equal(th.cpu().numpy(), want, f"order_mode={mode}")
 
 
 def test_ray_edge_cases():
@@ -139,7 +140,7 @@ def test_ray_edge_cases():
     with pytest.raises(ValueError):
         g.rays(np.zeros((2, 3)), np.zeros((3, 3)))
     with pytest.raises(fb.FeltError):
-        g.rays_device(0, 0, 4, 0, exact_order=2)
+        g.rays_device(0, 0, 4, 0, order_mode=3)
     # a zero direction never leaves its partition and finds no crossing: a miss on both sides
     org = np.array([[-3.0, 0.5, 0.25], [100.0, 0, 0], [-20.0, -20.0, -20.0]], np.float32)
     d = np.array([[0, 0, 0], [-1, 0, 0], [0, 0, 1]], np.float32)
@@ -181,3 +182,24 @@ def test_ray_convergence_leaving_the_grid_resumes():
     passes = (fb.launch_count() - l0) // 2
     assert passes >= 2, "no convergence left the grid: the scene no longer tests the resume"
     assert_rays_equal(hits, o.rays(org, d), "resumed rays")
+
+
+def test_ray_long_candidate_lists():
+    """Rays crossing many band partitions (three small circles in a row, 2x2 partitions) have
+    more candidates than the walk kernel lists per ray and take the cursor path; all three
+    candidate orders agree with the oracle."""
+    import torch
+    scene = ((64, 64), (2, 2), 2, [(-20, 0), (0, 1), (20, -1)], [(3, dict(c=-1.0))])
+    g, o = _scene(scene)
+    rng = np.random.default_rng(11)
+    m = 600
+    org = np.stack([np.full(m, -31.5), rng.uniform(-5, 5, m)], axis=1).astype(np.float32)
+    d = np.stack([np.ones(m), rng.uniform(-0.05, 0.05, m)], axis=1)
+    d = np.array([normalized(v) for v in d.astype(np.float32)], dtype=np.float32)
+    want = o.rays(org, d)
+    to, td = torch.from_numpy(org).cuda(), torch.from_numpy(d).cuda()
+    for mode in (0, 1, 2):
+        th = torch.empty_like(to)
+        g.rays_device(to.data_ptr(), td.data_ptr(), m, th.data_ptr(), order_mode=mode)
+        torch.cuda.synchronize()
+        assert_rays_equal(th.cpu().numpy(), want, f"order_mode={mode}")
