@@ -182,6 +182,34 @@ class Surface:
         _chk(lib().fg_get(self._h, _ivec(pos), C.byref(v)))
         return v.value
 
+    def save(self):
+        """Surface::save (include/Felt/Surface.hpp:180-183): the surface file, in the reference's
+        format, as bytes."""
+        n = C.c_size_t()
+        _chk(lib().fg_save(self._h, None, C.c_size_t(0), C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        _chk(lib().fg_save(self._h, buf, C.c_size_t(n.value), C.byref(n)))
+        return bytes(buf)
+
+    @classmethod
+    def load(cls, data, brick_capacity=0, vertex_capacity=0):
+        """Surface::load (include/Felt/Surface.hpp:185-196): a new surface from a surface file
+        (bytes); dimensions, layers and sizes come from the file."""
+        raw = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
+        h = C.c_void_p()
+        _chk(lib().fg_load(raw, C.c_size_t(len(data)), C.byref(cfg), C.byref(h)))
+        obj = cls.__new__(cls)
+        obj._h = h
+        d, l_ = C.c_int(), C.c_int()
+        cnt = C.c_size_t()
+        cs, co = (C.c_int * 3)(), (C.c_int * 3)()
+        _chk(lib().fg_surface_info(h, C.byref(d), C.byref(l_), cs, co))
+        obj.D, obj.L = d.value, l_.value
+        obj.size = tuple(cs[: obj.D])
+        obj.part = tuple(co[: obj.D])
+        return obj
+
     def rays(self, origins, dirs):
         """Surface::ray (include/Felt/Surface.hpp:468-616) for each (origin, direction) row: the
         point where the ray meets the zero curve, or a row of RAY_MISS where it misses."""

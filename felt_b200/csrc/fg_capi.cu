@@ -9,6 +9,7 @@
 #include "fg_engine.cuh"
 #include "fg_polys.cuh"
 #include "fg_ray.cuh"
+#include "fg_image.cuh"
 
 #include "fg_handles.cuh"
 
@@ -89,6 +90,44 @@ int fg_surface_create(int dims, int layers, const int* size, const int* part, co
 		FG_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
 		s->eng.reset(fg::make_engine(d, s->st));
 		*out = s.release();
+	});
+}
+
+int fg_save(fg_surface* s, uint8_t* buf, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(n, "length");
+		fg::SurfaceImage img;
+		fg::export_image(*s->eng, 0, img);
+		std::vector<uint8_t> out;
+		int csz[3];
+		for (int a = 0; a < s->eng->dims(); a++) csz[a] = s->eng->part(a);
+		fg::write_surface_file(img, s->eng->geometry(0), s->eng->dims(), s->eng->layers(), csz, out);
+		*n = out.size();
+		if (buf) std::memcpy(buf, out.data(), std::min(cap, out.size()));
+	});
+}
+
+int fg_load(const uint8_t* data, size_t n, const fg_config* cfg, fg_surface** out)
+{
+	return guard([&] {
+		need(data, "data");
+		need(out, "out");
+		int D = 0, L = 0, size[3] = {1, 1, 1}, csz[3] = {1, 1, 1};
+		fg::peek_surface_file(data, n, D, L, size, csz);
+		if (L > 4) throw fg::Error(FG_ERR_ARG, "surface file: more than 4 layers");
+		fg_surface* s = nullptr;
+		const int rc = fg_surface_create(D, L, size, csz, cfg, &s);
+		if (rc != FG_OK) throw fg::Error(rc, g_err);
+		std::unique_ptr<fg_surface> hold(s);
+		const fg::SurfGeom& g = s->eng->geometry(0);
+		for (int a = 0; a < D; a++)
+			if (g.off[a] != -size[a] / 2) throw fg::Error(FG_ERR_ARG, "surface file: grid offset other than -size/2");
+		fg::SurfaceImage img;
+		fg::read_surface_file(data, n, g, D, L, csz, s->eng->dev().BV, img);
+		fg::import_image(*s->eng, img);
+		*out = hold.release();
 	});
 }
 
@@ -631,6 +670,21 @@ int fg_work_units(fg_surface* s, unsigned long long* out, size_t n)
 		s->eng->sync();
 		FG_CUDA(cudaMemcpy(tmp, s->eng->dev().kstat, sizeof(tmp), cudaMemcpyDeviceToHost));
 		for (size_t i = 0; i < n && i < (size_t)fg::KS_N; i++) out[i] = tmp[i];
+	});
+}
+
+int fg_surface_info(fg_surface* s, int* dims, int* layers, int* size, int* part)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(dims, "dims");
+		need(layers, "layers");
+		*dims = s->eng->dims();
+		*layers = s->eng->layers();
+		for (int a = 0; a < *dims; a++) {
+			if (size) size[a] = s->eng->geometry(0).size[a];
+			if (part) part[a] = s->eng->part(a);
+		}
 	});
 }
 

@@ -16,6 +16,9 @@
 
 #include <array>
 #include <cstdint>
+#include <istream>
+#include <iterator>
+#include <ostream>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -98,6 +101,37 @@ public:
 	}
 	Surface(const Surface&) = delete;
 	Surface& operator=(const Surface&) = delete;
+	Surface(Surface&& o) noexcept : h_(o.h_), size_(o.size_) { o.h_ = nullptr; }
+
+	/// save(ostream) (Surface.hpp:180-183): the surface file, in the reference's format.
+	void save(std::ostream& out) const
+	{
+		size_t n = 0;
+		check(fg_save(h_, nullptr, 0, &n));
+		std::vector<uint8_t> buf(n);
+		check(fg_save(h_, buf.data(), buf.size(), &n));
+		out.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)buf.size());
+		out.flush();
+	}
+
+	/// load(istream) (Surface.hpp:185-196): a new surface from a surface file; its dimensions
+	/// and layers must be this type's.
+	static Surface load(std::istream& in, const fg_config* cfg = nullptr)
+	{
+		std::vector<uint8_t> buf((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+		fg_surface* h = nullptr;
+		check(fg_load(buf.data(), buf.size(), cfg, &h));
+		int dims = 0, layers = 0;
+		VecDi<D> size{}, part{};
+		int sz[3], pt[3];
+		const int rc = fg_surface_info(h, &dims, &layers, sz, pt);
+		if (rc != FG_OK || dims != D || layers != L) {
+			fg_surface_destroy(h);
+			throw Error(FG_ERR_ARG, "surface file of another dimension or layer count");
+		}
+		for (int a = 0; a < D; a++) size[a] = sz[a];
+		return Surface(h, size);
+	}
 
 	/// layer_idx(id) (Surface.hpp:672-675).
 	static constexpr int layer_idx(int id) { return id + L; }
@@ -230,6 +264,8 @@ private:
 		if (n) check(f(out.data(), n, &n));
 		return out;
 	}
+
+	Surface(fg_surface* h, const VecDi<D>& size) : h_(h), size_(size) {}
 
 	fg_surface* h_ = nullptr;
 	VecDi<D> size_;

@@ -140,6 +140,19 @@ FG_API int fg_ray(fg_surface* s, const float* origins, const float* dirs, size_t
 FG_API int fg_ray_device(fg_surface* s, const float* origins, const float* dirs, size_t n,
                          float* hits, int order_mode);
 
+/* Surface::save (include/Felt/Surface.hpp:180-183): the surface file in the reference's format
+ * (its isogrid through cereal's binary archive: backgrounds, values, leaf and partition lists
+ * and lookups, sizes). Writes min(n, cap) bytes to buf (buf may be NULL to ask for the length)
+ * and the full length to *n. */
+FG_API int fg_save(fg_surface* s, uint8_t* buf, size_t cap, size_t* n);
+
+/* Surface::load (include/Felt/Surface.hpp:185-196): a new surface from a surface file (its
+ * dimensions, layers, grid and partition sizes come from the file). The file is checked against
+ * the invariants the engine relies on (list entries in range, lookups agreeing with lists,
+ * every listed leaf in its own layer, partition lists matching the partitions' leaf lists);
+ * a file that breaks one is rejected with FG_ERR_ARG. cfg as for fg_surface_create. */
+FG_API int fg_load(const uint8_t* data, size_t n, const fg_config* cfg, fg_surface** out);
+
 /* Geometry of the children (partition) grid: count, size and offset of the children grid. */
 FG_API int fg_partitions(fg_surface* s, size_t* count, int* children_size, int* children_offset);
 
@@ -261,6 +274,9 @@ FG_API int fg_node_updates(fg_surface* s, unsigned long long* n);
 FG_API int fg_work_units(fg_surface* s, unsigned long long* out, size_t n);
 /* The CUDA stream (cudaStream_t) every call on this surface is issued to. */
 FG_API int fg_surface_stream(fg_surface* s, void** stream);
+/* Dimensions, layers, grid size and partition size of a surface (size and part: dims ints each,
+ * either may be NULL): what a surface made by fg_load was given by its file. */
+FG_API int fg_surface_info(fg_surface* s, int* dims, int* layers, int* size, int* part);
 FG_API int fg_launch_count(long long* n);
 FG_API int fg_profile_enable(int on);
 FG_API int fg_profile_reset(void);

@@ -2,6 +2,7 @@
 // prefix so that tests can drive the oracle and the device engine through identical call
 // sequences and compare their dumps. TEST INFRASTRUCTURE ONLY.
 #include "felt_oracle.hpp"
+#include "felt_oracle_serial.hpp"
 
 #include <chrono>
 #include <cstring>
@@ -34,6 +35,9 @@ struct SurfBase {
 	virtual size_t band_size() = 0;
 	virtual void curv(const int* p, float* out) = 0;
 	virtual void ray(const float* o, const float* d, float* out) = 0;
+	virtual void save(std::vector<uint8_t>& out) = 0;
+	virtual void geometry(int* size, int* part) = 0;
+	virtual void load(const uint8_t* p, size_t n) = 0;
 };
 
 struct PolysBase {
@@ -125,6 +129,15 @@ struct Surf : SurfBase {
 		return n;
 	}
 	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
+	void save(std::vector<uint8_t>& out) override { fo::save_surface<D, L>(s, out); }
+	void geometry(int* size, int* part) override
+	{
+		for (int a = 0; a < D; a++) {
+			size[a] = s.iso.size[a];
+			part[a] = s.iso.csize[a];
+		}
+	}
+	void load(const uint8_t* p, size_t n) override { fo::load_surface<D, L>(s, p, n); }
 	void ray(const float* o, const float* d, float* out) override
 	{
 		std::array<float, D> oo, dd;
@@ -251,6 +264,42 @@ int fo_surface_create(int dims, int layers, const int* size, const int* part, vo
 		*out = s;
 	});
 }
+/* Surface::save (Surface.hpp:180-183): the surface file, min(n, cap) bytes into buf, the
+ * full length in *n. */
+int fo_save(void* s, uint8_t* buf, size_t cap, size_t* n)
+{
+	return guard([&] {
+		std::vector<uint8_t> out;
+		static_cast<SurfBase*>(s)->save(out);
+		*n = out.size();
+		if (buf) std::memcpy(buf, out.data(), std::min(cap, out.size()));
+	});
+}
+
+/* Surface::load (Surface.hpp:185-196): a new surface from a surface file. */
+int fo_load(const uint8_t* p, size_t n, void** out)
+{
+	return guard([&] {
+		int dims = 0, lists = 0, size[3] = {0, 0, 0}, part[3] = {0, 0, 0};
+		fo::peek_surface(p, n, dims, lists, size, part);
+		std::unique_ptr<SurfBase> s(make(dims, (lists - 1) / 2, size, part));
+		if (!s) throw fo::Error(-1, "unsupported dims/layers");
+		s->load(p, n);
+		*out = s.release();
+	});
+}
+
+/* Dimensions, layers, grid size and partition size of a surface. */
+int fo_info(void* s, int* dims, int* layers, int* size, int* part)
+{
+	return guard([&] {
+		SurfBase* b = static_cast<SurfBase*>(s);
+		*dims = b->dims;
+		*layers = b->layers;
+		b->geometry(size, part);
+	});
+}
+
 int fo_surface_destroy(void* s)
 {
 	delete static_cast<SurfBase*>(s);

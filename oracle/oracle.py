@@ -139,6 +139,30 @@ class Surface:
         _chk(lib().fo_curv(self._h, _ivec(pos), C.byref(v)))
         return v.value
 
+    def save(self):
+        """Surface::save: the surface file (the reference's cereal binary layout) as bytes."""
+        n = C.c_size_t()
+        _chk(lib().fo_save(self._h, None, C.c_size_t(0), C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        _chk(lib().fo_save(self._h, buf, C.c_size_t(n.value), C.byref(n)))
+        return bytes(buf)
+
+    @classmethod
+    def load(cls, data):
+        """Surface::load: a new surface from a surface file."""
+        h = C.c_void_p()
+        raw = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        _chk(lib().fo_load(raw, C.c_size_t(len(data)), C.byref(h)))
+        obj = cls.__new__(cls)
+        obj._h = h
+        d, l_ = C.c_int(), C.c_int()
+        sz, pt = (C.c_int * 3)(), (C.c_int * 3)()
+        _chk(lib().fo_info(h, C.byref(d), C.byref(l_), sz, pt))
+        obj.D, obj.L = d.value, l_.value
+        obj.size = tuple(sz[: obj.D])
+        obj.part = tuple(pt[: obj.D])
+        return obj
+
     def rays(self, origins, dirs):
         """Surface::ray for each (origin, direction) row; rows of FLT_MAX where missed."""
         o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, self.D)

@@ -328,10 +328,26 @@ def ray_cases(root):
     return cases
 
 
+def serial_cases(root):
+    """Surface::save / Surface::load (test_Surface.cpp:464-500): the 9x9 surface after one
+    update of -0.6 is saved and loaded; the loaded surface's snapshot equals the original's, and
+    after an update of 0.6 it holds the grid literal that follows."""
+    f = "src/tests/test_Surface.cpp"
+    L = lines_of(root, f)
+    start = next(i for i, ln in enumerate(L, 1) if "surface is serialised to disk then loaded" in ln)
+    upd_at = next(i for i in range(start, start + 40) if "surface_loaded.update" in L[i - 1])
+    grid_at = next(i for i in range(upd_at, upd_at + 20) if "isogrid_check.data() =" in L[i - 1])
+    vals, end = data_block(L, grid_at)
+    return [dict(name="save_load_then_contract_9x9", ref=f"{f}:{start}-{end}", size=[9, 9],
+                 part=[3, 3], layers=2, before=[["seed", [0, 0]], ["update", -0.6]],
+                 after=[["update", 0.6]], grid=vals, grid_ref=f"{f}:{grid_at}-{end}")]
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
-               curvature=curvature_cases(root), neighs=neighs_case(root), ray=ray_cases(root))
+               curvature=curvature_cases(root), neighs=neighs_case(root), ray=ray_cases(root),
+               serial=serial_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)
