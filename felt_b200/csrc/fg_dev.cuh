@@ -111,6 +111,10 @@ struct Dev {
 	int* ndp;         // [S] delta partitions: a prefix of the affected partition list L
 	int* ring_first;  // [NL*NP] calc_affected ring bounds per (layer, partition entry)
 	int* ring_last;   // [NL*NP]
+	int* ring_src;    // [NL*NP] entries with leaves to expand in the current ring
+	int* ring_n;      // [2*NL] partition-list lengths at the start of the last two rings
+	unsigned long long* apkey;  // [NP*NL] first track key of (partition, list) in a ring
+	int* aq;          // [NP*NL] (partition, list) entries that join the affected lists
 };
 
 enum {
@@ -120,7 +124,11 @@ enum {
 	CNT_RETIRE = 3,
 	CNT_SUNION = 4,
 	CNT_CAND = 5,  // expansion candidates recorded this iteration
-	CNT_N = 8
+	CNT_ASRC = 8,     // calc_affected: source entries of the ring
+	CNT_AQ = 9,       // calc_affected: (partition, list) entries joining the lists
+	CNT_ATOUCH = 10,  // calc_affected: bricks with claimed leaves
+	CNT_ATC = 16,     // calc_affected: per list, partitions joining it (NL entries)
+	CNT_N = 32
 };
 
 /// Work-unit counters (Dev::kstat): band nodes through the distance passes, zero-layer nodes

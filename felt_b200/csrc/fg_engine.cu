@@ -208,14 +208,20 @@ public:
 		P.ndp = dalloc<int>(S, o);
 		P.ring_first = dalloc<int>(npl, o);
 		P.ring_last = dalloc<int>(npl, o);
+		P.ring_src = dalloc<int>(npl, o);
+		P.ring_n = dalloc<int>(2 * NL, o);
+		P.apkey = dalloc<unsigned long long>(npl, o);
+		P.aq = dalloc<int>(npl, o);
 		FG_CUDA(cudaMemsetAsync(P.kstat, 0, KS_N * sizeof(unsigned long long), st_));
 		acc_ = dalloc<unsigned long long>(1, o);
+		zcount_ = dalloc<unsigned long long>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
 
 		fill(P.slot, NP, -1);
 		fillf(P.bg, NP, (float)(L + 1));
 		fill(P.oslot, NP, -1);
 		fill(P.ppos, npl, -1);
+		FG_CUDA(cudaMemsetAsync(P.apkey, 0xff, npl * sizeof(unsigned long long), st_));
 		fill(P.sppos, npl, -1);
 		fill(P.appos[0], npl, -1);
 		fill(P.appos[1], npl, -1);
@@ -524,7 +530,7 @@ public:
 			FG_CUDA(cudaMemcpyAsync(d_lval_, vals.data(), n * sizeof(float),
 			                        cudaMemcpyHostToDevice, st_));
 		}
-		FG_RUN("k_local_seed", st_, k_local_seed<D, L><<<1, 1, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n););
+		local_seed(n);
 		local_end();
 	}
 
@@ -539,8 +545,11 @@ public:
 		}
 		check_not_frozen();
 		// capacity: every zero-layer leaf of the surface
+		FG_CUDA(cudaMemsetAsync(zcount_, 0, sizeof(unsigned long long), st_));
+		FG_RUN("k_count_layer", st_, k_count_layer<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0, L, zcount_););
 		unsigned long long nz = 0;
-		for (uint32_t p : partition_list(0, 0, L)) nz += layer_list(0, p, L).size();
+		FG_CUDA(cudaMemcpyAsync(&nz, zcount_, sizeof(nz), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
 		ensure_local_staging((int)nz + 1);
 		update_start();
 		FG_RUN("k_bounded_collect", st_, k_bounded_collect<D, L><<<1, 1, 0, st_>>>(P_, 0, vlo, vhi, d_lpos_, lcap_, d_lcount_););
@@ -548,8 +557,40 @@ public:
 		int n = 0;
 		FG_CUDA(cudaMemcpyAsync(&n, d_lcount_, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
-		FG_RUN("k_local_seed", st_, k_local_seed<D, L><<<1, 1, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n););
+		local_seed(n);
 		local_end();
+	}
+
+	/// The n staged delta calls of a local update on surface 0 (Surface.hpp:441-459) and the
+	/// first step of calc_affected (788-799), in parallel (fg_kernels.cuh).
+	void local_seed(int n)
+	{
+		constexpr int RING_CAP = 2048;
+		const int gb = grid_for(n);
+		FG_RUN("k_seed_claim", st_, k_seed_claim<D, L><<<gb, 256, 0, st_>>>(P_, 0, d_lpos_, n););
+		FG_RUN("k_ring_append", st_, k_ring_append<L><<<sm_count() * 4, 256, RING_CAP * 11, st_>>>(P_, RING_CAP, L););
+		FG_RUN("k_ring_plist", st_, k_ring_plist<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0););
+		FG_RUN("k_ring_finish", st_, k_ring_finish<L><<<1, 256, 0, st_>>>(P_, 0););
+		for (int phase = 0; phase < 4; phase++)
+			FG_RUN("k_seed_values", st_, k_seed_values<D, L><<<gb, 256, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n, phase););
+		FG_RUN("k_seed_finish", st_, k_seed_finish<L><<<sm_count(), 256, 0, st_>>>(P_, 0););
+	}
+
+	/// calc_affected's L rings (Surface.hpp:801-912) on surface 0, each a set of parallel
+	/// kernels that append in the reference's sequential order (fg_kernels.cuh).
+	void calc_affected()
+	{
+		constexpr int RING_CAP = 2048;  // claimed leaves a brick ranks in shared memory
+		const int np = geom_[0].np;
+		FG_CUDA(cudaMemsetAsync(P_.ring_n, 0, 2 * NL * sizeof(int), st_));
+		for (int ring = 1; ring <= L; ring++) {
+			const int cur = (ring - 1) & 1;
+			FG_RUN("k_ring_setup", st_, k_ring_setup<L><<<grid_for((long long)NL * np), 256, 0, st_>>>(P_, 0, np, cur););
+			FG_RUN("k_ring_claim", st_, k_ring_claim<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0););
+			FG_RUN("k_ring_append", st_, k_ring_append<L><<<sm_count() * 4, 256, RING_CAP * 11, st_>>>(P_, RING_CAP, -1););
+			FG_RUN("k_ring_plist", st_, k_ring_plist<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0););
+			FG_RUN("k_ring_finish", st_, k_ring_finish<L><<<1, 256, 0, st_>>>(P_, 0););
+		}
 	}
 
 	/// update_end after the deltas are tracked (Surface.hpp:404-430).
@@ -557,7 +598,7 @@ public:
 	{
 		const int A = 0, B = 1;
 		buf_dirty_[A] = true;
-		FG_RUN("k_calc_affected", st_, k_calc_affected<D, L><<<1, 1, 0, st_>>>(P_, 0););
+		calc_affected();
 		FG_RUN("k_local_children", st_, k_local_children<L><<<1, 1, 0, st_>>>(P_, 0););
 		count_band();
 		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
@@ -767,9 +808,13 @@ public:
 
 	unsigned long long band_size(int s) override
 	{
-		unsigned long long n = 0;
+		check_surface(s);
+		FG_CUDA(cudaMemsetAsync(zcount_, 0, sizeof(unsigned long long), st_));
 		for (int l = 0; l < NL; l++)
-			for (uint32_t p : partition_list(s, 0, l)) n += layer_list(s, p, l).size();
+			FG_RUN("k_count_layer", st_, k_count_layer<L><<<sm_count() * 2, 256, 0, st_>>>(P_, s, l, zcount_););
+		unsigned long long n = 0;
+		FG_CUDA(cudaMemcpyAsync(&n, zcount_, sizeof(n), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
 		return n;
 	}
 
@@ -951,7 +996,8 @@ private:
 	int csz_[3] = {1, 1, 1};
 	std::vector<SurfGeom> geom_;
 	std::vector<void*> owned_;
-	unsigned long long* acc_ = nullptr;
+	unsigned long long* acc_ = nullptr;     // node updates of all global updates so far
+	unsigned long long* zcount_ = nullptr;  // zero-layer leaf count of a bounded update
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;

@@ -1589,96 +1589,297 @@ __device__ void a_track(const Dev& P, int b, const SurfGeom& g, int s, int gp, i
 	}
 }
 
-/// The delta(pos, val) calls (Surface.hpp:441-459), in call order, followed by the first step of
-/// calc_affected (Surface.hpp:788-799), which tracks exactly those leaves, in the same order,
-/// into affected buffer 0. The delta grid's zero-layer lists are therefore the prefixes of the
-/// affected zero-layer lists recorded in dlcnt / ndp. Later values at a leaf overwrite earlier
-/// ones, as the delta grid's track does.
+/// The delta(pos, val) calls (Surface.hpp:441-459) and the first step of calc_affected
+/// (Surface.hpp:788-799), which tracks exactly those leaves, in call order, into affected buffer
+/// 0's zero-layer lists: the delta grid's zero-layer lists are therefore the prefixes of the
+/// affected zero-layer lists recorded in dlcnt / ndp. In parallel, with the call index as the
+/// order key (see the ring kernels below): a leaf, and a partition's zero-layer list entry, are
+/// claimed at their first call; k_ring_append / k_ring_plist then append them in call order.
+/// Calls at positions outside the grid or in inactive partitions set the error bit and do
+/// nothing, as the sequential loop does.
+template <int D>
+__device__ __forceinline__ bool seed_locate(const Dev& P, const SurfGeom& g, const int* pos, int i,
+                                            int& gp, int& sl, int& leaf, bool flag)
+{
+	Vec<D> p;
+	for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+	if (!in_grid<D>(g, p)) {
+		if (flag) atomicOr(P.err, EB_OUTSIDE);
+		return false;
+	}
+	locate<D>(P, g, p, gp, leaf);
+	sl = P.slot[gp];
+	if (sl < 0) {
+		if (flag) atomicOr(P.err, EB_INACTIVE);
+		return false;
+	}
+	return true;
+}
+
 template <int D, int L>
-__global__ void k_local_seed(Dev P, int s, const int* pos, const float* val, int n)
+__global__ void k_seed_claim(Dev P, int s, const int* pos, int n)
 {
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
-	for (int i = 0; i < n; i++) {
-		Vec<D> p;
-		for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
-		if (!in_grid<D>(g, p)) {
-			atomicOr(P.err, EB_OUTSIDE);
-			continue;
-		}
-		int gp, leaf;
-		locate<D>(P, g, p, gp, leaf);
-		const int sl = P.slot[gp];
-		if (sl < 0) {
-			atomicOr(P.err, EB_INACTIVE);
-			continue;
-		}
-		P.dlt[(size_t)sl * P.BV + leaf] = val[i];
-		a_track<L>(P, 0, g, s, gp, sl, leaf, L);
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		int gp, sl, leaf;
+		if (!seed_locate<D>(P, g, pos, i, gp, sl, leaf, true)) continue;
+		const unsigned long long key = (unsigned long long)i;
+		const int pe = gp * NL + L;
+		if (P.appos[0][pe] < 0 && atomicMin(&P.apkey[pe], key) == NOCLAIM)
+			P.aq[atomicAdd(&P.counters[CNT_AQ], 1)] = pe;
+		const size_t k = (size_t)sl * P.BV + leaf;
+		if (P.alkp[0][k] == NUL16 && atomicMin(&P.claim[k], key) == NOCLAIM &&
+		    atomicExch(&P.touched[sl], 1) == 0)
+			P.q_touch[atomicAdd(&P.counters[CNT_ATOUCH], 1)] = sl;
 	}
+}
+
+/// The delta values: a later call at a leaf overwrites an earlier one, so each leaf takes the
+/// value of its last call. Phases over the calls, using the leaf's claim word: 0 clears it, 1
+/// keeps the largest call index + 1, 2 lets that call write its value, 3 restores the word.
+template <int D, int L>
+__global__ void k_seed_values(Dev P, int s, const int* pos, const float* val, int n, int phase)
+{
+	const SurfGeom& g = P.geom[s];
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		int gp, sl, leaf;
+		if (!seed_locate<D>(P, g, pos, i, gp, sl, leaf, false)) continue;
+		const size_t k = (size_t)sl * P.BV + leaf;
+		const unsigned long long me = (unsigned long long)i + 1;
+		if (phase == 0) P.claim[k] = 0;
+		else if (phase == 1) atomicMax(&P.claim[k], me);
+		else if (phase == 2) { if (P.claim[k] == me) P.dlt[k] = val[i]; }
+		else P.claim[k] = NOCLAIM;
+	}
+}
+
+/// After the seed's appends: the delta grid's zero-layer prefix of each affected partition.
+template <int L>
+__global__ void k_seed_finish(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
 	const int np = P.apcnt[0][s * NL + L];
-	for (int i = 0; i < np; i++) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
 		const int gp = g.pbase + P.aplist[0][(size_t)L * P.NP + g.pbase + i];
 		const int sl = P.slot[gp];
 		P.dlcnt[sl] = P.acnt[0][sl * NL + L];
 	}
-	P.ndp[s] = np;
+	if (blockIdx.x == 0 && threadIdx.x == 0) P.ndp[s] = np;
 }
 
-/// calc_affected rings (Surface.hpp:801-912): L times, the in-band neighbours of the leaves
-/// added by the previous ring join affected buffer 0 under their current layer.
-template <int D, int L>
-__global__ void k_calc_affected(Dev P, int s)
+// ---------------------------------------------------------------------------------------------
+// calc_affected rings (Surface.hpp:801-912), in parallel. L times, the in-band neighbours of the
+// leaves added by the previous ring join affected buffer 0 under their current layer. The
+// reference does this in one sequential loop: per list l, per partition entry of the affected
+// list l (in list order, those present at the ring's start), per leaf added by the previous ring
+// (in list order), per neighbour direction, a track call that appends the leaf to its list and,
+// on the first call into a (partition, list), the partition to the affected partition list. Here
+// every track call gets the key (l, entry, leaf position, direction) of its place in that loop:
+// a leaf untracked at the ring's start goes to the smallest key that tracks it, a (partition,
+// list) joins at the smallest key of any call into it, and both are appended in key order, which
+// is the order the loop appends them in.
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long ring_key(int l, int entry, int pos, int nb)
+{
+	return ((unsigned long long)l << 47) | ((unsigned long long)entry << 19) |
+	       ((unsigned long long)pos << 3) | (unsigned long long)nb;
+}
+
+/// Ring bounds (Surface.hpp:801-815): entries present at the previous ring's start expand the
+/// leaves added since ([first, last) = [previous last, current count)); newer entries expand all
+/// their leaves. Entries with leaves to expand are queued. One thread per (list, entry).
+template <int L>
+__global__ void k_ring_setup(Dev P, int s, int np, int cur)
 {
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
-	int* first = P.ring_first;
-	int* last = P.ring_last;
-	int nsnap[NL], prev[NL];
-	for (int l = 0; l < NL; l++) prev[l] = 0;
-	for (int ud = 1; ud <= L; ud++) {
-		for (int l = 0; l < NL; l++) {
-			const int nc = P.apcnt[0][s * NL + l];
-			for (int i = 0; i < nc; i++) {
-				const size_t o = (size_t)l * P.NP + g.pbase + i;
-				if (i >= prev[l]) first[o] = 0;
-				const int gp = g.pbase + P.aplist[0][o];
-				last[o] = P.acnt[0][P.slot[gp] * NL + l];
-			}
-			nsnap[l] = nc;
-			prev[l] = nc;
-		}
-		for (int l = 0; l < NL; l++) {
-			for (int ic = 0; ic < nsnap[l]; ic++) {
-				const size_t o = (size_t)l * P.NP + g.pbase + ic;
-				const int gp = g.pbase + P.aplist[0][o];
-				const int sl = P.slot[gp];
-				for (int in = first[o]; in < last[o]; in++) {
-					const int leaf = P.alst[0][((size_t)sl * NL + l) * P.BV + in];
-					const Vec<D> c = leaf_pos<D>(P, gp, leaf);
-					for (int nb = 0; nb < 2 * D; nb++) {
-						Vec<D> q = c;
-						q[nb >> 1] += (nb & 1) ? 1 : -1;
-						const int lid = layer_id(get_phi<D, L>(P, g, q), P.err);
-						if (!inside_band(lid, L)) continue;
-						int gpn, leafn;
-						locate<D>(P, g, q, gpn, leafn);
-						const int sln = P.slot[gpn];
-						if (sln < 0) {
-							atomicOr(P.err, EB_INACTIVE);
-							continue;
-						}
-						a_track<L>(P, 0, g, s, gpn, sln, leafn, lid + L);
-					}
-				}
-			}
-		}
-		for (int l = 0; l < NL; l++)
-			for (int ic = 0; ic < nsnap[l]; ic++) {
-				const size_t o = (size_t)l * P.NP + g.pbase + ic;
-				first[o] = last[o];
-			}
+	const int prev = cur ^ 1;
+	for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < NL * np; t += gridDim.x * blockDim.x) {
+		const int l = t / np, i = t % np;
+		const int nc = P.apcnt[0][s * NL + l];
+		if (i == 0) P.ring_n[cur * NL + l] = nc;
+		if (i >= nc) continue;
+		const size_t o = (size_t)l * P.NP + g.pbase + i;
+		const int gp = g.pbase + P.aplist[0][o];
+		const int first = i < P.ring_n[prev * NL + l] ? P.ring_last[o] : 0;
+		const int last = P.acnt[0][P.slot[gp] * NL + l];
+		P.ring_first[o] = first;
+		P.ring_last[o] = last;
+		if (last > first) P.ring_src[atomicAdd(&P.counters[CNT_ASRC], 1)] = (int)o;
 	}
+}
+
+/// The track calls of one ring: one warp per queued entry, a lane per leaf; each call claims
+/// its leaf (if untracked) and its (partition, list) (if not yet listed) with its key.
+template <int D, int L>
+__global__ void k_ring_claim(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	const int lane = threadIdx.x & 31;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	const int n = P.counters[CNT_ASRC];
+	for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nw) {
+		const size_t o = (size_t)P.ring_src[w];
+		const int l = (int)((o - g.pbase) / P.NP), entry = (int)((o - g.pbase) % P.NP);
+		const int gp = g.pbase + P.aplist[0][o];
+		const int sl = P.slot[gp];
+		const int first = P.ring_first[o], last = P.ring_last[o];
+		for (int in = first + lane; in < last; in += 32) {
+			const int leaf = P.alst[0][((size_t)sl * NL + l) * P.BV + in];
+			const Vec<D> c = leaf_pos<D>(P, gp, leaf);
+			for (int nb = 0; nb < 2 * D; nb++) {
+				Vec<D> q = c;
+				q[nb >> 1] += (nb & 1) ? 1 : -1;
+				const int lid = layer_id(get_phi<D, L>(P, g, q), P.err);
+				if (!inside_band(lid, L)) continue;
+				int gpn, leafn;
+				locate<D>(P, g, q, gpn, leafn);
+				const int sln = P.slot[gpn];
+				if (sln < 0) {
+					atomicOr(P.err, EB_INACTIVE);
+					continue;
+				}
+				const int t = lid + L;
+				const unsigned long long key = ring_key(l, entry, in, nb);
+				const int pe = gpn * NL + t;
+				if (P.appos[0][pe] < 0 && atomicMin(&P.apkey[pe], key) == NOCLAIM)
+					P.aq[atomicAdd(&P.counters[CNT_AQ], 1)] = pe;
+				const size_t k = (size_t)sln * P.BV + leafn;
+				if (P.alkp[0][k] == NUL16 && atomicMin(&P.claim[k], key) == NOCLAIM &&
+				    atomicExch(&P.touched[sln], 1) == 0)
+					P.q_touch[atomicAdd(&P.counters[CNT_ATOUCH], 1)] = sln;
+			}
+		}
+	}
+}
+
+/// Appends each touched brick's claimed leaves to their lists (the list of the leaf's current
+/// layer) in key order, and clears the claims. One block per brick; up to `cap` claimed leaves
+/// are ranked in shared memory, more are ranked by scanning the brick's claims.
+template <int L>
+__global__ void k_ring_append(Dev P, int cap, int fixed_list)
+{
+	constexpr int NL = 2 * L + 1;
+	extern __shared__ unsigned char ring_smem[];
+	unsigned long long* skey = (unsigned long long*)ring_smem;
+	uint16_t* sleaf = (uint16_t*)(skey + cap);
+	uint8_t* slist = (uint8_t*)(sleaf + cap);
+	__shared__ int m, scnt[NL];
+	const int nb = P.counters[CNT_ATOUCH];
+	for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+		const int sl = P.q_touch[b];
+		const size_t base = (size_t)sl * P.BV;
+		if (threadIdx.x == 0) m = 0;
+		if (threadIdx.x < NL) scnt[threadIdx.x] = 0;
+		__syncthreads();
+		for (int j = threadIdx.x; j < P.BV; j += blockDim.x) {
+			const unsigned long long k = P.claim[base + j];
+			if (k == NOCLAIM) continue;
+			const int t = fixed_list >= 0 ? fixed_list : layer_id(P.phi[base + j], P.err) + L;
+			atomicAdd(&scnt[t], 1);
+			const int at = atomicAdd(&m, 1);
+			if (at < cap) {
+				skey[at] = k;
+				sleaf[at] = (uint16_t)j;
+				slist[at] = (uint8_t)t;
+			}
+		}
+		__syncthreads();
+		const int mm = m;
+		if (mm <= cap) {
+			for (int i = threadIdx.x; i < mm; i += blockDim.x) {
+				const unsigned long long ki = skey[i];
+				const int ti = slist[i];
+				int r = 0;
+				for (int j = 0; j < mm; j++) r += slist[j] == ti && skey[j] < ki;
+				const int leaf = sleaf[i];
+				const int c = P.acnt[0][sl * NL + ti] + r;
+				P.alst[0][((size_t)sl * NL + ti) * P.BV + c] = (uint16_t)leaf;
+				P.alkp[0][base + leaf] = (uint16_t)c;
+			}
+		} else {
+			for (int i = threadIdx.x; i < P.BV; i += blockDim.x) {
+				const unsigned long long ki = P.claim[base + i];
+				if (ki == NOCLAIM) continue;
+				const int ti = fixed_list >= 0 ? fixed_list : layer_id(P.phi[base + i], P.err) + L;
+				int r = 0;
+				for (int j = 0; j < P.BV; j++) {
+					const unsigned long long kj = P.claim[base + j];
+					if (kj < ki && (fixed_list >= 0 || layer_id(P.phi[base + j], P.err) + L == ti)) r++;
+				}
+				const int c = P.acnt[0][sl * NL + ti] + r;
+				P.alst[0][((size_t)sl * NL + ti) * P.BV + c] = (uint16_t)i;
+				P.alkp[0][base + i] = (uint16_t)c;
+			}
+		}
+		__syncthreads();
+		for (int j = threadIdx.x; j < P.BV; j += blockDim.x) P.claim[base + j] = NOCLAIM;
+		if (threadIdx.x < NL) P.acnt[0][sl * NL + threadIdx.x] += scnt[threadIdx.x];
+		if (threadIdx.x == 0) P.touched[sl] = 0;
+		__syncthreads();
+	}
+}
+
+/// Appends the (partition, list) entries that joined in this ring to the affected partition
+/// lists in key order. One thread per entry.
+template <int L>
+__global__ void k_ring_plist(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	const int n = P.counters[CNT_AQ];
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const int pe = P.aq[i];
+		const int t = pe % NL;
+		const unsigned long long ki = P.apkey[pe];
+		int r = 0;
+		for (int j = 0; j < n; j++) {
+			const int pj = P.aq[j];
+			r += pj % NL == t && P.apkey[pj] < ki;
+		}
+		const int c = P.apcnt[0][s * NL + t] + r;
+		P.aplist[0][(size_t)t * P.NP + g.pbase + c] = pe / NL - g.pbase;
+		P.appos[0][pe] = c;
+		atomicAdd(&P.counters[CNT_ATC + t], 1);
+	}
+}
+
+/// Closes a ring: list lengths, key and queue reset.
+template <int L>
+__global__ void k_ring_finish(Dev P, int s)
+{
+	constexpr int NL = 2 * L + 1;
+	const int n = P.counters[CNT_AQ];
+	for (int i = threadIdx.x; i < n; i += blockDim.x) P.apkey[P.aq[i]] = NOCLAIM;
+	__syncthreads();
+	if (threadIdx.x < NL) {
+		P.apcnt[0][s * NL + threadIdx.x] += P.counters[CNT_ATC + threadIdx.x];
+		P.counters[CNT_ATC + threadIdx.x] = 0;
+	}
+	if (threadIdx.x == 0) {
+		P.counters[CNT_AQ] = 0;
+		P.counters[CNT_ATOUCH] = 0;
+		P.counters[CNT_ASRC] = 0;
+	}
+}
+
+/// Zero-layer leaves of surface s (the capacity a bounded update's deltas need).
+template <int L>
+__global__ void k_count_layer(Dev P, int s, int li, unsigned long long* out)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	const int np = P.pcnt[s * NL + li];
+	unsigned long long c = 0;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+		const int gp = g.pbase + P.plist[(size_t)li * P.NP + g.pbase + i];
+		c += P.lcnt[P.slot[gp] * NL + li];
+	}
+	if (c) atomicAdd(out, c);
 }
 
 /// isogrid.track_children(affected) and delta.track_children(affected) of update_end
