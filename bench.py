@@ -65,6 +65,11 @@ CONFIGS = {
                         "log-uniform 32..256, 8^3 partitions, speed constant U[-0.6,-0.1] | "
                         "-0.3*curv-0.2 | 0.2*hash_noise-0.2, 1..64 steps, polygonise p=0.5, "
                         "admission by a 150 GB brick-pool budget"),
+    "local": dict(kind="local", D=3, L=2, size=(256, 256, 256), part=(8, 8, 8), expand=30,
+                  box=48, centre=(30, 0, 0), speeds=(-0.2, 0.2), steps=200, cpu_steps=5000,
+                  workload="Surface::update(lo, hi, fn) on Surface<3,2> 256^3 / 8^3 partitions, "
+                           "r~30 (30 steps of speed -1): each edit a 48^3 box on the surface "
+                           "(centre (30,0,0)), constant speed alternating -0.2 / +0.2"),
     "ray": dict(kind="ray", D=3, L=3, size=(512, 512, 512), part=(16, 16, 16), expand=100,
                 rays=1 << 20, steps=20, cpu_min_seconds=10.0,
                 workload="Surface::ray on Surface<3,3> 512^3 / 16^3 partitions, r~100 (100 "
@@ -446,6 +451,10 @@ def run_reference(args, name, cfg):
         steps = 1
         base = cpu_rays(cfg)
         metric, unit = "rays/s", "rays/s"
+    elif cfg["kind"] == "local":
+        steps = cfg["cpu_steps"]
+        base = cpu_local(cfg)
+        metric, unit = "local edits/s", "edits/s"
     else:
         steps = args.steps or cfg["steps"]
         steps = min(steps, 20 if cfg["kind"] == "single" else 10)
@@ -666,6 +675,112 @@ def run_ray(args, name, cfg):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": config, "roofline": roof, "cpu_baseline": cpu,
             "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def local_box(cfg):
+    h = cfg["box"] // 2
+    return ([c - h for c in cfg["centre"]], [c + h for c in cfg["centre"]])
+
+
+def cpu_local(cfg):
+    """The oracle's bounded updates: the same edits on the same surface, one after another, on
+    one thread (the oracle starts threads per parallel loop, which costs these small edits more
+    than it saves: one thread is its fastest here)."""
+    from oracle import oracle as O
+    threads = O.set_threads(1)
+    s = O.Surface(cfg["size"], cfg["part"], cfg["L"])
+    s.seed((0,) * cfg["D"])
+    s.run_steps(cfg["expand"], c=-1.0)
+    lo, hi = local_box(cfg)
+    secs = 0.0
+    n = cfg["cpu_steps"]
+    for i in range(n):
+        t0 = time.perf_counter()
+        s.update_bounded(lo, hi, c=cfg["speeds"][i % 2])
+        secs += time.perf_counter() - t0
+    return {"value": n / secs, "unit": "edits/s", "cores": threads, "kind": "port",
+            "sample": f"{n} edits of the workload after the same setup ({secs:.2f} s on "
+                      f"{threads} thread, the oracle's fastest setting for edits this small)"}
+
+
+def run_local(args, name, cfg):
+    """Interactive edits: value = bounded updates per second, device-timed; e2e = the same
+    through the C ABI with the band size read back after each edit."""
+    import torch
+    import felt_b200 as fb
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    steps = args.steps or cfg["steps"]
+    s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=args.brick_capacity)
+    s.seed((0,) * cfg["D"])
+    for _ in range(cfg["expand"]):
+        s.update(c=-1.0)
+    lo, hi = local_box(cfg)
+    sp = cfg["speeds"]
+    for i in range(max(args.warmup, 2) * 2):
+        s.update_bounded(lo, hi, c=sp[i % 2])
+    stream = torch.cuda.ExternalStream(s.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = fb.launch_count()
+    total = 0.0
+    if args.profile_region:
+        torch.cuda.profiler.start()
+    for i in range(steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.update_bounded(lo, hi, c=sp[i % 2])
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    if args.profile_region:
+        torch.cuda.profiler.stop()
+    wall = 0.0
+    for i in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.update_bounded(lo, hi, c=sp[i % 2])
+        s.band_size()
+        wall += time.perf_counter() - t0
+    launches = fb.launch_count() - l0
+    clk = clocks.stop()
+    if pg:
+        total, wall, _ = combine_ranks(pg, total, wall, 0.0, "cuda")
+    value = ws * steps / (total / 1e3)
+    cpu = None
+    if rank == 0:
+        if ws == 1 and not args.no_cpu:
+            cpu = cpu_local(cfg)
+        config = {"workload": cfg["workload"], "name": name, "parallelism": f"replicas{ws}",
+                  "band_nodes": s.band_size(),
+                  "l2": "flushed between timed edits (256 MB write)"}
+        line = {
+            "metric": "local edits/s", "value": value, "unit": "edits/s", "n_gpus": ws,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": total / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config, "roofline": None, "cpu_baseline": cpu,
+            "e2e": {"value": ws * steps / wall, "unit": "edits/s", "h2d_bytes_per_step": 44,
+                    "d2h_bytes_per_step": 8,
+                    "how": "fg_update_bounded then the band size read back, wall clock"},
+            "clocks": clk, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -940,6 +1055,8 @@ def main():
         run_serve(args, args.config, cfg)
     elif cfg["kind"] == "ray":
         run_ray(args, args.config, cfg)
+    elif cfg["kind"] == "local":
+        run_local(args, args.config, cfg)
     else:
         run_felt(args, args.config, cfg)
 
