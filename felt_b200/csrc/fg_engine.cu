@@ -552,7 +552,26 @@ public:
 		FG_CUDA(cudaStreamSynchronize(st_));
 		ensure_local_staging((int)nz + 1);
 		update_start();
-		FG_RUN("k_bounded_collect", st_, k_bounded_collect<D, L><<<1, 1, 0, st_>>>(P_, 0, vlo, vhi, d_lpos_, lcap_, d_lcount_););
+		// the partitions covering the box: pos_child (truncating division) of the grid's and
+		// the box's corners, zero-based (Surface.hpp:313-330)
+		const SurfGeom& g = geom_[0];
+		BoxParts<D> b;
+		long long nb = 1;
+		for (int a = 0; a < D; a++) {
+			const int grid_hi = (g.hi[a] - 1 - g.off[a]) / csz_[a];
+			b.cl[a] = std::max(0, (vlo[a] - g.off[a]) / csz_[a]);
+			const int cu = std::min(grid_hi, (vhi[a] - g.off[a]) / csz_[a]);
+			b.box[a] = cu - b.cl[a] + 1;
+			b.lo[a] = vlo[a];
+			b.lub[a] = std::min(g.hi[a], vhi[a] + 1);
+			nb *= b.box[a] > 0 ? b.box[a] : 0;
+		}
+		b.nb = (int)nb;
+		int* counts = P_.ring_src;  // idle until calc_affected's rings
+		int* offsets = P_.ring_first;
+		FG_RUN("k_bounded_count", st_, k_bounded_count<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0, b, counts););
+		FG_RUN("k_scan_offsets", st_, k_scan_offsets<<<1, 1024, 0, st_>>>(counts, b.nb, offsets, d_lcount_););
+		FG_RUN("k_bounded_write", st_, k_bounded_write<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0, b, offsets, d_lpos_, lcap_););
 		FG_RUN("k_bounded_speed", st_, k_bounded_speed<D, L><<<grid_for(nz + 1), 256, 0, st_>>>(P_, 0, sp, d_lpos_, d_lcount_, d_lval_););
 		int n = 0;
 		FG_CUDA(cudaMemcpyAsync(&n, d_lcount_, sizeof(int), cudaMemcpyDeviceToHost, st_));
@@ -599,7 +618,7 @@ public:
 		const int A = 0, B = 1;
 		buf_dirty_[A] = true;
 		calc_affected();
-		FG_RUN("k_local_children", st_, k_local_children<L><<<1, 1, 0, st_>>>(P_, 0););
+		FG_RUN("k_local_children", st_, k_local_children<L><<<NL, 1024, 0, st_>>>(P_, 0););
 		count_band();
 		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
 		// over the affected lists (update_distance(plookup = affected, buffer))

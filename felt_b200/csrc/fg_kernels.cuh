@@ -1883,79 +1883,174 @@ __global__ void k_count_layer(Dev P, int s, int li, unsigned long long* out)
 }
 
 /// isogrid.track_children(affected) and delta.track_children(affected) of update_end
-/// (Surface.hpp:409-410; PartitionedMixin.hpp:319-334). The delta partition lists, reset at
-/// update_start and holding the delta() partitions first, end up equal to the affected lists.
+/// (Surface.hpp:409-410; PartitionedMixin.hpp:319-334): per list, the affected partitions not
+/// yet in the isogrid's partition list are appended to it in affected-list order, and the delta
+/// partition lists (reset at update_start, holding the delta() partitions first) become equal to
+/// the affected lists. One block per list; an ordered append by block-wide prefix sums.
 template <int L>
-__global__ void k_local_children(Dev P, int s)
+__global__ void __launch_bounds__(1024) k_local_children(Dev P, int s)
 {
 	constexpr int NL = 2 * L + 1;
+	__shared__ int wsum[32];
+	__shared__ int base;
 	const SurfGeom& g = P.geom[s];
-	for (int l = 0; l < NL; l++) {
-		const int na = P.apcnt[0][s * NL + l];
-		for (int i = 0; i < na; i++) {
+	const int l = blockIdx.x;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	const int na = P.apcnt[0][s * NL + l];
+	if (threadIdx.x == 0) base = P.pcnt[s * NL + l];
+	__syncthreads();
+	for (int start = 0; start < na; start += blockDim.x) {
+		const int i = start + threadIdx.x;
+		int lp = 0, gp = 0;
+		bool add = false;
+		if (i < na) {
 			const size_t o = (size_t)l * P.NP + g.pbase + i;
-			const int lp = P.aplist[0][o];
-			const int gp = g.pbase + lp;
-			if (P.ppos[gp * NL + l] < 0) {
-				const int c = P.pcnt[s * NL + l];
-				P.plist[(size_t)l * P.NP + g.pbase + c] = lp;
-				P.ppos[gp * NL + l] = c;
-				P.pcnt[s * NL + l] = c + 1;
-			}
+			lp = P.aplist[0][o];
+			gp = g.pbase + lp;
+			add = P.ppos[gp * NL + l] < 0;
 			P.dplist[o] = lp;
 		}
+		const unsigned m = __ballot_sync(0xffffffffu, add);
+		if (lane == 0) wsum[warp] = __popc(m);
+		__syncthreads();
+		int before = 0, total = 0;
+		for (int w = 0; w < nwarp; w++) {
+			if (w < warp) before += wsum[w];
+			total += wsum[w];
+		}
+		if (add) {
+			const int c = base + before + __popc(m & ((1u << lane) - 1u));
+			P.plist[(size_t)l * P.NP + g.pbase + c] = lp;
+			P.ppos[gp * NL + l] = c;
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) base += total;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		P.pcnt[s * NL + l] = base;
 		P.dpcnt[s * NL + l] = na;
 	}
 }
 
-/// update(lo, hi, fn) (Surface.hpp:310-386): the zero-layer leaves of the partitions covering
-/// the box, in the reference's order (box partitions row-major, leaf list order), that lie in
-/// [lo, hi]. Writes their positions; *n receives the count (up to cap).
+/// The partitions of a bounded update's box (Surface.hpp:313-330): box[a] children from cl[a]
+/// along each axis, row-major; leaves with lo <= pos < lub are inside.
+template <int D>
+struct BoxParts {
+	Vec<D> cl, box, lo, lub;
+	int nb;
+};
+
+/// update(lo, hi, fn) (Surface.hpp:310-386), in three steps that keep the reference's order
+/// (box partitions row-major, each partition's zero-layer list in order): count each
+/// partition's leaves inside the box, scan the counts, write the positions at their offsets.
+template <int D>
+__device__ __forceinline__ int box_partition(const Dev& P, const SurfGeom& g, const BoxParts<D>& b,
+                                             int ci)
+{
+	Vec<D> pc;
+	int r = ci;
+	for (int a = D - 1; a >= 0; a--) {
+		pc[a] = r % b.box[a] + b.cl[a];
+		r /= b.box[a];
+	}
+	int idx = 0;
+	for (int a = 0; a < D; a++) idx = idx * g.ccount[a] + pc[a];
+	return g.pbase + idx;
+}
+
 template <int D, int L>
-__global__ void k_bounded_collect(Dev P, int s, Vec<D> lo, Vec<D> hi, int* pos, int cap, int* n)
+__device__ __forceinline__ bool leaf_in_box(const Dev& P, const BoxParts<D>& b, int gp, int leaf,
+                                            Vec<D>& p)
+{
+	p = leaf_pos<D>(P, gp, leaf);
+	for (int a = 0; a < D; a++)
+		if (p[a] < b.lo[a] || p[a] >= b.lub[a]) return false;
+	return true;
+}
+
+/// One warp per box partition: its zero-layer leaves inside the box (counts[ci]).
+template <int D, int L>
+__global__ void k_bounded_count(Dev P, int s, BoxParts<D> b, int* counts)
 {
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
-	Vec<D> cl, cu, box, lub;
-	long long nb = 1;
-	for (int a = 0; a < D; a++) {
-		// pos_child (truncating division, PartitionedMixin.hpp:233-245) of the grid's corners
-		// and of the box corners, in zero-based children coordinates (Surface.hpp:313-330)
-		const int grid_lo = 0;
-		const int grid_hi = (g.hi[a] - 1 - g.off[a]) / P.csz[a];
-		cl[a] = max(grid_lo, (lo[a] - g.off[a]) / P.csz[a]);
-		cu[a] = min(grid_hi, (hi[a] - g.off[a]) / P.csz[a]);
-		box[a] = cu[a] - cl[a] + 1;
-		lub[a] = min(g.hi[a], hi[a] + 1);
-		nb *= box[a] > 0 ? box[a] : 0;
-	}
-	int c = 0;
-	for (long long ci = 0; ci < nb; ci++) {
-		Vec<D> pc;
-		long long r = ci;
-		for (int a = D - 1; a >= 0; a--) {
-			pc[a] = (int)(r % box[a]) + cl[a];
-			r /= box[a];
+	const int lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < b.nb; ci += nw) {
+		const int gp = box_partition<D>(P, g, b, ci);
+		const int sl = P.slot[gp];
+		int c = 0;
+		if (sl >= 0) {
+			const int nl = P.lcnt[sl * NL + L];
+			const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
+			for (int j = lane; j < nl; j += 32) {
+				Vec<D> p;
+				c += leaf_in_box<D, L>(P, b, gp, lst[j], p);
+			}
 		}
-		int idx = 0;
-		for (int a = 0; a < D; a++) idx = idx * g.ccount[a] + pc[a];
-		const int gp = g.pbase + idx;
+		for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+		if (lane == 0) counts[ci] = c;
+	}
+}
+
+/// Exclusive scan of n counts into offsets (one block, in order); the total into *total.
+static __global__ void __launch_bounds__(1024) k_scan_offsets(const int* counts, int n, int* offsets,
+                                                       int* total)
+{
+	__shared__ int wsum[32];
+	__shared__ int base;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+	if (threadIdx.x == 0) base = 0;
+	__syncthreads();
+	for (int start = 0; start < n; start += blockDim.x) {
+		const int i = start + threadIdx.x;
+		const int v = i < n ? counts[i] : 0;
+		int x = v;
+		for (int o = 1; o < 32; o <<= 1) {
+			const int y = __shfl_up_sync(0xffffffffu, x, o);
+			if (lane >= o) x += y;
+		}
+		if (lane == 31) wsum[warp] = x;
+		__syncthreads();
+		int before = 0, tot = 0;
+		for (int w = 0; w < nwarp; w++) {
+			if (w < warp) before += wsum[w];
+			tot += wsum[w];
+		}
+		if (i < n) offsets[i] = base + before + x - v;
+		__syncthreads();
+		if (threadIdx.x == 0) base += tot;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) *total = base;
+}
+
+/// One warp per box partition: its inside leaves' positions at its offset, in list order (up to
+/// cap positions in all).
+template <int D, int L>
+__global__ void k_bounded_write(Dev P, int s, BoxParts<D> b, const int* offsets, int* pos, int cap)
+{
+	constexpr int NL = 2 * L + 1;
+	const SurfGeom& g = P.geom[s];
+	const int lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
+	for (int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < b.nb; ci += nw) {
+		const int gp = box_partition<D>(P, g, b, ci);
 		const int sl = P.slot[gp];
 		if (sl < 0) continue;
 		const int nl = P.lcnt[sl * NL + L];
-		for (int j = 0; j < nl; j++) {
-			const int leaf = P.lst[((size_t)sl * NL + L) * P.BV + j];
-			const Vec<D> p = leaf_pos<D>(P, gp, leaf);
-			bool in = true;
-			for (int a = 0; a < D; a++)
-				if (p[a] < lo[a] || p[a] >= lub[a]) in = false;
-			if (!in) continue;
-			if (c < cap)
+		const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
+		int at = offsets[ci];
+		for (int j0 = 0; j0 < nl; j0 += 32) {
+			const int j = j0 + lane;
+			Vec<D> p;
+			const bool in = j < nl && leaf_in_box<D, L>(P, b, gp, lst[j], p);
+			const unsigned m = __ballot_sync(0xffffffffu, in);
+			const int c = at + __popc(m & ((1u << lane) - 1u));
+			if (in && c < cap)
 				for (int a = 0; a < D; a++) pos[c * D + a] = p[a];
-			c++;
+			at += __popc(m);
 		}
 	}
-	*n = c;
 }
 
 /// The speed functor at each collected position, before any value changes.
