@@ -28,8 +28,19 @@ namespace felt_gpu {
 template <int D>
 using DevVec = fg::Vec<D>;
 
+/// A D-vector of floats returned by the gradient functions.
+template <int D>
+struct DevVecF {
+	float v[D];
+	__host__ __device__ float& operator[](int i) { return v[i]; }
+	__host__ __device__ const float& operator[](int i) const { return v[i]; }
+};
+
 /// Read access to the isogrid from a speed functor: get (Access::get with the lazy child get,
-/// PartitionedMixin.hpp:594-601), curv (NumericMixin.hpp:72-156), inside (GridMixin inside).
+/// PartitionedMixin.hpp:594-601), curv (NumericMixin.hpp:72-156), inside (GridMixin inside), and
+/// the rest of the reference's Numeric API at grid nodes (NumericMixin.hpp:165-355): grad,
+/// gradF, gradB, gradC, gradE, divergence. FP32 rounded step by step as the reference's code
+/// (the grid spacing dx is 1, so its final divisions by dx change nothing).
 template <int D, int L>
 struct IsoGridView {
 	const fg::Dev* P;
@@ -37,6 +48,101 @@ struct IsoGridView {
 	__device__ float get(const DevVec<D>& p) const { return fg::get_phi<D, L>(*P, *g, p); }
 	__device__ float curv(const DevVec<D>& p) const { return fg::curv<D, L>(*P, *g, p); }
 	__device__ bool inside(const DevVec<D>& p) const { return fg::in_grid<D>(*g, p); }
+
+	/// grad (NumericMixin.hpp:189-231): central difference, one-sided at the grid's edge, 0
+	/// where neither neighbour is inside.
+	__device__ DevVecF<D> grad(const DevVec<D>& p) const
+	{
+		DevVecF<D> r;
+		const float centre = get(p);
+		DevVec<D> t = p;
+		for (int a = 0; a < D; a++) {
+			float back = centre, fwd = centre;
+			int order = 0;
+			t[a] -= 1;
+			if (inside(t)) {
+				back = get(t);
+				order++;
+			}
+			t[a] += 2;
+			if (inside(t)) {
+				fwd = get(t);
+				order++;
+			}
+			t[a] -= 1;
+			r[a] = order ? __fdiv_rn(__fsub_rn(fwd, back), (float)order) : 0.0f;
+		}
+		return r;
+	}
+	/// gradE (NumericMixin.hpp:243-270): the upwind (entropy-satisfying) gradient,
+	/// max(centre - back, 0) + min(forward - centre, 0) per axis.
+	__device__ DevVecF<D> gradE(const DevVec<D>& p) const
+	{
+		DevVecF<D> r;
+		const float centre = get(p);
+		DevVec<D> t = p;
+		for (int a = 0; a < D; a++) {
+			t[a] -= 1;
+			const float back = __fsub_rn(centre, get(t));
+			t[a] += 2;
+			const float fwd = __fsub_rn(get(t), centre);
+			t[a] -= 1;
+			const float b = back < 0.0f ? 0.0f : back;  // std::max(back, 0.0f)
+			const float f = 0.0f < fwd ? 0.0f : fwd;    // std::min(fwd, 0.0f)
+			r[a] = __fadd_rn(f, b);
+		}
+		return r;
+	}
+	/// gradF (NumericMixin.hpp:279-298): forward difference.
+	__device__ DevVecF<D> gradF(const DevVec<D>& p) const
+	{
+		DevVecF<D> r;
+		const float centre = get(p);
+		DevVec<D> t = p;
+		for (int a = 0; a < D; a++) {
+			t[a] += 1;
+			r[a] = __fsub_rn(get(t), centre);
+			t[a] -= 1;
+		}
+		return r;
+	}
+	/// gradB (NumericMixin.hpp:308-326): backward difference.
+	__device__ DevVecF<D> gradB(const DevVec<D>& p) const
+	{
+		DevVecF<D> r;
+		const float centre = get(p);
+		DevVec<D> t = p;
+		for (int a = 0; a < D; a++) {
+			t[a] -= 1;
+			r[a] = __fsub_rn(centre, get(t));
+			t[a] += 1;
+		}
+		return r;
+	}
+	/// gradC (NumericMixin.hpp:335-355): central difference.
+	__device__ DevVecF<D> gradC(const DevVec<D>& p) const
+	{
+		DevVecF<D> r;
+		DevVec<D> t = p;
+		for (int a = 0; a < D; a++) {
+			t[a] -= 1;
+			const float back = get(t);
+			t[a] += 2;
+			const float fwd = get(t);
+			t[a] -= 1;
+			r[a] = __fdiv_rn(__fsub_rn(fwd, back), 2.0f);
+		}
+		return r;
+	}
+	/// divergence (NumericMixin.hpp:165-175): the sum of gradF - gradB over the axes (Eigen's
+	/// fixed-size sum: x0 + (x1 + x2) in 3D).
+	__device__ float divergence(const DevVec<D>& p) const
+	{
+		const DevVecF<D> f = gradF(p), b = gradB(p);
+		float d[D];
+		for (int a = 0; a < D; a++) d[a] = __fsub_rn(f[a], b[a]);
+		return D == 2 ? __fadd_rn(d[0], d[1]) : __fadd_rn(d[0], __fadd_rn(d[1], d[D - 1]));
+	}
 };
 
 namespace detail {

@@ -591,6 +591,47 @@ public:
 		return curv_at<D, Real>([this](const Vi<D>& p) { return get(p); }, pos);
 	}
 
+	/// The Numeric API at a node (NumericMixin.hpp:165-355, grid spacing 1), into out in this
+	/// order: grad (189-231), gradF (279-298), gradB (308-326), gradC (335-355), gradE (243-270),
+	/// each D values, then divergence (165-175).
+	void numeric(const Vi<D>& pos, Real* out) const
+	{
+		const Real centre = get(pos);
+		Vi<D> t = pos;
+		Real* grad = out;
+		Real* gf = out + D;
+		Real* gb = out + 2 * D;
+		Real* gc = out + 3 * D;
+		Real* ge = out + 4 * D;
+		for (int a = 0; a < D; a++) {
+			t[a] -= 1;
+			const Real back = get(t);
+			const bool in_back = iso.in_grid(t);
+			t[a] += 2;
+			const Real fwd = get(t);
+			const bool in_fwd = iso.in_grid(t);
+			t[a] -= 1;
+			int order = 0;
+			Real b = centre, f = centre;
+			if (in_back) {
+				b = back;
+				order++;
+			}
+			if (in_fwd) {
+				f = fwd;
+				order++;
+			}
+			grad[a] = order ? (f - b) / Real(order) : Real(0);
+			gf[a] = fwd - centre;
+			gb[a] = centre - back;
+			gc[a] = (fwd - back) / Real(2);
+			ge[a] = std::min(fwd - centre, Real(0)) + std::max(centre - back, Real(0));
+		}
+		std::array<Real, D> diff;
+		for (int a = 0; a < D; a++) diff[a] = gf[a] - gb[a];
+		out[5 * D] = eigen_sum<Real, D>(diff);
+	}
+
 	Real speed(const Speed& s, const Vi<D>& pos) const
 	{
 		Real acc = 0;

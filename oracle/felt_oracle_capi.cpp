@@ -34,6 +34,7 @@ struct SurfBase {
 	virtual void stats(size_t* a, size_t* b) = 0;
 	virtual size_t band_size() = 0;
 	virtual void curv(const int* p, float* out) = 0;
+	virtual void numeric(const int* p, float* out) = 0;
 	virtual void ray(const float* o, const float* d, float* out) = 0;
 	virtual void save(std::vector<uint8_t>& out) = 0;
 	virtual void geometry(int* size, int* part) = 0;
@@ -129,6 +130,7 @@ struct Surf : SurfBase {
 		return n;
 	}
 	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
+	void numeric(const int* p, float* out) override { s.numeric(v(p), out); }
 	void save(std::vector<uint8_t>& out) override { fo::save_surface<D, L>(s, out); }
 	void geometry(int* size, int* part) override
 	{
@@ -362,6 +364,12 @@ int fo_ray(void* s, const float* origins, const float* dirs, size_t n, float* hi
 			b->ray(origins + i * D, dirs + i * D, hits + i * D);
 		});
 	});
+}
+
+/* The Numeric API at a node: grad, gradF, gradB, gradC, gradE (dims values each), divergence. */
+int fo_numeric(void* s, const int* pos, float* out)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->numeric(pos, out); });
 }
 
 int fo_curv(void* s, const int* pos, float* out)

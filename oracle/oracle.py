@@ -139,6 +139,12 @@ class Surface:
         _chk(lib().fo_curv(self._h, _ivec(pos), C.byref(v)))
         return v.value
 
+    def numeric(self, pos):
+        """grad, gradF, gradB, gradC, gradE (D values each) and divergence at a node."""
+        out = (C.c_float * (5 * self.D + 1))()
+        _chk(lib().fo_numeric(self._h, _ivec(pos), out))
+        return np.array(out, dtype=np.float32)
+
     def save(self):
         """Surface::save: the surface file (the reference's cereal binary layout) as bytes."""
         n = C.c_size_t()

@@ -57,3 +57,52 @@ def test_device_functors_match_oracle(tmp_path):
     d = first_difference(dump, o.dump())
     assert d is None, d
     assert float(np.abs(phi - o.snapshot().reshape(-1)).max()) <= 1e-5
+
+
+PROBE = os.path.join(ROOT, "felt_b200", "examples", "numeric_probe.cu")
+
+
+def _compile_probe(out, link):
+    if not os.path.exists(NVCC):
+        pytest.skip("nvcc not available")
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+           "-fmad=false", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(ROOT, "felt_b200", "include"), PROBE]
+    if link:
+        cmd += ["-L", LIB_DIR, "-lfelt_gpu", "-Xlinker", "-rpath," + LIB_DIR, "-o", out]
+    else:
+        cmd += ["-c", "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
+
+
+def test_numeric_probe_compiles(tmp_path):
+    _compile_probe(str(tmp_path / "numeric_probe.o"), link=False)
+
+
+@pytest.mark.gpu
+def test_numeric_api_matches_oracle(tmp_path):
+    """grad, gradF, gradB, gradC, gradE and divergence (NumericMixin.hpp:165-355) called from a
+    __device__ functor at every zero-layer node equal the oracle's, bit for bit."""
+    from oracle import oracle as O
+    exe = str(tmp_path / "numeric_probe")
+    _compile_probe(exe, link=True)
+    out = str(tmp_path / "numeric.bin")
+    r = subprocess.run([exe, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    n = 32
+    vals = np.fromfile(out, dtype=np.float32).reshape(n, n, n, 17)
+    o = O.Surface((n, n, n), (8, 8, 8), 2)
+    o.seed((0, 0, 0))
+    for _ in range(6):
+        o.update(c=-1.0)
+    for _ in range(4):
+        o.update(a=-0.3, c=-0.2)
+    idx = np.argwhere(vals[..., 16] == 1.0)
+    assert len(idx) > 100
+    assert len(idx) == o.layer_size(0)
+    for i, j, k in idx:
+        pos = (int(i) - n // 2, int(j) - n // 2, int(k) - n // 2)
+        want = o.numeric(pos)
+        got = vals[i, j, k, :16]
+        assert np.array_equal(got, want), (pos, got, want)
