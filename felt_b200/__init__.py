@@ -369,6 +369,19 @@ class Batch:
                                 out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
+    def save(self, i):
+        """Surface::save of surface i: the surface file as bytes."""
+        n = C.c_size_t()
+        _chk(lib().fg_batch_save(self._h, C.c_size_t(i), None, C.c_size_t(0), C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        _chk(lib().fg_batch_save(self._h, C.c_size_t(i), buf, C.c_size_t(n.value), C.byref(n)))
+        return bytes(buf)
+
+    def restore(self, i, data):
+        """Surface::load of a surface file into surface i, which must be empty."""
+        raw = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        _chk(lib().fg_batch_restore(self._h, C.c_size_t(i), raw, C.c_size_t(len(data))))
+
     def dump(self, i):
         return np.array(_fetch(lib().fg_batch_dump, self._h, C.c_size_t(i)), dtype=np.uint32)
 

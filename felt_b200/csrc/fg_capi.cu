@@ -590,6 +590,44 @@ int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float*
 	});
 }
 
+int fg_batch_save(fg_batch* b, size_t surface, uint8_t* buf, size_t cap, size_t* n)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(n, "length");
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
+		fg::SurfaceImage img;
+		fg::export_image(*b->eng, (int)surface, img);
+		std::vector<uint8_t> out;
+		int csz[3];
+		for (int a = 0; a < b->eng->dims(); a++) csz[a] = b->eng->part(a);
+		fg::write_surface_file(img, b->eng->geometry((int)surface), b->eng->dims(), b->eng->layers(),
+		                       csz, out);
+		*n = out.size();
+		if (buf) std::memcpy(buf, out.data(), std::min(cap, out.size()));
+	});
+}
+
+int fg_batch_restore(fg_batch* b, size_t surface, const uint8_t* data, size_t n)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(data, "data");
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
+		int D = 0, L = 0, size[3] = {1, 1, 1}, csz[3] = {1, 1, 1};
+		fg::peek_surface_file(data, n, D, L, size, csz);
+		const fg::SurfGeom& g = b->eng->geometry((int)surface);
+		if (D != b->eng->dims() || L != b->eng->layers())
+			throw fg::Error(FG_ERR_ARG, "surface file of another dimension or layer count");
+		for (int a = 0; a < D; a++)
+			if (size[a] != g.size[a] || csz[a] != b->eng->part(a))
+				throw fg::Error(FG_ERR_ARG, "surface file of another grid or partition size");
+		fg::SurfaceImage img;
+		fg::read_surface_file(data, n, g, D, L, csz, b->eng->dev().BV, img);
+		fg::restore_image(*b->eng, (int)surface, img);
+	});
+}
+
 int fg_batch_dump(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n)
 {
 	return guard([&] {

@@ -66,6 +66,38 @@ __global__ void k_gather_bricks(Dev P, const int* slots, int n, float* phi, uint
 	}
 }
 
+/// Writes staged bricks into their slots (the inverse of k_gather_bricks) and sets the rest of
+/// each brick as activation leaves it (brick_init): no status, empty affected lists, no claims.
+template <int L>
+__global__ void k_scatter_bricks(Dev P, const int* slots, const int* gps, int n, const float* phi,
+                                 const uint16_t* lkp, const uint16_t* lst, const int* lcnt)
+{
+	constexpr int NL = 2 * L + 1;
+	for (int i = blockIdx.x; i < n; i += gridDim.x) {
+		const int sl = slots[i];
+		const size_t dst = (size_t)sl * P.BV, src = (size_t)i * P.BV;
+		for (int j = threadIdx.x; j < P.BV; j += blockDim.x) {
+			P.phi[dst + j] = phi[src + j];
+			P.lkp[dst + j] = lkp[src + j];
+			P.sto[dst + j] = (int8_t)(L + 1);
+			P.alkp[0][dst + j] = NUL16;
+			P.alkp[1][dst + j] = NUL16;
+			P.claim[dst + j] = NOCLAIM;
+		}
+		for (int j = threadIdx.x; j < NL * P.BV; j += blockDim.x) P.lst[dst * NL + j] = lst[src * NL + j];
+		for (int j = threadIdx.x; j < NL; j += blockDim.x) {
+			P.lcnt[sl * NL + j] = lcnt[i * NL + j];
+			P.ccnt[sl * NL + j] = 0;
+			P.acnt[0][sl * NL + j] = 0;
+			P.acnt[1][sl * NL + j] = 0;
+		}
+		if (threadIdx.x == 0) {
+			P.slot_gp[sl] = gps[i];
+			P.touched[sl] = 0;
+		}
+	}
+}
+
 template <class T>
 T* dev_alloc(size_t n, cudaStream_t st)
 {
@@ -269,6 +301,83 @@ void import_image(EngineBase& eng, const SurfaceImage& img)
 	}
 	const int ntop = P.nslots - nact;
 	FG_CUDA(cudaMemcpyAsync(P.counters + CNT_FREE_TOP, &ntop, sizeof(int), cudaMemcpyHostToDevice, st));
+	FG_CUDA(cudaStreamSynchronize(st));
+	eng.check_errors();
+}
+
+void restore_image(EngineBase& eng, int s, const SurfaceImage& img)
+{
+	const int L = eng.layers(), NL = 2 * L + 1;
+	const Dev& P = eng.dev();
+	if (s < 0 || s >= eng.surfaces()) throw Error(-1, "surface index out of range");
+	const SurfGeom& g = eng.geometry(s);
+	if (img.np != g.np || img.NL != NL || img.BV != P.BV)
+		throw Error(-1, "surface image does not fit this surface");
+	if (eng.frozen(s)) throw Error(-15, "restoring into a stopped surface");
+	cudaStream_t st = eng.stream();
+	eng.sync();
+	// the surface must be empty: no active partition, every list of it empty
+	std::vector<int> slot(g.np);
+	FG_CUDA(cudaMemcpy(slot.data(), P.slot + g.pbase, g.np * sizeof(int), cudaMemcpyDeviceToHost));
+	for (int v : slot)
+		if (v >= 0) throw Error(-15, "restoring needs an empty surface (no active partition)");
+	const int* counts[] = {P.pcnt, P.dpcnt, P.spcnt, P.apcnt[0], P.apcnt[1]};
+	for (const int* c : counts) {
+		std::vector<int> n(NL);
+		FG_CUDA(cudaMemcpy(n.data(), c + (size_t)s * NL, NL * sizeof(int), cudaMemcpyDeviceToHost));
+		for (int v : n)
+			if (v) throw Error(-15, "restoring needs an empty surface (a partition list is not empty)");
+	}
+	const int nact = (int)img.active.size();
+	int top = 0;
+	FG_CUDA(cudaMemcpy(&top, P.counters + CNT_FREE_TOP, sizeof(int), cudaMemcpyDeviceToHost));
+	if (nact > top) throw Error(-4, "brick pool too small for the restored surface");
+	// bricks from the top of the free stack, as activation takes them
+	std::vector<int> slots(nact), gps(nact);
+	if (nact)
+		FG_CUDA(cudaMemcpy(slots.data(), P.free_stack + (top - nact), nact * sizeof(int),
+		                   cudaMemcpyDeviceToHost));
+	for (int i = 0; i < nact; i++) {
+		gps[i] = g.pbase + img.active[i];
+		slot[img.active[i]] = slots[i];
+	}
+	const int ntop = top - nact;
+	FG_CUDA(cudaMemcpyAsync(P.counters + CNT_FREE_TOP, &ntop, sizeof(int), cudaMemcpyHostToDevice, st));
+	FG_CUDA(cudaMemcpyAsync(P.slot + g.pbase, slot.data(), g.np * sizeof(int), cudaMemcpyHostToDevice, st));
+	FG_CUDA(cudaMemcpyAsync(P.bg + g.pbase, img.bg.data(), g.np * sizeof(float), cudaMemcpyHostToDevice, st));
+	FG_CUDA(cudaMemcpyAsync(P.ppos + (size_t)g.pbase * NL, img.ppos.data(), (size_t)g.np * NL * sizeof(int),
+	                        cudaMemcpyHostToDevice, st));
+	std::vector<int> pcnt(NL);
+	for (int l = 0; l < NL; l++) {
+		pcnt[l] = (int)img.plist[l].size();
+		if (pcnt[l])
+			FG_CUDA(cudaMemcpyAsync(P.plist + (size_t)l * P.NP + g.pbase, img.plist[l].data(),
+			                        pcnt[l] * sizeof(int), cudaMemcpyHostToDevice, st));
+	}
+	FG_CUDA(cudaMemcpyAsync(P.pcnt + (size_t)s * NL, pcnt.data(), NL * sizeof(int), cudaMemcpyHostToDevice, st));
+	if (nact) {
+		const size_t bv = (size_t)P.BV;
+		int* dslots = dev_alloc<int>(nact, st);
+		int* dgps = dev_alloc<int>(nact, st);
+		float* dphi = dev_alloc<float>(nact * bv, st);
+		uint16_t* dlkp = dev_alloc<uint16_t>(nact * bv, st);
+		uint16_t* dlst = dev_alloc<uint16_t>(nact * bv * NL, st);
+		int* dlcnt = dev_alloc<int>((size_t)nact * NL, st);
+		FG_CUDA(cudaMemcpyAsync(dslots, slots.data(), nact * sizeof(int), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dgps, gps.data(), nact * sizeof(int), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dphi, img.phi.data(), nact * bv * sizeof(float), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dlkp, img.lkp.data(), nact * bv * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dlst, img.lst.data(), nact * bv * NL * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+		FG_CUDA(cudaMemcpyAsync(dlcnt, img.lcnt.data(), (size_t)nact * NL * sizeof(int), cudaMemcpyHostToDevice, st));
+		const unsigned blocks = (unsigned)std::min(nact, 148 * 8);
+#define FG_CASE(ll) \
+	if (L == ll) FG_RUN("k_scatter_bricks", st, k_scatter_bricks<ll><<<blocks, 256, 0, st>>>(P, dslots, dgps, nact, dphi, dlkp, dlst, dlcnt););
+		FG_CASE(1) FG_CASE(2) FG_CASE(3) FG_CASE(4)
+#undef FG_CASE
+		FG_CUDA(cudaGetLastError());
+		for (void* q : {(void*)dslots, (void*)dgps, (void*)dphi, (void*)dlkp, (void*)dlst, (void*)dlcnt})
+			FG_CUDA(cudaFreeAsync(q, st));
+	}
 	FG_CUDA(cudaStreamSynchronize(st));
 	eng.check_errors();
 }

@@ -27,6 +27,9 @@ struct SurfaceImage {
 void export_image(EngineBase& eng, int s, SurfaceImage& img);
 /// Writes img into a newly created single-surface engine of the same geometry.
 void import_image(EngineBase& eng, const SurfaceImage& img);
+/// Writes img into surface s of any pool, which must be empty (no active partition, every list
+/// empty) and of the same geometry; its bricks come from the pool's free stack.
+void restore_image(EngineBase& eng, int s, const SurfaceImage& img);
 
 /// The surface file of img (geometry g, partition size csz) appended to out.
 void write_surface_file(const SurfaceImage& img, const SurfGeom& g, int D, int L, const int* csz,

@@ -239,6 +239,15 @@ FG_API int fg_batch_polys_invalidate(fg_batch* b);
 /* Per-surface queries, as the fg_surface ones. */
 FG_API int fg_batch_snapshot(fg_batch* b, size_t surface, float* dst, size_t n);
 FG_API int fg_batch_dump(fg_batch* b, size_t surface, uint32_t* out, size_t cap, size_t* n);
+/* Surface::save (include/Felt/Surface.hpp:180-183) of one surface of a batch: the same file as
+ * fg_save writes (min(n, cap) bytes into buf, which may be NULL; the full length in *n). */
+FG_API int fg_batch_save(fg_batch* b, size_t surface, uint8_t* buf, size_t cap, size_t* n);
+/* Surface::load (include/Felt/Surface.hpp:185-196) into one surface of a batch, which must be
+ * empty (never seeded, or with no active partition and every list empty; else FG_ERR_STATE) and
+ * have the file's grid and partition size: a checkpoint taken with fg_batch_save or fg_save
+ * comes back into any batch, e.g. a served surface set aside and later resumed. Its bricks come
+ * from the batch's pool (FG_ERR_POOL when too few are free). */
+FG_API int fg_batch_restore(fg_batch* b, size_t surface, const uint8_t* data, size_t n);
 FG_API int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float* dirs,
                          size_t n, float* hits);
 FG_API int fg_batch_polys_partition(fg_batch* b, size_t surface, size_t part, float* vtx,

@@ -121,3 +121,83 @@ def test_malformed_and_oversized_files_are_rejected():
         fb.Surface.load(data, brick_capacity=1)
     assert ei.value.code == -4
     assert np.array_equal(t.snapshot(), g.snapshot())
+
+
+BATCH_SIZES = [(32, 32, 32), (40, 24, 32), (24, 24, 24)]
+BATCH_CENTRES = [(0, 0, 0), (3, -2, 1), (-1, 1, 0)]
+BATCH_SPEEDS = [dict(c=-1.0), dict(c=-0.7, n=0.3, seed=4), dict(a=-0.3, c=-0.5)]
+
+
+def _batch_and_oracles(steps):
+    fb = _fb()
+    part, L = (8, 8, 8), 2
+    b = fb.Batch(BATCH_SIZES, part, L)
+    b.seed(BATCH_CENTRES)
+    os_ = [O.Surface(sz, part, L) for sz in BATCH_SIZES]
+    for o, c in zip(os_, BATCH_CENTRES):
+        o.seed(c)
+    for _ in range(steps):
+        b.update(BATCH_SPEEDS)
+        for o, sp in zip(os_, BATCH_SPEEDS):
+            o.update(**sp)
+    return b, os_
+
+
+def test_batch_save_equals_oracle_file():
+    b, os_ = _batch_and_oracles(5)
+    for i, o in enumerate(os_):
+        assert b.save(i) == o.save(), f"surface {i}"
+
+
+def test_batch_restore_then_update():
+    """Checkpoint every surface of a batch, restore the files into a batch that was never
+    seeded (in another order, so each surface lands in bricks that another surface's data
+    held in the first batch), and advance both batches: every surface stays equal to its
+    oracle."""
+    fb = _fb()
+    b, os_ = _batch_and_oracles(4)
+    files = [b.save(i) for i in range(3)]
+    c = fb.Batch(BATCH_SIZES, (8, 8, 8), 2)
+    for i in (2, 0, 1):
+        c.restore(i, files[i])
+    for i, o in enumerate(os_):
+        assert np.array_equal(c.snapshot(i), o.snapshot())
+        assert c.save(i) == files[i]
+    for _ in range(4):
+        b.update(BATCH_SPEEDS)
+        c.update(BATCH_SPEEDS)
+        for o, sp in zip(os_, BATCH_SPEEDS):
+            o.update(**sp)
+    for i, o in enumerate(os_):
+        assert np.array_equal(c.snapshot(i), o.snapshot()), f"surface {i}"
+        assert c.save(i) == b.save(i) == o.save(), f"surface {i}"
+
+
+def test_batch_restore_from_a_single_surface_file():
+    """A file written by a single surface (or the oracle) restores into a batch position of
+    the same grid, next to surfaces that keep running."""
+    fb = _fb()
+    part, L = (8, 8, 8), 2
+    o = O.Surface((24, 24, 24), part, L)
+    o.seed((2, 2, -3))
+    for _ in range(5):
+        o.update(c=-1.0)
+    b = fb.Batch([(32, 32, 32), (24, 24, 24)], part, L)
+    b.seed([(0, 0, 0), (0, 0, 0)])
+    with pytest.raises(fb.FeltError):  # surface 1 is seeded: not empty
+        b.restore(1, o.save())
+    with pytest.raises(fb.FeltError):  # surface 0 has another grid size
+        b.restore(0, o.save())
+    e = fb.Batch([(32, 32, 32), (24, 24, 24)], part, L)
+    e.restore(1, fb.Surface.load(o.save()).save())
+    with pytest.raises(fb.FeltError):  # restored: no longer empty
+        e.restore(1, o.save())
+    for _ in range(3):
+        e.update([dict(c=-1.0), dict(c=-1.0)])
+        o.update(c=-1.0)
+    assert np.array_equal(e.snapshot(1), o.snapshot())
+    assert not np.any(e.snapshot(0) < 3)  # the never-seeded surface stays background
+    with pytest.raises(fb.FeltError):  # a truncated file
+        e.restore(0, b.save(0)[:-5])
+    e.restore(0, b.save(0))
+    assert np.array_equal(e.snapshot(0), b.snapshot(0))
