@@ -14,7 +14,7 @@ T* dalloc(size_t n, std::vector<void*>& owned)
 {
 	void* p = nullptr;
 	if (n == 0) n = 1;
-	cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+	cudaError_t e = locked_malloc(&p, n * sizeof(T));
 	if (e != cudaSuccess)
 		throw Error(-3, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
 	owned.push_back(p);
@@ -52,6 +52,12 @@ int sm_count()
 }
 
 }  // namespace
+
+std::recursive_mutex& device_lock()
+{
+	static std::recursive_mutex m;
+	return m;
+}
 
 template <int D, int L>
 class Engine final : public EngineBase {
@@ -278,10 +284,10 @@ public:
 		cudaStreamSynchronize(st_);
 		for (cudaGraphExec_t& ex : iter_exec_)
 			if (ex) cudaGraphExecDestroy(ex);
-		for (void* p : owned_) cudaFree(p);
-		if (d_lpos_) cudaFree(d_lpos_);
-		if (d_lval_) cudaFree(d_lval_);
-		if (d_lcount_) cudaFree(d_lcount_);
+		for (void* p : owned_) locked_free(p);
+		if (d_lpos_) locked_free(d_lpos_);
+		if (d_lval_) locked_free(d_lval_);
+		if (d_lcount_) locked_free(d_lcount_);
 	}
 
 	int dims() const override { return D; }
@@ -315,14 +321,14 @@ public:
 	void seed_all(const int* centres) override
 	{
 		int* d = nullptr;
-		FG_CUDA(cudaMalloc(&d, (size_t)P_.S * D * sizeof(int)));
+		FG_CUDA(locked_malloc(&d, (size_t)P_.S * D * sizeof(int)));
 		cudaError_t e = cudaMemcpyAsync(d, centres, (size_t)P_.S * D * sizeof(int),
 		                                cudaMemcpyHostToDevice, st_);
 		if (e == cudaSuccess) {
 			FG_RUN("k_seed_all", st_, k_seed_all<D, L><<<(P_.S + 63) / 64, 64, 0, st_>>>(P_, d););
 			e = cudaStreamSynchronize(st_);
 		}
-		cudaFree(d);
+		locked_free(d);
 		if (e != cudaSuccess) throw Error(-2, cudaGetErrorString(e));
 		check_errors();
 	}
@@ -430,6 +436,7 @@ public:
 		cudaGraphExec_t& ex = iter_exec_[cur];
 		if (!ex) {
 			cudaGraph_t gph = nullptr;
+			std::lock_guard<std::recursive_mutex> lock(device_lock());
 			if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
 				cudaGetLastError();
 				graphs_ok_ = false;
@@ -450,8 +457,9 @@ public:
 				if (gph) cudaGraphDestroy(gph);
 				ex = nullptr;
 				cudaGetLastError();
+				// nothing captured has run: the caller launches the iteration's kernels one by
+				// one, and a real fault shows there
 				graphs_ok_ = false;
-				if (threw) throw Error(-2, "capture of the update iteration failed");
 				return false;
 			}
 			cudaGraphDestroy(gph);
@@ -636,13 +644,13 @@ public:
 		if (n <= lcap_ && d_lpos_) return;
 		int cap = std::max(n, 1024);
 		cudaStreamSynchronize(st_);
-		if (d_lpos_) cudaFree(d_lpos_);
-		if (d_lval_) cudaFree(d_lval_);
+		if (d_lpos_) locked_free(d_lpos_);
+		if (d_lval_) locked_free(d_lval_);
 		d_lpos_ = nullptr;
 		d_lval_ = nullptr;
-		FG_CUDA(cudaMalloc(&d_lpos_, (size_t)cap * D * sizeof(int)));
-		FG_CUDA(cudaMalloc(&d_lval_, (size_t)cap * sizeof(float)));
-		if (!d_lcount_) FG_CUDA(cudaMalloc(&d_lcount_, sizeof(int)));
+		FG_CUDA(locked_malloc(&d_lpos_, (size_t)cap * D * sizeof(int)));
+		FG_CUDA(locked_malloc(&d_lval_, (size_t)cap * sizeof(float)));
+		if (!d_lcount_) FG_CUDA(locked_malloc(&d_lcount_, sizeof(int)));
 		lcap_ = cap;
 	}
 
@@ -656,7 +664,7 @@ public:
 		float* out = dst;
 		float* tmp = nullptr;
 		if (!dst_device) {
-			FG_CUDA(cudaMalloc(&tmp, tot * sizeof(float)));
+			FG_CUDA(locked_malloc(&tmp, tot * sizeof(float)));
 			out = tmp;
 		}
 		FG_RUN("k_snapshot", st_, k_snapshot<D, L><<<grid_for(tot), 256, 0, st_>>>(P_, s, out, tot););
@@ -664,7 +672,7 @@ public:
 		if (e == cudaSuccess && tmp)
 			e = cudaMemcpyAsync(dst, tmp, tot * sizeof(float), cudaMemcpyDeviceToHost, st_);
 		if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
-		if (tmp) cudaFree(tmp);
+		if (tmp) locked_free(tmp);
 		if (e != cudaSuccess) throw Error(-2, cudaGetErrorString(e));
 	}
 

@@ -8,6 +8,7 @@
 
 #include <array>
 #include <cstdint>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -119,6 +120,25 @@ struct ProfEntry {
 	long long launches;
 };
 std::vector<ProfEntry> prof_read();
+
+/// Graph captures and the library's calls that synchronise the whole device (cudaMalloc,
+/// cudaFree, cudaDeviceSynchronize) hold this lock: made from another thread while a stream is
+/// being captured, such a call can invalidate the capture (engines of one process run in
+/// several host threads when a server drives several batches).
+std::recursive_mutex& device_lock();
+
+template <class T>
+inline cudaError_t locked_malloc(T** p, size_t bytes)
+{
+	std::lock_guard<std::recursive_mutex> g(device_lock());
+	return cudaMalloc((void**)p, bytes);
+}
+
+inline cudaError_t locked_free(void* p)
+{
+	std::lock_guard<std::recursive_mutex> g(device_lock());
+	return cudaFree(p);
+}
 void prof_reset();
 
 #define FG_RUN(name, st, ...)            \

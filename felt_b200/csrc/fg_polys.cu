@@ -623,7 +623,7 @@ public:
 		const Dev& P = eng.dev();
 		auto al = [&](size_t bytes) {
 			void* p = nullptr;
-			FG_CUDA(cudaMalloc(&p, bytes ? bytes : 1));
+			FG_CUDA(locked_malloc(&p, bytes ? bytes : 1));
 			owned_.push_back(p);
 			return p;
 		};
@@ -673,6 +673,7 @@ public:
 		if (smem_ > 48 * 1024)
 			FG_CUDA(cudaFuncSetAttribute(k_polys_march<D, L>,
 			                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+		std::lock_guard<std::recursive_mutex> lock(device_lock());
 		FG_CUDA(cudaDeviceSynchronize());
 	}
 
@@ -685,7 +686,7 @@ public:
 		if (spare_s_) cudaFreeAsync(spare_s_, st);
 		if (stage_) cudaFreeAsync(stage_, st);
 		cudaStreamSynchronize(st);
-		for (void* p : owned_) cudaFree(p);
+		for (void* p : owned_) locked_free(p);
 	}
 
 	void notify() override
