@@ -13,6 +13,16 @@
 namespace fg {
 
 constexpr uint16_t NUL16 = 0xFFFFu;
+
+/// Programmatic dependent launch. The update's kernels are launched so that each may start
+/// while the previous kernel of its stream drains; every such kernel calls this first: it
+/// waits until the previous kernel has finished and its writes are visible (no wait for a
+/// kernel launched the ordinary way), then lets the next kernel begin its launch.
+__device__ __forceinline__ void pdl_enter()
+{
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 constexpr unsigned long long NOCLAIM = ~0ull;
 
 // error bits (Dev::err[0])

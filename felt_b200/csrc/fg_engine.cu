@@ -33,6 +33,34 @@ __global__ void k_fill_float(float* p, long long n, float v)
 	     i += (long long)gridDim.x * blockDim.x)
 		p[i] = v;
 }
+/// Start of the device-side convergence loop: the first flush and expansion count as iteration
+/// 1; the loop body runs while a layer changed.
+__global__ void k_loop_init(const int* changed, int* iters, cudaGraphConditionalHandle loop)
+{
+	pdl_enter();
+	if (threadIdx.x == 0) {
+		*iters = 1;
+		cudaGraphSetConditional(loop, *changed ? 1u : 0u);
+	}
+}
+
+/// End of one iteration of the device-side convergence loop: counts it and goes on while a
+/// layer changed and the count is not a multiple of cap (where the host looks for surfaces to
+/// stop, as the host loop does), so the loop ends after at most cap - 1 iterations. Sets both
+/// handles (the loop's and the one of the body's second iteration) where two are given.
+__global__ void k_loop_test(const int* changed, int* iters, int cap, cudaGraphConditionalHandle a,
+                            cudaGraphConditionalHandle b, int both)
+{
+	pdl_enter();
+	if (threadIdx.x == 0) {
+		const int it = *iters + 1;
+		*iters = it;
+		const unsigned go = (*changed != 0 && it % cap != 0) ? 1u : 0u;
+		cudaGraphSetConditional(a, go);
+		if (both) cudaGraphSetConditional(b, go);
+	}
+}
+
 __global__ void k_iota_rev(int* p, int n)
 {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -221,6 +249,7 @@ public:
 		FG_CUDA(cudaMemsetAsync(P.kstat, 0, KS_N * sizeof(unsigned long long), st_));
 		acc_ = dalloc<unsigned long long>(1, o);
 		zcount_ = dalloc<unsigned long long>(1, o);
+		d_iters_ = dalloc<int>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
 
 		fill(P.slot, NP, -1);
@@ -284,6 +313,7 @@ public:
 		cudaStreamSynchronize(st_);
 		for (cudaGraphExec_t& ex : iter_exec_)
 			if (ex) cudaGraphExecDestroy(ex);
+		if (loop_exec_) cudaGraphExecDestroy(loop_exec_);
 		for (void* p : owned_) locked_free(p);
 		if (d_lpos_) locked_free(d_lpos_);
 		if (d_lval_) locked_free(d_lval_);
@@ -342,9 +372,9 @@ public:
 		bool any_curv = false;
 		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
 		if (any_curv && smem_halo_)
-			FG_RUN("k_delta_smem", st_, k_delta_smem<D, L><<<sm_count() * 8, 128, smem_halo_, st_>>>(P_, d_speeds_););
+			FG_RUN("k_delta_smem", st_, launch_pdl((k_delta_smem<D, L>), sm_count() * 8, 128, smem_halo_, st_, P_, d_speeds_););
 		else
-			FG_RUN("k_delta_builtin", st_, k_delta_builtin<D, L><<<warp_grid_, 256, 0, st_>>>(P_, d_speeds_););
+			FG_RUN("k_delta_builtin", st_, launch_pdl((k_delta_builtin<D, L>), warp_grid_, 256, 0, st_, P_, d_speeds_););
 		update_finish_global();
 	}
 
@@ -386,9 +416,20 @@ public:
 		retire();
 		status_dirty_ = true;
 		buf_dirty_[B] = true;
-		int changed = read_changed();
+		int changed = 0;
 		int iters = 1;
 		int cur = B, oth = A;
+		if (!local && run_device_loop(changed, iters)) {
+			// iterations alternate the buffers; each global one clears the buffer it consumed
+			if ((iters - 1) % 2) std::swap(cur, oth);
+			if (iters > 1) {
+				buf_dirty_[cur] = true;
+				buf_dirty_[oth] = false;
+			}
+			if (changed) freeze_oscillating(cur);  // stopped at a multiple of kMaxIterations
+		} else {
+			changed = read_changed();
+		}
 		while (changed) {
 			if (local && buf_dirty_[oth]) clear_buffer(oth);
 			if (local || !replay_iteration(cur, oth)) iteration(local, cur, oth);
@@ -467,6 +508,115 @@ public:
 		}
 		FG_CUDA(cudaGraphLaunch(ex, st_));
 		add_launches(iter_launches_[cur]);
+		return true;
+	}
+
+	/// The global update's convergence loop on the device: one graph whose while node runs two
+	/// iterations per pass (buffer B then A, the second under an if node), each followed by a
+	/// test kernel that counts it and sets the conditions. Replaces a host read-back per
+	/// iteration with one per update. Returns false (the host loop runs instead) while
+	/// per-launch profiling is on or where the graph cannot be built; otherwise sets changed
+	/// and iters as the host loop leaves them when it stops at a multiple of kMaxIterations or
+	/// runs out of changes.
+	bool run_device_loop(int& changed, int& iters)
+	{
+		if (!loop_ok_ || !graphs_ok_ || prof_on()) return false;
+		if (!loop_exec_ && !build_device_loop()) return false;
+		FG_CUDA(cudaGraphLaunch(loop_exec_, st_));
+		int out[2] = {0, 0};
+		FG_CUDA(cudaMemcpyAsync(&out[0], d_iters_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaMemcpyAsync(&out[1], P_.changed, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		iters = out[0];
+		changed = out[1];
+		const int n = iters - 1;  // iterations run: n / 2 full passes, one more if n is odd
+		add_launches(1 + (long long)(n / 2) * (loop_launches_[0] + loop_launches_[1]) +
+		             (n % 2) * loop_launches_[0]);
+		return true;
+	}
+
+	bool build_device_loop()
+	{
+		std::lock_guard<std::recursive_mutex> lock(device_lock());
+		cudaGraph_t g = nullptr;
+		bool ok = false;
+		const long long l0 = launch_count();
+		// capturing the iterations runs their host side, which marks the grids it clears as
+		// clean; nothing captured has run yet
+		const bool sd = status_dirty_, bd0 = buf_dirty_[0], bd1 = buf_dirty_[1];
+		try {
+			ok = build_device_loop_into(g);
+		} catch (...) {
+			ok = false;
+		}
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		if (cudaStreamIsCapturing(st_, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+			cudaGraph_t dropped = nullptr;
+			cudaStreamEndCapture(st_, &dropped);
+			ok = false;
+		}
+		add_launches(-(launch_count() - l0));  // counted when they run
+		if (ok && cudaGraphInstantiate(&loop_exec_, g, 0) != cudaSuccess) {
+			loop_exec_ = nullptr;
+			ok = false;
+		}
+		if (g) cudaGraphDestroy(g);
+		cudaGetLastError();
+		if (!ok) loop_ok_ = false;
+		status_dirty_ = sd;
+		buf_dirty_[0] = bd0;
+		buf_dirty_[1] = bd1;
+		return ok;
+	}
+
+	/// Adds the node of a conditional of the given kind after the last node captured on the
+	/// stream, ends the capture and returns the conditional's body graph.
+	cudaGraph_t end_capture_with_conditional(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType kind)
+	{
+		cudaStreamCaptureStatus cs;
+		cudaGraph_t cg = nullptr;
+		const cudaGraphNode_t* deps = nullptr;
+		size_t nd = 0;
+		FG_CUDA(cudaStreamGetCaptureInfo(st_, &cs, nullptr, &cg, &deps, &nd));
+		std::vector<cudaGraphNode_t> last(deps, deps + nd);
+		cudaGraph_t done = nullptr;
+		FG_CUDA(cudaStreamEndCapture(st_, &done));
+		cudaGraphNodeParams p = {};
+		p.type = cudaGraphNodeTypeConditional;
+		p.conditional.handle = h;
+		p.conditional.type = kind;
+		p.conditional.size = 1;
+		cudaGraphNode_t node;
+		FG_CUDA(cudaGraphAddNode(&node, done, last.data(), last.size(), &p));
+		return p.conditional.phGraph_out[0];
+	}
+
+	bool build_device_loop_into(cudaGraph_t& g)
+	{
+		const int B = 1, A = 0;
+		const auto mode = cudaStreamCaptureModeThreadLocal;
+		FG_CUDA(cudaGraphCreate(&g, 0));
+		cudaGraphConditionalHandle hloop, hsecond;
+		FG_CUDA(cudaGraphConditionalHandleCreate(&hloop, g, 0, cudaGraphCondAssignDefault));
+		FG_CUDA(cudaStreamBeginCaptureToGraph(st_, g, nullptr, nullptr, 0, mode));
+		FG_RUN("k_loop_init", st_, launch_pdl((k_loop_init), 1, 32, 0, st_, P_.changed, d_iters_, hloop););
+		const cudaGraph_t body = end_capture_with_conditional(hloop, cudaGraphCondTypeWhile);
+		FG_CUDA(cudaGraphConditionalHandleCreate(&hsecond, body, 0, cudaGraphCondAssignDefault));
+		// first iteration of a pass: buffer B consumed, A recorded
+		FG_CUDA(cudaStreamBeginCaptureToGraph(st_, body, nullptr, nullptr, 0, mode));
+		long long l0 = launch_count();
+		iteration(false, B, A);
+		FG_RUN("k_loop_test", st_, launch_pdl((k_loop_test), 1, 32, 0, st_, P_.changed, d_iters_, kMaxIterations, hsecond, hloop, 1););
+		loop_launches_[0] = launch_count() - l0;
+		const cudaGraph_t second = end_capture_with_conditional(hsecond, cudaGraphCondTypeIf);
+		// second iteration: A consumed, B recorded
+		FG_CUDA(cudaStreamBeginCaptureToGraph(st_, second, nullptr, nullptr, 0, mode));
+		l0 = launch_count();
+		iteration(false, A, B);
+		FG_RUN("k_loop_test", st_, launch_pdl((k_loop_test), 1, 32, 0, st_, P_.changed, d_iters_, kMaxIterations, hloop, hloop, 0););
+		loop_launches_[1] = launch_count() - l0;
+		cudaGraph_t done = nullptr;
+		FG_CUDA(cudaStreamEndCapture(st_, &done));
 		return true;
 	}
 
@@ -630,7 +780,7 @@ public:
 		count_band();
 		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
 		// over the affected lists (update_distance(plookup = affected, buffer))
-		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
+		FG_RUN("k_scan_counts", st_, launch_pdl((k_scan_counts), 1, 1024, 0, st_, P_.ndp, 1, 0, 0, P_.S, P_.woff, P_.sfrozen););
 		const ListView aff{P_.aplist[A], P_.apcnt[A], P_.alst[A], P_.acnt[A]};
 		zero_apply(aff, P_.dlcnt, B);
 		defer_compact(P_.woff, P_.aplist[A], L, B);
@@ -890,7 +1040,7 @@ private:
 
 	void scan(const int* cnt, int l, int mode)
 	{
-		FG_RUN("k_scan_counts", st_, k_scan_counts<<<1, 1024, 0, st_>>>(cnt, NL, l, mode, P_.S, P_.woff, P_.sfrozen););
+		FG_RUN("k_scan_counts", st_, launch_pdl((k_scan_counts), 1, 1024, 0, st_, cnt, NL, l, mode, P_.S, P_.woff, P_.sfrozen););
 	}
 
 	/// update_start (Surface.hpp:393-399): resets of the status and affected grids left by the
@@ -907,13 +1057,13 @@ private:
 	{
 		dim3 grid(1, P_.S * NL);
 		if (grid.y > 65535) throw Error(-1, "too many surfaces for one pool");
-		FG_RUN("k_copy_plists", st_, k_copy_plists<<<grid, 256, 0, st_>>>(P_, NL););
+		FG_RUN("k_copy_plists", st_, launch_pdl((k_copy_plists), grid, 256, 0, st_, P_, NL););
 	}
 
 	void count_band()
 	{
 		scan(P_.pcnt, 0, 2);
-		FG_RUN("k_band_size", st_, k_band_size<L><<<warp_grid_, 256, 0, st_>>>(P_, acc_););
+		FG_RUN("k_band_size", st_, launch_pdl((k_band_size<L>), warp_grid_, 256, 0, st_, P_, acc_););
 	}
 
 	/// The 2L layer passes of update_distance (Surface.hpp:989-1125). The pass lists do not
@@ -921,12 +1071,12 @@ private:
 	/// entry offsets of every layer up front.
 	void distance_passes(const ListView& lv, int b)
 	{
-		FG_RUN("k_scan_layers", st_, k_scan_layers<<<1, 1024, 0, st_>>>(lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
+		FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
 		for (int k = -1; k >= -L; k--) layer_pass(lv, k, -1.0f, b);
 		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
 		const CompactArgs ca = take_compact();
 		if (ca.nblocks)
-			FG_RUN("k_compact", st_, k_compact<L><<<ca.nblocks, 256, 0, st_>>>(P_, ca););
+			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca););
 	}
 
 	/// A pass's compaction waits to ride on the next first-pass launch (k_dist1).
@@ -934,7 +1084,7 @@ private:
 	{
 		const CompactArgs stale = take_compact();  // none is left behind on the normal path
 		if (stale.nblocks)
-			FG_RUN("k_compact", st_, k_compact<L><<<stale.nblocks, 256, 0, st_>>>(P_, stale););
+			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), stale.nblocks, 256, 0, st_, P_, stale););
 		pending_ = CompactArgs{P_.S, woff, plist, li, b};
 	}
 	CompactArgs take_compact()
@@ -948,11 +1098,11 @@ private:
 	{
 		const int* woff = P_.woffl + (size_t)(k + L) * (P_.S + 1);
 		const CompactArgs ca = take_compact();
-		FG_RUN("k_dist1", st_, k_dist1<D, L><<<warp_grid_ + ca.nblocks, 256, 0, st_>>>(P_, woff, lv, k, side, dist_split_, ca););
+		FG_RUN("k_dist1", st_, launch_pdl((k_dist1<D, L>), warp_grid_ + ca.nblocks, 256, 0, st_, P_, woff, lv, k, side, dist_split_, ca););
 		if (block_passes_)
-			FG_RUN("k_dist2", st_, k_dist2<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
+			FG_RUN("k_dist2", st_, launch_pdl((k_dist2<D, L>), warp_grid_, 256, 0, st_, P_, woff, lv, k, b););
 		else
-			FG_RUN("k_dist2", st_, k_dist2_warp<D, L><<<warp_grid_, 256, 0, st_>>>(P_, woff, lv, k, b););
+			FG_RUN("k_dist2", st_, launch_pdl((k_dist2_warp<D, L>), warp_grid_, 256, 0, st_, P_, woff, lv, k, b););
 		defer_compact(woff, lv.plist, k + L, b);
 	}
 
@@ -960,18 +1110,18 @@ private:
 	void zero_apply(const ListView& lv, const int* ncount, int b)
 	{
 		if (block_passes_)
-			FG_RUN("k_zero_apply", st_, k_zero_apply<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, ncount, b););
+			FG_RUN("k_zero_apply", st_, launch_pdl((k_zero_apply<D, L>), warp_grid_, 256, 0, st_, P_, lv, ncount, b););
 		else
-			FG_RUN("k_zero_apply", st_, k_zero_apply_warp<D, L><<<warp_grid_, 256, 0, st_>>>(P_, lv, ncount, b););
+			FG_RUN("k_zero_apply", st_, launch_pdl((k_zero_apply_warp<D, L>), warp_grid_, 256, 0, st_, P_, lv, ncount, b););
 	}
 
 	void flush()
 	{
 		if (smem_flush_)
-			FG_RUN("k_flush_smem", st_, k_flush_smem<D, L><<<sm_count() * 8, 128, smem_flush_, st_>>>(P_););
+			FG_RUN("k_flush_smem", st_, launch_pdl((k_flush_smem<D, L>), sm_count() * 8, 128, smem_flush_, st_, P_););
 		else
-			FG_RUN("k_flush_leaf", st_, k_flush_leaf<D, L><<<grid_for(P_.NP), 128, 0, st_>>>(P_););
-		FG_RUN("k_flush_plist", st_, k_flush_plist<L><<<P_.S * NL, 256, 0, st_>>>(P_););
+			FG_RUN("k_flush_leaf", st_, launch_pdl((k_flush_leaf<D, L>), grid_for(P_.NP), 128, 0, st_, P_););
+		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 256, 0, st_, P_););
 	}
 
 	void expand()
@@ -979,23 +1129,23 @@ private:
 		scan(P_.spcnt, 0, 1);
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_CAND, 0, sizeof(int), st_));
-		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0););
-		FG_RUN("k_activate", st_, k_activate<L><<<sm_count() * 4, 256, 0, st_>>>(P_););
-		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 1););
-		FG_RUN("k_expand_gen", st_, k_expand_gen<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 2););
-		FG_RUN("k_expand_append", st_, k_expand_append<L><<<sm_count() * 4, 256, smem_sort_, st_>>>(P_););
-		FG_RUN("k_expand_plist", st_, k_expand_plist<L><<<P_.S, 256, 0, st_>>>(P_););
+		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 0););
+		FG_RUN("k_activate", st_, launch_pdl((k_activate<L>), sm_count() * 4, 256, 0, st_, P_););
+		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 1););
+		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 2););
+		FG_RUN("k_expand_append", st_, launch_pdl((k_expand_append<L>), sm_count() * 4, 256, smem_sort_, st_, P_););
+		FG_RUN("k_expand_plist", st_, launch_pdl((k_expand_plist<L>), P_.S, 256, 0, st_, P_););
 	}
 
 	void retire()
 	{
-		FG_RUN("k_retire", st_, k_retire<<<grid_for(P_.nslots), 256, 0, st_>>>(P_););
+		FG_RUN("k_retire", st_, launch_pdl((k_retire), grid_for(P_.nslots), 256, 0, st_, P_););
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_RETIRE, 0, sizeof(int), st_));
 	}
 
 	void clear_status()
 	{
-		FG_RUN("k_clear_status", st_, k_clear_status<L><<<warp_grid_, 256, 0, st_>>>(P_););
+		FG_RUN("k_clear_status", st_, launch_pdl((k_clear_status<L>), warp_grid_, 256, 0, st_, P_););
 		FG_CUDA(cudaMemsetAsync(P_.spcnt, 0, (size_t)P_.S * NL * sizeof(int), st_));
 		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_SUNION, 0, sizeof(int), st_));
 		status_dirty_ = false;
@@ -1004,7 +1154,7 @@ private:
 	void clear_buffer(int b)
 	{
 		scan(P_.apcnt[b], 0, 2);
-		FG_RUN("k_clear_buffer", st_, k_clear_buffer<L><<<warp_grid_, 256, 0, st_>>>(P_, b););
+		FG_RUN("k_clear_buffer", st_, launch_pdl((k_clear_buffer<L>), warp_grid_, 256, 0, st_, P_, b););
 		FG_CUDA(cudaMemsetAsync(P_.apcnt[b], 0, (size_t)P_.S * NL * sizeof(int), st_));
 		buf_dirty_[b] = false;
 	}
@@ -1025,6 +1175,7 @@ private:
 	std::vector<void*> owned_;
 	unsigned long long* acc_ = nullptr;     // node updates of all global updates so far
 	unsigned long long* zcount_ = nullptr;  // zero-layer leaf count of a bounded update
+	int* d_iters_ = nullptr;                 // iteration count of the device-side loop
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;
@@ -1038,6 +1189,9 @@ private:
 	cudaGraphExec_t iter_exec_[2] = {nullptr, nullptr};  // global iteration, by buffer parity
 	long long iter_launches_[2] = {0, 0};
 	bool graphs_ok_ = true;
+	cudaGraphExec_t loop_exec_ = nullptr;  // the global convergence loop (conditional nodes)
+	long long loop_launches_[2] = {0, 0};  // kernels of the loop's first and second iteration
+	bool loop_ok_ = true;
 	CompactArgs pending_{0, nullptr, nullptr, 0, 0};  // compaction riding on the next k_dist1
 	// whole blocks (not warps) per partition entry in the record-keeping passes: pays off when
 	// a brick holds thousands of leaves, costs idle threads when it holds a few hundred

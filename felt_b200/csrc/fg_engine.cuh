@@ -11,6 +11,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "fg_dev.cuh"
@@ -120,6 +121,26 @@ struct ProfEntry {
 	long long launches;
 };
 std::vector<ProfEntry> prof_read();
+
+/// Launches a kernel that begins with pdl_enter() with programmatic stream serialisation: its
+/// launch overlaps the end of the previous kernel on the stream instead of following it.
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                Args&&... args)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+	if (e != cudaSuccess) throw Error(-2, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
 
 /// Graph captures and the library's calls that synchronise the whole device (cudaMalloc,
 /// cudaFree, cudaDeviceSynchronize) hold this lock: made from another thread while a stream is

@@ -60,6 +60,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff,
                                      const int* frozen)
 {
+	pdl_enter();
 	__shared__ int carry;
 	if (threadIdx.x == 0) {
 		carry = 0;
@@ -89,6 +90,7 @@ static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, in
 /// k_scan_counts mode 0 for every layer index at once: woffl[l*(S+1) + s].
 static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, const int* frozen)
 {
+	pdl_enter();
 	__shared__ int carry;
 	for (int l = 0; l < NL; l++) {
 		int* woff = woffl + (size_t)l * (S + 1);
@@ -252,6 +254,7 @@ __device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int f
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -334,6 +337,7 @@ __host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
 template <int D, int L>
 __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	extern __shared__ float hbox[];
 	const int total = P.woff[P.S];
@@ -370,6 +374,7 @@ __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const int* ncount, int b)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	__shared__ uint16_t cl[256];
 	__shared__ int ct[256];
@@ -411,6 +416,7 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, const int* ncount, int b)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -529,6 +535,7 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 template <int L>
 __global__ void __launch_bounds__(256) k_compact(Dev P, CompactArgs a)
 {
+	pdl_enter();
 	compact_surface<L>(P, a, blockIdx.x);
 }
 
@@ -545,6 +552,7 @@ template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
                                                float side, int split, CompactArgs ca)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	if ((int)blockIdx.x < ca.nblocks) {
 		compact_surface<L>(P, ca, blockIdx.x);
@@ -585,6 +593,7 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView 
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
 	__shared__ uint16_t cl[256];
@@ -629,6 +638,7 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView 
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, ListView lv, int k, int b)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
 	FG_WARP_LOOP(woff)
@@ -681,6 +691,7 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 template <int D, int L>
 __global__ void k_flush_leaf(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_SUNION];
 	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -775,6 +786,7 @@ __host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
 template <int D, int L>
 __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	constexpr uint16_t TAG = 0x8000u;
 	extern __shared__ __align__(16) unsigned char fsm[];
@@ -994,6 +1006,7 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 template <int L>
 __global__ void __launch_bounds__(256) k_flush_plist(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	constexpr int TILE = 2048;
 	__shared__ int slp[TILE];
@@ -1074,6 +1087,7 @@ __global__ void __launch_bounds__(256) k_flush_plist(Dev P)
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	// Modes 1 and 2 take the candidates that mode 0 recorded, one thread each, unless there
 	// were more than the buffer holds: then they walk the status lists like mode 0.
@@ -1189,6 +1203,7 @@ __device__ void brick_init(const Dev& P, int sl, float bgv, int tid, int nth)
 template <int L>
 __global__ void k_activate(Dev P)
 {
+	pdl_enter();
 	__shared__ int sl;
 	const int n = P.counters[CNT_ACT];
 	for (int q = blockIdx.x; q < n; q += gridDim.x) {
@@ -1227,6 +1242,7 @@ __global__ void k_activate(Dev P)
 template <int L>
 __global__ void k_expand_append(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	extern __shared__ unsigned long long sk[];
 	__shared__ int ns, n0, base0, base1;
@@ -1310,6 +1326,7 @@ __global__ void k_expand_append(Dev P)
 template <int L>
 __global__ void k_expand_plist(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int s = blockIdx.x;
 	if (s >= P.S) return;
@@ -1361,6 +1378,7 @@ __global__ void k_expand_plist(Dev P)
 template <int L>
 __global__ void k_clear_status(Dev P)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_SUNION];
 	const int lane = lane_id();
@@ -1386,6 +1404,7 @@ __global__ void k_clear_status(Dev P)
 template <int L>
 __global__ void k_clear_buffer(Dev P, int b)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -1413,6 +1432,7 @@ __global__ void k_clear_buffer(Dev P, int b)
 /// Returns the bricks of partitions deactivated in this iteration to the free pool.
 static __global__ void k_retire(Dev P)
 {
+	pdl_enter();
 	const int n = P.counters[CNT_RETIRE];
 	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
 		const int sl = P.q_retire[e];
@@ -1428,6 +1448,7 @@ static __global__ void k_retire(Dev P)
 /// the isogrid lists into the freshly reset delta lists). Grid y = s*NL + l.
 static __global__ void k_copy_plists(Dev P, int NL)
 {
+	pdl_enter();
 	const int s = blockIdx.y / NL, l = blockIdx.y % NL;
 	const SurfGeom& g = P.geom[s];
 	const int n = P.pcnt[s * NL + l];
@@ -1441,6 +1462,7 @@ static __global__ void k_copy_plists(Dev P, int NL)
 template <int L>
 __global__ void k_band_size(Dev P, unsigned long long* acc)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	unsigned long long local = 0;
 	FG_WARP_LOOP(P.woff)
