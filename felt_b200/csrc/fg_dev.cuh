@@ -253,12 +253,15 @@ __device__ __forceinline__ Vec<D> leaf_pos(const Dev& P, int gp, int leaf)
 // -------------------------------------------------------------------------------------------
 
 /// Mean curvature by difference of normals (NumericMixin.hpp:72-156). The fixed-size Eigen sum
-/// of the normal differences is unrolled by halving: x0 + (x1 + x2) in 3D.
-template <int D, class Get>
-__device__ float curv_g(const Get& get, const Vec<D>& pos)
+/// of the normal differences is unrolled by halving: x0 + (x1 + x2) in 3D. The position is a
+/// node (Vec<D>) or a real position (any float D-vector with operator[], read through
+/// interpolation by get); its coordinates step by +-1 in their own type, as the reference's
+/// template on the position type does.
+template <int D, class Get, class Pos>
+__device__ float curv_g(const Get& get, const Pos& pos)
 {
 	const float centre = get(pos);
-	Vec<D> dir = pos;
+	Pos dir = pos;
 	float nf[D], nb[D];
 #pragma unroll
 	for (int axis = 0; axis < D; axis++) {
@@ -268,7 +271,7 @@ __device__ float curv_g(const Get& get, const Vec<D>& pos)
 #pragma unroll
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
-			Vec<D> dn = dir;
+			Pos dn = dir;
 			dn[an] -= 1;
 			const float lo = get(dn);
 			dn[an] += 2;
@@ -287,7 +290,7 @@ __device__ float curv_g(const Get& get, const Vec<D>& pos)
 #pragma unroll
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
-			Vec<D> dn = dir;
+			Pos dn = dir;
 			dn[an] -= 1;
 			const float lo = get(dn);
 			dn[an] += 2;

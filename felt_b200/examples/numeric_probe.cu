@@ -1,6 +1,7 @@
 // The Numeric API from a __device__ speed functor: grad, gradF, gradB, gradC, gradE and
 // divergence (the reference's NumericMixin.hpp:165-355) evaluated at every zero-layer node during
-// an update(fn), the way a speed functor calls them. The functor records the values into its own
+// an update(fn), the way a speed functor calls them, and the same functions with curv and interp
+// at the real position node + (0.3, -0.2, 0.45). The functor records the values into its own
 // device buffer and returns a speed of 0, so the surface does not move; the program writes them
 // out for comparison with the CPU restatement of the reference.
 //
@@ -8,7 +9,8 @@
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -fmad=false -Iinclude \
 //        -Ifelt_b200/include felt_b200/examples/numeric_probe.cu -Lfelt_b200 -lfelt_gpu \
 //        -Xlinker -rpath,$PWD/felt_b200 -o numeric_probe
-// Run: ./numeric_probe out_file   (per grid node: 16 values and a flag, row-major, 32^3 nodes)
+// Run: ./numeric_probe out_file   (per grid node, row-major, 32^3 nodes: 16 values at the node,
+//      a flag, 18 values at the real position)
 #include <cstdio>
 #include <vector>
 
@@ -17,7 +19,7 @@
 using felt_gpu::DevVec;
 
 constexpr int N = 32;     // grid edge
-constexpr int VALS = 17;  // 5 gradients x 3, divergence, flag
+constexpr int VALS = 35;  // node: 5 gradients x 3, divergence, flag; real: the same, curv, interp
 
 /// delta = a * curv(pos) + c.
 struct CurvatureDrift {
@@ -43,6 +45,16 @@ struct Recorder {
 			for (int a = 0; a < 3; a++) o[k * 3 + a] = g[k][a];
 		o[15] = iso.divergence(p);
 		o[16] = 1.0f;
+		felt_gpu::DevVecF<3> q;
+		const float off[3] = {0.3f, -0.2f, 0.45f};
+		for (int a = 0; a < 3; a++) q[a] = __fadd_rn((float)p[a], off[a]);
+		const felt_gpu::DevVecF<3> h[5] = {iso.grad(q), iso.gradF(q), iso.gradB(q), iso.gradC(q),
+		                                   iso.gradE(q)};
+		for (int k = 0; k < 5; k++)
+			for (int a = 0; a < 3; a++) o[17 + k * 3 + a] = h[k][a];
+		o[32] = iso.divergence(q);
+		o[33] = iso.curv(q);
+		o[34] = iso.get(q);
 		return 0.0f;
 	}
 };

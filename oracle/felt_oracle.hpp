@@ -452,12 +452,13 @@ inline Real eigen_sum(const std::array<Real, D>& v)
 
 /// Mean curvature by difference of normals (NumericMixin.hpp:72-156), over any grid read
 /// through `get`. Normals use forward/backward differences along each axis and central
-/// differences across the others; the result is sum(n_fwd - n_back) / 2.
-template <int D, class Real, class Get>
-inline Real curv_at(Get&& get, const Vi<D>& pos)
+/// differences across the others; the result is sum(n_fwd - n_back) / 2. The position is a node
+/// or a real position (read through interpolation by get), stepped in its own type.
+template <int D, class Real, class Get, class Pos>
+inline Real curv_at(Get&& get, const Pos& pos)
 {
 	const Real centre = get(pos);
-	Vi<D> dir = pos;
+	Pos dir = pos;
 	std::array<Real, D> nf, nb;
 	for (int axis = 0; axis < D; axis++) {
 		dir[axis] += 1;
@@ -465,7 +466,7 @@ inline Real curv_at(Get&& get, const Vi<D>& pos)
 		Real sq = 0;
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
-			Vi<D> dn = dir;
+			Pos dn = dir;
 			dn[an] -= 1;
 			const Real lo = get(dn);
 			dn[an] += 2;
@@ -482,7 +483,7 @@ inline Real curv_at(Get&& get, const Vi<D>& pos)
 		Real sq = 0;
 		for (int an = 0; an < D; an++) {
 			if (an == axis) continue;
-			Vi<D> dn = dir;
+			Pos dn = dir;
 			dn[an] -= 1;
 			const Real lo = get(dn);
 			dn[an] += 2;
@@ -1055,6 +1056,62 @@ std::array<float, D> field_grad_f(const Grid& iso, const std::array<float, D>& p
 	}
 	for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
 	return g;
+}
+
+/// The Numeric API at a real position (NumericMixin.hpp:165-355 with Pos = float: get is interp,
+/// inside the float bounds test), into out in this order: grad (189-231), gradF (279-298), gradB
+/// (308-326), gradC (335-355), gradE (243-270), each D values, then divergence (165-175), curv
+/// (72-156) and the interpolated value (403-481). Each function steps its own copy of the
+/// position as the reference's does (grad, gradC, gradE: -1, +2, -1 per axis; gradF: +1, -1;
+/// gradB: -1, +1): in float a step and its undo need not cancel, and the drift carries over to
+/// the next axes, so the samples of one function are not those of another.
+template <int D, class Grid>
+void field_numeric(const Grid& iso, const std::array<float, D>& p, float* out)
+{
+	using P = std::array<float, D>;
+	const auto get = [&](const P& q) { return field_interp<D>(iso, q); };
+	const float centre = get(p);
+	float* gf = out + D;
+	float* gb = out + 2 * D;
+	float* gc = out + 3 * D;
+	float* ge = out + 4 * D;
+	const std::array<float, D> g = field_grad_f<D>(iso, p);
+	for (int a = 0; a < D; a++) out[a] = g[a];
+	P t = p;
+	for (int a = 0; a < D; a++) {
+		t[a] += 1;
+		gf[a] = get(t) - centre;
+		t[a] -= 1;
+	}
+	t = p;
+	for (int a = 0; a < D; a++) {
+		t[a] -= 1;
+		gb[a] = centre - get(t);
+		t[a] += 1;
+	}
+	t = p;
+	for (int a = 0; a < D; a++) {
+		t[a] -= 1;
+		const float back = get(t);
+		t[a] += 2;
+		const float fwd = get(t);
+		t[a] -= 1;
+		gc[a] = (fwd - back) / 2.0f;
+	}
+	t = p;
+	for (int a = 0; a < D; a++) {
+		t[a] -= 1;
+		const float back = get(t);
+		t[a] += 2;
+		const float fwd = get(t);
+		t[a] -= 1;
+		ge[a] = std::min(fwd - centre, 0.0f) + std::max(centre - back, 0.0f);
+	}
+	std::array<float, D> diff;
+	for (int a = 0; a < D; a++) diff[a] = gf[a] - gb[a];
+	out[5 * D] = eigen_sum<float, D>(diff);
+	out[5 * D + 1] = curv_at<D, float>(get, p);
+	out[5 * D + 2] = centre;
 }
 
 /// Eigen normalize(): divide by sqrt(x0^2 + (x1^2 + x2^2)) when that is positive.

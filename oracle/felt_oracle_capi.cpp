@@ -35,6 +35,7 @@ struct SurfBase {
 	virtual size_t band_size() = 0;
 	virtual void curv(const int* p, float* out) = 0;
 	virtual void numeric(const int* p, float* out) = 0;
+	virtual void numeric_f(const float* p, float* out) = 0;
 	virtual void ray(const float* o, const float* d, float* out) = 0;
 	virtual void save(std::vector<uint8_t>& out) = 0;
 	virtual void geometry(int* size, int* part) = 0;
@@ -131,6 +132,12 @@ struct Surf : SurfBase {
 	}
 	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
 	void numeric(const int* p, float* out) override { s.numeric(v(p), out); }
+	void numeric_f(const float* p, float* out) override
+	{
+		std::array<float, D> q;
+		for (int a = 0; a < D; a++) q[a] = p[a];
+		fo::field_numeric<D>(s.iso, q, out);
+	}
 	void save(std::vector<uint8_t>& out) override { fo::save_surface<D, L>(s, out); }
 	void geometry(int* size, int* part) override
 	{
@@ -370,6 +377,11 @@ int fo_ray(void* s, const float* origins, const float* dirs, size_t n, float* hi
 int fo_numeric(void* s, const int* pos, float* out)
 {
 	return guard([&] { static_cast<SurfBase*>(s)->numeric(pos, out); });
+}
+
+int fo_numeric_f(void* s, const float* pos, float* out)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->numeric_f(pos, out); });
 }
 
 int fo_curv(void* s, const int* pos, float* out)

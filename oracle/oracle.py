@@ -145,6 +145,14 @@ class Surface:
         _chk(lib().fo_numeric(self._h, _ivec(pos), out))
         return np.array(out, dtype=np.float32)
 
+    def numeric_f(self, pos):
+        """The Numeric API at a real position: grad, gradF, gradB, gradC, gradE (D values
+        each), divergence, curv and the interpolated value."""
+        p = (C.c_float * self.D)(*[float(np.float32(x)) for x in pos])
+        out = (C.c_float * (5 * self.D + 3))()
+        _chk(lib().fo_numeric_f(self._h, p, out))
+        return np.array(out, dtype=np.float32)
+
     def save(self):
         """Surface::save: the surface file (the reference's cereal binary layout) as bytes."""
         n = C.c_size_t()

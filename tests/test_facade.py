@@ -83,7 +83,8 @@ def test_numeric_probe_compiles(tmp_path):
 @pytest.mark.gpu
 def test_numeric_api_matches_oracle(tmp_path):
     """grad, gradF, gradB, gradC, gradE and divergence (NumericMixin.hpp:165-355) called from a
-    __device__ functor at every zero-layer node equal the oracle's, bit for bit."""
+    __device__ functor at every zero-layer node, and the same with curv and interp at the real
+    position node + (0.3, -0.2, 0.45), equal the oracle's, bit for bit."""
     from oracle import oracle as O
     exe = str(tmp_path / "numeric_probe")
     _compile_probe(exe, link=True)
@@ -91,7 +92,7 @@ def test_numeric_api_matches_oracle(tmp_path):
     r = subprocess.run([exe, out], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     n = 32
-    vals = np.fromfile(out, dtype=np.float32).reshape(n, n, n, 17)
+    vals = np.fromfile(out, dtype=np.float32).reshape(n, n, n, 35)
     o = O.Surface((n, n, n), (8, 8, 8), 2)
     o.seed((0, 0, 0))
     for _ in range(6):
@@ -106,3 +107,7 @@ def test_numeric_api_matches_oracle(tmp_path):
         want = o.numeric(pos)
         got = vals[i, j, k, :16]
         assert np.array_equal(got, want), (pos, got, want)
+        q = np.float32(pos) + np.float32([0.3, -0.2, 0.45])
+        want_f = o.numeric_f(q)
+        got_f = vals[i, j, k, 17:]
+        assert np.array_equal(got_f, want_f, equal_nan=True), (tuple(q), got_f, want_f)
