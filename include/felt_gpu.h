@@ -246,7 +246,9 @@ FG_API int fg_batch_save(fg_batch* b, size_t surface, uint8_t* buf, size_t cap, 
  * empty (never seeded, or with no active partition and every list empty; else FG_ERR_STATE) and
  * have the file's grid and partition size: a checkpoint taken with fg_batch_save or fg_save
  * comes back into any batch, e.g. a served surface set aside and later resumed. Its bricks come
- * from the batch's pool (FG_ERR_POOL when too few are free). */
+ * from the batch's pool (FG_ERR_POOL when too few are free). The batch's polygonisation sees the
+ * restored partitions after fg_batch_polys_invalidate, as a Polys built for a loaded surface
+ * does after Polys::invalidate (include/Felt/Polys.hpp:171-180). */
 FG_API int fg_batch_restore(fg_batch* b, size_t surface, const uint8_t* data, size_t n);
 FG_API int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float* dirs,
                          size_t n, float* hits);
