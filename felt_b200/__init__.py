@@ -77,6 +77,32 @@ def _fetch(fn, *args):
         cap = n.value
 
 
+QUERY = {"get": 0, "curv": 1, "divergence": 2, "inside": 3, "grad": 4, "gradF": 5, "gradB": 6,
+         "gradC": 7, "gradE": 8}
+
+
+def _query(fn_real, fn_nodes, head, D, what, pos):
+    """Runs fg_query (float positions) or fg_query_nodes (integer positions) and shapes the
+    result: (n,) for scalar queries, (n, D) for the gradients."""
+    code = QUERY[what] if isinstance(what, str) else int(what)
+    p = np.asarray(pos)
+    if p.ndim == 1:
+        p = p[None, :]
+    if p.ndim != 2 or p.shape[1] != D:
+        raise ValueError("positions must be (n, %d)" % D)
+    w = D if code >= QUERY["grad"] else 1
+    out = np.empty((p.shape[0], w), dtype=np.float32)
+    optr = out.ctypes.data_as(C.POINTER(C.c_float))
+    n = C.c_size_t(p.shape[0])
+    if np.issubdtype(p.dtype, np.integer):
+        a = np.ascontiguousarray(p, dtype=np.int32)
+        _chk(fn_nodes(*head, C.c_int(code), a.ctypes.data_as(C.POINTER(C.c_int)), n, optr))
+    else:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        _chk(fn_real(*head, C.c_int(code), a.ctypes.data_as(C.POINTER(C.c_float)), n, optr))
+    return out if w > 1 else out[:, 0]
+
+
 def _ray_arrays(origins, dirs, D):
     o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, D)
     d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, D)
@@ -219,6 +245,12 @@ class Surface:
                           d.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(o.shape[0]),
                           out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
+
+    def query(self, what, positions):
+        """The isogrid's Numeric API at n positions: what is one of QUERY's names ("get",
+        "curv", "divergence", "inside", "grad", "gradF", "gradB", "gradC", "gradE"); integer
+        positions are nodes, float positions real positions (get = interp there)."""
+        return _query(lib().fg_query, lib().fg_query_nodes, (self._h,), self.D, what, positions)
 
     def ray(self, origin, direction):
         """Surface::ray(origin, dir) for one ray."""
@@ -368,6 +400,11 @@ class Batch:
                                 d.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(o.shape[0]),
                                 out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
+
+    def query(self, i, what, positions):
+        """Surface.query on surface i."""
+        return _query(lib().fg_batch_query, lib().fg_batch_query_nodes,
+                      (self._h, C.c_size_t(i)), self.D, what, positions)
 
     def save(self, i):
         """Surface::save of surface i: the surface file as bytes."""

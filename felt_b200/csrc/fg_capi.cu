@@ -10,6 +10,7 @@
 #include "fg_polys.cuh"
 #include "fg_ray.cuh"
 #include "fg_image.cuh"
+#include "fg_query.cuh"
 
 #include "fg_handles.cuh"
 
@@ -241,6 +242,32 @@ int fg_get(fg_surface* s, const int* pos, float* out)
 		need(pos, "pos");
 		need(out, "out");
 		*out = s->eng->get(0, pos);
+	});
+}
+
+static void query_args(size_t n, const void* pos, float* out)
+{
+	if (n) {
+		need(pos, "positions");
+		need(out, "out");
+	}
+}
+
+int fg_query(fg_surface* s, int what, const float* pos, size_t n, float* out)
+{
+	return guard([&] {
+		need(s, "surface");
+		query_args(n, pos, out);
+		fg::query(*s->eng, 0, what, pos, nullptr, n, out);
+	});
+}
+
+int fg_query_nodes(fg_surface* s, int what, const int* pos, size_t n, float* out)
+{
+	return guard([&] {
+		need(s, "surface");
+		query_args(n, pos, out);
+		fg::query(*s->eng, 0, what, nullptr, pos, n, out);
 	});
 }
 
@@ -587,6 +614,26 @@ int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float*
 		}
 		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
 		fg::ray_batch(*b->eng, (int)surface, origins, dirs, n, hits, false);
+	});
+}
+
+int fg_batch_query(fg_batch* b, size_t surface, int what, const float* pos, size_t n, float* out)
+{
+	return guard([&] {
+		need(b, "batch");
+		query_args(n, pos, out);
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
+		fg::query(*b->eng, (int)surface, what, pos, nullptr, n, out);
+	});
+}
+
+int fg_batch_query_nodes(fg_batch* b, size_t surface, int what, const int* pos, size_t n, float* out)
+{
+	return guard([&] {
+		need(b, "batch");
+		query_args(n, pos, out);
+		if (surface >= (size_t)b->eng->surfaces()) throw fg::Error(FG_ERR_ARG, "surface index out of range");
+		fg::query(*b->eng, (int)surface, what, nullptr, pos, n, out);
 	});
 }
 

@@ -16,7 +16,7 @@
 #include <type_traits>
 
 #include "../../csrc/fg_dev.cuh"
-#include "../../csrc/fg_field.cuh"
+#include "../../csrc/fg_numeric.cuh"
 #include "felt_gpu.h"
 
 /// The device view handed out by fg_update_begin_global: the engine's pool description.
@@ -29,143 +29,15 @@ namespace felt_gpu {
 template <int D>
 using DevVec = fg::Vec<D>;
 
-/// A D-vector of floats returned by the gradient functions.
+/// A D-vector of floats: a real position, or what the gradient functions return.
 template <int D>
-struct DevVecF {
-	float v[D];
-	__host__ __device__ float& operator[](int i) { return v[i]; }
-	__host__ __device__ const float& operator[](int i) const { return v[i]; }
-};
+using DevVecF = fg::VecF<D>;
 
-/// Read access to the isogrid from a speed functor: get (Access::get with the lazy child get,
-/// PartitionedMixin.hpp:594-601), curv (NumericMixin.hpp:72-156), inside (GridMixin inside), and
-/// the rest of the reference's Numeric API (NumericMixin.hpp:165-355): grad, gradF, gradB,
-/// gradC, gradE, divergence. Like the reference's templates on the position type, each takes a
-/// node (DevVec<D>) or a real position (DevVecF<D>); at a real position get is interp (linear
-/// interpolation of the 2^D corners, NumericMixin.hpp:382-481), inside is the float test
-/// offset <= p < offset + size, and the stencils step the coordinates by +-1 in float. FP32
-/// rounded step by step as the reference's code (the grid spacing dx is 1, so its final
-/// divisions by dx change nothing).
+/// Read access to the isogrid from a speed functor: get, curv, inside and the rest of the
+/// reference's Numeric API (NumericMixin.hpp:72-481), each at a node (DevVec<D>) or a real
+/// position (DevVecF<D>, read by interpolation); see fg::IsoView.
 template <int D, int L>
-struct IsoGridView {
-	const fg::Dev* P;
-	const fg::SurfGeom* g;
-	__device__ float get(const DevVec<D>& p) const { return fg::get_phi<D, L>(*P, *g, p); }
-	__device__ float get(const DevVecF<D>& p) const { return interp(p); }
-	__device__ bool inside(const DevVec<D>& p) const { return fg::in_grid<D>(*g, p); }
-	__device__ bool inside(const DevVecF<D>& p) const { return fg::inside_f<D, L>(*g, p.v); }
-	/// interp (NumericMixin.hpp:403-481): corners in bit order, reduced along axis 0 first.
-	__device__ float interp(const DevVecF<D>& p) const
-	{
-		return fg::interp<D>([this](const DevVec<D>& q) { return get(q); }, p.v);
-	}
-	template <class Pos>
-	__device__ float curv(const Pos& p) const
-	{
-		return fg::curv_g<D>([this](const Pos& q) { return get(q); }, p);
-	}
-
-	/// grad (NumericMixin.hpp:189-231): central difference, one-sided at the grid's edge, 0
-	/// where neither neighbour is inside.
-	template <class Pos>
-	__device__ DevVecF<D> grad(const Pos& p) const
-	{
-		DevVecF<D> r;
-		const float centre = get(p);
-		Pos t = p;
-		for (int a = 0; a < D; a++) {
-			float back = centre, fwd = centre;
-			int order = 0;
-			t[a] -= 1;
-			if (inside(t)) {
-				back = get(t);
-				order++;
-			}
-			t[a] += 2;
-			if (inside(t)) {
-				fwd = get(t);
-				order++;
-			}
-			t[a] -= 1;
-			r[a] = order ? __fdiv_rn(__fsub_rn(fwd, back), (float)order) : 0.0f;
-		}
-		return r;
-	}
-	/// gradE (NumericMixin.hpp:243-270): the upwind (entropy-satisfying) gradient,
-	/// max(centre - back, 0) + min(forward - centre, 0) per axis.
-	template <class Pos>
-	__device__ DevVecF<D> gradE(const Pos& p) const
-	{
-		DevVecF<D> r;
-		const float centre = get(p);
-		Pos t = p;
-		for (int a = 0; a < D; a++) {
-			t[a] -= 1;
-			const float back = __fsub_rn(centre, get(t));
-			t[a] += 2;
-			const float fwd = __fsub_rn(get(t), centre);
-			t[a] -= 1;
-			const float b = back < 0.0f ? 0.0f : back;  // std::max(back, 0.0f)
-			const float f = 0.0f < fwd ? 0.0f : fwd;    // std::min(fwd, 0.0f)
-			r[a] = __fadd_rn(f, b);
-		}
-		return r;
-	}
-	/// gradF (NumericMixin.hpp:279-298): forward difference.
-	template <class Pos>
-	__device__ DevVecF<D> gradF(const Pos& p) const
-	{
-		DevVecF<D> r;
-		const float centre = get(p);
-		Pos t = p;
-		for (int a = 0; a < D; a++) {
-			t[a] += 1;
-			r[a] = __fsub_rn(get(t), centre);
-			t[a] -= 1;
-		}
-		return r;
-	}
-	/// gradB (NumericMixin.hpp:308-326): backward difference.
-	template <class Pos>
-	__device__ DevVecF<D> gradB(const Pos& p) const
-	{
-		DevVecF<D> r;
-		const float centre = get(p);
-		Pos t = p;
-		for (int a = 0; a < D; a++) {
-			t[a] -= 1;
-			r[a] = __fsub_rn(centre, get(t));
-			t[a] += 1;
-		}
-		return r;
-	}
-	/// gradC (NumericMixin.hpp:335-355): central difference.
-	template <class Pos>
-	__device__ DevVecF<D> gradC(const Pos& p) const
-	{
-		DevVecF<D> r;
-		Pos t = p;
-		for (int a = 0; a < D; a++) {
-			t[a] -= 1;
-			const float back = get(t);
-			t[a] += 2;
-			const float fwd = get(t);
-			t[a] -= 1;
-			r[a] = __fdiv_rn(__fsub_rn(fwd, back), 2.0f);
-		}
-		return r;
-	}
-	/// divergence (NumericMixin.hpp:165-175): the sum of gradF - gradB over the axes (Eigen's
-	/// fixed-size sum: x0 + (x1 + x2) in 3D).
-	template <class Pos>
-	__device__ float divergence(const Pos& p) const
-	{
-		const DevVecF<D> f = gradF(p), b = gradB(p);
-		float d[D];
-		for (int a = 0; a < D; a++) d[a] = __fsub_rn(f[a], b[a]);
-		return D == 2 ? __fadd_rn(d[0], d[1]) : __fadd_rn(d[0], __fadd_rn(d[1], d[D - 1]));
-	}
-};
+using IsoGridView = fg::IsoView<D, L>;
 
 namespace detail {
 

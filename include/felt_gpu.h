@@ -126,6 +126,27 @@ FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n);
 /* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */
 FG_API int fg_get(fg_surface* s, const int* pos, float* out);
 
+/* The isogrid's Numeric API from the host, for n positions at once: what the reference's
+ * isogrid offers as get(VecDi | VecDf), curv, divergence, grad, gradF, gradB, gradC, gradE
+ * (include/Felt/Impl/Mixin/NumericMixin.hpp:72-481; get of a real position is interp) and
+ * inside (GridMixin). fg_query takes real positions (n*dims floats), fg_query_nodes nodes
+ * (n*dims ints); host arrays. out receives n floats, or n*dims for the gradients (inside: 1 or
+ * 0). Results equal a speed functor's calls on the same surface, bit for bit. Positions whose
+ * samples leave the grid (undefined in the reference) read the isogrid there as L+1. */
+enum {
+	FG_Q_GET = 0,
+	FG_Q_CURV = 1,
+	FG_Q_DIVERGENCE = 2,
+	FG_Q_INSIDE = 3,
+	FG_Q_GRAD = 4,
+	FG_Q_GRADF = 5,
+	FG_Q_GRADB = 6,
+	FG_Q_GRADC = 7,
+	FG_Q_GRADE = 8
+};
+FG_API int fg_query(fg_surface* s, int what, const float* pos, size_t n, float* out);
+FG_API int fg_query_nodes(fg_surface* s, int what, const int* pos, size_t n, float* out);
+
 /* ray(origin, dir) (include/Felt/Surface.hpp:468-616, 1450-1598) for n rays at once: the
  * point where each ray first meets the zero curve, or FLT_MAX in every component (the
  * reference's ray_miss) when it misses. origins, dirs and hits hold n*dims floats each, in host
@@ -250,6 +271,11 @@ FG_API int fg_batch_save(fg_batch* b, size_t surface, uint8_t* buf, size_t cap, 
  * restored partitions after fg_batch_polys_invalidate, as a Polys built for a loaded surface
  * does after Polys::invalidate (include/Felt/Polys.hpp:171-180). */
 FG_API int fg_batch_restore(fg_batch* b, size_t surface, const uint8_t* data, size_t n);
+/* fg_query / fg_query_nodes on one surface of a batch. */
+FG_API int fg_batch_query(fg_batch* b, size_t surface, int what, const float* pos, size_t n,
+                          float* out);
+FG_API int fg_batch_query_nodes(fg_batch* b, size_t surface, int what, const int* pos, size_t n,
+                                float* out);
 FG_API int fg_batch_ray(fg_batch* b, size_t surface, const float* origins, const float* dirs,
                          size_t n, float* hits);
 FG_API int fg_batch_polys_partition(fg_batch* b, size_t surface, size_t part, float* vtx,
