@@ -704,7 +704,7 @@ public:
 		check_not_frozen();
 		// capacity: every zero-layer leaf of the surface
 		FG_CUDA(cudaMemsetAsync(zcount_, 0, sizeof(unsigned long long), st_));
-		FG_RUN("k_count_layer", st_, k_count_layer<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0, L, zcount_););
+		FG_RUN("k_count_layer", st_, launch_pdl((k_count_layer<L>), sm_count() * 2, 256, 0, st_, P_, 0, L, zcount_););
 		unsigned long long nz = 0;
 		FG_CUDA(cudaMemcpyAsync(&nz, zcount_, sizeof(nz), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
@@ -727,10 +727,10 @@ public:
 		b.nb = (int)nb;
 		int* counts = P_.ring_src;  // idle until calc_affected's rings
 		int* offsets = P_.ring_first;
-		FG_RUN("k_bounded_count", st_, k_bounded_count<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0, b, counts););
-		FG_RUN("k_scan_offsets", st_, k_scan_offsets<<<1, 1024, 0, st_>>>(counts, b.nb, offsets, d_lcount_););
-		FG_RUN("k_bounded_write", st_, k_bounded_write<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0, b, offsets, d_lpos_, lcap_););
-		FG_RUN("k_bounded_speed", st_, k_bounded_speed<D, L><<<grid_for(nz + 1), 256, 0, st_>>>(P_, 0, sp, d_lpos_, d_lcount_, d_lval_););
+		FG_RUN("k_bounded_count", st_, launch_pdl((k_bounded_count<D, L>), warp_grid_, 256, 0, st_, P_, 0, b, counts););
+		FG_RUN("k_scan_offsets", st_, launch_pdl((k_scan_offsets), 1, 1024, 0, st_, counts, b.nb, offsets, d_lcount_););
+		FG_RUN("k_bounded_write", st_, launch_pdl((k_bounded_write<D, L>), warp_grid_, 256, 0, st_, P_, 0, b, offsets, d_lpos_, lcap_););
+		FG_RUN("k_bounded_speed", st_, launch_pdl((k_bounded_speed<D, L>), grid_for(nz + 1), 256, 0, st_, P_, 0, sp, d_lpos_, d_lcount_, d_lval_););
 		int n = 0;
 		FG_CUDA(cudaMemcpyAsync(&n, d_lcount_, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
@@ -744,13 +744,13 @@ public:
 	{
 		constexpr int RING_CAP = 2048;
 		const int gb = grid_for(n);
-		FG_RUN("k_seed_claim", st_, k_seed_claim<D, L><<<gb, 256, 0, st_>>>(P_, 0, d_lpos_, n););
-		FG_RUN("k_ring_append", st_, k_ring_append<L><<<sm_count() * 4, 256, RING_CAP * 11, st_>>>(P_, RING_CAP, L););
-		FG_RUN("k_ring_plist", st_, k_ring_plist<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0););
-		FG_RUN("k_ring_finish", st_, k_ring_finish<L><<<1, 256, 0, st_>>>(P_, 0););
+		FG_RUN("k_seed_claim", st_, launch_pdl((k_seed_claim<D, L>), gb, 256, 0, st_, P_, 0, d_lpos_, n););
+		FG_RUN("k_ring_append", st_, launch_pdl((k_ring_append<L>), sm_count() * 4, 256, RING_CAP * 11, st_, P_, RING_CAP, L););
+		FG_RUN("k_ring_plist", st_, launch_pdl((k_ring_plist<L>), sm_count() * 2, 256, 0, st_, P_, 0););
+		FG_RUN("k_ring_finish", st_, launch_pdl((k_ring_finish<L>), 1, 256, 0, st_, P_, 0););
 		for (int phase = 0; phase < 4; phase++)
-			FG_RUN("k_seed_values", st_, k_seed_values<D, L><<<gb, 256, 0, st_>>>(P_, 0, d_lpos_, d_lval_, n, phase););
-		FG_RUN("k_seed_finish", st_, k_seed_finish<L><<<sm_count(), 256, 0, st_>>>(P_, 0););
+			FG_RUN("k_seed_values", st_, launch_pdl((k_seed_values<D, L>), gb, 256, 0, st_, P_, 0, d_lpos_, d_lval_, n, phase););
+		FG_RUN("k_seed_finish", st_, launch_pdl((k_seed_finish<L>), sm_count(), 256, 0, st_, P_, 0););
 	}
 
 	/// calc_affected's L rings (Surface.hpp:801-912) on surface 0, each a set of parallel
@@ -762,11 +762,11 @@ public:
 		FG_CUDA(cudaMemsetAsync(P_.ring_n, 0, 2 * NL * sizeof(int), st_));
 		for (int ring = 1; ring <= L; ring++) {
 			const int cur = (ring - 1) & 1;
-			FG_RUN("k_ring_setup", st_, k_ring_setup<L><<<grid_for((long long)NL * np), 256, 0, st_>>>(P_, 0, np, cur););
-			FG_RUN("k_ring_claim", st_, k_ring_claim<D, L><<<warp_grid_, 256, 0, st_>>>(P_, 0););
-			FG_RUN("k_ring_append", st_, k_ring_append<L><<<sm_count() * 4, 256, RING_CAP * 11, st_>>>(P_, RING_CAP, -1););
-			FG_RUN("k_ring_plist", st_, k_ring_plist<L><<<sm_count() * 2, 256, 0, st_>>>(P_, 0););
-			FG_RUN("k_ring_finish", st_, k_ring_finish<L><<<1, 256, 0, st_>>>(P_, 0););
+			FG_RUN("k_ring_setup", st_, launch_pdl((k_ring_setup<L>), grid_for((long long)NL * np), 256, 0, st_, P_, 0, np, cur););
+			FG_RUN("k_ring_claim", st_, launch_pdl((k_ring_claim<D, L>), warp_grid_, 256, 0, st_, P_, 0););
+			FG_RUN("k_ring_append", st_, launch_pdl((k_ring_append<L>), sm_count() * 4, 256, RING_CAP * 11, st_, P_, RING_CAP, -1););
+			FG_RUN("k_ring_plist", st_, launch_pdl((k_ring_plist<L>), sm_count() * 2, 256, 0, st_, P_, 0););
+			FG_RUN("k_ring_finish", st_, launch_pdl((k_ring_finish<L>), 1, 256, 0, st_, P_, 0););
 		}
 	}
 
@@ -776,7 +776,7 @@ public:
 		const int A = 0, B = 1;
 		buf_dirty_[A] = true;
 		calc_affected();
-		FG_RUN("k_local_children", st_, k_local_children<L><<<NL, 1024, 0, st_>>>(P_, 0););
+		FG_RUN("k_local_children", st_, launch_pdl((k_local_children<L>), NL, 1024, 0, st_, P_, 0););
 		count_band();
 		// update_zero_layer(&affected_buffer) over the delta leaves, then the distance passes
 		// over the affected lists (update_distance(plookup = affected, buffer))
@@ -988,7 +988,7 @@ public:
 		check_surface(s);
 		FG_CUDA(cudaMemsetAsync(zcount_, 0, sizeof(unsigned long long), st_));
 		for (int l = 0; l < NL; l++)
-			FG_RUN("k_count_layer", st_, k_count_layer<L><<<sm_count() * 2, 256, 0, st_>>>(P_, s, l, zcount_););
+			FG_RUN("k_count_layer", st_, launch_pdl((k_count_layer<L>), sm_count() * 2, 256, 0, st_, P_, s, l, zcount_););
 		unsigned long long n = 0;
 		FG_CUDA(cudaMemcpyAsync(&n, zcount_, sizeof(n), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));

@@ -1641,6 +1641,7 @@ __device__ __forceinline__ bool seed_locate(const Dev& P, const SurfGeom& g, con
 template <int D, int L>
 __global__ void k_seed_claim(Dev P, int s, const int* pos, int n)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1663,6 +1664,7 @@ __global__ void k_seed_claim(Dev P, int s, const int* pos, int n)
 template <int D, int L>
 __global__ void k_seed_values(Dev P, int s, const int* pos, const float* val, int n, int phase)
 {
+	pdl_enter();
 	const SurfGeom& g = P.geom[s];
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 		int gp, sl, leaf;
@@ -1680,6 +1682,7 @@ __global__ void k_seed_values(Dev P, int s, const int* pos, const float* val, in
 template <int L>
 __global__ void k_seed_finish(Dev P, int s)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int np = P.apcnt[0][s * NL + L];
@@ -1716,6 +1719,7 @@ __device__ __forceinline__ unsigned long long ring_key(int l, int entry, int pos
 template <int L>
 __global__ void k_ring_setup(Dev P, int s, int np, int cur)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int prev = cur ^ 1;
@@ -1739,6 +1743,7 @@ __global__ void k_ring_setup(Dev P, int s, int np, int cur)
 template <int D, int L>
 __global__ void k_ring_claim(Dev P, int s)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int lane = threadIdx.x & 31;
@@ -1785,6 +1790,7 @@ __global__ void k_ring_claim(Dev P, int s)
 template <int L>
 __global__ void k_ring_append(Dev P, int cap, int fixed_list)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	extern __shared__ unsigned char ring_smem[];
 	unsigned long long* skey = (unsigned long long*)ring_smem;
@@ -1851,6 +1857,7 @@ __global__ void k_ring_append(Dev P, int cap, int fixed_list)
 template <int L>
 __global__ void k_ring_plist(Dev P, int s)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int n = P.counters[CNT_AQ];
@@ -1874,6 +1881,7 @@ __global__ void k_ring_plist(Dev P, int s)
 template <int L>
 __global__ void k_ring_finish(Dev P, int s)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_AQ];
 	for (int i = threadIdx.x; i < n; i += blockDim.x) P.apkey[P.aq[i]] = NOCLAIM;
@@ -1893,6 +1901,7 @@ __global__ void k_ring_finish(Dev P, int s)
 template <int L>
 __global__ void k_count_layer(Dev P, int s, int li, unsigned long long* out)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int np = P.pcnt[s * NL + li];
@@ -1912,6 +1921,7 @@ __global__ void k_count_layer(Dev P, int s, int li, unsigned long long* out)
 template <int L>
 __global__ void __launch_bounds__(1024) k_local_children(Dev P, int s)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	__shared__ int wsum[32];
 	__shared__ int base;
@@ -1995,6 +2005,7 @@ __device__ __forceinline__ bool leaf_in_box(const Dev& P, const BoxParts<D>& b, 
 template <int D, int L>
 __global__ void k_bounded_count(Dev P, int s, BoxParts<D> b, int* counts)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
@@ -2019,6 +2030,7 @@ __global__ void k_bounded_count(Dev P, int s, BoxParts<D> b, int* counts)
 static __global__ void __launch_bounds__(1024) k_scan_offsets(const int* counts, int n, int* offsets,
                                                        int* total)
 {
+	pdl_enter();
 	__shared__ int wsum[32];
 	__shared__ int base;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -2052,6 +2064,7 @@ static __global__ void __launch_bounds__(1024) k_scan_offsets(const int* counts,
 template <int D, int L>
 __global__ void k_bounded_write(Dev P, int s, BoxParts<D> b, const int* offsets, int* pos, int cap)
 {
+	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const SurfGeom& g = P.geom[s];
 	const int lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
@@ -2079,6 +2092,7 @@ __global__ void k_bounded_write(Dev P, int s, BoxParts<D> b, const int* offsets,
 template <int D, int L>
 __global__ void k_bounded_speed(Dev P, int s, Speed sp, const int* pos, const int* n, float* val)
 {
+	pdl_enter();
 	const SurfGeom& g = P.geom[s];
 	const int m = *n;
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
