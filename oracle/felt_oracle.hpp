@@ -499,6 +499,49 @@ inline Real curv_at(Get&& get, const Pos& pos)
 	return eigen_sum<Real, D>(dn) / 2;
 }
 
+/// The Numeric API at a node (NumericMixin.hpp:165-355, grid spacing 1) over any grid read
+/// through get, with in_grid its bounds test, into out in this order: grad (189-231), gradF
+/// (279-298), gradB (308-326), gradC (335-355), gradE (243-270), each D values, then divergence
+/// (165-175). Whole-number steps are exact, so the functions share their samples.
+template <int D, class Real, class Get, class In>
+inline void numeric_at(Get&& get, In&& in_grid, const Vi<D>& pos, Real* out)
+{
+	const Real centre = get(pos);
+	Vi<D> t = pos;
+	Real* grad = out;
+	Real* gf = out + D;
+	Real* gb = out + 2 * D;
+	Real* gc = out + 3 * D;
+	Real* ge = out + 4 * D;
+	for (int a = 0; a < D; a++) {
+		t[a] -= 1;
+		const Real back = get(t);
+		const bool in_back = in_grid(t);
+		t[a] += 2;
+		const Real fwd = get(t);
+		const bool in_fwd = in_grid(t);
+		t[a] -= 1;
+		int order = 0;
+		Real b = centre, f = centre;
+		if (in_back) {
+			b = back;
+			order++;
+		}
+		if (in_fwd) {
+			f = fwd;
+			order++;
+		}
+		grad[a] = order ? (f - b) / Real(order) : Real(0);
+		gf[a] = fwd - centre;
+		gb[a] = centre - back;
+		gc[a] = (fwd - back) / Real(2);
+		ge[a] = std::min(fwd - centre, Real(0)) + std::max(centre - back, Real(0));
+	}
+	std::array<Real, D> diff;
+	for (int a = 0; a < D; a++) diff[a] = gf[a] - gb[a];
+	out[5 * D] = eigen_sum<Real, D>(diff);
+}
+
 /// Neighbour enumeration order -x,+x,-y,+y,-z,+z (NumericMixin.hpp:489-500).
 template <int D, class Fn>
 inline void neighs(Vi<D> pos, Fn&& fn)
@@ -592,45 +635,12 @@ public:
 		return curv_at<D, Real>([this](const Vi<D>& p) { return get(p); }, pos);
 	}
 
-	/// The Numeric API at a node (NumericMixin.hpp:165-355, grid spacing 1), into out in this
-	/// order: grad (189-231), gradF (279-298), gradB (308-326), gradC (335-355), gradE (243-270),
-	/// each D values, then divergence (165-175).
+	/// The Numeric API at a node (NumericMixin.hpp:165-355, grid spacing 1): numeric_at on the
+	/// isogrid.
 	void numeric(const Vi<D>& pos, Real* out) const
 	{
-		const Real centre = get(pos);
-		Vi<D> t = pos;
-		Real* grad = out;
-		Real* gf = out + D;
-		Real* gb = out + 2 * D;
-		Real* gc = out + 3 * D;
-		Real* ge = out + 4 * D;
-		for (int a = 0; a < D; a++) {
-			t[a] -= 1;
-			const Real back = get(t);
-			const bool in_back = iso.in_grid(t);
-			t[a] += 2;
-			const Real fwd = get(t);
-			const bool in_fwd = iso.in_grid(t);
-			t[a] -= 1;
-			int order = 0;
-			Real b = centre, f = centre;
-			if (in_back) {
-				b = back;
-				order++;
-			}
-			if (in_fwd) {
-				f = fwd;
-				order++;
-			}
-			grad[a] = order ? (f - b) / Real(order) : Real(0);
-			gf[a] = fwd - centre;
-			gb[a] = centre - back;
-			gc[a] = (fwd - back) / Real(2);
-			ge[a] = std::min(fwd - centre, Real(0)) + std::max(centre - back, Real(0));
-		}
-		std::array<Real, D> diff;
-		for (int a = 0; a < D; a++) diff[a] = gf[a] - gb[a];
-		out[5 * D] = eigen_sum<Real, D>(diff);
+		numeric_at<D, Real>([this](const Vi<D>& p) { return get(p); },
+		                    [this](const Vi<D>& p) { return iso.in_grid(p); }, pos, out);
 	}
 
 	Real speed(const Speed& s, const Vi<D>& pos) const

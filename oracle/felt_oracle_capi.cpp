@@ -416,6 +416,52 @@ int fo_curv_dense(int dims, const float* vals, const int* size, const int* off, 
 			throw fo::Error(-1, "dims");
 	});
 }
+/* The Numeric API over a dense grid (values row-major, `bg` outside) at a node (real = 0; pos
+ * holds whole numbers) or a real position (real = 1), for the stencil golden tests: 5*dims + 3
+ * values as fo_numeric_f returns them. */
+int fo_numeric_dense(int dims, const float* vals, const int* size, const int* off, float bg,
+                     const float* pos, int real, float* out)
+{
+	return guard([&] {
+		auto run = [&](auto dtag) {
+			constexpr int D = decltype(dtag)::value;
+			struct Dense {
+				const float* vals;
+				fo::Vi<D> sz, off, hi;
+				float bg;
+				float get(const fo::Vi<D>& q) const
+				{
+					if (!fo::inside<D>(q, off, hi)) return bg;
+					return vals[fo::index_of<D>(q, sz, off)];
+				}
+			} g{vals, {}, {}, {}, bg};
+			for (int a = 0; a < D; a++) {
+				g.sz[a] = size[a];
+				g.off[a] = off[a];
+				g.hi[a] = off[a] + size[a];
+			}
+			if (real) {
+				std::array<float, D> p;
+				for (int a = 0; a < D; a++) p[a] = pos[a];
+				fo::field_numeric<D>(g, p, out);
+				return;
+			}
+			fo::Vi<D> p;
+			for (int a = 0; a < D; a++) p[a] = (int)pos[a];
+			const auto get = [&](const fo::Vi<D>& q) { return g.get(q); };
+			fo::numeric_at<D, float>(get, [&](const fo::Vi<D>& q) { return fo::inside<D>(q, g.off, g.hi); },
+			                         p, out);
+			out[5 * D + 1] = fo::curv_at<D, float>(get, p);
+			out[5 * D + 2] = g.get(p);
+		};
+		if (dims == 2)
+			run(std::integral_constant<int, 2>{});
+		else if (dims == 3)
+			run(std::integral_constant<int, 3>{});
+		else
+			throw fo::Error(-1, "dims");
+	});
+}
 int fo_partitions(void* s, size_t* count, int* csize, int* coff)
 {
 	return guard([&] {

@@ -235,6 +235,66 @@ def curvature_cases(root):
     return out
 
 
+def _nums(text):
+    return [float(x) for x in re.findall(NUM, text)]
+
+
+def numeric_queries(lines, start, end):
+    """The Numeric API calls of [start, end] and what the test expects of them: `grid.<fn>(Vec..)`
+    compared with a `Vec..f(...)` or an `Approx(...)`, inside a CHECK or through a named local
+    (`const ... <name> = grid.<fn>(...)`, then `CHECK(<name> == ...)`)."""
+    named, out = {}, []
+    call = r"grid\.(\w+)\(Vec\d([if])\(([^)]*)\)\)"
+    for ln in lines[start - 1: end]:
+        m = re.search(r"const \w+ (\w+) = " + call, ln)
+        if m:
+            named[m.group(1)] = (m.group(2), m.group(3) == "f", _nums(m.group(4)))
+            continue
+        m = re.search(r"CHECK\(" + call + r" == Vec\df\(([^)]*)\)\)", ln)
+        if m:
+            out.append(dict(fn=m.group(1), real=m.group(2) == "f", pos=_nums(m.group(3)),
+                            want=_nums(m.group(4)), approx=False))
+            continue
+        m = re.search(r"CHECK\((\w+) == (?:Vec\df\(([^)]*)\)|Approx\((" + NUM + r")f?\))\)", ln)
+        if m and m.group(1) in named:
+            fn, real, pos = named[m.group(1)]
+            exact = m.group(2) is not None
+            out.append(dict(fn=fn, real=real, pos=pos,
+                            want=_nums(m.group(2)) if exact else [float(m.group(3))],
+                            approx=not exact))
+    return out
+
+
+def numeric_cases(root):
+    """Known answers of the Numeric API on 3x3 and 3x3x3 grids (test_Grid.cpp:1993-2290): interp
+    and get at real positions, gradF, gradB, gradC, grad and gradE at nodes. The grid spacing is
+    1 on this path, so the dx = 2 variants after line 2290 are left out."""
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+
+    def sets(a, b, dims):
+        vals = [0.0] * 3 ** dims
+        for ln in L[a - 1: b]:
+            m = re.search(r"grid\.set\(Vec\di\(([^)]*)\), (" + NUM + r")f?\)", ln)
+            if m:
+                p = [int(x) + 1 for x in _nums(m.group(1))]
+                idx = 0
+                for x in p:
+                    idx = idx * 3 + x
+                vals[idx] = float(m.group(2))
+        return vals
+
+    out = []
+    for a, b, dims, block in [(2016, 2045, 2, False), (2049, 2075, 2, False),
+                              (2079, 2110, 2, False), (2138, 2151, 2, True),
+                              (2153, 2166, 2, True), (2168, 2180, 2, True),
+                              (2182, 2194, 2, True), (2234, 2290, 3, True)]:
+        vals = data_block(L, a)[0] if block else sets(a, b, dims)
+        out.append(dict(ref=f"{f}:{a}-{b}", dims=dims, size=[3] * dims, offset=[-1] * dims,
+                        background=0.0, values=vals, queries=numeric_queries(L, a, b)))
+    return out
+
+
 def neighs_case(root):
     f = "src/tests/test_Grid.cpp"
     L = lines_of(root, f)
@@ -346,8 +406,8 @@ def serial_cases(root):
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
-               curvature=curvature_cases(root), neighs=neighs_case(root), ray=ray_cases(root),
-               serial=serial_cases(root))
+               curvature=curvature_cases(root), numeric=numeric_cases(root),
+               neighs=neighs_case(root), ray=ray_cases(root), serial=serial_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

@@ -89,6 +89,41 @@ def test_curvature_golden(case):
     assert out.value == case["curv"]
 
 
+NUMERIC_SLOTS = {"grad": 0, "gradF": 1, "gradB": 2, "gradC": 3, "gradE": 4}
+
+
+@pytest.mark.parametrize("case", _cases("numeric"), ids=lambda c: c["ref"].split(":")[1])
+def test_numeric_golden(case):
+    """The Numeric API's known answers (interp and get at real positions, gradF, gradB, gradC,
+    grad, gradE at nodes) on the reference's 3x3 and 3x3x3 test grids. Exact where the test
+    compares vectors with ==, Catch's default Approx (100 FLT_EPSILON relative) where it uses
+    Approx."""
+    import ctypes as C
+    lib = O.lib()
+    D = case["dims"]
+    vals = np.array(case["values"], dtype=np.float32)
+    assert case["queries"]
+    for q in case["queries"]:
+        out = (C.c_float * (5 * D + 3))()
+        rc = lib.fo_numeric_dense(D, vals.ctypes.data_as(C.POINTER(C.c_float)),
+                                  (C.c_int * D)(*case["size"]), (C.c_int * D)(*case["offset"]),
+                                  C.c_float(case["background"]), (C.c_float * D)(*q["pos"]),
+                                  1 if q["real"] else 0, out)
+        assert rc == 0
+        v = np.array(out, dtype=np.float32)
+        if q["fn"] in ("interp", "get"):
+            got = v[5 * D + 2: 5 * D + 3]
+        else:
+            k = NUMERIC_SLOTS[q["fn"]]
+            got = v[k * D: (k + 1) * D]
+        want = np.array(q["want"], dtype=np.float32)
+        if q["approx"]:
+            eps = 100 * float(np.finfo(np.float32).eps)
+            assert np.all(np.abs(got - want) <= eps * np.abs(want)), (q, got)
+        else:
+            assert np.array_equal(got, want), (q, got)
+
+
 def test_layer_id_rounding():
     """layer_id = iround(v + FLT_EPSILON), half away from zero (Surface.hpp:1694-1697):
     the values 0.4/1.4/2.4 and -0.6 of the fractional golden grids land in layers 0,1,2,-1."""
