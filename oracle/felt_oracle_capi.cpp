@@ -245,6 +245,23 @@ void put_list(const std::vector<size_t>& l, uint32_t* out, size_t cap, size_t* n
 	for (size_t i = 0; i < l.size() && i < cap; i++) out[i] = uint32_t(l[i]);
 }
 
+/// A standalone leaf lookup (LookupMixin.hpp:298-386, MultiList::SingleIdx, 3 lists): one
+/// partition covering a 3D grid of the given size and offset, for the Lookup golden tests.
+struct LeafLookup {
+	fo::PGrid<3, 3, float> g;
+	LeafLookup(const int* size, const int* off)
+	    : g({size[0], size[1], size[2]}, {off[0], off[1], off[2]}, {size[0], size[1], size[2]}, 0.0f)
+	{
+		g.activate(0);
+	}
+	size_t leaf(const int* pos) const
+	{
+		const fo::Vi<3> p{pos[0], pos[1], pos[2]};
+		if (!g.in_grid(p)) throw fo::Error(-1, "position outside the lookup grid");
+		return g.leaf_of(0, p);
+	}
+};
+
 }  // namespace
 
 extern "C" {
@@ -460,6 +477,51 @@ int fo_numeric_dense(int dims, const float* vals, const int* size, const int* of
 			run(std::integral_constant<int, 3>{});
 		else
 			throw fo::Error(-1, "dims");
+	});
+}
+/* The standalone leaf lookup of the Lookup golden tests: track / untrack a position in list l
+ * (0..2), reset, read list l, and read a position's index in its list (-1 for none). */
+int fo_lookup_create(const int* size, const int* off, void** out)
+{
+	return guard([&] { *out = new LeafLookup(size, off); });
+}
+int fo_lookup_destroy(void* h)
+{
+	delete static_cast<LeafLookup*>(h);
+	return 0;
+}
+int fo_lookup_index(void* h, const int* pos, size_t* out)
+{
+	return guard([&] { *out = static_cast<LeafLookup*>(h)->leaf(pos); });
+}
+int fo_lookup_track(void* h, const int* pos, int l)
+{
+	return guard([&] {
+		auto* k = static_cast<LeafLookup*>(h);
+		k->g.ltrack(0, k->leaf(pos), l);
+	});
+}
+int fo_lookup_untrack(void* h, const int* pos, int l)
+{
+	return guard([&] {
+		auto* k = static_cast<LeafLookup*>(h);
+		k->g.luntrack(0, k->leaf(pos), l);
+	});
+}
+int fo_lookup_reset(void* h)
+{
+	return guard([&] { static_cast<LeafLookup*>(h)->g.child_reset(0, false); });
+}
+int fo_lookup_list(void* h, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(static_cast<LeafLookup*>(h)->g.ch[0].lists[l], out, cap, n); });
+}
+int fo_lookup_get(void* h, const int* pos, long long* out)
+{
+	return guard([&] {
+		auto* k = static_cast<LeafLookup*>(h);
+		const size_t at = k->g.ch[0].lkp[k->leaf(pos)];
+		*out = at == fo::NUL ? -1 : (long long)at;
 	});
 }
 int fo_partitions(void* s, size_t* count, int* csize, int* coff)

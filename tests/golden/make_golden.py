@@ -295,6 +295,88 @@ def numeric_cases(root):
     return out
 
 
+def catch_leaves(lines, start, end):
+    """The leaf sections (THEN) of the Catch scenario in [start, end]. Catch runs a leaf with the
+    statements of every enclosing section; each leaf comes back as those statements in order
+    (`actions`) and its own (`checks`)."""
+    frames = [dict(kind="ROOT", open=0, stmts=[])]
+    depth, pending, out = 0, None, []
+    for ln in lines[start - 1: end]:
+        code = re.sub(r"//.*", "", ln)
+        bare = re.sub(r'"[^"]*"', '""', code)
+        m = re.search(r"\b(SCENARIO|GIVEN|WHEN|AND_WHEN|THEN)\s*\(", bare)
+        if m:
+            pending = dict(kind=m.group(1), open=None, stmts=[])
+        elif pending is None and bare.strip() not in ("", "{", "}"):
+            frames[-1]["stmts"].append(code.strip())
+        for ch in bare:
+            if ch == "{":
+                depth += 1
+                if pending is not None:
+                    pending["open"] = depth
+                    frames.append(pending)
+                    pending = None
+            elif ch == "}":
+                if len(frames) > 1 and frames[-1]["open"] == depth:
+                    f = frames.pop()
+                    if f["kind"] == "THEN":
+                        out.append(dict(actions=[s for fr in frames for s in fr["stmts"]],
+                                        checks=f["stmts"]))
+                depth -= 1
+    return out
+
+
+def lookup_cases(root):
+    """Lookup::SingleListSingleIdx and Lookup::MultiListSingleIdx (test_Grid.cpp:151-500): the
+    leaf lists' order under track, untrack (swap with the last entry) and reset, and each
+    position's index in its list. One case per leaf section: the positions, the actions of its
+    enclosing sections, and its checks."""
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+    out = []
+    for a, b in [(151, 328), (330, 500)]:
+        text = "\n".join(L[a - 1: b])
+        pos = {m.group(1): [int(x) for x in _nums(m.group(2))]
+               for m in re.finditer(r"const Vec3i (pos\d+)\(([^)]*)\);", text)}
+        m = re.search(r"Grid grid\(Vec3i\(([^)]*)\), Vec3i\(([^)]*)\)\)", text)
+        size, off = [int(x) for x in _nums(m.group(1))], [int(x) for x in _nums(m.group(2))]
+        for k, leaf in enumerate(catch_leaves(L, a, b)):
+            steps = []
+            for s in leaf["actions"]:
+                m = re.match(r"grid\.track\((pos\d+)_idx(?:, (\d+))?\);", s)
+                if m:
+                    steps.append(["track", m.group(1), int(m.group(2) or 0)])
+                    continue
+                m = re.match(r"grid\.untrack\((?:grid\.index\((pos\d+)\)|(pos\d+)_idx)(?:, (\d+))?\);", s)
+                if m:
+                    steps.append(["untrack", m.group(1) or m.group(2), int(m.group(3) or 0)])
+                    continue
+                if re.match(r"grid\.reset\(\);", s):
+                    steps.append(["reset"])
+            checks = []
+            for s in leaf["checks"]:
+                m = re.match(r"CHECK\(grid\.list\((\d*)\)\.size\(\) == (\d+)\);", s)
+                if m:
+                    checks.append(["size", int(m.group(1) or 0), int(m.group(2))])
+                    continue
+                m = re.match(r"CHECK\(grid\.list\((\d*)\)\[(\d+)\] == (pos\d+)_idx\);", s)
+                if m:
+                    checks.append(["entry", int(m.group(1) or 0), int(m.group(2)), m.group(3)])
+                    continue
+                m = re.match(r"CHECK\(grid\.get\((pos\d+)\) == (\d+|null_idx)\);", s)
+                if m:
+                    v = -1 if m.group(2) == "null_idx" else int(m.group(2))
+                    checks.append(["get", m.group(1), v])
+                    continue
+                m = re.match(r"CHECK\(grid\.is_tracked\((pos\d+)_idx\) == (true|false)\);", s)
+                if m:
+                    checks.append(["tracked", m.group(1), m.group(2) == "true"])
+            if checks:
+                out.append(dict(ref=f"{f}:{a}-{b}#{k}", size=size, offset=off, positions=pos,
+                                steps=steps, checks=checks))
+    return out
+
+
 def neighs_case(root):
     f = "src/tests/test_Grid.cpp"
     L = lines_of(root, f)
@@ -406,7 +488,7 @@ def serial_cases(root):
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
-               curvature=curvature_cases(root), numeric=numeric_cases(root),
+               curvature=curvature_cases(root), numeric=numeric_cases(root), lookup=lookup_cases(root),
                neighs=neighs_case(root), ray=ray_cases(root), serial=serial_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(dst, "w") as f:

@@ -124,6 +124,55 @@ def test_numeric_golden(case):
             assert np.array_equal(got, want), (q, got)
 
 
+@pytest.mark.parametrize("case", _cases("lookup"), ids=lambda c: c["ref"].split(":")[1])
+def test_lookup_golden(case):
+    """The ordered leaf lists every list order on this path rests on (LookupMixin.hpp:298-386):
+    track appends, untrack moves the last entry into the freed slot, reset empties; each
+    position's lookup holds its index in its list (test_Grid.cpp Lookup scenarios)."""
+    import ctypes as C
+    lib = O.lib()
+    h = C.c_void_p()
+    iv = lambda v: (C.c_int * 3)(*v)  # noqa: E731
+    assert lib.fo_lookup_create(iv(case["size"]), iv(case["offset"]), C.byref(h)) == 0
+    try:
+        pos = case["positions"]
+
+        def index(name):
+            n = C.c_size_t()
+            assert lib.fo_lookup_index(h, iv(pos[name]), C.byref(n)) == 0
+            return n.value
+
+        def lst(li):
+            n = C.c_size_t()
+            out = (C.c_uint32 * 64)()
+            assert lib.fo_lookup_list(h, li, out, C.c_size_t(64), C.byref(n)) == 0
+            return list(out[: n.value])
+
+        def get(name):
+            v = C.c_longlong()
+            assert lib.fo_lookup_get(h, iv(pos[name]), C.byref(v)) == 0
+            return v.value
+
+        for st in case["steps"]:
+            if st[0] == "track":
+                assert lib.fo_lookup_track(h, iv(pos[st[1]]), st[2]) == 0
+            elif st[0] == "untrack":
+                assert lib.fo_lookup_untrack(h, iv(pos[st[1]]), st[2]) == 0
+            else:
+                assert lib.fo_lookup_reset(h) == 0
+        for ck in case["checks"]:
+            if ck[0] == "size":
+                assert len(lst(ck[1])) == ck[2], ck
+            elif ck[0] == "entry":
+                assert lst(ck[1])[ck[2]] == index(ck[3]), ck
+            elif ck[0] == "get":
+                assert get(ck[1]) == ck[2], ck
+            else:
+                assert (get(ck[1]) >= 0) == ck[2], ck
+    finally:
+        lib.fo_lookup_destroy(h)
+
+
 def test_layer_id_rounding():
     """layer_id = iround(v + FLT_EPSILON), half away from zero (Surface.hpp:1694-1697):
     the values 0.4/1.4/2.4 and -0.6 of the fractional golden grids land in layers 0,1,2,-1."""
