@@ -262,6 +262,30 @@ struct LeafLookup {
 	}
 };
 
+/// A standalone partitioned lookup (Partitioned::Lookup: PartitionedMixin.hpp:388-413 over
+/// LookupMixin's children and leaf lists), for the partitioned Lookup golden test.
+struct PartLookup {
+	fo::PGrid<3, 3, float> g;
+	PartLookup(const int* size, const int* off, const int* part)
+	    : g({size[0], size[1], size[2]}, {off[0], off[1], off[2]}, {part[0], part[1], part[2]}, 0.0f)
+	{
+	}
+	size_t child(const int* cpos) const
+	{
+		const fo::Vi<3> c{cpos[0], cpos[1], cpos[2]};
+		for (int a = 0; a < 3; a++)
+			if (c[a] < g.coff[a] || c[a] >= g.coff[a] + g.ccount[a])
+				throw fo::Error(-1, "partition outside the children grid");
+		return fo::index_of<3>(c, g.ccount, g.coff);
+	}
+	fo::Vi<3> pos(const int* p) const
+	{
+		const fo::Vi<3> q{p[0], p[1], p[2]};
+		if (!g.in_grid(q)) throw fo::Error(-1, "position outside the grid");
+		return q;
+	}
+};
+
 }  // namespace
 
 extern "C" {
@@ -522,6 +546,64 @@ int fo_lookup_get(void* h, const int* pos, long long* out)
 		auto* k = static_cast<LeafLookup*>(h);
 		const size_t at = k->g.ch[0].lkp[k->leaf(pos)];
 		*out = at == fo::NUL ? -1 : (long long)at;
+	});
+}
+/* The standalone partitioned lookup: track a position in list l, the children list l, a
+ * partition's index in children list l (-1 for none), a partition's leaf list l and a
+ * position's index in its partition's list (-1 for none). Partitions are children-grid
+ * positions. */
+int fo_plookup_create(const int* size, const int* off, const int* part, void** out)
+{
+	return guard([&] { *out = new PartLookup(size, off, part); });
+}
+int fo_plookup_destroy(void* h)
+{
+	delete static_cast<PartLookup*>(h);
+	return 0;
+}
+int fo_plookup_track(void* h, const int* pos, int l)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		k->g.track_lookup(k->pos(pos), l);
+	});
+}
+int fo_plookup_child_index(void* h, const int* part, size_t* out)
+{
+	return guard([&] { *out = static_cast<PartLookup*>(h)->child(part); });
+}
+int fo_plookup_children(void* h, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] { put_list(static_cast<PartLookup*>(h)->g.clists[l], out, cap, n); });
+}
+int fo_plookup_child_get(void* h, const int* part, int l, long long* out)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		const size_t at = k->g.cpos[k->child(part)][l];
+		*out = at == fo::NUL ? -1 : (long long)at;
+	});
+}
+int fo_plookup_leaves(void* h, const int* part, int l, uint32_t* out, size_t cap, size_t* n)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		put_list(k->g.ch[k->child(part)].lists[l], out, cap, n);
+	});
+}
+int fo_plookup_leaf_get(void* h, const int* part, const int* pos, long long* out)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		const size_t pc = k->child(part);
+		const fo::Vi<3> q = k->pos(pos);
+		if (k->g.pidx_child(q) != pc) throw fo::Error(-1, "position outside the partition");
+		const auto& c = k->g.ch[pc];
+		*out = -1;
+		if (!c.lkp.empty()) {
+			const size_t at = c.lkp[k->g.leaf_of(pc, q)];
+			if (at != fo::NUL) *out = (long long)at;
+		}
 	});
 }
 int fo_partitions(void* s, size_t* count, int* csize, int* coff)

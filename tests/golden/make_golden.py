@@ -377,6 +377,54 @@ def lookup_cases(root):
     return out
 
 
+def partitioned_lookup_case(root):
+    """Partitioned::Lookup (test_Grid.cpp:1175-1243, the block before the masked reset): leaf
+    positions tracked into lists of a 9^3 grid in 3^3 partitions, and the children lists, the
+    children lookup, each partition's leaf lists and the leaves' indices that result."""
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+    a, b = 1175, 1243
+    text = "\n".join(L[a - 1: b])
+    m = re.search(r"Grid grid\(Vec3i\(([^)]*)\), Vec3i\(([^)]*)\), Vec3i\(([^)]*)\)\)", text)
+    size, off, part = ([int(x) for x in _nums(m.group(i))] for i in (1, 2, 3))
+    vecs = {m.group(1): [int(x) for x in _nums(m.group(2))]
+            for m in re.finditer(r"const Vec3i (\w+)\(([^)]*)\);", text)}
+    leaves = [lf for lf in catch_leaves(L, a, b) if any("track(" in s for s in lf["actions"])]
+    assert len(leaves) == 1
+    steps = []
+    for s in leaves[0]["actions"]:
+        m = re.match(r"grid\.track\((pos\d+), (\d+)\);", s)
+        if m:
+            steps.append([m.group(1), int(m.group(2))])
+            continue
+        m = re.match(r"grid\.track\(\w+_idx, grid\.children\(\)\.get\(\w+\)\.index\((pos\d+)\), (\d+)\);", s)
+        if m:
+            steps.append([m.group(1), int(m.group(2))])
+    checks = []
+    for s in leaves[0]["checks"]:
+        m = re.match(r"CHECK\(grid\.children\(\)\.lookup\(\)\.list\((\d+)\)\.size\(\) == (\d+)\);", s)
+        if m:
+            checks.append(["children_size", int(m.group(1)), int(m.group(2))])
+            continue
+        m = re.match(r"CHECK\(grid\.children\(\)\.lookup\(\)\.list\((\d+)\)\[(\d+)\] == (\w+)_idx\);", s)
+        if m:
+            checks.append(["children_entry", int(m.group(1)), int(m.group(2)), m.group(3)])
+            continue
+        m = re.match(r"CHECK\(grid\.children\(\)\.lookup\(\)\.get\((\w+)\)\((\d+)\) == (\d+)\);", s)
+        if m:
+            checks.append(["children_get", m.group(1), int(m.group(2)), int(m.group(3))])
+            continue
+        m = re.match(r"CHECK\(grid\.children\(\)\.get\((\w+)\)\.list\((\d+)\)\.size\(\) == (\d+)\);", s)
+        if m:
+            checks.append(["leaves_size", m.group(1), int(m.group(2)), int(m.group(3))])
+            continue
+        m = re.match(r"CHECK\(grid\.children\(\)\.get\((\w+)\)\.get\((pos\d+)\) == (\d+)\);", s)
+        if m:
+            checks.append(["leaf_get", m.group(1), m.group(2), int(m.group(3))])
+    return dict(ref=f"{f}:{a}-{b}", size=size, offset=off, part=part, vectors=vecs, steps=steps,
+                checks=checks)
+
+
 def neighs_case(root):
     f = "src/tests/test_Grid.cpp"
     L = lines_of(root, f)
@@ -489,6 +537,7 @@ def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
                curvature=curvature_cases(root), numeric=numeric_cases(root), lookup=lookup_cases(root),
+               partitioned_lookup=partitioned_lookup_case(root),
                neighs=neighs_case(root), ray=ray_cases(root), serial=serial_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
     with open(dst, "w") as f:

@@ -173,6 +173,54 @@ def test_lookup_golden(case):
         lib.fo_lookup_destroy(h)
 
 
+def test_partitioned_lookup_golden():
+    """The two-level lists (Partitioned::Lookup, test_Grid.cpp:1175-1243): tracking a leaf
+    appends its partition to that list's children list on first use, and the leaf to the
+    partition's own list."""
+    import ctypes as C
+    case = _cases("partitioned_lookup")
+    lib = O.lib()
+    iv = lambda v: (C.c_int * 3)(*v)  # noqa: E731
+    vec = case["vectors"]
+    h = C.c_void_p()
+    assert lib.fo_plookup_create(iv(case["size"]), iv(case["offset"]), iv(case["part"]),
+                                 C.byref(h)) == 0
+    try:
+        def ulist(fn, *args):
+            n = C.c_size_t()
+            out = (C.c_uint32 * 64)()
+            assert fn(h, *args, out, C.c_size_t(64), C.byref(n)) == 0
+            return list(out[: n.value])
+
+        def ll(fn, *args):
+            v = C.c_longlong()
+            assert fn(h, *args, C.byref(v)) == 0
+            return v.value
+
+        def child(name):
+            n = C.c_size_t()
+            assert lib.fo_plookup_child_index(h, iv(vec[name]), C.byref(n)) == 0
+            return n.value
+
+        for name, li in case["steps"]:
+            assert lib.fo_plookup_track(h, iv(vec[name]), li) == 0
+        assert len(case["checks"]) == 15
+        for ck in case["checks"]:
+            kind = ck[0]
+            if kind == "children_size":
+                assert len(ulist(lib.fo_plookup_children, ck[1])) == ck[2], ck
+            elif kind == "children_entry":
+                assert ulist(lib.fo_plookup_children, ck[1])[ck[2]] == child(ck[3]), ck
+            elif kind == "children_get":
+                assert ll(lib.fo_plookup_child_get, iv(vec[ck[1]]), ck[2]) == ck[3], ck
+            elif kind == "leaves_size":
+                assert len(ulist(lib.fo_plookup_leaves, iv(vec[ck[1]]), ck[2])) == ck[3], ck
+            else:
+                assert ll(lib.fo_plookup_leaf_get, iv(vec[ck[1]]), iv(vec[ck[2]])) == ck[3], ck
+    finally:
+        lib.fo_plookup_destroy(h)
+
+
 def test_layer_id_rounding():
     """layer_id = iround(v + FLT_EPSILON), half away from zero (Surface.hpp:1694-1697):
     the values 0.4/1.4/2.4 and -0.6 of the fractional golden grids land in layers 0,1,2,-1."""
