@@ -606,6 +606,38 @@ int fo_plookup_leaf_get(void* h, const int* part, const int* pos, long long* out
 		}
 	});
 }
+/* The children-level lookup alone (LookupMixin.hpp:457-570, MultiList::MultiIdx: one index
+ * per list), as a partitioned lookup with 1^3 partitions so that partitions are positions: for
+ * the Lookup::Multi golden test. */
+int fo_clookup_create(const int* size, const int* off, void** out)
+{
+	const int one[3] = {1, 1, 1};
+	return guard([&] { *out = new PartLookup(size, off, one); });
+}
+int fo_clookup_track(void* h, const int* pos, int l)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		k->g.ctrack(k->child(pos), l);
+	});
+}
+int fo_clookup_untrack(void* h, const int* pos, int l)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		k->g.cuntrack(k->child(pos), l);
+	});
+}
+int fo_clookup_reset(void* h)
+{
+	return guard([&] {
+		auto* k = static_cast<PartLookup*>(h);
+		for (int l = 0; l < 3; l++) {
+			const std::vector<size_t> listed = k->g.clists[l];
+			for (size_t pc : listed) k->g.cuntrack(pc, l);
+		}
+	});
+}
 int fo_partitions(void* s, size_t* count, int* csize, int* coff)
 {
 	return guard([&] {

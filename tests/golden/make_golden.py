@@ -377,6 +377,47 @@ def lookup_cases(root):
     return out
 
 
+def multi_lookup_cases(root):
+    """Lookup::Multi (test_Grid.cpp:502-731), the lookup with one index per list: list order
+    under track (a second track in the same list does nothing), untrack (swap with the last
+    entry) and reset, and each position's index in each list. One case per leaf section."""
+    f = "src/tests/test_Grid.cpp"
+    L = lines_of(root, f)
+    a, b = 525, 731
+    text = "\n".join(L[a - 1: b])
+    pos = {m.group(1): [int(x) for x in _nums(m.group(2))]
+           for m in re.finditer(r"const Vec3i (pos\d+)\(([^)]*)\);", text)}
+    m = re.search(r"Grid grid\(Vec3i\(([^)]*)\), Vec3i\(([^)]*)\)\)", text)
+    size, off = [int(x) for x in _nums(m.group(1))], [int(x) for x in _nums(m.group(2))]
+    out = []
+    for k, leaf in enumerate(catch_leaves(L, a, b)):
+        steps = []
+        for s in leaf["actions"]:
+            m = re.match(r"grid\.(track|untrack)\((pos\d+)_idx, (\d+)\);", s)
+            if m:
+                steps.append([m.group(1), m.group(2), int(m.group(3))])
+            elif re.match(r"grid\.reset\(\);", s):
+                steps.append(["reset"])
+        checks = []
+        for s in leaf["checks"]:
+            m = re.match(r"(?:CHECK|REQUIRE)\(grid\.list\((\d+)\)\.size\(\) == (\d+)\);", s)
+            if m:
+                checks.append(["size", int(m.group(1)), int(m.group(2))])
+                continue
+            m = re.match(r"(?:CHECK|REQUIRE)\(grid\.list\((\d+)\)\[(\d+)\] == (pos\d+)_idx\);", s)
+            if m:
+                checks.append(["entry", int(m.group(1)), int(m.group(2)), m.group(3)])
+                continue
+            m = re.match(r"(?:CHECK|REQUIRE)\(grid\.get\((pos\d+)\)\((\d+)\) == (\d+|Felt::null_idx)\);", s)
+            if m:
+                v = -1 if "null" in m.group(3) else int(m.group(3))
+                checks.append(["get", m.group(1), int(m.group(2)), v])
+        if checks:
+            out.append(dict(ref=f"{f}:{a}-{b}#{k}", size=size, offset=off, positions=pos,
+                            steps=steps, checks=checks))
+    return out
+
+
 def partitioned_lookup_case(root):
     """Partitioned::Lookup (test_Grid.cpp:1175-1243, the block before the masked reset): leaf
     positions tracked into lists of a 9^3 grid in 3^3 partitions, and the children lists, the
@@ -537,6 +578,7 @@ def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
                curvature=curvature_cases(root), numeric=numeric_cases(root), lookup=lookup_cases(root),
+               multi_lookup=multi_lookup_cases(root),
                partitioned_lookup=partitioned_lookup_case(root),
                neighs=neighs_case(root), ray=ray_cases(root), serial=serial_cases(root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
