@@ -434,9 +434,13 @@ def cpu_baseline(name, cfg, steps):
         k = cfg["cpu_subset"]
         rate, nu, secs = cpu_batch(name, cfg, steps, k)
         sample = f"first {k} surfaces of the workload, {steps} steps each, one after another"
-    return {"value": rate, "unit": "node-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{sample} ({nu:.3g} node-updates in {secs:.2f} s; the reference's "
-                      f"parallel loops on {threads} threads)"}
+    out = {"value": rate, "unit": "node-updates/s", "cores": threads, "kind": "port",
+           "sample": f"{sample} ({nu:.3g} node-updates in {secs:.2f} s; the reference's "
+                     f"parallel loops on {threads} threads)"}
+    # a step of a single-surface config is the whole workload's step; a batch config's sample
+    # is a subset of its surfaces, so its time is not a step of the workload
+    step_ms = secs * 1e3 / steps if cfg["kind"] == "single" and steps else None
+    return out, step_ms
 
 
 def run_reference(args, name, cfg):
@@ -444,6 +448,7 @@ def run_reference(args, name, cfg):
     if rank != 0:
         return
     metric, unit = "narrow-band node-updates/s", "node-updates/s"
+    step_ms = None
     if cfg["kind"] == "serve":
         steps = None
         base = serve_cpu(cfg, cfg["cpu_subset"])
@@ -458,11 +463,11 @@ def run_reference(args, name, cfg):
     else:
         steps = args.steps or cfg["steps"]
         steps = min(steps, 20 if cfg["kind"] == "single" else 10)
-        base = cpu_baseline(name, cfg, steps)
+        base, step_ms = cpu_baseline(name, cfg, steps)
     line = {
         "impl": "reference", "metric": metric, "value": base["value"],
         "unit": unit, "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
-        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": cfg["workload"], "name": name},
         "cpu_baseline": base,
@@ -1011,8 +1016,8 @@ def run_felt(args, name, cfg):
             extra["batched_over_plain"] = value / p_rate
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(name, cfg, args.cpu_steps if cfg["kind"] == "single"
-                           else cfg["cpu_steps"])
+        cpu, _ = cpu_baseline(name, cfg, args.cpu_steps if cfg["kind"] == "single"
+                              else cfg["cpu_steps"])
 
     if rank == 0:
         par = (f"replicas{ws}" if cfg["kind"] == "single"
