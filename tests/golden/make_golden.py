@@ -298,7 +298,8 @@ def numeric_cases(root):
 def catch_leaves(lines, start, end):
     """The leaf sections (THEN) of the Catch scenario in [start, end]. Catch runs a leaf with the
     statements of every enclosing section; each leaf comes back as those statements in order
-    (`actions`) and its own (`checks`)."""
+    (`actions`) and its own (`checks`). Statements on a section's header line are not read (the
+    reference's tests put none there)."""
     frames = [dict(kind="ROOT", open=0, stmts=[])]
     depth, pending, out = 0, None, []
     for ln in lines[start - 1: end]:
