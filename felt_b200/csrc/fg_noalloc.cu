@@ -1,25 +1,27 @@
 // fg_snapshot_noalloc: a dense isogrid snapshot into a caller's host buffer that allocates no
 // memory at all.
 //
-// fg_snapshot with a host destination stages the dense grid in a device buffer it allocates
-// and frees on every call. Some callers cannot allow that: code running while a CUDA stream is
-// being captured into a graph (cudaMalloc/cudaFree are not capturable), a host process whose
-// device memory is owned and budgeted by another allocator (a framework's caching allocator or
-// a fixed memory reservation), or a real-time loop that must not hit the driver's allocator
-// and its implicit synchronisation. This entry point stages through a fixed device array
-// instead, declared below at file scope, so it never calls cudaMalloc, cudaFree or any
-// allocating library routine.
+// fg_snapshot with a host destination stages the dense grid in a device buffer that it
+// allocates and frees on every call. Some callers cannot allow that: a host process whose
+// device memory is owned and budgeted by another allocator (a framework's caching allocator,
+// or a fixed reservation that leaves no room for the driver's allocations), or a real-time loop
+// that must not enter the driver's allocator, whose cudaMalloc and cudaFree can stall or
+// synchronise the whole device. This entry point stages through a fixed device array instead,
+// declared below at file scope, so it never calls cudaMalloc, cudaFree or any allocating
+// library routine.
 //
 // Limits and sharing:
 //  - At most FG_NOALLOC_SNAPSHOT_MAX floats (2^21 = 2,097,152, e.g. a 128^3 or 1448^2 grid,
 //    8 MiB) per call; larger grids are rejected with FG_ERR_CAPACITY.
 //  - The array lives in every GPU that loads this library, for the life of the process.
 //  - Every call shares it and it keeps the previous call's contents; the kernel writes every
-//    element it later copies out, so nothing needs clearing. Calls that overlap on the GPU
+//    element it later copies out, so nothing needs clearing. Calls that overlapped on the GPU
 //    would race on the array, so calls are serialised by a process-wide lock and each call
 //    waits for its copy to finish before returning.
-//  - The first call on a device looks up the array's device address with that device
-//    current (cudaGetSymbolAddress), so that first call should come before any stream capture.
+//  - The call runs on the surface's own device (made current for the call when another device
+//    is current). The first call on a device looks up the array's device address with that
+//    device current (cudaGetSymbolAddress); that first call should come before any stream
+//    capture.
 #include <mutex>
 #include <string>
 
@@ -86,6 +88,30 @@ void launch(int D, int L, const fg::Dev& P, float* scratch, long long total, cud
 	throw fg::Error(FG_ERR_ARG, "unsupported dims/layers");
 }
 
+/// Makes `dev` the current device for the life of the guard, and restores the caller's.
+struct DeviceGuard {
+	int prev = -1;
+	explicit DeviceGuard(int dev)
+	{
+		FG_CUDA(cudaGetDevice(&prev));
+		if (prev != dev) FG_CUDA(cudaSetDevice(dev));
+	}
+	~DeviceGuard()
+	{
+		int cur = -1;
+		if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+	}
+};
+
+/// The device whose memory holds the surface's pool (its geometry table lives there).
+int surface_device(const fg::EngineBase& eng)
+{
+	cudaPointerAttributes at{};
+	FG_CUDA(cudaPointerGetAttributes(&at, eng.dev().geom));
+	if (at.type != cudaMemoryTypeDevice) throw fg::Error(FG_ERR_ARG, "surface not on a device");
+	return at.device;
+}
+
 }  // namespace
 
 extern "C" FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n)
@@ -94,10 +120,9 @@ extern "C" FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n)
 		if (!s || !dst) throw fg::Error(FG_ERR_ARG, "null surface or destination");
 		std::lock_guard<std::mutex> lk(g_mu);
 		fg::EngineBase& eng = *s->eng;
+		const DeviceGuard on(surface_device(eng));
 		const fg::Dev& P = eng.dev();
-		fg::SurfGeom g;
-		FG_CUDA(cudaMemcpyAsync(&g, P.geom, sizeof(g), cudaMemcpyDeviceToHost, eng.stream()));
-		FG_CUDA(cudaStreamSynchronize(eng.stream()));
+		const fg::SurfGeom& g = eng.geometry(0);  // host copy of P.geom[0]
 		long long total = 1;
 		for (int a = 0; a < eng.dims(); a++) total *= g.size[a];
 		if (total > (long long)FG_NOALLOC_SNAPSHOT_MAX)

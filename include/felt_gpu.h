@@ -113,14 +113,16 @@ FG_API int fg_update_end(fg_surface* s);
 FG_API int fg_snapshot(fg_surface* s, float* dst, size_t n, int dst_is_device);
 
 /* Dense snapshot into a host buffer that allocates no memory. No counterpart in the reference:
- * it exists for callers that cannot allocate device memory while they run (code inside a CUDA
- * stream capture, processes whose device memory is budgeted by another allocator, real-time
- * loops that must not enter the driver's allocator). It stages through a fixed device array of
- * 2^21 floats (8 MiB) that every GPU loading this library holds until exit; grids with more
- * nodes are rejected with FG_ERR_CAPACITY. Calls share that array (each call writes all it
- * reads), are serialised by a process-wide lock and wait for their copy; calls that overlapped
- * on the GPU would race. The first call on a device looks up the array's address on that device
- * and should come before any stream capture. dst holds n >= prod(size) floats. */
+ * it exists for callers that cannot allocate device memory while they run: processes whose
+ * device memory is owned and budgeted by another allocator (a framework's caching allocator or
+ * a fixed reservation), and real-time loops that must not enter the driver's allocator, whose
+ * cudaMalloc/cudaFree can stall or synchronise the device. It stages through a fixed device
+ * array of 2^21 floats (8 MiB) that every GPU loading this library holds until exit; grids with
+ * more nodes are rejected with FG_ERR_CAPACITY. Calls share that array (each call writes all
+ * it reads), are serialised by a process-wide lock and wait for their copy; calls that
+ * overlapped on the GPU would race. The call runs on the surface's device. The first call on a
+ * device looks up the array's address on that device and should come before any stream
+ * capture. dst holds n >= prod(size) floats. */
 FG_API int fg_snapshot_noalloc(fg_surface* s, float* dst, size_t n);
 
 /* isogrid().get(pos) (include/Felt/Impl/Mixin/PartitionedMixin.hpp:594-601). */

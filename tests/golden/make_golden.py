@@ -576,7 +576,9 @@ def serial_cases(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FELT_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <reference source root> (or set FELT_REFERENCE)")
     out = dict(surface=surface_cases(root), poly=poly_cases(root),
                curvature=curvature_cases(root), numeric=numeric_cases(root), lookup=lookup_cases(root),
                multi_lookup=multi_lookup_cases(root),

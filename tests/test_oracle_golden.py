@@ -300,8 +300,11 @@ def test_oracle_determinism():
 
 def test_tables_match_reference_source():
     """The packed marching-cubes ordering table equals the reference's table, when the
-    reference source tree is available (skipped otherwise)."""
-    src = "/root/reference/include/Felt/Impl/Mixin/PolyMixin.hpp"
+    reference source tree is available: FELT_REFERENCE names its root (skipped otherwise)."""
+    root = os.environ.get("FELT_REFERENCE")
+    if not root:
+        pytest.skip("FELT_REFERENCE (the reference source tree) is not set")
+    src = os.path.join(root, "include", "Felt", "Impl", "Mixin", "PolyMixin.hpp")
     if not os.path.exists(src):
         pytest.skip("reference source tree not present")
     import re

@@ -1,6 +1,6 @@
 """fg_snapshot_noalloc: the dense snapshot for callers that cannot allocate device memory while
-they run (inside a CUDA stream capture, under another allocator's memory budget, or in a
-real-time loop that must stay out of the driver's allocator). It must return exactly what
+they run (under another allocator's memory budget, or in a real-time loop that must stay out of
+the driver's allocator). It must return exactly what
 fg_snapshot returns, on consecutive calls that share its fixed staging array, and reject grids
 larger than that array. This file is collected last so that a failure here leaves every other
 test already run."""
