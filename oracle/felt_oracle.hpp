@@ -26,38 +26,125 @@
 #include <atomic>
 #include <exception>
 #include <thread>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 
 namespace fo {
 
 /// Threads of the loops the reference runs in parallel (set through fo_set_threads; 1 = the
-/// plain sequential order, which these loops do not depend on anyway).
+/// plain sequential order). Every threaded loop below only writes state owned by its item, or
+/// records its shared edits per item and applies them afterwards in item order, so results and
+/// list orders are the same for any thread count.
 inline std::atomic<int> g_threads{1};
 
-/// fn(i) for i in [0, n): on g_threads threads taking indices in turn when the loop has enough
-/// items to pay for them, else inline. fn must only write state owned by item i.
+/// Set on the threads of a running parallel loop: a loop started from inside one runs inline.
+inline thread_local bool t_in_loop = false;
+
+/// A persistent pool of host threads for the parallel loops, started on first use (the
+/// reference's OpenMP runtime keeps its threads between regions too; starting threads per loop
+/// would cost more than these loops take).
+class ThreadPool {
+public:
+	static ThreadPool& get()
+	{
+		static ThreadPool pool;
+		return pool;
+	}
+	/// fn(i) for i in [0, n) on nt threads (the caller included), indices taken in turn.
+	template <class Fn>
+	void run(long n, int nt, Fn&& fn)
+	{
+		std::lock_guard<std::mutex> one(run_mu_);  // one parallel loop at a time
+		ensure(nt - 1);
+		std::atomic<long> next{0};
+		std::exception_ptr err;
+		std::atomic<bool> failed{false};
+		std::mutex err_mu;
+		auto body = [&] {
+			t_in_loop = true;
+			struct Clear {
+				~Clear() { t_in_loop = false; }
+			} clear;
+			try {
+				for (long i; (i = next.fetch_add(1)) < n && !failed.load();) fn(i);
+			} catch (...) {
+				std::lock_guard<std::mutex> g(err_mu);
+				if (!failed.exchange(true)) err = std::current_exception();
+			}
+		};
+		std::function<void()> job(body);
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			job_ = &job;
+			want_ = nt - 1;
+			taken_ = 0;
+			done_ = 0;
+			gen_++;
+		}
+		cv_.notify_all();
+		body();
+		{
+			std::unique_lock<std::mutex> g(mu_);
+			done_cv_.wait(g, [&] { return done_ == want_; });
+			job_ = nullptr;
+		}
+		if (err) std::rethrow_exception(err);
+	}
+	~ThreadPool()
+	{
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			stop_ = true;
+			gen_++;
+		}
+		cv_.notify_all();
+		for (auto& t : workers_) t.join();
+	}
+
+private:
+	void ensure(int n)
+	{
+		while ((int)workers_.size() < n) workers_.emplace_back([this] { loop(); });
+	}
+	void loop()
+	{
+		unsigned long long seen = 0;
+		std::unique_lock<std::mutex> g(mu_);
+		for (;;) {
+			cv_.wait(g, [&] { return stop_ || (gen_ != seen && taken_ < want_); });
+			if (stop_) return;
+			seen = gen_;
+			taken_++;
+			std::function<void()>* job = job_;
+			g.unlock();
+			(*job)();
+			g.lock();
+			if (++done_ == want_) done_cv_.notify_one();
+		}
+	}
+	std::mutex run_mu_, mu_;
+	std::condition_variable cv_, done_cv_;
+	std::vector<std::thread> workers_;
+	std::function<void()>* job_ = nullptr;
+	unsigned long long gen_ = 0;
+	int want_ = 0, taken_ = 0, done_ = 0;
+	bool stop_ = false;
+};
+
+/// fn(i) for i in [0, n) across g_threads threads. min_items is the size below which the loop
+/// runs inline: the reference's regions are parallel only from 32 active partitions
+/// (Surface.hpp:19-27), Polys::march always (Polys.hpp:140). fn must only write state owned by
+/// item i.
 template <class Fn>
-void parallel_items(long n, Fn&& fn)
+void parallel_items(long n, Fn&& fn, long min_items = 32)
 {
-	const int nt = (int)std::min<long>(g_threads.load(), n / 8);
-	if (nt <= 1) {
+	const int nt = (int)std::min<long>(g_threads.load(), n);
+	if (nt <= 1 || n < min_items || t_in_loop) {
 		for (long i = 0; i < n; i++) fn(i);
 		return;
 	}
-	std::atomic<long> next{0};
-	std::exception_ptr err;
-	std::atomic<bool> failed{false};
-	auto work = [&] {
-		try {
-			for (long i; (i = next.fetch_add(1)) < n && !failed.load();) fn(i);
-		} catch (...) {
-			if (!failed.exchange(true)) err = std::current_exception();
-		}
-	};
-	std::vector<std::thread> pool;
-	for (int t = 1; t < nt; t++) pool.emplace_back(work);
-	work();
-	for (auto& th : pool) th.join();
-	if (err) std::rethrow_exception(err);
+	ThreadPool::get().run(n, nt, fn);
 }
 
 using PosIdx = std::size_t;
@@ -720,19 +807,23 @@ public:
 		PosIdx nb = 1;
 		for (int a = 0; a < D; a++) nb *= PosIdx(box[a]);
 		update_start();
-		for (PosIdx ci = 0; ci < nb; ci++) {
-			Vi<D> pc = pos_of<D>(ci, box, zero);
+		// The reference runs the box's partitions across OpenMP threads (Surface.hpp:336): the
+		// functor values are taken per partition on one thread each, then tracked into the delta
+		// grid in the sequential order.
+		std::vector<PosIdx> pcs((size_t)nb);
+		std::vector<std::vector<std::pair<PosIdx, Real>>> vals((size_t)nb);
+		parallel_items((long)nb, [&](long ci) {
+			Vi<D> pc = pos_of<D>(PosIdx(ci), box, zero);
 			for (int a = 0; a < D; a++) pc[a] += cl[a];
 			const PosIdx pci = index_of<D>(pc, iso.ccount, iso.coff);
-			const std::vector<PosIdx> leaves = iso.ch[pci].lists[lidx(0)];
-			for (PosIdx leaf : leaves) {
+			pcs[(size_t)ci] = pci;
+			for (PosIdx leaf : iso.ch[pci].lists[lidx(0)]) {
 				const Vi<D> pos = iso.pos_leaf(pci, leaf);
-				if (inside<D>(pos, lo, lub)) {
-					const Real d = fn(pos);
-					delta_.track(d, pci, leaf, lidx(0));
-				}
+				if (inside<D>(pos, lo, lub)) vals[(size_t)ci].emplace_back(leaf, fn(pos));
 			}
-		}
+		});
+		for (size_t ci = 0; ci < (size_t)nb; ci++)
+			for (const auto& v : vals[ci]) delta_.track(v.second, pcs[ci], v.first, lidx(0));
 		update_end();
 	}
 	void update_bounded(const Vi<D>& lo, const Vi<D>& hi, const Speed& s)
@@ -833,22 +924,27 @@ public:
 		}
 	}
 
-	/// update_zero_layer (Surface.hpp:920-979).
+	/// update_zero_layer (Surface.hpp:920-979). The reference runs the partitions across OpenMP
+	/// threads (Surface.hpp:929); here each partition's new values are written by one thread and
+	/// its layer changes recorded, then the status changes are made in the sequential order.
 	void update_zero_layer(Affected& buf)
 	{
 		const int l0 = lidx(0);
 		const std::vector<PosIdx> parts = delta_.clists[l0];
-		for (PosIdx pc : parts) {
-			const std::vector<PosIdx> leaves = delta_.ch[pc].lists[l0];
-			for (PosIdx leaf : leaves) {
+		std::vector<std::vector<std::pair<PosIdx, int>>> moved(parts.size());
+		parallel_items((long)parts.size(), [&](long i) {
+			const PosIdx pc = parts[(size_t)i];
+			for (PosIdx leaf : delta_.ch[pc].lists[l0]) {
 				const Real prev = iso.cget(pc, leaf);
 				const Real d = delta_.cget(pc, leaf);
 				const Real nw = prev + d;
 				const int lid = layer_of(nw);
 				iso.cset(pc, leaf, nw);
-				status_change(pc, leaf, 0, lid, buf);
+				if (lid != 0) moved[(size_t)i].emplace_back(leaf, lid);
 			}
-		}
+		});
+		for (size_t i = 0; i < parts.size(); i++)
+			for (const auto& m : moved[i]) status_change(parts[i], m.first, 0, m.second, buf);
 	}
 
 	/// update_distance over all layers (Surface.hpp:989-1003).
@@ -877,15 +973,21 @@ public:
 				delta_.child_track(d, pc, leaf, li);
 			}
 		});
-		for (PosIdx pc : parts) {
-			const std::vector<PosIdx> leaves = g.ch[pc].lists[li];
-			for (PosIdx leaf : leaves) {
+		// second pass, across threads as the reference runs it (Surface.hpp:1075-1121): values
+		// written per partition, layer changes recorded and then made in the sequential order
+		std::vector<std::vector<std::pair<PosIdx, int>>> moved(parts.size());
+		parallel_items((long)parts.size(), [&](long i) {
+			const PosIdx pc = parts[(size_t)i];
+			for (PosIdx leaf : g.ch[pc].lists[li]) {
 				const Real d = delta_.cget(pc, leaf);
 				const int lid = layer_of(d);
 				iso.cset(pc, leaf, d);
-				changed |= status_change(pc, leaf, id, lid, buf);
+				if (lid != id) moved[(size_t)i].emplace_back(leaf, lid);
 			}
-		}
+		});
+		for (size_t i = 0; i < parts.size(); i++)
+			for (const auto& m : moved[i])
+				changed |= status_change(parts[i], m.first, id, m.second, buf);
 		return changed;
 	}
 
@@ -902,22 +1004,66 @@ public:
 		return true;
 	}
 
-	/// flush_status_change (Surface.hpp:1183-1244).
+	/// flush_status_change (Surface.hpp:1183-1244). The reference runs each from-layer's
+	/// partitions across OpenMP threads (Surface.hpp:1195), the children lookup edits under a
+	/// mutex. Here each partition's leaf edits (PGrid::retrack / untrack) run on one thread
+	/// against its own copy of its children-lookup membership, its children-lookup calls are
+	/// recorded, and the calls are then made in the sequential order (from-layer, status list
+	/// order, leaf order), so the children lists come out as the sequential loop leaves them.
 	void flush_status_change()
 	{
+		constexpr int N = NL;
 		for (int from = -L; from <= L; from++) {
 			const int lf = lidx(from);
 			const std::vector<PosIdx> parts = status.clists[lf];
-			for (PosIdx pc : parts) {
-				const std::vector<PosIdx> leaves = status.ch[pc].lists[lf];
-				for (PosIdx leaf : leaves) {
+			// recorded children-lookup calls: list index, +1 = ctrack, -1 = cuntrack
+			std::vector<std::vector<std::pair<int, int>>> calls(parts.size());
+			parallel_items((long)parts.size(), [&](long i) {
+				const PosIdx pc = parts[(size_t)i];
+				auto& rec = calls[(size_t)i];
+				std::array<bool, N> tracked;
+				for (int l = 0; l < N; l++) tracked[l] = iso.ctracked(pc, l);
+				auto ctrack = [&](int l) {
+					rec.emplace_back(l, 1);
+					tracked[l] = true;
+				};
+				auto cuntrack = [&](int l) {
+					rec.emplace_back(l, -1);
+					tracked[l] = false;
+				};
+				for (PosIdx leaf : status.ch[pc].lists[lf]) {
 					const int to = status.cget(pc, leaf);
-					if (inside_band(to, L))
-						iso.retrack(pc, leaf, lf, lidx(to));
-					else
-						iso.untrack(Real(to), pc, leaf, lf);
+					if (inside_band(to, L)) {
+						// PGrid::retrack (PartitionedMixin.hpp:519-558)
+						const int lt = lidx(to);
+						iso.luntrack(pc, leaf, lf);
+						iso.ltrack(pc, leaf, lt);
+						const bool from_empty = iso.ch[pc].lists[lf].empty();
+						if (!tracked[lt] || from_empty) {
+							ctrack(lt);
+							if (from_empty) cuntrack(lf);
+						}
+					} else {
+						// PGrid::untrack (PartitionedMixin.hpp:489-517)
+						const Real bgv = Real(to);
+						iso.luntrack(pc, leaf, lf);
+						iso.ch[pc].data[leaf] = bgv;
+						if (iso.ch[pc].lists[lf].empty()) {
+							cuntrack(lf);
+							bool any = false;
+							for (int l = 0; l < N; l++) any = any || tracked[l];
+							if (!any) iso.deactivate(pc, bgv);
+						}
+					}
 				}
-			}
+			});
+			for (size_t i = 0; i < parts.size(); i++)
+				for (const auto& c : calls[i]) {
+					if (c.second > 0)
+						iso.ctrack(parts[i], c.first);
+					else
+						iso.cuntrack(parts[i], c.first);
+				}
 		}
 	}
 
@@ -1011,17 +1157,17 @@ template <> struct Geom<3> {
 
 /// interp (NumericMixin.hpp:403-481) of a grid at a real position: corners gathered in bit
 /// order, reduced axis 0 first.
-template <int D, class Grid>
-float field_interp(const Grid& iso, const std::array<float, D>& p)
+template <int D, class Grid, class Real>
+Real field_interp(const Grid& iso, const std::array<Real, D>& p)
 {
 	Vi<D> fl;
-	std::array<float, D> pc;
+	std::array<Real, D> pc;
 	for (int ax = 0; ax < D; ax++) {
-		const float f = std::floor(p[ax]);
+		const Real f = std::floor(p[ax]);
 		fl[ax] = int(f);
 		pc[ax] = p[ax] - f;
 	}
-	float v[1 << D];
+	Real v[1 << D];
 	for (int i = 0; i < (1 << D); i++) {
 		Vi<D> q = fl;
 		for (int ax = 0; ax < D; ax++) q[ax] += (i >> ax) & 1;
@@ -1030,10 +1176,10 @@ float field_interp(const Grid& iso, const std::array<float, D>& p)
 	int n = 1 << D;
 	while (n > 1) {
 		const int axis = D - __builtin_ctz(unsigned(n));
-		const float t = pc[axis];
+		const Real t = pc[axis];
 		for (int i = 0; i < n / 2; i++) {
-			const float lo = v[2 * i], hi = v[2 * i + 1];
-			v[i] = t * hi + (1.0f - t) * lo;
+			const Real lo = v[2 * i], hi = v[2 * i + 1];
+			v[i] = t * hi + (Real(1) - t) * lo;
 		}
 		n >>= 1;
 	}
@@ -1042,14 +1188,14 @@ float field_interp(const Grid& iso, const std::array<float, D>& p)
 
 /// grad (NumericMixin.hpp:188-231) at a real position: the probe coordinate is stepped -1, +2,
 /// -1 in float, so it can drift by rounding, exactly as in the reference.
-template <int D, class Grid>
-std::array<float, D> field_grad_f(const Grid& iso, const std::array<float, D>& p)
+template <int D, class Grid, class Real>
+std::array<Real, D> field_grad_f(const Grid& iso, const std::array<Real, D>& p)
 {
-	std::array<float, D> g;
-	const float centre = field_interp<D>(iso, p);
-	std::array<float, D> t = p;
+	std::array<Real, D> g;
+	const Real centre = field_interp<D>(iso, p);
+	std::array<Real, D> t = p;
 	for (int ax = 0; ax < D; ax++) {
-		float back = centre, fwd = centre;
+		Real back = centre, fwd = centre;
 		int order = 0;
 		t[ax] -= 1;
 		if (inside<D>(t, iso.off, iso.hi)) {
@@ -1062,9 +1208,9 @@ std::array<float, D> field_grad_f(const Grid& iso, const std::array<float, D>& p
 			order++;
 		}
 		t[ax] -= 1;
-		g[ax] = order != 0 ? (fwd - back) / float(order) : 0.0f;
+		g[ax] = order != 0 ? (fwd - back) / Real(order) : Real(0);
 	}
-	for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
+	for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / Real(1);
 	return g;
 }
 
@@ -1125,29 +1271,32 @@ void field_numeric(const Grid& iso, const std::array<float, D>& p, float* out)
 }
 
 /// Eigen normalize(): divide by sqrt(x0^2 + (x1^2 + x2^2)) when that is positive.
-template <int D>
-void eigen_normalize(std::array<float, D>& v)
+template <int D, class Real = float>
+void eigen_normalize(std::array<Real, D>& v)
 {
-	std::array<float, D> sq;
+	std::array<Real, D> sq;
 	for (int ax = 0; ax < D; ax++) sq[ax] = v[ax] * v[ax];
-	const float z = eigen_sum<float, D>(sq);
+	const Real z = eigen_sum<Real, D>(sq);
 	if (z > 0) {
-		const float r = std::sqrt(z);
+		const Real r = std::sqrt(z);
 		for (int ax = 0; ax < D; ax++) v[ax] = v[ax] / r;
 	}
 }
 
-template <int D>
+template <int D, class Real = float>
 struct Vertex {
-	std::array<float, D> pos;
-	std::array<float, D> norm;  // 3D only
+	std::array<Real, D> pos;
+	std::array<Real, D> norm;  // 3D only
 };
 
-/// Polys<Surface> (Polys.hpp:1-229) over Poly::Single children (Poly.hpp:17-368).
-template <int D, int L>
+/// Polys<Surface> (Polys.hpp:1-229) over Poly::Single children (Poly.hpp:17-368). Real is
+/// the surface's arithmetic type: float as in the reference, double for the FP64 run of the
+/// same method that error figures are taken against.
+template <int D, int L, class Real = float>
 class Polys {
 public:
-	using Surf = Surface<D, L, float>;
+	using Surf = Surface<D, L, Real>;
+	using V = Vertex<D, Real>;
 	static constexpr int NL = Surf::NL;
 	using IdxTuple = std::array<std::size_t, D>;
 
@@ -1156,7 +1305,7 @@ public:
 		std::vector<IdxTuple> cache;  // empty when inactive
 		std::vector<std::size_t> lkp;
 		std::vector<std::size_t> list;
-		std::vector<Vertex<D>> vtxs;
+		std::vector<V> vtxs;
 		std::vector<std::array<unsigned, D>> spxs;
 		bool active() const { return !cache.empty(); }
 	};
@@ -1233,7 +1382,11 @@ public:
 	/// march (Polys.hpp:138-165).
 	void march()
 	{
-		for (std::size_t pc : pend->list) {
+		// across threads as in the reference (Polys.hpp:140): each pending partition's child is
+		// its own state, and marching only reads the surface
+		const std::vector<std::size_t>& todo = pend->list;
+		parallel_items((long)todo.size(), [&](long i) {
+			const std::size_t pc = todo[(size_t)i];
 			Single& c = ch[pc];
 			if (s->iso.active(pc)) {
 				if (c.active())
@@ -1244,7 +1397,7 @@ public:
 			} else if (c.active()) {
 				deactivate(c);
 			}
-		}
+		}, 1);
 		std::swap(pend, done);
 		pend->reset();
 	}
@@ -1305,7 +1458,7 @@ public:
 		std::vector<IdxTuple>().swap(c.cache);
 		std::vector<std::size_t>().swap(c.lkp);
 		std::vector<std::size_t>().swap(c.list);
-		std::vector<Vertex<D>>().swap(c.vtxs);
+		std::vector<V>().swap(c.vtxs);
 		std::vector<std::array<unsigned, D>>().swap(c.spxs);
 	}
 
@@ -1328,7 +1481,7 @@ public:
 			const Vi<D> co = Geom<D>::corner(i);
 			Vi<D> p;
 			for (int ax = 0; ax < D; ax++) p[ax] = pcalc[ax] + co[ax];
-			const float v = s->iso.get(p);
+			const Real v = s->iso.get(p);
 			mask = mask | (unsigned(v > 0) << i);
 		}
 		const unsigned emask = Geom<D>::edge_mask(int(mask));
@@ -1357,24 +1510,24 @@ public:
 		if (cached != NUL) return cached;
 		Vi<D> pb = pa;
 		pb[axis] += 1;
-		const float va = s->iso.get(pa);
-		const float vb = s->iso.get(pb);
-		const float eps = std::numeric_limits<float>::epsilon();
-		Vertex<D> vtx;
+		const Real va = s->iso.get(pa);
+		const Real vb = s->iso.get(pb);
+		const Real eps = Real(std::numeric_limits<float>::epsilon());
+		V vtx;
 		if (std::fabs(va) <= eps) {
 			vtx = make_vertex_i(pa);
 		} else if (std::fabs(vb) <= eps) {
 			vtx = make_vertex_i(pb);
 		} else {
-			float mu;
+			Real mu;
 			if (std::fabs(va - vb) <= eps)
-				mu = 0.5f;
+				mu = Real(0.5);
 			else
 				mu = va / (va - vb);
-			std::array<float, D> vc;
+			std::array<Real, D> vc;
 			for (int ax = 0; ax < D; ax++) {
-				const float fa = float(pa[ax]);
-				const float fb = float(pb[ax]);
+				const Real fa = Real(pa[ax]);
+				const Real fb = Real(pb[ax]);
 				vc[ax] = fa + (fb - fa) * mu;
 			}
 			vtx = make_vertex_f(vc);
@@ -1391,16 +1544,16 @@ public:
 
 	// --- 3D vertex normals: Vertex ctor (PolyMixin.hpp:142-148) ---
 
-	float interp(const std::array<float, D>& p) const { return field_interp<D>(s->iso, p); }
+	Real interp(const std::array<Real, D>& p) const { return field_interp<D>(s->iso, p); }
 
 	/// grad (NumericMixin.hpp:188-231) at an integer position.
-	std::array<float, D> grad_i(const Vi<D>& p) const
+	std::array<Real, D> grad_i(const Vi<D>& p) const
 	{
-		std::array<float, D> g;
-		const float centre = s->iso.get(p);
+		std::array<Real, D> g;
+		const Real centre = s->iso.get(p);
 		Vi<D> t = p;
 		for (int ax = 0; ax < D; ax++) {
-			float back = centre, fwd = centre;
+			Real back = centre, fwd = centre;
 			int order = 0;
 			t[ax] -= 1;
 			if (s->iso.in_grid(t)) {
@@ -1413,37 +1566,37 @@ public:
 				order++;
 			}
 			t[ax] -= 1;
-			g[ax] = order != 0 ? (fwd - back) / float(order) : 0.0f;
+			g[ax] = order != 0 ? (fwd - back) / Real(order) : Real(0);
 		}
-		for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / 1.0f;
+		for (int ax = 0; ax < D; ax++) g[ax] = g[ax] / Real(1);
 		return g;
 	}
-	std::array<float, D> grad_f(const std::array<float, D>& p) const
+	std::array<Real, D> grad_f(const std::array<Real, D>& p) const
 	{
 		return field_grad_f<D>(s->iso, p);
 	}
-	static void normalize(std::array<float, D>& v) { eigen_normalize<D>(v); }
-	Vertex<D> make_vertex_i(const Vi<D>& p) const
+	static void normalize(std::array<Real, D>& v) { eigen_normalize<D, Real>(v); }
+	V make_vertex_i(const Vi<D>& p) const
 	{
-		Vertex<D> v;
-		for (int ax = 0; ax < D; ax++) v.pos[ax] = float(p[ax]);
+		V v;
+		for (int ax = 0; ax < D; ax++) v.pos[ax] = Real(p[ax]);
 		if (D == 3) {
 			v.norm = grad_i(p);
 			normalize(v.norm);
 		} else {
-			v.norm.fill(0.0f);
+			v.norm.fill(Real(0));
 		}
 		return v;
 	}
-	Vertex<D> make_vertex_f(const std::array<float, D>& p) const
+	V make_vertex_f(const std::array<Real, D>& p) const
 	{
-		Vertex<D> v;
+		V v;
 		v.pos = p;
 		if (D == 3) {
 			v.norm = grad_f(p);
 			normalize(v.norm);
 		} else {
-			v.norm.fill(0.0f);
+			v.norm.fill(Real(0));
 		}
 		return v;
 	}

@@ -40,6 +40,9 @@ struct SurfBase {
 	virtual void save(std::vector<uint8_t>& out) = 0;
 	virtual void geometry(int* size, int* part) = 0;
 	virtual void load(const uint8_t* p, size_t n) = 0;
+	/// The dense snapshot in the surface's own arithmetic type, widened to double.
+	virtual void snapshot64(double* dst, size_t n) = 0;
+	virtual bool fp64() const = 0;
 };
 
 struct PolysBase {
@@ -52,11 +55,19 @@ struct PolysBase {
 	virtual void part(size_t pc, float* vtx, size_t vcap, uint32_t* spx, size_t scap, size_t* nv,
 	                  size_t* ns, int* active) = 0;
 	virtual void totals(size_t* nv, size_t* ns) = 0;
+	/// part() with the vertices in the surface's own arithmetic type, widened to double.
+	virtual void part64(size_t pc, double* vtx, size_t vcap, size_t* nv) = 0;
 };
 
-template <int D, int L>
+/// One oracle surface. Real = float is the reference's arithmetic; Real = double is the FP64
+/// run of the same method (the reference hard-wires float, Impl/Common.hpp:40), which error
+/// figures are taken against. Raycasting, surface files and the real-position Numeric API exist
+/// for float surfaces only.
+template <int D, int L, class Real = float>
 struct Surf : SurfBase {
-	fo::Surface<D, L, float> s;
+	fo::Surface<D, L, Real> s;
+	static constexpr bool F32 = std::is_same<Real, float>::value;
+	[[noreturn]] static void f32_only() { throw fo::Error(-1, "not available in an FP64 run"); }
 	static fo::Vi<D> v(const int* p)
 	{
 		fo::Vi<D> r;
@@ -84,9 +95,18 @@ struct Surf : SurfBase {
 		size_t tot = 1;
 		for (int a = 0; a < D; a++) tot *= size_t(size[a]);
 		if (n < tot) throw fo::Error(-13, "snapshot buffer too small");
-		for (size_t i = 0; i < tot; i++) dst[i] = s.iso.get(fo::pos_of<D>(i, size, off));
+		for (size_t i = 0; i < tot; i++) dst[i] = float(s.iso.get(fo::pos_of<D>(i, size, off)));
 	}
-	float get(const int* p) override { return s.iso.get(v(p)); }
+	void snapshot64(double* dst, size_t n) override
+	{
+		fo::Vi<D> size = s.iso.size, off = s.iso.off;
+		size_t tot = 1;
+		for (int a = 0; a < D; a++) tot *= size_t(size[a]);
+		if (n < tot) throw fo::Error(-13, "snapshot buffer too small");
+		for (size_t i = 0; i < tot; i++) dst[i] = double(s.iso.get(fo::pos_of<D>(i, size, off)));
+	}
+	bool fp64() const override { return !F32; }
+	float get(const int* p) override { return float(s.iso.get(v(p))); }
 	size_t nparts() override { return s.iso.nchildren(); }
 	void partitions(int* csize, int* coff) override
 	{
@@ -116,7 +136,7 @@ struct Surf : SurfBase {
 	void pstate(size_t part, int* active, float* bg) override
 	{
 		*active = s.iso.active(part) ? 1 : 0;
-		*bg = s.iso.ch[part].bg;
+		*bg = float(s.iso.ch[part].bg);
 	}
 	void stats(size_t* a, size_t* b) override
 	{
@@ -130,15 +150,30 @@ struct Surf : SurfBase {
 			for (size_t pc : s.iso.clists[l]) n += s.iso.ch[pc].lists[l].size();
 		return n;
 	}
-	void curv(const int* p, float* out) override { *out = s.curv(v(p)); }
-	void numeric(const int* p, float* out) override { s.numeric(v(p), out); }
+	void curv(const int* p, float* out) override { *out = float(s.curv(v(p))); }
+	void numeric(const int* p, float* out) override
+	{
+		Real r[5 * D + 1];
+		s.numeric(v(p), r);
+		for (int i = 0; i < 5 * D + 1; i++) out[i] = float(r[i]);
+	}
 	void numeric_f(const float* p, float* out) override
 	{
-		std::array<float, D> q;
-		for (int a = 0; a < D; a++) q[a] = p[a];
-		fo::field_numeric<D>(s.iso, q, out);
+		if constexpr (F32) {
+			std::array<float, D> q;
+			for (int a = 0; a < D; a++) q[a] = p[a];
+			fo::field_numeric<D>(s.iso, q, out);
+		} else {
+			f32_only();
+		}
 	}
-	void save(std::vector<uint8_t>& out) override { fo::save_surface<D, L>(s, out); }
+	void save(std::vector<uint8_t>& out) override
+	{
+		if constexpr (F32)
+			fo::save_surface<D, L>(s, out);
+		else
+			f32_only();
+	}
 	void geometry(int* size, int* part) override
 	{
 		for (int a = 0; a < D; a++) {
@@ -146,23 +181,33 @@ struct Surf : SurfBase {
 			part[a] = s.iso.csize[a];
 		}
 	}
-	void load(const uint8_t* p, size_t n) override { fo::load_surface<D, L>(s, p, n); }
+	void load(const uint8_t* p, size_t n) override
+	{
+		if constexpr (F32)
+			fo::load_surface<D, L>(s, p, n);
+		else
+			f32_only();
+	}
 	void ray(const float* o, const float* d, float* out) override
 	{
-		std::array<float, D> oo, dd;
-		for (int a = 0; a < D; a++) {
-			oo[a] = o[a];
-			dd[a] = d[a];
+		if constexpr (F32) {
+			std::array<float, D> oo, dd;
+			for (int a = 0; a < D; a++) {
+				oo[a] = o[a];
+				dd[a] = d[a];
+			}
+			const auto h = fo::Raycast<D, L>(s).ray(oo, dd);
+			for (int a = 0; a < D; a++) out[a] = h[a];
+		} else {
+			f32_only();
 		}
-		const auto h = fo::Raycast<D, L>(s).ray(oo, dd);
-		for (int a = 0; a < D; a++) out[a] = h[a];
 	}
 };
 
-template <int D, int L>
+template <int D, int L, class Real = float>
 struct PolysImpl : PolysBase {
-	fo::Polys<D, L> p;
-	explicit PolysImpl(const fo::Surface<D, L, float>& s) : p(s) {}
+	fo::Polys<D, L, Real> p;
+	explicit PolysImpl(const fo::Surface<D, L, Real>& s) : p(s) {}
 	void notify() override { p.notify(); }
 	void march() override { p.march(); }
 	void invalidate() override { p.invalidate(); }
@@ -177,12 +222,23 @@ struct PolysImpl : PolysBase {
 		*active = c.active() ? 1 : 0;
 		const size_t per = (D == 3) ? 2 * D : D;
 		for (size_t i = 0; i < c.vtxs.size() && (i + 1) * per <= vcap; i++) {
-			for (int a = 0; a < D; a++) vtx[i * per + a] = c.vtxs[i].pos[a];
+			for (int a = 0; a < D; a++) vtx[i * per + a] = float(c.vtxs[i].pos[a]);
 			if (D == 3)
-				for (int a = 0; a < D; a++) vtx[i * per + D + a] = c.vtxs[i].norm[a];
+				for (int a = 0; a < D; a++) vtx[i * per + D + a] = float(c.vtxs[i].norm[a]);
 		}
 		for (size_t i = 0; i < c.spxs.size() && (i + 1) * D <= scap; i++)
 			for (int a = 0; a < D; a++) spx[i * D + a] = c.spxs[i][a];
+	}
+	void part64(size_t pc, double* vtx, size_t vcap, size_t* nv) override
+	{
+		const auto& c = p.ch[pc];
+		*nv = c.vtxs.size();
+		const size_t per = (D == 3) ? 2 * D : D;
+		for (size_t i = 0; i < c.vtxs.size() && (i + 1) * per <= vcap; i++) {
+			for (int a = 0; a < D; a++) vtx[i * per + a] = double(c.vtxs[i].pos[a]);
+			if (D == 3)
+				for (int a = 0; a < D; a++) vtx[i * per + D + a] = double(c.vtxs[i].norm[a]);
+		}
 	}
 	void totals(size_t* nv, size_t* ns) override
 	{
@@ -214,10 +270,13 @@ int guard(F&& f)
 	}
 }
 
-SurfBase* make(int D, int L, const int* size, const int* part)
+SurfBase* make(int D, int L, const int* size, const int* part, bool fp64 = false)
 {
-#define FO_CASE(d, l) \
-	if (D == d && L == l) return new Surf<d, l>(size, part);
+#define FO_CASE(d, l)                                                          \
+	if (D == d && L == l) {                                                    \
+		if (fp64) return new Surf<d, l, double>(size, part);                   \
+		return new Surf<d, l>(size, part);                                     \
+	}
 	FO_CASE(2, 1) FO_CASE(2, 2) FO_CASE(2, 3) FO_CASE(2, 4)
 	FO_CASE(3, 1) FO_CASE(3, 2) FO_CASE(3, 3) FO_CASE(3, 4)
 #undef FO_CASE
@@ -226,8 +285,11 @@ SurfBase* make(int D, int L, const int* size, const int* part)
 
 PolysBase* make_polys(SurfBase* s)
 {
-#define FO_CASE(d, l) \
-	if (s->dims == d && s->layers == l) return new PolysImpl<d, l>(static_cast<Surf<d, l>*>(s)->s);
+#define FO_CASE(d, l)                                                                         \
+	if (s->dims == d && s->layers == l) {                                                     \
+		if (s->fp64()) return new PolysImpl<d, l, double>(static_cast<Surf<d, l, double>*>(s)->s); \
+		return new PolysImpl<d, l>(static_cast<Surf<d, l>*>(s)->s);                           \
+	}
 	FO_CASE(2, 1) FO_CASE(2, 2) FO_CASE(2, 3) FO_CASE(2, 4)
 	FO_CASE(3, 1) FO_CASE(3, 2) FO_CASE(3, 3) FO_CASE(3, 4)
 #undef FO_CASE
@@ -298,7 +360,7 @@ struct fo_speed {
 
 const char* fo_last_error(void) { return g_err.c_str(); }
 
-/// Threads of the parallel loops (the functor loop and the first distance pass); results do not
+/// Threads of the parallel loops (the reference's seven OpenMP loops); results do not
 /// depend on it. Returns the count in effect.
 int fo_set_threads(int n)
 {
@@ -313,6 +375,21 @@ int fo_surface_create(int dims, int layers, const int* size, const int* part, vo
 		if (!s) throw fo::Error(-1, "unsupported dims/layers");
 		*out = s;
 	});
+}
+/* The same surface computed in FP64 (Real = double): the method's error figures are taken
+ * against it. Lists, dumps and polygons work as for fo_surface_create; raycasting, surface
+ * files and the real-position Numeric API do not. */
+int fo_surface_create64(int dims, int layers, const int* size, const int* part, void** out)
+{
+	return guard([&] {
+		SurfBase* s = make(dims, layers, size, part, true);
+		if (!s) throw fo::Error(-1, "unsupported dims/layers");
+		*out = s;
+	});
+}
+int fo_snapshot64(void* s, double* dst, size_t n)
+{
+	return guard([&] { static_cast<SurfBase*>(s)->snapshot64(dst, n); });
 }
 /* Surface::save (Surface.hpp:180-183): the surface file, min(n, cap) bytes into buf, the
  * full length in *n. */
@@ -747,6 +824,12 @@ int fo_polys_partition(void* p, size_t part, float* vtx, size_t vcap, uint32_t* 
 {
 	return guard(
 	    [&] { static_cast<PolysBase*>(p)->part(part, vtx, vcap, spx, scap, nv, ns, active); });
+}
+/* fo_polys_partition's vertices (position then, in 3D, normal) as doubles, in the surface's own
+ * arithmetic (FP64 for an fo_surface_create64 surface). */
+int fo_polys_partition64(void* p, size_t part, double* vtx, size_t vcap, size_t* nv)
+{
+	return guard([&] { static_cast<PolysBase*>(p)->part64(part, vtx, vcap, nv); });
 }
 int fo_polys_totals(void* p, size_t* nv, size_t* ns)
 {

@@ -47,8 +47,10 @@ def lib():
 
 
 def set_threads(n):
-    """Threads of the oracle's parallel loops (the speed functor loop and the first distance
-    pass, which the reference runs with OpenMP). Returns the count in effect."""
+    """Threads of the oracle's parallel loops: the seven loops the reference runs with OpenMP
+    (the speed functor loops of the global and bounded update, the zero-layer update, both
+    distance passes, the status-change flush and Polys::march). Results and list orders do not
+    depend on it. Returns the count in effect."""
     return int(lib().fo_set_threads(int(n)))
 
 
@@ -73,15 +75,20 @@ def _fetch_list(fn, *args):
 
 
 class Surface:
-    """Oracle Surface<D,L>(size, part) with the same call surface as felt_b200.Surface."""
+    """Oracle Surface<D,L>(size, part) with the same call surface as felt_b200.Surface.
 
-    def __init__(self, size, part, layers):
+    fp64=True runs the same method with distances in double precision (the reference hard-wires
+    float, include/Felt/Impl/Common.hpp:40): the run error figures are taken against."""
+
+    def __init__(self, size, part, layers, fp64=False):
         self.D = len(size)
         self.L = layers
         self.size = tuple(int(s) for s in size)
         self.part = tuple(int(p) for p in part)
+        self.fp64 = bool(fp64)
         h = C.c_void_p()
-        _chk(lib().fo_surface_create(self.D, self.L, _ivec(size), _ivec(part), C.byref(h)))
+        make = lib().fo_surface_create64 if fp64 else lib().fo_surface_create
+        _chk(make(self.D, self.L, _ivec(size), _ivec(part), C.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -127,6 +134,14 @@ class Surface:
         n = int(np.prod(self.size))
         out = np.zeros(n, dtype=np.float32)
         _chk(lib().fo_snapshot(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), C.c_size_t(n)))
+        return out.reshape(self.size)
+
+    def snapshot64(self):
+        """The dense snapshot in the surface's own arithmetic, as float64."""
+        n = int(np.prod(self.size))
+        out = np.zeros(n, dtype=np.float64)
+        _chk(lib().fo_snapshot64(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                 C.c_size_t(n)))
         return out.reshape(self.size)
 
     def get(self, pos):
@@ -298,8 +313,63 @@ class Polys:
         return (vtx[: nv.value * per].reshape(nv.value, per), spx[: ns.value * D].reshape(
             ns.value, D), bool(act.value))
 
+    def partition64(self, part):
+        """partition()'s vertices in the surface's own arithmetic, as float64 rows."""
+        D = self.surface.D
+        per = 2 * D if D == 3 else D
+        nv = C.c_size_t()
+        _chk(lib().fo_polys_partition64(self._h, C.c_size_t(part), None, C.c_size_t(0),
+                                        C.byref(nv)))
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float64)
+        _chk(lib().fo_polys_partition64(self._h, C.c_size_t(part),
+                                        vtx.ctypes.data_as(C.POINTER(C.c_double)),
+                                        C.c_size_t(vtx.size), C.byref(nv)))
+        return vtx[: nv.value * per].reshape(nv.value, per)
+
     def totals(self):
         nv = C.c_size_t()
         ns = C.c_size_t()
         _chk(lib().fo_polys_totals(self._h, C.byref(nv), C.byref(ns)))
         return nv.value, ns.value
+
+
+FLT_EPS = float(np.finfo(np.float32).eps)
+
+
+def layer_ids(phi):
+    """Surface::layer_id of every value (Surface.hpp:1694-1697): round(v + FLT_EPSILON), halves
+    away from zero."""
+    x = np.asarray(phi, dtype=np.float64) + FLT_EPS
+    return (np.sign(x) * np.floor(np.abs(x) + 0.5)).astype(np.int64)
+
+
+def fp64_errors(snap32, snap64, L, polys=()):
+    """Error of an FP32 result against the FP64 run of the same method.
+
+    phi: max |phi32 - phi64| over the nodes whose layer is the same in both runs and inside the
+    band (|layer| <= L), with the count of such nodes and of nodes whose layer differs.
+    vertices: polys yields (vtx32, spx32, vtx64, spx64) per partition; over the partitions with
+    identical simplices (same topology) the max difference of positions and, in 3D, of normals."""
+    a = np.asarray(snap32, dtype=np.float64)
+    b = np.asarray(snap64, dtype=np.float64)
+    la, lb = layer_ids(a), layer_ids(b)
+    band = (np.abs(la) <= L) | (np.abs(lb) <= L)
+    same = band & (la == lb)
+    out = {"phi_max_abs": float(np.abs(a - b)[same].max()) if same.any() else 0.0,
+           "phi_nodes": int(same.sum()), "layer_differs": int((band & (la != lb)).sum())}
+    vmax = nmax = 0.0
+    nparts = ndiff = 0
+    for v32, s32, v64, s64 in polys:
+        if s32.shape != s64.shape or not np.array_equal(s32, s64) or v32.shape != v64.shape:
+            ndiff += 1
+            continue
+        nparts += 1
+        if v32.size:
+            d = np.abs(np.asarray(v32, dtype=np.float64) - v64)
+            D = s32.shape[1] if s32.ndim == 2 and s32.shape[1] else (v32.shape[1] // 2)
+            vmax = max(vmax, float(d[:, :D].max()))
+            if v32.shape[1] > D:
+                nmax = max(nmax, float(d[:, D:].max()))
+    out.update({"vertex_max_abs": vmax, "normal_max_abs": nmax, "poly_partitions": nparts,
+                "poly_topology_differs": ndiff})
+    return out

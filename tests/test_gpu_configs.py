@@ -1,0 +1,210 @@
+"""Parity at the benchmark configurations' own sizes, with the error against an FP64 run.
+
+The device engine is compared with the oracle on the workloads the benchmark times:
+  * the plain 512^3 surface (16^3 partitions, L=3): expanded by 100 steps of speed -1, then 5
+    steps of -0.2*curv + 0.1*hash_noise with Polys::notify each step and Polys::march after the
+    5th (the same 32768-partition grid, automatic brick pool and arena growth as the bench);
+  * the first 16 surfaces of the 4096-surface 2D batch and the first 8 of the 256-surface 3D
+    batch, drawn by the benchmark's own seeded generator, through the batch API at their real
+    sizes, speeds and step counts;
+  * the 64^3 surface of 50 steps at -0.5 with marching cubes at the end.
+Lists, orders, partition lists and simplex index triplets are bit-exact; distances and vertex
+positions within 1e-5. Each test also runs the oracle in FP64 (the same method with double
+distances) and checks the FP32 result's error against it: max |phi32 - phi64| over nodes of
+equal layer membership, max vertex position and normal error over partitions of equal topology.
+With FELT_FP64_REPORT set, the figures are appended there as JSON lines."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.dumps import first_difference
+
+pytestmark = pytest.mark.gpu
+
+PHI_TOL = 1e-5
+VTX_TOL = 1e-5
+# The FP32 method's error against its FP64 run is stated (FELT_FP64_REPORT), not bounded
+# tightly: it is ~1e-7..1e-6 for smooth speeds and can reach ~1e-3 where curvature of a
+# noise-roughened surface amplifies rounding (vertices, interpolated between nearly equal
+# values, move further). A layer the FP32 run gets wrong is counted as a membership
+# difference. These bounds only catch a broken FP64 run.
+FP64_PHI_BOUND = 0.05
+FP64_VTX_BOUND = 0.5
+
+
+def _fb():
+    import felt_b200
+    return felt_b200
+
+
+def _report(name, errs):
+    path = os.environ.get("FELT_FP64_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(dict(test=name, **errs)) + "\n")
+
+
+def _polys_pairs(n_parts, dev_part, o32, o64):
+    """Per partition: device geometry checked against the FP32 oracle's (simplices exact,
+    vertices within VTX_TOL); yields (device vertices, simplices, FP64 vertices, simplices)."""
+    for pc in range(n_parts):
+        gv, gs, ga = dev_part(pc)
+        ov, os_, oa = o32.partition(pc)
+        assert ga == oa, f"partition {pc} active"
+        assert np.array_equal(gs, os_), f"partition {pc} simplices"
+        if ov.size:
+            err = float(np.abs(gv - ov).max())
+            assert err <= VTX_TOL, f"partition {pc} vertices: {err}"
+        v64 = o64.partition64(pc)
+        _, s64, _ = o64.partition(pc)
+        yield gv, gs, v64, s64
+
+
+def _check_fp64(name, snap, o64, L, pairs):
+    errs = O.fp64_errors(snap, o64.snapshot64(), L, pairs)
+    _report(name, errs)
+    assert errs["phi_max_abs"] <= FP64_PHI_BOUND, errs
+    assert errs["vertex_max_abs"] <= FP64_VTX_BOUND, errs
+    return errs
+
+
+def test_c2_512cubed_full_size():
+    fb = _fb()
+    O.set_threads(os.cpu_count() or 1)  # order-independent: results equal the 1-thread run
+    size, part, L = (512, 512, 512), (16, 16, 16), 3
+    g = fb.Surface(size, part, L)
+    o = O.Surface(size, part, L)
+    o64 = O.Surface(size, part, L, fp64=True)
+    gp, op, op64 = fb.Polys(g), O.Polys(o), O.Polys(o64)
+    for s in (g, o, o64):
+        s.seed((0, 0, 0))
+    for _ in range(100):
+        g.update(c=-1.0)
+    o.run_steps(100, c=-1.0)
+    o64.run_steps(100, c=-1.0)
+    speed = dict(a=-0.2, n=0.1, seed=1234)
+    for k in range(5):
+        for s, p in ((g, gp), (o, op), (o64, op64)):
+            s.update(**speed)
+            p.notify()
+    for p in (gp, op, op64):
+        p.march()
+    d = first_difference(g.dump(), o.dump())
+    assert d is None, d
+    snap = g.snapshot()
+    err = float(np.abs(snap - o.snapshot()).max())
+    assert err <= PHI_TOL, err
+    assert gp.changes() == op.changes()
+    n = o.partitions()[0]
+    pairs = list(_polys_pairs(n, gp.partition, op, op64))
+    errs = _check_fp64("c2_512cubed", snap, o64, L, pairs)
+    assert g.band_size() > 300_000  # the band of the r~100 sphere, not a degenerate run
+    assert errs["phi_nodes"] > 300_000
+
+
+def _batch_config(name, k, steps, march_every, march_end):
+    import bench
+    fb = _fb()
+    O.set_threads(os.cpu_count() or 1)
+    cfg = bench.CONFIGS[name]
+    sizes, centres, speeds = bench.batch_surfaces(name, cfg)
+    sizes, centres, speeds = sizes[:k], centres[:k], speeds[:k]
+    L, part = cfg["L"], cfg["part"]
+    b = fb.Batch(sizes, part, L)
+    b.seed(centres)
+    sp = b.speed_array(speeds)
+    runs = []
+    for sz, c in zip(sizes, centres):
+        o, o64 = O.Surface(sz, part, L), O.Surface(sz, part, L, fp64=True)
+        o.seed(c)
+        o64.seed(c)
+        runs.append([o, O.Polys(o), o64, O.Polys(o64), False, False])
+    for i in range(steps):
+        b.update(sp)
+        b.polys_notify()
+        march = (march_every and (i + 1) % march_every == 0) or (march_end and i == steps - 1)
+        for j, r in enumerate(runs):
+            if r[4]:
+                continue
+            try:
+                r[0].update(**speeds[j])
+            except O.OracleError as e:  # the oscillation stop: the batch stops it too
+                assert e.code == -14
+                r[4] = True
+                continue
+            r[1].notify()
+            if march:
+                r[1].march()
+            if r[5]:
+                continue
+            try:
+                r[2].update(**speeds[j])
+            except O.OracleError as e:  # the FP64 run oscillates where the FP32 one does not
+                assert e.code == -14
+                r[5] = True
+                continue
+            r[3].notify()
+            if march:
+                r[3].march()
+        if march:
+            b.polys_march()
+    worst = dict(phi_max_abs=0.0, vertex_max_abs=0.0, normal_max_abs=0.0, layer_differs=0,
+                 poly_topology_differs=0)
+    for j, (o, op, o64, op64, stopped, stopped64) in enumerate(runs):
+        assert b.stopped(j) == stopped, f"surface {j} stopped"
+        if stopped:  # both stopped it in the same update; the states at the stop are not compared
+            continue
+        d = first_difference(b.dump(j), o.dump())
+        assert d is None, f"surface {j} {sizes[j]}: {d}"
+        snap = b.snapshot(j)
+        err = float(np.abs(snap - o.snapshot()).max())
+        assert err <= PHI_TOL, f"surface {j}: {err}"
+        pairs = list(_polys_pairs(o.partitions()[0], lambda pc: b.polys_partition(j, pc), op,
+                                  op64))
+        if stopped64:
+            continue
+        errs = O.fp64_errors(snap, o64.snapshot64(), L, pairs)
+        for key in worst:
+            worst[key] = max(worst[key], errs[key])
+    _report(f"{name}_first{k}", worst)
+    assert worst["phi_max_abs"] <= FP64_PHI_BOUND, worst
+    assert worst["vertex_max_abs"] <= FP64_VTX_BOUND, worst
+
+
+def test_c3_first16_surfaces_of_the_batch():
+    """The 2D batch (edges 128..1024, 16^2 partitions, constant speeds), 100 steps, marching
+    squares every step."""
+    _batch_config("c3", 16, 100, 1, False)
+
+
+def test_c4_first8_surfaces_of_the_batch():
+    """The 3D batch (edges 32..128, 8^3 partitions, -0.3*curv + c), 100 steps, marching cubes
+    at the end."""
+    _batch_config("c4", 8, 100, 0, True)
+
+
+def test_c1_with_marching_cubes():
+    fb = _fb()
+    size, part, L = (64, 64, 64), (8, 8, 8), 2
+    g, o, o64 = fb.Surface(size, part, L), O.Surface(size, part, L), O.Surface(size, part, L,
+                                                                               fp64=True)
+    gp, op, op64 = fb.Polys(g), O.Polys(o), O.Polys(o64)
+    for s in (g, o, o64):
+        s.seed((0, 0, 0))
+    for _ in range(50):
+        for s, p in ((g, gp), (o, op), (o64, op64)):
+            s.update(c=-0.5)
+            p.notify()
+    for p in (gp, op, op64):
+        p.march()
+    d = first_difference(g.dump(), o.dump())
+    assert d is None, d
+    snap = g.snapshot()
+    assert float(np.abs(snap - o.snapshot()).max()) <= PHI_TOL
+    assert gp.changes() == op.changes()
+    assert gp.totals() == op.totals()
+    pairs = list(_polys_pairs(o.partitions()[0], gp.partition, op, op64))
+    _check_fp64("c1_64cubed", snap, o64, L, pairs)
