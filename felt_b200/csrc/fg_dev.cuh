@@ -115,6 +115,8 @@ struct Dev {
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes
 	unsigned long long* kstat;  // [8] work units processed, see KS_* below
+	unsigned long long* snu;    // [S] narrow-band node updates per surface (band size at the
+	                            // start of each of its global updates, summed)
 
 	// local update (update_start / delta / update_end)
 	int* dlcnt;       // [nslots] delta leaves of a partition: a prefix of its affected list L

@@ -105,29 +105,28 @@ public:
 		}
 		if (BV > 65535) throw Error(-1, "partition volume must be < 65536");
 		geom_.resize(S);
+		np_cap_.resize(S);
+		if (!desc.caps.empty() && desc.caps.size() != (size_t)S)
+			throw Error(-1, "one capacity per surface");
 		long long NP = 0;
 		for (int s = 0; s < S; s++) {
 			SurfGeom& g = geom_[s];
-			std::memset(&g, 0, sizeof(g));
-			bool exact = true;
-			long long np = 1;
-			for (int a = 0; a < D; a++) {
-				const int sz = desc.sizes[s][a];
-				if (sz <= 0) throw Error(-1, "grid size must be positive");
-				g.size[a] = sz;
-				g.off[a] = (-1 * sz) / 2;
-				g.hi[a] = g.off[a] + sz;
-				g.ccount[a] = sz / csz_[a];
-				if (g.ccount[a] * csz_[a] != sz) exact = false;
-				g.coff[a] = g.off[a] / csz_[a];
+			g = grid_geom(desc.sizes[s].data(), 0);
+			long long cap = g.np;
+			if (!desc.caps.empty()) {
+				// any grid up to caps[s] on every axis: a partial partition on one axis adds a
+				// partition along every axis, so the most is prod(caps / part + 1)
+				long long m = 1;
+				for (int a = 0; a < D; a++) {
+					if (desc.caps[s][a] <= 0) throw Error(-1, "capacity must be positive");
+					m *= desc.caps[s][a] / csz_[a] + 1;
+				}
+				if (m >= (1 << 24)) throw Error(-1, "too many partitions in one surface");
+				cap = std::max(cap, m);
 			}
-			if (!exact)
-				for (int a = 0; a < D; a++) g.ccount[a] += 1;
-			for (int a = 0; a < D; a++) np *= g.ccount[a];
-			if (np >= (1 << 24)) throw Error(-1, "too many partitions in one surface");
 			g.pbase = (int)NP;
-			g.np = (int)np;
-			NP += np;
+			np_cap_[s] = (int)cap;
+			NP += cap;
 		}
 		if (NP >= (1LL << 31) / NL) throw Error(-1, "pool too large");
 		size_t nslots = desc.brick_capacity;
@@ -152,6 +151,7 @@ public:
 		std::vector<int> surf_of(NP), porig(NP * 3);
 		for (int s = 0; s < S; s++) {
 			const SurfGeom& g = geom_[s];
+			for (int i = g.np; i < np_cap_[s]; i++) surf_of[g.pbase + i] = s;
 			for (int i = 0; i < g.np; i++) {
 				int r = i;
 				int c[3] = {0, 0, 0};
@@ -238,6 +238,8 @@ public:
 		P.err = dalloc<int>(1, o);
 		P.changed = dalloc<int>(1, o);
 		P.kstat = dalloc<unsigned long long>(KS_N, o);
+		P.snu = dalloc<unsigned long long>(S, o);
+		FG_CUDA(cudaMemsetAsync(P.snu, 0, S * sizeof(unsigned long long), st_));
 		P.dlcnt = dalloc<int>(nslots, o);
 		P.ndp = dalloc<int>(S, o);
 		P.ring_first = dalloc<int>(npl, o);
@@ -336,6 +338,91 @@ public:
 	const SurfGeom& geometry(int s) const override { return geom_[s]; }
 	void sync() override { FG_CUDA(cudaStreamSynchronize(st_)); }
 	int part(int a) const override { return csz_[a]; }
+
+	/// Geometry of a grid of the given size (Surface ctor, Surface.hpp:163-173, and the
+	/// children grid, PartitionedMixin.hpp:59-86, 131-141), its partitions from pbase.
+	SurfGeom grid_geom(const int* size, int pbase) const
+	{
+		SurfGeom g;
+		std::memset(&g, 0, sizeof(g));
+		bool exact = true;
+		long long np = 1;
+		for (int a = 0; a < D; a++) {
+			const int sz = size[a];
+			if (sz <= 0) throw Error(-1, "grid size must be positive");
+			g.size[a] = sz;
+			g.off[a] = (-1 * sz) / 2;
+			g.hi[a] = g.off[a] + sz;
+			g.ccount[a] = sz / csz_[a];
+			if (g.ccount[a] * csz_[a] != sz) exact = false;
+			g.coff[a] = g.off[a] / csz_[a];
+		}
+		if (!exact)
+			for (int a = 0; a < D; a++) g.ccount[a] += 1;
+		for (int a = 0; a < D; a++) np *= g.ccount[a];
+		if (np >= (1 << 24)) throw Error(-1, "too many partitions in one surface");
+		g.pbase = pbase;
+		g.np = (int)np;
+		return g;
+	}
+
+	// ---- serving: reuse of a surface of the pool ----
+	void reset_surface(int s, const int* size) override
+	{
+		check_surface(s);
+		const SurfGeom ng = grid_geom(size, geom_[s].pbase);
+		if (ng.np > np_cap_[s])
+			throw Error(-1, "grid larger than the partition range of this surface");
+		FG_RUN("k_reset_surface", st_, k_reset_surface<D, L><<<grid_for(np_cap_[s]), 256, 0, st_>>>(P_, s, ng, np_cap_[s]););
+		FG_CUDA(cudaGetLastError());
+		geom_[s] = ng;
+		frozen_[s] = 0;
+	}
+
+	void seed_async(int s, const int* pos) override
+	{
+		check_surface(s);
+		Vec<D> c;
+		for (int a = 0; a < D; a++) c[a] = pos[a];
+		FG_RUN("k_seed", st_, k_seed<D, L><<<1, 1, 0, st_>>>(P_, s, c););
+		FG_CUDA(cudaGetLastError());
+	}
+
+	void set_paused_n(const int* surfaces, const int* on, int n) override
+	{
+		bool any = false;
+		for (int i = 0; i < n; i++) {
+			check_surface(surfaces[i]);
+			const int v = on[i] ? 1 : 0;
+			if (paused_[surfaces[i]] != v) {
+				paused_[surfaces[i]] = v;
+				any = true;
+			}
+		}
+		if (any) push_stopped();
+	}
+
+	void surface_node_updates(unsigned long long* out) override
+	{
+		FG_CUDA(cudaMemcpyAsync(out, P_.snu, (size_t)P_.S * sizeof(unsigned long long),
+		                        cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+	}
+
+	long long free_bricks() override
+	{
+		int top = 0;
+		FG_CUDA(cudaMemcpyAsync(&top, P_.counters + CNT_FREE_TOP, sizeof(int),
+		                        cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		return top;
+	}
+
+	int partition_capacity(int s) const override
+	{
+		check_surface(s);
+		return np_cap_[s];
+	}
 
 	// ---- seed ----
 	void seed(int s, const int* pos) override
@@ -1172,6 +1259,7 @@ private:
 	Dev P_;
 	int csz_[3] = {1, 1, 1};
 	std::vector<SurfGeom> geom_;
+	std::vector<int> np_cap_;  // partitions reserved per surface (its range at geom_[s].pbase)
 	std::vector<void*> owned_;
 	unsigned long long* acc_ = nullptr;     // node updates of all global updates so far
 	unsigned long long* zcount_ = nullptr;  // zero-layer leaf count of a bounded update

@@ -35,6 +35,10 @@ struct PoolDesc {
 	int D = 3, L = 2;
 	int part[3] = {8, 8, 8};
 	std::vector<std::array<int, 3>> sizes;  // per surface grid size
+	/// Per surface, the largest grid (per axis) it may be given later by reset_surface: its
+	/// partition range is sized for any grid up to this and for its own size; empty = its own
+	/// size only.
+	std::vector<std::array<int, 3>> caps;
 	size_t brick_capacity = 0;              // 0 = automatic
 };
 
@@ -89,6 +93,20 @@ public:
 	/// exactly as after its last update. Used to retire finished requests of a served batch.
 	virtual void set_paused(int s, bool on) = 0;
 	virtual bool paused(int s) const = 0;
+	/// Serving: makes surface s empty (its bricks back to the pool, no partition active or
+	/// listed, no status, no record of its stop) with grid `size`, whose partitions must fit
+	/// the range the surface was created with. Its paused state is left as it is. Asynchronous.
+	virtual void reset_surface(int s, const int* size) = 0;
+	/// seed(pos) of surface s without waiting for it; errors show at the next check.
+	virtual void seed_async(int s, const int* pos) = 0;
+	/// set_paused for several surfaces at once (one device update).
+	virtual void set_paused_n(const int* surfaces, const int* on, int n) = 0;
+	/// Node updates per surface since it was created or last reset (S values; synchronises).
+	virtual void surface_node_updates(unsigned long long* out) = 0;
+	/// Bricks on the pool's free stack (synchronises).
+	virtual long long free_bricks() = 0;
+	/// Partitions reserved for surface s (the most any grid it is given may have).
+	virtual int partition_capacity(int s) const = 0;
 	virtual const Dev& dev() const = 0;
 	/// Host copy of surface s's geometry (the same as dev().geom[s]).
 	virtual const SurfGeom& geometry(int s) const = 0;

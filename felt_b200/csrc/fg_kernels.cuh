@@ -1476,9 +1476,69 @@ __global__ void k_band_size(Dev P, unsigned long long* acc)
 			t++;
 		}
 		const int gp = g.pbase + P.plist[(size_t)t * P.NP + g.pbase + i];
-		if (lane == 0) local += (unsigned long long)P.lcnt[P.slot[gp] * NL + t];
+		if (lane == 0) {
+			const unsigned long long n = (unsigned long long)P.lcnt[P.slot[gp] * NL + t];
+			local += n;
+			if (n) atomicAdd(&P.snu[s], n);
+		}
 	}
 	if (lane_id() == 0 && local) atomicAdd(acc, local);
+}
+
+/// Makes surface s empty, with geometry ng (its partition range at pbase holds npcap
+/// partitions, ng.np of them used): every brick it holds goes back to the pool's free stack and
+/// every partition-level entry of the range returns to its state in a new pool (inactive,
+/// background L+1, in no list), so that a seed then starts it exactly as a new Surface. The
+/// world origins of the used partitions are recomputed for the new grid. Serving reuses a
+/// finished request's surface this way for the next request.
+template <int D, int L>
+__global__ void k_reset_surface(Dev P, int s, SurfGeom ng, int npcap)
+{
+	constexpr int NL = 2 * L + 1;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npcap; i += gridDim.x * blockDim.x) {
+		const int gp = ng.pbase + i;
+		const int sl = P.slot[gp];
+		if (sl >= 0) {
+			P.slot_gp[sl] = -1;
+			P.touched[sl] = 0;
+			P.free_stack[atomicAdd(&P.counters[CNT_FREE_TOP], 1)] = sl;
+		}
+		P.slot[gp] = -1;
+		P.bg[gp] = (float)(L + 1);
+		P.oslot[gp] = -1;
+		P.actflag[gp] = 0;
+		P.sflag[gp] = 0;
+		for (int l = 0; l < NL; l++) {
+			const size_t k = (size_t)gp * NL + l;
+			P.ppos[k] = -1;
+			P.sppos[k] = -1;
+			P.appos[0][k] = -1;
+			P.appos[1][k] = -1;
+			P.apkey[k] = NOCLAIM;
+		}
+		if (i < ng.np) {
+			int r = i, c[3] = {0, 0, 0};
+			for (int a = D - 1; a >= 0; a--) {
+				c[a] = r % ng.ccount[a];
+				r /= ng.ccount[a];
+			}
+			int* po = const_cast<int*>(P.porig) + (size_t)gp * 3;
+			for (int a = 0; a < 3; a++) po[a] = a < D ? c[a] * P.csz[a] + ng.off[a] : 0;
+		}
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		const_cast<SurfGeom*>(P.geom)[s] = ng;
+		for (int l = 0; l < NL; l++) {
+			P.pcnt[s * NL + l] = 0;
+			P.dpcnt[s * NL + l] = 0;
+			P.spcnt[s * NL + l] = 0;
+			P.apcnt[0][s * NL + l] = 0;
+			P.apcnt[1][s * NL + l] = 0;
+		}
+		P.papn[s] = 0;
+		P.ndp[s] = 0;
+		P.snu[s] = 0;
+	}
 }
 
 /// Dense snapshot (PartitionedMixin.hpp:642-660) of surface s.

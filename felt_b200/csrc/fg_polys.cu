@@ -39,6 +39,7 @@ struct PolysDev {
 	int* err;
 	int* ovf;           // set when a march ran out of arena space
 	unsigned long long* vstart;  // [1] vertex arena position when the current march began
+	int* off;           // [S] 1 = notify leaves the surface out (serving: no polygons asked)
 };
 
 namespace {
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(256) k_polys_notify(Dev P, PolysDev Q)
 	__shared__ unsigned char sdec[TILE];  // bit 0 append, bit 1 remove
 	__shared__ int cnt_s;
 	const int s = blockIdx.x;
-	if (s >= P.S || P.sfrozen[s]) return;
+	if (s >= P.S || P.sfrozen[s] || Q.off[s]) return;
 	const int lane = lane_id();
 	const unsigned lt = (1u << lane) - 1u;
 	const SurfGeom& g = P.geom[s];
@@ -276,6 +277,24 @@ __global__ void k_polys_invalidate(Dev P, PolysDev Q)
 		}
 	}
 	Q.pend_cnt[Q.pend][s] = cnt;
+}
+
+/// Serving: surface s's polygon children all inactive and empty, both pending lists empty
+/// (the state of a new Polys), over the npcap partitions of its range.
+__global__ void k_polys_reset_surface(PolysDev Q, int s, int pbase, int npcap)
+{
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npcap; i += gridDim.x * blockDim.x) {
+		const int gp = pbase + i;
+		Q.pend_lkp[0][gp] = -1;
+		Q.pend_lkp[1][gp] = -1;
+		Q.pact[gp] = 0;
+		Q.gnv[gp] = 0;
+		Q.gns[gp] = 0;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		Q.pend_cnt[0][s] = 0;
+		Q.pend_cnt[1][s] = 0;
+	}
 }
 
 /// Clears list `which` (the reset of the swapped-out pending list, Polys.hpp:163-164).
@@ -645,6 +664,8 @@ public:
 		FG_CUDA(cudaMemset(Q_.gns, 0, P.NP * sizeof(int)));
 		FG_CUDA(cudaMemset(Q_.gvoff, 0, P.NP * sizeof(int)));
 		FG_CUDA(cudaMemset(Q_.gsoff, 0, P.NP * sizeof(int)));
+		Q_.off = (int*)al(P.S * sizeof(int));
+		FG_CUDA(cudaMemset(Q_.off, 0, P.S * sizeof(int)));
 		Q_.used = (unsigned long long*)al(2 * sizeof(unsigned long long));
 		FG_CUDA(cudaMemset(Q_.used, 0, 2 * sizeof(unsigned long long)));
 		woff_ = (int*)al((P.S + 1) * sizeof(int));
@@ -927,6 +948,24 @@ private:
 
 
 public:
+	void reset_surface(int s) override
+	{
+		if (s < 0 || s >= eng_.surfaces()) throw Error(-1, "surface index out of range");
+		const int npcap = eng_.partition_capacity(s);
+		const int blocks = std::max(1, std::min((npcap + 255) / 256, 1024));
+		FG_RUN("k_polys_reset_surface", eng_.stream(), k_polys_reset_surface<<<blocks, 256, 0, eng_.stream()>>>(Q_, s, eng_.geometry(s).pbase, npcap););
+		FG_CUDA(cudaGetLastError());
+	}
+
+	void set_enabled(int s, bool on) override
+	{
+		if (s < 0 || s >= eng_.surfaces()) throw Error(-1, "surface index out of range");
+		if (off_host_.empty()) off_host_.assign((size_t)eng_.surfaces(), 0);
+		off_host_[s] = on ? 0 : 1;
+		FG_CUDA(cudaMemcpyAsync(Q_.off + s, &off_host_[s], sizeof(int), cudaMemcpyHostToDevice,
+		                        eng_.stream()));
+	}
+
 	void select(int s) override
 	{
 		if (s < 0 || s >= eng_.surfaces()) throw Error(-1, "surface index out of range");
@@ -1021,6 +1060,7 @@ private:
 	uint32_t* spare_s_ = nullptr;            // the other simplex arena
 	long long spare_vcap_ = 0, spare_scap_ = 0;
 	std::vector<void*> owned_;
+	std::vector<int> off_host_;  // host copy of Q_.off (sources of its updates)
 };
 
 }  // namespace

@@ -27,6 +27,12 @@ public:
 	/// (one gather kernel, two copies); counts receives (vertices, simplices) per partition.
 	virtual void gather(const uint32_t* parts, size_t n, float* vtx, size_t vcap, uint32_t* spx,
 	                    size_t scap, uint32_t* counts, size_t* nv, size_t* ns) = 0;
+	/// Serving: forgets surface s's polygons and pending partitions (after the engine's
+	/// reset_surface), as a new Polys of an empty surface has none.
+	virtual void reset_surface(int s) = 0;
+	/// Serving: whether notify tracks surface s's changes (a request that asks for no
+	/// polygons is left out, so marches find nothing pending for it).
+	virtual void set_enabled(int s, bool on) = 0;
 };
 
 /// Polygonisation of surface s of an engine's pool. vertex_capacity: initial vertex arena

@@ -1,41 +1,67 @@
-"""Serving many independent level-set requests on one GPU.
+"""Serving many independent level-set requests on one GPU: a thin client of the fg_server_* C ABI.
 
-A request is one Surface<3,L> job: grid size, seed position, speed, number of global updates,
-and whether to polygonise the result. The reference runs one surface at a time; here requests
-that arrive close together form a *wave*: one Batch whose surfaces advance in the same kernel
-launches. A wave runs on its own worker thread and CUDA stream, so several waves overlap on the
-GPU. Requests in a wave may ask for different step counts: a request that has had its last
-update (and, if asked, its polygonisation) is paused, so later launches skip it and its state
-stays exactly what a separate Surface given the same updates would hold.
+A request is one Surface<D,L> job: grid size, seed position, builtin speed, number of global
+updates, and whether to polygonise the result. The reference runs one surface at a time; the
+server (libfelt_gpu.so, fg_server.cu) batches them continuously: one long-lived pool of
+`slots` surfaces sharing one brick pool, advanced together one Surface::update per step by a
+worker thread, with requests that arrive while others run taking freed slots at the next step
+boundary. Each result equals a separate Surface run alone on the same request.
 
-Admission is by device memory: each request reserves an upper bound of the brick-pool bytes it
-can reach (partitions within reach of its band after its steps, at the worst speed its kind
-allows), and a request that would push the reserved total over the budget is rejected at
-arrival. Reservations are returned when the request's wave ends.
+Admission is by the brick pool: a request reserves the bricks its band can reach and is
+rejected at submission when the reservations in flight and queued would exceed the pool
+(budget_bytes of device memory, or brick_capacity bricks).
 """
 from __future__ import annotations
 
-import math
-import queue
-import threading
+import ctypes as C
 import time
 from dataclasses import dataclass
 
-from . import Batch
+import numpy as np
 
-# Largest |delta| per update for each builtin speed kind of a request (bounds the band's reach).
-_VMAX = {"constant": 0.6, "curvature": 0.8, "noise": 0.4}
+from . import FeltError, Speed, _chk, lib, make_speed
+
+ERR_CAPACITY = -13
+ERR_TIMEOUT = -14
+
+
+class _Config(C.Structure):
+    _fields_ = [("dims", C.c_int), ("layers", C.c_int), ("part", C.c_int * 3),
+                ("max_size", C.c_int * 3), ("slots", C.c_size_t),
+                ("brick_capacity", C.c_size_t), ("budget_bytes", C.c_double),
+                ("vertex_capacity", C.c_size_t), ("keep_outputs", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("size", C.c_int * 3), ("centre", C.c_int * 3), ("speed", Speed),
+                ("steps", C.c_int), ("polygonise", C.c_int), ("tag", C.c_uint64)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int), ("steps_done", C.c_int),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("node_updates", C.c_ulonglong), ("vertices", C.c_ulonglong),
+                ("simplices", C.c_ulonglong)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [(k, C.c_ulonglong) for k in (
+        "submitted", "admitted", "rejected", "started", "completed", "failed", "steps",
+        "node_updates", "capacity_bricks", "reserved_bricks", "peak_reserved_bricks",
+        "peak_used_bricks", "queued", "in_flight")] + [("fault_code", C.c_int),
+                                                       ("reserved", C.c_int * 7)]
 
 
 @dataclass
 class Request:
-    size: tuple            # grid size (3 ints)
+    size: tuple            # grid size
     centre: tuple          # seed position
-    speed: dict            # dict(c=, a=, n=, seed=) as for Batch.update
+    speed: dict            # dict(c=, a=, n=, seed=) as for Surface.update
     steps: int             # global updates
     polys: bool            # polygonise after the last update
     kind: str = "constant"
-    arrival: float = 0.0   # seconds on the server clock
+    arrival: float = 0.0   # seconds on the server clock (set by the caller, else submission)
     rid: int = -1
 
 
@@ -46,175 +72,198 @@ class Result:
     done: float            # seconds on the server clock when the result was ready
     stopped: bool = False  # the update's convergence loop did not settle (surface stopped)
     dump: object = None    # the surface's state encoding (fg_dump), when the server keeps it
+    admitted: float = 0.0  # when it took a slot
+    status: int = 0
+    steps_done: int = 0
+    node_updates: int = 0
+    vertices: int = 0
+    simplices: int = 0
 
     @property
     def latency(self):
         return self.done - self.arrival
 
 
+def _as_request(req: Request, D):
+    r = _Request()
+    for a in range(D):
+        r.size[a] = int(req.size[a])
+        r.centre[a] = int(req.centre[a])
+    r.speed = make_speed(**req.speed)
+    r.steps = int(req.steps)
+    r.polygonise = 1 if req.polys else 0
+    r.tag = int(req.rid)
+    return r
+
+
+def reserve_bricks(req: Request, L, part):
+    """The bricks a server with this layer count and partition shape reserves for a request
+    (its admission bound; fg_request_bricks, host arithmetic only)."""
+    D = len(part)
+    cfg = _Config()
+    cfg.dims, cfg.layers = D, int(L)
+    for a in range(D):
+        cfg.part[a] = int(part[a])
+    n = C.c_ulonglong()
+    _chk(lib().fg_request_bricks(C.byref(cfg), C.byref(_as_request(req, D)), C.byref(n)))
+    return n.value
+
+
 def brick_bytes(L, part):
-    """Device bytes of one brick slot: phi, delta, lookup, 2L+1 lists, status, status lists, two
-    affected buffers, expansion claims (per leaf), as the engine allocates them."""
-    nl = 2 * L + 1
-    bv = math.prod(part)
-    return bv * (4 + 4 + 2 + 2 * nl + 1 + 2 * nl + 2 * 2 + 2 * 2 * nl + 8) + 4 * (3 * nl + 6)
-
-
-def partition_bytes(L):
-    """Device bytes per partition of a grid (lists, lookups, flags), engine and polygoniser."""
-    nl = 2 * L + 1
-    return 4 * (12 * nl + 24)
-
-
-def reserve_bytes(req: Request, L, part):
-    """Upper bound of the device bytes a request can occupy: every partition that the band can
-    reach within its steps holds a brick (the ball of radius 1 + steps * vmax + L + 1 around the
-    seed, by its bounding box, clipped to the grid), plus the grid's partition-level arrays."""
-    reach = 1.0 + req.steps * _VMAX.get(req.kind, 1.0) + L + 1
-    nb = 1
-    npart = 1
-    for a in range(3):
-        span = min(req.size[a], int(math.ceil(2 * reach)) + 1)
-        nb *= min(-(-req.size[a] // part[a]) + 1, -(-span // part[a]) + 1)
-        npart *= -(-req.size[a] // part[a]) + 1
-    return nb, nb * brick_bytes(L, part) + npart * partition_bytes(L)
-
-
-@dataclass
-class _Wave:
-    reqs: list
-    bricks: int
-    bytes: int
+    """Device bytes of one brick of the pool (fg_brick_bytes)."""
+    v = C.c_double()
+    _chk(lib().fg_brick_bytes(len(part), int(L), (C.c_int * len(part))(*part), C.byref(v)))
+    return v.value
 
 
 class Server:
-    """Poisson-fed request server over batched surfaces.
+    """Continuous-batching level-set server (fg_server_*).
 
-    submit() admits or rejects a request at its arrival; a scheduler thread groups the admitted
-    requests into waves every `tick` seconds and hands each wave to a worker (at most `workers`
-    waves in flight). results() returns the finished requests; with keep_outputs each result
-    carries its surface's final state encoding."""
+    submit() admits or rejects a request at its arrival; results() returns the finished ones.
+    With keep_outputs each result carries its surface's final state encoding, and polys(rid)
+    its polygons."""
 
-    def __init__(self, layers=2, part=(8, 8, 8), budget_bytes=150e9, workers=4, tick=0.002,
-                 max_wave=512, keep_outputs=False):
-        self.L = layers
-        self.keep_outputs = keep_outputs
-        self.part = tuple(part)
-        self.budget = float(budget_bytes)
-        self.tick = tick
-        self.max_wave = max_wave
-        self.t0 = time.perf_counter()
-        self._lock = threading.Lock()
-        self._reserved = 0.0
-        self._pending = []
+    def __init__(self, layers=2, part=(8, 8, 8), budget_bytes=150e9, slots=256,
+                 max_size=(256, 256, 256), keep_outputs=False, brick_capacity=0,
+                 vertex_capacity=0):
+        self.D = len(part)
+        self.L = int(layers)
+        self.part = tuple(int(p) for p in part)
+        self.keep_outputs = bool(keep_outputs)
+        cfg = _Config()
+        cfg.dims, cfg.layers = self.D, self.L
+        for a in range(self.D):
+            cfg.part[a] = self.part[a]
+            cfg.max_size[a] = int(max_size[a])
+        cfg.slots = int(slots)
+        cfg.brick_capacity = int(brick_capacity)
+        cfg.budget_bytes = float(budget_bytes)
+        cfg.vertex_capacity = int(vertex_capacity)
+        cfg.keep_outputs = 1 if keep_outputs else 0
+        h = C.c_void_p()
+        _chk(lib().fg_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._requests = {}
         self._results = []
-        self._errors = []
-        self.admitted = 0
-        self.rejected = 0
-        self.node_updates = 0  # band nodes processed by the finished waves
-        self._waves = queue.Queue()
-        self._stop = threading.Event()
-        self._inflight = threading.Semaphore(workers)
-        self._workers = [threading.Thread(target=self._work, daemon=True) for _ in range(workers)]
-        self._sched = threading.Thread(target=self._schedule, daemon=True)
-        for w in self._workers:
-            w.start()
-        self._sched.start()
+        self.brick_bytes = brick_bytes(self.L, self.part)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            lib().fg_server_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
     def now(self):
-        return time.perf_counter() - self.t0
+        t = C.c_double()
+        _chk(lib().fg_server_now(self._h, C.byref(t)))
+        return t.value
 
     def submit(self, req: Request):
         """Admit (True) or reject (False) a request at its arrival."""
-        _, need = reserve_bytes(req, self.L, self.part)
-        with self._lock:
-            if self._reserved + need > self.budget:
-                self.rejected += 1
-                return False
-            self._reserved += need
-            self.admitted += 1
-            self._pending.append(req)
+        rc = lib().fg_server_submit(self._h, C.byref(_as_request(req, self.D)))
+        if rc == ERR_CAPACITY:
+            return False
+        _chk(rc)
+        self._requests[int(req.rid)] = req
         return True
 
-    def _schedule(self):
-        while not self._stop.is_set():
-            time.sleep(self.tick)
-            with self._lock:
-                take, self._pending = self._pending[:self.max_wave], self._pending[self.max_wave:]
-            if not take:
-                continue
-            self._inflight.acquire()
-            nb = sum(reserve_bytes(r, self.L, self.part)[0] for r in take)
-            by = sum(reserve_bytes(r, self.L, self.part)[1] for r in take)
-            self._waves.put(_Wave(take, nb, by))
+    def request_bricks(self, req: Request):
+        """The bricks the server reserves for a request."""
+        return reserve_bricks(req, self.L, self.part)
 
-    def _work(self):
+    def _poll(self, wait_s=0.0):
+        buf = (_Result * 256)()
+        n = C.c_size_t()
+        got = 0
         while True:
-            w = self._waves.get()
-            if w is None:
-                return
-            try:
-                self._run_wave(w)
-            except Exception as e:  # recorded, the server keeps serving
-                self._errors.append(repr(e))
-            finally:
-                with self._lock:
-                    self._reserved -= w.bytes
-                self._inflight.release()
+            _chk(lib().fg_server_poll(self._h, buf, C.c_size_t(256), C.byref(n),
+                                      C.c_double(wait_s if not got else 0.0)))
+            for i in range(n.value):
+                self._results.append(self._convert(buf[i]))
+            got += n.value
+            if n.value < 256:
+                return got
 
-    def _run_wave(self, w: _Wave):
-        reqs = w.reqs
-        b = Batch([r.size for r in reqs], self.part, self.L, brick_capacity=max(w.bricks, 1))
-        try:
-            b.seed([r.centre for r in reqs])
-            speeds = b.speed_array([r.speed for r in reqs])
-            nu = 0
-            for step in range(1, max(r.steps for r in reqs) + 1):
-                b.update(speeds)
-                b.polys_notify()
-                finishing = [i for i, r in enumerate(reqs) if r.steps == step]
-                if not finishing:
-                    continue
-                if any(reqs[i].polys for i in finishing):
-                    b.polys_march()
-                nu = b.node_updates()  # synchronises the wave's stream: results are ready
-                t = self.now()
-                out = [Result(reqs[i].rid, reqs[i].arrival, t, b.stopped(i),
-                              b.dump(i) if self.keep_outputs else None) for i in finishing]
-                for i in finishing:
-                    b.pause(i)
-                with self._lock:
-                    self._results.extend(out)
-            with self._lock:
-                self.node_updates += nu
-        finally:
-            b.close()
+    def _convert(self, r):
+        req = self._requests.pop(int(r.tag), None)
+        arrival = req.arrival if req is not None and req.arrival > 0 else r.t_submit
+        dump = None
+        if self.keep_outputs and r.status in (0, ERR_TIMEOUT):
+            dump = self._kept_dump(int(r.tag))
+        return Result(int(r.tag), arrival, r.t_done, r.status == ERR_TIMEOUT, dump,
+                      r.t_admit, r.status, r.steps_done, r.node_updates, r.vertices,
+                      r.simplices)
+
+    def _kept_dump(self, tag):
+        n = C.c_size_t()
+        _chk(lib().fg_server_result_dump(self._h, C.c_uint64(tag), None, C.c_size_t(0),
+                                         C.byref(n)))
+        out = np.zeros(max(1, n.value), dtype=np.uint32)
+        _chk(lib().fg_server_result_dump(self._h, C.c_uint64(tag),
+                                         out.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                         C.c_size_t(out.size), C.byref(n)))
+        return out[: n.value]
+
+    def polys(self, rid):
+        """A kept result's polygons: per partition (vertices (nv, per), simplices (ns, D))."""
+        nv, ns, npt = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        tag = C.c_uint64(int(rid))
+        _chk(lib().fg_server_result_polys(self._h, tag, None, 0, None, 0, None, 0, C.byref(nv),
+                                          C.byref(ns), C.byref(npt)))
+        per = 2 * self.D if self.D == 3 else self.D
+        vtx = np.zeros(max(1, nv.value * per), dtype=np.float32)
+        spx = np.zeros(max(1, ns.value * self.D), dtype=np.uint32)
+        cnt = np.zeros(max(1, 2 * npt.value), dtype=np.uint32)
+        _chk(lib().fg_server_result_polys(self._h, tag, vtx.ctypes.data_as(C.POINTER(C.c_float)),
+                                          C.c_size_t(vtx.size),
+                                          spx.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          C.c_size_t(spx.size),
+                                          cnt.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          C.c_size_t(cnt.size), C.byref(nv), C.byref(ns),
+                                          C.byref(npt)))
+        out, v0, s0 = [], 0, 0
+        for p in range(npt.value):
+            a, b = int(cnt[2 * p]), int(cnt[2 * p + 1])
+            out.append((vtx[v0 * per:(v0 + a) * per].reshape(a, per),
+                        spx[s0 * self.D:(s0 + b) * self.D].reshape(b, self.D)))
+            v0 += a
+            s0 += b
+        return out
+
+    def stats(self):
+        st = _Stats()
+        _chk(lib().fg_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _Stats._fields_ if k != "reserved"}
 
     def drain(self, timeout=600.0):
         """Waits until every admitted request has finished."""
         t_end = time.perf_counter() + timeout
         while time.perf_counter() < t_end:
-            with self._lock:
-                n = len(self._results)
-                busy = self._pending or self._reserved > 0
-            if n >= self.admitted and not busy:
+            self._poll(0.05)
+            st = self.stats()
+            if st["fault_code"]:
+                raise FeltError(st["fault_code"], "serving worker failed")
+            if st["completed"] + st["failed"] >= st["admitted"] and not st["queued"] \
+                    and not st["in_flight"]:
+                self._poll(0.0)
                 return True
-            if self._errors:
-                raise RuntimeError("serving worker failed: " + self._errors[0])
-            time.sleep(0.002)
         return False
 
-    def close(self):
-        self._stop.set()
-        self._sched.join(timeout=5)
-        for _ in self._workers:
-            self._waves.put(None)
-        for w in self._workers:
-            w.join(timeout=60)
-
     def results(self):
+        self._poll(0.0)
         return list(self._results)
 
     @property
-    def errors(self):
-        return list(self._errors)
+    def admitted(self):
+        return self.stats()["admitted"]
+
+    @property
+    def rejected(self):
+        return self.stats()["rejected"]
+
+    @property
+    def node_updates(self):
+        return self.stats()["node_updates"]

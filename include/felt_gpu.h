@@ -301,6 +301,87 @@ FG_API int fg_batch_pause(fg_batch* b, size_t surface, int paused);
 FG_API int fg_batch_work_units(fg_batch* b, unsigned long long* out, size_t n);
 FG_API int fg_batch_stream(fg_batch* b, void** stream);
 
+/* ---- serving: continuous batching of level-set requests ----
+ * No counterpart in the reference, which advances one Surface at a time. A server owns one
+ * long-lived pool of `slots` surfaces, each sized for grids up to max_size, sharing one brick
+ * pool, and a worker thread that advances every surface in flight by one batched
+ * Surface::update (include/Felt/Surface.hpp:254-296) per step, with Polys::notify
+ * (include/Felt/Polys.hpp:92-133) for requests that want polygons and Polys::march
+ * (Polys.hpp:138-165) when one of them has had its last update. Requests that arrive while
+ * others run take freed slots at the next step boundary (reset to the request's grid, seeded,
+ * then advanced in the same launches as the rest), so their work overlaps on the device. Each
+ * request's result equals a separate fg_surface given the same seed and updates.
+ * Admission: a request reserves the bricks its band can reach (the partitions within
+ * L + 2 + steps * max(1, largest |delta| of its speed) cells of its seed, clipped to its grid;
+ * fg_request_bricks) and is rejected at submission (FG_ERR_CAPACITY) when the reservations of
+ * requests queued and in flight would exceed the brick pool. */
+typedef struct fg_server fg_server;
+typedef struct fg_server_config {
+	int dims;               /* 2 or 3 */
+	int layers;             /* L, 1..4 */
+	int part[3];            /* partition size */
+	int max_size[3];        /* largest grid a request may ask for (each slot's capacity) */
+	size_t slots;           /* surfaces in flight at most */
+	size_t brick_capacity;  /* bricks in the shared pool; 0 = budget_bytes / bytes per brick */
+	double budget_bytes;    /* device bytes of the brick pool, when brick_capacity is 0 */
+	size_t vertex_capacity; /* initial polygon arena (vertices), 0 = 2^20; grows on demand */
+	int keep_outputs;       /* keep each result's state dump and polygons until released */
+	int reserved[7];
+} fg_server_config;
+typedef struct fg_request {
+	int size[3];            /* grid size */
+	int centre[3];          /* seed position (Surface::seed, Surface.hpp:207-241) */
+	fg_speed speed;         /* builtin speed of every update */
+	int steps;              /* global updates, >= 1 */
+	int polygonise;         /* march the polygons after the last update */
+	uint64_t tag;           /* the caller's id, returned with the result */
+} fg_request;
+typedef struct fg_result {
+	uint64_t tag;
+	int status;             /* FG_OK; FG_ERR_TIMEOUT when the surface was stopped (its update's
+	                           convergence loop did not settle); another code on a fault */
+	int steps_done;
+	double t_submit, t_admit, t_done;   /* seconds on the server's clock (fg_server_now) */
+	unsigned long long node_updates;    /* band size at the start of each of its updates */
+	unsigned long long vertices, simplices;  /* its polygons, when it asked for them */
+} fg_result;
+typedef struct fg_server_stats {
+	unsigned long long submitted, admitted, rejected;  /* at submission */
+	unsigned long long started;          /* taken into a slot */
+	unsigned long long completed;        /* finished (stopped surfaces included) */
+	unsigned long long failed;           /* ended by a fault */
+	unsigned long long steps;            /* batched steps run */
+	unsigned long long node_updates;     /* of finished requests */
+	unsigned long long capacity_bricks, reserved_bricks, peak_reserved_bricks, peak_used_bricks;
+	unsigned long long queued, in_flight;
+	int fault_code;
+	int reserved[7];
+} fg_server_stats;
+FG_API int fg_server_create(const fg_server_config* cfg, fg_server** out);
+/* Stops the worker after its current step and frees the pool. */
+FG_API int fg_server_destroy(fg_server* s);
+/* Seconds since the server was created (the clock of fg_result's times). */
+FG_API int fg_server_now(fg_server* s, double* t);
+/* Queues a request, or rejects it with FG_ERR_CAPACITY (budget reserved, or a grid larger
+ * than max_size). Any thread. */
+FG_API int fg_server_submit(fg_server* s, const fg_request* r);
+/* Up to cap finished results, oldest first (waits up to wait_s seconds for the first). */
+FG_API int fg_server_poll(fg_server* s, fg_result* out, size_t cap, size_t* n, double wait_s);
+FG_API int fg_server_get_stats(fg_server* s, fg_server_stats* out);
+/* With keep_outputs: a finished request's state (the fg_dump encoding) and its polygons (every
+ * partition's vertices and simplices concatenated in partition order, counts[2p], counts[2p+1]
+ * the vertex and simplex count of partition p); fg_server_release drops them. */
+FG_API int fg_server_result_dump(fg_server* s, uint64_t tag, uint32_t* out, size_t cap, size_t* n);
+FG_API int fg_server_result_polys(fg_server* s, uint64_t tag, float* vtx, size_t vtx_cap,
+                                  uint32_t* spx, size_t spx_cap, uint32_t* counts,
+                                  size_t counts_cap, size_t* nv, size_t* ns, size_t* nparts);
+FG_API int fg_server_release(fg_server* s, uint64_t tag);
+/* The bricks a request reserves on a server of this configuration (host arithmetic only), and
+ * the device bytes of one brick of the pool. */
+FG_API int fg_request_bricks(const fg_server_config* cfg, const fg_request* r,
+                             unsigned long long* bricks);
+FG_API int fg_brick_bytes(int dims, int layers, const int* part, double* bytes);
+
 /* ---- instrumentation (no counterpart in the reference; Surface.hpp has no timers) ----
  * fg_node_updates: narrow-band node-updates processed by all global updates of a surface so
  * far (band size at the start of each update, summed). fg_launch_count: kernels this library

@@ -1,6 +1,6 @@
 """Host-side logic of the serving path (no GPU): the request stream is deterministic and has the
-configured distribution, and the admission reservation bounds grow with a request's reach and
-stop at the grid."""
+configured distribution, and the server's admission bound (fg_request_bricks, host arithmetic
+in the C ABI) grows with a request's reach and its speed and stops at the grid."""
 import math
 import os
 import sys
@@ -31,16 +31,35 @@ def test_request_stream_is_seeded_and_in_range():
     assert kinds == {"constant", "curvature", "noise"}
 
 
+def _bricks(size, steps, speed, L=2, part=(8, 8, 8)):
+    from felt_b200.serving import Request, reserve_bricks
+    return reserve_bricks(Request(size, (0,) * len(size), speed, steps, False), L, part)
+
+
 def test_reservation_bounds():
-    from felt_b200.serving import Request, brick_bytes, reserve_bytes
-    part = (8, 8, 8)
-    small = Request((128, 128, 128), (0, 0, 0), dict(c=-0.5), 4, False, "constant")
-    big = Request((128, 128, 128), (0, 0, 0), dict(c=-0.5), 60, False, "constant")
-    nb_s, by_s = reserve_bytes(small, 2, part)
-    nb_b, by_b = reserve_bytes(big, 2, part)
-    assert nb_s < nb_b and by_s < by_b
-    # never more bricks than the grid has partitions
-    huge = Request((64, 64, 64), (0, 0, 0), dict(c=-0.5), 64, False, "curvature")
-    nb_h, _ = reserve_bytes(huge, 2, part)
-    assert nb_h <= (math.ceil(64 / 8) + 1) ** 3
-    assert brick_bytes(2, part) == 512 * 63 + 4 * 21
+    small = _bricks((128, 128, 128), 4, dict(c=-0.5))
+    big = _bricks((128, 128, 128), 60, dict(c=-0.5))
+    assert small < big
+    # a 4-step request reaches L + 2 + 4 = 8 cells: a 17-cell span, at most 4 partitions per axis
+    assert small == 4 ** 3
+    # never more bricks than the grid has partitions (a partial one adds one per axis)
+    huge = _bricks((64, 64, 64), 64, dict(a=-0.3, c=-0.2))
+    assert huge <= (64 // 8 + 1) ** 3
+    # a speed that can exceed one cell per step reaches further
+    slow = _bricks((256, 256, 256), 10, dict(c=-0.5))
+    fast = _bricks((256, 256, 256), 10, dict(c=-3.0))
+    assert fast > slow
+    # curvature counts with its largest magnitude (D): 0.5 * 3 + 0.2 > 1
+    curv = _bricks((256, 256, 256), 10, dict(a=-0.5, c=-0.2))
+    assert curv > slow
+    # reach 2 + 2 + 5 = 9 cells: a 19-cell span, at most 3 partitions of 16 per axis
+    assert _bricks((512, 512), 5, dict(c=-0.4), part=(16, 16)) == 3 ** 2
+
+
+def test_brick_bytes():
+    from felt_b200.serving import brick_bytes
+    # per leaf phi, delta, lookup, 5 lists, status, 5 status lists, 2 affected lookups,
+    # 2 x 5 affected lists, claim; per brick the list counts and queues
+    assert brick_bytes(2, (8, 8, 8)) == 512 * 63 + 4 * 26
+    assert math.isclose(brick_bytes(3, (16, 16, 16)), 4096 * (4 + 4 + 2 + 14 + 1 + 14 + 4 + 28 + 8)
+                        + 4 * 34)
