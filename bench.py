@@ -59,8 +59,8 @@ CONFIGS = {
                workload="256 x Surface<3,2>, edges from {32,48,64,96,128}, 8^3 partitions, "
                         "speed -0.3*curv + U[-0.6,0.3], marching cubes at the end"),
     "c5": dict(kind="serve", D=3, L=2, part=(8, 8, 8), lambdas=(100, 300, 1000, 3000, 10000),
-               max_requests=3000, max_seconds=2.0, budget=150e9, workers=4, plain_subset=24,
-               cpu_subset=200,
+               max_requests=3000, max_seconds=2.0, budget=150e9, slots=512,
+               max_size=(256, 256, 256), plain_subset=24, cpu_subset=200,
                workload="served requests, Poisson arrivals at 100..10k/s: Surface<3,2>, edge "
                         "log-uniform 32..256, 8^3 partitions, speed constant U[-0.6,-0.1] | "
                         "-0.3*curv-0.2 | 0.2*hash_noise-0.2, 1..64 steps, polygonise p=0.5, "
@@ -78,18 +78,15 @@ CONFIGS = {
                          "centre"),
 }
 
-# Algorithmic bytes per work unit of the kernels whose roofline is reported:
-#  k_dist1: per band node of the layer: 2 B list index + 4 B phi read + 4 B delta write.
-#  k_dist2: per band node: 2 B list index + 4 B delta read + 4 B phi write.
-#  k_delta_*: per zero-layer node: 2 B index + 4 B phi + 4 B delta write.
-#  k_flush_*: per leaf edit: 2 B status entry + 1 B to-layer + 2 B lookup read + 2 B list
-#             write + 2 B lookup write + 4 B swap-in (moved entry and its lookup).
-#  k_polys_march: per cell: 2 B leaf index + 4 B phi (corners are neighbours' phi).
-#  k_ray: per ray: origin and direction in, hit out (3 x 12 B in 3D); the nodes it samples
-#         are reads of the resident isogrid and are not counted.
-UNIT_BYTES = {"k_dist1": (0, 10), "k_dist2": (0, 10), "k_delta_builtin": (1, 10),
-              "k_delta_smem": (1, 10), "k_flush_smem": (2, 13), "k_flush_leaf": (2, 13),
-              "k_polys_march": (3, 6)}
+# Algorithmic bytes: 16 B per narrow-band node-update (a 4 B list index read, a 4 B value read,
+# a 4 B value write and 4 B of per-node auxiliary traffic: the delta of a zero-layer node, the
+# status or list write of the others; neighbour reads are other nodes' value reads and are not
+# counted twice). A kernel's launch is credited 16 B per work unit it processes: band nodes for
+# the distance passes, zero-layer nodes for the speed functor and the zero-layer update, leaf
+# edits for the status-change flush, cells for the march.
+BYTES_PER_NODE_UPDATE = 16
+UNIT_OF = {"k_dist1": 0, "k_dist2": 0, "k_delta_builtin": 1, "k_delta_smem": 1,
+           "k_zero_apply": 1, "k_flush_smem": 2, "k_flush_leaf": 2, "k_polys_march": 3}
 
 
 def batch_surfaces(name, cfg, shard=0):
@@ -214,10 +211,9 @@ class SingleWork:
         self.fetch_geometry()
 
     def step(self, i, last=False):
-        c = self.cfg
-        self.s.update(**c["speed"])
+        self.s.update(**self.cfg["speed"])
         self.p.notify()
-        if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+        if march_due(self.cfg, i, last):
             self.p.march()
             return True
         return False
@@ -236,6 +232,10 @@ class SingleWork:
         in one gather call, into pinned host buffers kept between steps."""
         vtx, spx, _ = self.p.gather(self.p.changes(), *self._pinned())
         return vtx.nbytes + spx.nbytes
+
+    def close(self):
+        self.p.close()
+        self.s.close()
 
     def _pinned(self, vfloats=16 << 20, sints=24 << 20):
         """Pinned destination arrays (grown by the gather's own fallback if ever too small)."""
@@ -263,10 +263,9 @@ class BatchWork:
         self.surface0 = None
 
     def step(self, i, last=False):
-        c = self.cfg
         self.b.update(self.speeds)
         self.b.polys_notify()
-        if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+        if march_due(self.cfg, i, last):
             self.b.polys_march()
             return True
         return False
@@ -285,39 +284,146 @@ class BatchWork:
         self.b.polys_totals()
         return 16
 
+    def close(self):
+        self.b.close()
+
 
 class PlainSubset:
     """The plain path on the first k surfaces of a batched config: one Surface each, advanced
-    one surface at a time (every update its own launch sequence)."""
+    one surface at a time (every update its own launch sequence). step() times each surface's
+    update and polygonisation with CUDA events on that surface's stream, so the plain path has
+    a device time like the batch's."""
 
     def __init__(self, fb, cfg, name, k):
         sizes, centres, speeds = batch_surfaces(name, cfg)
         self.cfg = cfg
         self.items = []
+        self.done = 0
         for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
             s = fb.Surface(sz, cfg["part"], cfg["L"])
             s.seed(c)
             self.items.append((s, fb.Polys(s), sp))
 
-    def step(self, i, last=False):
-        c = self.cfg
+    def step(self, i, last=False, torch=None):
+        """One step of every surface; returns the device time of the step in ms (summed over
+        the surfaces' streams) when torch is given."""
+        dev_ms = 0.0
         keep = []
         for s, p, sp in self.items:
+            if torch is not None:
+                st = torch.cuda.ExternalStream(s.stream())
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(st)
             try:
                 s.update(**sp)
             except Exception:  # stopped: its convergence loop did not terminate
                 self.done += s.node_updates()
                 continue
             p.notify()
-            if (c["march_every"] and (i + 1) % c["march_every"] == 0) or (last and c["march_end"]):
+            if march_due(self.cfg, i, last):
                 p.march()
+            if torch is not None:
+                b.record(st)
+                b.synchronize()
+                dev_ms += a.elapsed_time(b)
             keep.append((s, p, sp))
         self.items = keep
-
-    done = 0
+        return dev_ms
 
     def node_updates(self):
         return self.done + sum(s.node_updates() for s, _, _ in self.items)
+
+    def close(self):
+        for s, p, _ in self.items:
+            p.close()
+            s.close()
+        self.items = []
+
+
+def measure_batched(fb, name, steps, warm):
+    """The batched workload against the plain path on the same surfaces and steps: every
+    surface of the config in one batch (the same launches for all), and its first
+    `plain_subset` surfaces one Surface each, one after another. Both are timed two ways over
+    the same steps: device time (CUDA events on the launching streams) and wall clock with the
+    host calls and synchronisation. The ratios compare like with like."""
+    import torch
+    cfg = CONFIGS[name]
+    work = BatchWork(fb, cfg, name)
+    stream = torch.cuda.ExternalStream(work.stream())
+    for i in range(warm):
+        work.step(i)
+    torch.cuda.synchronize()
+    nu0 = work.node_updates()
+    dev_ms, wall = 0.0, 0.0
+    for i in range(steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        work.step(warm + i, last=(i == steps - 1))
+        b.record(stream)
+        b.synchronize()
+        wall += time.perf_counter() - t0
+        dev_ms += a.elapsed_time(b)
+    nu = work.node_updates() - nu0
+    work.close()
+    k = cfg["plain_subset"]
+    plain = PlainSubset(fb, cfg, name, k)
+    for i in range(warm):
+        plain.step(i)
+    torch.cuda.synchronize()
+    pnu0 = plain.node_updates()
+    pdev_ms, pwall = 0.0, 0.0
+    for i in range(steps):
+        t0 = time.perf_counter()
+        pdev_ms += plain.step(warm + i, last=(i == steps - 1), torch=torch)
+        torch.cuda.synchronize()
+        pwall += time.perf_counter() - t0
+    pnu = plain.node_updates() - pnu0
+    plain.close()
+    b_dev, b_wall = nu / (dev_ms * 1e-3), nu / wall
+    p_dev, p_wall = pnu / (pdev_ms * 1e-3), pnu / pwall
+    return {"workload": cfg["workload"], "name": name, "steps": steps, "warmup": warm,
+            "batched": {"surfaces": cfg["n"], "node_updates": nu, "device_per_s": b_dev,
+                        "wall_per_s": b_wall, "ms_per_step": dev_ms / steps},
+            "plain": {"surfaces": k, "node_updates": pnu, "device_per_s": p_dev,
+                      "wall_per_s": p_wall, "ms_per_step": pdev_ms / steps},
+            "batched_over_plain_device": b_dev / p_dev,
+            "batched_over_plain_wall": b_wall / p_wall,
+            "how": "node-updates/s of the same steps; batched: all surfaces in one batch; plain: "
+                   "the first surfaces as separate Surfaces one after another (every update its "
+                   "own launch sequence); device = CUDA events on the launching streams, wall = "
+                   "host clock around the calls with synchronisation"}
+
+
+def measure_served(fb, name, lambdas):
+    """The served workload at the given arrival rates, and the plain path on the same request
+    mix (one Surface per request, one request after another, seed to result, wall clock)."""
+    from felt_b200.serving import Server
+    cfg = CONFIGS[name]
+    budget = serve_budget(cfg)
+    srv = Server(layers=cfg["L"], part=cfg["part"], budget_bytes=budget, slots=cfg["slots"],
+                 max_size=cfg["max_size"])
+    try:
+        serve_one_rate(srv, cfg, 1000,
+                       stream=[(t, r) for t, r in serve_requests(cfg, 1000, shard=99)[:16]])
+        sweep = [serve_one_rate(srv, cfg, lam) for lam in lambdas]
+    finally:
+        srv.close()
+    p_rate, p_nu, p_secs, p_make = serve_plain(fb, cfg, cfg["plain_subset"])
+    best = max(sweep, key=lambda r: r["node_updates_per_s"])
+    return {"workload": cfg["workload"], "name": name, "budget_bytes": budget,
+            "slots": cfg["slots"], "sweep": sweep, "best_lambda_per_s": best["lambda_per_s"],
+            "node_updates_per_s": best["node_updates_per_s"],
+            "plain": {"node_updates_per_s": p_rate, "requests": cfg["plain_subset"],
+                      "seconds": p_secs, "surface_create_s": p_make,
+                      "how": "one Surface per request, requests one after another, wall clock "
+                             "from seed to result (construction timed apart)"},
+            "served_over_plain": best["node_updates_per_s"] / p_rate,
+            "how": "wall clock from each request's scheduled arrival to its result on the "
+                   "server's clock; throughput = node updates of the rate's requests / the time "
+                   "from its first arrival to its last result"}
 
 
 def time_steps(torch, work, stream, steps, warm, flush, start=0, profile=False):
@@ -372,27 +478,37 @@ def cpu_threads():
     return O.set_threads(os.cpu_count() or 1)
 
 
-def cpu_single(cfg, steps, warm=3):
+def march_due(cfg, i, last):
+    """Whether step i (counted from the first step after setup) repolygonises."""
+    return bool((cfg["march_every"] and (i + 1) % cfg["march_every"] == 0)
+                or (last and cfg["march_end"]))
+
+
+def cpu_single(cfg, steps, warm=3, fp64=False, timed=True):
+    """The oracle on a single-surface config with the device arm's schedule: setup, `warm`
+    untimed steps, then `steps` timed steps (Polys::notify every step, march where the device
+    arm marches). Returns (rate, node updates, seconds, surface, polys)."""
     from oracle import oracle as O
-    s = O.Surface(cfg["size"], cfg["part"], cfg["L"])
+    s = O.Surface(cfg["size"], cfg["part"], cfg["L"], fp64=fp64)
     p = O.Polys(s)
     s.seed((0,) * cfg["D"])
     if cfg["expand"]:
         s.run_steps(cfg["expand"], c=-1.0)
-    for _ in range(warm):
+    for i in range(warm):
         s.update(**cfg["speed"])
         p.notify()
+        if march_due(cfg, i, False):
+            p.march()
     nu, secs = 0.0, 0.0
     for i in range(steps):
         nu += s.band_size()
         t0 = time.perf_counter()
         s.update(**cfg["speed"])
         p.notify()
-        if (cfg["march_every"] and (i + 1) % cfg["march_every"] == 0) or (
-                i == steps - 1 and cfg["march_end"]):
+        if march_due(cfg, warm + i, i == steps - 1):
             p.march()
         secs += time.perf_counter() - t0
-    return nu / secs, nu, secs
+    return (nu / secs if timed and secs else None), nu, secs, s, p
 
 
 def cpu_batch(name, cfg, steps, k):
@@ -425,22 +541,32 @@ def cpu_batch(name, cfg, steps, k):
     return nu / secs, nu, secs
 
 
-def cpu_baseline(name, cfg, steps):
+def cpu_baseline(name, cfg, steps, warm=3):
     threads = cpu_threads()
     if cfg["kind"] == "single":
-        rate, nu, secs = cpu_single(cfg, steps)
-        sample = f"{steps} timed steps after the same setup"
+        rate, nu, secs, _, _ = cpu_single(cfg, steps, warm)
+        sample = f"{steps} timed steps after the same setup and {warm} warm-up steps"
     else:
         k = cfg["cpu_subset"]
         rate, nu, secs = cpu_batch(name, cfg, steps, k)
         sample = f"first {k} surfaces of the workload, {steps} steps each, one after another"
     out = {"value": rate, "unit": "node-updates/s", "cores": threads, "kind": "port",
-           "sample": f"{sample} ({nu:.3g} node-updates in {secs:.2f} s; the reference's "
+           "sample": f"{sample} ({nu:.3g} node-updates in {secs:.2f} s; the reference's seven "
                      f"parallel loops on {threads} threads)"}
     # a step of a single-surface config is the whole workload's step; a batch config's sample
     # is a subset of its surfaces, so its time is not a step of the workload
     step_ms = secs * 1e3 / steps if cfg["kind"] == "single" and steps else None
-    return out, step_ms
+    return out, step_ms, nu
+
+
+def single_config(name, cfg, steps, warmup, node_updates=None):
+    """The config object both arms print for a single-surface workload (same keys and values,
+    so that the two lines describe the same work)."""
+    out = {"workload": cfg["workload"], "name": name, "steps": steps, "warmup": warmup,
+           "parallelism": "replicas1"}
+    if node_updates is not None:
+        out["node_updates"] = int(node_updates)
+    return out
 
 
 def run_reference(args, name, cfg):
@@ -462,14 +588,19 @@ def run_reference(args, name, cfg):
         metric, unit = "local edits/s", "edits/s"
     else:
         steps = args.steps or cfg["steps"]
-        steps = min(steps, 20 if cfg["kind"] == "single" else 10)
-        base, step_ms = cpu_baseline(name, cfg, steps)
+        if cfg["kind"] != "single":
+            steps = min(steps, 10)
+        base, step_ms, nu = cpu_baseline(name, cfg, steps, warm=args.warmup)
+    if cfg["kind"] == "single":
+        config = single_config(name, cfg, steps, args.warmup, nu)
+    else:
+        config = {"workload": cfg["workload"], "name": name}
     line = {
         "impl": "reference", "metric": metric, "value": base["value"],
         "unit": unit, "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "name": name},
+        "config": config,
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -481,42 +612,110 @@ def run_reference(args, name, cfg):
 # Device arm
 # ---------------------------------------------------------------------------------------------
 
-def roofline(fb, work, cfg, stream_steps):
-    units0 = work.work_units()
-    fb.profile_reset()
-    fb.profile_enable(True)
-    for i in range(stream_steps):
-        work.step(10_000 + i, last=(i == stream_steps - 1))
+def roofline(fb, make_work, cfg, steps, warm, ms_per_step, node_updates):
+    """Roofline of the timed steps, replayed on an identical surface (same setup, warm-up and
+    step schedule; the workload is deterministic). Pass A brackets every launch with CUDA events
+    on its stream and ranks the kernels by time (shares); pass B brackets only the dominant
+    kernel, so its launch durations are not inflated by events around the others. achieved =
+    16 B x the work units the kernel processed per launch / its mean launch duration; the
+    whole step's fraction (16 B x node updates / the timed step time) is reported beside it."""
     import torch
-    torch.cuda.synchronize()
-    fb.profile_enable(False)
-    prof = fb.profile_read()
-    units1 = work.work_units()
+    hbm, peak_kind = load_peaks()
+
+    def profiled(only):
+        work = make_work()
+        for i in range(warm):
+            work.step(i)
+        torch.cuda.synchronize()
+        fb.profile_reset()
+        fb.profile_only(only)
+        fb.profile_enable(True)
+        u0 = work.work_units()
+        for i in range(steps):
+            work.step(warm + i, last=(i == steps - 1))
+        torch.cuda.synchronize()
+        fb.profile_enable(False)
+        fb.profile_only(None)
+        prof = fb.profile_read()
+        u1 = work.work_units()
+        work.close()
+        return prof, [b - a for a, b in zip(u0, u1)]
+
+    prof, units = profiled(None)
     tot = sum(v[0] for v in prof.values())
     ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
-    hbm, peak_kind = load_peaks()
+    step_s = ms_per_step * steps * 1e-3
+    step_achieved = BYTES_PER_NODE_UPDATE * node_updates / step_s / 1e9
     out = {"bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_kind": peak_kind,
-           "kernel_ms_per_step": tot / stream_steps,
-           "top_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:10]]}
-    dom = next((k for k, _ in ranked if k in UNIT_BYTES), None)
-    if dom and any(units1[i] - units0[i] for i in range(4)):
-        ms, nl = prof[dom]
-        ui, per = UNIT_BYTES[dom]
-        units = units1[ui] - units0[ui]
-        bpl = per * units / nl
+           "bytes_per_node_update": BYTES_PER_NODE_UPDATE,
+           "step": {"achieved": step_achieved, "frac": step_achieved / hbm,
+                    "bytes": BYTES_PER_NODE_UPDATE * node_updates, "seconds": step_s},
+           "shares_kernel_ms_per_step": tot / steps,
+           "top_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:12]]}
+    dom = next((k for k, _ in ranked if k in UNIT_OF), None)
+    if dom and units[UNIT_OF[dom]]:
+        prof_b, _ = profiled(dom)
+        ms, nl = prof_b[dom]
+        bpl = BYTES_PER_NODE_UPDATE * units[UNIT_OF[dom]] / nl
         achieved = bpl / (ms / nl * 1e-3) / 1e9
         out.update({"kernel": dom, "achieved": achieved, "frac": achieved / hbm,
                     "traffic": None, "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
-                    "share_of_step_kernel_time": ms / tot})
+                    "kernel_ms_per_step": ms / steps, "launches": nl,
+                    "share_of_step": (ms / steps) / ms_per_step,
+                    "is_top_kernel": dom == ranked[0][0]})
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
             try:
-                t = json.load(open(tf)).get(dom)
+                tj = json.load(open(tf))
+                t = tj.get(dom)
                 if t:
-                    out["traffic"] = t["bytes_per_unit"] * units / nl
+                    out["traffic"] = t["bytes_per_unit"] * units[UNIT_OF[dom]] / nl
+                    out["traffic_source"] = t.get("_source") or tj.get("_source")
             except Exception:
                 pass
     return out
+
+
+def capture_single(work):
+    """The device state after the timed steps, for the parity check against the oracle."""
+    s, p = work.s, work.p
+    n = s.partitions()[0]
+    vtx, spx, counts = p.gather(range(n))
+    return {"dump": s.dump(), "snapshot": s.snapshot(), "changes": p.changes(),
+            "totals": p.totals(), "vtx": vtx, "spx": spx, "counts": counts}
+
+
+def single_parity(cfg, dev, o, op, o64, op64):
+    """Device state against the oracle run of the same steps (bit-exact lists, orders,
+    partition lists and simplices; values and vertices within 1e-5), and its error against the
+    FP64 run of the same method."""
+    import numpy as np
+    from oracle import oracle as O
+    from tests.dumps import first_difference
+    diff = first_difference(dev["dump"], o.dump())
+    phi_err = float(np.abs(dev["snapshot"] - o.snapshot()).max())
+    n = o.partitions()[0]
+    poly_ok, vtx_err, pairs = True, 0.0, []
+    v0 = s0 = 0
+    for pc in range(n):
+        nv, ns = (int(x) for x in dev["counts"][pc])
+        gv, gs = dev["vtx"][v0:v0 + nv], dev["spx"][s0:s0 + ns]
+        v0, s0 = v0 + nv, s0 + ns
+        ov, os_, _ = op.partition(pc)
+        if gs.shape != os_.shape or not np.array_equal(gs, os_):
+            poly_ok = False
+        elif ov.size:
+            vtx_err = max(vtx_err, float(np.abs(gv - ov).max()))
+        pairs.append((gv, gs, op64.partition64(pc), op64.partition(pc)[1]))
+    fp64 = O.fp64_errors(dev["snapshot"], o64.snapshot64(), cfg["L"], pairs)
+    ok = diff is None and phi_err <= 1e-5 and poly_ok and vtx_err <= 1e-5 and \
+        list(dev["changes"]) == list(op.changes())
+    return {"matches_oracle": ok, "first_difference": diff, "phi_max_abs_vs_oracle": phi_err,
+            "simplices_equal": poly_ok, "vertex_max_abs_vs_oracle": vtx_err,
+            "tolerance": 1e-5, "fp64": fp64,
+            "how": "device state after the timed steps against the oracle port run of the same "
+                   "setup, warm-up and steps (the CPU baseline run), and against the oracle's "
+                   "FP64 run of the same method"}
 
 
 def ray_inputs(cfg, n, seed):
@@ -819,55 +1018,78 @@ def serve_requests(cfg, lam, shard=0):
     return out
 
 
-def serve_one_rate(fb, cfg, lam, shard=0):
-    """Feeds one rate's stream into a Server in real time; latency and throughput figures."""
-    from felt_b200.serving import Server
-    stream = serve_requests(cfg, lam, shard)
-    srv = Server(layers=cfg["L"], part=cfg["part"], budget_bytes=cfg["budget"],
-                 workers=cfg["workers"])
-    try:
-        t_first = srv.now()
-        for off, req in stream:
-            due = t_first + off
-            while srv.now() < due:
-                time.sleep(min(0.0005, max(0.0, due - srv.now())))
-            req.arrival = due
-            srv.submit(req)
-        if not srv.drain(timeout=900):
-            raise RuntimeError("serving did not drain")
-        res = srv.results()
-        t_end = max((r.done for r in res), default=t_first)
-        lat = sorted(r.latency for r in res)
-        pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] * 1e3) if lat else (lambda q: None)
-        return {"lambda_per_s": lam, "requests": len(stream), "admitted": srv.admitted,
-                "rejected": srv.rejected, "stopped": sum(r.stopped for r in res),
-                "p50_ms": pct(0.50), "p99_ms": pct(0.99),
-                "node_updates_per_s": srv.node_updates / max(t_end - t_first, 1e-9),
-                "node_updates": srv.node_updates, "seconds": t_end - t_first}
-    finally:
-        srv.close()
+def serve_budget(cfg):
+    """The brick-pool budget of the served config, less what the device cannot spare (the pool
+    is allocated up front; 8 GB stay free for the partition tables, arenas and the rest)."""
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    return min(cfg["budget"], max(1e9, free - 8e9 - 2e9 * cfg["slots"] / 512))
+
+
+def serve_one_rate(srv, cfg, lam, shard=0, stream=None):
+    """Feeds one rate's stream into the server in real time (arrival = the scheduled time on
+    the server's clock); latency (arrival to result) and throughput figures."""
+    stream = serve_requests(cfg, lam, shard) if stream is None else stream
+    st0 = srv.stats()
+    t_first = srv.now()
+    for off, req in stream:
+        due = t_first + off
+        while srv.now() < due:
+            time.sleep(min(0.0005, max(0.0, due - srv.now())))
+        req.arrival = due
+        srv.submit(req)
+    if not srv.drain(timeout=900):
+        raise RuntimeError("serving did not drain")
+    ids = {req.rid for _, req in stream}
+    res = [r for r in srv.results() if r.rid in ids]
+    st = srv.stats()
+    t_end = max((r.done for r in res), default=t_first)
+    lat = sorted(r.latency for r in res)
+    pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] * 1e3) if lat else (lambda q: None)
+    nu = st["node_updates"] - st0["node_updates"]
+    steps = st["steps"] - st0["steps"]
+    return {"lambda_per_s": lam, "requests": len(stream),
+            "admitted": st["admitted"] - st0["admitted"],
+            "rejected": st["rejected"] - st0["rejected"], "stopped": sum(r.stopped for r in res),
+            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "mean_ms": 1e3 * sum(lat) / max(len(lat), 1),
+            "node_updates_per_s": nu / max(t_end - t_first, 1e-9), "node_updates": nu,
+            "seconds": t_end - t_first, "batched_steps": steps,
+            "mean_in_flight": sum((r.done - r.admitted) for r in res) / max(t_end - t_first,
+                                                                             1e-9),
+            "peak_reserved_gb": st["peak_reserved_bricks"] * srv.brick_bytes / 1e9,
+            "peak_used_gb": st["peak_used_bricks"] * srv.brick_bytes / 1e9}
 
 
 def serve_plain(fb, cfg, k):
     """The plain path on the first k requests of the 1k/s stream: one Surface (+ Polys) per
-    request, one request after another, wall clock."""
+    request, one request after another, wall clock from the seed to the result (the request's
+    updates, its polygonisation when asked, the node-update count read back). Surface
+    construction is timed apart. Returns (rate, node updates, seconds, construction seconds)."""
     reqs = [r for _, r in serve_requests(cfg, 1000)[:k]]
-    nu, secs = 0, 0.0
+    nu, secs, make = 0, 0.0, 0.0
     for r in reqs:
         t0 = time.perf_counter()
         s = fb.Surface(r.size, cfg["part"], cfg["L"])
         p = fb.Polys(s)
+        t1 = time.perf_counter()
         s.seed(r.centre)
         for _ in range(r.steps):
-            s.update(**r.speed)
+            try:
+                s.update(**r.speed)
+            except fb.FeltError:  # stopped: its convergence loop did not terminate
+                break
             p.notify()
         if r.polys:
             p.march()
+            p.totals()
         n = s.node_updates()
-        secs += time.perf_counter() - t0
+        t2 = time.perf_counter()
+        make += t1 - t0
+        secs += t2 - t1
         nu += n
-        del p, s
-    return nu / secs, nu, secs
+        p.close()
+        s.close()
+    return nu / secs, nu, secs, make
 
 
 def serve_cpu(cfg, k):
@@ -912,14 +1134,22 @@ def run_serve(args, name, cfg):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    # warm-up: one small wave through every code path
-    serve_one_rate(fb, dict(cfg, max_requests=8), 1000, shard=rank)
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = fb.launch_count()
-    sweep = [serve_one_rate(fb, cfg, lam, shard=rank) for lam in cfg["lambdas"]]
-    launches = fb.launch_count() - l0
-    clk = clocks.stop()
+    from felt_b200.serving import Server
+    budget = serve_budget(cfg)
+    srv = Server(layers=cfg["L"], part=cfg["part"], budget_bytes=budget, slots=cfg["slots"],
+                 max_size=cfg["max_size"])
+    try:
+        # warm-up: a few requests through every code path (graph captures, arenas)
+        serve_one_rate(srv, cfg, 1000, shard=rank,
+                       stream=[(t, r) for t, r in serve_requests(cfg, 1000, shard=rank + 99)[:16]])
+        clocks = ClockSampler(local)
+        clocks.start()
+        l0 = fb.launch_count()
+        sweep = [serve_one_rate(srv, cfg, lam, shard=rank) for lam in cfg["lambdas"]]
+        launches = fb.launch_count() - l0
+        clk = clocks.stop()
+    finally:
+        srv.close()
     best = max(sweep, key=lambda r: r["node_updates_per_s"])
     value = best["node_updates_per_s"]
     if pg:
@@ -928,7 +1158,7 @@ def run_serve(args, name, cfg):
     extra = {}
     cpu = None
     if rank == 0:
-        p_rate, _, _ = serve_plain(fb, cfg, cfg["plain_subset"])
+        p_rate, _, _, _ = serve_plain(fb, cfg, cfg["plain_subset"])
         extra["plain"] = {"value": p_rate, "unit": "node-updates/s",
                           "requests": cfg["plain_subset"],
                           "how": "one Surface per request, requests one after another, wall clock"}
@@ -995,41 +1225,62 @@ def run_felt(args, name, cfg):
            "d2h_bytes_per_step": d2h // steps}
 
     extra = {}
-    roof = None
+    roof = cpu = parity = batched = served = None
+    dev_state = None
+    single = cfg["kind"] == "single"
+    if rank == 0 and single and ws == 1 and not args.no_cpu:
+        dev_state = capture_single(work)
+    work.close()
+    del flush
     if rank == 0:
-        roof = roofline(fb, work, cfg, max(cfg["march_every"] or 5, 5))
+        def make_work():
+            return (SingleWork(fb, cfg, args.brick_capacity) if single
+                    else BatchWork(fb, cfg, name, shard=rank))
+        roof = roofline(fb, make_work, cfg, steps, args.warmup, t_ms / steps, nu)
         if cfg["kind"] == "batch" and not args.no_plain:
-            plain = PlainSubset(fb, cfg, name, cfg["plain_subset"])
-            ps = torch.cuda.ExternalStream(0)
-            p_steps = min(steps, 10)
-            t0 = time.perf_counter()
-            nu0 = plain.node_updates()
-            for i in range(p_steps):
-                plain.step(i, last=(i == p_steps - 1))
-            torch.cuda.synchronize()
-            p_rate = (plain.node_updates() - nu0) / (time.perf_counter() - t0)
-            del ps
-            extra["plain"] = {"value": p_rate, "unit": "node-updates/s",
-                              "surfaces": cfg["plain_subset"], "steps": p_steps,
-                              "how": "one Surface per launch sequence, surfaces one after "
-                                     "another, wall clock"}
-            extra["batched_over_plain"] = value / p_rate
-    cpu = None
+            extra["plain_comparison"] = measure_batched(fb, name, min(steps, 20), args.warmup)
+        if name == "c2" and not args.no_extras:
+            # the headline metric's other halves, on the same GPU in the same run: the batched
+            # 3D workload against the plain path, and the served request mix
+            batched = measure_batched(fb, "c4", 20, 3)
+            served = measure_served(fb, "c5", (300, 1000, 3000))
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu, _ = cpu_baseline(name, cfg, args.cpu_steps if cfg["kind"] == "single"
-                              else cfg["cpu_steps"])
+        if single:
+            threads = cpu_threads()
+            rate, cnu, secs, o, op = cpu_single(cfg, steps, args.warmup)
+            cpu = {"value": rate, "unit": "node-updates/s", "cores": threads, "kind": "port",
+                   "sample": f"the same {steps} timed steps after the same setup and "
+                             f"{args.warmup} warm-up steps ({cnu:.3g} node-updates in "
+                             f"{secs:.2f} s; the reference's seven parallel loops on {threads} "
+                             f"threads)"}
+            _, _, _, o64, op64 = cpu_single(cfg, steps, args.warmup, fp64=True, timed=False)
+            parity = single_parity(cfg, dev_state, o, op, o64, op64)
+            parity["oracle_node_updates_equal"] = int(cnu) == int(nu)
+            del o, op, o64, op64, dev_state
+        else:
+            cpu, _, _ = cpu_baseline(name, cfg, cfg["cpu_steps"])
 
     if rank == 0:
-        par = (f"replicas{ws}" if cfg["kind"] == "single"
-               else f"surface shards x{ws} (independent surfaces per rank)")
-        config = {"workload": cfg["workload"], "name": name, "parallelism": par,
-                  "l2": "flushed between timed steps (256 MB write)", "node_updates": nu}
+        if single:
+            config = single_config(name, cfg, steps, args.warmup, nu)
+        else:
+            config = {"workload": cfg["workload"], "name": name,
+                      "parallelism": f"surface shards x{ws} (independent surfaces per rank)",
+                      "node_updates": nu}
         config.update(extra)
         line = {
             "metric": "narrow-band node-updates/s", "value": value, "unit": "node-updates/s",
             "n_gpus": ws, "steps": steps, "warmup": args.warmup, "ms_per_step": t_ms / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config, "roofline": roof, "cpu_baseline": cpu,
+            "data": "synthetic", "config": config,
+            "timing": {"l2": "flushed between timed steps (256 MB write)",
+                       "value": "device time of the timed steps (CUDA events on the surface's "
+                                "stream), inputs resident",
+                       "e2e": "wall clock through the C ABI with the speed going in and the "
+                              "step's result (band size; the re-marched polygons on march "
+                              "steps) coming out each step"},
+            "roofline": roof, "cpu_baseline": cpu, "parity": parity,
+            "batched": batched, "served": served,
             "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
@@ -1048,6 +1299,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default config only: skip the batched and served measurements")
     ap.add_argument("--brick-capacity", type=int, default=0,
                     help="brick pool capacity of single-surface configs (0 = automatic)")
     ap.add_argument("--profile-region", action="store_true",

@@ -127,6 +127,11 @@ def profile_reset():
     _chk(lib().fg_profile_reset())
 
 
+def profile_only(kernel=None):
+    """Bracket only the launches of one kernel while profiling (None = every kernel)."""
+    _chk(lib().fg_profile_only(kernel.encode() if kernel else None))
+
+
 def profile_read():
     """{kernel name: (total ms, launches)} accumulated while profiling was enabled."""
     n = C.c_size_t()

@@ -800,6 +800,11 @@ int fg_profile_reset(void)
 	return guard([&] { fg::prof_reset(); });
 }
 
+int fg_profile_only(const char* kernel)
+{
+	return guard([&] { fg::prof_only(kernel); });
+}
+
 static std::vector<fg::ProfEntry> g_prof_snapshot;
 
 int fg_profile_count(size_t* n)

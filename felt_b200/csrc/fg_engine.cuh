@@ -132,6 +132,8 @@ void add_launches(long long n);
 /// Whether per-launch profiling is on (launches then go one by one, not through graphs).
 bool prof_on();
 void prof_enable(bool on);
+/// Brackets only the launches of the named kernel (NULL or "" = every kernel).
+void prof_only(const char* name);
 /// Synchronises pending events and returns (name, total ms, launches) per kernel name.
 struct ProfEntry {
 	std::string name;

@@ -1,6 +1,7 @@
 // Launch counting and optional per-kernel CUDA-event timing for every kernel of the library.
 #include <atomic>
 #include <map>
+#include <string>
 #include <mutex>
 
 #include "fg_engine.cuh"
@@ -22,6 +23,7 @@ struct Prof {
 	std::map<std::string, std::pair<double, long long>> acc;
 	const char* cur = nullptr;
 	cudaEvent_t cur_a = nullptr;
+	std::string only;  // when set, only launches of this kernel are bracketed
 };
 
 Prof& prof()
@@ -66,6 +68,7 @@ void prof_begin(const char* name, cudaStream_t st)
 	Prof& p = prof();
 	if (!p.on) return;
 	std::lock_guard<std::mutex> lk(p.mu);
+	if (!p.only.empty() && p.only != name) return;
 	p.cur = name;
 	p.cur_a = take(p);
 	cudaEventRecord(p.cur_a, st);
@@ -109,6 +112,13 @@ std::vector<ProfEntry> prof_read()
 	std::vector<ProfEntry> out;
 	for (auto& kv : p.acc) out.push_back(ProfEntry{kv.first, kv.second.first, kv.second.second});
 	return out;
+}
+
+void prof_only(const char* name)
+{
+	Prof& p = prof();
+	std::lock_guard<std::mutex> lk(p.mu);
+	p.only = name ? name : "";
 }
 
 void prof_reset()

@@ -400,6 +400,9 @@ FG_API int fg_surface_info(fg_surface* s, int* dims, int* layers, int* size, int
 FG_API int fg_launch_count(long long* n);
 FG_API int fg_profile_enable(int on);
 FG_API int fg_profile_reset(void);
+/* Limits the event bracketing to launches of one kernel (NULL or "" = every kernel), so that a
+ * kernel can be timed without events around every other launch. */
+FG_API int fg_profile_only(const char* kernel);
 FG_API int fg_profile_count(size_t* n);
 FG_API int fg_profile_entry(size_t i, char* name, size_t name_cap, double* ms, long long* launches);
 
