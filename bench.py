@@ -237,6 +237,9 @@ class SingleWork:
         self.p.close()
         self.s.close()
 
+    def tuning(self):
+        return self.s.tuning()
+
     def _pinned(self, vfloats=16 << 20, sints=24 << 20):
         """Pinned destination arrays (grown by the gather's own fallback if ever too small)."""
         if getattr(self, "_pv", None) is None:
@@ -286,6 +289,9 @@ class BatchWork:
 
     def close(self):
         self.b.close()
+
+    def tuning(self):
+        return self.b.tuning()
 
 
 class PlainSubset:
@@ -650,29 +656,62 @@ def roofline(fb, make_work, cfg, steps, warm, ms_per_step, node_updates):
            "bytes_per_node_update": BYTES_PER_NODE_UPDATE,
            "step": {"achieved": step_achieved, "frac": step_achieved / hbm,
                     "bytes": BYTES_PER_NODE_UPDATE * node_updates, "seconds": step_s},
-           "shares_kernel_ms_per_step": tot / steps,
-           "top_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:12]]}
+           "phase_shares_kernel_ms_per_step": tot / steps,
+           "phase_kernels": [[k, round(v[0] / tot, 4), v[1]] for k, v in ranked[:12]],
+           "phase_kernels_how": "every phase as its own launch, each bracketed by CUDA events "
+                                "(the per-phase path), shares of their summed time"}
     dom = next((k for k, _ in ranked if k in UNIT_OF), None)
     if dom and units[UNIT_OF[dom]]:
         prof_b, _ = profiled(dom)
         ms, nl = prof_b[dom]
         bpl = BYTES_PER_NODE_UPDATE * units[UNIT_OF[dom]] / nl
         achieved = bpl / (ms / nl * 1e-3) / 1e9
-        out.update({"kernel": dom, "achieved": achieved, "frac": achieved / hbm,
-                    "traffic": None, "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
-                    "kernel_ms_per_step": ms / steps, "launches": nl,
-                    "share_of_step": (ms / steps) / ms_per_step,
-                    "is_top_kernel": dom == ranked[0][0]})
+        out["phase_kernel"] = {"kernel": dom, "achieved": achieved, "frac": achieved / hbm,
+                               "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
+                               "ms_per_step": ms / steps, "launches": nl}
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
             try:
                 tj = json.load(open(tf))
                 t = tj.get(dom)
                 if t:
-                    out["traffic"] = t["bytes_per_unit"] * units[UNIT_OF[dom]] / nl
-                    out["traffic_source"] = t.get("_source") or tj.get("_source")
+                    out["phase_kernel"]["traffic"] = t["bytes_per_unit"] * units[UNIT_OF[dom]] / nl
             except Exception:
                 pass
+    # the kernel the timed steps run: the persistent update launch when it is in use (one per
+    # step, timed alone), else the dominant per-phase kernel
+    work = make_work()
+    persistent = work.tuning()["launch_mode"] == 1
+    work.close()
+    if persistent:
+        work = make_work()
+        for i in range(warm):
+            work.step(i)
+        torch.cuda.synchronize()
+        nu0 = work.node_updates()
+        fb.profile_reset()
+        fb.profile_only("k_update_step")
+        fb.profile_enable(True)
+        for i in range(steps):
+            work.step(warm + i, last=(i == steps - 1))
+        torch.cuda.synchronize()
+        fb.profile_enable(False)
+        fb.profile_only(None)
+        ms, nl = fb.profile_read()["k_update_step"]
+        nu_k = work.node_updates() - nu0
+        work.close()
+        bpl = BYTES_PER_NODE_UPDATE * nu_k / nl
+        achieved = bpl / (ms / nl * 1e-3) / 1e9
+        out.update({"kernel": "k_update_step", "achieved": achieved, "frac": achieved / hbm,
+                    "traffic": None, "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
+                    "kernel_ms_per_step": ms / steps, "launches": nl,
+                    "share_of_step": (ms / steps) / ms_per_step})
+    elif "phase_kernel" in out:
+        pk = out["phase_kernel"]
+        out.update({"kernel": pk["kernel"], "achieved": pk["achieved"], "frac": pk["frac"],
+                    "traffic": pk.get("traffic"), "bytes_per_launch": pk["bytes_per_launch"],
+                    "avg_launch_us": pk["avg_launch_us"], "kernel_ms_per_step": pk["ms_per_step"],
+                    "launches": pk["launches"], "share_of_step": pk["ms_per_step"] / ms_per_step})
     return out
 
 

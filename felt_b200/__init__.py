@@ -39,7 +39,25 @@ class Speed(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("brick_capacity", C.c_size_t), ("vertex_capacity", C.c_size_t),
-                ("use_graph", C.c_int), ("reserved", C.c_int * 7)]
+                ("launch_mode", C.c_int), ("dist_split", C.c_int), ("record_passes", C.c_int),
+                ("blocks_per_sm", C.c_int), ("reserved", C.c_int * 4)]
+
+
+def make_config(brick_capacity=0, vertex_capacity=0, launch_mode=0, dist_split=0,
+                record_passes=0, blocks_per_sm=0):
+    """fg_config: pool sizes and launch tuning (launch_mode 0 automatic, 1 persistent, 2 one
+    kernel per phase; dist_split warps per partition entry in the first distance pass;
+    record_passes 1 warp / 2 block per entry in the recording passes; blocks_per_sm of the
+    persistent launch; 0 = automatic everywhere)."""
+    return Config(int(brick_capacity), int(vertex_capacity), int(launch_mode), int(dist_split),
+                  int(record_passes), int(blocks_per_sm))
+
+
+def _tuning(fn, h):
+    out = (C.c_int * 4)()
+    _chk(fn(h, out))
+    return dict(launch_mode=out[0], dist_split=out[1], record_passes=out[2],
+                blocks_per_sm=out[3])
 
 
 def build():
@@ -157,12 +175,13 @@ def make_speed(c=None, a=None, n=None, seed=0):
 class Surface:
     """Felt::Surface<D,L>(size, size_partition) on the GPU (include/Felt/Surface.hpp:163-173)."""
 
-    def __init__(self, size, part, layers, brick_capacity=0, vertex_capacity=0):
+    def __init__(self, size, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
+        """tuning: launch_mode, dist_split, record_passes, blocks_per_sm (see make_config)."""
         self.D = len(size)
         self.L = int(layers)
         self.size = tuple(int(s) for s in size)
         self.part = tuple(int(p) for p in part)
-        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
+        cfg = make_config(brick_capacity, vertex_capacity, **tuning)
         h = C.c_void_p()
         _chk(lib().fg_surface_create(self.D, self.L, _ivec(size), _ivec(part), C.byref(cfg),
                                      C.byref(h)))
@@ -197,6 +216,15 @@ class Surface:
     def update_end(self):
         _chk(lib().fg_update_end(self._h))
 
+    def check_step_timeout(self, wait_s=0.2):
+        """fg_check_step_timeout: the persistent update launch with a barrier that can never
+        complete; returns the status code (FG_ERR_TIMEOUT, -14, expected)."""
+        return int(lib().fg_check_step_timeout(self._h, C.c_double(wait_s)))
+
+    def tuning(self):
+        """The launch tuning in effect (fg_surface_tuning)."""
+        return _tuning(lib().fg_surface_tuning, self._h)
+
     def snapshot(self):
         n = int(np.prod(self.size))
         out = np.zeros(n, dtype=np.float32)
@@ -223,11 +251,11 @@ class Surface:
         return bytes(buf)
 
     @classmethod
-    def load(cls, data, brick_capacity=0, vertex_capacity=0):
+    def load(cls, data, brick_capacity=0, vertex_capacity=0, **tuning):
         """Surface::load (include/Felt/Surface.hpp:185-196): a new surface from a surface file
         (bytes); dimensions, layers and sizes come from the file."""
         raw = (C.c_uint8 * len(data)).from_buffer_copy(data)
-        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
+        cfg = make_config(brick_capacity, vertex_capacity, **tuning)
         h = C.c_void_p()
         _chk(lib().fg_load(raw, C.c_size_t(len(data)), C.byref(cfg), C.byref(h)))
         obj = cls.__new__(cls)
@@ -340,14 +368,15 @@ class Batch:
     """Many independent Surface<D,L> (same D, L, partition shape; any grid sizes) advanced by the
     same kernel launches. Per surface the results equal a separate Surface's."""
 
-    def __init__(self, sizes, part, layers, brick_capacity=0, vertex_capacity=0):
+    def __init__(self, sizes, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
+        """tuning: launch_mode, dist_split, record_passes, blocks_per_sm (see make_config)."""
         self.n = len(sizes)
         self.D = len(part)
         self.L = int(layers)
         self.part = tuple(int(p) for p in part)
         self.sizes = [tuple(int(x) for x in s) for s in sizes]
         flat = [x for s in self.sizes for x in s]
-        cfg = Config(int(brick_capacity), int(vertex_capacity), 0)
+        cfg = make_config(brick_capacity, vertex_capacity, **tuning)
         h = C.c_void_p()
         _chk(lib().fg_batch_create(self.D, self.L, _ivec(part), C.c_size_t(self.n), _ivec(flat),
                                    C.byref(cfg), C.byref(h)))
@@ -482,6 +511,10 @@ class Batch:
         p = C.c_void_p()
         _chk(lib().fg_batch_stream(self._h, C.byref(p)))
         return p.value or 0
+
+    def tuning(self):
+        """The launch tuning in effect (fg_batch_tuning)."""
+        return _tuning(lib().fg_batch_tuning, self._h)
 
 
 class Polys:

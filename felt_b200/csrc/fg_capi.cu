@@ -48,6 +48,23 @@ fg::Speed to_speed(const fg_speed* s)
 	return fg::Speed{s->kind, s->c, s->a, s->n, s->seed};
 }
 
+void apply_tuning(fg::EngineBase& eng, const fg_config* cfg)
+{
+	if (!cfg) return;
+	if (cfg->launch_mode < 0 || cfg->launch_mode > 2)
+		throw fg::Error(FG_ERR_ARG, "launch_mode must be 0, 1 or 2");
+	if (cfg->dist_split != 0 && cfg->dist_split != 1 && cfg->dist_split != 2 &&
+	    cfg->dist_split != 4 && cfg->dist_split != 8)
+		throw fg::Error(FG_ERR_ARG, "dist_split must be 0, 1, 2, 4 or 8");
+	if (cfg->record_passes < 0 || cfg->record_passes > 2)
+		throw fg::Error(FG_ERR_ARG, "record_passes must be 0, 1 or 2");
+	if (cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 32)
+		throw fg::Error(FG_ERR_ARG, "blocks_per_sm must be in 0..32");
+	if (cfg->launch_mode == 1 && !eng.persistent_available())
+		throw fg::Error(FG_ERR_ARG, "the persistent update launch is not available here");
+	eng.set_tuning(cfg->launch_mode, cfg->dist_split, cfg->record_passes, cfg->blocks_per_sm);
+}
+
 void put_list(const std::vector<uint32_t>& v, uint32_t* out, size_t cap, size_t* n)
 {
 	need(n, "count");
@@ -90,6 +107,7 @@ int fg_surface_create(int dims, int layers, const int* size, const int* part, co
 		if (cfg) s->vertex_capacity = cfg->vertex_capacity;
 		FG_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
 		s->eng.reset(fg::make_engine(d, s->st));
+		apply_tuning(*s->eng, cfg);
 		*out = s.release();
 	});
 }
@@ -513,6 +531,7 @@ int fg_batch_create(int dims, int layers, const int* part, size_t n, const int* 
 		if (cfg) b->vertex_capacity = cfg->vertex_capacity;
 		FG_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
 		b->eng.reset(fg::make_engine(d, b->st));
+		apply_tuning(*b->eng, cfg);
 		b->eng->set_throw_on_freeze(false);
 		*out = b.release();
 	});
@@ -798,6 +817,33 @@ int fg_profile_enable(int on)
 int fg_profile_reset(void)
 {
 	return guard([&] { fg::prof_reset(); });
+}
+
+int fg_check_step_timeout(fg_surface* s, double wait_s)
+{
+	return guard([&] {
+		need(s, "surface");
+		if (!(wait_s > 0) || wait_s > 30) throw fg::Error(FG_ERR_ARG, "wait_s must be in (0, 30]");
+		s->eng->check_step_timeout(wait_s);
+	});
+}
+
+int fg_surface_tuning(fg_surface* s, int* out)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(out, "out");
+		s->eng->tuning(out);
+	});
+}
+
+int fg_batch_tuning(fg_batch* b, int* out)
+{
+	return guard([&] {
+		need(b, "batch");
+		need(out, "out");
+		b->eng->tuning(out);
+	});
 }
 
 int fg_profile_only(const char* kernel)

@@ -4,6 +4,7 @@
 
 #include "fg_engine.cuh"
 #include "fg_kernels.cuh"
+#include "fg_step.cuh"
 
 namespace fg {
 
@@ -253,6 +254,10 @@ public:
 		zcount_ = dalloc<unsigned long long>(1, o);
 		d_iters_ = dalloc<int>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
+		d_bar_ = dalloc<unsigned>(2, o);
+		d_out_ = dalloc<int>(4, o);
+		d_newfrozen_ = dalloc<int>(S, o);
+		FG_CUDA(cudaMemsetAsync(d_newfrozen_, 0, S * sizeof(int), st_));
 
 		fill(P.slot, NP, -1);
 		fillf(P.bg, NP, (float)(L + 1));
@@ -308,7 +313,171 @@ public:
 		} else {
 			smem_flush_ = 0;  // brick too large to stage: replay in global memory
 		}
+		setup_persistent();
 	}
+
+	/// Shared memory and resident blocks of the persistent update launch (k_update_step). It
+	/// is off where the device cannot launch cooperatively or a block's staging does not fit.
+	void setup_persistent()
+	{
+		persistent_ok_ = false;
+		int dev = 0, coop = 0;
+		if (cudaGetDevice(&dev) != cudaSuccess ||
+		    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) {
+			cudaGetLastError();
+			return;
+		}
+		size_t smem = smem_sort_;
+		if (smem_halo_) smem = std::max(smem, smem_halo_);
+		if (smem_flush_) smem = std::max(smem, smem_flush_);
+		step_smem_ = (smem + 15) & ~(size_t)15;
+		if (step_smem_ > 160 * 1024) return;
+		if (step_smem_ > 48 * 1024 &&
+		    cudaFuncSetAttribute(k_update_step<D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                         (int)step_smem_) != cudaSuccess) {
+			cudaGetLastError();
+			return;
+		}
+		int per_sm = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_step<D, L>, 256,
+		                                                  step_smem_) != cudaSuccess ||
+		    per_sm < 1) {
+			cudaGetLastError();
+			return;
+		}
+		step_max_per_sm_ = per_sm;
+		persistent_ok_ = true;
+	}
+
+public:
+	/// Launch tuning (fg_config): how the global update launches (0 automatic, 1 persistent,
+	/// 2 one kernel per phase), warps per partition entry in the first distance pass (0 =
+	/// automatic), warp (1) or block (2) per entry in the record passes (0 = automatic), and
+	/// blocks per SM of the persistent launch (0 = as many as fit, at most 4).
+	void set_tuning(int launch_mode, int dist_split, int record_passes, int blocks_per_sm) override
+	{
+		launch_mode_ = launch_mode;
+		if (dist_split > 0) dist_split_ = dist_split;
+		if (record_passes == 1) block_passes_ = false;
+		if (record_passes == 2) block_passes_ = true;
+		step_blocks_per_sm_ = blocks_per_sm;
+	}
+	bool persistent_available() const override { return persistent_ok_; }
+	void tuning(int* out) const override
+	{
+		out[0] = use_persistent() ? 1 : 2;
+		out[1] = dist_split_;
+		out[2] = block_passes_ ? 2 : 1;
+		out[3] = step_blocks();
+	}
+
+private:
+	bool use_persistent() const
+	{
+		return persistent_ok_ && launch_mode_ != 2 && !prof_per_launch();
+	}
+	int step_blocks() const
+	{
+		int per_sm = step_max_per_sm_;
+		if (step_blocks_per_sm_ > 0) per_sm = std::min(per_sm, step_blocks_per_sm_);
+		else per_sm = std::min(per_sm, 4);
+		return per_sm;
+	}
+
+	StepArgs step_args(bool curv) const
+	{
+		StepArgs a;
+		std::memset(&a, 0, sizeof(a));
+		a.speeds = d_speeds_;
+		a.bar = d_bar_;
+		a.out = d_out_;
+		a.newfrozen = d_newfrozen_;
+		a.acc = acc_;
+		a.wait_ns = 2000000000ull;
+		a.clear_status = status_dirty_ ? 1 : 0;
+		a.clear_buf0 = buf_dirty_[0] ? 1 : 0;
+		a.clear_buf1 = buf_dirty_[1] ? 1 : 0;
+		a.delta_smem = (curv && smem_halo_) ? 1 : 0;
+		a.block_passes = block_passes_ ? 1 : 0;
+		a.flush_smem = smem_flush_ ? 1 : 0;
+		a.split = dist_split_;
+		a.max_iters = kMaxIterations;
+		return a;
+	}
+
+	void launch_step(const StepArgs& a)
+	{
+		FG_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), st_));
+		FG_CUDA(cudaMemsetAsync(d_out_, 0, 4 * sizeof(int), st_));
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(step_blocks() * sm_count());
+		cfg.blockDim = dim3(256);
+		cfg.dynamicSmemBytes = step_smem_;
+		cfg.stream = st_;
+		cudaLaunchAttribute at[1];
+		at[0].id = cudaLaunchAttributeCooperative;
+		at[0].val.cooperative = 1;
+		cfg.attrs = at;
+		cfg.numAttrs = 1;
+		cudaError_t e = cudaSuccess;
+		FG_RUN("k_update_step", st_, e = cudaLaunchKernelEx(&cfg, k_update_step<D, L>, P_, a););
+		if (e != cudaSuccess)
+			throw Error(-2, std::string("persistent update launch: ") + cudaGetErrorString(e));
+	}
+
+	/// After a persistent launch that ran update_end_global: the host-side record of what it
+	/// left (the status grid and the last recorded buffer need resets at the next update start,
+	/// the surfaces it stopped), then the error check.
+	void finish_persistent()
+	{
+		int out[4] = {0, 0, 0, 0};
+		FG_CUDA(cudaMemcpyAsync(out, d_out_, sizeof(out), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		check_errors();
+		status_dirty_ = true;
+		const int cur = out[1] ? 1 : 0;
+		buf_dirty_[cur] = true;
+		buf_dirty_[1 - cur] = false;
+		stats_.iterations = out[0];
+		if (out[2]) {
+			std::vector<int> nf((size_t)P_.S);
+			FG_CUDA(cudaMemcpyAsync(nf.data(), d_newfrozen_, nf.size() * sizeof(int),
+			                        cudaMemcpyDeviceToHost, st_));
+			FG_CUDA(cudaMemsetAsync(d_newfrozen_, 0, nf.size() * sizeof(int), st_));
+			FG_CUDA(cudaStreamSynchronize(st_));
+			for (int s = 0; s < P_.S; s++)
+				if (nf[s] && !frozen_[s]) {
+					frozen_[s] = 1;
+					newly_frozen_.push_back(s);
+				}
+			push_stopped();
+		}
+		if (!newly_frozen_.empty() && throw_on_freeze_) {
+			newly_frozen_.clear();
+			throw Error(-14, "the convergence loop of the update did not terminate (layer "
+			                 "changes keep oscillating, typically where the band meets the grid "
+			                 "edge); the surface is stopped");
+		}
+		newly_frozen_.clear();
+	}
+
+public:
+	/// Runs the persistent update kernel with a grid barrier that can never complete, to check
+	/// that its bounded waits give up: throws FG_ERR_TIMEOUT after about wait_s seconds, having
+	/// changed nothing (the kernel stops at its entry barrier, before any work).
+	void check_step_timeout(double wait_s) override
+	{
+		if (!persistent_ok_) throw Error(-1, "the persistent update launch is not available");
+		StepArgs a = step_args(false);
+		a.stall = 1;
+		a.wait_ns = (unsigned long long)(wait_s * 1e9);
+		a.do_begin = a.do_delta = a.do_finish = 1;
+		launch_step(a);
+		FG_CUDA(cudaStreamSynchronize(st_));
+		check_errors();
+	}
+
+private:
 
 	~Engine() override
 	{
@@ -453,6 +622,18 @@ public:
 	// ---- global update ----
 	void update_builtin(const Speed* speeds) override
 	{
+		if (use_persistent()) {
+			check_not_frozen();
+			FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed),
+			                        cudaMemcpyHostToDevice, st_));
+			bool any_curv = false;
+			for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
+			StepArgs a = step_args(any_curv);
+			a.do_begin = a.do_delta = a.do_finish = 1;
+			launch_step(a);
+			finish_persistent();
+			return;
+		}
 		update_begin_global();
 		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
@@ -468,6 +649,14 @@ public:
 	void update_begin_global() override
 	{
 		check_not_frozen();
+		if (use_persistent()) {
+			StepArgs a = step_args(false);
+			a.do_begin = 1;
+			launch_step(a);
+			status_dirty_ = false;
+			buf_dirty_[0] = buf_dirty_[1] = false;
+			return;
+		}
 		update_start();
 		// delta.track_children(isogrid) on freshly reset delta lists = a copy of the lists.
 		copy_plists();
@@ -478,6 +667,13 @@ public:
 
 	void update_finish_global() override
 	{
+		if (use_persistent()) {
+			StepArgs a = step_args(false);
+			a.do_finish = 1;
+			launch_step(a);
+			finish_persistent();
+			return;
+		}
 		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
 		// update_zero_layer(&affected_buffer)
 		scan(P_.pcnt, L, 0);
@@ -1264,6 +1460,14 @@ private:
 	unsigned long long* acc_ = nullptr;     // node updates of all global updates so far
 	unsigned long long* zcount_ = nullptr;  // zero-layer leaf count of a bounded update
 	int* d_iters_ = nullptr;                 // iteration count of the device-side loop
+	unsigned* d_bar_ = nullptr;              // grid barrier of the persistent update launch
+	int* d_out_ = nullptr;                   // what the persistent launch reports back
+	int* d_newfrozen_ = nullptr;             // [S] surfaces the persistent launch stopped
+	bool persistent_ok_ = false;             // the persistent launch can run on this device
+	int step_max_per_sm_ = 0;                // its resident blocks per SM at most
+	int step_blocks_per_sm_ = 0;             // blocks per SM asked for (0 = automatic)
+	size_t step_smem_ = 0;                   // its dynamic shared memory
+	int launch_mode_ = 0;                    // 0 automatic, 1 persistent, 2 one kernel per phase
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;

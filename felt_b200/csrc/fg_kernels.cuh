@@ -57,10 +57,9 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 // mode 0: cnt[s*NL + l]; mode 1: cnt[s*NL] + cnt[s*NL + NL-1]; mode 2: sum over layers.
 // Frozen surfaces (frozen[s] != 0) contribute no entries, so no kernel works on them.
 // ---------------------------------------------------------------------------------------------
-static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff,
-                                     const int* frozen)
+static __device__ __noinline__ void d_scan_counts(const int* cnt, int NL, int l, int mode, int S,
+                                                  int* woff, const int* frozen)
 {
-	pdl_enter();
 	__shared__ int carry;
 	if (threadIdx.x == 0) {
 		carry = 0;
@@ -86,11 +85,17 @@ static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, in
 		__syncthreads();
 	}
 }
-
-/// k_scan_counts mode 0 for every layer index at once: woffl[l*(S+1) + s].
-static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, const int* frozen)
+static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, int S, int* woff,
+                                     const int* frozen)
 {
 	pdl_enter();
+	d_scan_counts(cnt, NL, l, mode, S, woff, frozen);
+}
+
+/// k_scan_counts mode 0 for every layer index at once: woffl[l*(S+1) + s].
+static __device__ __noinline__ void d_scan_layers(const int* cnt, int NL, int S, int* woffl,
+                                                  const int* frozen)
+{
 	__shared__ int carry;
 	for (int l = 0; l < NL; l++) {
 		int* woff = woffl + (size_t)l * (S + 1);
@@ -111,12 +116,26 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 		}
 	}
 }
+static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, const int* frozen)
+{
+	pdl_enter();
+	d_scan_layers(cnt, NL, S, woffl, frozen);
+}
 
-#define FG_WARP_LOOP(woff_)                                                         \
+/// The block index and block count a kernel body works with: the hardware grid's when the body
+/// runs as its own launch, or a share of a persistent launch's blocks when it runs as one phase
+/// of the whole-update kernel (fg_step.cuh).
+struct GridPos {
+	int bid, nb;
+};
+__device__ __forceinline__ GridPos hw_grid() { return GridPos{(int)blockIdx.x, (int)gridDim.x}; }
+
+#define FG_WARP_LOOP_G(woff_, G_)                                                   \
 	const int lane = lane_id();                                                     \
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;                              \
+	const int nwarps = ((G_).nb * blockDim.x) >> 5;                                \
 	const int total = (woff_)[P.S];                                                 \
-	for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < total; e += nwarps)
+	for (int e = ((G_).bid * blockDim.x + threadIdx.x) >> 5; e < total; e += nwarps)
+#define FG_WARP_LOOP(woff_) FG_WARP_LOOP_G(woff_, G)
 
 // ---------------------------------------------------------------------------------------------
 // status_change (Surface.hpp:1138-1178) for one 32-leaf chunk of partition gp processed by a
@@ -252,9 +271,8 @@ __device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int f
 // leaf, written to the brick's delta array.
 // ---------------------------------------------------------------------------------------------
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds)
+__device__ void d_delta_builtin(const Dev& P, const Speed* speeds, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -271,6 +289,12 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 		}
 		if (lane == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
 	}
+}
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds)
+{
+	pdl_enter();
+	d_delta_builtin<D, L>(P, speeds, hw_grid());
 }
 
 /// Fills box with the isogrid over a partition and a one-node halo ((part+2)^D values, row-major,
@@ -335,13 +359,11 @@ __host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
 /// curvature term: every stencil read of the zero-layer nodes hits shared memory. One block per
 /// zero-layer partition.
 template <int D, int L>
-__global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
+__device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float* hbox)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
-	extern __shared__ float hbox[];
 	const int total = P.woff[P.S];
-	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+	for (int e = G.bid; e < total; e += G.nb) {
 		const int s = entry_surface(P.woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const Speed sp = speeds[s];
@@ -366,20 +388,26 @@ __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
 		__syncthreads();
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
+{
+	pdl_enter();
+	extern __shared__ float hbox[];
+	d_delta_smem<D, L>(P, speeds, hw_grid(), hbox);
+}
 
 /// update_zero_layer (Surface.hpp:920-979) over the isogrid's zero-layer lists, which the delta
 /// grid mirrors in the global update. One block per partition entry (bricks of thousands of
 /// leaves): every thread applies one leaf, and the rare layer changes are recorded in list order
 /// (status_round).
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const int* ncount, int b)
+__device__ void d_zero_apply(const Dev& P, ListView lv, const int* ncount, int b, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	__shared__ uint16_t cl[256];
 	__shared__ int ct[256];
 	const int total = P.woff[P.S];
-	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+	for (int e = G.bid; e < total; e += G.nb) {
 		const int s = entry_surface(P.woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const int gp = g.pbase + lv.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
@@ -410,13 +438,18 @@ __global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const in
 		}
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_zero_apply(Dev P, ListView lv, const int* ncount, int b)
+{
+	pdl_enter();
+	d_zero_apply<D, L>(P, lv, ncount, b, hw_grid());
+}
 
 /// update_zero_layer (Surface.hpp:920-979) over the isogrid's zero-layer lists, which the delta
 /// grid mirrors in the global update. One warp per partition entry (bricks of few leaves).
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, const int* ncount, int b)
+__device__ void d_zero_apply_warp(const Dev& P, ListView lv, const int* ncount, int b, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -448,6 +481,12 @@ __global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, con
 		flags = warp_or(flags);
 		if (lane == 0) P.eflag[e] = flags;
 	}
+}
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_zero_apply_warp(Dev P, ListView lv, const int* ncount, int b)
+{
+	pdl_enter();
+	d_zero_apply_warp<D, L>(P, lv, ncount, b, hw_grid());
 }
 
 /// Appends, in the pass's partition order, the partitions that gained status changes to the
@@ -549,21 +588,14 @@ __global__ void __launch_bounds__(256) k_compact(Dev P, CompactArgs a)
 /// buffer lists, none of which this pass reads, so it overlaps this pass instead of taking a
 /// launch of its own.
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
-                                               float side, int split, CompactArgs ca)
+__device__ void d_dist1_work(const Dev& P, const int* woff, ListView lv, int k, float side,
+                             int split, int first_warp, int nwarps)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
-	if ((int)blockIdx.x < ca.nblocks) {
-		compact_surface<L>(P, ca, blockIdx.x);
-		return;
-	}
 	const int li = k + L;
 	const int lane = lane_id();
-	const int nwarps = ((gridDim.x - ca.nblocks) * blockDim.x) >> 5;
 	const int total = woff[P.S] * split;
-	for (int v = ((blockIdx.x - ca.nblocks) * blockDim.x + threadIdx.x) >> 5; v < total;
-	     v += nwarps) {
+	for (int v = first_warp; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
 		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
@@ -586,20 +618,45 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView 
 		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
+                                               float side, int split, CompactArgs ca)
+{
+	pdl_enter();
+	if ((int)blockIdx.x < ca.nblocks) {
+		compact_surface<L>(P, ca, blockIdx.x);
+		return;
+	}
+	d_dist1_work<D, L>(P, woff, lv, k, side, split,
+	                   ((blockIdx.x - ca.nblocks) * blockDim.x + threadIdx.x) >> 5,
+	                   ((gridDim.x - ca.nblocks) * blockDim.x) >> 5);
+}
+/// k_dist1 as a phase of a persistent launch: the previous pass's compaction (one surface per
+/// block, in turn), then the distance pass over all the launch's warps.
+template <int D, int L>
+__device__ void d_dist1(const Dev& P, const int* woff, ListView lv, int k, float side, int split,
+                        const CompactArgs& ca, GridPos G)
+{
+	for (int s = G.bid; s < ca.nblocks; s += G.nb) {
+		compact_surface<L>(P, ca, s);
+		__syncthreads();
+	}
+	d_dist1_work<D, L>(P, woff, lv, k, side, split, (G.bid * blockDim.x + threadIdx.x) >> 5,
+	                   (G.nb * blockDim.x) >> 5);
+}
 
 /// update_distance second pass (Surface.hpp:1075-1121): apply and record status changes. One
 /// block per partition entry (bricks of thousands of leaves): every thread commits one leaf,
 /// and the rare layer changes are recorded in list order (status_round).
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
+__device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
 	__shared__ uint16_t cl[256];
 	__shared__ int ct[256];
 	const int total = woff[P.S];
-	for (int e = blockIdx.x; e < total; e += gridDim.x) {
+	for (int e = G.bid; e < total; e += G.nb) {
 		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
@@ -631,14 +688,19 @@ __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView 
 		}
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
+{
+	pdl_enter();
+	d_dist2<D, L>(P, woff, lv, k, b, hw_grid());
+}
 
 /// k_dist2 with one warp per partition entry (bricks of few leaves). The next chunk's list
 /// entry and delta are loaded before the current chunk's status records (which must stay in
 /// list order), so the two load latencies overlap the record work.
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, ListView lv, int k, int b)
+__device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
 	FG_WARP_LOOP(woff)
@@ -681,6 +743,12 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 		}
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, ListView lv, int k, int b)
+{
+	pdl_enter();
+	d_dist2_warp<D, L>(P, woff, lv, k, b, hw_grid());
+}
 
 // ---------------------------------------------------------------------------------------------
 // flush_status_change (Surface.hpp:1183-1244) with Untrack::retrack / untrack
@@ -689,12 +757,11 @@ __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, List
 // partition, and records the children-level events for k_flush_plist.
 // ---------------------------------------------------------------------------------------------
 template <int D, int L>
-__global__ void k_flush_leaf(Dev P)
+__device__ void d_flush_leaf(const Dev& P, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_SUNION];
-	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+	for (int e = G.bid * blockDim.x + threadIdx.x; e < n; e += G.nb * blockDim.x) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
 		const size_t bv = (size_t)P.BV;
@@ -760,6 +827,12 @@ __global__ void k_flush_leaf(Dev P)
 		}
 	}
 }
+template <int D, int L>
+__global__ void k_flush_leaf(Dev P)
+{
+	pdl_enter();
+	d_flush_leaf<D, L>(P, hw_grid());
+}
 
 /// Shared-memory bytes k_flush_smem needs for a brick of BV leaves.
 __host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
@@ -784,12 +857,10 @@ __host__ __device__ inline size_t flush_smem_bytes(int BV, int NL)
 /// (to == from: it changed twice in one iteration) is removed and re-appended within its own
 /// phase by the removal lane.
 template <int D, int L>
-__global__ void __launch_bounds__(128) k_flush_smem(Dev P)
+__device__ void d_flush_smem(const Dev& P, GridPos G, unsigned char* fsm)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	constexpr uint16_t TAG = 0x8000u;
-	extern __shared__ __align__(16) unsigned char fsm[];
 	const int BV = P.BV;
 	uint16_t* slkp = (uint16_t*)fsm;       // [BV] positions of the leaves the removals touch
 	uint16_t* schg = slkp + BV;            // [BV] status entries, phase-major
@@ -807,7 +878,7 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 	constexpr int LONG_CHAIN = 64;
 	__shared__ int take;
 	for (int sweep = 0; sweep < 2; sweep++)
-	for (int e = blockIdx.x; e < n; e += gridDim.x) {
+	for (int e = G.bid; e < n; e += G.nb) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
 		if (threadIdx.x == 0) {
@@ -997,6 +1068,13 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 		__syncthreads();
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(128) k_flush_smem(Dev P)
+{
+	pdl_enter();
+	extern __shared__ __align__(16) unsigned char fsm[];
+	d_flush_smem<D, L>(P, hw_grid(), fsm);
+}
 
 /// Children-level half of the flush: one block per (surface, list k) replays, in the
 /// reference's order (from-layer ascending, then status partition list order), the appends to
@@ -1004,15 +1082,13 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 /// read the leaf flush's records (app, rem), which this kernel does not change: the block loads
 /// a tile of them into shared memory at once, then one warp replays the (rare) events in order.
 template <int L>
-__global__ void __launch_bounds__(256) k_flush_plist(Dev P)
+__device__ void d_flush_plist(const Dev& P, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	constexpr int TILE = 2048;
 	__shared__ int slp[TILE];
 	__shared__ unsigned char sev[TILE];  // 1 append, 2 removal
-	const int w = blockIdx.x;
-	if (w >= P.S * NL) return;
+	for (int w = G.bid; w < P.S * NL; w += G.nb) {
 	const int lane = lane_id();
 	const int s = w / NL, k = w % NL;
 	const SurfGeom& g = P.geom[s];
@@ -1072,6 +1148,14 @@ __global__ void __launch_bounds__(256) k_flush_plist(Dev P)
 		}
 	}
 	if (threadIdx.x == 0) P.pcnt[s * NL + k] = cnt;
+	__syncthreads();
+	}
+}
+template <int L>
+__global__ void __launch_bounds__(256) k_flush_plist(Dev P)
+{
+	pdl_enter();
+	d_flush_plist<L>(P, hw_grid());
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1085,15 +1169,14 @@ __global__ void __launch_bounds__(256) k_flush_plist(Dev P)
 // 2 compute the winners' distances into the delta array.
 // ---------------------------------------------------------------------------------------------
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
+__device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	// Modes 1 and 2 take the candidates that mode 0 recorded, one thread each, unless there
 	// were more than the buffer holds: then they walk the status lists like mode 0.
 	const int ncand = P.counters[CNT_CAND];
 	if (mode > 0 && ncand <= P.cand_cap) {
-		for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
+		for (int i = G.bid * blockDim.x + threadIdx.x; i < ncand; i += G.nb * blockDim.x) {
 			const unsigned long long key = P.cand_key[i];
 			const int gpn = P.cand_gp[i], leafn = P.cand_leaf[i];
 			const int sn = P.slot[gpn];
@@ -1176,6 +1259,12 @@ __global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
 		}
 	}
 }
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_expand_gen(Dev P, int mode)
+{
+	pdl_enter();
+	d_expand_gen<D, L>(P, mode, hw_grid());
+}
 
 /// Reset a brick to an activated, empty partition: values = background, no lists.
 template <int L>
@@ -1201,12 +1290,11 @@ __device__ void brick_init(const Dev& P, int sl, float bgv, int tid, int nth)
 
 /// Child activation (TrackedMixin.hpp:37-41) of queued partitions: one block per partition.
 template <int L>
-__global__ void k_activate(Dev P)
+__device__ void d_activate(const Dev& P, GridPos G)
 {
-	pdl_enter();
 	__shared__ int sl;
 	const int n = P.counters[CNT_ACT];
-	for (int q = blockIdx.x; q < n; q += gridDim.x) {
+	for (int q = G.bid; q < n; q += G.nb) {
 		const int gp = P.q_act[q];
 		if (threadIdx.x == 0) {
 			const int t = atomicSub(&P.counters[CNT_FREE_TOP], 1) - 1;
@@ -1235,20 +1323,24 @@ __global__ void k_activate(Dev P)
 		__syncthreads();
 	}
 }
+template <int L>
+__global__ void k_activate(Dev P)
+{
+	pdl_enter();
+	d_activate<L>(P, hw_grid());
+}
 
 /// Appends each touched brick's claimed nodes to its outermost lists in claim-key order (the
 /// reference's sequential track order) and records the partition's first key per side for the
 /// children-level append. One block per touched brick; keys sorted in shared memory.
 template <int L>
-__global__ void k_expand_append(Dev P)
+__device__ void d_expand_append(const Dev& P, GridPos G, unsigned long long* sk)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
-	extern __shared__ unsigned long long sk[];
 	__shared__ int ns, n0, base0, base1;
 	const int n = P.counters[CNT_TOUCH];
 	const size_t bv = (size_t)P.BV;
-	for (int q = blockIdx.x; q < n; q += gridDim.x) {
+	for (int q = G.bid; q < n; q += G.nb) {
 		const int sl = P.q_touch[q];
 		const int gp = P.slot_gp[sl];
 		if (threadIdx.x == 0) ns = 0;
@@ -1320,18 +1412,23 @@ __global__ void k_expand_append(Dev P)
 		__syncthreads();
 	}
 }
+template <int L>
+__global__ void k_expand_append(Dev P)
+{
+	pdl_enter();
+	extern __shared__ unsigned long long sk[];
+	d_expand_append<L>(P, hw_grid(), sk);
+}
 
 /// Children-level appends of the expansion (track_child of PartitionedMixin.hpp:201-213, in
 /// first-claim order). One block per surface; entries ranked by key.
 template <int L>
-__global__ void k_expand_plist(Dev P)
+__device__ void d_expand_plist(const Dev& P, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
-	const int s = blockIdx.x;
-	if (s >= P.S) return;
+	for (int s = G.bid; s < P.S; s += G.nb) {
 	const int m = P.papn[s];
-	if (m == 0) return;
+	if (m == 0) continue;
 	const SurfGeom& g = P.geom[s];
 	const unsigned long long* ent = P.pap + 2 * (size_t)g.pbase;
 	const int* entg = P.papg + 2 * (size_t)g.pbase;
@@ -1368,6 +1465,14 @@ __global__ void k_expand_plist(Dev P)
 		P.pcnt[s * NL + NL - 1] = c1 + a1;
 		P.papn[s] = 0;
 	}
+	__syncthreads();
+	}
+}
+template <int L>
+__global__ void k_expand_plist(Dev P)
+{
+	pdl_enter();
+	d_expand_plist<L>(P, hw_grid());
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1376,14 +1481,13 @@ __global__ void k_expand_plist(Dev P)
 
 /// status_change grid reset (Reset::MultiList::reset, PartitionedMixin.hpp:336-360).
 template <int L>
-__global__ void k_clear_status(Dev P)
+__device__ void d_clear_status(const Dev& P, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_SUNION];
 	const int lane = lane_id();
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
-	for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < n; e += nwarps) {
+	const int nwarps = (G.nb * blockDim.x) >> 5;
+	for (int e = (G.bid * blockDim.x + threadIdx.x) >> 5; e < n; e += nwarps) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
 		if (sl >= 0) {
@@ -1399,12 +1503,17 @@ __global__ void k_clear_status(Dev P)
 		if (lane == 0) P.sflag[gp] = 0;
 	}
 }
+template <int L>
+__global__ void k_clear_status(Dev P)
+{
+	pdl_enter();
+	d_clear_status<L>(P, hw_grid());
+}
 
 /// Affected buffer reset: clears the leaf lookups and lists of buffer b.
 template <int L>
-__global__ void k_clear_buffer(Dev P, int b)
+__device__ void d_clear_buffer(const Dev& P, int b, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	FG_WARP_LOOP(P.woff)
 	{
@@ -1428,13 +1537,18 @@ __global__ void k_clear_buffer(Dev P, int b)
 		if (lane == 0) P.appos[b][gp * NL + t] = -1;
 	}
 }
-
-/// Returns the bricks of partitions deactivated in this iteration to the free pool.
-static __global__ void k_retire(Dev P)
+template <int L>
+__global__ void k_clear_buffer(Dev P, int b)
 {
 	pdl_enter();
+	d_clear_buffer<L>(P, b, hw_grid());
+}
+
+/// Returns the bricks of partitions deactivated in this iteration to the free pool.
+static __device__ __forceinline__ void d_retire(const Dev& P, GridPos G)
+{
 	const int n = P.counters[CNT_RETIRE];
-	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+	for (int e = G.bid * blockDim.x + threadIdx.x; e < n; e += G.nb * blockDim.x) {
 		const int sl = P.q_retire[e];
 		const int gp = P.slot_gp[sl];
 		if (P.oslot[gp] == sl) P.oslot[gp] = -1;
@@ -1442,27 +1556,37 @@ static __global__ void k_retire(Dev P)
 		P.free_stack[atomicAdd(&P.counters[CNT_FREE_TOP], 1)] = sl;
 	}
 }
+static __global__ void k_retire(Dev P)
+{
+	pdl_enter();
+	d_retire(P, hw_grid());
+}
 
 /// Copies the isogrid partition lists to the delta partition lists (track_children of the
 /// delta grid at update start, Surface.hpp:261 / PartitionedMixin.hpp:319-334, which mirrors
 /// the isogrid lists into the freshly reset delta lists). Grid y = s*NL + l.
+static __device__ __forceinline__ void d_copy_plists(const Dev& P, int NL, GridPos G)
+{
+	for (int w = G.bid; w < P.S * NL; w += G.nb) {
+		const int s = w / NL, l = w % NL;
+		const SurfGeom& g = P.geom[s];
+		const int n = P.pcnt[s * NL + l];
+		const size_t o = (size_t)l * P.NP + g.pbase;
+		for (int i = threadIdx.x; i < n; i += blockDim.x) P.dplist[o + i] = P.plist[o + i];
+		if (threadIdx.x == 0) P.dpcnt[s * NL + l] = n;
+	}
+}
 static __global__ void k_copy_plists(Dev P, int NL)
 {
 	pdl_enter();
-	const int s = blockIdx.y / NL, l = blockIdx.y % NL;
-	const SurfGeom& g = P.geom[s];
-	const int n = P.pcnt[s * NL + l];
-	const size_t o = (size_t)l * P.NP + g.pbase;
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-		P.dplist[o + i] = P.plist[o + i];
-	if (blockIdx.x == 0 && threadIdx.x == 0) P.dpcnt[s * NL + l] = n;
+	// one block per (surface, list): grid (1, S*NL)
+	d_copy_plists(P, NL, GridPos{(int)blockIdx.y, (int)gridDim.y});
 }
 
 /// Narrow-band size: sum over all isogrid lists of the leaf counts (64-bit accumulator).
 template <int L>
-__global__ void k_band_size(Dev P, unsigned long long* acc)
+__device__ void d_band_size(const Dev& P, unsigned long long* acc, GridPos G)
 {
-	pdl_enter();
 	constexpr int NL = 2 * L + 1;
 	unsigned long long local = 0;
 	FG_WARP_LOOP(P.woff)
@@ -1483,6 +1607,12 @@ __global__ void k_band_size(Dev P, unsigned long long* acc)
 		}
 	}
 	if (lane_id() == 0 && local) atomicAdd(acc, local);
+}
+template <int L>
+__global__ void k_band_size(Dev P, unsigned long long* acc)
+{
+	pdl_enter();
+	d_band_size<L>(P, acc, hw_grid());
 }
 
 /// Makes surface s empty, with geometry ng (its partition range at pbase holds npcap

@@ -35,11 +35,13 @@ struct PolysDev {
 	uint32_t* spx;      // arena: per simplex D indices
 	unsigned long long* used;  // [2] vertices, simplices used
 	long long vcap, scap;
-	int pend;           // which of the two lists is pending
+	int* pendv;         // [S] which of the two lists is pending, per surface
 	int* err;
 	int* ovf;           // set when a march ran out of arena space
 	unsigned long long* vstart;  // [1] vertex arena position when the current march began
 	int* off;           // [S] 1 = notify leaves the surface out (serving: no polygons asked)
+	int* sel;           // [S] surfaces a march works on (1), when it works on a selection
+	int* cnt_sel;       // [S] pending counts of the surfaces a march works on
 };
 
 namespace {
@@ -179,9 +181,10 @@ __global__ void __launch_bounds__(256) k_polys_notify(Dev P, PolysDev Q)
 	const int lane = lane_id();
 	const unsigned lt = (1u << lane) - 1u;
 	const SurfGeom& g = P.geom[s];
-	int* lkp = Q.pend_lkp[Q.pend];
-	int* lst = Q.pend_list[Q.pend] + g.pbase;
-	if (threadIdx.x == 0) cnt_s = Q.pend_cnt[Q.pend][s];
+	const int pd = Q.pendv[s];
+	int* lkp = Q.pend_lkp[pd];
+	int* lst = Q.pend_list[pd] + g.pbase;
+	if (threadIdx.x == 0) cnt_s = Q.pend_cnt[pd][s];
 	for (int pass = 0; pass < 4; pass++) {
 		const bool status = pass >= 2;
 		const int li = (pass & 1) ? NL - 1 : 0;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(256) k_polys_notify(Dev P, PolysDev Q)
 		}
 	}
 	__syncthreads();
-	if (threadIdx.x == 0) Q.pend_cnt[Q.pend][s] = cnt_s;
+	if (threadIdx.x == 0) Q.pend_cnt[pd][s] = cnt_s;
 }
 
 /// Polys::invalidate (Polys.hpp:171-191), one thread per surface.
@@ -260,9 +263,10 @@ __global__ void k_polys_invalidate(Dev P, PolysDev Q)
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= P.S) return;
 	const SurfGeom& g = P.geom[s];
-	int* lkp = Q.pend_lkp[Q.pend];
-	int* lst = Q.pend_list[Q.pend] + g.pbase;
-	int cnt = Q.pend_cnt[Q.pend][s];
+	const int pd = Q.pendv[s];
+	int* lkp = Q.pend_lkp[pd];
+	int* lst = Q.pend_list[pd] + g.pbase;
+	int cnt = Q.pend_cnt[pd][s];
 	for (int i = 0; i < cnt; i++) lkp[g.pbase + lst[i]] = -1;
 	cnt = 0;
 	for (int li = 0; li <= NL; li += NL - 1) {
@@ -276,7 +280,7 @@ __global__ void k_polys_invalidate(Dev P, PolysDev Q)
 			}
 		}
 	}
-	Q.pend_cnt[Q.pend][s] = cnt;
+	Q.pend_cnt[pd][s] = cnt;
 }
 
 /// Serving: surface s's polygon children all inactive and empty, both pending lists empty
@@ -294,21 +298,36 @@ __global__ void k_polys_reset_surface(PolysDev Q, int s, int pbase, int npcap)
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		Q.pend_cnt[0][s] = 0;
 		Q.pend_cnt[1][s] = 0;
+		Q.pendv[s] = 0;
 	}
 }
 
-/// Clears list `which` (the reset of the swapped-out pending list, Polys.hpp:163-164).
-__global__ void k_polys_reset_list(Dev P, PolysDev Q, int which)
+/// The pending counts of the surfaces a march works on (all, or those with sel[s] set), for
+/// the scan of its entries; the others contribute none.
+__global__ void k_polys_counts(Dev P, PolysDev Q, int selected)
+{
+	for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P.S; s += gridDim.x * blockDim.x)
+		Q.cnt_sel[s] = (!selected || Q.sel[s]) ? Q.pend_cnt[Q.pendv[s]][s] : 0;
+}
+
+/// After a march (Polys.hpp:163-164): for every surface it worked on, the pending list becomes
+/// the done list and the other list, reset, the new pending one. One block per surface.
+__global__ void k_polys_flip(Dev P, PolysDev Q, int selected)
 {
 	const int s = blockIdx.x;
-	if (s >= P.S) return;
+	if (s >= P.S || (selected && !Q.sel[s])) return;
 	const SurfGeom& g = P.geom[s];
+	const int which = Q.pendv[s] ^ 1;
 	const int n = Q.pend_cnt[which][s];
 	for (int i = threadIdx.x; i < n; i += blockDim.x)
 		Q.pend_lkp[which][g.pbase + Q.pend_list[which][g.pbase + i]] = -1;
 	__syncthreads();
-	if (threadIdx.x == 0) Q.pend_cnt[which][s] = 0;
+	if (threadIdx.x == 0) {
+		Q.pend_cnt[which][s] = 0;
+		Q.pendv[s] = which;
+	}
 }
+
 
 /// Polys::march body (Polys.hpp:138-161) for every pending partition of every surface (woff
 /// over the pending counts), or for a single partition when single >= 0: classification of the
@@ -346,7 +365,7 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 		} else {
 			const int s = entry_surface(woff, P.S, e);
 			const SurfGeom& gs = P.geom[s];
-			gp = gs.pbase + Q.pend_list[Q.pend][gs.pbase + (e - woff[s])];
+			gp = gs.pbase + Q.pend_list[Q.pendv[s]][gs.pbase + (e - woff[s])];
 		}
 		const SurfGeom& g = P.geom[P.surf_of[gp]];
 		const int sl = P.slot[gp];
@@ -677,7 +696,11 @@ public:
 		nsoff_ = (int*)al(P.NP * sizeof(int));
 		csum_ = (unsigned long long*)al(2 * (size_t)nchunks_ * sizeof(unsigned long long));
 		ctot_ = (unsigned long long*)al(2 * sizeof(unsigned long long));
-		Q_.pend = 0;
+		Q_.pendv = (int*)al(P.S * sizeof(int));
+		FG_CUDA(cudaMemset(Q_.pendv, 0, P.S * sizeof(int)));
+		Q_.sel = (int*)al(P.S * sizeof(int));
+		Q_.cnt_sel = (int*)al(P.S * sizeof(int));
+		pend_host_.assign((size_t)P.S, 0);
 		const long long vc = vertex_capacity ? std::max<long long>((long long)vertex_capacity, 64)
 		                                     : (1LL << 20);
 		if (vc >= (1LL << 30)) throw Error(-1, "vertex capacity too large");
@@ -724,11 +747,32 @@ public:
 		FG_CUDA(cudaGetLastError());
 	}
 
-	void march() override
+	void march() override { march_sel(nullptr, 0); }
+
+	void march_some(const int* surfaces, int n) override
+	{
+		if (n <= 0) return;
+		const Dev& P = eng_.dev();
+		sel_host_.assign((size_t)P.S, 0);
+		for (int i = 0; i < n; i++) {
+			if (surfaces[i] < 0 || surfaces[i] >= P.S) throw Error(-1, "surface index out of range");
+			sel_host_[surfaces[i]] = 1;
+		}
+		FG_CUDA(cudaMemcpyAsync(Q_.sel, sel_host_.data(), sel_host_.size() * sizeof(int),
+		                        cudaMemcpyHostToDevice, eng_.stream()));
+		march_sel(surfaces, n);
+	}
+
+	/// Polys::march (Polys.hpp:138-165) of every surface of the pool (surfaces == nullptr) or
+	/// of the listed ones only (Q_.sel set): the others keep their pending lists for their own
+	/// march later.
+	void march_sel(const int* surfaces, int n)
 	{
 		const Dev& P = eng_.dev();
 		cudaStream_t st = eng_.stream();
-		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.pend_cnt[Q_.pend], 1, 0, 0, P.S, woff_, P.sfrozen););
+		const int selected = surfaces ? 1 : 0;
+		FG_RUN("k_polys_counts", st, k_polys_counts<<<(P.S + 255) / 256, 256, 0, st>>>(P, Q_, selected););
+		FG_RUN("k_scan_counts", st, k_scan_counts<<<1, 1024, 0, st>>>(Q_.cnt_sel, 1, 0, 0, P.S, woff_, P.sfrozen););
 		// Re-marching a partition recomputes it from the isogrid, so a march that ran out of
 		// arena space is simply repeated after the arena has grown.
 		for (int attempt = 0;; attempt++) {
@@ -740,9 +784,12 @@ public:
 		}
 		vertices();
 		// swap pending and done, then reset the new pending list
-		Q_.pend ^= 1;
-		FG_RUN("k_polys_reset_list", st, k_polys_reset_list<<<P.S, 256, 0, st>>>(P, Q_, Q_.pend););
+		FG_RUN("k_polys_flip", st, k_polys_flip<<<P.S, 256, 0, st>>>(P, Q_, selected););
 		FG_CUDA(cudaGetLastError());
+		if (surfaces)
+			for (int i = 0; i < n; i++) pend_host_[surfaces[i]] ^= 1;
+		else
+			for (int& v : pend_host_) v ^= 1;
 		eng_.check_errors();
 	}
 
@@ -791,7 +838,7 @@ public:
 	{
 		const Dev& P = eng_.dev();
 		eng_.sync();
-		const int done = Q_.pend ^ 1;
+		const int done = pend_host_[s_] ^ 1;
 		int n = 0;
 		int pbase = pbase_of();
 		FG_CUDA(cudaMemcpy(&n, Q_.pend_cnt[done] + s_, sizeof(int), cudaMemcpyDeviceToHost));
@@ -955,6 +1002,7 @@ public:
 		const int blocks = std::max(1, std::min((npcap + 255) / 256, 1024));
 		FG_RUN("k_polys_reset_surface", eng_.stream(), k_polys_reset_surface<<<blocks, 256, 0, eng_.stream()>>>(Q_, s, eng_.geometry(s).pbase, npcap););
 		FG_CUDA(cudaGetLastError());
+		pend_host_[s] = 0;
 	}
 
 	void set_enabled(int s, bool on) override
@@ -1061,6 +1109,8 @@ private:
 	long long spare_vcap_ = 0, spare_scap_ = 0;
 	std::vector<void*> owned_;
 	std::vector<int> off_host_;  // host copy of Q_.off (sources of its updates)
+	std::vector<int> pend_host_; // host copy of Q_.pendv
+	std::vector<int> sel_host_;  // host copy of Q_.sel
 };
 
 }  // namespace

@@ -15,6 +15,10 @@ public:
 	virtual ~PolysBase() = default;
 	virtual void notify() = 0;
 	virtual void march() = 0;
+	/// march() of the listed surfaces of the pool only; the others keep their pending
+	/// partitions for their own march (serving: a request is marched when it finishes, as it
+	/// would be alone).
+	virtual void march_some(const int* surfaces, int n) = 0;
 	virtual void invalidate() = 0;
 	virtual void march_partition(size_t part) = 0;
 	virtual std::vector<uint32_t> changes() = 0;

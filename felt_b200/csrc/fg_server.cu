@@ -6,9 +6,10 @@
 // one brick pool that all of them share. A worker thread owns the pool and runs steps: every
 // step is one batched Surface::update (include/Felt/Surface.hpp:254-296) of all surfaces in
 // flight with their own builtin speeds, Polys::notify (include/Felt/Polys.hpp:92-133) for those
-// that asked for polygons, and Polys::march (Polys.hpp:138-165) when one of those has had its
-// last update. Between steps, requests that arrived meanwhile take the slots of finished ones:
-// the slot's surface is reset (its bricks back to the pool) to the request's grid size and
+// that asked for polygons, and Polys::march (Polys.hpp:138-165) of each of those after its
+// last update (of that surface only, so that its marches are those of the request alone).
+// Between steps, requests that arrived meanwhile take the slots of finished ones: the slot's
+// surface is reset (its bricks back to the pool) to the request's grid size and
 // seeded, and from then on it advances in the same launches as the others. Finished slots are
 // paused, so no kernel touches them, and their results are exactly those of a separate
 // Surface given the same seed and updates.
@@ -172,18 +173,19 @@ void fg_server::step()
 	for (size_t s = 0; s < slots.size(); s++)
 		if (slots[s].busy && slots[s].req.polygonise) any_polys = true;
 	if (any_polys) polys->notify();
-	std::vector<int> fin;
-	bool march = false;
+	std::vector<int> fin, fin_polys;
 	for (size_t s = 0; s < slots.size(); s++) {
 		Slot& sl = slots[s];
 		if (!sl.busy) continue;
 		sl.remaining--;
 		if (sl.remaining <= 0 || eng->frozen((int)s)) {
 			fin.push_back((int)s);
-			if (sl.req.polygonise) march = true;
+			if (sl.req.polygonise) fin_polys.push_back((int)s);
 		}
 	}
-	if (march) polys->march();
+	// only the finishing requests are marched: a request in flight keeps its pending
+	// partitions for its own march, so its polygons are those of the same request alone
+	if (!fin_polys.empty()) polys->march_some(fin_polys.data(), (int)fin_polys.size());
 	const long long used = (long long)eng->dev().nslots - eng->free_bricks();
 	{
 		std::lock_guard<std::mutex> g(mu);

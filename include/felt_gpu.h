@@ -66,8 +66,15 @@ typedef struct fg_config {
 	size_t brick_capacity; /* bricks (partitions) the device pool can hold; 0 = automatic   */
 	size_t vertex_capacity;/* initial polygonisation arena, vertices (simplices: twice that);
 	                          0 = 2^20; it grows on demand                                  */
-	int use_graph;         /* reserved, must be 0                                          */
-	int reserved[7];
+	int launch_mode;       /* how a global update launches: 0 automatic (the whole update as
+	                          one persistent launch where the device can launch cooperatively),
+	                          1 persistent, 2 one kernel per phase                         */
+	int dist_split;        /* threads per brick in the first distance pass, in warps per
+	                          partition entry (1, 2, 4, 8); 0 = automatic                  */
+	int record_passes;     /* threads per brick in the passes that record status changes:
+	                          1 a warp, 2 a block per partition entry; 0 = automatic        */
+	int blocks_per_sm;     /* resident blocks per SM of the persistent launch; 0 = automatic */
+	int reserved[4];
 } fg_config;
 
 typedef struct fg_surface fg_surface;
@@ -381,6 +388,17 @@ FG_API int fg_server_release(fg_server* s, uint64_t tag);
 FG_API int fg_request_bricks(const fg_server_config* cfg, const fg_request* r,
                              unsigned long long* bricks);
 FG_API int fg_brick_bytes(int dims, int layers, const int* part, double* bytes);
+
+/* Check of the persistent update launch's bounded waits (no counterpart in the reference): runs
+ * it with a grid barrier that can never complete; every block gives up after about wait_s
+ * seconds and the call returns FG_ERR_TIMEOUT, the surface unchanged (the kernel stops at its
+ * entry barrier, before any work) and usable. FG_ERR_ARG where the persistent launch is not
+ * available. */
+FG_API int fg_check_step_timeout(fg_surface* s, double wait_s);
+/* The launch tuning in effect on a surface or batch: out[0] launch mode (1 persistent, 2 one
+ * kernel per phase), out[1] dist_split, out[2] record_passes, out[3] blocks per SM. */
+FG_API int fg_surface_tuning(fg_surface* s, int* out);
+FG_API int fg_batch_tuning(fg_batch* b, int* out);
 
 /* ---- instrumentation (no counterpart in the reference; Surface.hpp has no timers) ----
  * fg_node_updates: narrow-band node-updates processed by all global updates of a surface so
