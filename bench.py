@@ -517,14 +517,19 @@ def cpu_single(cfg, steps, warm=3, fp64=False, timed=True):
     return (nu / secs if timed and secs else None), nu, secs, s, p
 
 
-def cpu_batch(name, cfg, steps, k):
+def cpu_batch(name, cfg, steps, k, shard=0, digest=None):
+    """The first k surfaces of a batched config's shard through the oracle for `steps` steps:
+    (node updates per second, node updates, seconds). With a list as digest, a hash of each
+    surface's final state encoding is appended to it (surfaces the convergence cap dropped:
+    None)."""
     from oracle import oracle as O
-    sizes, centres, speeds = batch_surfaces(name, cfg)
+    sizes, centres, speeds = batch_surfaces(name, cfg, shard)
     items = []
     for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
         s = O.Surface(sz, cfg["part"], cfg["L"])
         s.seed(c)
         items.append((s, O.Polys(s), sp))
+    start = list(items)
     nu, secs = 0.0, 0.0
     for i in range(steps):
         keep = []
@@ -544,6 +549,11 @@ def cpu_batch(name, cfg, steps, k):
             nu += band
             keep.append((s, p, sp))
         items = keep
+    if digest is not None:
+        import hashlib
+        final = {id(s) for s, _, _ in items}
+        digest.extend(hashlib.sha1(s.dump().tobytes()).hexdigest() if id(s) in final else None
+                      for s, _, _ in start)
     return nu / secs, nu, secs
 
 
@@ -678,35 +688,7 @@ def roofline(fb, make_work, cfg, steps, warm, ms_per_step, node_updates):
                     out["phase_kernel"]["traffic"] = t["bytes_per_unit"] * units[UNIT_OF[dom]] / nl
             except Exception:
                 pass
-    # the kernel the timed steps run: the persistent update launch when it is in use (one per
-    # step, timed alone), else the dominant per-phase kernel
-    work = make_work()
-    persistent = work.tuning()["launch_mode"] == 1
-    work.close()
-    if persistent:
-        work = make_work()
-        for i in range(warm):
-            work.step(i)
-        torch.cuda.synchronize()
-        nu0 = work.node_updates()
-        fb.profile_reset()
-        fb.profile_only("k_update_step")
-        fb.profile_enable(True)
-        for i in range(steps):
-            work.step(warm + i, last=(i == steps - 1))
-        torch.cuda.synchronize()
-        fb.profile_enable(False)
-        fb.profile_only(None)
-        ms, nl = fb.profile_read()["k_update_step"]
-        nu_k = work.node_updates() - nu0
-        work.close()
-        bpl = BYTES_PER_NODE_UPDATE * nu_k / nl
-        achieved = bpl / (ms / nl * 1e-3) / 1e9
-        out.update({"kernel": "k_update_step", "achieved": achieved, "frac": achieved / hbm,
-                    "traffic": None, "bytes_per_launch": bpl, "avg_launch_us": 1e3 * ms / nl,
-                    "kernel_ms_per_step": ms / steps, "launches": nl,
-                    "share_of_step": (ms / steps) / ms_per_step})
-    elif "phase_kernel" in out:
+    if "phase_kernel" in out:
         pk = out["phase_kernel"]
         out.update({"kernel": pk["kernel"], "achieved": pk["achieved"], "frac": pk["frac"],
                     "traffic": pk.get("traffic"), "bytes_per_launch": pk["bytes_per_launch"],

@@ -40,24 +40,45 @@ class Speed(C.Structure):
 class Config(C.Structure):
     _fields_ = [("brick_capacity", C.c_size_t), ("vertex_capacity", C.c_size_t),
                 ("launch_mode", C.c_int), ("dist_split", C.c_int), ("record_passes", C.c_int),
-                ("blocks_per_sm", C.c_int), ("reserved", C.c_int * 4)]
+                ("autotune", C.c_int), ("reserved", C.c_int * 4)]
 
 
 def make_config(brick_capacity=0, vertex_capacity=0, launch_mode=0, dist_split=0,
-                record_passes=0, blocks_per_sm=0):
-    """fg_config: pool sizes and launch tuning (launch_mode 0 automatic, 1 persistent, 2 one
-    kernel per phase; dist_split warps per partition entry in the first distance pass;
-    record_passes 1 warp / 2 block per entry in the recording passes; blocks_per_sm of the
-    persistent launch; 0 = automatic everywhere)."""
+                record_passes=0, autotune=False):
+    """fg_config: pool sizes and launch tuning (launch_mode 0 automatic, 1 the whole global
+    update as one CUDA graph, 2 its phases launched one by one; dist_split warps per partition
+    entry in the first distance pass; record_passes 1 warp / 2 block per entry in the
+    recording passes; 0 = automatic everywhere; autotune: the knobs left at 0 take the values
+    autotune() measures)."""
     return Config(int(brick_capacity), int(vertex_capacity), int(launch_mode), int(dist_split),
-                  int(record_passes), int(blocks_per_sm))
+                  int(record_passes), 1 if autotune else 0)
+
+
+def autotune_candidates(part):
+    """The (dist_split, record_passes) pairs the tuner times for a partition shape."""
+    buf = (C.c_int * 32)()
+    n = C.c_size_t()
+    _chk(lib().fg_autotune_candidates(len(part), _ivec(part), buf, C.c_size_t(32), C.byref(n)))
+    return [(buf[2 * i], buf[2 * i + 1]) for i in range(n.value)]
+
+
+def autotune(part, layers, force=False):
+    """fg_autotune: the fastest (dist_split, record_passes) for this partition shape and layer
+    count on the current device, timed on a scratch surface (or cached); with each candidate's
+    device ms per update when it was timed."""
+    cfg = make_config()
+    ms = (C.c_double * 32)()
+    n = C.c_size_t()
+    _chk(lib().fg_autotune(len(part), int(layers), _ivec(part), 1 if force else 0, C.byref(cfg),
+                           ms, C.c_size_t(32), C.byref(n)))
+    return dict(dist_split=cfg.dist_split, record_passes=cfg.record_passes,
+                ms=dict(zip(autotune_candidates(part), list(ms)[:n.value])))
 
 
 def _tuning(fn, h):
     out = (C.c_int * 4)()
     _chk(fn(h, out))
-    return dict(launch_mode=out[0], dist_split=out[1], record_passes=out[2],
-                blocks_per_sm=out[3])
+    return dict(launch_mode=out[0], dist_split=out[1], record_passes=out[2])
 
 
 def build():
@@ -176,7 +197,7 @@ class Surface:
     """Felt::Surface<D,L>(size, size_partition) on the GPU (include/Felt/Surface.hpp:163-173)."""
 
     def __init__(self, size, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
-        """tuning: launch_mode, dist_split, record_passes, blocks_per_sm (see make_config)."""
+        """tuning: launch_mode, dist_split, record_passes (see make_config)."""
         self.D = len(size)
         self.L = int(layers)
         self.size = tuple(int(s) for s in size)
@@ -215,11 +236,6 @@ class Surface:
 
     def update_end(self):
         _chk(lib().fg_update_end(self._h))
-
-    def check_step_timeout(self, wait_s=0.2):
-        """fg_check_step_timeout: the persistent update launch with a barrier that can never
-        complete; returns the status code (FG_ERR_TIMEOUT, -14, expected)."""
-        return int(lib().fg_check_step_timeout(self._h, C.c_double(wait_s)))
 
     def tuning(self):
         """The launch tuning in effect (fg_surface_tuning)."""
@@ -369,7 +385,7 @@ class Batch:
     same kernel launches. Per surface the results equal a separate Surface's."""
 
     def __init__(self, sizes, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
-        """tuning: launch_mode, dist_split, record_passes, blocks_per_sm (see make_config)."""
+        """tuning: launch_mode, dist_split, record_passes (see make_config)."""
         self.n = len(sizes)
         self.D = len(part)
         self.L = int(layers)

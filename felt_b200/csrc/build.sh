@@ -7,7 +7,7 @@ NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 FLAGS=(-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 -fmad=false
        -Xcompiler -fPIC -Xcompiler -fvisibility=hidden --expt-relaxed-constexpr
        -I"$HERE/../include")
-SRCS=(fg_engine.cu fg_polys.cu fg_ray.cu fg_image.cu fg_query.cu fg_capi.cu fg_prof.cu fg_noalloc.cu fg_server.cu)
+SRCS=(fg_engine.cu fg_polys.cu fg_ray.cu fg_image.cu fg_query.cu fg_capi.cu fg_prof.cu fg_noalloc.cu fg_server.cu fg_tune.cu)
 OBJS=()
 PIDS=()
 mkdir -p "$OUT/_build"

@@ -58,11 +58,17 @@ void apply_tuning(fg::EngineBase& eng, const fg_config* cfg)
 		throw fg::Error(FG_ERR_ARG, "dist_split must be 0, 1, 2, 4 or 8");
 	if (cfg->record_passes < 0 || cfg->record_passes > 2)
 		throw fg::Error(FG_ERR_ARG, "record_passes must be 0, 1 or 2");
-	if (cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 32)
-		throw fg::Error(FG_ERR_ARG, "blocks_per_sm must be in 0..32");
-	if (cfg->launch_mode == 1 && !eng.persistent_available())
-		throw fg::Error(FG_ERR_ARG, "the persistent update launch is not available here");
-	eng.set_tuning(cfg->launch_mode, cfg->dist_split, cfg->record_passes, cfg->blocks_per_sm);
+	if (cfg->autotune < 0 || cfg->autotune > 1) throw fg::Error(FG_ERR_ARG, "autotune must be 0 or 1");
+	int ds = cfg->dist_split, rp = cfg->record_passes;
+	if (cfg->autotune && (ds == 0 || rp == 0)) {
+		int part[3] = {1, 1, 1};
+		for (int a = 0; a < eng.dims(); a++) part[a] = eng.part(a);
+		int tds = 0, trp = 0;
+		fg::autotune(eng.dims(), eng.layers(), part, tds, trp, nullptr, false);
+		if (ds == 0) ds = tds;
+		if (rp == 0) rp = trp;
+	}
+	eng.set_tuning(cfg->launch_mode, ds, rp);
 }
 
 void put_list(const std::vector<uint32_t>& v, uint32_t* out, size_t cap, size_t* n)
@@ -819,12 +825,42 @@ int fg_profile_reset(void)
 	return guard([&] { fg::prof_reset(); });
 }
 
-int fg_check_step_timeout(fg_surface* s, double wait_s)
+int fg_autotune_candidates(int dims, const int* part, int* pairs, size_t cap, size_t* n)
 {
 	return guard([&] {
-		need(s, "surface");
-		if (!(wait_s > 0) || wait_s > 30) throw fg::Error(FG_ERR_ARG, "wait_s must be in (0, 30]");
-		s->eng->check_step_timeout(wait_s);
+		need(part, "part");
+		need(n, "n");
+		if (dims != 2 && dims != 3) throw fg::Error(FG_ERR_ARG, "dims must be 2 or 3");
+		std::vector<std::pair<int, int>> c;
+		fg::tune_candidates(dims, part, c);
+		*n = c.size();
+		for (size_t i = 0; pairs && i < c.size() && i < cap / 2; i++) {
+			pairs[2 * i] = c[i].first;
+			pairs[2 * i + 1] = c[i].second;
+		}
+	});
+}
+
+int fg_autotune(int dims, int layers, const int* part, int force, fg_config* cfg, double* ms,
+                size_t ms_cap, size_t* n)
+{
+	return guard([&] {
+		need(part, "part");
+		need(cfg, "config");
+		if (dims != 2 && dims != 3) throw fg::Error(FG_ERR_ARG, "dims must be 2 or 3");
+		if (layers < 1 || layers > 4) throw fg::Error(FG_ERR_ARG, "layers must be in 1..4");
+		for (int a = 0; a < dims; a++)
+			if (part[a] < 1 || part[a] > 32) throw fg::Error(FG_ERR_ARG, "partition edge must be in 1..32");
+		int ndev = 0;
+		if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+			throw fg::Error(FG_ERR_CUDA, "no CUDA device");
+		std::vector<double> t;
+		int ds = 0, rp = 0;
+		fg::autotune(dims, layers, part, ds, rp, &t, force != 0);
+		cfg->dist_split = ds;
+		cfg->record_passes = rp;
+		if (n) *n = t.size();
+		for (size_t i = 0; ms && i < t.size() && i < ms_cap; i++) ms[i] = t[i];
 	});
 }
 

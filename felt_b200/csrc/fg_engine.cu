@@ -4,7 +4,6 @@
 
 #include "fg_engine.cuh"
 #include "fg_kernels.cuh"
-#include "fg_step.cuh"
 
 namespace fg {
 
@@ -254,10 +253,6 @@ public:
 		zcount_ = dalloc<unsigned long long>(1, o);
 		d_iters_ = dalloc<int>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
-		d_bar_ = dalloc<unsigned>(2, o);
-		d_out_ = dalloc<int>(4, o);
-		d_newfrozen_ = dalloc<int>(S, o);
-		FG_CUDA(cudaMemsetAsync(d_newfrozen_, 0, S * sizeof(int), st_));
 
 		fill(P.slot, NP, -1);
 		fillf(P.bg, NP, (float)(L + 1));
@@ -313,168 +308,28 @@ public:
 		} else {
 			smem_flush_ = 0;  // brick too large to stage: replay in global memory
 		}
-		setup_persistent();
-	}
-
-	/// Shared memory and resident blocks of the persistent update launch (k_update_step). It
-	/// is off where the device cannot launch cooperatively or a block's staging does not fit.
-	void setup_persistent()
-	{
-		persistent_ok_ = false;
-		int dev = 0, coop = 0;
-		if (cudaGetDevice(&dev) != cudaSuccess ||
-		    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) {
-			cudaGetLastError();
-			return;
-		}
-		size_t smem = smem_sort_;
-		if (smem_halo_) smem = std::max(smem, smem_halo_);
-		if (smem_flush_) smem = std::max(smem, smem_flush_);
-		step_smem_ = (smem + 15) & ~(size_t)15;
-		if (step_smem_ > 160 * 1024) return;
-		if (step_smem_ > 48 * 1024 &&
-		    cudaFuncSetAttribute(k_update_step<D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                         (int)step_smem_) != cudaSuccess) {
-			cudaGetLastError();
-			return;
-		}
-		int per_sm = 0;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_step<D, L>, 256,
-		                                                  step_smem_) != cudaSuccess ||
-		    per_sm < 1) {
-			cudaGetLastError();
-			return;
-		}
-		step_max_per_sm_ = per_sm;
-		persistent_ok_ = true;
 	}
 
 public:
-	/// Launch tuning (fg_config): how the global update launches (0 automatic, 1 persistent,
-	/// 2 one kernel per phase), warps per partition entry in the first distance pass (0 =
-	/// automatic), warp (1) or block (2) per entry in the record passes (0 = automatic), and
-	/// blocks per SM of the persistent launch (0 = as many as fit, at most 4).
-	void set_tuning(int launch_mode, int dist_split, int record_passes, int blocks_per_sm) override
+	/// Launch tuning (fg_config): how the global update launches (0 automatic = 1, 1 the
+	/// whole update as one CUDA graph, 2 the update's phases launched from the host with the
+	/// convergence loop as a device graph), warps per partition entry in the first distance
+	/// pass (0 = automatic), warp (1) or block (2) per entry in the record passes (0 =
+	/// automatic). Graphs captured under the previous tuning are dropped.
+	void set_tuning(int launch_mode, int dist_split, int record_passes) override
 	{
 		launch_mode_ = launch_mode;
 		if (dist_split > 0) dist_split_ = dist_split;
 		if (record_passes == 1) block_passes_ = false;
 		if (record_passes == 2) block_passes_ = true;
-		step_blocks_per_sm_ = blocks_per_sm;
+		drop_graphs();
 	}
-	bool persistent_available() const override { return persistent_ok_; }
 	void tuning(int* out) const override
 	{
-		out[0] = use_persistent() ? 1 : 2;
+		out[0] = launch_mode_ == 2 ? 2 : 1;
 		out[1] = dist_split_;
 		out[2] = block_passes_ ? 2 : 1;
-		out[3] = step_blocks();
-	}
-
-private:
-	bool use_persistent() const
-	{
-		return persistent_ok_ && launch_mode_ != 2 && !prof_per_launch();
-	}
-	int step_blocks() const
-	{
-		int per_sm = step_max_per_sm_;
-		if (step_blocks_per_sm_ > 0) per_sm = std::min(per_sm, step_blocks_per_sm_);
-		else per_sm = std::min(per_sm, 4);
-		return per_sm;
-	}
-
-	StepArgs step_args(bool curv) const
-	{
-		StepArgs a;
-		std::memset(&a, 0, sizeof(a));
-		a.speeds = d_speeds_;
-		a.bar = d_bar_;
-		a.out = d_out_;
-		a.newfrozen = d_newfrozen_;
-		a.acc = acc_;
-		a.wait_ns = 2000000000ull;
-		a.clear_status = status_dirty_ ? 1 : 0;
-		a.clear_buf0 = buf_dirty_[0] ? 1 : 0;
-		a.clear_buf1 = buf_dirty_[1] ? 1 : 0;
-		a.delta_smem = (curv && smem_halo_) ? 1 : 0;
-		a.block_passes = block_passes_ ? 1 : 0;
-		a.flush_smem = smem_flush_ ? 1 : 0;
-		a.split = dist_split_;
-		a.max_iters = kMaxIterations;
-		return a;
-	}
-
-	void launch_step(const StepArgs& a)
-	{
-		FG_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), st_));
-		FG_CUDA(cudaMemsetAsync(d_out_, 0, 4 * sizeof(int), st_));
-		cudaLaunchConfig_t cfg = {};
-		cfg.gridDim = dim3(step_blocks() * sm_count());
-		cfg.blockDim = dim3(256);
-		cfg.dynamicSmemBytes = step_smem_;
-		cfg.stream = st_;
-		cudaLaunchAttribute at[1];
-		at[0].id = cudaLaunchAttributeCooperative;
-		at[0].val.cooperative = 1;
-		cfg.attrs = at;
-		cfg.numAttrs = 1;
-		cudaError_t e = cudaSuccess;
-		FG_RUN("k_update_step", st_, e = cudaLaunchKernelEx(&cfg, k_update_step<D, L>, P_, a););
-		if (e != cudaSuccess)
-			throw Error(-2, std::string("persistent update launch: ") + cudaGetErrorString(e));
-	}
-
-	/// After a persistent launch that ran update_end_global: the host-side record of what it
-	/// left (the status grid and the last recorded buffer need resets at the next update start,
-	/// the surfaces it stopped), then the error check.
-	void finish_persistent()
-	{
-		int out[4] = {0, 0, 0, 0};
-		FG_CUDA(cudaMemcpyAsync(out, d_out_, sizeof(out), cudaMemcpyDeviceToHost, st_));
-		FG_CUDA(cudaStreamSynchronize(st_));
-		check_errors();
-		status_dirty_ = true;
-		const int cur = out[1] ? 1 : 0;
-		buf_dirty_[cur] = true;
-		buf_dirty_[1 - cur] = false;
-		stats_.iterations = out[0];
-		if (out[2]) {
-			std::vector<int> nf((size_t)P_.S);
-			FG_CUDA(cudaMemcpyAsync(nf.data(), d_newfrozen_, nf.size() * sizeof(int),
-			                        cudaMemcpyDeviceToHost, st_));
-			FG_CUDA(cudaMemsetAsync(d_newfrozen_, 0, nf.size() * sizeof(int), st_));
-			FG_CUDA(cudaStreamSynchronize(st_));
-			for (int s = 0; s < P_.S; s++)
-				if (nf[s] && !frozen_[s]) {
-					frozen_[s] = 1;
-					newly_frozen_.push_back(s);
-				}
-			push_stopped();
-		}
-		if (!newly_frozen_.empty() && throw_on_freeze_) {
-			newly_frozen_.clear();
-			throw Error(-14, "the convergence loop of the update did not terminate (layer "
-			                 "changes keep oscillating, typically where the band meets the grid "
-			                 "edge); the surface is stopped");
-		}
-		newly_frozen_.clear();
-	}
-
-public:
-	/// Runs the persistent update kernel with a grid barrier that can never complete, to check
-	/// that its bounded waits give up: throws FG_ERR_TIMEOUT after about wait_s seconds, having
-	/// changed nothing (the kernel stops at its entry barrier, before any work).
-	void check_step_timeout(double wait_s) override
-	{
-		if (!persistent_ok_) throw Error(-1, "the persistent update launch is not available");
-		StepArgs a = step_args(false);
-		a.stall = 1;
-		a.wait_ns = (unsigned long long)(wait_s * 1e9);
-		a.do_begin = a.do_delta = a.do_finish = 1;
-		launch_step(a);
-		FG_CUDA(cudaStreamSynchronize(st_));
-		check_errors();
+		out[3] = 0;
 	}
 
 private:
@@ -483,6 +338,8 @@ private:
 	{
 		cudaStreamSynchronize(st_);
 		for (cudaGraphExec_t& ex : iter_exec_)
+			if (ex) cudaGraphExecDestroy(ex);
+		for (cudaGraphExec_t& ex : step_exec_)
 			if (ex) cudaGraphExecDestroy(ex);
 		if (loop_exec_) cudaGraphExecDestroy(loop_exec_);
 		for (void* p : owned_) locked_free(p);
@@ -622,41 +479,21 @@ private:
 	// ---- global update ----
 	void update_builtin(const Speed* speeds) override
 	{
-		if (use_persistent()) {
-			check_not_frozen();
-			FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed),
-			                        cudaMemcpyHostToDevice, st_));
-			bool any_curv = false;
-			for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
-			StepArgs a = step_args(any_curv);
-			a.do_begin = a.do_delta = a.do_finish = 1;
-			launch_step(a);
-			finish_persistent();
-			return;
-		}
-		update_begin_global();
+		check_not_frozen();
 		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
 		bool any_curv = false;
 		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
-		if (any_curv && smem_halo_)
-			FG_RUN("k_delta_smem", st_, launch_pdl((k_delta_smem<D, L>), sm_count() * 8, 128, smem_halo_, st_, P_, d_speeds_););
-		else
-			FG_RUN("k_delta_builtin", st_, launch_pdl((k_delta_builtin<D, L>), warp_grid_, 256, 0, st_, P_, d_speeds_););
+		const bool curv = any_curv && smem_halo_;
+		if (run_step_graph(curv)) return;
+		update_begin_global();
+		delta_builtin(curv);
 		update_finish_global();
 	}
 
 	void update_begin_global() override
 	{
 		check_not_frozen();
-		if (use_persistent()) {
-			StepArgs a = step_args(false);
-			a.do_begin = 1;
-			launch_step(a);
-			status_dirty_ = false;
-			buf_dirty_[0] = buf_dirty_[1] = false;
-			return;
-		}
 		update_start();
 		// delta.track_children(isogrid) on freshly reset delta lists = a copy of the lists.
 		copy_plists();
@@ -667,22 +504,121 @@ private:
 
 	void update_finish_global() override
 	{
-		if (use_persistent()) {
-			StepArgs a = step_args(false);
-			a.do_finish = 1;
-			launch_step(a);
-			finish_persistent();
-			return;
-		}
+		first_passes();
+		converge();
+	}
+
+private:
+	/// The builtin speed functor over the zero layer (Surface.hpp:263-294): with curvature,
+	/// over staged bricks with their halo.
+	void delta_builtin(bool curv)
+	{
+		if (curv)
+			FG_RUN("k_delta_smem", st_, launch_pdl((k_delta_smem<D, L>), sm_count() * 8, 128, smem_halo_, st_, P_, d_speeds_););
+		else
+			FG_RUN("k_delta_builtin", st_, launch_pdl((k_delta_builtin<D, L>), warp_grid_, 256, 0, st_, P_, d_speeds_););
+	}
+
+	/// update_end_global up to the convergence loop (Surface.hpp:739-751):
+	/// update_zero_layer(&affected_buffer), the first distance passes recording into buffer B.
+	void first_passes()
+	{
 		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
-		// update_zero_layer(&affected_buffer)
 		scan(P_.pcnt, L, 0);
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		zero_apply(iso, nullptr, B);
 		defer_compact(P_.woff, P_.plist, L, B);
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		distance_passes(iso, B);
-		converge();
+	}
+
+	/// The whole global update with a builtin speed as ONE CUDA graph: update_start's due
+	/// resets, the delta track_children copy, the band count, the speed functor, the zero-layer
+	/// update and first distance passes, flush, expansion and retirement, then the convergence
+	/// loop's while node (the body of run_device_loop's graph). One graph per combination of
+	/// due resets and delta kernel, captured on first use; a step is then one graph launch and
+	/// one read-back of the loop's count. Returns false (the caller launches phase by phase)
+	/// under launch mode 2, while per-launch profiling is on, or where the graph cannot be
+	/// built.
+	bool run_step_graph(bool curv)
+	{
+		if (launch_mode_ == 2 || !loop_ok_ || !graphs_ok_ || !step_ok_ || prof_on()) return false;
+		const int key = (status_dirty_ ? 1 : 0) | (buf_dirty_[0] ? 2 : 0) |
+		                (buf_dirty_[1] ? 4 : 0) | (curv ? 8 : 0);
+		if (!step_exec_[key] && !build_step_graph(key, curv)) return false;
+		FG_CUDA(cudaGraphLaunch(step_exec_[key], st_));
+		int out[2] = {0, 0};
+		FG_CUDA(cudaMemcpyAsync(&out[0], d_iters_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaMemcpyAsync(&out[1], P_.changed, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		FG_CUDA(cudaStreamSynchronize(st_));
+		const int iters = out[0], changed = out[1];
+		const int n = iters - 1;
+		add_launches(step_launches_[key] + (long long)(n / 2) * (loop_launches_[0] + loop_launches_[1]) +
+		             (n % 2) * loop_launches_[0]);
+		// what update_start left
+		status_dirty_ = false;
+		buf_dirty_[0] = buf_dirty_[1] = false;
+		converge_after(false, true, changed, iters);
+		return true;
+	}
+
+	bool build_step_graph(int key, bool curv)
+	{
+		std::lock_guard<std::recursive_mutex> lock(device_lock());
+		cudaGraph_t g = nullptr;
+		bool ok = false;
+		const long long l0 = launch_count();
+		// capturing runs the host side of update_start and the passes, which marks the grids
+		// it clears as clean and leaves a compaction pending; nothing captured has run yet
+		const bool sd = status_dirty_, bd0 = buf_dirty_[0], bd1 = buf_dirty_[1];
+		long long prefix = 0;
+		try {
+			ok = build_loop_into(g, prefix, [&] {
+				update_start();
+				copy_plists();
+				count_band();
+				scan(P_.pcnt, L, 0);
+				delta_builtin(curv);
+				first_passes();
+				flush();
+				expand();
+				retire();
+			});
+		} catch (...) {
+			ok = false;
+		}
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		if (cudaStreamIsCapturing(st_, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+			cudaGraph_t dropped = nullptr;
+			cudaStreamEndCapture(st_, &dropped);
+			if (dropped) cudaGraphDestroy(dropped);
+			ok = false;
+		}
+		add_launches(-(launch_count() - l0));  // counted when they run
+		if (ok && cudaGraphInstantiate(&step_exec_[key], g, 0) != cudaSuccess) {
+			step_exec_[key] = nullptr;
+			ok = false;
+		}
+		if (g) cudaGraphDestroy(g);
+		cudaGetLastError();
+		pending_ = CompactArgs{0, nullptr, nullptr, 0, 0};
+		status_dirty_ = sd;
+		buf_dirty_[0] = bd0;
+		buf_dirty_[1] = bd1;
+		if (!ok) step_ok_ = false;
+		step_launches_[key] = prefix;
+		return ok;
+	}
+
+	/// Graphs captured with the current launch parameters.
+	void drop_graphs()
+	{
+		cudaStreamSynchronize(st_);
+		for (cudaGraphExec_t& ex : iter_exec_)
+			if (ex) cudaGraphExecDestroy(ex), ex = nullptr;
+		for (cudaGraphExec_t& ex : step_exec_)
+			if (ex) cudaGraphExecDestroy(ex), ex = nullptr;
+		if (loop_exec_) cudaGraphExecDestroy(loop_exec_), loop_exec_ = nullptr;
 	}
 
 	/// The rest of update_end_global / update_end after the first distance passes, which
@@ -693,16 +629,26 @@ private:
 	/// affected() lookup a local update leaves behind.
 	void converge(bool local = false)
 	{
-		const int B = 1, A = 0;
 		flush();
 		expand();
 		retire();
-		status_dirty_ = true;
-		buf_dirty_[B] = true;
 		int changed = 0;
 		int iters = 1;
+		const bool dev = !local && run_device_loop(changed, iters);
+		if (!dev) changed = read_changed();
+		converge_after(local, dev, changed, iters);
+	}
+
+	/// converge() after the first flush and expansion, and after the device-side loop when it
+	/// ran (dev): the host-side record of the buffers it left, the surfaces to stop when it
+	/// stopped at a multiple of kMaxIterations, and the host loop for what is left.
+	void converge_after(bool local, bool dev, int changed, int iters)
+	{
+		const int B = 1, A = 0;
+		status_dirty_ = true;
+		buf_dirty_[B] = true;
 		int cur = B, oth = A;
-		if (!local && run_device_loop(changed, iters)) {
+		if (dev) {
 			// iterations alternate the buffers; each global one clears the buffer it consumed
 			if ((iters - 1) % 2) std::swap(cur, oth);
 			if (iters > 1) {
@@ -710,8 +656,6 @@ private:
 				buf_dirty_[oth] = false;
 			}
 			if (changed) freeze_oscillating(cur);  // stopped at a multiple of kMaxIterations
-		} else {
-			changed = read_changed();
 		}
 		while (changed) {
 			if (local && buf_dirty_[oth]) clear_buffer(oth);
@@ -827,8 +771,9 @@ private:
 		// capturing the iterations runs their host side, which marks the grids it clears as
 		// clean; nothing captured has run yet
 		const bool sd = status_dirty_, bd0 = buf_dirty_[0], bd1 = buf_dirty_[1];
+		long long prefix = 0;
 		try {
-			ok = build_device_loop_into(g);
+			ok = build_loop_into(g, prefix, [] {});
 		} catch (...) {
 			ok = false;
 		}
@@ -874,7 +819,10 @@ private:
 		return p.conditional.phGraph_out[0];
 	}
 
-	bool build_device_loop_into(cudaGraph_t& g)
+	/// Captures into g what `prefix` launches, then the convergence loop (k_loop_init and the
+	/// while node); `launches` = the kernels before the while node.
+	template <class Prefix>
+	bool build_loop_into(cudaGraph_t& g, long long& launches, Prefix&& prefix)
 	{
 		const int B = 1, A = 0;
 		const auto mode = cudaStreamCaptureModeThreadLocal;
@@ -882,7 +830,10 @@ private:
 		cudaGraphConditionalHandle hloop, hsecond;
 		FG_CUDA(cudaGraphConditionalHandleCreate(&hloop, g, 0, cudaGraphCondAssignDefault));
 		FG_CUDA(cudaStreamBeginCaptureToGraph(st_, g, nullptr, nullptr, 0, mode));
+		const long long p0 = launch_count();
+		prefix();
 		FG_RUN("k_loop_init", st_, launch_pdl((k_loop_init), 1, 32, 0, st_, P_.changed, d_iters_, hloop););
+		launches = launch_count() - p0;
 		const cudaGraph_t body = end_capture_with_conditional(hloop, cudaGraphCondTypeWhile);
 		FG_CUDA(cudaGraphConditionalHandleCreate(&hsecond, body, 0, cudaGraphCondAssignDefault));
 		// first iteration of a pass: buffer B consumed, A recorded
@@ -1460,14 +1411,10 @@ private:
 	unsigned long long* acc_ = nullptr;     // node updates of all global updates so far
 	unsigned long long* zcount_ = nullptr;  // zero-layer leaf count of a bounded update
 	int* d_iters_ = nullptr;                 // iteration count of the device-side loop
-	unsigned* d_bar_ = nullptr;              // grid barrier of the persistent update launch
-	int* d_out_ = nullptr;                   // what the persistent launch reports back
-	int* d_newfrozen_ = nullptr;             // [S] surfaces the persistent launch stopped
-	bool persistent_ok_ = false;             // the persistent launch can run on this device
-	int step_max_per_sm_ = 0;                // its resident blocks per SM at most
-	int step_blocks_per_sm_ = 0;             // blocks per SM asked for (0 = automatic)
-	size_t step_smem_ = 0;                   // its dynamic shared memory
-	int launch_mode_ = 0;                    // 0 automatic, 1 persistent, 2 one kernel per phase
+	int launch_mode_ = 0;  // 0 automatic (= 1), 1 the update as one graph, 2 phase by phase
+	cudaGraphExec_t step_exec_[16] = {};  // the whole update, by due resets and delta kernel
+	long long step_launches_[16] = {};    // kernels before its while node
+	bool step_ok_ = true;
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;

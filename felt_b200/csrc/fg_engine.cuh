@@ -107,19 +107,15 @@ public:
 	virtual long long free_bricks() = 0;
 	/// Partitions reserved for surface s (the most any grid it is given may have).
 	virtual int partition_capacity(int s) const = 0;
-	/// Launch tuning: launch_mode 0 automatic (the persistent update launch where available),
-	/// 1 persistent, 2 one kernel per phase; dist_split warps per partition entry in the first
-	/// distance pass (0 = automatic); record_passes 1 warp, 2 block per entry in the passes that
-	/// record status changes (0 = automatic); blocks_per_sm of the persistent launch (0 = as
-	/// many as fit, at most 4).
-	virtual void set_tuning(int launch_mode, int dist_split, int record_passes, int blocks_per_sm) = 0;
-	virtual bool persistent_available() const = 0;
-	/// The tuning in effect: launch mode (1 persistent, 2 per phase), dist_split,
-	/// record_passes (1 warp, 2 block), blocks per SM of the persistent launch.
+	/// Launch tuning: launch_mode 0 automatic (= 1), 1 the whole global update as one CUDA
+	/// graph, 2 the update's phases launched from the host (the convergence loop still a device
+	/// graph); dist_split warps per partition entry in the first distance pass (0 = automatic);
+	/// record_passes 1 warp, 2 block per entry in the passes that record status changes (0 =
+	/// automatic).
+	virtual void set_tuning(int launch_mode, int dist_split, int record_passes) = 0;
+	/// The tuning in effect: launch mode (1 one graph, 2 phase by phase), dist_split,
+	/// record_passes (1 warp, 2 block), 0.
 	virtual void tuning(int* out) const = 0;
-	/// Check of the persistent launch's bounded waits (see k_update_step): throws
-	/// FG_ERR_TIMEOUT after about wait_s seconds, having changed nothing.
-	virtual void check_step_timeout(double wait_s) = 0;
 	virtual const Dev& dev() const = 0;
 	/// Host copy of surface s's geometry (the same as dev().geom[s]).
 	virtual const SurfGeom& geometry(int s) const = 0;
@@ -128,6 +124,14 @@ public:
 };
 
 EngineBase* make_engine(const PoolDesc& desc, cudaStream_t stream);
+
+/// Launch tuning by measurement (fg_tune.cu): the (dist_split, record_passes) pairs worth
+/// timing for a partition shape, and the fastest of them for (D, L, part) on the current
+/// device, timed on a scratch surface unless cached (ms: each candidate's device time per
+/// update, empty when cached; force: time again).
+void tune_candidates(int D, const int* part, std::vector<std::pair<int, int>>& out);
+void autotune(int D, int L, const int* part, int& ds, int& rp, std::vector<double>* ms,
+              bool force);
 
 /// Makes memory freed by cudaFreeAsync stay in the current device's stream-ordered pool for
 /// the next cudaMallocAsync (polygon arenas, ray queues) instead of going back to the driver
@@ -147,9 +151,6 @@ bool prof_on();
 void prof_enable(bool on);
 /// Brackets only the launches of the named kernel (NULL or "" = every kernel).
 void prof_only(const char* name);
-/// Whether profiling needs every phase as its own launch (on, and not limited to the
-/// persistent update kernel k_update_step).
-bool prof_per_launch();
 /// Synchronises pending events and returns (name, total ms, launches) per kernel name.
 struct ProfEntry {
 	std::string name;

@@ -122,9 +122,8 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 	d_scan_layers(cnt, NL, S, woffl, frozen);
 }
 
-/// The block index and block count a kernel body works with: the hardware grid's when the body
-/// runs as its own launch, or a share of a persistent launch's blocks when it runs as one phase
-/// of the whole-update kernel (fg_step.cuh).
+/// The block index and block count a kernel body works with (the hardware grid's, or another
+/// grid dimension's where the launch is two-dimensional).
 struct GridPos {
 	int bid, nb;
 };
@@ -631,20 +630,6 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView 
 	                   ((blockIdx.x - ca.nblocks) * blockDim.x + threadIdx.x) >> 5,
 	                   ((gridDim.x - ca.nblocks) * blockDim.x) >> 5);
 }
-/// k_dist1 as a phase of a persistent launch: the previous pass's compaction (one surface per
-/// block, in turn), then the distance pass over all the launch's warps.
-template <int D, int L>
-__device__ void d_dist1(const Dev& P, const int* woff, ListView lv, int k, float side, int split,
-                        const CompactArgs& ca, GridPos G)
-{
-	for (int s = G.bid; s < ca.nblocks; s += G.nb) {
-		compact_surface<L>(P, ca, s);
-		__syncthreads();
-	}
-	d_dist1_work<D, L>(P, woff, lv, k, side, split, (G.bid * blockDim.x + threadIdx.x) >> 5,
-	                   (G.nb * blockDim.x) >> 5);
-}
-
 /// update_distance second pass (Surface.hpp:1075-1121): apply and record status changes. One
 /// block per partition entry (bricks of thousands of leaves): every thread commits one leaf,
 /// and the rare layer changes are recorded in list order (status_round).

@@ -114,13 +114,6 @@ std::vector<ProfEntry> prof_read()
 	return out;
 }
 
-bool prof_per_launch()
-{
-	Prof& p = prof();
-	std::lock_guard<std::mutex> lk(p.mu);
-	return p.on && p.only != "k_update_step";
-}
-
 void prof_only(const char* name)
 {
 	Prof& p = prof();

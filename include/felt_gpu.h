@@ -66,14 +66,17 @@ typedef struct fg_config {
 	size_t brick_capacity; /* bricks (partitions) the device pool can hold; 0 = automatic   */
 	size_t vertex_capacity;/* initial polygonisation arena, vertices (simplices: twice that);
 	                          0 = 2^20; it grows on demand                                  */
-	int launch_mode;       /* how a global update launches: 0 automatic (the whole update as
-	                          one persistent launch where the device can launch cooperatively),
-	                          1 persistent, 2 one kernel per phase                         */
+	int launch_mode;       /* how a global update with a builtin speed launches: 0 automatic
+	                          (= 1), 1 the whole update as one CUDA graph (its convergence
+	                          loop a while node), 2 the update's phases launched one by one
+	                          from the host, the convergence loop a device graph            */
 	int dist_split;        /* threads per brick in the first distance pass, in warps per
 	                          partition entry (1, 2, 4, 8); 0 = automatic                  */
 	int record_passes;     /* threads per brick in the passes that record status changes:
 	                          1 a warp, 2 a block per partition entry; 0 = automatic        */
-	int blocks_per_sm;     /* resident blocks per SM of the persistent launch; 0 = automatic */
+	int autotune;          /* 1: dist_split and record_passes left at 0 take the values
+	                          fg_autotune finds for this D, L, partition and device (timed
+	                          once per process, or read from the file FELT_TUNE_CACHE names) */
 	int reserved[4];
 } fg_config;
 
@@ -389,14 +392,20 @@ FG_API int fg_request_bricks(const fg_server_config* cfg, const fg_request* r,
                              unsigned long long* bricks);
 FG_API int fg_brick_bytes(int dims, int layers, const int* part, double* bytes);
 
-/* Check of the persistent update launch's bounded waits (no counterpart in the reference): runs
- * it with a grid barrier that can never complete; every block gives up after about wait_s
- * seconds and the call returns FG_ERR_TIMEOUT, the surface unchanged (the kernel stops at its
- * entry barrier, before any work) and usable. FG_ERR_ARG where the persistent launch is not
- * available. */
-FG_API int fg_check_step_timeout(fg_surface* s, double wait_s);
-/* The launch tuning in effect on a surface or batch: out[0] launch mode (1 persistent, 2 one
- * kernel per phase), out[1] dist_split, out[2] record_passes, out[3] blocks per SM. */
+/* Launch tuning by measurement (no counterpart in the reference). fg_autotune_candidates lists
+ * the (dist_split, record_passes) pairs worth timing for a partition shape (pairs[2i],
+ * pairs[2i+1]). fg_autotune times each on a scratch surface of this dimension, layer count and
+ * partition shape on the current device (a sphere grown to a quarter of a grid of 64..256 per
+ * axis, then curvature-plus-constant updates) and writes the fastest pair into cfg's
+ * dist_split and record_passes (other fields untouched); ms receives each candidate's device
+ * time per update in candidate order and *n their number, 0 when the result came from the
+ * process's cache or the FELT_TUNE_CACHE file (force = 1 times again). The knobs change launch
+ * shapes only: results are the same under every pair. */
+FG_API int fg_autotune_candidates(int dims, const int* part, int* pairs, size_t cap, size_t* n);
+FG_API int fg_autotune(int dims, int layers, const int* part, int force, fg_config* cfg,
+                       double* ms, size_t ms_cap, size_t* n);
+/* The launch tuning in effect on a surface or batch: out[0] launch mode (1 one graph, 2 phase
+ * by phase), out[1] dist_split, out[2] record_passes, out[3] 0. */
 FG_API int fg_surface_tuning(fg_surface* s, int* out);
 FG_API int fg_batch_tuning(fg_batch* b, int* out);
 
