@@ -194,12 +194,18 @@ def combine_ranks(dist, t_ms, wall_s, node_updates, device):
 # Device workloads
 # ---------------------------------------------------------------------------------------------
 
+# Launch tuning of every surface and batch the bench creates (fg_config: launch_mode,
+# autotune), from the command line.
+TUNING = {}
+
+
 class SingleWork:
     """One Surface (+ Polys) through the C ABI."""
 
     def __init__(self, fb, cfg, brick_capacity=0):
         self.fb, self.cfg = fb, cfg
-        self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=brick_capacity)
+        self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=brick_capacity,
+                            **TUNING)
         self.p = fb.Polys(self.s)
         self.s.seed((0,) * cfg["D"])
         for _ in range(cfg["expand"]):
@@ -256,7 +262,7 @@ class BatchWork:
     def __init__(self, fb, cfg, name, shard=0):
         self.fb, self.cfg = fb, cfg
         sizes, centres, speeds = batch_surfaces(name, cfg, shard)
-        self.b = fb.Batch(sizes, cfg["part"], cfg["L"])
+        self.b = fb.Batch(sizes, cfg["part"], cfg["L"], **TUNING)
         self.b.seed(centres)
         self.speeds = self.b.speed_array(speeds)  # converted once; the speeds are fixed
         # a full polygonisation at setup, so that its buffers exist before timing
@@ -306,7 +312,7 @@ class PlainSubset:
         self.items = []
         self.done = 0
         for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
-            s = fb.Surface(sz, cfg["part"], cfg["L"])
+            s = fb.Surface(sz, cfg["part"], cfg["L"], **TUNING)
             s.seed(c)
             self.items.append((s, fb.Polys(s), sp))
 
@@ -1090,7 +1096,7 @@ def serve_plain(fb, cfg, k):
     nu, secs, make = 0, 0.0, 0.0
     for r in reqs:
         t0 = time.perf_counter()
-        s = fb.Surface(r.size, cfg["part"], cfg["L"])
+        s = fb.Surface(r.size, cfg["part"], cfg["L"], **TUNING)
         p = fb.Polys(s)
         t1 = time.perf_counter()
         s.seed(r.centre)
@@ -1326,7 +1332,13 @@ def main():
                     help="brick pool capacity of single-surface configs (0 = automatic)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop")
+    ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="fg_config.launch_mode: 1 one CUDA graph per update (0 = automatic = "
+                         "1), 2 every kernel launched from the host (per-kernel profilers)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="launch shapes by measurement (fg_autotune) instead of by brick size")
     args = ap.parse_args()
+    TUNING.update(launch_mode=args.launch_mode, autotune=args.autotune)
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, args.config, cfg)

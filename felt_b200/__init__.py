@@ -46,7 +46,7 @@ class Config(C.Structure):
 def make_config(brick_capacity=0, vertex_capacity=0, launch_mode=0, dist_split=0,
                 record_passes=0, autotune=False):
     """fg_config: pool sizes and launch tuning (launch_mode 0 automatic, 1 the whole global
-    update as one CUDA graph, 2 its phases launched one by one; dist_split warps per partition
+    update as one CUDA graph, 2 every kernel launched from the host, no graphs; dist_split warps per partition
     entry in the first distance pass; record_passes 1 warp / 2 block per entry in the
     recording passes; 0 = automatic everywhere; autotune: the knobs left at 0 take the values
     autotune() measures)."""
@@ -352,6 +352,12 @@ class Surface:
     def band_size(self):
         n = C.c_size_t()
         _chk(lib().fg_band_size(self._h, C.byref(n)))
+        return n.value
+
+    def iterations(self):
+        """Convergence-loop iterations of the last update (fg_update_iterations)."""
+        n = C.c_int()
+        _chk(lib().fg_update_iterations(self._h, C.byref(n)))
         return n.value
 
     def work_units(self):

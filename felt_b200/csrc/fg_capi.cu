@@ -395,6 +395,15 @@ int fg_partition_state(fg_surface* s, size_t part, int* active, float* backgroun
 	});
 }
 
+int fg_update_iterations(fg_surface* s, int* iterations)
+{
+	return guard([&] {
+		need(s, "surface");
+		need(iterations, "iterations");
+		*iterations = s->eng->stats().iterations;
+	});
+}
+
 int fg_stats(fg_surface* s, size_t* iso, size_t* delta)
 {
 	return guard([&] {

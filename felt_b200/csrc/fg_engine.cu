@@ -312,10 +312,10 @@ public:
 
 public:
 	/// Launch tuning (fg_config): how the global update launches (0 automatic = 1, 1 the
-	/// whole update as one CUDA graph, 2 the update's phases launched from the host with the
-	/// convergence loop as a device graph), warps per partition entry in the first distance
-	/// pass (0 = automatic), warp (1) or block (2) per entry in the record passes (0 =
-	/// automatic). Graphs captured under the previous tuning are dropped.
+	/// whole update as one CUDA graph, 2 every kernel launched from the host, no graphs),
+	/// warps per partition entry in the first distance pass (0 = automatic), warp (1) or block
+	/// (2) per entry in the record passes (0 = automatic). Graphs captured under the previous
+	/// tuning are dropped.
 	void set_tuning(int launch_mode, int dist_split, int record_passes) override
 	{
 		launch_mode_ = launch_mode;
@@ -488,7 +488,8 @@ private:
 		if (run_step_graph(curv)) return;
 		update_begin_global();
 		delta_builtin(curv);
-		update_finish_global();
+		first_passes(true);
+		converge();
 	}
 
 	void update_begin_global() override
@@ -504,7 +505,7 @@ private:
 
 	void update_finish_global() override
 	{
-		first_passes();
+		first_passes(false);
 		converge();
 	}
 
@@ -521,10 +522,12 @@ private:
 
 	/// update_end_global up to the convergence loop (Surface.hpp:739-751):
 	/// update_zero_layer(&affected_buffer), the first distance passes recording into buffer B.
-	void first_passes()
+	/// woff_ready: the zero layer's entry offsets are still those update_begin_global scanned
+	/// (a builtin speed changes no list in between).
+	void first_passes(bool woff_ready)
 	{
 		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
-		scan(P_.pcnt, L, 0);
+		if (!woff_ready) scan(P_.pcnt, L, 0);
 		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
 		zero_apply(iso, nullptr, B);
 		defer_compact(P_.woff, P_.plist, L, B);
@@ -579,7 +582,7 @@ private:
 				count_band();
 				scan(P_.pcnt, L, 0);
 				delta_builtin(curv);
-				first_passes();
+				first_passes(true);
 				flush();
 				expand();
 				retire();
@@ -700,7 +703,7 @@ private:
 	/// profiling is on or if capture is not possible.
 	bool replay_iteration(int cur, int oth)
 	{
-		if (!graphs_ok_ || prof_on()) return false;
+		if (launch_mode_ == 2 || !graphs_ok_ || prof_on()) return false;
 		cudaGraphExec_t& ex = iter_exec_[cur];
 		if (!ex) {
 			cudaGraph_t gph = nullptr;
@@ -747,7 +750,7 @@ private:
 	/// runs out of changes.
 	bool run_device_loop(int& changed, int& iters)
 	{
-		if (!loop_ok_ || !graphs_ok_ || prof_on()) return false;
+		if (launch_mode_ == 2 || !loop_ok_ || !graphs_ok_ || prof_on()) return false;
 		if (!loop_exec_ && !build_device_loop()) return false;
 		FG_CUDA(cudaGraphLaunch(loop_exec_, st_));
 		int out[2] = {0, 0};

@@ -108,8 +108,7 @@ public:
 	/// Partitions reserved for surface s (the most any grid it is given may have).
 	virtual int partition_capacity(int s) const = 0;
 	/// Launch tuning: launch_mode 0 automatic (= 1), 1 the whole global update as one CUDA
-	/// graph, 2 the update's phases launched from the host (the convergence loop still a device
-	/// graph); dist_split warps per partition entry in the first distance pass (0 = automatic);
+	/// graph, 2 every kernel launched from the host, no graphs; dist_split warps per partition entry in the first distance pass (0 = automatic);
 	/// record_passes 1 warp, 2 block per entry in the passes that record status changes (0 =
 	/// automatic).
 	virtual void set_tuning(int launch_mode, int dist_split, int record_passes) = 0;

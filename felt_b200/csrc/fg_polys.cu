@@ -893,13 +893,9 @@ public:
 	}
 
 private:
-	int pbase_of()
-	{
-		int cc[3], co[3];
-		int base = 0;
-		for (int t = 0; t < s_; t++) base += (int)eng_.partitions(t, cc, co);
-		return base;
-	}
+	/// First global partition index of the selected surface: its range in the pool, which
+	/// holds its partition capacity (more than its grid's partitions on a serving pool).
+	int pbase_of() { return eng_.geometry(s_).pbase; }
 	int check_part(size_t part)
 	{
 		int cc[3], co[3];

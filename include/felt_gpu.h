@@ -68,8 +68,8 @@ typedef struct fg_config {
 	                          0 = 2^20; it grows on demand                                  */
 	int launch_mode;       /* how a global update with a builtin speed launches: 0 automatic
 	                          (= 1), 1 the whole update as one CUDA graph (its convergence
-	                          loop a while node), 2 the update's phases launched one by one
-	                          from the host, the convergence loop a device graph            */
+	                          loop a while node), 2 every kernel launched one by one from
+	                          the host, no graphs (per-kernel profilers, debugging)          */
 	int dist_split;        /* threads per brick in the first distance pass, in warps per
 	                          partition entry (1, 2, 4, 8); 0 = automatic                  */
 	int record_passes;     /* threads per brick in the passes that record status changes:
@@ -215,6 +215,11 @@ FG_API int fg_partition_state(fg_surface* s, size_t part, int* active, float* ba
 
 /* stats() (include/Felt/Surface.hpp:623-629). */
 FG_API int fg_stats(fg_surface* s, size_t* active_isogrid_partitions, size_t* active_delta_partitions);
+
+/* Iterations of the convergence loop (distance passes, flush, expansion) the last global or
+ * local update ran, the first one included (the reference's loop at Surface.hpp:747-761 and
+ * 417-428 does not count them). */
+FG_API int fg_update_iterations(fg_surface* s, int* iterations);
 
 /* Narrow-band node count at the start of the last update: sum over the 2L+1 layers. */
 FG_API int fg_band_size(fg_surface* s, size_t* n);

@@ -1,5 +1,5 @@
 """The whole global update as one CUDA graph (launch mode 1, the default) against the same update
-with its phases launched one by one from the host (launch mode 2): every list, order, partition
+with every kernel launched one by one from the host (launch mode 2, no graphs): every list, order, partition
 list and value must be the same, for single surfaces, batches of uneven surfaces (including one
 the convergence cap stops), alternating speed kinds (which select different captured graphs) and
 every launch-tuning knob; both count the same kernels per step."""
@@ -27,7 +27,7 @@ def _run(mode, size, part, L, seed, schedule, **tuning):
         for _ in range(n):
             l0 = fb.launch_count()
             s.update(**kw)
-            launches.append(fb.launch_count() - l0)
+            launches.append((fb.launch_count() - l0, s.iterations()))
         states.append((s.dump(), s.snapshot()))
     return s, states, launches
 
@@ -56,8 +56,10 @@ def test_step_graph_equals_phase_by_phase(case):
         assert d is None, d
         assert np.array_equal(pa, pb)
     assert a.node_updates() == b.node_updates()
-    # the same kernels run either way (the graph's are counted when it replays)
-    assert la == lb
+    # the same kernels run either way (the graph's are counted when it replays), plus the
+    # device loop's control kernels: one to start it and one test per further iteration
+    assert [it for _, it in la] == [it for _, it in lb]
+    assert [na - nb for (na, _), (nb, _) in zip(la, lb)] == [it for _, it in la]
 
 
 def test_step_graph_matches_oracle_with_polys():
