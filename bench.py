@@ -1337,8 +1337,15 @@ def main():
                          "1), 2 every kernel launched from the host (per-kernel profilers)")
     ap.add_argument("--autotune", action="store_true",
                     help="launch shapes by measurement (fg_autotune) instead of by brick size")
+    ap.add_argument("--delta-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="fg_config.delta_kernel: the curvature speed functor 1 reading the pool "
+                         "directly, 2 over bricks staged with their halo (0 = automatic)")
+    ap.add_argument("--fuse-passes", type=int, default=0, choices=[0, 1, 2],
+                    help="fg_config.fuse_passes: the distance passes 1 as 4L launches, 2 as 2L+1 "
+                         "fused ones (0 = automatic)")
     args = ap.parse_args()
-    TUNING.update(launch_mode=args.launch_mode, autotune=args.autotune)
+    TUNING.update(launch_mode=args.launch_mode, autotune=args.autotune,
+                  delta_kernel=args.delta_kernel, fuse_passes=args.fuse_passes)
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, args.config, cfg)

@@ -40,18 +40,22 @@ class Speed(C.Structure):
 class Config(C.Structure):
     _fields_ = [("brick_capacity", C.c_size_t), ("vertex_capacity", C.c_size_t),
                 ("launch_mode", C.c_int), ("dist_split", C.c_int), ("record_passes", C.c_int),
-                ("autotune", C.c_int), ("reserved", C.c_int * 4)]
+                ("autotune", C.c_int), ("delta_kernel", C.c_int), ("fuse_passes", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 def make_config(brick_capacity=0, vertex_capacity=0, launch_mode=0, dist_split=0,
-                record_passes=0, autotune=False):
+                record_passes=0, autotune=False, delta_kernel=0, fuse_passes=0):
     """fg_config: pool sizes and launch tuning (launch_mode 0 automatic, 1 the whole global
     update as one CUDA graph, 2 every kernel launched from the host, no graphs; dist_split warps per partition
     entry in the first distance pass; record_passes 1 warp / 2 block per entry in the
-    recording passes; 0 = automatic everywhere; autotune: the knobs left at 0 take the values
+    recording passes; delta_kernel of curvature speeds 1 direct / 2 staged brick + halo;
+    fuse_passes 1 separate / 2 fused distance passes;
+    0 = automatic everywhere; autotune: dist_split and record_passes left at 0 take the values
     autotune() measures)."""
     return Config(int(brick_capacity), int(vertex_capacity), int(launch_mode), int(dist_split),
-                  int(record_passes), 1 if autotune else 0)
+                  int(record_passes), 1 if autotune else 0, int(delta_kernel),
+                  int(fuse_passes))
 
 
 def autotune_candidates(part):
@@ -76,9 +80,10 @@ def autotune(part, layers, force=False):
 
 
 def _tuning(fn, h):
-    out = (C.c_int * 4)()
+    out = (C.c_int * 8)()
     _chk(fn(h, out))
-    return dict(launch_mode=out[0], dist_split=out[1], record_passes=out[2])
+    return dict(launch_mode=out[0], dist_split=out[1], record_passes=out[2],
+                delta_kernel=out[3], fuse_passes=out[4])
 
 
 def build():
@@ -197,7 +202,8 @@ class Surface:
     """Felt::Surface<D,L>(size, size_partition) on the GPU (include/Felt/Surface.hpp:163-173)."""
 
     def __init__(self, size, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
-        """tuning: launch_mode, dist_split, record_passes (see make_config)."""
+        """tuning: launch_mode, dist_split, record_passes, delta_kernel, autotune (see
+        make_config)."""
         self.D = len(size)
         self.L = int(layers)
         self.size = tuple(int(s) for s in size)
@@ -391,7 +397,8 @@ class Batch:
     same kernel launches. Per surface the results equal a separate Surface's."""
 
     def __init__(self, sizes, part, layers, brick_capacity=0, vertex_capacity=0, **tuning):
-        """tuning: launch_mode, dist_split, record_passes (see make_config)."""
+        """tuning: launch_mode, dist_split, record_passes, delta_kernel, autotune (see
+        make_config)."""
         self.n = len(sizes)
         self.D = len(part)
         self.L = int(layers)

@@ -68,7 +68,11 @@ void apply_tuning(fg::EngineBase& eng, const fg_config* cfg)
 		if (ds == 0) ds = tds;
 		if (rp == 0) rp = trp;
 	}
-	eng.set_tuning(cfg->launch_mode, ds, rp);
+	if (cfg->delta_kernel < 0 || cfg->delta_kernel > 2)
+		throw fg::Error(FG_ERR_ARG, "delta_kernel must be 0, 1 or 2");
+	if (cfg->fuse_passes < 0 || cfg->fuse_passes > 2)
+		throw fg::Error(FG_ERR_ARG, "fuse_passes must be 0, 1 or 2");
+	eng.set_tuning(cfg->launch_mode, ds, rp, cfg->delta_kernel, cfg->fuse_passes);
 }
 
 void put_list(const std::vector<uint32_t>& v, uint32_t* out, size_t cap, size_t* n)

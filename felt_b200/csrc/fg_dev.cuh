@@ -104,6 +104,7 @@ struct Dev {
 	int* q_sunion;    // [NP] partitions with status changes this iteration
 	int* sflag;       // [NP] membership flag for q_sunion
 	unsigned int* eflag;  // [NP] per-entry flags of the current pass
+	unsigned int* eflag2; // [NP] the same for the odd passes of the fused distance passes
 	unsigned* app;    // [NP*NL] flush: lists that went 0->1 during phase f (bitmask over to)
 	unsigned* rem;    // [NP] flush: lists that went ->0 during their own phase (bitmask)
 	unsigned long long* pap;  // [2*NP] expansion partition appends: first claim key per surface
@@ -318,6 +319,29 @@ struct PoolGet {
 	const Dev& P;
 	const SurfGeom& g;
 	__device__ float operator()(const Vec<D>& p) const { return get_phi<D, L>(P, g, p); }
+};
+
+/// Reads the isogrid around one brick: positions inside the brick's partition and the grid
+/// straight from the brick (no partition lookup), the others through the pool. The same values
+/// as PoolGet.
+template <int D, int L>
+struct BrickGet {
+	const Dev& P;
+	const SurfGeom& g;
+	const float* brick;
+	Vec<D> org;  // world position of the brick's leaf 0
+	__device__ float operator()(const Vec<D>& p) const
+	{
+		int leaf = 0;
+		bool in = true;
+#pragma unroll
+		for (int a = 0; a < D; a++) {
+			const int q = p[a] - org[a];
+			in = in && (unsigned)q < (unsigned)P.csz[a] && p[a] < g.hi[a];
+			leaf += q * P.lstr[a];
+		}
+		return in ? brick[leaf] : get_phi<D, L>(P, g, p);
+	}
 };
 
 template <int D, int L>

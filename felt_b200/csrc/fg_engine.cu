@@ -224,6 +224,7 @@ public:
 		P.q_sunion = dalloc<int>(NP, o);
 		P.sflag = dalloc<int>(NP, o);
 		P.eflag = dalloc<unsigned>(NP, o);
+		P.eflag2 = dalloc<unsigned>(NP, o);
 		P.app = dalloc<unsigned>(npl, o);
 		P.rem = dalloc<unsigned>(NP, o);
 		P.pap = dalloc<unsigned long long>(2 * (size_t)NP, o);
@@ -297,6 +298,9 @@ public:
 			                             cudaFuncAttributeMaxDynamicSharedMemorySize,
 			                             (int)smem_halo_));
 		}
+		// staging pays off once a brick's zero layer is dense: measured on C2 (16^3 bricks) the
+		// staged kernel took a third of the direct one's time per step over 40 steps
+		delta_staged_ = smem_halo_ != 0;
 		dist_split_ = BV >= 4096 ? 4 : BV >= 1024 ? 2 : 1;
 		block_passes_ = BV >= 2048;
 		smem_flush_ = flush_smem_bytes(BV, NL);
@@ -316,12 +320,17 @@ public:
 	/// warps per partition entry in the first distance pass (0 = automatic), warp (1) or block
 	/// (2) per entry in the record passes (0 = automatic). Graphs captured under the previous
 	/// tuning are dropped.
-	void set_tuning(int launch_mode, int dist_split, int record_passes) override
+	void set_tuning(int launch_mode, int dist_split, int record_passes, int delta_kernel,
+	                int fuse_passes) override
 	{
+		if (fuse_passes == 1) fused_ = false;
+		if (fuse_passes == 2) fused_ = true;
 		launch_mode_ = launch_mode;
 		if (dist_split > 0) dist_split_ = dist_split;
 		if (record_passes == 1) block_passes_ = false;
 		if (record_passes == 2) block_passes_ = true;
+		if (delta_kernel == 1) delta_staged_ = false;
+		if (delta_kernel == 2) delta_staged_ = smem_halo_ != 0;
 		drop_graphs();
 	}
 	void tuning(int* out) const override
@@ -329,7 +338,8 @@ public:
 		out[0] = launch_mode_ == 2 ? 2 : 1;
 		out[1] = dist_split_;
 		out[2] = block_passes_ ? 2 : 1;
-		out[3] = 0;
+		out[3] = delta_staged_ ? 2 : 1;
+		out[4] = fused_ ? 2 : 1;
 	}
 
 private:
@@ -484,10 +494,11 @@ private:
 		                        st_));
 		bool any_curv = false;
 		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
-		const bool curv = any_curv && smem_halo_;
-		if (run_step_graph(curv)) return;
+		// staging a brick with its halo pays only for the curvature stencil
+		const bool staged = any_curv && smem_halo_ && delta_staged_;
+		if (run_step_graph(staged)) return;
 		update_begin_global();
-		delta_builtin(curv);
+		delta_builtin(staged);
 		first_passes(true);
 		converge();
 	}
@@ -510,14 +521,15 @@ private:
 	}
 
 private:
-	/// The builtin speed functor over the zero layer (Surface.hpp:263-294): with curvature,
-	/// over staged bricks with their halo.
-	void delta_builtin(bool curv)
+	/// The builtin speed functor over the zero layer (Surface.hpp:263-294): staged, over
+	/// bricks staged with their halo in shared memory (one block each), else warps reading the
+	/// pool directly.
+	void delta_builtin(bool staged)
 	{
-		if (curv)
+		if (staged)
 			FG_RUN("k_delta_smem", st_, launch_pdl((k_delta_smem<D, L>), sm_count() * 8, 128, smem_halo_, st_, P_, d_speeds_););
 		else
-			FG_RUN("k_delta_builtin", st_, launch_pdl((k_delta_builtin<D, L>), warp_grid_, 256, 0, st_, P_, d_speeds_););
+			FG_RUN("k_delta_builtin", st_, launch_pdl((k_delta_builtin<D, L>), warp_grid_, 256, 0, st_, P_, d_speeds_, dist_split_););
 	}
 
 	/// update_end_global up to the convergence loop (Surface.hpp:739-751):
@@ -528,7 +540,7 @@ private:
 	{
 		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
 		if (!woff_ready) scan(P_.pcnt, L, 0);
-		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt};
+		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt, P_.lkp};
 		zero_apply(iso, nullptr, B);
 		defer_compact(P_.woff, P_.plist, L, B);
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
@@ -543,12 +555,12 @@ private:
 	/// one read-back of the loop's count. Returns false (the caller launches phase by phase)
 	/// under launch mode 2, while per-launch profiling is on, or where the graph cannot be
 	/// built.
-	bool run_step_graph(bool curv)
+	bool run_step_graph(bool staged)
 	{
 		if (launch_mode_ == 2 || !loop_ok_ || !graphs_ok_ || !step_ok_ || prof_on()) return false;
 		const int key = (status_dirty_ ? 1 : 0) | (buf_dirty_[0] ? 2 : 0) |
-		                (buf_dirty_[1] ? 4 : 0) | (curv ? 8 : 0);
-		if (!step_exec_[key] && !build_step_graph(key, curv)) return false;
+		                (buf_dirty_[1] ? 4 : 0) | (staged ? 8 : 0);
+		if (!step_exec_[key] && !build_step_graph(key, staged)) return false;
 		FG_CUDA(cudaGraphLaunch(step_exec_[key], st_));
 		int out[2] = {0, 0};
 		FG_CUDA(cudaMemcpyAsync(&out[0], d_iters_, sizeof(int), cudaMemcpyDeviceToHost, st_));
@@ -565,7 +577,7 @@ private:
 		return true;
 	}
 
-	bool build_step_graph(int key, bool curv)
+	bool build_step_graph(int key, bool staged)
 	{
 		std::lock_guard<std::recursive_mutex> lock(device_lock());
 		cudaGraph_t g = nullptr;
@@ -581,7 +593,7 @@ private:
 				copy_plists();
 				count_band();
 				scan(P_.pcnt, L, 0);
-				delta_builtin(curv);
+				delta_builtin(staged);
 				first_passes(true);
 				flush();
 				expand();
@@ -689,7 +701,9 @@ private:
 	{
 		clear_status();
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
-		const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur]};
+		// the fused passes (lookup given) on the global update's iterations only
+		const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur],
+		                  local ? nullptr : P_.alkp[cur]};
 		distance_passes(bv, oth);
 		flush();
 		expand();
@@ -1309,11 +1323,40 @@ private:
 	void distance_passes(const ListView& lv, int b)
 	{
 		FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
+		if (fused_ && lv.lkp) {
+			fused_passes(lv, b);
+			return;
+		}
 		for (int k = -1; k >= -L; k--) layer_pass(lv, k, -1.0f, b);
 		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
 		const CompactArgs ca = take_compact();
 		if (ca.nblocks)
 			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca););
+	}
+
+	/// The 2L layer passes as 2L+1 launches (k_dist_fused): launch j runs the second pass of
+	/// layer j-1 and the first pass of layer j, with the compaction of layer j-2's records (or
+	/// the zero-layer update's, pending from before the passes) in its first blocks. The
+	/// passes' entry flags alternate between the two arrays by pass parity, so a compaction
+	/// never reads flags the second pass beside it writes.
+	void fused_passes(const ListView& lv, int b)
+	{
+		auto layer = [](int j) { return j < L ? -(j + 1) : j - L + 1; };
+		auto woff_of = [&](int j) { return P_.woffl + (size_t)(layer(j) + L) * (P_.S + 1); };
+		auto flags_of = [&](int j) { return (j & 1) ? P_.eflag : P_.eflag2; };
+		CompactArgs ca = take_compact();  // the zero-layer update's, flags in Dev::eflag
+		for (int j = 0; j <= 2 * L; j++) {
+			const FusedPass p2 = j >= 1 ? FusedPass{woff_of(j - 1), layer(j - 1)} : FusedPass{nullptr, 0};
+			const FusedPass p1 = j < 2 * L ? FusedPass{woff_of(j), layer(j)} : FusedPass{nullptr, 0};
+			const float side = j < L ? -1.0f : 1.0f;
+			unsigned* ef2 = j >= 1 ? flags_of(j - 1) : nullptr;
+			const int grid = (p2.woff && p1.woff ? 2 : 1) * warp_grid_ + ca.nblocks;
+			FG_RUN("k_dist_fused", st_, launch_pdl((k_dist_fused<D, L>), grid, 256, 0, st_, P_, lv, p2, p1, side, dist_split_, b, ef2, ca, block_passes_ ? 1 : 0););
+			ca = j >= 1 ? CompactArgs{P_.S, woff_of(j - 1), lv.plist, layer(j - 1) + L, b, flags_of(j - 1)}
+			            : CompactArgs{0, nullptr, nullptr, 0, 0};
+		}
+		// the last pass's records: compacted before the flush reads them
+		FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca););
 	}
 
 	/// A pass's compaction waits to ride on the next first-pass launch (k_dist1).
@@ -1418,6 +1461,11 @@ private:
 	cudaGraphExec_t step_exec_[16] = {};  // the whole update, by due resets and delta kernel
 	long long step_launches_[16] = {};    // kernels before its while node
 	bool step_ok_ = true;
+	bool delta_staged_ = true;   // curvature speeds over staged bricks (k_delta_smem)
+	// the global update's distance passes fused (k_dist_fused): the same results in 2L+1
+	// launches instead of 4L, but no faster on C2 (1.33 against 1.28 ms per step), so off
+	// unless asked for
+	bool fused_ = false;
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;

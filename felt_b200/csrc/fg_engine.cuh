@@ -110,10 +110,14 @@ public:
 	/// Launch tuning: launch_mode 0 automatic (= 1), 1 the whole global update as one CUDA
 	/// graph, 2 every kernel launched from the host, no graphs; dist_split warps per partition entry in the first distance pass (0 = automatic);
 	/// record_passes 1 warp, 2 block per entry in the passes that record status changes (0 =
-	/// automatic).
-	virtual void set_tuning(int launch_mode, int dist_split, int record_passes) = 0;
-	/// The tuning in effect: launch mode (1 one graph, 2 phase by phase), dist_split,
-	/// record_passes (1 warp, 2 block), 0.
+	/// automatic); delta_kernel of curvature speeds 1 direct, 2 staged brick + halo (0 =
+	/// automatic); fuse_passes 1 the global update's distance passes as 4L launches, 2 as 2L+1
+	/// fused ones (0 = automatic).
+	virtual void set_tuning(int launch_mode, int dist_split, int record_passes, int delta_kernel,
+	                        int fuse_passes) = 0;
+	/// The tuning in effect (5 values): launch mode (1 one graph, 2 phase by phase),
+	/// dist_split, record_passes (1 warp, 2 block), delta kernel (1 direct, 2 staged), distance
+	/// passes (1 separate, 2 fused).
 	virtual void tuning(int* out) const = 0;
 	virtual const Dev& dev() const = 0;
 	/// Host copy of surface s's geometry (the same as dev().geom[s]).

@@ -13,12 +13,14 @@ namespace fg {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-/// A partition-list + leaf-list pair: the isogrid's own lists, or one affected buffer's.
+/// A partition-list + leaf-list pair: the isogrid's own lists, or one affected buffer's, with
+/// the leaf lookup (a leaf's position in its list) where a kernel needs it.
 struct ListView {
 	const int* plist;
 	const int* pcnt;
 	const uint16_t* lst;
 	const int* lcnt;
+	const uint16_t* lkp = nullptr;
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -269,12 +271,17 @@ __device__ __forceinline__ void status_round(const Dev& P, int gp, int sl, int f
 // update(fn) functor loop (Surface.hpp:263-294) with a builtin speed: delta of every zero-layer
 // leaf, written to the brick's delta array.
 // ---------------------------------------------------------------------------------------------
+/// `split` warps per partition entry take interleaved 32-leaf chunks of its zero layer; the
+/// stencil reads inside the brick skip the partition lookup (BrickGet).
 template <int D, int L>
-__device__ void d_delta_builtin(const Dev& P, const Speed* speeds, GridPos G)
+__device__ void d_delta_builtin(const Dev& P, const Speed* speeds, int split, GridPos G)
 {
 	constexpr int NL = 2 * L + 1;
-	FG_WARP_LOOP(P.woff)
-	{
+	const int lane = lane_id();
+	const int nwarps = (G.nb * blockDim.x) >> 5;
+	const int total = P.woff[P.S] * split;
+	for (int v = (G.bid * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
+		const int e = v / split, part = v - e * split;
 		const int s = entry_surface(P.woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const Speed sp = speeds[s];
@@ -282,18 +289,21 @@ __device__ void d_delta_builtin(const Dev& P, const Speed* speeds, GridPos G)
 		const int sl = P.slot[gp];
 		const int n = P.lcnt[sl * NL + L];
 		const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
-		for (int j = lane; j < n; j += 32) {
+		BrickGet<D, L> get{P, g, P.phi + (size_t)sl * P.BV, Vec<D>()};
+#pragma unroll
+		for (int a = 0; a < D; a++) get.org[a] = P.porig[gp * 3 + a];
+		for (int j = part * 32 + lane; j < n; j += 32 * split) {
 			const int leaf = lst[j];
-			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval<D, L>(P, g, sp, leaf_pos<D>(P, gp, leaf));
+			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval_g<D>(get, sp, leaf_pos<D>(P, gp, leaf));
 		}
-		if (lane == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
+		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
 	}
 }
 template <int D, int L>
-__global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds)
+__global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds, int split)
 {
 	pdl_enter();
-	d_delta_builtin<D, L>(P, speeds, hw_grid());
+	d_delta_builtin<D, L>(P, speeds, split, hw_grid());
 }
 
 /// Fills box with the isogrid over a partition and a one-node halo ((part+2)^D values, row-major,
@@ -502,6 +512,7 @@ struct CompactArgs {
 	const int* plist;   // its partition lists
 	int li;             // its layer index
 	int b;              // affected buffer its changes went to
+	const unsigned* ef = nullptr;  // its entry flags (nullptr = Dev::eflag)
 };
 
 template <int L>
@@ -513,6 +524,7 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 	__shared__ int slp[TILE];
 	__shared__ int scnt[NL + 1];
 	const int li = a.li, b = a.b;
+	const unsigned* ef = a.ef ? a.ef : P.eflag;
 	const SurfGeom& g = P.geom[s];
 	const int e0 = a.woff[s], e1 = a.woff[s + 1];
 	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -524,7 +536,7 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 		const int nt = min(TILE, e1 - t0);
 		__syncthreads();
 		for (int i = threadIdx.x; i < nt; i += blockDim.x) {
-			const unsigned f = P.eflag[t0 + i];
+			const unsigned f = ef[t0 + i];
 			sf[i] = f;
 			slp[i] = f ? a.plist[(size_t)li * P.NP + g.pbase + (t0 + i - e0)] : 0;
 		}
@@ -634,7 +646,8 @@ __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView 
 /// block per partition entry (bricks of thousands of leaves): every thread commits one leaf,
 /// and the rare layer changes are recorded in list order (status_round).
 template <int D, int L>
-__device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G)
+__device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G,
+                        unsigned* eflag)
 {
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
@@ -667,7 +680,7 @@ __device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b
 			status_store<L>(P, sl, k, b, sc);
 			flags = warp_or(flags);
 			if (threadIdx.x == 0) {
-				P.eflag[e] = flags;
+				eflag[e] = flags;
 				if (any) atomicOr(P.changed, 1);
 			}
 		}
@@ -677,14 +690,15 @@ template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist2(Dev P, const int* woff, ListView lv, int k, int b)
 {
 	pdl_enter();
-	d_dist2<D, L>(P, woff, lv, k, b, hw_grid());
+	d_dist2<D, L>(P, woff, lv, k, b, hw_grid(), P.eflag);
 }
 
 /// k_dist2 with one warp per partition entry (bricks of few leaves). The next chunk's list
 /// entry and delta are loaded before the current chunk's status records (which must stay in
 /// list order), so the two load latencies overlap the record work.
 template <int D, int L>
-__device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G)
+__device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, int b, GridPos G,
+                             unsigned* eflag)
 {
 	constexpr int NL = 2 * L + 1;
 	const int li = k + L;
@@ -723,7 +737,7 @@ __device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, 
 		status_store<L>(P, sl, k, b, sc);
 		flags = warp_or(flags);
 		if (lane == 0) {
-			P.eflag[e] = flags;
+			eflag[e] = flags;
 			if (any) atomicOr(P.changed, 1);
 		}
 	}
@@ -732,7 +746,149 @@ template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist2_warp(Dev P, const int* woff, ListView lv, int k, int b)
 {
 	pdl_enter();
-	d_dist2_warp<D, L>(P, woff, lv, k, b, hw_grid());
+	d_dist2_warp<D, L>(P, woff, lv, k, b, hw_grid(), P.eflag);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused distance passes. update_distance (Surface.hpp:989-1125) runs, per layer in the order
+// -1..-L, +1..+L, a first pass (the distance of every leaf of the layer's list into the delta
+// grid) and a second pass (the delta into the isogrid, status changes recorded). The first pass
+// of layer j only depends on the second pass of layer j-1 through the values it commits, and
+// those are the delta values the first pass of j-1 computed. So one launch runs the second pass
+// of layer j-1 and the first pass of layer j together, the latter reading the delta value of
+// every leaf the pass of j-1 processed (a leaf of that layer's list) and the isogrid elsewhere:
+// the same values the reference reads, 2L+1 launches per iteration instead of 4L. The two
+// passes touch different leaves (a leaf is in one list), and the compaction of the records of
+// layer j-2 rides in the same launch on entry flags of the other parity.
+// ---------------------------------------------------------------------------------------------
+
+/// The value the first pass of a layer reads at leaf `leaf` of brick sl when the second pass of
+/// the layer before (layer index lip, -1 = none) runs in the same launch: that pass's new value
+/// for a leaf in its list (lv's list lip of the brick, found through the lookup), else the
+/// isogrid value. The isogrid value is loaded alongside the lookup and discarded for a listed
+/// leaf (its commit may be in flight).
+template <int L>
+__device__ __forceinline__ float fused_value(const Dev& P, const ListView& lv, int lip, int sl,
+                                             int leaf)
+{
+	constexpr int NL = 2 * L + 1;
+	const size_t i = (size_t)sl * P.BV + leaf;
+	const float v = P.phi[i];
+	if (lip < 0) return v;
+	const int p = lv.lkp[i];
+	if (p == NUL16 || p >= lv.lcnt[sl * NL + lip]) return v;
+	if (lv.lst[((size_t)sl * NL + lip) * P.BV + p] != leaf) return v;
+	return P.dlt[i];
+}
+
+/// distance_leaf with every neighbour read through fused_value (same result as distance() on
+/// the values the reference's pass reads).
+template <int D, int L>
+__device__ __forceinline__ float distance_leaf_fused(const Dev& P, const SurfGeom& g,
+                                                     const ListView& lv, int lip, int gp, int sl,
+                                                     int leaf, float dist, float dir)
+{
+	dist = __fmul_rn(dist, dir);
+	int q[D];
+	Vec<D> pos;
+	int rem = leaf;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+		q[a] = rem / P.lstr[a];
+		rem -= q[a] * P.lstr[a];
+		pos[a] = P.porig[gp * 3 + a] + q[a];
+	}
+	Vec<D> n = pos;
+#pragma unroll
+	for (int a = 0; a < D; a++) {
+#pragma unroll
+		for (int s = -1; s <= 1; s += 2) {
+			n[a] = pos[a] + s;
+			if (in_grid<D>(g, n)) {
+				const int qa = q[a] + s;
+				float v;
+				if (qa >= 0 && qa < P.csz[a]) {
+					v = fused_value<L>(P, lv, lip, sl, leaf + s * P.lstr[a]);
+				} else {
+					int gp2, leaf2;
+					locate<D>(P, g, n, gp2, leaf2);
+					const int sl2 = P.slot[gp2];
+					v = sl2 < 0 ? P.bg[gp2] : fused_value<L>(P, lv, lip, sl2, leaf2);
+				}
+				const float dn = __fmul_rn(v, dir);
+				if (dn < dist) dist = dn;
+			}
+		}
+		n[a] = pos[a];
+	}
+	return __fadd_rn(__fmul_rn(dist, dir), dir);
+}
+
+/// One pass of the fused sequence: the layer, its entry offsets, nullptr = no such pass.
+struct FusedPass {
+	const int* woff;
+	int k;
+};
+
+/// Second pass of layer p2 (records into buffer b, entry flags into ef2) and first pass of
+/// layer p1 (side `side`, `split` warps per entry), after the compaction of the pass before p2
+/// in the first ca.nblocks blocks. With both passes, the even blocks after those run the
+/// second pass and the odd ones the first, so that their chains of dependent loads overlap
+/// instead of following each other on the same warps.
+template <int D, int L>
+__global__ void __launch_bounds__(256) k_dist_fused(Dev P, ListView lv, FusedPass p2, FusedPass p1,
+                                                    float side, int split, int b, unsigned* ef2,
+                                                    CompactArgs ca, int block_passes)
+{
+	constexpr int NL = 2 * L + 1;
+	pdl_enter();
+	if ((int)blockIdx.x < ca.nblocks) {
+		compact_surface<L>(P, ca, blockIdx.x);
+		return;
+	}
+	GridPos G{(int)blockIdx.x - ca.nblocks, (int)gridDim.x - ca.nblocks};
+	// the layer the first pass reads new values of: the second pass's, in this launch
+	const int lip = p2.woff ? p2.k + L : -1;
+	const bool both = p2.woff && p1.woff;
+	if (both) {
+		const bool second = (G.bid & 1) == 0;
+		G = GridPos{G.bid >> 1, second ? (G.nb + 1) >> 1 : G.nb >> 1};
+		if (!second) p2.woff = nullptr;
+	}
+	if (p2.woff) {
+		if (block_passes)
+			d_dist2<D, L>(P, p2.woff, lv, p2.k, b, G, ef2);
+		else
+			d_dist2_warp<D, L>(P, p2.woff, lv, p2.k, b, G, ef2);
+		return;
+	}
+	if (!p1.woff) return;
+	const int li = p1.k + L;
+	const int lane = lane_id();
+	const int nwarps = (G.nb * blockDim.x) >> 5;
+	const int total = p1.woff[P.S] * split;
+	for (int v = (G.bid * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
+		const int e = v / split, part = v - e * split;
+		const int s = entry_surface(p1.woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - p1.woff[s])];
+		const int sl = P.slot[gp];
+		const int n = lv.lcnt[sl * NL + li];
+		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
+		const size_t b0 = (size_t)sl * P.BV;
+		const int STRIDE = 32 * split;
+		for (int j = part * 32 + lane; j < n; j += 2 * STRIDE) {
+			const bool two = j + STRIDE < n;
+			const int l1 = lst[j];
+			const int l2 = two ? lst[j + STRIDE] : l1;
+			const float q1 = P.phi[b0 + l1], q2 = P.phi[b0 + l2];
+			const float d1 = distance_leaf_fused<D, L>(P, g, lv, lip, gp, sl, l1, q1, side);
+			const float d2 = distance_leaf_fused<D, L>(P, g, lv, lip, gp, sl, l2, q2, side);
+			P.dlt[b0 + l1] = d1;
+			if (two) P.dlt[b0 + l2] = d2;
+		}
+		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
+	}
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1061,29 +1217,25 @@ __global__ void __launch_bounds__(128) k_flush_smem(Dev P)
 	d_flush_smem<D, L>(P, hw_grid(), fsm);
 }
 
-/// Children-level half of the flush: one block per (surface, list k) replays, in the
-/// reference's order (from-layer ascending, then status partition list order), the appends to
-/// list k and the swap-with-last removals from it (LookupMixin.hpp:483-556). The events only
-/// read the leaf flush's records (app, rem), which this kernel does not change: the block loads
-/// a tile of them into shared memory at once, then one warp replays the (rare) events in order.
-template <int L>
-__device__ void d_flush_plist(const Dev& P, GridPos G)
+/// Children-level half of the flush, for list k of surface s: replays, in the reference's order
+/// (from-layer ascending, then status partition list order), the appends to list k and the
+/// swap-with-last removals from it (LookupMixin.hpp:483-556). The events only read the leaf
+/// flush's records (app, rem), which this kernel does not change. This is the general path:
+/// tiles of the status lists staged in shared memory, events replayed by one lane on the
+/// global lists (used when a list has more events than flush_plist_fast stages).
+template <int L, int ECAP>
+__device__ void flush_plist_serial(const Dev& P, int s, int k, int* slp, unsigned char* sev)
 {
 	constexpr int NL = 2 * L + 1;
-	constexpr int TILE = 2048;
-	__shared__ int slp[TILE];
-	__shared__ unsigned char sev[TILE];  // 1 append, 2 removal
-	for (int w = G.bid; w < P.S * NL; w += G.nb) {
 	const int lane = lane_id();
-	const int s = w / NL, k = w % NL;
 	const SurfGeom& g = P.geom[s];
 	int* pl = P.plist + (size_t)k * P.NP + g.pbase;
 	int cnt = P.pcnt[s * NL + k];  // kept by warp 0
 	for (int fi = 0; fi < NL; fi++) {
 		const int ns = P.spcnt[s * NL + fi];
 		const int* sp = P.splist + (size_t)fi * P.NP + g.pbase;
-		for (int t0 = 0; t0 < ns; t0 += TILE) {
-			const int nt = min(TILE, ns - t0);
+		for (int t0 = 0; t0 < ns; t0 += ECAP) {
+			const int nt = min(ECAP, ns - t0);
 			__syncthreads();
 			for (int i = threadIdx.x; i < nt; i += blockDim.x) {
 				const int lp = sp[t0 + i];
@@ -1134,6 +1286,186 @@ __device__ void d_flush_plist(const Dev& P, GridPos G)
 	}
 	if (threadIdx.x == 0) P.pcnt[s * NL + k] = cnt;
 	__syncthreads();
+}
+
+/// Open-addressing map in shared memory from a partition's local index to its position in the
+/// list being replayed (-1: not in it); keys -1 = empty slot. Returns the key's slot, or the
+/// empty slot that ends its probe when it is absent (the map is never full).
+template <int HCAP>
+__device__ __forceinline__ int plist_slot(const int* hkey, int lp)
+{
+	int h = (int)(((unsigned)lp * 2654435761u) >> 20) & (HCAP - 1);
+	while (hkey[h] != lp && hkey[h] != -1) h = (h + 1) & (HCAP - 1);
+	return h;
+}
+
+/// flush_plist_serial with every event's lookups in shared memory. A list of length n that
+/// loses at most R entries only ever moves entries from positions >= n - R (each swap-with-last
+/// removal takes the current last entry, and the list is longer than n - R before each of its
+/// removals), so only that window and the appended entries are staged; entries below it are
+/// overwritten at most, never read. The positions of the window's and the events' partitions
+/// live in a map in shared memory while one lane replays the events in order; the window and
+/// the positions are written back after. Returns false, having changed nothing, when the list
+/// has more than ECAP events (flush_plist_serial replays it then).
+template <int L, int ECAP, int HCAP>
+__device__ bool flush_plist_fast(const Dev& P, int s, int k, int* ev_lp, unsigned char* ev_kind,
+                                 int* wnd, int* hkey, int* hval)
+{
+	constexpr int NL = 2 * L + 1;
+	constexpr int PER = 8;  // status entries per thread per round, loaded together
+	__shared__ int fo[NL + 1], nev_s, nrem_s;
+	const SurfGeom& g = P.geom[s];
+	int* pl = P.plist + (size_t)k * P.NP + g.pbase;
+	const int cnt0 = P.pcnt[s * NL + k];
+	if (threadIdx.x == 0) {
+		int c = 0;
+		for (int fi = 0; fi < NL; fi++) {
+			fo[fi] = c;
+			c += P.spcnt[s * NL + fi];
+		}
+		fo[NL] = c;
+		nev_s = 0;
+		nrem_s = 0;
+	}
+	for (int h = threadIdx.x; h < HCAP; h += blockDim.x) hkey[h] = -1;
+	__syncthreads();
+	// 1. the events in replay order: the status lists concatenated in from-layer order
+	const int T = fo[NL];
+	for (int base = 0; base < T; base += blockDim.x * PER) {
+		int lp[PER];
+		unsigned char ev[PER];
+		int c = 0;
+#pragma unroll
+		for (int q = 0; q < PER; q++) {
+			const int t = base + threadIdx.x * PER + q;
+			ev[q] = 0;
+			lp[q] = 0;
+			if (t < T) {
+				int fi = 0;
+				while (t >= fo[fi + 1]) fi++;
+				lp[q] = P.splist[(size_t)fi * P.NP + g.pbase + (t - fo[fi])];
+				const int gp = g.pbase + lp[q];
+				if (fi == k)
+					ev[q] = ((P.rem[gp] >> k) & 1u) ? 2 : 0;
+				else
+					ev[q] = ((P.app[gp * NL + fi] >> k) & 1u) ? 1 : 0;
+				c += ev[q] != 0;
+			}
+		}
+		int tot;
+		const int off = nev_s + block_excl_scan(c, &tot);
+		int r = 0;
+#pragma unroll
+		for (int q = 0; q < PER; q++)
+			if (ev[q]) {
+				if (off + r < ECAP) {
+					ev_lp[off + r] = lp[q];
+					ev_kind[off + r] = ev[q];
+				}
+				r++;
+				if (ev[q] == 2) atomicAdd(&nrem_s, 1);
+			}
+		__syncthreads();
+		if (threadIdx.x == 0) nev_s += tot;
+		__syncthreads();
+	}
+	const int nev = nev_s;
+	if (nev > ECAP) return false;
+	if (nev == 0) return true;
+	// 2. the removal window and the positions of its and the events' partitions
+	const int w0 = max(0, cnt0 - nrem_s);
+	for (int i = threadIdx.x; i < cnt0 - w0; i += blockDim.x) {
+		const int lp = pl[w0 + i];
+		wnd[i] = lp;
+		int h = (int)(((unsigned)lp * 2654435761u) >> 20) & (HCAP - 1);
+		while (true) {
+			const int prev = atomicCAS(&hkey[h], -1, lp);
+			if (prev == -1) {
+				hval[h] = w0 + i;
+				break;
+			}
+			if (prev == lp) break;
+			h = (h + 1) & (HCAP - 1);
+		}
+	}
+	__syncthreads();
+	for (int j = threadIdx.x; j < nev; j += blockDim.x) {
+		const int lp = ev_lp[j];
+		int h = (int)(((unsigned)lp * 2654435761u) >> 20) & (HCAP - 1);
+		while (true) {
+			const int prev = atomicCAS(&hkey[h], -1, lp);
+			if (prev == -1) {
+				hval[h] = P.ppos[(g.pbase + lp) * NL + k];
+				break;
+			}
+			if (prev == lp) break;  // a window entry, or another event of the same partition
+			h = (h + 1) & (HCAP - 1);
+		}
+	}
+	__syncthreads();
+	// 3. the replay, in order, on one lane
+	if (threadIdx.x == 0) {
+		int len = cnt0;
+		for (int j = 0; j < nev; j++) {
+			const int lp = ev_lp[j];
+			const int h = plist_slot<HCAP>(hkey, lp);
+			if (hkey[h] != lp) {  // every event's partition was entered above
+				atomicOr(P.err, EB_CAPACITY);
+				continue;
+			}
+			const int pos = hval[h];
+			if (ev_kind[j] == 1) {
+				if (pos < 0) {
+					wnd[len - w0] = lp;
+					hval[h] = len;
+					len++;
+				}
+			} else if (pos >= 0) {
+				const int last = len - 1;
+				if (pos < last) {
+					const int mv = wnd[last - w0];
+					if (pos >= w0)
+						wnd[pos - w0] = mv;
+					else
+						pl[pos] = mv;
+					const int hm = plist_slot<HCAP>(hkey, mv);
+					if (hkey[hm] == mv)  // window and appended entries are all in the map
+						hval[hm] = pos;
+					else
+						atomicOr(P.err, EB_CAPACITY);
+				}
+				hval[h] = -1;
+				len = last;
+			}
+		}
+		nev_s = len;
+	}
+	__syncthreads();
+	// 4. the window back, and the positions of every partition the replay saw
+	const int len = nev_s;
+	for (int i = threadIdx.x; i < len - w0; i += blockDim.x) pl[w0 + i] = wnd[i];
+	for (int h = threadIdx.x; h < HCAP; h += blockDim.x)
+		if (hkey[h] >= 0) P.ppos[(g.pbase + hkey[h]) * NL + k] = hval[h];
+	if (threadIdx.x == 0) P.pcnt[s * NL + k] = len;
+	__syncthreads();
+	return true;
+}
+
+/// Children-level half of the flush: one block per (surface, list k).
+template <int L>
+__device__ void d_flush_plist(const Dev& P, GridPos G)
+{
+	constexpr int NL = 2 * L + 1;
+	constexpr int ECAP = 1024, HCAP = 4096;
+	__shared__ int ev_lp[ECAP];
+	__shared__ unsigned char ev_kind[ECAP];
+	__shared__ int wnd[ECAP];
+	__shared__ int hkey[HCAP];
+	__shared__ int hval[HCAP];
+	for (int w = G.bid; w < P.S * NL; w += G.nb) {
+		const int s = w / NL, k = w % NL;
+		if (!flush_plist_fast<L, ECAP, HCAP>(P, s, k, ev_lp, ev_kind, wnd, hkey, hval))
+			flush_plist_serial<L, ECAP>(P, s, k, ev_lp, ev_kind);
 	}
 }
 template <int L>

@@ -102,7 +102,7 @@ double time_candidate(int D, int L, const int* part, int ds, int rp)
 	double ms = 0;
 	try {
 		std::unique_ptr<EngineBase> eng(make_engine(d, st));
-		eng->set_tuning(0, ds, rp);
+		eng->set_tuning(0, ds, rp, 0, 0);
 		const int centre[3] = {0, 0, 0};
 		eng->seed(0, centre);
 		const Speed grow{1, -1.0f, 0.0f, 0.0f, 0u};

@@ -77,7 +77,13 @@ typedef struct fg_config {
 	int autotune;          /* 1: dist_split and record_passes left at 0 take the values
 	                          fg_autotune finds for this D, L, partition and device (timed
 	                          once per process, or read from the file FELT_TUNE_CACHE names) */
-	int reserved[4];
+	int delta_kernel;      /* the speed functor of curvature speeds: 1 warps reading the pool,
+	                          2 one block per brick staged with its halo in shared memory;
+	                          0 = automatic                                                  */
+	int fuse_passes;       /* the global update's 2L distance-pass pairs: 1 as 4L launches,
+	                          2 as 2L+1 launches (each the second pass of one layer with the
+	                          first pass of the next); 0 = automatic                         */
+	int reserved[2];
 } fg_config;
 
 typedef struct fg_surface fg_surface;
@@ -409,8 +415,9 @@ FG_API int fg_brick_bytes(int dims, int layers, const int* part, double* bytes);
 FG_API int fg_autotune_candidates(int dims, const int* part, int* pairs, size_t cap, size_t* n);
 FG_API int fg_autotune(int dims, int layers, const int* part, int force, fg_config* cfg,
                        double* ms, size_t ms_cap, size_t* n);
-/* The launch tuning in effect on a surface or batch: out[0] launch mode (1 one graph, 2 phase
- * by phase), out[1] dist_split, out[2] record_passes, out[3] 0. */
+/* The launch tuning in effect on a surface or batch (5 values): out[0] launch mode (1 one graph,
+ * 2 phase by phase), out[1] dist_split, out[2] record_passes, out[3] delta kernel (1 direct,
+ * 2 staged), out[4] distance passes (1 separate, 2 fused). */
 FG_API int fg_surface_tuning(fg_surface* s, int* out);
 FG_API int fg_batch_tuning(fg_batch* b, int* out);
 

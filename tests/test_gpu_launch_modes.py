@@ -113,7 +113,9 @@ def test_step_graph_between_local_updates():
 
 
 @pytest.mark.parametrize("tuning", [dict(dist_split=1), dict(dist_split=8),
-                                    dict(record_passes=1), dict(record_passes=2)],
+                                    dict(record_passes=1), dict(record_passes=2),
+                                    dict(delta_kernel=1), dict(delta_kernel=2),
+                                    dict(fuse_passes=1), dict(fuse_passes=2)],
                          ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
 def test_tuning_knobs_keep_results(tuning):
     size, part, L, seed, sched = CASES[1]
