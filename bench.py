@@ -262,7 +262,8 @@ class BatchWork:
     def __init__(self, fb, cfg, name, shard=0):
         self.fb, self.cfg = fb, cfg
         sizes, centres, speeds = batch_surfaces(name, cfg, shard)
-        self.b = fb.Batch(sizes, cfg["part"], cfg["L"], **TUNING)
+        # threads per brick from the launch-shape tuner (fg_autotune), as the batched configs ask
+        self.b = fb.Batch(sizes, cfg["part"], cfg["L"], **{**TUNING, "autotune": True})
         self.b.seed(centres)
         self.speeds = self.b.speed_array(speeds)  # converted once; the speeds are fixed
         # a full polygonisation at setup, so that its buffers exist before timing
@@ -312,7 +313,7 @@ class PlainSubset:
         self.items = []
         self.done = 0
         for sz, c, sp in list(zip(sizes, centres, speeds))[:k]:
-            s = fb.Surface(sz, cfg["part"], cfg["L"], **TUNING)
+            s = fb.Surface(sz, cfg["part"], cfg["L"], **{**TUNING, "autotune": True})
             s.seed(c)
             self.items.append((s, fb.Polys(s), sp))
 
@@ -379,6 +380,7 @@ def measure_batched(fb, name, steps, warm):
         wall += time.perf_counter() - t0
         dev_ms += a.elapsed_time(b)
     nu = work.node_updates() - nu0
+    tuning = work.tuning()
     work.close()
     k = cfg["plain_subset"]
     plain = PlainSubset(fb, cfg, name, k)
@@ -403,6 +405,7 @@ def measure_batched(fb, name, steps, warm):
                       "wall_per_s": p_wall, "ms_per_step": pdev_ms / steps},
             "batched_over_plain_device": b_dev / p_dev,
             "batched_over_plain_wall": b_wall / p_wall,
+            "tuning": tuning,
             "how": "node-updates/s of the same steps; batched: all surfaces in one batch; plain: "
                    "the first surfaces as separate Surfaces one after another (every update its "
                    "own launch sequence); device = CUDA events on the launching streams, wall = "

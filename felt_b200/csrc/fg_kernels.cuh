@@ -307,38 +307,66 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 }
 
 /// Fills box with the isogrid over a partition and a one-node halo ((part+2)^D values, row-major,
-/// last axis fastest): interior nodes straight from the brick, halo nodes through the pool
-/// (neighbour bricks, inactive-partition backgrounds, the grid background outside the grid).
+/// last axis fastest). The brick slots (or backgrounds) of the 3^D partitions around it are
+/// looked up once, so every value is a single independent load: interior nodes from the brick,
+/// halo nodes from the neighbour partition's brick or its background (an inactive partition),
+/// the grid background L+1 outside the grid; the values get_phi reads at those positions.
 template <int D, int L>
 __device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, float* box)
 {
+	constexpr int ND = D == 3 ? 27 : 9;
+	__shared__ int nsl[27];    // slot of the partition in each direction (-1 inactive)
+	__shared__ float nbg[27];  // its background
 	int ext[D], vol = 1;
 #pragma unroll
 	for (int a = 0; a < D; a++) {
 		ext[a] = P.csz[a] + 2;
 		vol *= ext[a];
 	}
-	const float* brick = P.phi + (size_t)sl * P.BV;
+	if (threadIdx.x < ND) {
+		// a node of the neighbour partition: one outside the brick on the axes the direction
+		// leaves it, the brick's first node elsewhere
+		int r = threadIdx.x;
+		Vec<D> p;
+		for (int a = D - 1; a >= 0; a--) {
+			const int d = r % 3 - 1;
+			r /= 3;
+			p[a] = P.porig[gp * 3 + a] + (d < 0 ? -1 : d > 0 ? P.csz[a] : 0);
+		}
+		int s2 = -1;
+		float b2 = (float)(L + 1);
+		if (in_grid<D>(g, p)) {
+			int gp2, leaf2;
+			locate<D>(P, g, p, gp2, leaf2);
+			s2 = P.slot[gp2];
+			b2 = P.bg[gp2];
+		}
+		nsl[threadIdx.x] = s2;
+		nbg[threadIdx.x] = b2;
+	}
+	__syncthreads();
 	for (int i = threadIdx.x; i < vol; i += blockDim.x) {
-		int r = i, leaf = 0;
-		bool interior = true;
-		Vec<D> c;
+		int r = i, dir = 0, mul = 1, leaf = 0;
+		bool ing = true;
 #pragma unroll
 		for (int a = D - 1; a >= 0; a--) {
-			c[a] = r % ext[a] - 1;
+			const int c = r % ext[a] - 1;
 			r /= ext[a];
-			if (c[a] < 0 || c[a] >= P.csz[a]) interior = false;
-			leaf += c[a] * P.lstr[a];
+			const int cs = P.csz[a];
+			dir += (c < 0 ? 0 : c >= cs ? 2 : 1) * mul;
+			mul *= 3;
+			leaf += (c < 0 ? cs - 1 : c >= cs ? 0 : c) * P.lstr[a];
+			const int pa = P.porig[gp * 3 + a] + c;
+			ing = ing && pa >= g.off[a] && pa < g.hi[a];
 		}
-		if (interior) {
-			box[i] = brick[leaf];
-		} else {
-			Vec<D> p;
-#pragma unroll
-			for (int a = 0; a < D; a++) p[a] = P.porig[gp * 3 + a] + c[a];
-			box[i] = get_phi<D, L>(P, g, p);
+		float v = (float)(L + 1);
+		if (ing) {
+			const int s2 = nsl[dir];
+			v = s2 >= 0 ? P.phi[(size_t)s2 * P.BV + leaf] : nbg[dir];
 		}
+		box[i] = v;
 	}
+	(void)sl;
 }
 
 /// Reads a staged box (stage_halo) by world position.

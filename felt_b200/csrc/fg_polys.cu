@@ -357,6 +357,8 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 	uint16_t* cleaf = cnew + P.BV;                              // [BV]
 	__shared__ int lstart[NL + 1];
 	__shared__ int tot_v, tot_s, vb, sb, ok;
+	__shared__ int msl[8];    // slots of the partition and its upper neighbours (-1 inactive)
+	__shared__ float mbg[8];  // their backgrounds
 	const int nent = single >= 0 ? 1 : woff[P.S];
 	for (int e = blockIdx.x; e < nent; e += gridDim.x) {
 		int gp;
@@ -388,22 +390,44 @@ __global__ void __launch_bounds__(256) k_polys_march(Dev P, PolysDev Q, const in
 		}
 		Vec<D> bo;  // world position of box index 0
 		for (int a = 0; a < D; a++) bo[a] = P.porig[gp * 3 + a];
-		const float* brick = P.phi + (size_t)sl * P.BV;
+		// the slots (or backgrounds) of the partition and of its upper neighbours, looked up
+		// once: every staged value is then one independent load, the value get_phi reads there
+		if (threadIdx.x < (1 << D)) {
+			Vec<D> p;
+			for (int a = 0; a < D; a++)
+				p[a] = bo[a] + (((threadIdx.x >> (D - 1 - a)) & 1) ? P.csz[a] : 0);
+			int s2 = -1;
+			float b2 = (float)(L + 1);
+			if (in_grid<D>(g, p)) {
+				int gp2, leaf2;
+				locate<D>(P, g, p, gp2, leaf2);
+				s2 = P.slot[gp2];
+				b2 = P.bg[gp2];
+			}
+			msl[threadIdx.x] = s2;
+			mbg[threadIdx.x] = b2;
+		}
+		__syncthreads();
 		for (int i = threadIdx.x; i < bvol; i += blockDim.x) {
 			first[i * D] = 0x7fffffff;
 			for (int a = 1; a < D; a++) first[i * D + a] = 0x7fffffff;
-			int r = i, leaf = 0;
-			bool own = true;
-			Vec<D> p;
+			int r = i, leaf = 0, dir = 0;
+			bool ing = true;
 			for (int a = D - 1; a >= 0; a--) {
 				const int c = r % bext[a];
 				r /= bext[a];
-				p[a] = bo[a] + c;
-				const int lc = p[a] - P.porig[gp * 3 + a];
-				own = own && lc < P.csz[a] && p[a] < g.hi[a];
-				leaf += lc * P.lstr[a];
+				const int pa = bo[a] + c;
+				const bool up = c >= P.csz[a];
+				dir |= (up ? 1 : 0) << (D - 1 - a);
+				leaf += (up ? 0 : c) * P.lstr[a];
+				ing = ing && pa < g.hi[a];  // pa >= off: the partition starts inside the grid
 			}
-			box[i] = own ? brick[leaf] : get_phi<D, L>(P, g, p);
+			float v = (float)(L + 1);
+			if (ing) {
+				const int s2 = msl[dir];
+				v = s2 >= 0 ? P.phi[(size_t)s2 * P.BV + leaf] : mbg[dir];
+			}
+			box[i] = v;
 		}
 		__syncthreads();
 		const int n = lstart[NL];
