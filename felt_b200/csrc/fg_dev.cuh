@@ -112,6 +112,7 @@ struct Dev {
 	int* papn;        // [S]
 	int* woff;        // [S+1] entry offsets of the current pass
 	int* woffl;       // [NL*(S+1)] entry offsets of every layer's list, for the distance passes
+	int4* etab;       // [NL*NP] the distance passes' entries decoded (k_entry_table)
 	int* sfrozen;     // [S] surfaces stopped after a non-terminating update (no further work)
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes
@@ -373,9 +374,25 @@ __device__ __forceinline__ float distance(const Dev& P, const SurfGeom& g, const
 	return __fadd_rn(__fmul_rn(dist, dir), dir);
 }
 
+/// The partition next to gp along axis a (s = -1 or +1) and the leaf of it next to `leaf`, for
+/// a neighbour that lies in the grid: the children grid is row-major with the last axis
+/// fastest, so the partition index moves by the product of the later axes' counts, and the
+/// leaf coordinate wraps to the neighbour's far face. No division (get_phi's locate).
+template <int D>
+__device__ __forceinline__ void next_partition(const Dev& P, const SurfGeom& g, int gp, int leaf,
+                                               int a, int s, int& gp2, int& leaf2)
+{
+	int cst = 1;
+#pragma unroll
+	for (int b = D - 1; b > a; b--) cst *= g.ccount[b];
+	gp2 = gp + s * cst;
+	leaf2 = leaf + (s < 0 ? P.csz[a] - 1 : 1 - P.csz[a]) * P.lstr[a];
+}
+
 /// distance() for leaf `leaf` of partition gp (brick slot sl): neighbours inside the same
-/// partition are read straight from the brick (no partition lookup); the others through
-/// get_phi. Same result as distance() at the leaf's position.
+/// partition are read straight from the brick; the others from the next partition along the
+/// axis (next_partition), its brick or its background. Same result as distance() at the
+/// leaf's position (get_phi there).
 template <int D, int L>
 __device__ __forceinline__ float distance_leaf(const Dev& P, const SurfGeom& g, int gp, int sl,
                                                int leaf, float dist, float dir)
@@ -399,8 +416,15 @@ __device__ __forceinline__ float distance_leaf(const Dev& P, const SurfGeom& g, 
 			n[a] = pos[a] + s;
 			if (in_grid<D>(g, n)) {
 				const int qa = q[a] + s;
-				const float v = (qa >= 0 && qa < P.csz[a]) ? brick[leaf + s * P.lstr[a]]
-				                                           : get_phi<D, L>(P, g, n);
+				float v;
+				if (qa >= 0 && qa < P.csz[a]) {
+					v = brick[leaf + s * P.lstr[a]];
+				} else {
+					int gp2, leaf2;
+					next_partition<D>(P, g, gp, leaf, a, s, gp2, leaf2);
+					const int sl2 = P.slot[gp2];
+					v = sl2 < 0 ? P.bg[gp2] : P.phi[(size_t)sl2 * P.BV + leaf2];
+				}
 				const float dn = __fmul_rn(v, dir);
 				if (dn < dist) dist = dn;
 			}

@@ -232,6 +232,7 @@ public:
 		P.papn = dalloc<int>(S, o);
 		P.woff = dalloc<int>(S + 1, o);
 		P.woffl = dalloc<int>((size_t)NL * (S + 1), o);
+		P.etab = dalloc<int4>((size_t)NL * NP, o);
 		P.sfrozen = dalloc<int>(S, o);
 		FG_CUDA(cudaMemsetAsync(P.sfrozen, 0, S * sizeof(int), st_));
 		frozen_.assign(S, 0);
@@ -1323,6 +1324,7 @@ private:
 	void distance_passes(const ListView& lv, int b)
 	{
 		FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
+		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L););
 		if (fused_ && lv.lkp) {
 			fused_passes(lv, b);
 			return;
@@ -1398,7 +1400,7 @@ private:
 	void flush()
 	{
 		if (smem_flush_)
-			FG_RUN("k_flush_smem", st_, launch_pdl((k_flush_smem<D, L>), sm_count() * 8, 128, smem_flush_, st_, P_););
+			FG_RUN("k_flush_smem", st_, launch_pdl((k_flush_smem<D, L>), sm_count() * 8, 256, smem_flush_, st_, P_););
 		else
 			FG_RUN("k_flush_leaf", st_, launch_pdl((k_flush_leaf<D, L>), grid_for(P_.NP), 128, 0, st_, P_););
 		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 256, 0, st_, P_););

@@ -124,6 +124,37 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 	d_scan_layers(cnt, NL, S, woffl, frozen);
 }
 
+/// The entries of the distance passes decoded once per iteration: for every layer but the zero
+/// layer and every entry e of its list (entry offsets woffl), {partition, brick slot, surface,
+/// leaves in the brick's list} at etab[l*NP + e]. The passes then start from one 16-byte load
+/// instead of the chain entry offsets -> partition list -> slot -> list count.
+static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, int NL, int L)
+{
+	__shared__ int lo[10];  // the layers' entries concatenated: layer l from lo[l]
+	pdl_enter();
+	if (threadIdx.x == 0) {
+		int c = 0;
+		for (int l = 0; l < NL; l++) {
+			lo[l] = c;
+			if (l != L) c += P.woffl[(size_t)l * (P.S + 1) + P.S];
+		}
+		lo[NL] = c;
+	}
+	__syncthreads();
+	const int total = lo[NL];
+	for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+		int l = 0;
+		while (t >= lo[l + 1]) l++;
+		const int e = t - lo[l];
+		const int* woff = P.woffl + (size_t)l * (P.S + 1);
+		const int s = entry_surface(woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const int gp = g.pbase + plist[(size_t)l * P.NP + g.pbase + (e - woff[s])];
+		const int sl = P.slot[gp];
+		P.etab[(size_t)l * P.NP + e] = make_int4(gp, sl, s, lcnt[sl * NL + l]);
+	}
+}
+
 /// The block index and block count a kernel body works with (the hardware grid's, or another
 /// grid dimension's where the launch is two-dimensional).
 struct GridPos {
@@ -636,11 +667,9 @@ __device__ void d_dist1_work(const Dev& P, const int* woff, ListView lv, int k, 
 	const int total = woff[P.S] * split;
 	for (int v = first_warp; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
-		const int s = entry_surface(woff, P.S, e);
-		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
-		const int sl = P.slot[gp];
-		const int n = lv.lcnt[sl * NL + li];
+		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
+		const SurfGeom& g = P.geom[et.z];
+		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
 		const int STRIDE = 32 * split;
@@ -683,11 +712,9 @@ __device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b
 	__shared__ int ct[256];
 	const int total = woff[P.S];
 	for (int e = G.bid; e < total; e += G.nb) {
-		const int s = entry_surface(woff, P.S, e);
-		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
-		const int sl = P.slot[gp];
-		const int n = lv.lcnt[sl * NL + li];
+		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
+		const SurfGeom& g = P.geom[et.z];
+		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
@@ -732,11 +759,9 @@ __device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, 
 	const int li = k + L;
 	FG_WARP_LOOP(woff)
 	{
-		const int s = entry_surface(woff, P.S, e);
-		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - woff[s])];
-		const int sl = P.slot[gp];
-		const int n = lv.lcnt[sl * NL + li];
+		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
+		const SurfGeom& g = P.geom[et.z];
+		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
 		unsigned flags = 0;
@@ -839,7 +864,7 @@ __device__ __forceinline__ float distance_leaf_fused(const Dev& P, const SurfGeo
 					v = fused_value<L>(P, lv, lip, sl, leaf + s * P.lstr[a]);
 				} else {
 					int gp2, leaf2;
-					locate<D>(P, g, n, gp2, leaf2);
+					next_partition<D>(P, g, gp, leaf, a, s, gp2, leaf2);
 					const int sl2 = P.slot[gp2];
 					v = sl2 < 0 ? P.bg[gp2] : fused_value<L>(P, lv, lip, sl2, leaf2);
 				}
@@ -897,11 +922,9 @@ __global__ void __launch_bounds__(256) k_dist_fused(Dev P, ListView lv, FusedPas
 	const int total = p1.woff[P.S] * split;
 	for (int v = (G.bid * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
-		const int s = entry_surface(p1.woff, P.S, e);
-		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + lv.plist[(size_t)li * P.NP + g.pbase + (e - p1.woff[s])];
-		const int sl = P.slot[gp];
-		const int n = lv.lcnt[sl * NL + li];
+		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
+		const SurfGeom& g = P.geom[et.z];
+		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
 		const int STRIDE = 32 * split;
@@ -1238,7 +1261,7 @@ __device__ void d_flush_smem(const Dev& P, GridPos G, unsigned char* fsm)
 	}
 }
 template <int D, int L>
-__global__ void __launch_bounds__(128) k_flush_smem(Dev P)
+__global__ void __launch_bounds__(256) k_flush_smem(Dev P)
 {
 	pdl_enter();
 	extern __shared__ __align__(16) unsigned char fsm[];
@@ -1559,33 +1582,67 @@ __device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 		const int want = L * side - side;
 		const int nc = P.ccnt[sl * NL + fi];
 		const uint16_t* ch = P.chg + ((size_t)sl * NL + fi) * P.BV;
-		for (int c = lane; c < nc; c += 32) {
-			const int leaf = ch[c];
-			if (P.sto[(size_t)sl * P.BV + leaf] != want) continue;
-			const Vec<D> pos = leaf_pos<D>(P, gp, leaf);
+		const unsigned lt = (1u << lane) - 1u;
+		// whole-warp rounds, so that the candidate slots are taken with one atomic per warp
+		for (int c0 = 0; c0 < nc; c0 += 32) {
+			const int c = c0 + lane;
+			const int leaf = c < nc ? ch[c] : 0;
+			const bool src = c < nc && P.sto[(size_t)sl * P.BV + leaf] == want;
+			int qd[D];
+			Vec<D> pos;
+			{
+				int rem = leaf;
+#pragma unroll
+				for (int a = 0; a < D; a++) {
+					qd[a] = rem / P.lstr[a];
+					rem -= qd[a] * P.lstr[a];
+					pos[a] = P.porig[gp * 3 + a] + qd[a];
+				}
+			}
 #pragma unroll
 			for (int nb = 0; nb < 2 * D; nb++) {
+				const int ax = nb >> 1, sg = (nb & 1) ? 1 : -1;
 				Vec<D> q = pos;
-				q[nb >> 1] += (nb & 1) ? 1 : -1;
-				if (!in_grid<D>(g, q)) continue;
-				const float v = get_phi<D, L>(P, g, q);
-				if (inside_band(layer_id(v, P.err), L)) continue;
-				int gpn, leafn;
-				locate<D>(P, g, q, gpn, leafn);
+				q[ax] += sg;
+				bool cand = false;
+				int gpn = 0, leafn = 0;
+				float v = 0.0f;
+				if (src && in_grid<D>(g, q)) {
+					// the neighbour in this partition or the next one along the axis; the value
+					// get_phi reads there
+					const int qa = qd[ax] + sg;
+					if (qa >= 0 && qa < P.csz[ax]) {
+						gpn = gp;
+						leafn = leaf + sg * P.lstr[ax];
+					} else {
+						next_partition<D>(P, g, gp, leaf, ax, sg, gpn, leafn);
+					}
+					const int sv = P.slot[gpn];
+					v = sv < 0 ? P.bg[gpn] : P.phi[(size_t)sv * P.BV + leafn];
+					cand = !inside_band(layer_id(v, P.err), L);
+				}
 				// key: phase (1 bit) | rank (24) | position in status list (16) | neighbour (3)
 				const unsigned long long key = ((unsigned long long)phase << 43) |
 				                               ((unsigned long long)rank << 19) |
 				                               ((unsigned long long)c << 3) | (unsigned long long)nb;
 				if (mode == 0) {
-					if (P.slot[gpn] < 0 && atomicExch(&P.actflag[gpn], 1) == 0)
-						P.q_act[atomicAdd(&P.counters[CNT_ACT], 1)] = gpn;
-					const int ci = atomicAdd(&P.counters[CNT_CAND], 1);
-					if (ci < P.cand_cap) {
-						P.cand_key[ci] = key;
-						P.cand_gp[ci] = gpn;
-						P.cand_leaf[ci] = leafn;
+					const unsigned m = __ballot_sync(FULL, cand);
+					if (!m) continue;
+					const int ldr = __ffs(m) - 1;
+					int base = 0;
+					if (lane == ldr) base = atomicAdd(&P.counters[CNT_CAND], __popc(m));
+					base = __shfl_sync(FULL, base, ldr);
+					if (cand) {
+						if (P.slot[gpn] < 0 && atomicExch(&P.actflag[gpn], 1) == 0)
+							P.q_act[atomicAdd(&P.counters[CNT_ACT], 1)] = gpn;
+						const int ci = base + __popc(m & lt);
+						if (ci < P.cand_cap) {
+							P.cand_key[ci] = key;
+							P.cand_gp[ci] = gpn;
+							P.cand_leaf[ci] = leafn;
+						}
 					}
-				} else {
+				} else if (cand) {
 					const int sn = P.slot[gpn];
 					if (sn < 0) {
 						atomicOr(P.err, EB_POOL);
