@@ -25,6 +25,55 @@ __device__ __forceinline__ void pdl_enter()
 }
 constexpr unsigned long long NOCLAIM = ~0ull;
 
+// -------------------------------------------------------------------------------------------
+// Bulk copies global -> shared memory through the tensor memory accelerator (untiled
+// cp.async.bulk, no multicast), completed on a shared-memory mbarrier. Every wait is bounded.
+// -------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+	return (unsigned)__cvta_generic_to_shared(p);
+}
+/// One thread: the barrier expects one arrival per phase.
+__device__ __forceinline__ void mbar_init(unsigned long long* bar)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+/// One thread: arrives on bar expecting `bytes` and copies them from global src to shared dst
+/// (both 16-byte aligned, bytes a multiple of 16). Shared memory the block read before is
+/// ordered before the copy's writes by the proxy fence.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* bar)
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	asm volatile("{\n\t.reg .b64 st;\n\t"
+	             "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+	             "r"(bytes)
+	             : "memory");
+	asm volatile(
+	    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+	        "r"(smem_u32(dst)),
+	    "l"(src), "r"(bytes), "r"(smem_u32(bar))
+	    : "memory");
+}
+/// Waits for the completion of phase `parity` of bar, at most `tries` polls (each poll may
+/// suspend the thread for a short, hardware-chosen time). False if it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int tries)
+{
+	for (int i = 0; i < tries; i++) {
+		unsigned ok;
+		asm volatile("{\n\t.reg .pred p;\n\t"
+		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}"
+		             : "=r"(ok)
+		             : "r"(smem_u32(bar)), "r"(parity)
+		             : "memory");
+		if (ok) return true;
+	}
+	return false;
+}
+
 // error bits (Dev::err[0])
 enum : int {
 	EB_NONFINITE = 1,  // layer_id of NaN/inf

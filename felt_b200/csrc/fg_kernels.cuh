@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 /// halo nodes from the neighbour partition's brick or its background (an inactive partition),
 /// the grid background L+1 outside the grid; the values get_phi reads at those positions.
 template <int D, int L>
-__device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, float* box)
+__device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, float* box,
+                           bool halo_only = false)
 {
 	constexpr int ND = D == 3 ? 27 : 9;
 	__shared__ int nsl[27];    // slot of the partition in each direction (-1 inactive)
@@ -390,6 +391,8 @@ __device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, floa
 			const int pa = P.porig[gp * 3 + a] + c;
 			ing = ing && pa >= g.off[a] && pa < g.hi[a];
 		}
+		constexpr int CENTRE = D == 3 ? 13 : 4;
+		if (halo_only && dir == CENTRE && ing) continue;  // the brick's own node: copied in bulk
 		float v = (float)(L + 1);
 		if (ing) {
 			const int s2 = nsl[dir];
@@ -416,28 +419,80 @@ struct BoxGet {
 };
 
 /// Shared-memory bytes of a staged partition with a one-node halo.
-__host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
+__host__ __device__ inline size_t halo_box_bytes(int D, const int* csz)
 {
 	size_t v = 1;
 	for (int a = 0; a < D; a++) v *= (size_t)(csz[a] + 2);
-	return v * sizeof(float);
+	return (v * sizeof(float) + 15) & ~(size_t)15;
+}
+/// Shared-memory bytes of k_delta_smem: the staged box, then the brick itself (the bulk
+/// copy's destination, 16-byte aligned).
+__host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
+{
+	size_t bv = 1;
+	for (int a = 0; a < D; a++) bv *= (size_t)csz[a];
+	return halo_box_bytes(D, csz) + bv * sizeof(float);
 }
 
 /// k_delta_builtin with the partition and its halo staged in shared memory, for speeds with a
 /// curvature term: every stencil read of the zero-layer nodes hits shared memory. One block per
-/// zero-layer partition.
+/// zero-layer partition. The brick itself arrives by one bulk copy (cp.async.bulk on an
+/// mbarrier) while the threads load the halo, then moves into the box's interior; a brick
+/// whose bytes are not a multiple of 16 is loaded by the threads with the halo.
 template <int D, int L>
 __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float* hbox)
 {
 	constexpr int NL = 2 * L + 1;
+	constexpr int WAIT_TRIES = 1 << 20;  // bound of the copy's wait (each poll may suspend)
+	__shared__ __align__(8) unsigned long long bar;
+	__shared__ int copy_ok;
 	const int total = P.woff[P.S];
+	const bool bulk = (P.BV * sizeof(float)) % 16 == 0;
+	float* sbrick = hbox + halo_box_bytes(D, P.csz) / sizeof(float);
+	if (bulk && threadIdx.x == 0) mbar_init(&bar);
+	__syncthreads();
+	unsigned parity = 0;
 	for (int e = G.bid; e < total; e += G.nb) {
 		const int s = entry_surface(P.woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const Speed sp = speeds[s];
 		const int gp = g.pbase + P.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
 		const int sl = P.slot[gp];
-		stage_halo<D, L>(P, g, gp, sl, hbox);
+		if (bulk && threadIdx.x == 0)
+			bulk_g2s(sbrick, P.phi + (size_t)sl * P.BV, (unsigned)(P.BV * sizeof(float)), &bar);
+		stage_halo<D, L>(P, g, gp, sl, hbox, bulk);
+		if (bulk) {
+			if (threadIdx.x == 0) copy_ok = mbar_wait(&bar, parity, WAIT_TRIES) ? 1 : 0;
+			__syncthreads();
+			if (!copy_ok) {
+				// the copy did not land: report it and leave; a last bounded wait lets a late
+				// copy finish before the block's shared memory goes
+				if (threadIdx.x == 0) {
+					atomicOr(P.err, EB_TIMEOUT);
+					mbar_wait(&bar, parity, WAIT_TRIES);
+				}
+				return;
+			}
+			mbar_wait(&bar, parity, WAIT_TRIES);  // completed: every thread observes it
+			parity ^= 1u;
+			int ext[D];
+#pragma unroll
+			for (int a = 0; a < D; a++) ext[a] = P.csz[a] + 2;
+			// the brick's in-grid nodes into the box's interior (the others hold L+1)
+			for (int leaf = threadIdx.x; leaf < P.BV; leaf += blockDim.x) {
+				int r = leaf, bi = 0, mul = 1;
+				bool ing = true;
+#pragma unroll
+				for (int a = D - 1; a >= 0; a--) {
+					const int q = r % P.csz[a];
+					r /= P.csz[a];
+					bi += (q + 1) * mul;
+					mul *= ext[a];
+					ing = ing && P.porig[gp * 3 + a] + q < g.hi[a];
+				}
+				if (ing) hbox[bi] = sbrick[leaf];
+			}
+		}
 		__syncthreads();
 		BoxGet<D> get;
 		get.box = hbox;
@@ -460,7 +515,7 @@ template <int D, int L>
 __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
 {
 	pdl_enter();
-	extern __shared__ float hbox[];
+	extern __shared__ __align__(16) float hbox[];
 	d_delta_smem<D, L>(P, speeds, hw_grid(), hbox);
 }
 
