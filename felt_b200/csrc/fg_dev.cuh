@@ -40,15 +40,15 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar)
 	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
 	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-/// One thread: arrives on bar expecting `bytes` and copies them from global src to shared dst
-/// (both 16-byte aligned, bytes a multiple of 16). Shared memory the block read before is
-/// ordered before the copy's writes by the proxy fence.
+/// Orders the block's earlier generic accesses of shared memory before later bulk copies into
+/// it (called by each issuing thread after a barrier).
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+/// Any thread: `bytes` more to arrive on bar's current phase, then copies them from global src
+/// to shared dst (both 16-byte aligned, bytes a multiple of 16), completing on bar.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
                                          unsigned long long* bar)
 {
-	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-	asm volatile("{\n\t.reg .b64 st;\n\t"
-	             "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+	asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
 	             "r"(bytes)
 	             : "memory");
 	asm volatile(
@@ -56,6 +56,13 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 	        "r"(smem_u32(dst)),
 	    "l"(src), "r"(bytes), "r"(smem_u32(bar))
 	    : "memory");
+}
+/// One thread: the phase's single arrival (after every bulk_g2s of the phase was issued).
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+	asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+	                 smem_u32(bar))
+	             : "memory");
 }
 /// Waits for the completion of phase `parity` of bar, at most `tries` polls (each poll may
 /// suspend the thread for a short, hardware-chosen time). False if it gave up.

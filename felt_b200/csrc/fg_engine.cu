@@ -1403,7 +1403,7 @@ private:
 			FG_RUN("k_flush_smem", st_, launch_pdl((k_flush_smem<D, L>), sm_count() * 8, 256, smem_flush_, st_, P_););
 		else
 			FG_RUN("k_flush_leaf", st_, launch_pdl((k_flush_leaf<D, L>), grid_for(P_.NP), 128, 0, st_, P_););
-		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 256, 0, st_, P_););
+		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 1024, 0, st_, P_););
 	}
 
 	void expand()

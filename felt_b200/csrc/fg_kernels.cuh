@@ -59,9 +59,39 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 // mode 0: cnt[s*NL + l]; mode 1: cnt[s*NL] + cnt[s*NL + NL-1]; mode 2: sum over layers.
 // Frozen surfaces (frozen[s] != 0) contribute no entries, so no kernel works on them.
 // ---------------------------------------------------------------------------------------------
+/// One surface count per lane of warp 0 (S <= 32): the scan in registers, no block barrier.
+static __device__ __forceinline__ int surface_count(const int* cnt, int NL, int l, int mode, int s,
+                                                    const int* frozen)
+{
+	if (frozen && frozen[s]) return 0;
+	if (mode == 0) return cnt[s * NL + l];
+	if (mode == 1) return cnt[s * NL] + cnt[s * NL + NL - 1];
+	int v = 0;
+	for (int t = 0; t < NL; t++) v += cnt[s * NL + t];
+	return v;
+}
+static __device__ __forceinline__ void warp_scan_counts(const int* cnt, int NL, int l, int mode,
+                                                        int S, int* woff, const int* frozen)
+{
+	const int lane = lane_id();
+	int v = lane < S ? surface_count(cnt, NL, l, mode, lane, frozen) : 0;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int y = __shfl_up_sync(FULL, v, o);
+		if (lane >= o) v += y;
+	}
+	if (lane == 0) woff[0] = 0;
+	if (lane < S) woff[lane + 1] = v;
+}
+
 static __device__ __noinline__ void d_scan_counts(const int* cnt, int NL, int l, int mode, int S,
                                                   int* woff, const int* frozen)
 {
+	if (S <= 32) {
+		if (threadIdx.x < 32) warp_scan_counts(cnt, NL, l, mode, S, woff, frozen);
+		__syncthreads();
+		return;
+	}
 	__shared__ int carry;
 	if (threadIdx.x == 0) {
 		carry = 0;
@@ -98,6 +128,13 @@ static __global__ void k_scan_counts(const int* cnt, int NL, int l, int mode, in
 static __device__ __noinline__ void d_scan_layers(const int* cnt, int NL, int S, int* woffl,
                                                   const int* frozen)
 {
+	if (S <= 32 && (int)(blockDim.x >> 5) >= NL) {
+		// a warp per layer
+		const int w = threadIdx.x >> 5;
+		if (w < NL) warp_scan_counts(cnt, NL, w, 0, S, woffl + (size_t)w * (S + 1), frozen);
+		__syncthreads();
+		return;
+	}
 	__shared__ int carry;
 	for (int l = 0; l < NL; l++) {
 		int* woff = woffl + (size_t)l * (S + 1);
@@ -337,24 +374,37 @@ __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speed
 	d_delta_builtin<D, L>(P, speeds, split, hw_grid());
 }
 
-/// Fills box with the isogrid over a partition and a one-node halo ((part+2)^D values, row-major,
-/// last axis fastest). The brick slots (or backgrounds) of the 3^D partitions around it are
-/// looked up once, so every value is a single independent load: interior nodes from the brick,
-/// halo nodes from the neighbour partition's brick or its background (an inactive partition),
-/// the grid background L+1 outside the grid; the values get_phi reads at those positions.
+/// The staged box of k_delta_smem: the partition and a one-node halo, row-major with the last
+/// axis fastest. Along the last axis a row holds 3 unused slots, the -1 halo node, the brick's
+/// row and the +1 halo node, padded to a multiple of 4 floats, so that every brick row starts on
+/// a 16-byte boundary and arrives by one bulk copy.
+struct HaloBox {
+	int ext[3];  // extents: csz + 2 on the leading axes, the padded row on the last
+	int vol;
+	__host__ __device__ HaloBox(int D, const int* csz)
+	{
+		vol = 1;
+		for (int a = 0; a < D; a++) {
+			ext[a] = a == D - 1 ? ((csz[a] + 5 + 3) & ~3) : csz[a] + 2;
+			vol *= ext[a];
+		}
+	}
+};
+
+/// Fills the box of partition gp (brick slot sl). The slots (or backgrounds) of the 3^D
+/// partitions around it are looked up once. Each row of the box along the last axis is one
+/// thread's: a row inside the brick and the grid takes its brick row by one bulk copy
+/// (cp.async.bulk completing on bar; rows = number issued, returned) and loads its two halo
+/// nodes; every other node is one load from the neighbour partition's brick, its background
+/// (inactive), or L+1 outside the grid: the values get_phi reads there. bulk = false: every
+/// node by a load.
 template <int D, int L>
-__device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, float* box,
-                           bool halo_only = false)
+__device__ int stage_halo(const Dev& P, const SurfGeom& g, int gp, float* box, const HaloBox& hb,
+                          bool bulk, unsigned long long* bar)
 {
 	constexpr int ND = D == 3 ? 27 : 9;
 	__shared__ int nsl[27];    // slot of the partition in each direction (-1 inactive)
 	__shared__ float nbg[27];  // its background
-	int ext[D], vol = 1;
-#pragma unroll
-	for (int a = 0; a < D; a++) {
-		ext[a] = P.csz[a] + 2;
-		vol *= ext[a];
-	}
 	if (threadIdx.x < ND) {
 		// a node of the neighbour partition: one outside the brick on the axes the direction
 		// leaves it, the brick's first node elsewhere
@@ -377,79 +427,89 @@ __device__ void stage_halo(const Dev& P, const SurfGeom& g, int gp, int sl, floa
 		nbg[threadIdx.x] = b2;
 	}
 	__syncthreads();
-	for (int i = threadIdx.x; i < vol; i += blockDim.x) {
-		int r = i, dir = 0, mul = 1, leaf = 0;
-		bool ing = true;
+	constexpr int X = D - 1;
+	const int cx = P.csz[X];
+	const int ex = hb.ext[X];
+	const int nrows = hb.vol / ex;
+	const int ox = P.porig[gp * 3 + X];
+	const bool rows_bulk = bulk && (cx * sizeof(float)) % 16 == 0;
+	int issued = 0;
+	for (int row = threadIdx.x; row < nrows; row += blockDim.x) {
+		// the row's coordinates on the leading axes (-1..csz), its direction digits and leaf base
+		int r = row, dir = 0, mul = 3, leaf0 = 0;
+		bool ing = true, inner = true;
 #pragma unroll
-		for (int a = D - 1; a >= 0; a--) {
-			const int c = r % ext[a] - 1;
-			r /= ext[a];
+		for (int a = D - 2; a >= 0; a--) {
+			const int c = r % hb.ext[a] - 1;
+			r /= hb.ext[a];
 			const int cs = P.csz[a];
 			dir += (c < 0 ? 0 : c >= cs ? 2 : 1) * mul;
 			mul *= 3;
-			leaf += (c < 0 ? cs - 1 : c >= cs ? 0 : c) * P.lstr[a];
+			leaf0 += (c < 0 ? cs - 1 : c >= cs ? 0 : c) * P.lstr[a];
 			const int pa = P.porig[gp * 3 + a] + c;
 			ing = ing && pa >= g.off[a] && pa < g.hi[a];
+			inner = inner && c >= 0 && c < cs;
 		}
-		constexpr int CENTRE = D == 3 ? 13 : 4;
-		if (halo_only && dir == CENTRE && ing) continue;  // the brick's own node: copied in bulk
-		float v = (float)(L + 1);
-		if (ing) {
-			const int s2 = nsl[dir];
-			v = s2 >= 0 ? P.phi[(size_t)s2 * P.BV + leaf] : nbg[dir];
+		float* out = box + (size_t)row * ex + 3;  // node x = -1 of the row
+		// the brick's row in one bulk copy when it lies wholly inside the grid
+		const bool copy = rows_bulk && inner && ing && ox + cx <= g.hi[X];
+		if (copy) {
+			bulk_g2s(out + 1, P.phi + (size_t)P.slot[gp] * P.BV + leaf0,
+			         (unsigned)(cx * sizeof(float)), bar);
+			issued++;
 		}
-		box[i] = v;
+		for (int x = -1; x <= cx; x++) {
+			if (copy && x >= 0 && x < cx) continue;
+			const int d = x < 0 ? 0 : x >= cx ? 2 : 1;
+			const int leaf = leaf0 + (x < 0 ? cx - 1 : x >= cx ? 0 : x);
+			const int px = ox + x;
+			float v = (float)(L + 1);
+			if (ing && px >= g.off[X] && px < g.hi[X]) {
+				const int s2 = nsl[dir + d];
+				v = s2 >= 0 ? P.phi[(size_t)s2 * P.BV + leaf] : nbg[dir + d];
+			}
+			out[x + 1] = v;
+		}
 	}
-	(void)sl;
+	return issued;
 }
 
 /// Reads a staged box (stage_halo) by world position.
 template <int D>
 struct BoxGet {
 	const float* box;
-	int org[D];  // world position of box index 0
+	int org[D];  // world position of the box's first node on each axis (the -1 halo node)
 	int ext[D];
 	__device__ float operator()(const Vec<D>& p) const
 	{
 		int i = 0;
 #pragma unroll
 		for (int a = 0; a < D; a++) i = i * ext[a] + (p[a] - org[a]);
-		return box[i];
+		return box[i + 3];  // the 3 unused slots at the start of each row
 	}
 };
 
-/// Shared-memory bytes of a staged partition with a one-node halo.
-__host__ __device__ inline size_t halo_box_bytes(int D, const int* csz)
-{
-	size_t v = 1;
-	for (int a = 0; a < D; a++) v *= (size_t)(csz[a] + 2);
-	return (v * sizeof(float) + 15) & ~(size_t)15;
-}
-/// Shared-memory bytes of k_delta_smem: the staged box, then the brick itself (the bulk
-/// copy's destination, 16-byte aligned).
+/// Shared-memory bytes of k_delta_smem's box.
 __host__ __device__ inline size_t halo_smem_bytes(int D, const int* csz)
 {
-	size_t bv = 1;
-	for (int a = 0; a < D; a++) bv *= (size_t)csz[a];
-	return halo_box_bytes(D, csz) + bv * sizeof(float);
+	return (size_t)HaloBox(D, csz).vol * sizeof(float);
 }
 
 /// k_delta_builtin with the partition and its halo staged in shared memory, for speeds with a
 /// curvature term: every stencil read of the zero-layer nodes hits shared memory. One block per
-/// zero-layer partition. The brick itself arrives by one bulk copy (cp.async.bulk on an
-/// mbarrier) while the threads load the halo, then moves into the box's interior; a brick
-/// whose bytes are not a multiple of 16 is loaded by the threads with the halo.
+/// zero-layer partition. The brick's rows arrive by bulk copies (cp.async.bulk on an mbarrier,
+/// one per row, issued by the threads that stage the halo around them); a brick whose rows are
+/// not a multiple of 16 bytes is loaded by the threads.
 template <int D, int L>
 __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float* hbox)
 {
 	constexpr int NL = 2 * L + 1;
-	constexpr int WAIT_TRIES = 1 << 20;  // bound of the copy's wait (each poll may suspend)
+	constexpr int WAIT_TRIES = 1 << 20;  // bound of the copies' wait (each poll may suspend)
 	__shared__ __align__(8) unsigned long long bar;
-	__shared__ int copy_ok;
+	__shared__ int copy_ok, any_copy;
 	const int total = P.woff[P.S];
-	const bool bulk = (P.BV * sizeof(float)) % 16 == 0;
-	float* sbrick = hbox + halo_box_bytes(D, P.csz) / sizeof(float);
-	if (bulk && threadIdx.x == 0) mbar_init(&bar);
+	const HaloBox hb(D, P.csz);
+	if (threadIdx.x == 0) mbar_init(&bar);
 	__syncthreads();
 	unsigned parity = 0;
 	for (int e = G.bid; e < total; e += G.nb) {
@@ -458,15 +518,20 @@ __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float
 		const Speed sp = speeds[s];
 		const int gp = g.pbase + P.plist[(size_t)L * P.NP + g.pbase + (e - P.woff[s])];
 		const int sl = P.slot[gp];
-		if (bulk && threadIdx.x == 0)
-			bulk_g2s(sbrick, P.phi + (size_t)sl * P.BV, (unsigned)(P.BV * sizeof(float)), &bar);
-		stage_halo<D, L>(P, g, gp, sl, hbox, bulk);
-		if (bulk) {
-			if (threadIdx.x == 0) copy_ok = mbar_wait(&bar, parity, WAIT_TRIES) ? 1 : 0;
+		if (threadIdx.x == 0) any_copy = 0;
+		fence_proxy_async();  // the previous entry's reads of the box come before the copies
+		const int issued = stage_halo<D, L>(P, g, gp, hbox, hb, true, &bar);
+		if (issued) atomicOr(&any_copy, 1);
+		__syncthreads();  // every copy of the phase issued
+		if (any_copy) {
+			if (threadIdx.x == 0) {
+				mbar_arrive(&bar);
+				copy_ok = mbar_wait(&bar, parity, WAIT_TRIES) ? 1 : 0;
+			}
 			__syncthreads();
 			if (!copy_ok) {
-				// the copy did not land: report it and leave; a last bounded wait lets a late
-				// copy finish before the block's shared memory goes
+				// the copies did not land: report it and leave; a last bounded wait lets late
+				// copies finish before the block's shared memory goes
 				if (threadIdx.x == 0) {
 					atomicOr(P.err, EB_TIMEOUT);
 					mbar_wait(&bar, parity, WAIT_TRIES);
@@ -475,23 +540,6 @@ __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float
 			}
 			mbar_wait(&bar, parity, WAIT_TRIES);  // completed: every thread observes it
 			parity ^= 1u;
-			int ext[D];
-#pragma unroll
-			for (int a = 0; a < D; a++) ext[a] = P.csz[a] + 2;
-			// the brick's in-grid nodes into the box's interior (the others hold L+1)
-			for (int leaf = threadIdx.x; leaf < P.BV; leaf += blockDim.x) {
-				int r = leaf, bi = 0, mul = 1;
-				bool ing = true;
-#pragma unroll
-				for (int a = D - 1; a >= 0; a--) {
-					const int q = r % P.csz[a];
-					r /= P.csz[a];
-					bi += (q + 1) * mul;
-					mul *= ext[a];
-					ing = ing && P.porig[gp * 3 + a] + q < g.hi[a];
-				}
-				if (ing) hbox[bi] = sbrick[leaf];
-			}
 		}
 		__syncthreads();
 		BoxGet<D> get;
@@ -499,7 +547,7 @@ __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float
 #pragma unroll
 		for (int a = 0; a < D; a++) {
 			get.org[a] = P.porig[gp * 3 + a] - 1;
-			get.ext[a] = P.csz[a] + 2;
+			get.ext[a] = hb.ext[a];
 		}
 		const int n = P.lcnt[sl * NL + L];
 		const uint16_t* lst = P.lst + ((size_t)sl * NL + L) * P.BV;
@@ -1575,7 +1623,7 @@ __device__ void d_flush_plist(const Dev& P, GridPos G)
 	}
 }
 template <int L>
-__global__ void __launch_bounds__(256) k_flush_plist(Dev P)
+__global__ void __launch_bounds__(1024) k_flush_plist(Dev P)
 {
 	pdl_enter();
 	d_flush_plist<L>(P, hw_grid());
