@@ -25,6 +25,19 @@ struct ListView {
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+/// Adds every thread's count to a global work counter with one atomic per block instead of one
+/// per partition entry on the same word. Every thread of the block calls it once, at the end
+/// of the kernel's work.
+__device__ __forceinline__ void block_add(unsigned long long* dst, unsigned long long v)
+{
+	__shared__ unsigned long long acc;
+	if (threadIdx.x == 0) acc = 0;
+	__syncthreads();
+	if (v) atomicAdd(&acc, v);
+	__syncthreads();
+	if (threadIdx.x == 0 && acc) atomicAdd(dst, acc);
+}
+
 /// Exclusive block scan of one int per thread; returns the prefix, total in *total.
 __device__ __forceinline__ int block_excl_scan(int v, int* total)
 {
@@ -348,6 +361,7 @@ __device__ void d_delta_builtin(const Dev& P, const Speed* speeds, int split, Gr
 	const int lane = lane_id();
 	const int nwarps = (G.nb * blockDim.x) >> 5;
 	const int total = P.woff[P.S] * split;
+	unsigned long long done = 0;
 	for (int v = (G.bid * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
 		const int s = entry_surface(P.woff, P.S, e);
@@ -364,8 +378,9 @@ __device__ void d_delta_builtin(const Dev& P, const Speed* speeds, int split, Gr
 			const int leaf = lst[j];
 			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval_g<D>(get, sp, leaf_pos<D>(P, gp, leaf));
 		}
-		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
+		if (lane == 0 && part == 0) done += n;
 	}
+	block_add(&P.kstat[KS_ZERO], done);
 }
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_delta_builtin(Dev P, const Speed* speeds, int split)
@@ -509,6 +524,7 @@ __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float
 	__shared__ int copy_ok, any_copy;
 	const int total = P.woff[P.S];
 	const HaloBox hb(D, P.csz);
+	unsigned long long done = 0;
 	if (threadIdx.x == 0) mbar_init(&bar);
 	__syncthreads();
 	unsigned parity = 0;
@@ -555,9 +571,10 @@ __device__ void d_delta_smem(const Dev& P, const Speed* speeds, GridPos G, float
 			const int leaf = lst[j];
 			P.dlt[(size_t)sl * P.BV + leaf] = speed_eval_g<D>(get, sp, leaf_pos<D>(P, gp, leaf));
 		}
-		if (threadIdx.x == 0) atomicAdd(&P.kstat[KS_ZERO], (unsigned long long)n);
+		if (threadIdx.x == 0) done += n;
 		__syncthreads();
 	}
+	block_add(&P.kstat[KS_ZERO], done);
 }
 template <int D, int L>
 __global__ void __launch_bounds__(128) k_delta_smem(Dev P, const Speed* speeds)
@@ -730,7 +747,7 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 		for (int i = threadIdx.x; i < nt; i += blockDim.x) {
 			if (!(sf[i] & 0x80000000u)) continue;
 			const int gp = g.pbase + slp[i];
-			if (atomicExch(&P.sflag[gp], 1) == 0)
+			if (*(volatile int*)&P.sflag[gp] == 0 && atomicExch(&P.sflag[gp], 1) == 0)
 				P.q_sunion[atomicAdd(&P.counters[CNT_SUNION], 1)] = gp;
 		}
 	}
@@ -768,6 +785,7 @@ __device__ void d_dist1_work(const Dev& P, const int* woff, ListView lv, int k, 
 	const int li = k + L;
 	const int lane = lane_id();
 	const int total = woff[P.S] * split;
+	unsigned long long done = 0;
 	for (int v = first_warp; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
 		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
@@ -786,8 +804,9 @@ __device__ void d_dist1_work(const Dev& P, const int* woff, ListView lv, int k, 
 			P.dlt[b0 + l1] = d1;
 			if (two) P.dlt[b0 + l2] = d2;
 		}
-		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
+		if (lane == 0 && part == 0) done += n;
 	}
+	block_add(&P.kstat[KS_DIST], done);
 }
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_dist1(Dev P, const int* woff, ListView lv, int k,
@@ -839,7 +858,7 @@ __device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b
 			flags = warp_or(flags);
 			if (threadIdx.x == 0) {
 				eflag[e] = flags;
-				if (any) atomicOr(P.changed, 1);
+				if (any && !*(volatile int*)P.changed) atomicOr(P.changed, 1);
 			}
 		}
 	}
@@ -894,7 +913,7 @@ __device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, 
 		flags = warp_or(flags);
 		if (lane == 0) {
 			eflag[e] = flags;
-			if (any) atomicOr(P.changed, 1);
+			if (any && !*(volatile int*)P.changed) atomicOr(P.changed, 1);
 		}
 	}
 }
@@ -1023,6 +1042,7 @@ __global__ void __launch_bounds__(256) k_dist_fused(Dev P, ListView lv, FusedPas
 	const int lane = lane_id();
 	const int nwarps = (G.nb * blockDim.x) >> 5;
 	const int total = p1.woff[P.S] * split;
+	unsigned long long done = 0;
 	for (int v = (G.bid * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
 		const int e = v / split, part = v - e * split;
 		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
@@ -1041,8 +1061,9 @@ __global__ void __launch_bounds__(256) k_dist_fused(Dev P, ListView lv, FusedPas
 			P.dlt[b0 + l1] = d1;
 			if (two) P.dlt[b0 + l2] = d2;
 		}
-		if (lane == 0 && part == 0) atomicAdd(&P.kstat[KS_DIST], (unsigned long long)n);
+		if (lane == 0 && part == 0) done += n;
 	}
+	block_add(&P.kstat[KS_DIST], done);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1056,6 +1077,7 @@ __device__ void d_flush_leaf(const Dev& P, GridPos G)
 {
 	constexpr int NL = 2 * L + 1;
 	const int n = P.counters[CNT_SUNION];
+	unsigned long long done = 0;
 	for (int e = G.bid * blockDim.x + threadIdx.x; e < n; e += G.nb * blockDim.x) {
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
@@ -1113,7 +1135,7 @@ __device__ void d_flush_leaf(const Dev& P, GridPos G)
 		{
 			int edits = 0;
 			for (int fi = 0; fi < NL; fi++) edits += P.ccnt[sl * NL + fi];
-			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)edits);
+			done += edits;
 		}
 		if (dead) {
 			P.oslot[gp] = sl;
@@ -1121,6 +1143,7 @@ __device__ void d_flush_leaf(const Dev& P, GridPos G)
 			P.q_retire[atomicAdd(&P.counters[CNT_RETIRE], 1)] = sl;
 		}
 	}
+	block_add(&P.kstat[KS_FLUSH], done);
 }
 template <int D, int L>
 __global__ void k_flush_leaf(Dev P)
@@ -1172,6 +1195,7 @@ __device__ void d_flush_smem(const Dev& P, GridPos G, unsigned char* fsm)
 	// a first sweep, so that they all start at once; the rest follow.
 	constexpr int LONG_CHAIN = 64;
 	__shared__ int take;
+	unsigned long long done = 0;  // leaf edits replayed (thread 0)
 	for (int sweep = 0; sweep < 2; sweep++)
 	for (int e = G.bid; e < n; e += G.nb) {
 		const int gp = P.q_sunion[e];
@@ -1350,7 +1374,7 @@ __device__ void d_flush_smem(const Dev& P, GridPos G, unsigned char* fsm)
 		}
 		if (threadIdx.x == 0) {
 			P.rem[gp] = remb;
-			atomicAdd(&P.kstat[KS_FLUSH], (unsigned long long)total);
+			done += total;
 			if (nout > 0 && nout == live0) {
 				// the last leaf left the band: the partition deactivates with the background
 				// of that leaf's side (PartitionedMixin.hpp:530-558)
@@ -1362,6 +1386,7 @@ __device__ void d_flush_smem(const Dev& P, GridPos G, unsigned char* fsm)
 		}
 		__syncthreads();
 	}
+	block_add(&P.kstat[KS_FLUSH], done);
 }
 template <int D, int L>
 __global__ void __launch_bounds__(256) k_flush_smem(Dev P)
@@ -1658,7 +1683,9 @@ __device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 			unsigned long long* cl = &P.claim[(size_t)sn * P.BV + leafn];
 			if (mode == 1) {
 				atomicMin(cl, key);
-				if (atomicExch(&P.touched[sn], 1) == 0)
+				// most candidates of a brick find it touched already: a read first keeps them
+				// off the one word's atomic queue
+				if (*(volatile int*)&P.touched[sn] == 0 && atomicExch(&P.touched[sn], 1) == 0)
 					P.q_touch[atomicAdd(&P.counters[CNT_TOUCH], 1)] = sn;
 			} else if (*cl == key) {
 				const SurfGeom& g = P.geom[P.surf_of[gpn]];
@@ -1754,7 +1781,8 @@ __device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 					unsigned long long* cl = &P.claim[(size_t)sn * P.BV + leafn];
 					if (mode == 1) {
 						atomicMin(cl, key);
-						if (atomicExch(&P.touched[sn], 1) == 0)
+						if (*(volatile int*)&P.touched[sn] == 0 &&
+						    atomicExch(&P.touched[sn], 1) == 0)
 							P.q_touch[atomicAdd(&P.counters[CNT_TOUCH], 1)] = sn;
 					} else if (*cl == key) {
 						P.dlt[(size_t)sn * P.BV + leafn] = distance<D, L>(P, g, q, v, (float)side);
