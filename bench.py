@@ -1255,7 +1255,7 @@ def run_felt(args, name, cfg):
            "d2h_bytes_per_step": d2h // steps}
 
     extra = {}
-    roof = cpu = parity = batched = served = None
+    roof = cpu = parity = batched = batched_2d = served = None
     dev_state = None
     single = cfg["kind"] == "single"
     if rank == 0 and single and ws == 1 and not args.no_cpu:
@@ -1273,6 +1273,7 @@ def run_felt(args, name, cfg):
             # the headline metric's other halves, on the same GPU in the same run: the batched
             # 3D workload against the plain path, and the served request mix
             batched = measure_batched(fb, "c4", 20, 3)
+            batched_2d = measure_batched(fb, "c3", 20, 3)
             served = measure_served(fb, "c5", (300, 1000, 3000))
     if rank == 0 and ws == 1 and not args.no_cpu:
         if single:
@@ -1310,7 +1311,7 @@ def run_felt(args, name, cfg):
                               "step's result (band size; the re-marched polygons on march "
                               "steps) coming out each step"},
             "roofline": roof, "cpu_baseline": cpu, "parity": parity,
-            "batched": batched, "served": served,
+            "batched": batched, "batched_2d": batched_2d, "served": served,
             "e2e": e2e, "clocks": clk, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
