@@ -1347,9 +1347,16 @@ def main():
     ap.add_argument("--fuse-passes", type=int, default=0, choices=[0, 1, 2],
                     help="fg_config.fuse_passes: the distance passes 1 as 4L launches, 2 as 2L+1 "
                          "fused ones (0 = automatic)")
+    ap.add_argument("--dist-split", type=int, default=0, choices=[0, 1, 2, 4, 8],
+                    help="fg_config.dist_split: warps per partition entry in the first distance "
+                         "pass (0 = automatic)")
+    ap.add_argument("--record-passes", type=int, default=0, choices=[0, 1, 2],
+                    help="fg_config.record_passes: 1 a warp, 2 a block per partition entry in the "
+                         "passes that record status changes (0 = automatic)")
     args = ap.parse_args()
     TUNING.update(launch_mode=args.launch_mode, autotune=args.autotune,
-                  delta_kernel=args.delta_kernel, fuse_passes=args.fuse_passes)
+                  delta_kernel=args.delta_kernel, fuse_passes=args.fuse_passes,
+                  dist_split=args.dist_split, record_passes=args.record_passes)
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, args.config, cfg)
