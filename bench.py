@@ -197,6 +197,8 @@ def combine_ranks(dist, t_ms, wall_s, node_updates, device):
 # Launch tuning of every surface and batch the bench creates (fg_config: launch_mode,
 # autotune), from the command line.
 TUNING = {}
+# Device time of each step of the last timed run (ms).
+STEP_MS = []
 
 
 class SingleWork:
@@ -204,8 +206,10 @@ class SingleWork:
 
     def __init__(self, fb, cfg, brick_capacity=0):
         self.fb, self.cfg = fb, cfg
+        # the polygon arena sized for the surface's geometry with the polygoniser's headroom
+        # (16x the live vertices), so that no timed march grows it
         self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=brick_capacity,
-                            **TUNING)
+                            vertex_capacity=1 << 22, **TUNING)
         self.p = fb.Polys(self.s)
         self.s.seed((0,) * cfg["D"])
         for _ in range(cfg["expand"]):
@@ -457,6 +461,7 @@ def time_steps(torch, work, stream, steps, warm, flush, start=0, profile=False):
         torch.cuda.profiler.start()
     nu0 = work.node_updates()
     total, wall, d2h = 0.0, 0.0, 0
+    per_step = []
     for i in range(steps):
         flush.fill_(float(i))
         torch.cuda.synchronize()
@@ -472,8 +477,10 @@ def time_steps(torch, work, stream, steps, warm, flush, start=0, profile=False):
         d2h += 8
         wall += time.perf_counter() - t0
         b.synchronize()
-        total += a.elapsed_time(b)
+        per_step.append(a.elapsed_time(b))
+        total += per_step[-1]
     torch.cuda.synchronize()
+    STEP_MS[:] = per_step
     if profile:
         torch.cuda.profiler.stop()
         u1 = work.work_units()
@@ -1245,6 +1252,7 @@ def run_felt(args, name, cfg):
     t_ms, wall_s, nu, d2h = time_steps(torch, work, stream, steps, args.warmup, flush,
                                        profile=args.profile_region)
     launches = fb.launch_count() - l0
+    step_ms = sorted(STEP_MS)
     clk = clocks.stop()
     if pg:
         t_ms, wall_s, nu = combine_ranks(pg, t_ms, wall_s, nu, "cuda")
@@ -1309,7 +1317,9 @@ def run_felt(args, name, cfg):
                                 "stream), inputs resident",
                        "e2e": "wall clock through the C ABI with the speed going in and the "
                               "step's result (band size; the re-marched polygons on march "
-                              "steps) coming out each step"},
+                              "steps) coming out each step",
+                       "step_ms": {"min": step_ms[0], "median": step_ms[len(step_ms) // 2],
+                                   "max": step_ms[-1]} if step_ms else None},
             "roofline": roof, "cpu_baseline": cpu, "parity": parity,
             "batched": batched, "batched_2d": batched_2d, "served": served,
             "e2e": e2e, "clocks": clk, "gpu_launches": launches,

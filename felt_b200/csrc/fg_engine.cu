@@ -255,6 +255,8 @@ public:
 		zcount_ = dalloc<unsigned long long>(1, o);
 		d_iters_ = dalloc<int>(1, o);
 		d_speeds_ = dalloc<Speed>(S, o);
+		FG_CUDA(cudaHostAlloc((void**)&h_speeds_, (size_t)S * sizeof(Speed), cudaHostAllocDefault));
+		FG_CUDA(cudaHostAlloc((void**)&h_out_, 2 * sizeof(int), cudaHostAllocDefault));
 
 		fill(P.slot, NP, -1);
 		fillf(P.bg, NP, (float)(L + 1));
@@ -360,6 +362,8 @@ private:
 		if (d_lpos_) locked_free(d_lpos_);
 		if (d_lval_) locked_free(d_lval_);
 		if (d_lcount_) locked_free(d_lcount_);
+		if (h_speeds_) cudaFreeHost(h_speeds_);
+		if (h_out_) cudaFreeHost(h_out_);
 	}
 
 	int dims() const override { return D; }
@@ -494,7 +498,10 @@ private:
 	void update_builtin(const Speed* speeds) override
 	{
 		check_not_frozen();
-		FG_CUDA(cudaMemcpyAsync(d_speeds_, speeds, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
+		// through pinned staging: the copy is a plain DMA, no driver bounce buffer (the previous
+		// update synchronised, so the staging is free)
+		std::memcpy(h_speeds_, speeds, P_.S * sizeof(Speed));
+		FG_CUDA(cudaMemcpyAsync(d_speeds_, h_speeds_, P_.S * sizeof(Speed), cudaMemcpyHostToDevice,
 		                        st_));
 		bool any_curv = false;
 		for (int s = 0; s < P_.S; s++) any_curv = any_curv || (speeds[s].kind & 2);
@@ -580,7 +587,7 @@ private:
 			buf_dirty_[1] = b1;
 		}
 		FG_CUDA(cudaGraphLaunch(step_exec_[key], st_));
-		int out[2] = {0, 0};
+		int* out = h_out_;  // pinned
 		FG_CUDA(cudaMemcpyAsync(&out[0], d_iters_, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaMemcpyAsync(&out[1], P_.changed, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
@@ -785,7 +792,7 @@ private:
 		if (launch_mode_ == 2 || !loop_ok_ || !graphs_ok_ || prof_on()) return false;
 		if (!loop_exec_ && !build_device_loop()) return false;
 		FG_CUDA(cudaGraphLaunch(loop_exec_, st_));
-		int out[2] = {0, 0};
+		int* out = h_out_;  // pinned
 		FG_CUDA(cudaMemcpyAsync(&out[0], d_iters_, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaMemcpyAsync(&out[1], P_.changed, sizeof(int), cudaMemcpyDeviceToHost, st_));
 		FG_CUDA(cudaStreamSynchronize(st_));
@@ -1480,6 +1487,8 @@ private:
 	cudaGraphExec_t step_exec_[16] = {};  // the whole update, by due resets and delta kernel
 	long long step_launches_[16] = {};    // kernels before its while node
 	bool step_ok_ = true;
+	Speed* h_speeds_ = nullptr;  // pinned staging of the builtin speeds
+	int* h_out_ = nullptr;       // pinned read-back of the device loop's count and flag
 	bool delta_staged_ = true;   // curvature speeds over staged bricks (k_delta_smem)
 	// the global update's distance passes fused (k_dist_fused): the same results in 2L+1
 	// launches instead of 4L, but no faster on C2 (1.33 against 1.28 ms per step), so off

@@ -730,6 +730,19 @@ public:
 		if (vc >= (1LL << 30)) throw Error(-1, "vertex capacity too large");
 		keep_pool_memory();
 		alloc_arena(vc, 2 * vc);
+		// the compaction's other arena up front: the first compaction then allocates nothing
+		// (a pool that has to grow from the driver mid-march stalls the step)
+		FG_CUDA(cudaMallocAsync((void**)&spare_v_, (size_t)vc * VF * sizeof(float), eng.stream()));
+		FG_CUDA(cudaMallocAsync((void**)&spare_s_, (size_t)2 * vc * D * sizeof(uint32_t), eng.stream()));
+		spare_vcap_ = vc;
+		spare_scap_ = 2 * vc;
+		// kernels that first run when the arena fills, possibly many steps later: loaded now
+		// (with lazy module loading a kernel's first launch also loads it)
+		cudaFuncAttributes fa;
+		FG_CUDA(cudaFuncGetAttributes(&fa, k_arena_chunk_sums));
+		FG_CUDA(cudaFuncGetAttributes(&fa, k_arena_chunk_scan));
+		FG_CUDA(cudaFuncGetAttributes(&fa, k_arena_offsets));
+		FG_CUDA(cudaFuncGetAttributes(&fa, k_polys_compact<D>));
 		int bvol = 1;
 		for (int a = 0; a < D; a++) bvol *= eng.part(a) + 1;
 		smem_ = (size_t)bvol * (D * sizeof(int) + sizeof(float)) +
