@@ -207,9 +207,9 @@ class SingleWork:
     def __init__(self, fb, cfg, brick_capacity=0):
         self.fb, self.cfg = fb, cfg
         # the polygon arena sized for the surface's geometry with the polygoniser's headroom
-        # (16x the live vertices), so that no timed march grows it
+        # (16x the live vertices: C2 holds up to ~0.7 M), so that no timed march grows it
         self.s = fb.Surface(cfg["size"], cfg["part"], cfg["L"], brick_capacity=brick_capacity,
-                            vertex_capacity=1 << 22, **TUNING)
+                            vertex_capacity=1 << 24, **TUNING)
         self.p = fb.Polys(self.s)
         self.s.seed((0,) * cfg["D"])
         for _ in range(cfg["expand"]):
