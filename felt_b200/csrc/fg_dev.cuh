@@ -142,6 +142,8 @@ struct Dev {
 	uint16_t* alst[2];  // affected buffer leaf lists
 	int* acnt[2];
 	unsigned long long* claim;  // [slot*BV + leaf] expansion claim keys
+	uint16_t* ccl;    // [slot*BV + i] leaves of the brick with an expansion claim, first claim order
+	int* ccln;        // [slot] their number
 	// expansion candidates of the current iteration (key, partition, leaf), cand_cap at most
 	unsigned long long* cand_key;
 	int* cand_gp;

@@ -207,6 +207,9 @@ public:
 			P.acnt[b] = dalloc<int>(nslots * NL, o);
 		}
 		P.claim = dalloc<unsigned long long>(nb, o);
+		P.ccl = dalloc<uint16_t>(nb, o);
+		P.ccln = dalloc<int>(nslots, o);
+		FG_CUDA(cudaMemsetAsync(P.ccln, 0, nslots * sizeof(int), st_));
 		// expansion candidates: most iterations need a few thousand; past the cap the claim
 		// and compute phases walk the status lists again instead
 		P.cand_cap = (int)std::min<size_t>(nb / 4 + 1024, (size_t)1 << 22);

@@ -1682,7 +1682,9 @@ __device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 			}
 			unsigned long long* cl = &P.claim[(size_t)sn * P.BV + leafn];
 			if (mode == 1) {
-				atomicMin(cl, key);
+				// the first claim of a leaf lists it for the append
+				if (atomicMin(cl, key) == NOCLAIM)
+					P.ccl[(size_t)sn * P.BV + atomicAdd(&P.ccln[sn], 1)] = (uint16_t)leafn;
 				// most candidates of a brick find it touched already: a read first keeps them
 				// off the one word's atomic queue
 				if (*(volatile int*)&P.touched[sn] == 0 && atomicExch(&P.touched[sn], 1) == 0)
@@ -1780,7 +1782,9 @@ __device__ void d_expand_gen(const Dev& P, int mode, GridPos G)
 					}
 					unsigned long long* cl = &P.claim[(size_t)sn * P.BV + leafn];
 					if (mode == 1) {
-						atomicMin(cl, key);
+						if (atomicMin(cl, key) == NOCLAIM)
+							P.ccl[(size_t)sn * P.BV + atomicAdd(&P.ccln[sn], 1)] =
+							    (uint16_t)leafn;
 						if (*(volatile int*)&P.touched[sn] == 0 &&
 						    atomicExch(&P.touched[sn], 1) == 0)
 							P.q_touch[atomicAdd(&P.counters[CNT_TOUCH], 1)] = sn;
@@ -1819,6 +1823,7 @@ __device__ void brick_init(const Dev& P, int sl, float bgv, int tid, int nth)
 		P.acnt[0][sl * NL + i] = 0;
 		P.acnt[1][sl * NL + i] = 0;
 	}
+	if (tid == 0) P.ccln[sl] = 0;
 }
 
 /// Child activation (TrackedMixin.hpp:37-41) of queued partitions: one block per partition.
@@ -1870,24 +1875,22 @@ template <int L>
 __device__ void d_expand_append(const Dev& P, GridPos G, unsigned long long* sk)
 {
 	constexpr int NL = 2 * L + 1;
-	__shared__ int ns, n0, base0, base1;
+	__shared__ int n0, base0, base1;
 	const int n = P.counters[CNT_TOUCH];
 	const size_t bv = (size_t)P.BV;
 	for (int q = G.bid; q < n; q += G.nb) {
 		const int sl = P.q_touch[q];
 		const int gp = P.slot_gp[sl];
-		if (threadIdx.x == 0) ns = 0;
-		__syncthreads();
-		for (int leaf = threadIdx.x; leaf < P.BV; leaf += blockDim.x) {
+		// the brick's claimed leaves, listed by their first claims (no scan of every claim key)
+		const int m = P.ccln[sl];
+		for (int i = threadIdx.x; i < m; i += blockDim.x) {
+			const int leaf = P.ccl[sl * bv + i];
 			const unsigned long long k = P.claim[sl * bv + leaf];
-			if (k != NOCLAIM) {
-				// keys use 44 bits; the leaf is packed below them.
-				sk[atomicAdd(&ns, 1)] = (k << 16) | (unsigned long long)leaf;
-				P.claim[sl * bv + leaf] = NOCLAIM;
-			}
+			// keys use 44 bits; the leaf is packed below them.
+			sk[i] = (k << 16) | (unsigned long long)leaf;
+			P.claim[sl * bv + leaf] = NOCLAIM;
 		}
 		__syncthreads();
-		const int m = ns;
 		int p2 = 1;
 		while (p2 < m) p2 <<= 1;
 		for (int i = m + threadIdx.x; i < p2; i += blockDim.x) sk[i] = ~0ull;
@@ -1941,6 +1944,7 @@ __device__ void d_expand_append(const Dev& P, GridPos G, unsigned long long* sk)
 				P.papg[2 * (size_t)pb + at] = gp - pb;
 			}
 			P.touched[sl] = 0;
+			P.ccln[sl] = 0;
 		}
 		__syncthreads();
 	}

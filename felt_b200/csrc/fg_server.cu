@@ -41,15 +41,15 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 /// Device bytes of one brick as the engine allocates it: per leaf the value, delta, lookup,
-/// 2L+1 ordered lists, status, status lists, two affected lookups and lists, expansion claim;
-/// per brick the list counts and the allocator's queues.
+/// 2L+1 ordered lists, status, status lists, two affected lookups and lists, expansion claim
+/// and claimed-leaf list; per brick the list counts and the allocator's queues.
 double brick_bytes(int D, int L, const int* part)
 {
 	const int NL = 2 * L + 1;
 	double bv = 1;
 	for (int a = 0; a < D; a++) bv *= part[a];
-	const double leaf = 4 + 4 + 2 + 2.0 * NL + 1 + 2.0 * NL + 2 * 2 + 2 * 2.0 * NL + 8;
-	return bv * leaf + 4.0 * (4 * NL + 6);
+	const double leaf = 4 + 4 + 2 + 2.0 * NL + 1 + 2.0 * NL + 2 * 2 + 2 * 2.0 * NL + 8 + 2;
+	return bv * leaf + 4.0 * (4 * NL + 7);
 }
 
 /// Largest |delta| a builtin speed can produce: |c| + |n| + |a| * D (a node's mean curvature

@@ -59,7 +59,7 @@ def test_reservation_bounds():
 def test_brick_bytes():
     from felt_b200.serving import brick_bytes
     # per leaf phi, delta, lookup, 5 lists, status, 5 status lists, 2 affected lookups,
-    # 2 x 5 affected lists, claim; per brick the list counts and queues
-    assert brick_bytes(2, (8, 8, 8)) == 512 * 63 + 4 * 26
-    assert math.isclose(brick_bytes(3, (16, 16, 16)), 4096 * (4 + 4 + 2 + 14 + 1 + 14 + 4 + 28 + 8)
-                        + 4 * 34)
+    # 2 x 5 affected lists, claim, claimed-leaf list; per brick the list counts and queues
+    assert brick_bytes(2, (8, 8, 8)) == 512 * 65 + 4 * 27
+    assert math.isclose(brick_bytes(3, (16, 16, 16)),
+                        4096 * (4 + 4 + 2 + 14 + 1 + 14 + 4 + 28 + 8 + 2) + 4 * 35)
