@@ -200,6 +200,7 @@ enum {
 	CNT_AQ = 9,       // calc_affected: (partition, list) entries joining the lists
 	CNT_ATOUCH = 10,  // calc_affected: bricks with claimed leaves
 	CNT_ATC = 16,     // calc_affected: per list, partitions joining it (NL entries)
+	CNT_CDONE = 26,   // blocks of the last compaction done (its last block prepares expansion)
 	CNT_N = 32
 };
 

@@ -1360,7 +1360,18 @@ private:
 		for (int k = 1; k <= L; k++) layer_pass(lv, k, 1.0f, b);
 		const CompactArgs ca = take_compact();
 		if (ca.nblocks)
-			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca););
+			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca, 1););
+		else
+			expand_prep();
+	}
+
+	/// What the last compaction's last block does before the expansion, for a pass sequence
+	/// that left none (k_compact with expand_prep).
+	void expand_prep()
+	{
+		scan(P_.spcnt, 0, 1);
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
+		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_CAND, 0, sizeof(int), st_));
 	}
 
 	/// The 2L layer passes as 2L+1 launches (k_dist_fused): launch j runs the second pass of
@@ -1385,7 +1396,7 @@ private:
 			            : CompactArgs{0, nullptr, nullptr, 0, 0};
 		}
 		// the last pass's records: compacted before the flush reads them
-		FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca););
+		FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca, 1););
 	}
 
 	/// A pass's compaction waits to ride on the next first-pass launch (k_dist1).
@@ -1393,7 +1404,7 @@ private:
 	{
 		const CompactArgs stale = take_compact();  // none is left behind on the normal path
 		if (stale.nblocks)
-			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), stale.nblocks, 256, 0, st_, P_, stale););
+			FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), stale.nblocks, 256, 0, st_, P_, stale, 0););
 		pending_ = CompactArgs{P_.S, woff, plist, li, b};
 	}
 	CompactArgs take_compact()
@@ -1433,11 +1444,10 @@ private:
 		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 1024, 0, st_, P_););
 	}
 
+	/// The status lists' entry offsets and the counters were prepared by the last compaction
+	/// of the distance passes (k_compact's last block).
 	void expand()
 	{
-		scan(P_.spcnt, 0, 1);
-		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_ACT, 0, 2 * sizeof(int), st_));
-		FG_CUDA(cudaMemsetAsync(P_.counters + CNT_CAND, 0, sizeof(int), st_));
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 0););
 		FG_RUN("k_activate", st_, launch_pdl((k_activate<L>), sm_count() * 4, 256, 0, st_, P_););
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 1););

@@ -73,21 +73,27 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 // Frozen surfaces (frozen[s] != 0) contribute no entries, so no kernel works on them.
 // ---------------------------------------------------------------------------------------------
 /// One surface count per lane of warp 0 (S <= 32): the scan in registers, no block barrier.
+/// cg: the counts were written by other blocks of the same launch, read past L1.
+static __device__ __forceinline__ int count_at(const int* cnt, int i, bool cg)
+{
+	return cg ? __ldcg(cnt + i) : cnt[i];
+}
 static __device__ __forceinline__ int surface_count(const int* cnt, int NL, int l, int mode, int s,
-                                                    const int* frozen)
+                                                    const int* frozen, bool cg = false)
 {
 	if (frozen && frozen[s]) return 0;
-	if (mode == 0) return cnt[s * NL + l];
-	if (mode == 1) return cnt[s * NL] + cnt[s * NL + NL - 1];
+	if (mode == 0) return count_at(cnt, s * NL + l, cg);
+	if (mode == 1) return count_at(cnt, s * NL, cg) + count_at(cnt, s * NL + NL - 1, cg);
 	int v = 0;
-	for (int t = 0; t < NL; t++) v += cnt[s * NL + t];
+	for (int t = 0; t < NL; t++) v += count_at(cnt, s * NL + t, cg);
 	return v;
 }
 static __device__ __forceinline__ void warp_scan_counts(const int* cnt, int NL, int l, int mode,
-                                                        int S, int* woff, const int* frozen)
+                                                        int S, int* woff, const int* frozen,
+                                                        bool cg = false)
 {
 	const int lane = lane_id();
-	int v = lane < S ? surface_count(cnt, NL, l, mode, lane, frozen) : 0;
+	int v = lane < S ? surface_count(cnt, NL, l, mode, lane, frozen, cg) : 0;
 #pragma unroll
 	for (int o = 1; o < 32; o <<= 1) {
 		const int y = __shfl_up_sync(FULL, v, o);
@@ -98,10 +104,10 @@ static __device__ __forceinline__ void warp_scan_counts(const int* cnt, int NL, 
 }
 
 static __device__ __noinline__ void d_scan_counts(const int* cnt, int NL, int l, int mode, int S,
-                                                  int* woff, const int* frozen)
+                                                  int* woff, const int* frozen, bool cg = false)
 {
 	if (S <= 32) {
-		if (threadIdx.x < 32) warp_scan_counts(cnt, NL, l, mode, S, woff, frozen);
+		if (threadIdx.x < 32) warp_scan_counts(cnt, NL, l, mode, S, woff, frozen, cg);
 		__syncthreads();
 		return;
 	}
@@ -113,15 +119,7 @@ static __device__ __noinline__ void d_scan_counts(const int* cnt, int NL, int l,
 	__syncthreads();
 	for (int base = 0; base < S; base += blockDim.x) {
 		const int s = base + threadIdx.x;
-		int v = 0;
-		if (s < S && !(frozen && frozen[s])) {
-			if (mode == 0)
-				v = cnt[s * NL + l];
-			else if (mode == 1)
-				v = cnt[s * NL] + cnt[s * NL + NL - 1];
-			else
-				for (int t = 0; t < NL; t++) v += cnt[s * NL + t];
-		}
+		const int v = s < S ? surface_count(cnt, NL, l, mode, s, frozen, cg) : 0;
 		int tot;
 		const int ex = block_excl_scan(v, &tot);
 		if (s < S) woff[s + 1] = carry + ex + v;
@@ -762,10 +760,31 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 
 /// The compaction of one pass on its own launch, one block per surface.
 template <int L>
-__global__ void __launch_bounds__(256) k_compact(Dev P, CompactArgs a)
+__global__ void __launch_bounds__(256) k_compact(Dev P, CompactArgs a, int expand_prep)
 {
+	constexpr int NL = 2 * L + 1;
 	pdl_enter();
 	compact_surface<L>(P, a, blockIdx.x);
+	if (!expand_prep) return;
+	// The last pass's compaction completes the status partition lists; its last block to
+	// finish prepares the expansion: the entry offsets of the outer status lists (the counts
+	// the other blocks wrote, read past L1) and the expansion's counters reset.
+	__shared__ int last;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		__threadfence();
+		last = atomicAdd(&P.counters[CNT_CDONE], 1) == (int)gridDim.x - 1;
+	}
+	__syncthreads();
+	if (!last) return;
+	__threadfence();
+	d_scan_counts(P.spcnt, NL, 0, 1, P.S, P.woff, P.sfrozen, true);
+	if (threadIdx.x == 0) {
+		P.counters[CNT_ACT] = 0;
+		P.counters[CNT_TOUCH] = 0;
+		P.counters[CNT_CAND] = 0;
+		P.counters[CNT_CDONE] = 0;
+	}
 }
 
 /// update_distance first pass (Surface.hpp:1028-1073): distance of every leaf of layer k to
