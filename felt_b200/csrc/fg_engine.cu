@@ -1350,8 +1350,11 @@ private:
 	/// entry offsets of every layer up front.
 	void distance_passes(const ListView& lv, int b)
 	{
-		FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
-		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L););
+		// entry offsets of every layer, then the entries decoded; one launch for small pools
+		const bool small = P_.S <= 32;
+		if (!small)
+			FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
+		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L, small ? lv.pcnt : nullptr););
 		if (fused_ && lv.lkp) {
 			fused_passes(lv, b);
 			return;
@@ -1472,8 +1475,9 @@ private:
 
 	void clear_buffer(int b)
 	{
-		scan(P_.apcnt[b], 0, 2);
-		FG_RUN("k_clear_buffer", st_, launch_pdl((k_clear_buffer<L>), warp_grid_, 256, 0, st_, P_, b););
+		const bool small = P_.S <= 32;
+		if (!small) scan(P_.apcnt[b], 0, 2);
+		FG_RUN("k_clear_buffer", st_, launch_pdl((k_clear_buffer<L>), warp_grid_, 256, 0, st_, P_, b, small ? 1 : 0););
 		FG_CUDA(cudaMemsetAsync(P_.apcnt[b], 0, (size_t)P_.S * NL * sizeof(int), st_));
 		buf_dirty_[b] = false;
 	}

@@ -176,15 +176,33 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 /// layer and every entry e of its list (entry offsets woffl), {partition, brick slot, surface,
 /// leaves in the brick's list} at etab[l*NP + e]. The passes then start from one 16-byte load
 /// instead of the chain entry offsets -> partition list -> slot -> list count.
-static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, int NL, int L)
+///
+/// pcnt given (a pool of at most 32 surfaces): the entry offsets are scanned here too, every
+/// block for itself (a warp per layer) and block 0 for the passes (Dev::woffl), in place of
+/// k_scan_layers.
+static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, int NL, int L,
+                                     const int* pcnt)
 {
-	__shared__ int lo[10];  // the layers' entries concatenated: layer l from lo[l]
+	__shared__ int lo[10];          // the layers' entries concatenated: layer l from lo[l]
+	__shared__ int swoff[9 * 33];   // the offsets, when scanned here
 	pdl_enter();
+	const int* woffl = P.woffl;
+	if (pcnt) {
+		for (int w = threadIdx.x >> 5; w < NL; w += blockDim.x >> 5) {
+			warp_scan_counts(pcnt, NL, w, 0, P.S, swoff + w * (P.S + 1), P.sfrozen);
+			__syncwarp();
+			if (blockIdx.x == 0)
+				for (int i = lane_id(); i <= P.S; i += 32)
+					P.woffl[(size_t)w * (P.S + 1) + i] = swoff[w * (P.S + 1) + i];
+		}
+		__syncthreads();
+		woffl = swoff;
+	}
 	if (threadIdx.x == 0) {
 		int c = 0;
 		for (int l = 0; l < NL; l++) {
 			lo[l] = c;
-			if (l != L) c += P.woffl[(size_t)l * (P.S + 1) + P.S];
+			if (l != L) c += woffl[(size_t)l * (P.S + 1) + P.S];
 		}
 		lo[NL] = c;
 	}
@@ -194,7 +212,7 @@ static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, i
 		int l = 0;
 		while (t >= lo[l + 1]) l++;
 		const int e = t - lo[l];
-		const int* woff = P.woffl + (size_t)l * (P.S + 1);
+		const int* woff = woffl + (size_t)l * (P.S + 1);
 		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
 		const int gp = g.pbase + plist[(size_t)l * P.NP + g.pbase + (e - woff[s])];
@@ -2068,14 +2086,14 @@ __global__ void k_clear_status(Dev P)
 
 /// Affected buffer reset: clears the leaf lookups and lists of buffer b.
 template <int L>
-__device__ void d_clear_buffer(const Dev& P, int b, GridPos G)
+__device__ void d_clear_buffer(const Dev& P, int b, GridPos G, const int* woff)
 {
 	constexpr int NL = 2 * L + 1;
-	FG_WARP_LOOP(P.woff)
+	FG_WARP_LOOP(woff)
 	{
-		const int s = entry_surface(P.woff, P.S, e);
+		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
-		int i = e - P.woff[s];
+		int i = e - woff[s];
 		int t = 0;
 		while (i >= P.apcnt[b][s * NL + t]) {
 			i -= P.apcnt[b][s * NL + t];
@@ -2093,11 +2111,21 @@ __device__ void d_clear_buffer(const Dev& P, int b, GridPos G)
 		if (lane == 0) P.appos[b][gp * NL + t] = -1;
 	}
 }
+/// scan_here (a pool of at most 32 surfaces): every block scans the buffer's entry offsets
+/// itself (one warp), in place of a k_scan_counts launch before.
 template <int L>
-__global__ void k_clear_buffer(Dev P, int b)
+__global__ void k_clear_buffer(Dev P, int b, int scan_here)
 {
+	constexpr int NL = 2 * L + 1;
+	__shared__ int swoff[33];
 	pdl_enter();
-	d_clear_buffer<L>(P, b, hw_grid());
+	const int* woff = P.woff;
+	if (scan_here) {
+		if (threadIdx.x < 32) warp_scan_counts(P.apcnt[b], NL, 0, 2, P.S, swoff, P.sfrozen);
+		__syncthreads();
+		woff = swoff;
+	}
+	d_clear_buffer<L>(P, b, hw_grid(), woff);
 }
 
 /// Returns the bricks of partitions deactivated in this iteration to the free pool.
