@@ -1354,9 +1354,9 @@ def main():
     ap.add_argument("--delta-kernel", type=int, default=0, choices=[0, 1, 2],
                     help="fg_config.delta_kernel: the curvature speed functor 1 reading the pool "
                          "directly, 2 over bricks staged with their halo (0 = automatic)")
-    ap.add_argument("--fuse-passes", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--fuse-passes", type=int, default=0, choices=[0, 1, 2, 3],
                     help="fg_config.fuse_passes: the distance passes 1 as 4L launches, 2 as 2L+1 "
-                         "fused ones (0 = automatic)")
+                         "fused ones, 3 tiled per brick in shared memory (0 = automatic)")
     ap.add_argument("--dist-split", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="fg_config.dist_split: warps per partition entry in the first distance "
                          "pass (0 = automatic)")

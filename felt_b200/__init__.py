@@ -50,7 +50,7 @@ def make_config(brick_capacity=0, vertex_capacity=0, launch_mode=0, dist_split=0
     update as one CUDA graph, 2 every kernel launched from the host, no graphs; dist_split warps per partition
     entry in the first distance pass; record_passes 1 warp / 2 block per entry in the
     recording passes; delta_kernel of curvature speeds 1 direct / 2 staged brick + halo;
-    fuse_passes 1 separate / 2 fused distance passes;
+    fuse_passes 1 separate / 2 fused / 3 tiled (per brick in shared memory) distance passes;
     0 = automatic everywhere; autotune: dist_split and record_passes left at 0 take the values
     autotune() measures)."""
     return Config(int(brick_capacity), int(vertex_capacity), int(launch_mode), int(dist_split),

@@ -70,8 +70,8 @@ void apply_tuning(fg::EngineBase& eng, const fg_config* cfg)
 	}
 	if (cfg->delta_kernel < 0 || cfg->delta_kernel > 2)
 		throw fg::Error(FG_ERR_ARG, "delta_kernel must be 0, 1 or 2");
-	if (cfg->fuse_passes < 0 || cfg->fuse_passes > 2)
-		throw fg::Error(FG_ERR_ARG, "fuse_passes must be 0, 1 or 2");
+	if (cfg->fuse_passes < 0 || cfg->fuse_passes > 3)
+		throw fg::Error(FG_ERR_ARG, "fuse_passes must be 0, 1, 2 or 3");
 	eng.set_tuning(cfg->launch_mode, ds, rp, cfg->delta_kernel, cfg->fuse_passes);
 }
 

@@ -171,6 +171,8 @@ struct Dev {
 	int* woff;        // [S+1] entry offsets of the current pass
 	int* woffl;       // [NL*(S+1)] entry offsets of every layer's list, for the distance passes
 	int4* etab;       // [NL*NP] the distance passes' entries decoded (k_entry_table)
+	int* dq;          // [nslots] partitions of the tiled distance passes (k_entry_table)
+	unsigned* eflagl; // [NL*NP] entry flags of every layer's pass (tiled distance passes)
 	int* sfrozen;     // [S] surfaces stopped after a non-terminating update (no further work)
 	int* err;         // [1] error bits
 	int* changed;     // [1] status-change flag of the distance passes
@@ -201,6 +203,7 @@ enum {
 	CNT_ATOUCH = 10,  // calc_affected: bricks with claimed leaves
 	CNT_ATC = 16,     // calc_affected: per list, partitions joining it (NL entries)
 	CNT_CDONE = 26,   // blocks of the last compaction done (its last block prepares expansion)
+	CNT_DQ = 27,      // partitions queued for the tiled distance passes
 	CNT_N = 32
 };
 

@@ -236,6 +236,8 @@ public:
 		P.woff = dalloc<int>(S + 1, o);
 		P.woffl = dalloc<int>((size_t)NL * (S + 1), o);
 		P.etab = dalloc<int4>((size_t)NL * NP, o);
+		P.dq = dalloc<int>(nslots, o);
+		P.eflagl = dalloc<unsigned>(npl, o);
 		P.sfrozen = dalloc<int>(S, o);
 		FG_CUDA(cudaMemsetAsync(P.sfrozen, 0, S * sizeof(int), st_));
 		frozen_.assign(S, 0);
@@ -321,6 +323,35 @@ public:
 		} else {
 			smem_flush_ = 0;  // brick too large to stage: replay in global memory
 		}
+		// tiled distance passes: the brick with a halo of 2L nodes per side in shared memory
+		// (the halo may reach no further than the next partition along each axis)
+		{
+			TileShape t{};
+			t.H = 2 * L;
+			t.NT = 1;
+			bool ok = true;
+			for (int a = 2; a >= 0; a--) {
+				t.T[a] = a < D ? csz_[a] + 2 * t.H : 1;
+				t.ts[a] = t.NT;
+				t.NT *= t.T[a];
+				if (a < D && t.H > csz_[a]) ok = false;
+			}
+			tiled_threads_ = t.NT >= 4096 ? 1024 : 256;
+			smem_tiled_ = tiled_smem_bytes(t.NT, tiled_threads_);
+			if (ok && smem_tiled_ <= 220 * 1024) {
+				if (smem_tiled_ > 48 * 1024)
+					FG_CUDA(cudaFuncSetAttribute(k_dist_tiled<D, L>,
+					                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+					                             (int)smem_tiled_));
+				int per_sm = 0;
+				FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+				    &per_sm, k_dist_tiled<D, L>, tiled_threads_, smem_tiled_));
+				tiled_grid_ = sm_count() * std::max(1, per_sm);
+				tile_ = t;
+			} else {
+				smem_tiled_ = 0;
+			}
+		}
 	}
 
 public:
@@ -332,8 +363,15 @@ public:
 	void set_tuning(int launch_mode, int dist_split, int record_passes, int delta_kernel,
 	                int fuse_passes) override
 	{
-		if (fuse_passes == 1) fused_ = false;
-		if (fuse_passes == 2) fused_ = true;
+		if (fuse_passes == 1) fused_ = tiled_ = false;
+		if (fuse_passes == 2) {
+			fused_ = true;
+			tiled_ = false;
+		}
+		if (fuse_passes == 3) {
+			fused_ = false;
+			tiled_ = smem_tiled_ != 0;
+		}
 		launch_mode_ = launch_mode;
 		if (dist_split > 0) dist_split_ = dist_split;
 		if (record_passes == 1) block_passes_ = false;
@@ -348,7 +386,7 @@ public:
 		out[1] = dist_split_;
 		out[2] = block_passes_ ? 2 : 1;
 		out[3] = delta_staged_ ? 2 : 1;
-		out[4] = fused_ ? 2 : 1;
+		out[4] = tiled_ ? 3 : fused_ ? 2 : 1;
 	}
 
 private:
@@ -554,7 +592,7 @@ private:
 	{
 		const int B = 1;  // buffers: B = m_grid_affected_buffer, A = m_grid_affected
 		if (!woff_ready) scan(P_.pcnt, L, 0);
-		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt, P_.lkp};
+		const ListView iso{P_.plist, P_.pcnt, P_.lst, P_.lcnt, P_.lkp, P_.ppos};
 		zero_apply(iso, nullptr, B);
 		defer_compact(P_.woff, P_.plist, L, B);
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
@@ -731,7 +769,7 @@ private:
 		FG_CUDA(cudaMemsetAsync(P_.changed, 0, sizeof(int), st_));
 		// the fused passes (lookup given) on the global update's iterations only
 		const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur],
-		                  local ? nullptr : P_.alkp[cur]};
+		                  local ? nullptr : P_.alkp[cur], P_.appos[cur]};
 		distance_passes(bv, oth);
 		flush();
 		expand();
@@ -1354,7 +1392,12 @@ private:
 		const bool small = P_.S <= 32;
 		if (!small)
 			FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
-		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L, small ? lv.pcnt : nullptr););
+		const bool tiled = tiled_ && lv.lkp && lv.ppos;
+		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L, small ? lv.pcnt : nullptr, lv.ppos, tiled ? P_.dq : nullptr););
+		if (tiled) {
+			tiled_passes(lv, b);
+			return;
+		}
 		if (fused_ && lv.lkp) {
 			fused_passes(lv, b);
 			return;
@@ -1400,6 +1443,17 @@ private:
 		}
 		// the last pass's records: compacted before the flush reads them
 		FG_RUN("k_compact", st_, launch_pdl((k_compact<L>), ca.nblocks, 256, 0, st_, P_, ca, 1););
+	}
+
+	/// The 2L layer passes as two launches: k_dist_tiled runs every pass of a brick in shared
+	/// memory (a block per brick of the passes' lists, queued by k_entry_table), then
+	/// k_dist_tiled_end commits the results and compacts the records of the zero-layer update
+	/// (pending from before the passes) and of the passes in pass order.
+	void tiled_passes(const ListView& lv, int b)
+	{
+		const CompactArgs stale = take_compact();
+		FG_RUN("k_dist_tiled", st_, launch_pdl((k_dist_tiled<D, L>), tiled_grid_, tiled_threads_, smem_tiled_, st_, P_, lv, b, tile_););
+		FG_RUN("k_dist_tiled_end", st_, launch_pdl((k_dist_tiled_end<L>), P_.S + sm_count() * 4, 256, 0, st_, P_, lv, b, stale););
 	}
 
 	/// A pass's compaction waits to ride on the next first-pass launch (k_dist1).
@@ -1511,6 +1565,13 @@ private:
 	// launches instead of 4L, but no faster on C2 (1.33 against 1.28 ms per step), so off
 	// unless asked for
 	bool fused_ = false;
+	// the 2L distance passes per brick in shared memory (k_dist_tiled); smem_tiled_ = 0 where
+	// the brick with its halo does not fit
+	bool tiled_ = false;
+	TileShape tile_{};
+	size_t smem_tiled_ = 0;
+	int tiled_threads_ = 256;
+	int tiled_grid_ = 0;
 	Speed* d_speeds_ = nullptr;
 	size_t smem_sort_ = 0;
 	size_t smem_flush_ = 0;

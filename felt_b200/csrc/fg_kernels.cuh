@@ -21,6 +21,7 @@ struct ListView {
 	const uint16_t* lst;
 	const int* lcnt;
 	const uint16_t* lkp = nullptr;
+	const int* ppos = nullptr;  // [NP*NL] position of a partition in plist's list, -1 = none
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -180,8 +181,13 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 /// pcnt given (a pool of at most 32 surfaces): the entry offsets are scanned here too, every
 /// block for itself (a warp per layer) and block 0 for the passes (Dev::woffl), in place of
 /// k_scan_layers.
+///
+/// dq given (tiled distance passes, ppos the lists' partition positions): every partition of the
+/// passes is queued once, at its entry in the lowest layer index whose list holds it, and every
+/// entry's flags (Dev::eflagl) start at zero.
 static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, int NL, int L,
-                                     const int* pcnt)
+                                     const int* pcnt, const int* ppos = nullptr,
+                                     int* dq = nullptr)
 {
 	__shared__ int lo[10];          // the layers' entries concatenated: layer l from lo[l]
 	__shared__ int swoff[9 * 33];   // the offsets, when scanned here
@@ -218,6 +224,13 @@ static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, i
 		const int gp = g.pbase + plist[(size_t)l * P.NP + g.pbase + (e - woff[s])];
 		const int sl = P.slot[gp];
 		P.etab[(size_t)l * P.NP + e] = make_int4(gp, sl, s, lcnt[sl * NL + l]);
+		if (dq) {
+			P.eflagl[(size_t)l * P.NP + e] = 0;
+			bool first = true;
+			for (int l2 = 0; l2 < l; l2++)
+				if (l2 != L && ppos[gp * NL + l2] >= 0) first = false;
+			if (first) dq[atomicAdd(&P.counters[CNT_DQ], 1)] = gp;
+		}
 	}
 }
 
@@ -708,6 +721,8 @@ struct CompactArgs {
 	int li;             // its layer index
 	int b;              // affected buffer its changes went to
 	const unsigned* ef = nullptr;  // its entry flags (nullptr = Dev::eflag)
+	int dedup = 0;      // 1: a partition already in a buffer list is not appended again (the
+	                    // pass recorded before the compaction of the passes ahead of it)
 };
 
 template <int L>
@@ -744,7 +759,9 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 			int cnt = scnt[t];
 			for (int base = 0; base < nt; base += 32) {
 				const int i = base + lane;
-				const bool hit = i < nt && (sf[i] & bit);
+				const bool hit = i < nt && (sf[i] & bit) &&
+				                 (status || !a.dedup ||
+				                  P.appos[b][(g.pbase + slp[i]) * NL + t] < 0);
 				const unsigned m = __ballot_sync(FULL, hit);
 				if (hit) {
 					const int lp = slp[i];
@@ -1101,6 +1118,262 @@ __global__ void __launch_bounds__(256) k_dist_fused(Dev P, ListView lv, FusedPas
 		if (lane == 0 && part == 0) done += n;
 	}
 	block_add(&P.kstat[KS_DIST], done);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tiled distance passes. The 2L passes of update_distance (Surface.hpp:989-1125; layers -1..-L,
+// then +1..+L, each a first loop writing distance() of every leaf of the layer's list into the
+// delta grid and a second loop committing it) run for one brick at a time in shared memory: the
+// block stages the brick with a halo of H = 2L nodes on every side (isogrid values, the list
+// each node belongs to), runs every pass over the whole tile, and keeps the brick's own results.
+// A node's value after pass m depends on nodes at most m steps away, so after the 2L passes the
+// brick's nodes hold exactly what the reference's passes give them; the halo's work is
+// redundant (other blocks own those nodes). The status changes of each pass are recorded over
+// the brick's own list in list order, as in the untiled second pass; the entry flags of every
+// pass go to their own array (Dev::eflagl), and the next launch commits the values and compacts
+// the passes' records in pass order. Nothing is written to the isogrid during the passes,
+// because other blocks are still staging their halos from it: the results go to the delta grid
+// (where the untiled first pass puts them too) and the next launch copies them over.
+// ---------------------------------------------------------------------------------------------
+
+/// The staged tile: the brick (partition shape) with a halo of H nodes on every side.
+struct TileShape {
+	int T[3];   // extent per axis
+	int ts[3];  // strides, row-major, last axis fastest
+	int NT;     // nodes
+	int H;      // halo width
+};
+
+/// Dynamic shared memory of k_dist_tiled: values and new values (float), the status-round
+/// scratch (int, uint16 per thread) and the list index of every node (byte).
+__host__ __device__ inline size_t tiled_smem_bytes(int NT, int threads)
+{
+	return (size_t)NT * 9 + (size_t)threads * 6 + 16;
+}
+
+/// Layer index of the list that holds `leaf` of brick sl (lookup position lk, not NUL16), or
+/// 0xFF: the list its value rounds to is tried first, then the others.
+template <int L>
+__device__ __forceinline__ int tiled_member(const ListView& lv, const int* cnt, int sl, int BV,
+                                            int leaf, int lk, float v)
+{
+	constexpr int NL = 2 * L + 1;
+	const float x = __fadd_rn(v, 1.1920928955078125e-07f);
+	int h = 0;
+	if (isfinite(x)) h = x >= (float)L ? L : x <= (float)-L ? -L : (int)roundf(x);
+	const int h0 = h + L;
+	if (lk < cnt[h0] && lv.lst[((size_t)sl * NL + h0) * BV + lk] == leaf) return h0;
+	for (int l = 0; l < NL; l++)
+		if (l != h0 && lk < cnt[l] && lv.lst[((size_t)sl * NL + l) * BV + lk] == leaf) return l;
+	return 0xFF;
+}
+
+/// One block per queued partition (persistent grid): stage, 2L passes, records per pass.
+template <int D, int L>
+__global__ void __launch_bounds__(1024, 1) k_dist_tiled(Dev P, ListView lv, int b, TileShape ts)
+{
+	constexpr int NL = 2 * L + 1;
+	constexpr int NN = D == 3 ? 27 : 9;  // the partition and its neighbours, offsets in {-1,0,1}^D
+	constexpr int CTR = (NN - 1) / 2;     // the partition itself
+	extern __shared__ __align__(16) unsigned char tsm[];
+	float* ph = reinterpret_cast<float*>(tsm);
+	float* nv = ph + ts.NT;
+	int* ct = reinterpret_cast<int*>(nv + ts.NT);
+	uint16_t* cl = reinterpret_cast<uint16_t*>(ct + blockDim.x);
+	uint8_t* mb = reinterpret_cast<uint8_t*>(cl + blockDim.x);
+	__shared__ int nsl[NN];
+	__shared__ float nbg[NN];
+	__shared__ int ncnt[NN * NL];
+	pdl_enter();
+	const int nq = P.counters[CNT_DQ];
+	const int H = ts.H;
+	const float qnan = __int_as_float(0x7fc00000);
+	unsigned long long done = 0;
+	for (int q = blockIdx.x; q < nq; q += gridDim.x) {
+		const int gp = P.dq[q];
+		const int sl = P.slot[gp];
+		const int s = P.surf_of[gp];
+		const SurfGeom& g = P.geom[s];
+		__syncthreads();  // the previous partition's shared state is no longer read
+		if (threadIdx.x < NN) {
+			int lp = gp - g.pbase, r = threadIdx.x, gp2 = gp, cst = 1;
+			bool ok = true;
+#pragma unroll
+			for (int a = D - 1; a >= 0; a--) {
+				const int c = lp % g.ccount[a];
+				lp /= g.ccount[a];
+				const int o = r % 3 - 1;
+				r /= 3;
+				if (c + o < 0 || c + o >= g.ccount[a]) ok = false;
+				gp2 += o * cst;
+				cst *= g.ccount[a];
+			}
+			const int sl2 = ok ? P.slot[gp2] : -2;
+			nsl[threadIdx.x] = sl2;
+			nbg[threadIdx.x] = (ok && sl2 < 0) ? P.bg[gp2] : 0.0f;
+			for (int l = 0; l < NL; l++)
+				ncnt[threadIdx.x * NL + l] = sl2 >= 0 ? lv.lcnt[sl2 * NL + l] : 0;
+		}
+		__syncthreads();
+		// stage: value (NaN outside the grid, where distance() reads nothing) and list index
+		// (0xFF: none, or a node on the tile's outer face, whose neighbours are not all staged)
+		int po[D];
+#pragma unroll
+		for (int a = 0; a < D; a++) po[a] = P.porig[gp * 3 + a] - H;
+		for (int t = threadIdx.x; t < ts.NT; t += blockDim.x) {
+			int rem = t, ni = 0, leaf = 0;
+			bool in = true, face = false;
+#pragma unroll
+			for (int a = 0; a < D; a++) {
+				const int c = rem / ts.ts[a];
+				rem -= c * ts.ts[a];
+				const int p = po[a] + c;
+				in = in && p >= g.off[a] && p < g.hi[a];
+				face = face || c == 0 || c == ts.T[a] - 1;
+				const int o = c < H ? -1 : (c >= H + P.csz[a] ? 1 : 0);
+				ni = ni * 3 + o + 1;
+				leaf += (c - H - o * P.csz[a]) * P.lstr[a];
+			}
+			float v = qnan;
+			int m = 0xFF;
+			if (in) {
+				const int sl2 = nsl[ni];
+				if (sl2 < 0) {
+					v = nbg[ni];
+				} else {
+					const size_t i = (size_t)sl2 * P.BV + leaf;
+					v = P.phi[i];
+					const int lk = lv.lkp[i];
+					if (!face && lk != NUL16)
+						m = tiled_member<L>(lv, ncnt + ni * NL, sl2, P.BV, leaf, lk, v);
+				}
+			}
+			ph[t] = v;
+			mb[t] = (uint8_t)m;
+		}
+		__syncthreads();
+		const size_t b0 = (size_t)sl * P.BV;
+		for (int pm = 0; pm < 2 * L; pm++) {
+			const int k = pm < L ? -(pm + 1) : pm - L + 1;
+			const int li = k + L;
+			const float dir = k < 0 ? -1.0f : 1.0f;
+			// first loop: distance() of every member of the layer in the tile (Jacobi)
+			for (int t = threadIdx.x; t < ts.NT; t += blockDim.x) {
+				if (mb[t] != li) continue;
+				float dist = __fmul_rn(ph[t], dir);
+#pragma unroll
+				for (int a = 0; a < D; a++) {
+#pragma unroll
+					for (int sg = -1; sg <= 1; sg += 2) {
+						const float dn = __fmul_rn(ph[t + sg * ts.ts[a]], dir);
+						if (dn < dist) dist = dn;
+					}
+				}
+				nv[t] = __fadd_rn(__fmul_rn(dist, dir), dir);
+			}
+			__syncthreads();
+			// second loop: commit
+			for (int t = threadIdx.x; t < ts.NT; t += blockDim.x)
+				if (mb[t] == li) ph[t] = nv[t];
+			__syncthreads();
+			// the brick's own leaves of the layer, in list order: result and status records
+			const int pp = lv.ppos[gp * NL + li];
+			if (pp < 0) continue;  // block-uniform: the partition is not in this layer's list
+			const int n = ncnt[CTR * NL + li];
+			const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
+			unsigned flags = 0;
+			bool any = false;
+			StatusCache sc;
+			for (int base = 0; base < n; base += blockDim.x) {
+				const int j = base + threadIdx.x;
+				int leaf = 0, to = k;
+				if (j < n) {
+					leaf = lst[j];
+					int rem = leaf, ti = 0;
+#pragma unroll
+					for (int a = 0; a < D; a++) {
+						const int c = rem / P.lstr[a];
+						rem -= c * P.lstr[a];
+						ti += (c + H) * ts.ts[a];
+					}
+					const float d = ph[ti];
+					P.dlt[b0 + leaf] = d;
+					to = layer_id(d, P.err);
+				}
+				status_round<L>(P, gp, sl, k, j < n && to != k, leaf, to, b, flags, any, cl, ct,
+				                sc);
+			}
+			if (threadIdx.x < 32) {
+				status_store<L>(P, sl, k, b, sc);
+				flags = warp_or(flags);
+				if (threadIdx.x == 0) {
+					const int e = P.woffl[(size_t)li * (P.S + 1) + s] + pp;
+					P.eflagl[(size_t)li * P.NP + e] = flags;
+					if (any && !*(volatile int*)P.changed) atomicOr(P.changed, 1);
+					done += n;
+				}
+			}
+		}
+	}
+	block_add(&P.kstat[KS_DIST], done);
+}
+
+/// After k_dist_tiled: the first P.S blocks compact the records of the pending zero-layer update
+/// (`stale`, if any) and of the 2L passes in pass order, one block per surface, a partition
+/// joining a buffer list once (dedup: the passes recorded before any of these compactions ran);
+/// the other blocks copy the passes' results from the delta grid into the isogrid, a warp per
+/// (partition, layer). The last block to finish prepares the expansion (as k_compact's does) and
+/// empties the partition queue.
+template <int L>
+__global__ void __launch_bounds__(256) k_dist_tiled_end(Dev P, ListView lv, int b, CompactArgs stale)
+{
+	constexpr int NL = 2 * L + 1;
+	pdl_enter();
+	if ((int)blockIdx.x < P.S) {
+		const int s = blockIdx.x;
+		if (stale.nblocks) compact_surface<L>(P, stale, s);
+		for (int pm = 0; pm < 2 * L; pm++) {
+			const int li = (pm < L ? -(pm + 1) : pm - L + 1) + L;
+			CompactArgs a{P.S, P.woffl + (size_t)li * (P.S + 1), lv.plist, li, b,
+			              P.eflagl + (size_t)li * P.NP};
+			a.dedup = 1;
+			compact_surface<L>(P, a, s);
+		}
+	} else {
+		const int nq = P.counters[CNT_DQ];
+		const int lane = lane_id();
+		const int nw = ((gridDim.x - P.S) * blockDim.x) >> 5;
+		for (int v = ((blockIdx.x - P.S) * blockDim.x + threadIdx.x) >> 5; v < nq * 2 * L;
+		     v += nw) {
+			const int q = v / (2 * L), pm = v - q * (2 * L);
+			const int li = pm < L ? pm : pm + 1;  // every layer but the zero layer
+			const int sl = P.slot[P.dq[q]];
+			const int n = lv.lcnt[sl * NL + li];
+			const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
+			const size_t b0 = (size_t)sl * P.BV;
+			for (int j = lane; j < n; j += 32) {
+				const int leaf = lst[j];
+				P.phi[b0 + leaf] = P.dlt[b0 + leaf];
+			}
+		}
+	}
+	__shared__ int last;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		__threadfence();
+		last = atomicAdd(&P.counters[CNT_CDONE], 1) == (int)gridDim.x - 1;
+	}
+	__syncthreads();
+	if (!last) return;
+	__threadfence();
+	d_scan_counts(P.spcnt, NL, 0, 1, P.S, P.woff, P.sfrozen, true);
+	if (threadIdx.x == 0) {
+		P.counters[CNT_ACT] = 0;
+		P.counters[CNT_TOUCH] = 0;
+		P.counters[CNT_CAND] = 0;
+		P.counters[CNT_CDONE] = 0;
+		P.counters[CNT_DQ] = 0;
+	}
 }
 
 // ---------------------------------------------------------------------------------------------

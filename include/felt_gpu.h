@@ -82,7 +82,10 @@ typedef struct fg_config {
 	                          0 = automatic                                                  */
 	int fuse_passes;       /* the global update's 2L distance-pass pairs: 1 as 4L launches,
 	                          2 as 2L+1 launches (each the second pass of one layer with the
-	                          first pass of the next); 0 = automatic                         */
+	                          first pass of the next), 3 as two launches: every pass of a
+	                          brick in shared memory, the brick staged with a halo of 2L
+	                          nodes (where that fits and reaches only the next partitions;
+	                          elsewhere as 1); 0 = automatic                                 */
 	int reserved[2];
 } fg_config;
 

@@ -115,7 +115,8 @@ def test_step_graph_between_local_updates():
 @pytest.mark.parametrize("tuning", [dict(dist_split=1), dict(dist_split=8),
                                     dict(record_passes=1), dict(record_passes=2),
                                     dict(delta_kernel=1), dict(delta_kernel=2),
-                                    dict(fuse_passes=1), dict(fuse_passes=2)],
+                                    dict(fuse_passes=1), dict(fuse_passes=2),
+                                    dict(fuse_passes=3)],
                          ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
 def test_tuning_knobs_keep_results(tuning):
     size, part, L, seed, sched = CASES[1]
@@ -127,6 +128,24 @@ def test_tuning_knobs_keep_results(tuning):
         for (da, pa), (db, pb) in zip(sa, sref):
             assert first_difference(da, db) is None
             assert np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[0])))
+@pytest.mark.parametrize("mode", [1, 2])
+def test_tiled_passes_match_oracle(case, mode):
+    """fuse_passes 3 (every distance pass of a brick in shared memory, the brick staged with a
+    halo of 2L nodes) against the oracle: lists, orders and values after every segment."""
+    size, part, L, seed, sched = case
+    g, sg, _ = _run(mode, size, part, L, seed, sched, fuse_passes=3)
+    assert g.tuning()["fuse_passes"] == 3
+    o = O.Surface(size, part, L)
+    o.seed(seed)
+    for (n, kw), (dg, pg) in zip(sched, sg):
+        for _ in range(n):
+            o.update(**kw)
+        d = first_difference(dg, o.dump())
+        assert d is None, d
+        assert float(np.abs(pg - o.snapshot()).max()) <= 1e-5
 
 
 def test_batch_step_graph_equals_phase_by_phase_with_a_stopped_surface():
