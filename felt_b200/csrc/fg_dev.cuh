@@ -204,6 +204,7 @@ enum {
 	CNT_ATC = 16,     // calc_affected: per list, partitions joining it (NL entries)
 	CNT_CDONE = 26,   // blocks of the last compaction done (its last block prepares expansion)
 	CNT_DQ = 27,      // partitions queued for the tiled distance passes
+	CNT_LDONE = 28,   // blocks done of a launch whose last block resets counters (last_block)
 	CNT_N = 32
 };
 

@@ -39,6 +39,25 @@ __device__ __forceinline__ void block_add(unsigned long long* dst, unsigned long
 	if (threadIdx.x == 0 && acc) atomicAdd(dst, acc);
 }
 
+/// True in exactly one block of the launch, the last to arrive; every thread of every block
+/// calls it once, after the block's work. The arrival counter is left at zero for the next
+/// launch. Where it returns true, every other block's global reads and writes are complete, so
+/// that block may reset what the launch read (the update's graph then needs no memset nodes,
+/// which would break the chain of programmatic launches).
+__device__ __forceinline__ bool last_block(int* counter)
+{
+	__shared__ int last;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		__threadfence();
+		last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+		if (last) *counter = 0;
+	}
+	__syncthreads();
+	if (last) __threadfence();
+	return last;
+}
+
 /// Exclusive block scan of one int per thread; returns the prefix, total in *total.
 __device__ __forceinline__ int block_excl_scan(int v, int* total)
 {
@@ -173,7 +192,8 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 	d_scan_layers(cnt, NL, S, woffl, frozen);
 }
 
-/// The entries of the distance passes decoded once per iteration: for every layer but the zero
+/// The entries of the distance passes decoded once per iteration, and Dev::changed cleared for
+/// the passes: for every layer but the zero
 /// layer and every entry e of its list (entry offsets woffl), {partition, brick slot, surface,
 /// leaves in the brick's list} at etab[l*NP + e]. The passes then start from one 16-byte load
 /// instead of the chain entry offsets -> partition list -> slot -> list count.
@@ -192,6 +212,8 @@ static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, i
 	__shared__ int lo[10];          // the layers' entries concatenated: layer l from lo[l]
 	__shared__ int swoff[9 * 33];   // the offsets, when scanned here
 	pdl_enter();
+	// the passes' status-change flag starts at zero (nothing before the passes reads it)
+	if (blockIdx.x == 0 && threadIdx.x == 0) *P.changed = 0;
 	const int* woffl = P.woffl;
 	if (pcnt) {
 		for (int w = threadIdx.x >> 5; w < NL; w += blockDim.x >> 5) {
@@ -2353,8 +2375,12 @@ __device__ void d_clear_status(const Dev& P, GridPos G)
 template <int L>
 __global__ void k_clear_status(Dev P)
 {
+	constexpr int NL = 2 * L + 1;
 	pdl_enter();
 	d_clear_status<L>(P, hw_grid());
+	if (!last_block(&P.counters[CNT_LDONE])) return;
+	for (int i = threadIdx.x; i < P.S * NL; i += blockDim.x) P.spcnt[i] = 0;
+	if (threadIdx.x == 0) P.counters[CNT_SUNION] = 0;
 }
 
 /// Affected buffer reset: clears the leaf lookups and lists of buffer b.
@@ -2399,6 +2425,8 @@ __global__ void k_clear_buffer(Dev P, int b, int scan_here)
 		woff = swoff;
 	}
 	d_clear_buffer<L>(P, b, hw_grid(), woff);
+	if (!last_block(&P.counters[CNT_LDONE])) return;
+	for (int i = threadIdx.x; i < P.S * NL; i += blockDim.x) P.apcnt[b][i] = 0;
 }
 
 /// Returns the bricks of partitions deactivated in this iteration to the free pool.
@@ -2417,6 +2445,7 @@ static __global__ void k_retire(Dev P)
 {
 	pdl_enter();
 	d_retire(P, hw_grid());
+	if (last_block(&P.counters[CNT_LDONE]) && threadIdx.x == 0) P.counters[CNT_RETIRE] = 0;
 }
 
 /// Copies the isogrid partition lists to the delta partition lists (track_children of the

@@ -85,7 +85,7 @@ typedef struct fg_config {
 	                          first pass of the next), 3 as two launches: every pass of a
 	                          brick in shared memory, the brick staged with a halo of 2L
 	                          nodes (where that fits and reaches only the next partitions;
-	                          elsewhere as 1); 0 = automatic                                 */
+	                          elsewhere as 1); 0 = automatic (= 1)                           */
 	int reserved[2];
 } fg_config;
 
