@@ -768,15 +768,16 @@ private:
 	/// flush, expansion and, in the global update, the reset of buffer cur.
 	void iteration(bool local, int cur, int oth)
 	{
-		clear_status();
 		// the fused passes (lookup given) on the global update's iterations only
 		const ListView bv{P_.aplist[cur], P_.apcnt[cur], P_.alst[cur], P_.acnt[cur],
 		                  local ? nullptr : P_.alkp[cur], P_.appos[cur]};
-		distance_passes(bv, oth);
+		distance_passes(bv, oth, true);  // with the status reset (clear_status)
 		flush();
 		expand();
-		retire();
-		if (!local) clear_buffer(cur);
+		if (local)
+			retire();
+		else
+			clear_buffer(cur, true);  // with the brick retirement (retire)
 	}
 
 	/// The global update's iteration as a CUDA graph, captured on first use (one per buffer
@@ -1387,14 +1388,19 @@ private:
 	/// The 2L layer passes of update_distance (Surface.hpp:989-1125). The pass lists do not
 	/// change while the passes run (they append to the other buffer), so one launch scans the
 	/// entry offsets of every layer up front.
-	void distance_passes(const ListView& lv, int b)
+	/// clear_status: the iteration's status reset runs in the entry-table launch (in place of
+	/// k_clear_status).
+	void distance_passes(const ListView& lv, int b, bool clear_status = false)
 	{
-		// entry offsets of every layer, then the entries decoded; one launch for small pools
-		const bool small = P_.S <= 32;
-		if (!small)
+		// entry offsets of every layer, then the entries decoded; one launch for pools of up to
+		// kScanHereMax surfaces
+		const bool here = P_.S <= kScanHereMax;
+		if (!here)
 			FG_RUN("k_scan_layers", st_, launch_pdl((k_scan_layers), 1, 1024, 0, st_, lv.pcnt, NL, P_.S, P_.woffl, P_.sfrozen););
 		const bool tiled = tiled_ && lv.lkp && lv.ppos;
-		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table), sm_count() * 4, 256, 0, st_, P_, lv.plist, lv.lcnt, NL, L, small ? lv.pcnt : nullptr, lv.ppos, tiled ? P_.dq : nullptr););
+		const size_t sm = here ? (size_t)NL * (P_.S + 1) * sizeof(int) : 0;
+		FG_RUN("k_entry_table", st_, launch_pdl((k_entry_table<L>), sm_count() * 4, 256, sm, st_, P_, lv.plist, lv.lcnt, here ? lv.pcnt : nullptr, lv.ppos, tiled ? P_.dq : nullptr, clear_status ? 1 : 0););
+		if (clear_status) status_dirty_ = false;
 		if (tiled) {
 			tiled_passes(lv, b);
 			return;
@@ -1527,12 +1533,15 @@ private:
 		status_dirty_ = false;
 	}
 
-	void clear_buffer(int b)
+	/// retire_too: the iteration's brick retirement runs in the same launch (in place of
+	/// k_retire).
+	void clear_buffer(int b, bool retire_too = false)
 	{
-		const bool small = P_.S <= 32;
-		if (!small) scan(P_.apcnt[b], 0, 2);
-		// its last block resets the buffer's partition counts
-		FG_RUN("k_clear_buffer", st_, launch_pdl((k_clear_buffer<L>), warp_grid_, 256, 0, st_, P_, b, small ? 1 : 0););
+		const bool here = P_.S <= kScanHereMax;
+		if (!here) scan(P_.apcnt[b], 0, 2);
+		const size_t sm = here ? (size_t)(P_.S + 1) * sizeof(int) : 0;
+		// its last block resets the buffer's partition counts (and the retire queue)
+		FG_RUN("k_clear_buffer", st_, launch_pdl((k_clear_buffer<L>), warp_grid_, 256, sm, st_, P_, b, here ? 1 : 0, retire_too ? 1 : 0););
 		buf_dirty_[b] = false;
 	}
 

@@ -192,69 +192,10 @@ static __global__ void k_scan_layers(const int* cnt, int NL, int S, int* woffl, 
 	d_scan_layers(cnt, NL, S, woffl, frozen);
 }
 
-/// The entries of the distance passes decoded once per iteration, and Dev::changed cleared for
-/// the passes: for every layer but the zero
-/// layer and every entry e of its list (entry offsets woffl), {partition, brick slot, surface,
-/// leaves in the brick's list} at etab[l*NP + e]. The passes then start from one 16-byte load
-/// instead of the chain entry offsets -> partition list -> slot -> list count.
-///
-/// pcnt given (a pool of at most 32 surfaces): the entry offsets are scanned here too, every
-/// block for itself (a warp per layer) and block 0 for the passes (Dev::woffl), in place of
-/// k_scan_layers.
-///
-/// dq given (tiled distance passes, ppos the lists' partition positions): every partition of the
-/// passes is queued once, at its entry in the lowest layer index whose list holds it, and every
-/// entry's flags (Dev::eflagl) start at zero.
-static __global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, int NL, int L,
-                                     const int* pcnt, const int* ppos = nullptr,
-                                     int* dq = nullptr)
-{
-	__shared__ int lo[10];          // the layers' entries concatenated: layer l from lo[l]
-	__shared__ int swoff[9 * 33];   // the offsets, when scanned here
-	pdl_enter();
-	// the passes' status-change flag starts at zero (nothing before the passes reads it)
-	if (blockIdx.x == 0 && threadIdx.x == 0) *P.changed = 0;
-	const int* woffl = P.woffl;
-	if (pcnt) {
-		for (int w = threadIdx.x >> 5; w < NL; w += blockDim.x >> 5) {
-			warp_scan_counts(pcnt, NL, w, 0, P.S, swoff + w * (P.S + 1), P.sfrozen);
-			__syncwarp();
-			if (blockIdx.x == 0)
-				for (int i = lane_id(); i <= P.S; i += 32)
-					P.woffl[(size_t)w * (P.S + 1) + i] = swoff[w * (P.S + 1) + i];
-		}
-		__syncthreads();
-		woffl = swoff;
-	}
-	if (threadIdx.x == 0) {
-		int c = 0;
-		for (int l = 0; l < NL; l++) {
-			lo[l] = c;
-			if (l != L) c += woffl[(size_t)l * (P.S + 1) + P.S];
-		}
-		lo[NL] = c;
-	}
-	__syncthreads();
-	const int total = lo[NL];
-	for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-		int l = 0;
-		while (t >= lo[l + 1]) l++;
-		const int e = t - lo[l];
-		const int* woff = woffl + (size_t)l * (P.S + 1);
-		const int s = entry_surface(woff, P.S, e);
-		const SurfGeom& g = P.geom[s];
-		const int gp = g.pbase + plist[(size_t)l * P.NP + g.pbase + (e - woff[s])];
-		const int sl = P.slot[gp];
-		P.etab[(size_t)l * P.NP + e] = make_int4(gp, sl, s, lcnt[sl * NL + l]);
-		if (dq) {
-			P.eflagl[(size_t)l * P.NP + e] = 0;
-			bool first = true;
-			for (int l2 = 0; l2 < l; l2++)
-				if (l2 != L && ppos[gp * NL + l2] >= 0) first = false;
-			if (first) dq[atomicAdd(&P.counters[CNT_DQ], 1)] = gp;
-		}
-	}
-}
+/// Entry-offset scans run inside the kernel that needs them, every block for itself from
+/// shared memory, for pools of at most this many surfaces; larger pools scan in a launch of
+/// their own.
+constexpr int kScanHereMax = 512;
 
 /// The block index and block count a kernel body works with (the hardware grid's, or another
 /// grid dimension's where the launch is two-dimensional).
@@ -2383,6 +2324,74 @@ __global__ void k_clear_status(Dev P)
 	if (threadIdx.x == 0) P.counters[CNT_SUNION] = 0;
 }
 
+/// The entries of the distance passes decoded once per iteration, and Dev::changed cleared for
+/// the passes: for every layer but the zero layer and every entry e of its list (entry offsets
+/// woffl), {partition, brick slot, surface, leaves in the brick's list} at etab[l*NP + e]. The
+/// passes then start from one 16-byte load instead of the chain entry offsets -> partition
+/// list -> slot -> list count.
+///
+/// pcnt given (a pool of at most kScanHereMax surfaces): the entry offsets are scanned here too,
+/// every block for itself into dynamic shared memory (NL*(S+1) ints) and block 0 for the passes
+/// (Dev::woffl), in place of k_scan_layers.
+///
+/// clear_status: the iteration's status reset (k_clear_status's work, the status lists of the
+/// previous iteration) runs here too; nothing this kernel reads is status data.
+///
+/// dq given (tiled distance passes, ppos the lists' partition positions): every partition of the
+/// passes is queued once, at its entry in the lowest layer index whose list holds it, and every
+/// entry's flags (Dev::eflagl) start at zero.
+template <int L>
+__global__ void k_entry_table(Dev P, const int* plist, const int* lcnt, const int* pcnt,
+                              const int* ppos, int* dq, int clear_status)
+{
+	constexpr int NL = 2 * L + 1;
+	extern __shared__ int swoff[];  // the offsets, when scanned here
+	__shared__ int lo[NL + 1];      // the layers' entries concatenated: layer l from lo[l]
+	pdl_enter();
+	// the passes' status-change flag starts at zero (nothing before the passes reads it)
+	if (blockIdx.x == 0 && threadIdx.x == 0) *P.changed = 0;
+	if (clear_status) d_clear_status<L>(P, hw_grid());
+	const int* woffl = P.woffl;
+	if (pcnt) {
+		d_scan_layers(pcnt, NL, P.S, swoff, P.sfrozen);
+		if (blockIdx.x == 0)
+			for (int i = threadIdx.x; i < NL * (P.S + 1); i += blockDim.x) P.woffl[i] = swoff[i];
+		woffl = swoff;
+	}
+	if (threadIdx.x == 0) {
+		int c = 0;
+		for (int l = 0; l < NL; l++) {
+			lo[l] = c;
+			if (l != L) c += woffl[(size_t)l * (P.S + 1) + P.S];
+		}
+		lo[NL] = c;
+	}
+	__syncthreads();
+	const int total = lo[NL];
+	for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+		int l = 0;
+		while (t >= lo[l + 1]) l++;
+		const int e = t - lo[l];
+		const int* woff = woffl + (size_t)l * (P.S + 1);
+		const int s = entry_surface(woff, P.S, e);
+		const SurfGeom& g = P.geom[s];
+		const int gp = g.pbase + plist[(size_t)l * P.NP + g.pbase + (e - woff[s])];
+		const int sl = P.slot[gp];
+		P.etab[(size_t)l * P.NP + e] = make_int4(gp, sl, s, lcnt[sl * NL + l]);
+		if (dq) {
+			P.eflagl[(size_t)l * P.NP + e] = 0;
+			bool first = true;
+			for (int l2 = 0; l2 < l; l2++)
+				if (l2 != L && ppos[gp * NL + l2] >= 0) first = false;
+			if (first) dq[atomicAdd(&P.counters[CNT_DQ], 1)] = gp;
+		}
+	}
+	if (clear_status && last_block(&P.counters[CNT_LDONE])) {
+		for (int i = threadIdx.x; i < P.S * NL; i += blockDim.x) P.spcnt[i] = 0;
+		if (threadIdx.x == 0) P.counters[CNT_SUNION] = 0;
+	}
+}
+
 /// Affected buffer reset: clears the leaf lookups and lists of buffer b.
 template <int L>
 __device__ void d_clear_buffer(const Dev& P, int b, GridPos G, const int* woff)
@@ -2410,24 +2419,7 @@ __device__ void d_clear_buffer(const Dev& P, int b, GridPos G, const int* woff)
 		if (lane == 0) P.appos[b][gp * NL + t] = -1;
 	}
 }
-/// scan_here (a pool of at most 32 surfaces): every block scans the buffer's entry offsets
-/// itself (one warp), in place of a k_scan_counts launch before.
-template <int L>
-__global__ void k_clear_buffer(Dev P, int b, int scan_here)
-{
-	constexpr int NL = 2 * L + 1;
-	__shared__ int swoff[33];
-	pdl_enter();
-	const int* woff = P.woff;
-	if (scan_here) {
-		if (threadIdx.x < 32) warp_scan_counts(P.apcnt[b], NL, 0, 2, P.S, swoff, P.sfrozen);
-		__syncthreads();
-		woff = swoff;
-	}
-	d_clear_buffer<L>(P, b, hw_grid(), woff);
-	if (!last_block(&P.counters[CNT_LDONE])) return;
-	for (int i = threadIdx.x; i < P.S * NL; i += blockDim.x) P.apcnt[b][i] = 0;
-}
+
 
 /// Returns the bricks of partitions deactivated in this iteration to the free pool.
 static __device__ __forceinline__ void d_retire(const Dev& P, GridPos G)
@@ -2446,6 +2438,29 @@ static __global__ void k_retire(Dev P)
 	pdl_enter();
 	d_retire(P, hw_grid());
 	if (last_block(&P.counters[CNT_LDONE]) && threadIdx.x == 0) P.counters[CNT_RETIRE] = 0;
+}
+
+/// The affected buffer reset (d_clear_buffer). scan_here (a pool of at most kScanHereMax
+/// surfaces): every block scans the buffer's entry offsets itself into dynamic shared memory
+/// (S+1 ints), in place of a k_scan_counts launch before. retire_too: the iteration's brick
+/// retirement (k_retire's work, which touches no buffer data) runs here too. The last block
+/// resets the buffer's partition counts (and the retire queue).
+template <int L>
+__global__ void k_clear_buffer(Dev P, int b, int scan_here, int retire_too)
+{
+	constexpr int NL = 2 * L + 1;
+	extern __shared__ int swoff[];
+	pdl_enter();
+	if (retire_too) d_retire(P, hw_grid());
+	const int* woff = P.woff;
+	if (scan_here) {
+		d_scan_counts(P.apcnt[b], NL, 0, 2, P.S, swoff, P.sfrozen);
+		woff = swoff;
+	}
+	d_clear_buffer<L>(P, b, hw_grid(), woff);
+	if (!last_block(&P.counters[CNT_LDONE])) return;
+	for (int i = threadIdx.x; i < P.S * NL; i += blockDim.x) P.apcnt[b][i] = 0;
+	if (retire_too && threadIdx.x == 0) P.counters[CNT_RETIRE] = 0;
 }
 
 /// Copies the isogrid partition lists to the delta partition lists (track_children of the
