@@ -1374,8 +1374,7 @@ private:
 
 	void copy_plists()
 	{
-		dim3 grid(1, P_.S * NL);
-		if (grid.y > 65535) throw Error(-1, "too many surfaces for one pool");
+		dim3 grid(1, std::min(P_.S * NL, sm_count() * 8));  // blocks loop over (surface, list)
 		FG_RUN("k_copy_plists", st_, launch_pdl((k_copy_plists), grid, 256, 0, st_, P_, NL););
 	}
 
@@ -1505,7 +1504,9 @@ private:
 			FG_RUN("k_flush_smem", st_, launch_pdl((k_flush_smem<D, L>), sm_count() * 8, 256, smem_flush_, st_, P_););
 		else
 			FG_RUN("k_flush_leaf", st_, launch_pdl((k_flush_leaf<D, L>), grid_for(P_.NP), 128, 0, st_, P_););
-		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), P_.S * NL, 1024, 0, st_, P_););
+		// a block per (surface, list), looping where there are more than two per SM: in a large
+		// batch most have no events and leave at once, without a block launch each
+		FG_RUN("k_flush_plist", st_, launch_pdl((k_flush_plist<L>), std::min(P_.S * NL, sm_count() * 2), 1024, 0, st_, P_););
 	}
 
 	/// The status lists' entry offsets and the counters were prepared by the last compaction
@@ -1517,7 +1518,7 @@ private:
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 1););
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 2););
 		FG_RUN("k_expand_append", st_, launch_pdl((k_expand_append<L>), sm_count() * 4, 256, smem_sort_, st_, P_););
-		FG_RUN("k_expand_plist", st_, launch_pdl((k_expand_plist<L>), P_.S, 256, 0, st_, P_););
+		FG_RUN("k_expand_plist", st_, launch_pdl((k_expand_plist<L>), std::min(P_.S, sm_count() * 8), 256, 0, st_, P_););
 	}
 
 	void retire()

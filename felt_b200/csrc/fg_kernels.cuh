@@ -700,6 +700,7 @@ __device__ void compact_surface(const Dev& P, const CompactArgs& a, int s)
 	const unsigned* ef = a.ef ? a.ef : P.eflag;
 	const SurfGeom& g = P.geom[s];
 	const int e0 = a.woff[s], e1 = a.woff[s + 1];
+	if (e0 == e1) return;  // no entries in this pass: every count stays as it is
 	const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const unsigned lt = (1u << lane) - 1u;
 	if (threadIdx.x <= NL)
@@ -1903,7 +1904,10 @@ __device__ bool flush_plist_fast(const Dev& P, int s, int k, int* ev_lp, unsigne
 	return true;
 }
 
-/// Children-level half of the flush: one block per (surface, list k).
+/// Children-level half of the flush: a block per (surface, list k), looping over pairs
+/// w = bid, bid + nb, ... Warp 0 first checks 32 of the block's pairs at once for events (the
+/// surface's status lists non-empty); the block then replays only those, so that the pairs of a
+/// large batch's converged surfaces cost one load each.
 template <int L>
 __device__ void d_flush_plist(const Dev& P, GridPos G)
 {
@@ -1914,10 +1918,30 @@ __device__ void d_flush_plist(const Dev& P, GridPos G)
 	__shared__ int wnd[ECAP];
 	__shared__ int hkey[HCAP];
 	__shared__ int hval[HCAP];
-	for (int w = G.bid; w < P.S * NL; w += G.nb) {
-		const int s = w / NL, k = w % NL;
-		if (!flush_plist_fast<L, ECAP, HCAP>(P, s, k, ev_lp, ev_kind, wnd, hkey, hval))
-			flush_plist_serial<L, ECAP>(P, s, k, ev_lp, ev_kind);
+	__shared__ unsigned busy_s;
+	const int npairs = P.S * NL;
+	for (int j0 = 0; G.bid + j0 * G.nb < npairs; j0 += 32) {
+		if (threadIdx.x < 32) {
+			const int w = G.bid + (j0 + (int)threadIdx.x) * G.nb;
+			int T = 0;
+			if (w < npairs) {
+				const int s = w / NL;
+				for (int fi = 0; fi < NL; fi++) T += P.spcnt[s * NL + fi];
+			}
+			const unsigned m = __ballot_sync(FULL, T != 0);
+			if (threadIdx.x == 0) busy_s = m;
+		}
+		__syncthreads();
+		unsigned m = busy_s;
+		__syncthreads();
+		while (m) {
+			const int i = __ffs(m) - 1;
+			m &= m - 1;
+			const int w = G.bid + (j0 + i) * G.nb;
+			const int s = w / NL, k = w - s * NL;
+			if (!flush_plist_fast<L, ECAP, HCAP>(P, s, k, ev_lp, ev_kind, wnd, hkey, hval))
+				flush_plist_serial<L, ECAP>(P, s, k, ev_lp, ev_kind);
+		}
 	}
 }
 template <int L>
