@@ -1518,13 +1518,14 @@ private:
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 1););
 		FG_RUN("k_expand_gen", st_, launch_pdl((k_expand_gen<D, L>), warp_grid_, 256, 0, st_, P_, 2););
 		FG_RUN("k_expand_append", st_, launch_pdl((k_expand_append<L>), sm_count() * 4, 256, smem_sort_, st_, P_););
-		FG_RUN("k_expand_plist", st_, launch_pdl((k_expand_plist<L>), std::min(P_.S, sm_count() * 8), 256, 0, st_, P_););
+		// the partition-list appends (d_expand_plist) run in the launch after, which retires
+		// bricks (k_retire, or k_clear_buffer with retire_too)
 	}
 
 	void retire()
 	{
 		// its last block resets the retire queue
-		FG_RUN("k_retire", st_, launch_pdl((k_retire), grid_for(P_.nslots), 256, 0, st_, P_););
+		FG_RUN("k_retire", st_, launch_pdl((k_retire<L>), std::max(grid_for(P_.nslots), std::min(P_.S, sm_count() * 8)), 256, 0, st_, P_););
 	}
 
 	void clear_status()

@@ -2457,25 +2457,33 @@ static __device__ __forceinline__ void d_retire(const Dev& P, GridPos G)
 		P.free_stack[atomicAdd(&P.counters[CNT_FREE_TOP], 1)] = sl;
 	}
 }
-static __global__ void k_retire(Dev P)
+/// The tail of an iteration after the expansion: its partition-list appends (d_expand_plist,
+/// which touch no brick of the retire queue) and the brick retirement, in one launch.
+template <int L>
+__global__ void k_retire(Dev P)
 {
 	pdl_enter();
+	d_expand_plist<L>(P, hw_grid());
 	d_retire(P, hw_grid());
 	if (last_block(&P.counters[CNT_LDONE]) && threadIdx.x == 0) P.counters[CNT_RETIRE] = 0;
 }
 
 /// The affected buffer reset (d_clear_buffer). scan_here (a pool of at most kScanHereMax
 /// surfaces): every block scans the buffer's entry offsets itself into dynamic shared memory
-/// (S+1 ints), in place of a k_scan_counts launch before. retire_too: the iteration's brick
-/// retirement (k_retire's work, which touches no buffer data) runs here too. The last block
-/// resets the buffer's partition counts (and the retire queue).
+/// (S+1 ints), in place of a k_scan_counts launch before. retire_too: the iteration's
+/// expansion partition appends and brick retirement (k_retire's work, which touches no buffer
+/// data) run here too. The last block resets the buffer's partition counts (and the retire
+/// queue).
 template <int L>
 __global__ void k_clear_buffer(Dev P, int b, int scan_here, int retire_too)
 {
 	constexpr int NL = 2 * L + 1;
 	extern __shared__ int swoff[];
 	pdl_enter();
-	if (retire_too) d_retire(P, hw_grid());
+	if (retire_too) {
+		d_expand_plist<L>(P, hw_grid());
+		d_retire(P, hw_grid());
+	}
 	const int* woff = P.woff;
 	if (scan_here) {
 		d_scan_counts(P.apcnt[b], NL, 0, 2, P.S, swoff, P.sfrozen);
