@@ -2325,10 +2325,26 @@ __device__ void d_clear_status(const Dev& P, GridPos G)
 		const int gp = P.q_sunion[e];
 		const int sl = P.slot[gp];
 		if (sl >= 0) {
-			for (int fi = 0; fi < NL; fi++) {
-				const int nc = P.ccnt[sl * NL + fi];
+			// every from-layer's count at once (lane fi), then the status lists' leaves as one
+			// flat range, so that the loads of all the lists are in flight together
+			const int c = lane < NL ? P.ccnt[sl * NL + lane] : 0;
+			int inc = c;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const int y = __shfl_up_sync(FULL, inc, o);
+				if (lane >= o) inc += y;
+			}
+			const int tot = __shfl_sync(FULL, inc, NL - 1);
+			int exf[NL];  // first flat index of from-layer f
+#pragma unroll
+			for (int f = 0; f < NL; f++) exf[f] = __shfl_sync(FULL, inc - c, f);
+			for (int i = lane; i < tot; i += 32) {
+				int fi = 0;
+#pragma unroll
+				for (int f = 1; f < NL; f++)
+					if (exf[f] <= i) fi = f;
 				const uint16_t* ch = P.chg + ((size_t)sl * NL + fi) * P.BV;
-				for (int c = lane; c < nc; c += 32) P.sto[(size_t)sl * P.BV + ch[c]] = (int8_t)(L + 1);
+				P.sto[(size_t)sl * P.BV + ch[i - exf[fi]]] = (int8_t)(L + 1);
 			}
 			__syncwarp();
 			if (lane < NL) P.ccnt[sl * NL + lane] = 0;
@@ -2425,12 +2441,19 @@ __device__ void d_clear_buffer(const Dev& P, int b, GridPos G, const int* woff)
 	{
 		const int s = entry_surface(woff, P.S, e);
 		const SurfGeom& g = P.geom[s];
-		int i = e - woff[s];
-		int t = 0;
-		while (i >= P.apcnt[b][s * NL + t]) {
-			i -= P.apcnt[b][s * NL + t];
-			t++;
+		// the list t of entry e: the surface's list counts loaded at once (lane t) and summed
+		// with shuffles, instead of one dependent load per list passed
+		const int i0 = e - woff[s];
+		const int cl = lane < NL ? P.apcnt[b][s * NL + lane] : 0;
+		int inc = cl;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int y = __shfl_up_sync(FULL, inc, o);
+			if (lane >= o) inc += y;
 		}
+		const unsigned past = __ballot_sync(FULL, lane < NL && inc <= i0);
+		const int t = __popc(past);  // lists that end at or before i0
+		const int i = i0 - __shfl_sync(FULL, inc - cl, t < NL ? t : NL - 1);
 		const int gp = g.pbase + P.aplist[b][(size_t)t * P.NP + g.pbase + i];
 		const int sl = P.slot[gp];
 		if (sl >= 0) {
