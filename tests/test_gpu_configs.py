@@ -187,6 +187,12 @@ def test_c4_first8_surfaces_of_the_batch():
     _batch_config("c4", 8, 100, 0, True)
 
 
+def test_c4_first40_surfaces_block_scans():
+    """40 surfaces of the 3D batch, 12 steps: a pool of more than 32 surfaces, whose entry
+    offsets are scanned by whole blocks inside the entry-table and buffer-reset launches."""
+    _batch_config("c4", 40, 12, 0, True)
+
+
 def test_c1_with_marching_cubes():
     fb = _fb()
     size, part, L = (64, 64, 64), (8, 8, 8), 2
