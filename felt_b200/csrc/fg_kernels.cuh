@@ -853,7 +853,6 @@ __device__ void d_dist2(const Dev& P, const int* woff, ListView lv, int k, int b
 	const int total = woff[P.S];
 	for (int e = G.bid; e < total; e += G.nb) {
 		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
-		const SurfGeom& g = P.geom[et.z];
 		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
@@ -900,7 +899,6 @@ __device__ void d_dist2_warp(const Dev& P, const int* woff, ListView lv, int k, 
 	FG_WARP_LOOP(woff)
 	{
 		const int4 et = P.etab[(size_t)li * P.NP + e];  // entry_table
-		const SurfGeom& g = P.geom[et.z];
 		const int gp = et.x, sl = et.y, n = et.w;
 		const uint16_t* lst = lv.lst + ((size_t)sl * NL + li) * P.BV;
 		const size_t b0 = (size_t)sl * P.BV;
